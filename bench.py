@@ -1,0 +1,313 @@
+"""Benchmark of the reference's headline metric on the B200 path.
+
+Workload (the configuration the reference's PID metric is quoted on here): compressible
+Navier-Stokes Taylor-Green vortex, FP64, N=7, 32^3 hexahedra on [-pi,pi]^3 with interior nodes
+deformed by 0.05*sin(x)sin(y)sin(z) (NGeo=2, curved metrics), Re=1600 (mu0=1/1600), Ma=0.1,
+Pr=0.72, BR1 lifting of the entropy variables, EC-KEP split-form volume flux (VolumeFlux=5),
+entropy-stable matrix-dissipation surface flux (Riemann=44), Carpenter LSERK4-5, CFL 0.9, DFL 0.4.
+Synthetic data: the mesh and the initial state are generated in-code (no mesh file, no dataset).
+
+One step = CALCTIMESTEP + one 5-stage LSERK step (5 right-hand sides).  The metric is the
+reference's PID per RHS evaluation, ns per DOF per RHS (lower is better); `value` is the whole-job
+figure: timed seconds / (total DOFs over all ranks * RHS evaluations).  The state (671 MB) is
+larger than L2, so no extra flush is needed between steps.
+
+Multi-GPU: independent replicas, one per rank (weak scaling); the timed region is bracketed by a
+barrier + device synchronisation and the maximum over ranks is reported.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic FP64 operations per DOF of one right-hand side for this workload, from one RHS of
+# the CPU oracle's counting build (oracle/counted.h rules), split by the phase that each GPU
+# kernel implements.  tests/test_bench_constants.py re-derives these numbers.
+FALG_PER_DOF = {
+    "volume_split_form": 1124.5,
+    "lifting": 519.75,
+    "volume_viscous": 384.0,
+    "face_flux": 200.625,
+    "surface_integral": 7.5,
+    "jacobian_source": 5.0,
+}
+FALG_RK_STAGE_PER_DOF = 20.0  # Ut_tmp = Ut - A*Ut_tmp; U += b*dt*Ut_tmp (2+2 flops x 5 variables)
+VOLUME_KERNEL_FALG = (FALG_PER_DOF["volume_split_form"] + FALG_PER_DOF["volume_viscous"] +
+                      FALG_PER_DOF["surface_integral"] + FALG_PER_DOF["jacobian_source"] + FALG_RK_STAGE_PER_DOF)
+
+METRIC = "PID ns/DOF/RHS, NS Taylor-Green N=7 32^3 curved, BR1 + EC-KEP + ES (Riemann 44), LSERK4-5"
+
+
+def workload(elems=32, N=7):
+    return dict(N=N, elems=(elems,) * 3, xmin=(-np.pi,) * 3, xmax=(np.pi,) * 3, NGeo=2, deform_amp=0.05,
+                eqn=1, lifting=1, lifting_var=3, visc=0, riemann=44, volume_flux=5, mu0=1.0 / 1600.0, Pr=0.72,
+                kappa=1.4, ini_exact_func=7, cfl_scale=0.9, dfl_scale=0.4, time_disc=0)
+
+
+def config_dict(w, n_gpus, steps):
+    return {"workload": "navierstokes_tgv_N%d_%dx%dx%d_curved" % ((w["N"],) + w["elems"]), "N": w["N"],
+            "elements": list(w["elems"]), "dofs_per_gpu": int(np.prod(w["elems"]) * (w["N"] + 1) ** 3),
+            "riemann": w["riemann"], "volume_flux": w["volume_flux"], "lifting": "br1_entropy_var",
+            "time_disc": "carpenterrk4-5", "rhs_per_step": 5, "parallelism": "replicas x%d" % n_gpus,
+            "l2": "inputs larger than L2 (state 671 MB)", "steps": steps}
+
+
+# ------------------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(x, world, device):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ------------------------------------------------------------------------------------------------
+def cpu_baseline(threads, seconds=15.0):
+    """The oracle (a C++ restatement of the reference loop by loop, OpenMP over elements) timed on
+    the host cores on a bounded sample of the same workload: 4^3 elements of the N=7 TGV."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle.oracle import OracleCase
+
+    w = workload(elems=4)
+    c = OracleCase(N=w["N"], nElems=w["elems"], xmin=w["xmin"], xmax=w["xmax"], NGeo=w["NGeo"],
+                   deform_amp=w["deform_amp"], eqn=1, lifting=1, lifting_var=3, mu0=w["mu0"], riemann=44,
+                   volume_flux=5, ini_exact_func=7, cfl_scale=0.9, dfl_scale=0.4)
+    c.run(0.0, 1e9, max_iter=1)  # warm-up
+    nd = c.nElems * c.np ** 3
+    t0 = time.perf_counter()
+    steps = 0
+    while time.perf_counter() - t0 < seconds:
+        c.run(0.0, 1e9, max_iter=1)
+        steps += 1
+    el = time.perf_counter() - t0
+    pid = el / (nd * 5 * steps) * 1e9
+    return {"value": pid, "unit": "ns/DOF/RHS", "cores": threads, "kind": "port",
+            "sample": "oracle, TGV N=7 4x4x4 elements (32768 DOFs), %d LSERK4-5 steps in %.1f s" % (steps, el)}
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    steps = []
+    for _ in range(args.warmup):
+        cpu_baseline(threads, seconds=1.0)
+    for _ in range(args.steps):
+        steps.append(cpu_baseline(threads, seconds=max(2.0, 60.0 / max(args.steps, 1))))
+    vals = [s["value"] for s in steps]
+    v = float(np.median(vals))
+    w = workload()
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "ns/DOF/RHS", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(w, args.gpus, args.steps),
+            "cpu_baseline": dict(steps[-1], value=v),
+            "e2e": {"value": v, "unit": "ns/DOF/RHS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference Fortran not buildable here (no Fortran compiler/MPI/HDF5); its C++ restatement "
+                    "(oracle) runs on %d host threads" % threads}
+    print(json.dumps(line))
+
+
+def run_fluxo(args):
+    import torch
+
+    import fluxo_b200 as fb
+    from fluxo_b200.solver import fp64_peak, get_state_ptr, profile, set_profiling, set_state_ptr
+
+    world, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = workload(elems=args.elems, N=args.N)
+    t0 = time.time()
+    mesh = fb.box_mesh(w["N"], w["elems"], w["xmin"], w["xmax"], NGeo=w["NGeo"], deform_amp=w["deform_amp"])
+    op = fb.DGOperator(N=w["N"], eqn=1, riemann=w["riemann"], volume_flux=w["volume_flux"], lifting=1,
+                       lifting_var=3, visc=0, mu0=w["mu0"], Pr=w["Pr"], kappa=w["kappa"],
+                       cfl_scale=w["cfl_scale"], dfl_scale=w["dfl_scale"], time_disc=0, device=local)
+    op.set_mesh(mesh)
+    U0 = fb.exact_func(7, 0.0, mesh["Elem_xGP"], kappa=w["kappa"])
+    del mesh
+    op.set_state(U0)
+    setup_s = time.time() - t0
+    nd = op.nElems * (w["N"] + 1) ** 3
+    _, _, stream_ptr = op.device_buffers()
+    stream = torch.cuda.ExternalStream(stream_ptr, device=dev)
+    peak = fp64_peak(local)
+
+    t = 0.0
+    t, n, err = op.time_disc(t, 1e30, args.warmup)
+    assert err == 0 and n == args.warmup
+
+    # ---- device-resident timed region ----
+    n0 = op.launch_count()
+    set_profiling(op, True)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        t, n, err = op.time_disc(t, 1e30, args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    barrier(world)
+    assert err == 0 and n == args.steps, (err, n)
+    ms = ev0.elapsed_time(ev1)
+    launches = op.launch_count() - n0
+    vol_ms, vol_n = profile(op, 3)
+    kinds = {k: profile(op, i) for i, k in enumerate(("lift_flux", "gradient", "face_flux", "volume", "timestep"))
+             if i != 3}
+    kinds["volume"] = (vol_ms, vol_n)
+    set_profiling(op, False)
+    ms_max = max_over_ranks(ms, world, dev)
+    rhs = 5 * args.steps
+    value = ms_max * 1e6 / (world * nd * rhs)
+
+    # ---- end-to-end through the public API with pinned host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        hostU = torch.empty(nd * 5, dtype=torch.float64, pin_memory=True)
+        get_state_ptr(op, hostU.data_ptr())
+        e2e_steps = max(2, min(args.steps, 5))
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            set_state_ptr(op, hostU.data_ptr())
+            t, n, err = op.time_disc(t, 1e30, 1)
+            get_state_ptr(op, hostU.data_ptr())
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        ems = max_over_ranks(e0.elapsed_time(e1), world, dev)
+        e2e = {"value": ems * 1e6 / (world * nd * 5 * e2e_steps), "unit": "ns/DOF/RHS",
+               "h2d_bytes_per_step": nd * 5 * 8, "d2h_bytes_per_step": nd * 5 * 8, "steps": e2e_steps,
+               "path": "fluxo_gpu_set_state + fluxo_gpu_time_disc(1 step) + fluxo_gpu_get_state, pinned host"}
+
+    if rank != 0:
+        op.close()
+        return
+    vol_avg_ms = vol_ms / max(vol_n, 1)
+    achieved = VOLUME_KERNEL_FALG * nd / (vol_avg_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp64", "kernel": "volume_kernel<8,5,true>", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "flops_per_dof_launch": VOLUME_KERNEL_FALG, "launch_ms": vol_avg_ms,
+                "peak_source": "measured in this job: DFMA loop (fluxo_gpu_fp64_peak); MEASURED_PEAKS.json has no FP64"}
+    line = {"metric": METRIC, "value": value, "unit": "ns/DOF/RHS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(w, world, args.steps), "roofline": roofline, "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clk.summary(),
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kinds.items()},
+            "rhs_roofline_frac": (sum(FALG_PER_DOF.values()) * nd * rhs / (ms * 1e-3) / 1e12) / peak,
+            "setup_s": setup_s}
+    if world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1, seconds=args.cpu_seconds)
+    print(json.dumps(line))
+    op.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fluxo", choices=("fluxo", "reference"))
+    ap.add_argument("--elems", type=int, default=32)
+    ap.add_argument("--N", type=int, default=7)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_fluxo(args)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

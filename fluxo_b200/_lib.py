@@ -1,0 +1,112 @@
+"""ctypes binding of ``libfluxo_gpu.so`` (the C ABI declared in ``include/fluxo_gpu.h``).
+
+The library is built in-tree by ``fluxo_b200/build.py``.  There is no fallback: if the
+library is missing or fails to load, importing this module raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfluxo_gpu.so")
+
+FLUXO_OK = 0
+ERRORS = {
+    -1: "FLUXO_EINVAL_CFG",
+    -2: "FLUXO_ENOMEM_HBM",
+    -3: "FLUXO_ECUDA",
+    -4: "FLUXO_ENAN_STATE",
+    -5: "FLUXO_ETIMEOUT",
+    -6: "FLUXO_ENOTREADY",
+}
+
+
+class FluxoError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (ERRORS.get(code, "FLUXO_E?"), code, msg))
+        self.code = code
+
+
+class FluxoCfg(ctypes.Structure):
+    _fields_ = [
+        ("struct_size", ctypes.c_int),
+        ("N", ctypes.c_int),
+        ("eqn", ctypes.c_int),
+        ("riemann", ctypes.c_int),
+        ("volume_flux", ctypes.c_int),
+        ("lifting", ctypes.c_int),
+        ("lifting_var", ctypes.c_int),
+        ("visc", ctypes.c_int),
+        ("kappa", ctypes.c_double),
+        ("R", ctypes.c_double),
+        ("Pr", ctypes.c_double),
+        ("mu0", ctypes.c_double),
+        ("Ts", ctypes.c_double),
+        ("Tref", ctypes.c_double),
+        ("ExpoSuth", ctypes.c_double),
+        ("ExpoPow", ctypes.c_double),
+        ("etaBR2", ctypes.c_double),
+        ("time_disc", ctypes.c_int),
+        ("cfl_scale", ctypes.c_double),
+        ("dfl_scale", ctypes.c_double),
+        ("ini_exact_func", ctypes.c_int),
+        ("ini_frequency", ctypes.c_double),
+        ("ini_amplitude", ctypes.c_double),
+        ("device", ctypes.c_int),
+    ]
+
+
+EXPORTS = [
+    "fluxo_gpu_create", "fluxo_gpu_set_mesh", "fluxo_gpu_set_state", "fluxo_gpu_get_state", "fluxo_gpu_get_ut",
+    "fluxo_gpu_get_gradients", "fluxo_gpu_dg_time_derivative", "fluxo_gpu_calc_timestep", "fluxo_gpu_timestep",
+    "fluxo_gpu_time_disc", "fluxo_gpu_device_buffers", "fluxo_gpu_launch_count", "fluxo_gpu_destroy",
+    "fluxo_gpu_last_error", "fluxo_gpu_set_profiling", "fluxo_gpu_get_profile", "fluxo_gpu_fp64_peak",
+    "fluxo_host_box_sizes", "fluxo_host_box_mesh", "fluxo_host_exact_func",
+]
+
+_lib = None
+
+
+def load():
+    """Loads the library once and declares the argument types of every export."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libfluxo_gpu.so not built (run fluxo_b200/build.py): " + LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, i, d, P = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.POINTER
+    lib.fluxo_gpu_create.argtypes = [P(FluxoCfg), P(vp)]
+    lib.fluxo_gpu_set_mesh.argtypes = [vp, i, i] + [vp] * 11
+    lib.fluxo_gpu_set_state.argtypes = [vp, vp]
+    lib.fluxo_gpu_get_state.argtypes = [vp, vp]
+    lib.fluxo_gpu_get_ut.argtypes = [vp, vp]
+    lib.fluxo_gpu_get_gradients.argtypes = [vp, vp, vp, vp]
+    lib.fluxo_gpu_dg_time_derivative.argtypes = [vp, d]
+    lib.fluxo_gpu_calc_timestep.argtypes = [vp, P(d), P(i)]
+    lib.fluxo_gpu_timestep.argtypes = [vp, d, d]
+    lib.fluxo_gpu_time_disc.argtypes = [vp, d, d, i, P(d), P(i), P(i)]
+    lib.fluxo_gpu_device_buffers.argtypes = [vp, P(vp), P(vp), P(vp)]
+    lib.fluxo_gpu_launch_count.argtypes = [vp, P(ctypes.c_uint64)]
+    lib.fluxo_gpu_destroy.argtypes = [vp]
+    lib.fluxo_gpu_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+    lib.fluxo_gpu_set_profiling.argtypes = [vp, i]
+    lib.fluxo_gpu_get_profile.argtypes = [vp, i, P(d), P(ctypes.c_uint64)]
+    lib.fluxo_gpu_fp64_peak.argtypes = [i, P(d)]
+    lib.fluxo_host_box_sizes.argtypes = [vp, P(i), P(i)]
+    lib.fluxo_host_box_mesh.argtypes = [i, vp, vp, vp, i, d] + [vp] * 11
+    lib.fluxo_host_exact_func.argtypes = [i, d, ctypes.c_size_t, vp, d, vp, d, vp, d, vp, vp]
+    for name in EXPORTS:
+        getattr(lib, name).restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def last_error(h):
+    buf = ctypes.create_string_buffer(1024)
+    load().fluxo_gpu_last_error(h, buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def check(code, h=None):
+    if code != FLUXO_OK:
+        raise FluxoError(code, last_error(h))

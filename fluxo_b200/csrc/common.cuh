@@ -1,0 +1,77 @@
+// Shared definitions of the sm_100a FP64 DGSEM kernels.
+//
+// Device layouts (per handle, all FP64 unless noted):
+//   U, Ut, UtTmp   [elem][node][var]            var fastest = the reference's U(nVar,i,j,k,iElem)
+//   metrics        [elem][9][node]              Ja^1 (x,y,z), Ja^2 (x,y,z), Ja^3 (x,y,z), node fastest
+//   sJ             [elem][node]
+//   facegeo        [side][10][pt]               nx,ny,nz, t1x..t1z, t2x..t2z, SurfElem; pt = p + (N+1)*q
+//   flux           [side][var][pt]              Flux_master*SurfElem (slave flux is the same value)
+//   lflux          [side][var][pt]              lifting surface flux 0.5*(V_slave-V_master)*SurfElem
+//   grad           [elem][node][3][var]         primitive gradients (x,y,z) of Navier-Stokes
+//   s2e            [side][5]                    SideToElem, 0-based elements (-1 none)
+//   e2s            [elem][6][2]                 ElemToSide, 0-based side ids
+// node = i + (N+1)*(j + (N+1)*k).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define FLUXO_NPMAX 9  // N <= 8
+
+namespace fluxo {
+
+// local side ids of the reference (src/defines.h:67-72)
+enum { ZETA_MINUS = 1, ETA_MINUS = 2, XI_PLUS = 3, ETA_PLUS = 4, XI_MINUS = 5, ZETA_PLUS = 6 };
+
+// Per-N operator tables, filled on the host from the LGL basis (dg/dg.f90:181-252).
+struct BasisTables {
+  double Dvs[FLUXO_NPMAX * FLUXO_NPMAX];   // Dvolsurf(i,l) at [i*NP+l], diagonal forced to 0
+  double Dhat[FLUXO_NPMAX * FLUXO_NPMAX];  // D_hat(i,l) at [i*NP+l]
+  double D[FLUXO_NPMAX * FLUXO_NPMAX];     // D(i,l) at [i*NP+l]
+  double LhatM0;                           // L_HatMinus(0)
+  double wGP[FLUXO_NPMAX];
+  // face point -> volume node for (locSide-1, flip): node index, pt = p + NP*q  (mappings.f90 S2V, l=0)
+  int s2v[6][5][FLUXO_NPMAX * FLUXO_NPMAX];
+  // in-plane volume coordinates (a,b) -> face point for (locSide-1, flip); XI: (j,k), ETA: (i,k), ZETA: (i,j)
+  int v2s[6][5][FLUXO_NPMAX * FLUXO_NPMAX];
+};
+
+// Everything a kernel needs, passed by value.
+struct KParams {
+  int nElems, nSides;
+  // state
+  double* U;
+  double* Ut;
+  double* UtTmp;
+  double* grad;
+  // geometry
+  const double* metrics;
+  const double* sJ;
+  const double* facegeo;
+  const double* xGP;      // Elem_xGP [elem][node][3] or null
+  const int* s2e;
+  const int* e2s;
+  // face buffers
+  double* flux;
+  double* lflux;
+  double* gtrace;         // BR2 face gradient traces [side][master|slave][15][pt]
+  const BasisTables* basis;
+  // physics constants (navierstokes/equation.f90:162-260)
+  double kappa, kappaM1, sKappaM1, kappaP1, R, s23, KappasPr, mu0, Ts, sTref, ExpoSuth, cSuth, ExpoPow;
+  double etaBR2;
+  int visc, lifting_var, lifting;
+  // source term (IniExactFunc 4)
+  int source;
+  double srcOmega, srcTmp[6];
+  // time stepping
+  double t;               // stage time (host value) ...
+  const double* dtDev;    // ... or device dt (time_disc loop): dtDev[0]=dt, dtDev[1]=t
+  double dt;
+  double rkA, rkB, rkC;   // A_s, b_s, c_s of the current stage
+  int stage;              // 1-based stage; 0 = plain DGTimeDerivative (write Ut)
+  const int* haltFlag;    // device flag: nonzero -> kernels return at once
+  double CFLScale, DFLScale, KappasPrMax;
+};
+
+__device__ __forceinline__ bool halted(const KParams& P) { return P.haltFlag && *P.haltFlag != 0; }
+
+}  // namespace fluxo

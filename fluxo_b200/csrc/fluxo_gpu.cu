@@ -1,0 +1,654 @@
+// C ABI of the B200 DGSEM right-hand side / LSERK step (include/fluxo_gpu.h).
+// Host orchestration only: buffers, geometry repacking, kernel sequencing per RHS and per RK stage,
+// and the device-resident TimeDisc loop.  No numerical work happens on the host.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/fluxo_gpu.h"
+#include "common.cuh"
+#include "host_basis.h"
+#include "host_setup.h"
+#include "launch.h"
+
+using namespace fluxo;
+
+namespace {
+
+// State of the device-resident time loop (one per handle, in device memory).
+struct TDState {
+  double dt;                   // current step size (dtDev[0])
+  double t;                    // time at the start of the current step (dtDev[1])
+  double tEnd;
+  unsigned long long dtBits;   // CALCTIMESTEP result (bits of a non-negative double)
+  int errKey;                  // elem*8+errType of the first bad element, INT_MAX if none
+  int iter, maxIter, last, done, err;
+  int halt;                    // kernels return at once when nonzero
+};
+
+__global__ void td_begin_kernel(TDState* s, double t, double tEnd, int maxIter) {
+  s->t = t; s->tEnd = tEnd; s->dt = 0.; s->iter = 0; s->maxIter = maxIter;
+  s->last = 0; s->done = 0; s->err = 0;
+  s->halt = (t >= tEnd || maxIter == 0) ? 1 : 0;
+  if (s->halt) s->done = 1;
+  s->dtBits = 0x7FF0000000000000ull;
+  s->errKey = INT_MAX;
+}
+
+// after CALCTIMESTEP: error check and dt clipping to tEnd (timedisc.f90:289-317)
+__global__ void td_finalize_kernel(TDState* s) {
+  if (s->halt) return;
+  if (s->errKey != INT_MAX) { s->err = s->errKey & 7; s->halt = 1; return; }
+  double dt = __longlong_as_double((long long)s->dtBits);
+  s->last = 0;
+  if (s->tEnd - s->t <= dt * (1. + 1.e-4)) { dt = s->tEnd - s->t; s->last = 1; }
+  s->dt = dt;
+}
+
+// after the stages: t += dt, iteration count, termination (timedisc.f90:329-359)
+__global__ void td_advance_kernel(TDState* s) {
+  if (s->halt) return;
+  s->t = s->t + s->dt;
+  s->iter += 1;
+  if (s->last || (s->maxIter > 0 && s->iter >= s->maxIter)) { s->done = 1; s->halt = 1; }
+  s->dtBits = 0x7FF0000000000000ull;
+  s->errKey = INT_MAX;
+}
+
+__global__ void dt_reset_kernel(unsigned long long* bits, int* key) {
+  *bits = 0x7FF0000000000000ull;
+  *key = INT_MAX;
+}
+
+}  // namespace
+
+struct fluxo_handle {
+  fluxo_cfg cfg{};
+  int N = 0, NP = 0, nElems = 0, nSides = 0;
+  bool visc = false, meshSet = false, stateSet = false, haveXGP = false;
+  cudaStream_t stream = nullptr;
+  BasisTables hb{};
+  BasisTables* dBasis = nullptr;
+  double *dU = nullptr, *dUt = nullptr, *dUtTmp = nullptr, *dGrad = nullptr;
+  double *dMetrics = nullptr, *dsJ = nullptr, *dFaceGeo = nullptr, *dXGP = nullptr;
+  double *dFlux = nullptr, *dLFlux = nullptr, *dGTrace = nullptr;
+  int *dS2E = nullptr, *dE2S = nullptr;
+  TDState* dTD = nullptr;
+  unsigned long long* dDtBits = nullptr;
+  int* dErrKey = nullptr;
+  int nStages = 0;
+  double RKA[8]{}, RKb[8]{}, RKc[8]{};
+  double CFLScale = 0., DFLScale = 0.;
+  uint64_t launches = 0;
+  std::string lastError;
+  bool profiling = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof[5];
+};
+
+namespace {
+
+std::mutex g_err_mutex;
+std::string g_create_error;
+
+int fail(fluxo_handle* h, int code, const std::string& msg) {
+  if (h) h->lastError = msg;
+  else {
+    std::lock_guard<std::mutex> lk(g_err_mutex);
+    g_create_error = msg;
+  }
+  return code;
+}
+
+int cuda_fail(fluxo_handle* h, cudaError_t e, const char* where) {
+  return fail(h, FLUXO_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define FLUXO_CUDA(h, call)                                  \
+  do {                                                       \
+    cudaError_t _e = (call);                                 \
+    if (_e != cudaSuccess) return cuda_fail((h), _e, #call); \
+  } while (0)
+
+template <class T>
+int dalloc(fluxo_handle* h, T** p, size_t n) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(h, FLUXO_ENOMEM_HBM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  return FLUXO_OK;
+}
+
+void build_basis_tables(int N, BasisTables& B) {
+  host::LGLBasis b(N);
+  const int NP = N + 1;
+  std::memset(&B, 0, sizeof(B));
+  for (int i = 0; i < NP; ++i)
+    for (int l = 0; l < NP; ++l) {
+      B.Dvs[i * NP + l] = (i == l) ? 0. : b.Dvs[(size_t)i * NP + l];  // diagonal is zero (dg.f90:232-240)
+      B.Dhat[i * NP + l] = b.Dhat[(size_t)i * NP + l];
+      B.D[i * NP + l] = b.D[(size_t)i * NP + l];
+    }
+  B.LhatM0 = b.LhatM0;
+  for (int i = 0; i < NP; ++i) B.wGP[i] = b.w[i];
+  for (int s = 1; s <= 6; ++s)
+    for (int f = 0; f <= 4; ++f)
+      for (int q = 0; q < NP; ++q)
+        for (int p = 0; p < NP; ++p) {
+          int ijk[3];
+          host::side_to_vol(N, 0, p, q, f, s, ijk);
+          const int pt = p + NP * q;
+          B.s2v[s - 1][f][pt] = ijk[0] + NP * (ijk[1] + NP * ijk[2]);
+          int a, bb;
+          if (s == XI_MINUS || s == XI_PLUS) { a = ijk[1]; bb = ijk[2]; }
+          else if (s == ETA_MINUS || s == ETA_PLUS) { a = ijk[0]; bb = ijk[2]; }
+          else { a = ijk[0]; bb = ijk[1]; }
+          B.v2s[s - 1][f][a + NP * bb] = pt;
+        }
+}
+
+KParams base_params(fluxo_handle* h) {
+  KParams P{};
+  const fluxo_cfg& c = h->cfg;
+  P.nElems = h->nElems; P.nSides = h->nSides;
+  P.U = h->dU; P.Ut = h->dUt; P.UtTmp = h->dUtTmp; P.grad = h->dGrad;
+  P.metrics = h->dMetrics; P.sJ = h->dsJ; P.facegeo = h->dFaceGeo; P.xGP = h->dXGP;
+  P.s2e = h->dS2E; P.e2s = h->dE2S;
+  P.flux = h->dFlux; P.lflux = h->dLFlux; P.gtrace = h->dGTrace;
+  P.basis = h->dBasis;
+  P.kappa = c.kappa; P.kappaM1 = c.kappa - 1.; P.sKappaM1 = 1. / (c.kappa - 1.); P.kappaP1 = c.kappa + 1.;
+  P.R = c.R; P.s23 = 2. / 3.; P.KappasPr = c.kappa / c.Pr; P.mu0 = c.mu0;
+  P.visc = c.visc; P.lifting_var = c.lifting_var; P.lifting = c.lifting; P.etaBR2 = c.etaBR2;
+  if (c.visc == 1) {  // equation.f90:226-233 (Sutherland constants)
+    P.sTref = 1. / c.Tref; P.ExpoSuth = c.ExpoSuth; P.Ts = c.Ts * P.sTref;
+    P.cSuth = std::pow(P.Ts, P.ExpoSuth) * (1 + P.Ts) / (2 * P.Ts * P.Ts);
+  } else if (c.visc == 2) {  // equation.f90:236-241 (power law)
+    P.ExpoPow = c.ExpoPow; P.mu0 = c.mu0 / std::pow(c.Tref, c.ExpoPow);
+  }
+  P.source = (c.ini_exact_func == 4 && h->haveXGP) ? 1 : 0;
+  if (P.source) {  // CalcSource CASE(4) constants, equation.f90:1000-1012
+    double Omega = M_PI * c.ini_frequency, A = c.ini_amplitude, km1 = c.kappa - 1.;
+    double tmp[6] = {2., 2. + 2.5 * km1, A * km1, 0.5 * (9. + c.kappa * 15.) - 4., A * (3. * c.kappa - 1.),
+                     h->visc ? 3. * c.mu0 * c.kappa * Omega / c.Pr : 0.};
+    P.srcOmega = Omega;
+    for (int z = 0; z < 6; ++z) P.srcTmp[z] = tmp[z] * A * Omega;
+  }
+  P.CFLScale = h->CFLScale; P.DFLScale = h->DFLScale;
+  P.KappasPrMax = std::max(4. / 3., P.KappasPr);
+  return P;
+}
+
+// Brackets one launch with CUDA events when profiling is on.
+struct ProfScope {
+  fluxo_handle* h;
+  int kind;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(fluxo_handle* h_, int k) : h(h_), kind(k) {
+    if (h->profiling) {
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, h->stream);
+    }
+  }
+  ~ProfScope() {
+    if (h->profiling) {
+      cudaEventRecord(b, h->stream);
+      h->prof[kind].emplace_back(a, b);
+    }
+  }
+};
+
+// One DGTimeDerivative; stage 0 writes Ut, stage >= 1 applies the fused LSERK stage update.
+int rhs(fluxo_handle* h, KParams P) {
+  cudaStream_t s = h->stream;
+  if (h->visc) {
+    {
+      ProfScope ps(h, 0);
+      FLUXO_CUDA(h, launch_lift_flux(h->NP, h->nSides, s, P));
+    }
+    {
+      ProfScope ps(h, 1);
+      FLUXO_CUDA(h, launch_gradient(h->NP, h->nElems, s, P));
+    }
+    h->launches += 2;
+  }
+  {
+    ProfScope ps(h, 2);
+    FLUXO_CUDA(h, launch_face_flux(h->cfg.riemann, h->visc, h->NP, h->nSides, s, P));
+  }
+  {
+    ProfScope ps(h, 3);
+    FLUXO_CUDA(h, launch_volume(h->NP, h->cfg.volume_flux, h->visc, h->nElems, s, P));
+  }
+  h->launches += 2;
+  return FLUXO_OK;
+}
+
+// FP64 roofline denominator: 8 independent DFMA chains per thread, all in registers.
+__global__ void fp64_fma_kernel(double* out, int iters, double a, double b) {
+  double x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = threadIdx.x * 1e-3 + k;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = fma(x[k], a, b);
+  }
+  double s = 0.;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += x[k];
+  if (s == 1234.5678) out[threadIdx.x] = s;  // keeps the chains alive
+}
+
+// One LSERK-2reg step (timedisc.f90:424-480): host dt (dtDev == null) or device dt.
+int rk_step(fluxo_handle* h, double t, double dt, const double* dtDev, const int* halt) {
+  KParams P = base_params(h);
+  P.dtDev = dtDev; P.haltFlag = halt; P.dt = dt;
+  for (int st = 1; st <= h->nStages; ++st) {
+    P.stage = st;
+    P.rkA = h->RKA[st]; P.rkB = h->RKb[st]; P.rkC = h->RKc[st];
+    P.t = t + dt * h->RKc[st];
+    int r = rhs(h, P);
+    if (r) return r;
+  }
+  return FLUXO_OK;
+}
+
+int check_ready(fluxo_handle* h) {
+  if (!h) return FLUXO_EINVAL_CFG;
+  if (!h->meshSet) return fail(h, FLUXO_ENOTREADY, "mesh not set");
+  if (!h->stateSet) return fail(h, FLUXO_ENOTREADY, "state not set");
+  FLUXO_CUDA(h, cudaSetDevice(h->cfg.device));
+  return FLUXO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {
+  if (!cfg || !out) return fail(nullptr, FLUXO_EINVAL_CFG, "null argument");
+  *out = nullptr;
+  if (cfg->struct_size != (int)sizeof(fluxo_cfg)) return fail(nullptr, FLUXO_EINVAL_CFG, "fluxo_cfg size mismatch");
+  if (cfg->N < 1 || cfg->N > 7) return fail(nullptr, FLUXO_EINVAL_CFG, "N must be in 1..7");
+  if (cfg->eqn != FLUXO_EQN_EULER && cfg->eqn != FLUXO_EQN_NAVIERSTOKES)
+    return fail(nullptr, FLUXO_EINVAL_CFG, "unknown equation system");
+  if (!riemann_supported(cfg->riemann)) return fail(nullptr, FLUXO_EINVAL_CFG, "Riemann solver not implemented");
+  if (!volume_flux_supported(cfg->volume_flux)) return fail(nullptr, FLUXO_EINVAL_CFG, "volume flux not implemented");
+  if (cfg->eqn == FLUXO_EQN_NAVIERSTOKES) {
+    if (cfg->lifting != 1 && cfg->lifting != 2) return fail(nullptr, FLUXO_EINVAL_CFG, "lifting must be BR1 or BR2");
+    if (cfg->lifting_var < 1 || cfg->lifting_var > 3) return fail(nullptr, FLUXO_EINVAL_CFG, "lifting_var must be 1..3");
+    if (cfg->visc < 0 || cfg->visc > 2) return fail(nullptr, FLUXO_EINVAL_CFG, "visc must be 0..2");
+  }
+  if (!(cfg->kappa > 1.)) return fail(nullptr, FLUXO_EINVAL_CFG, "kappa must be > 1");
+  fluxo_handle* h = new fluxo_handle();
+  h->cfg = *cfg;
+  h->N = cfg->N; h->NP = cfg->N + 1;
+  h->visc = (cfg->eqn == FLUXO_EQN_NAVIERSTOKES);
+  // time discretisation coefficients and CFL/DFL scaling (timedisc_vars.f90:204-235, timedisc.f90:697-741)
+  double cflAlpha[15], relDFL;
+  if (cfg->time_disc == 0) {
+    const double a[15] = {4.7497, 3.4144, 2.8451, 2.4739, 2.2027, 1.9912, 1.8225, 1.6830,
+                          1.5682, 1.4692, 1.3849, 1.3106, 1.2454, 1.1880, 1.1362};
+    std::copy(a, a + 15, cflAlpha);
+    relDFL = 1.853;
+    h->nStages = 5;
+    const double A[6] = {0., 0., 567301805773.0 / 1357537059087.0, 2404267990393.0 / 2016746695238.0,
+                         3550918686646.0 / 2091501179385.0, 1275806237668.0 / 842570457699.0};
+    const double B[6] = {0., 1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                         1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                         2277821191437.0 / 14882151754819.0};
+    const double C[6] = {0., 0., 1432997174477.0 / 9575080441755.0, 2526269341429.0 / 6820363962896.0,
+                         2006345519317.0 / 3224310063776.0, 2802321613138.0 / 2924317926251.0};
+    std::copy(A, A + 6, h->RKA); std::copy(B, B + 6, h->RKb); std::copy(C, C + 6, h->RKc);
+  } else if (cfg->time_disc == 1) {
+    const double a[15] = {3.1871, 2.2444, 1.7797, 1.5075, 1.3230, 1.1857, 1.0800, 0.9945,
+                          0.9247, 0.8651, 0.8134, 0.7695, 0.7301, 0.6952, 0.6649};
+    std::copy(a, a + 15, cflAlpha);
+    relDFL = 1.;
+    h->nStages = 3;
+    const double A[4] = {0., 0., 5. / 9., 153. / 128.}, B[4] = {0., 1. / 3., 15. / 16., 8. / 15.},
+                 C[4] = {0., 0., 1. / 3., 0.75};
+    std::copy(A, A + 4, h->RKA); std::copy(B, B + 4, h->RKb); std::copy(C, C + 4, h->RKc);
+  } else {
+    delete h;
+    return fail(nullptr, FLUXO_EINVAL_CFG, "time_disc must be 0 (carpenterrk4-5) or 1 (standardrk3-3)");
+  }
+  const double dflAlpha[10] = {4.50, 1.95, 1.18, 0.79, 0.56, 0.42, 0.32, 0.25, 0.20, 0.17};
+  h->CFLScale = cfg->cfl_scale * cflAlpha[std::min(15, h->N) - 1] / (2. * h->N + 1.);
+  h->DFLScale = cfg->dfl_scale * dflAlpha[std::min(10, h->N) - 1] * relDFL / ((2. * h->N + 1.) * (2. * h->N + 1.));
+  cudaError_t e = cudaSetDevice(cfg->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    std::string m = std::string("CUDA init: ") + cudaGetErrorString(e);
+    delete h;
+    return fail(nullptr, FLUXO_ECUDA, m);
+  }
+  build_basis_tables(h->N, h->hb);
+  if (dalloc(h, &h->dBasis, 1) || dalloc(h, &h->dTD, 1) || dalloc(h, &h->dDtBits, 1) || dalloc(h, &h->dErrKey, 1)) {
+    std::string m = h->lastError;
+    fluxo_gpu_destroy(h);
+    return fail(nullptr, FLUXO_ENOMEM_HBM, m);
+  }
+  e = cudaMemcpy(h->dBasis, &h->hb, sizeof(BasisTables), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    fluxo_gpu_destroy(h);
+    return fail(nullptr, FLUXO_ECUDA, cudaGetErrorString(e));
+  }
+  *out = h;
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* S2E, const int* E2S, const double* Mf,
+                       const double* Mg, const double* Mh, const double* sJ, const double* NormVec,
+                       const double* TangVec1, const double* TangVec2, const double* SurfElem,
+                       const double* Elem_xGP) {
+  if (!h) return FLUXO_EINVAL_CFG;
+  if (nElems < 1 || nSides < 1 || !S2E || !E2S || !Mf || !Mg || !Mh || !sJ || !NormVec || !TangVec1 || !TangVec2 ||
+      !SurfElem)
+    return fail(h, FLUXO_EINVAL_CFG, "set_mesh: missing array");
+  if (h->cfg.ini_exact_func == 4 && !Elem_xGP) return fail(h, FLUXO_EINVAL_CFG, "source term needs Elem_xGP");
+  FLUXO_CUDA(h, cudaSetDevice(h->cfg.device));
+  const int NP = h->NP, NP3 = NP * NP * NP, NPT = NP * NP;
+  // connectivity: 1-based -> 0-based, checked
+  std::vector<int> s2e((size_t)5 * nSides), e2s((size_t)12 * nElems);
+  for (int s = 0; s < nSides; ++s) {
+    const int* a = S2E + 5 * (size_t)s;
+    if (a[0] < 1 || a[0] > nElems || a[1] < 1 || a[1] > nElems || a[2] < 1 || a[2] > 6 || a[3] < 1 || a[3] > 6 ||
+        a[4] < 1 || a[4] > 4)
+      return fail(h, FLUXO_EINVAL_CFG, "set_mesh: SideToElem entry out of range (only inner sides are supported)");
+    s2e[5 * (size_t)s + 0] = a[0] - 1; s2e[5 * (size_t)s + 1] = a[1] - 1;
+    s2e[5 * (size_t)s + 2] = a[2]; s2e[5 * (size_t)s + 3] = a[3]; s2e[5 * (size_t)s + 4] = a[4];
+  }
+  for (int e = 0; e < nElems; ++e)
+    for (int ls = 0; ls < 6; ++ls) {
+      const int sid = E2S[2 * (6 * (size_t)e + ls)], fl = E2S[2 * (6 * (size_t)e + ls) + 1];
+      if (sid < 1 || sid > nSides || fl < 0 || fl > 4) return fail(h, FLUXO_EINVAL_CFG, "set_mesh: ElemToSide out of range");
+      e2s[2 * (6 * (size_t)e + ls)] = sid - 1;
+      e2s[2 * (6 * (size_t)e + ls) + 1] = fl;
+    }
+  // repack geometry: metrics [elem][9][node], face geometry [side][10][pt]
+  std::vector<double> met((size_t)9 * NP3 * nElems), geo((size_t)10 * NPT * nSides);
+  for (int e = 0; e < nElems; ++e)
+    for (int n = 0; n < NP3; ++n)
+      for (int d = 0; d < 3; ++d) {
+        const size_t src = 3 * ((size_t)e * NP3 + n) + d;
+        met[((size_t)e * 9 + d) * NP3 + n] = Mf[src];
+        met[((size_t)e * 9 + 3 + d) * NP3 + n] = Mg[src];
+        met[((size_t)e * 9 + 6 + d) * NP3 + n] = Mh[src];
+      }
+  for (int s = 0; s < nSides; ++s)
+    for (int p = 0; p < NPT; ++p) {
+      const size_t src = (size_t)s * NPT + p;
+      for (int d = 0; d < 3; ++d) {
+        geo[((size_t)s * 10 + d) * NPT + p] = NormVec[3 * src + d];
+        geo[((size_t)s * 10 + 3 + d) * NPT + p] = TangVec1[3 * src + d];
+        geo[((size_t)s * 10 + 6 + d) * NPT + p] = TangVec2[3 * src + d];
+      }
+      geo[((size_t)s * 10 + 9) * NPT + p] = SurfElem[src];
+    }
+  h->nElems = nElems; h->nSides = nSides;
+  const size_t nU = (size_t)5 * NP3 * nElems, nF = (size_t)5 * NPT * nSides;
+  int r = FLUXO_OK;
+  if ((r = dalloc(h, &h->dU, nU)) || (r = dalloc(h, &h->dUt, nU)) || (r = dalloc(h, &h->dUtTmp, nU)) ||
+      (r = dalloc(h, &h->dMetrics, met.size())) || (r = dalloc(h, &h->dsJ, (size_t)NP3 * nElems)) ||
+      (r = dalloc(h, &h->dFaceGeo, geo.size())) || (r = dalloc(h, &h->dFlux, nF)) ||
+      (r = dalloc(h, &h->dS2E, s2e.size())) || (r = dalloc(h, &h->dE2S, e2s.size())))
+    return r;
+  if (h->visc) {
+    if ((r = dalloc(h, &h->dGrad, 3 * nU)) || (r = dalloc(h, &h->dLFlux, nF))) return r;
+    if (h->cfg.lifting == 2 && (r = dalloc(h, &h->dGTrace, (size_t)2 * 15 * NPT * nSides))) return r;
+  }
+  cudaStream_t s = h->stream;
+  FLUXO_CUDA(h, cudaMemcpyAsync(h->dMetrics, met.data(), met.size() * 8, cudaMemcpyHostToDevice, s));
+  FLUXO_CUDA(h, cudaMemcpyAsync(h->dsJ, sJ, (size_t)NP3 * nElems * 8, cudaMemcpyHostToDevice, s));
+  FLUXO_CUDA(h, cudaMemcpyAsync(h->dFaceGeo, geo.data(), geo.size() * 8, cudaMemcpyHostToDevice, s));
+  FLUXO_CUDA(h, cudaMemcpyAsync(h->dS2E, s2e.data(), s2e.size() * 4, cudaMemcpyHostToDevice, s));
+  FLUXO_CUDA(h, cudaMemcpyAsync(h->dE2S, e2s.data(), e2s.size() * 4, cudaMemcpyHostToDevice, s));
+  FLUXO_CUDA(h, cudaMemsetAsync(h->dUtTmp, 0, nU * 8, s));
+  FLUXO_CUDA(h, cudaMemsetAsync(h->dUt, 0, nU * 8, s));
+  if (Elem_xGP) {
+    if ((r = dalloc(h, &h->dXGP, (size_t)3 * NP3 * nElems))) return r;
+    FLUXO_CUDA(h, cudaMemcpyAsync(h->dXGP, Elem_xGP, (size_t)3 * NP3 * nElems * 8, cudaMemcpyHostToDevice, s));
+    h->haveXGP = true;
+  }
+  FLUXO_CUDA(h, cudaStreamSynchronize(s));
+  h->meshSet = true;
+  h->stateSet = false;
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_set_state(fluxo_handle* h, const double* U) {
+  if (!h || !U) return FLUXO_EINVAL_CFG;
+  if (!h->meshSet) return fail(h, FLUXO_ENOTREADY, "mesh not set");
+  FLUXO_CUDA(h, cudaSetDevice(h->cfg.device));
+  const size_t nU = (size_t)5 * h->NP * h->NP * h->NP * h->nElems;
+  FLUXO_CUDA(h, cudaMemcpyAsync(h->dU, U, nU * 8, cudaMemcpyHostToDevice, h->stream));
+  FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->stateSet = true;
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_get_state(fluxo_handle* h, double* U) {
+  int r = check_ready(h);
+  if (r) return r;
+  const size_t nU = (size_t)5 * h->NP * h->NP * h->NP * h->nElems;
+  FLUXO_CUDA(h, cudaMemcpyAsync(U, h->dU, nU * 8, cudaMemcpyDeviceToHost, h->stream));
+  FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_get_ut(fluxo_handle* h, double* Ut) {
+  int r = check_ready(h);
+  if (r) return r;
+  const size_t nU = (size_t)5 * h->NP * h->NP * h->NP * h->nElems;
+  FLUXO_CUDA(h, cudaMemcpyAsync(Ut, h->dUt, nU * 8, cudaMemcpyDeviceToHost, h->stream));
+  FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_get_gradients(fluxo_handle* h, double* gx, double* gy, double* gz) {
+  int r = check_ready(h);
+  if (r) return r;
+  if (!h->visc) return fail(h, FLUXO_EINVAL_CFG, "gradients exist for Navier-Stokes only");
+  const size_t nD = (size_t)h->NP * h->NP * h->NP * h->nElems;
+  std::vector<double> g(15 * nD);
+  FLUXO_CUDA(h, cudaMemcpyAsync(g.data(), h->dGrad, g.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+  FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
+  for (size_t z = 0; z < nD; ++z)
+    for (int v = 0; v < 5; ++v) {
+      if (gx) gx[5 * z + v] = g[15 * z + v];
+      if (gy) gy[5 * z + v] = g[15 * z + 5 + v];
+      if (gz) gz[5 * z + v] = g[15 * z + 10 + v];
+    }
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_dg_time_derivative(fluxo_handle* h, double t) {
+  int r = check_ready(h);
+  if (r) return r;
+  KParams P = base_params(h);
+  P.stage = 0;
+  P.t = t;
+  if ((r = rhs(h, P))) return r;
+  FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
+  FLUXO_CUDA(h, cudaGetLastError());
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_calc_timestep(fluxo_handle* h, double* dt, int* errType) {
+  int r = check_ready(h);
+  if (r) return r;
+  KParams P = base_params(h);
+  dt_reset_kernel<<<1, 1, 0, h->stream>>>(h->dDtBits, h->dErrKey);
+  FLUXO_CUDA(h, cudaGetLastError());
+  FLUXO_CUDA(h, launch_timestep(h->NP, h->visc, h->nElems, h->stream, P, h->dDtBits, h->dErrKey));
+  h->launches += 2;
+  unsigned long long bits = 0;
+  int key = 0;
+  FLUXO_CUDA(h, cudaMemcpyAsync(&bits, h->dDtBits, 8, cudaMemcpyDeviceToHost, h->stream));
+  FLUXO_CUDA(h, cudaMemcpyAsync(&key, h->dErrKey, 4, cudaMemcpyDeviceToHost, h->stream));
+  FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
+  double d;
+  std::memcpy(&d, &bits, 8);
+  if (dt) *dt = d;
+  int err = (key == INT_MAX) ? 0 : (key & 7);
+  if (errType) *errType = err;
+  return err ? FLUXO_ENAN_STATE : FLUXO_OK;
+}
+
+int fluxo_gpu_timestep(fluxo_handle* h, double t, double dt) {
+  int r = check_ready(h);
+  if (r) return r;
+  if ((r = rk_step(h, t, dt, nullptr, nullptr))) return r;
+  FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_time_disc(fluxo_handle* h, double t, double tEnd, int maxIter, double* tOut, int* nIter,
+                        int* errType) {
+  int r = check_ready(h);
+  if (r) return r;
+  cudaStream_t s = h->stream;
+  TDState* td = h->dTD;
+  td_begin_kernel<<<1, 1, 0, s>>>(td, t, tEnd, maxIter);
+  FLUXO_CUDA(h, cudaGetLastError());
+  h->launches += 1;
+  const int chunk = 16;
+  for (;;) {
+    for (int c = 0; c < chunk; ++c) {
+      KParams P = base_params(h);
+      P.haltFlag = &td->halt;
+      {
+        ProfScope ps(h, 4);
+        FLUXO_CUDA(h, launch_timestep(h->NP, h->visc, h->nElems, s, P, &td->dtBits, &td->errKey));
+      }
+      td_finalize_kernel<<<1, 1, 0, s>>>(td);
+      FLUXO_CUDA(h, cudaGetLastError());
+      if ((r = rk_step(h, 0., 0., &td->dt, &td->halt))) return r;
+      td_advance_kernel<<<1, 1, 0, s>>>(td);
+      FLUXO_CUDA(h, cudaGetLastError());
+      h->launches += 3;
+      if (maxIter > 0 && c + 1 >= maxIter) break;
+    }
+    TDState hs;
+    FLUXO_CUDA(h, cudaMemcpyAsync(&hs, td, sizeof(TDState), cudaMemcpyDeviceToHost, s));
+    FLUXO_CUDA(h, cudaStreamSynchronize(s));
+    if (hs.halt) {
+      if (tOut) *tOut = hs.t;
+      if (nIter) *nIter = hs.iter;
+      if (errType) *errType = hs.err;
+      return hs.err ? FLUXO_ENAN_STATE : FLUXO_OK;
+    }
+  }
+}
+
+int fluxo_gpu_device_buffers(fluxo_handle* h, double** dU, double** dUt, void** stream) {
+  if (!h) return FLUXO_EINVAL_CFG;
+  if (dU) *dU = h->dU;
+  if (dUt) *dUt = h->dUt;
+  if (stream) *stream = (void*)h->stream;
+  if (h->meshSet && dU) h->stateSet = true;  // caller may fill U directly on the device
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_launch_count(fluxo_handle* h, uint64_t* n) {
+  if (!h || !n) return FLUXO_EINVAL_CFG;
+  *n = h->launches;
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_set_profiling(fluxo_handle* h, int enable) {
+  if (!h) return FLUXO_EINVAL_CFG;
+  h->profiling = enable != 0;
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_get_profile(fluxo_handle* h, int kind, double* total_ms, uint64_t* count) {
+  if (!h || kind < 0 || kind > 4) return FLUXO_EINVAL_CFG;
+  FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
+  double tot = 0.;
+  for (auto& pr : h->prof[kind]) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, pr.first, pr.second);
+    tot += ms;
+    cudaEventDestroy(pr.first);
+    cudaEventDestroy(pr.second);
+  }
+  if (total_ms) *total_ms = tot;
+  if (count) *count = h->prof[kind].size();
+  h->prof[kind].clear();
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_fp64_peak(int device, double* tflops) {
+  if (!tflops) return FLUXO_EINVAL_CFG;
+  if (cudaSetDevice(device) != cudaSuccess) return FLUXO_ECUDA;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  double* out = nullptr;
+  if (cudaMalloc(&out, 1024 * sizeof(double)) != cudaSuccess) return FLUXO_ENOMEM_HBM;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const int threads = 512, blocks = sms * 4, iters = 4096;
+  fp64_fma_kernel<<<blocks, threads>>>(out, 64, 1.0000001, 1e-9);  // warm-up
+  double best = 0.;
+  for (int rep = 0; rep < 5; ++rep) {
+    cudaEventRecord(a);
+    fp64_fma_kernel<<<blocks, threads>>>(out, iters, 1.0000001, 1e-9);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    const double fl = 2.0 * 8.0 * iters * (double)threads * blocks;
+    best = std::max(best, fl / (ms * 1e-3) / 1e12);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return FLUXO_ECUDA;
+  *tflops = best;
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_destroy(fluxo_handle* h) {
+  if (!h) return FLUXO_OK;
+  for (int k = 0; k < 5; ++k) {
+    for (auto& pr : h->prof[k]) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+    h->prof[k].clear();
+  }
+  cudaSetDevice(h->cfg.device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  void* ptrs[] = {h->dBasis, h->dU, h->dUt, h->dUtTmp, h->dGrad, h->dMetrics, h->dsJ, h->dFaceGeo, h->dXGP,
+                  h->dFlux, h->dLFlux, h->dGTrace, h->dS2E, h->dE2S, h->dTD, h->dDtBits, h->dErrKey};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_last_error(fluxo_handle* h, char* buf, size_t len) {
+  if (!buf || len == 0) return FLUXO_EINVAL_CFG;
+  std::string m;
+  if (h) m = h->lastError;
+  else {
+    std::lock_guard<std::mutex> lk(g_err_mutex);
+    m = g_create_error;
+  }
+  std::snprintf(buf, len, "%s", m.c_str());
+  return FLUXO_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,351 @@
+// Host-side setup of the product (no GPU): side/volume index maps, a periodic hexahedral box
+// with optional curved (NGeo) deformation, its curl-form metrics and surface metrics, and the
+// initial states of the reference's exact functions.  This stands in for the reference's
+// InitMesh / CalcMetrics (src/mesh/mesh.f90:89-296, src/mesh/metrics.f90:78-484), which read a
+// HOPR HDF5 mesh; the arrays it produces have the reference layouts of include/fluxo_gpu.h.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <vector>
+
+#include "../../include/fluxo_gpu.h"
+#include "host_basis.h"
+#include "host_setup.h"
+
+namespace fluxo {
+namespace host {
+
+// Side <-> volume index maps with the reference's conventions (src/mesh/mappings.f90:262-464):
+// flip maps master (p,q) to slave coordinates; CGNS orientation of each local side.
+void flip_pq(int N, int p, int q, int flip, int& a, int& b) {
+  switch (flip) {
+    case 0: a = p; b = q; return;
+    case 1: a = q; b = p; return;
+    case 2: a = N - p; b = q; return;
+    case 3: a = N - q; b = N - p; return;
+    default: a = p; b = N - q; return;
+  }
+}
+
+void side_to_vol(int N, int l, int p, int q, int flip, int side, int* ijk) {
+  int a, b;
+  flip_pq(N, p, q, flip, a, b);
+  switch (side) {
+    case 5: ijk[0] = l; ijk[1] = b; ijk[2] = a; return;          // XI_MINUS
+    case 3: ijk[0] = N - l; ijk[1] = a; ijk[2] = b; return;      // XI_PLUS
+    case 2: ijk[0] = a; ijk[1] = l; ijk[2] = b; return;          // ETA_MINUS
+    case 4: ijk[0] = N - a; ijk[1] = N - l; ijk[2] = b; return;  // ETA_PLUS
+    case 1: ijk[0] = b; ijk[1] = a; ijk[2] = l; return;          // ZETA_MINUS
+    default: ijk[0] = a; ijk[1] = b; ijk[2] = N - l; return;     // ZETA_PLUS
+  }
+}
+
+namespace {
+
+// tensor-product interpolation of `dim` interleaved fields from (ni)^3 to (no)^3 nodes, V is no x ni
+void tp_interp(int dim, int ni, int no, const std::vector<double>& V, const double* in, double* out) {
+  std::vector<double> a((size_t)dim * no * ni * ni, 0.), b((size_t)dim * no * no * ni, 0.);
+  for (int k = 0; k < ni; ++k)
+    for (int j = 0; j < ni; ++j)
+      for (int o = 0; o < no; ++o)
+        for (int i = 0; i < ni; ++i) {
+          const double v = V[(size_t)o * ni + i];
+          for (int d = 0; d < dim; ++d) a[d + dim * (o + no * (j + ni * k))] += v * in[d + dim * (i + ni * (j + ni * k))];
+        }
+  for (int k = 0; k < ni; ++k)
+    for (int o = 0; o < no; ++o)
+      for (int j = 0; j < ni; ++j) {
+        const double v = V[(size_t)o * ni + j];
+        for (int i = 0; i < no; ++i)
+          for (int d = 0; d < dim; ++d) b[d + dim * (i + no * (o + no * k))] += v * a[d + dim * (i + no * (j + ni * k))];
+      }
+  std::fill(out, out + (size_t)dim * no * no * no, 0.);
+  for (int o = 0; o < no; ++o)
+    for (int k = 0; k < ni; ++k) {
+      const double v = V[(size_t)o * ni + k];
+      for (int j = 0; j < no; ++j)
+        for (int i = 0; i < no; ++i)
+          for (int d = 0; d < dim; ++d) out[d + dim * (i + no * (j + no * o))] += v * b[d + dim * (i + no * (j + no * k))];
+    }
+}
+
+// derivative along reference direction `dir` of `dim` interleaved fields on n^3 nodes
+void tp_deriv(int dim, int n, const std::vector<double>& D, int dir, const double* in, double* out) {
+  for (int k = 0; k < n; ++k)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        const int me = dir == 0 ? i : (dir == 1 ? j : k);
+        for (int d = 0; d < dim; ++d) {
+          double s = 0.;
+          for (int l = 0; l < n; ++l) {
+            const int ii = dir == 0 ? l : i, jj = dir == 1 ? l : j, kk = dir == 2 ? l : k;
+            s += D[(size_t)me * n + l] * in[d + dim * (ii + n * (jj + n * kk))];
+          }
+          out[d + dim * (i + n * (j + n * k))] = s;
+        }
+      }
+}
+
+const int kNormalDir[7] = {0, 3, 2, 1, 2, 1, 3};  // src/mesh/mesh_vars.f90:91-93
+const int kTangDir[7] = {0, 1, 3, 2, 3, 2, 1};
+const double kNormalSign[7] = {0, -1., -1., 1., 1., -1., 1.};
+
+}  // namespace
+
+void box_connectivity(const int* ne, int N, std::vector<int>& S2E, std::vector<int>& E2S) {
+  const int nx = ne[0], ny = ne[1], nz = ne[2];
+  const int nElems = nx * ny * nz, nSides = 3 * nElems, n = N + 1;
+  S2E.assign((size_t)5 * nSides, -1);
+  E2S.assign((size_t)12 * nElems, 0);
+  auto eid = [&](int x, int y, int z) { return ((z + nz) % nz) * nx * ny + ((y + ny) % ny) * nx + ((x + nx) % nx); };
+  std::vector<int> owner((size_t)6 * nElems, 0);
+  int next = 0;
+  for (int e = 0; e < nElems; ++e) {
+    const int ix = e % nx, iy = (e / nx) % ny, iz = e / (nx * ny);
+    for (int s = 1; s <= 6; ++s) {
+      if (owner[(size_t)6 * e + s - 1]) continue;
+      int nb, nbs;
+      switch (s) {
+        case 5: nb = eid(ix - 1, iy, iz); nbs = 3; break;
+        case 3: nb = eid(ix + 1, iy, iz); nbs = 5; break;
+        case 2: nb = eid(ix, iy - 1, iz); nbs = 4; break;
+        case 4: nb = eid(ix, iy + 1, iz); nbs = 2; break;
+        case 1: nb = eid(ix, iy, iz - 1); nbs = 6; break;
+        default: nb = eid(ix, iy, iz + 1); nbs = 1; break;
+      }
+      const int sid = ++next;
+      owner[(size_t)6 * e + s - 1] = sid;
+      owner[(size_t)6 * nb + nbs - 1] = sid;
+      // slave flip: the one that maps every master face node onto the same global lattice node
+      auto lat = [&](int el, const int* ijk, long* g) {
+        const int x = el % nx, y = (el / nx) % ny, z = el / (nx * ny);
+        g[0] = ((long)x * N + ijk[0]) % ((long)nx * N);
+        g[1] = ((long)y * N + ijk[1]) % ((long)ny * N);
+        g[2] = ((long)z * N + ijk[2]) % ((long)nz * N);
+      };
+      int flip = -1;
+      for (int f = 1; f <= 4 && flip < 0; ++f) {
+        bool ok = true;
+        for (int q = 0; q < n && ok; ++q)
+          for (int p = 0; p < n && ok; ++p) {
+            int a[3], b[3];
+            long ga[3], gb[3];
+            side_to_vol(N, 0, p, q, 0, s, a);
+            side_to_vol(N, 0, p, q, f, nbs, b);
+            lat(e, a, ga);
+            lat(nb, b, gb);
+            ok = ga[0] == gb[0] && ga[1] == gb[1] && ga[2] == gb[2];
+          }
+        if (ok) flip = f;
+      }
+      if (flip < 0) throw std::runtime_error("box_connectivity: no flip");
+      int* se = &S2E[(size_t)5 * (sid - 1)];
+      se[0] = e + 1; se[1] = nb + 1; se[2] = s; se[3] = nbs; se[4] = flip;
+      E2S[(size_t)2 * (6 * e + s - 1)] = sid;
+      E2S[(size_t)2 * (6 * e + s - 1) + 1] = 0;
+      E2S[(size_t)2 * (6 * nb + nbs - 1)] = sid;
+      E2S[(size_t)2 * (6 * nb + nbs - 1) + 1] = flip;
+    }
+  }
+  if (next != nSides) throw std::runtime_error("box_connectivity: side count");
+}
+
+void box_geometry(int N, const int* ne, const double* xmin, const double* xmax, int NGeo, double amp,
+                  const std::vector<int>& E2S, double* Mf, double* Mg, double* Mh, double* sJ, double* NormVec,
+                  double* TangVec1, double* TangVec2, double* SurfElem, double* Elem_xGP) {
+  const int nx = ne[0], ny = ne[1], nz = ne[2], nElems = nx * ny * nz;
+  const int n = N + 1, ng = NGeo + 1, NR = 3 * NGeo, nr = NR + 1;
+  const size_t nv = (size_t)n * n * n;
+  LGLBasis bN(N);
+  std::vector<double> xeq(ng), xg, wg, xr, wr;
+  for (int i = 0; i < ng; ++i) xeq[i] = NGeo > 0 ? 2. * i / NGeo - 1. : 0.;
+  lgl(NGeo, xg, wg);
+  lgl(NR, xr, wr);
+  const std::vector<double> V_eq_g = interp_matrix(xeq, xg);
+  const std::vector<double> V_g_N = interp_matrix(xg, bN.x);
+  const std::vector<double> V_g_r = interp_matrix(xg, xr);
+  std::vector<double> V_r_N;
+  if (NR > N) V_r_N = modal_projection(xr, bN.x);
+  else V_r_N = interp_matrix(xr, bN.x);
+  const std::vector<double> Dg = deriv_matrix(xg);
+  const double L[3] = {xmax[0] - xmin[0], xmax[1] - xmin[1], xmax[2] - xmin[2]};
+  const double c[3] = {0.5 * (xmax[0] + xmin[0]), 0.5 * (xmax[1] + xmin[1]), 0.5 * (xmax[2] + xmin[2])};
+  const double h[3] = {L[0] / nx, L[1] / ny, L[2] / nz};
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int e = 0; e < nElems; ++e) {
+    const int ix = e % nx, iy = (e / nx) % ny, iz = e / (nx * ny);
+    std::vector<double> Xeq(3 * ng * ng * ng), Xg(3 * ng * ng * ng), XN(3 * nv), dXg(9 * ng * ng * ng), tmp(3 * ng * ng * ng);
+    for (int k = 0; k < ng; ++k)
+      for (int j = 0; j < ng; ++j)
+        for (int i = 0; i < ng; ++i) {
+          const double xs[3] = {xmin[0] + h[0] * (ix + (double)i / NGeo), xmin[1] + h[1] * (iy + (double)j / NGeo),
+                                xmin[2] + h[2] * (iz + (double)k / NGeo)};
+          double f = amp;
+          if (f != 0.)
+            for (int d = 0; d < 3; ++d) f *= std::sin(2. * M_PI * (xs[d] - c[d]) / L[d]);
+          for (int d = 0; d < 3; ++d) Xeq[3 * (i + ng * (j + ng * k)) + d] = xs[d] + f;
+        }
+    tp_interp(3, ng, ng, V_eq_g, Xeq.data(), Xg.data());
+    tp_interp(3, ng, n, V_g_N, Xg.data(), XN.data());
+    std::copy(XN.begin(), XN.end(), Elem_xGP + 3 * nv * e);
+    // dXg[dir][node][coord]: derivative of the coordinates along reference direction dir (NGeo nodes)
+    for (int dir = 0; dir < 3; ++dir) {
+      tp_deriv(3, ng, Dg, dir, Xg.data(), tmp.data());
+      for (int z = 0; z < ng * ng * ng; ++z)
+        for (int d = 0; d < 3; ++d) dXg[9 * z + 3 * dir + d] = tmp[3 * z + d];
+    }
+    // Jacobian determinant at 3*NGeo, then projected (or interpolated) to N
+    std::vector<double> dXr((size_t)9 * nr * nr * nr), detr((size_t)nr * nr * nr), detN(nv);
+    tp_interp(9, ng, nr, V_g_r, dXg.data(), dXr.data());
+    for (int z = 0; z < nr * nr * nr; ++z) {
+      const double* a = &dXr[9 * z];  // a[3*dir + coord] = dX_coord/dxi_dir
+      const double* t = a;
+      const double* u = a + 3;
+      const double* w = a + 6;
+      detr[z] = t[0] * (u[1] * w[2] - u[2] * w[1]) - t[1] * (u[0] * w[2] - u[2] * w[0]) + t[2] * (u[0] * w[1] - u[1] * w[0]);
+    }
+    if (NR == N) std::copy(detr.begin(), detr.end(), detN.begin());
+    else tp_interp(1, nr, n, V_r_N, detr.data(), detN.data());
+    for (size_t z = 0; z < nv; ++z) sJ[nv * e + z] = 1. / detN[z];
+    // coordinate derivatives on the N nodes
+    std::vector<double> dXN((size_t)9 * nv), tN(3 * nv);
+    if (N >= NGeo) {
+      tp_interp(9, ng, n, V_g_N, dXg.data(), dXN.data());
+    } else {
+      for (int dir = 0; dir < 3; ++dir) {
+        tp_deriv(3, n, bN.D, dir, XN.data(), tN.data());
+        for (size_t z = 0; z < nv; ++z)
+          for (int d = 0; d < 3; ++d) dXN[9 * z + 3 * dir + d] = tN[3 * z + d];
+      }
+    }
+    // curl form: Ja^i_c = -(curl_xi R_c)_i with R_c(dir) = 1/2 (X_{c+2} dX_{c+1}/dxi_dir - X_{c+1} dX_{c+2}/dxi_dir)
+    std::vector<double> R((size_t)9 * nv), dR((size_t)9 * nv), Ja((size_t)9 * nv, 0.);  // R[9*z + 3*dir + c]
+    for (size_t z = 0; z < nv; ++z)
+      for (int dir = 0; dir < 3; ++dir)
+        for (int cc = 0; cc < 3; ++cc) {
+          const int c1 = (cc + 1) % 3, c2 = (cc + 2) % 3;
+          R[9 * z + 3 * dir + cc] = 0.5 * (XN[3 * z + c2] * dXN[9 * z + 3 * dir + c1] - XN[3 * z + c1] * dXN[9 * z + 3 * dir + c2]);
+        }
+    // Ja(i,c) += d/dxi_{i+2} R(i+1,c) - d/dxi_{i+1} R(i+2,c)
+    for (int dd = 0; dd < 3; ++dd) {
+      tp_deriv(9, n, bN.D, dd, R.data(), dR.data());  // dR[.. 3*dir + c] = d/dxi_dd R(dir,c)
+      for (size_t z = 0; z < nv; ++z)
+        for (int i = 0; i < 3; ++i)
+          for (int cc = 0; cc < 3; ++cc) {
+            if (dd == (i + 2) % 3) Ja[9 * z + 3 * i + cc] += dR[9 * z + 3 * ((i + 1) % 3) + cc];
+            if (dd == (i + 1) % 3) Ja[9 * z + 3 * i + cc] -= dR[9 * z + 3 * ((i + 2) % 3) + cc];
+          }
+    }
+    for (size_t z = 0; z < nv; ++z)
+      for (int cc = 0; cc < 3; ++cc) {
+        Mf[3 * (nv * e + z) + cc] = Ja[9 * z + 0 + cc];
+        Mg[3 * (nv * e + z) + cc] = Ja[9 * z + 3 + cc];
+        Mh[3 * (nv * e + z) + cc] = Ja[9 * z + 6 + cc];
+      }
+    // surface metrics of the master sides (CalcSurfMetrics / SurfMetricsFromJa)
+    for (int s = 1; s <= 6; ++s) {
+      const int sid = E2S[(size_t)2 * (6 * e + s - 1)], flip = E2S[(size_t)2 * (6 * e + s - 1) + 1];
+      if (flip != 0) continue;
+      const int nd = kNormalDir[s] - 1, td = kTangDir[s] - 1;
+      for (int q = 0; q < n; ++q)
+        for (int p = 0; p < n; ++p) {
+          int ijk[3];
+          side_to_vol(N, 0, p, q, 0, s, ijk);
+          const size_t z = ijk[0] + n * (ijk[1] + (size_t)n * ijk[2]);
+          const double* jn = &Ja[9 * z + 3 * nd];
+          const double* jt = &Ja[9 * z + 3 * td];
+          const size_t fi = p + n * (q + (size_t)n * (sid - 1));
+          const double se = std::sqrt(jn[0] * jn[0] + jn[1] * jn[1] + jn[2] * jn[2]);
+          double nv3[3], t1[3];
+          for (int d = 0; d < 3; ++d) nv3[d] = kNormalSign[s] * jn[d] / se;
+          const double dot = jt[0] * nv3[0] + jt[1] * nv3[1] + jt[2] * nv3[2];
+          for (int d = 0; d < 3; ++d) t1[d] = jt[d] - dot * nv3[d];
+          const double tn = std::sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+          for (int d = 0; d < 3; ++d) t1[d] /= tn;
+          SurfElem[fi] = se;
+          for (int d = 0; d < 3; ++d) {
+            NormVec[3 * fi + d] = nv3[d];
+            TangVec1[3 * fi + d] = t1[d];
+          }
+          TangVec2[3 * fi + 0] = nv3[1] * t1[2] - nv3[2] * t1[1];
+          TangVec2[3 * fi + 1] = nv3[2] * t1[0] - nv3[0] * t1[2];
+          TangVec2[3 * fi + 2] = nv3[0] * t1[1] - nv3[1] * t1[0];
+        }
+    }
+  }
+}
+
+}  // namespace host
+}  // namespace fluxo
+
+using namespace fluxo::host;
+
+extern "C" int fluxo_host_box_sizes(const int* ne, int* nElems, int* nSides) {
+  if (!ne || ne[0] < 1 || ne[1] < 1 || ne[2] < 1) return FLUXO_EINVAL_CFG;
+  *nElems = ne[0] * ne[1] * ne[2];
+  *nSides = 3 * *nElems;
+  return FLUXO_OK;
+}
+
+extern "C" int fluxo_host_box_mesh(int N, const int* ne, const double* xmin, const double* xmax, int NGeo,
+                                   double amp, int* SideToElem, int* ElemToSide, double* Mf, double* Mg, double* Mh,
+                                   double* sJ, double* NormVec, double* TangVec1, double* TangVec2,
+                                   double* SurfElem, double* Elem_xGP) {
+  if (N < 1 || N > 8 || NGeo < 1 || !ne) return FLUXO_EINVAL_CFG;
+  try {
+    std::vector<int> S2E, E2S;
+    box_connectivity(ne, N, S2E, E2S);
+    std::copy(S2E.begin(), S2E.end(), SideToElem);
+    std::copy(E2S.begin(), E2S.end(), ElemToSide);
+    box_geometry(N, ne, xmin, xmax, NGeo, amp, E2S, Mf, Mg, Mh, sJ, NormVec, TangVec1, TangVec2, SurfElem, Elem_xGP);
+  } catch (...) {
+    return FLUXO_EINVAL_CFG;
+  }
+  return FLUXO_OK;
+}
+
+extern "C" int fluxo_host_exact_func(int func, double t, size_t np, const double* x, double kappa,
+                                     const double* adv, double amp, const double* wave, double freq,
+                                     const double* ref, double* U) {
+  const double km1 = kappa - 1., skm1 = 1. / km1;
+  for (size_t z = 0; z < np; ++z) {
+    const double* X = x + 3 * z;
+    double* u = U + 5 * z;
+    double prim[5];
+    switch (func) {
+      case 1:  // constant state
+        for (int v = 0; v < 5; ++v) prim[v] = ref[v];
+        break;
+      case 2: {  // density sine wave advected with AdvVel
+        double arg = 0.;
+        for (int d = 0; d < 3; ++d) arg += wave[d] * (X[d] - adv[d] * t);
+        prim[0] = 1. + amp * std::sin(M_PI * arg);
+        for (int d = 0; d < 3; ++d) prim[1 + d] = adv[d];
+        prim[4] = 1.;
+        break;
+      }
+      case 4: {  // manufactured solution rho = rho v_i = 2 + A sin(pi f (x+y+z-t)), rho E = rho^2
+        const double r = 2. + amp * std::sin(M_PI * freq * (X[0] + X[1] + X[2] - t));
+        u[0] = u[1] = u[2] = u[3] = r;
+        u[4] = r * r;
+        continue;
+      }
+      case 7: {  // Taylor-Green vortex, Mach 0.1
+        prim[0] = 1.;
+        prim[1] = std::sin(X[0]) * std::cos(X[1]) * std::cos(X[2]);
+        prim[2] = -std::cos(X[0]) * std::sin(X[1]) * std::cos(X[2]);
+        prim[3] = 0.;
+        prim[4] = 100. / kappa + 1. / 16. * (std::cos(2 * X[0]) * std::cos(2. * X[2]) + 2. * std::cos(2. * X[1]) +
+                                           2. * std::cos(2. * X[0]) + std::cos(2 * X[1]) * std::cos(2. * X[2]));
+        break;
+      }
+      default:
+        return FLUXO_EINVAL_CFG;
+    }
+    u[0] = prim[0];
+    for (int d = 0; d < 3; ++d) u[1 + d] = prim[0] * prim[1 + d];
+    u[4] = skm1 * prim[4] + 0.5 * (u[1] * prim[1] + u[2] * prim[2] + u[3] * prim[3]);
+  }
+  return FLUXO_OK;
+}

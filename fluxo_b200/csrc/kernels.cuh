@@ -1,0 +1,486 @@
+// sm_100a FP64 kernels of the DGSEM right-hand side and LSERK stage.
+//
+// Per RHS evaluation (dg/dg.f90:282-452 on one GPU, all sides inner sides):
+//   Euler:          face_flux  ->  volume (split form + surface integral + Jacobian [+ RK stage])
+//   Navier-Stokes:  lift_flux  ->  gradient (BR1/BR2 lifting)  ->  face_flux (+ viscous)  ->  volume (+ viscous)
+// The element kernels hold one element's state, metrics and per-node auxiliaries in shared
+// memory (one thread per volume node); face kernels use one thread per face point.
+#pragma once
+#include "common.cuh"
+#include "physics_ns.cuh"
+
+namespace fluxo {
+
+__device__ __forceinline__ int side_plane_coords(int s, int i, int j, int k, int NP) {
+  // in-plane volume coordinates of a node on local side s (see BasisTables::v2s)
+  if (s == XI_MINUS || s == XI_PLUS) return j + NP * k;
+  if (s == ETA_MINUS || s == ETA_PLUS) return i + NP * k;
+  return i + NP * j;
+}
+
+// Up to three local sides touched by volume node (i,j,k); returns the count.
+__device__ __forceinline__ int boundary_sides(int i, int j, int k, int N, int* s) {
+  int c = 0;
+  if (i == 0) s[c++] = XI_MINUS;
+  if (i == N) s[c++] = XI_PLUS;
+  if (j == 0) s[c++] = ETA_MINUS;
+  if (j == N) s[c++] = ETA_PLUS;
+  if (k == 0) s[c++] = ZETA_MINUS;
+  if (k == N) s[c++] = ZETA_PLUS;
+  return c;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Face kernel: ProlongToFace (LGL copy) + FillFlux (Riemann, viscous average) + SurfElem scaling.
+// prolongtoface.f90:43-132, fillflux.f90:41-110, riemann.f90:104-246.
+// ------------------------------------------------------------------------------------------------
+template <int RS, bool VISC>
+__global__ void face_flux_kernel(KParams P, int NP) {
+  if (halted(P)) return;
+  const int npts = NP * NP;
+  const int spb = blockDim.x / npts;
+  const int ls = threadIdx.x / npts;  // side slot in block
+  const int pt = threadIdx.x - ls * npts;
+  const int side = blockIdx.x * spb + ls;
+  const bool valid = (ls < spb) && (side < P.nSides);
+  __shared__ double s_lam[256];
+  double L[5], R[5], F[5];
+  double nv[3], t1[3], t2[3], se = 0.;
+  int eM = 0, eS = 0, nM = 0, nS = 0;
+  if (valid) {
+    const int* se5 = P.s2e + 5 * side;
+    eM = se5[0]; eS = se5[1];
+    int lsM = se5[2], lsS = se5[3], fl = se5[4];
+    nM = P.basis->s2v[lsM - 1][0][pt];
+    nS = P.basis->s2v[lsS - 1][fl][pt];
+    const double* UM = P.U + 5 * ((size_t)eM * NP * NP * NP + nM);
+    const double* US = P.U + 5 * ((size_t)eS * NP * NP * NP + nS);
+    const double* g = P.facegeo + (size_t)side * 10 * npts + pt;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { nv[d] = g[d * npts]; t1[d] = g[(3 + d) * npts]; t2[d] = g[(6 + d) * npts]; }
+    se = g[9 * npts];
+    double uL[5], uR[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) { uL[v] = UM[v]; uR[v] = US[v]; }
+    // RotateState (riemann.f90:218-231)
+    L[0] = uL[0]; L[4] = uL[4];
+    R[0] = uR[0]; R[4] = uR[4];
+    L[1] = uL[1] * nv[0] + uL[2] * nv[1] + uL[3] * nv[2];
+    L[2] = uL[1] * t1[0] + uL[2] * t1[1] + uL[3] * t1[2];
+    L[3] = uL[1] * t2[0] + uL[2] * t2[1] + uL[3] * t2[2];
+    R[1] = uR[1] * nv[0] + uR[2] * nv[1] + uR[3] * nv[2];
+    R[2] = uR[1] * t1[0] + uR[2] * t1[1] + uR[3] * t1[2];
+    R[3] = uR[1] * t2[0] + uR[2] * t2[1] + uR[3] * t2[2];
+  }
+  double lmm = 0.;
+  if constexpr (riemann_needs_side_max<RS>()) {
+    s_lam[threadIdx.x] = valid ? lambda_max_pair(P, L, R) : 0.;
+    __syncthreads();
+    if (valid) {
+      const double* b = s_lam + ls * npts;
+      for (int z = 0; z < npts; ++z) lmm = fmax(lmm, b[z]);
+    }
+  }
+  if (!valid) return;
+  riemann_rotated<RS>(P, L, R, lmm, F);
+  // RotateFluxBack (riemann.f90:235-246)
+  double f2 = F[1], f3 = F[2], f4 = F[3];
+  F[1] = nv[0] * f2 + t1[0] * f3 + t2[0] * f4;
+  F[2] = nv[1] * f2 + t1[1] * f3 + t2[1] * f4;
+  F[3] = nv[2] * f2 + t1[2] * f3 + t2[2] * f4;
+  if constexpr (VISC) {  // riemann.f90:155-168: + 1/2 n.(F_v(L) + F_v(R))
+    const double* U0 = P.U + 5 * ((size_t)eM * NP * NP * NP + nM);
+    const double* U1 = P.U + 5 * ((size_t)eS * NP * NP * NP + nS);
+    const double* gM = P.grad + 15 * ((size_t)eM * NP * NP * NP + nM);
+    const double* gS = P.grad + 15 * ((size_t)eS * NP * NP * NP + nS);
+    double uL[5], uR[5], gl[15], gr[15];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) { uL[v] = U0[v]; uR[v] = U1[v]; }
+    if (P.lifting == 2) {  // BR2 face traces: side buffers written by the gradient kernel
+      const double* tM = P.gtrace + ((size_t)side * 2 + 0) * 15 * npts + pt;
+      const double* tS = P.gtrace + ((size_t)side * 2 + 1) * 15 * npts + pt;
+      for (int c = 0; c < 15; ++c) { gl[c] = tM[(size_t)c * npts]; gr[c] = tS[(size_t)c * npts]; }
+    } else {
+      for (int c = 0; c < 15; ++c) { gl[c] = gM[c]; gr[c] = gS[c]; }
+    }
+    double kL[4], gL[4], jL[4], kR[4], gR[4], jR[4];
+    diff_flux_3d(P, uL, gl, gl + 5, gl + 10, kL, gL, jL);
+    diff_flux_3d(P, uR, gr, gr + 5, gr + 10, kR, gR, jR);
+#pragma unroll
+    for (int v = 1; v < 5; ++v)
+      F[v] = F[v] + 0.5 * (nv[0] * (kL[v - 1] + kR[v - 1]) + nv[1] * (gL[v - 1] + gR[v - 1]) +
+                           nv[2] * (jL[v - 1] + jR[v - 1]));
+  }
+  double* out = P.flux + (size_t)side * 5 * npts + pt;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) out[v * npts] = F[v] * se;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Lifting surface flux (Lifting_FillFlux br1_fillflux.f90:49-91, EvalLiftingSurfFlux flux.f90:677-716):
+// lflux = 1/2 (V_slave - V_master) * SurfElem; the normal components are applied where consumed.
+// ------------------------------------------------------------------------------------------------
+static __global__ void lift_flux_kernel(KParams P, int NP, double* lf) {
+  if (halted(P)) return;
+  const int npts = NP * NP;
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (size_t)P.nSides * npts) return;
+  const int side = (int)(idx / npts), pt = (int)(idx - (size_t)side * npts);
+  const int* se5 = P.s2e + 5 * side;
+  int nM = P.basis->s2v[se5[2] - 1][0][pt];
+  int nS = P.basis->s2v[se5[3] - 1][se5[4]][pt];
+  const double* UM = P.U + 5 * ((size_t)se5[0] * NP * NP * NP + nM);
+  const double* US = P.U + 5 * ((size_t)se5[1] * NP * NP * NP + nS);
+  double uM[5], uS[5], VM[5], VS[5];
+  for (int v = 0; v < 5; ++v) { uM[v] = UM[v]; uS[v] = US[v]; }
+  lifting_var(P, uM, VM);
+  lifting_var(P, uS, VS);
+  double se = P.facegeo[(size_t)side * 10 * npts + 9 * npts + pt];
+  double* o = lf + (size_t)side * 5 * npts + pt;
+  for (int v = 0; v < 5; ++v) o[v * npts] = 0.5 * (VS[v] - VM[v]) * se;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Gradient kernel: BR1/BR2 lifting volume integral (br1_volint.f90:45-98 / br2_volint.f90),
+// surface integral (br1_surfint.f90:52-131 / br2_surfint.f90:53-148), Jacobian and
+// ConvertToGradPrimVec (equation_vars.f90:571-647).  One thread per volume node.
+// BR2 additionally writes the face traces gradP_master/slave = vol + etaBR2 * own-side surface term
+// into side buffers [side][master|slave][15][pt].
+// ------------------------------------------------------------------------------------------------
+template <int NP>
+__global__ void __launch_bounds__(512) gradient_kernel(KParams P, const double* lf, double* traces) {
+  if (halted(P)) return;
+  constexpr int NP3 = NP * NP * NP, N = NP - 1, NPT = NP * NP;
+  constexpr int EPB = (256 / NP3) > 0 ? (256 / NP3) : 1;
+  extern __shared__ double smem[];
+  double* sD = smem;                 // NP*NP
+  double* sV = sD + NP * NP;         // EPB * 5 * NP3
+  const int eb = threadIdx.x / NP3, n = threadIdx.x - eb * NP3;
+  const int e = blockIdx.x * EPB + eb;
+  const bool valid = e < P.nElems;
+  for (int z = threadIdx.x; z < NP * NP; z += blockDim.x) sD[z] = P.basis->D[(z / NP) * NP + (z % NP)];
+  const int i = n % NP, j = (n / NP) % NP, k = n / NPT;
+  double u[5];
+  double* myV = sV + (size_t)eb * 5 * NP3;
+  if (valid) {
+    const double* Ug = P.U + 5 * ((size_t)e * NP3 + n);
+    for (int v = 0; v < 5; ++v) u[v] = Ug[v];
+    double V[5];
+    lifting_var(P, u, V);
+    for (int v = 0; v < 5; ++v) myV[v * NP3 + n] = V[v];
+  }
+  __syncthreads();
+  if (!valid) return;
+  double gxi[5], geta[5], gzeta[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) { gxi[v] = 0.; geta[v] = 0.; gzeta[v] = 0.; }
+#pragma unroll
+  for (int l = 0; l < NP; ++l) {
+    const double di = sD[i * NP + l], dj = sD[j * NP + l], dk = sD[k * NP + l];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      gxi[v] += di * myV[v * NP3 + l + NP * (j + NP * k)];
+      geta[v] += dj * myV[v * NP3 + i + NP * (l + NP * k)];
+      gzeta[v] += dk * myV[v * NP3 + i + NP * (j + NP * l)];
+    }
+  }
+  const double* M = P.metrics + (size_t)e * 9 * NP3 + n;
+  double m[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) m[c] = M[c * NP3];
+  const double sj = P.sJ[(size_t)e * NP3 + n];
+  double g[3][5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) g[d][v] = m[0 + d] * gxi[v] + m[3 + d] * geta[v] + m[6 + d] * gzeta[v];
+  if (P.lifting == 2) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) g[d][v] *= sj;
+  }
+  int sides[3];
+  const int ns = boundary_sides(i, j, k, N, sides);
+  const double lh = P.basis->LhatM0;
+  double vol[3][5];
+  if (P.lifting == 2 && ns > 0) {
+    for (int d = 0; d < 3; ++d)
+      for (int v = 0; v < 5; ++v) vol[d][v] = g[d][v];
+  }
+  for (int z = 0; z < ns; ++z) {
+    const int s = sides[z];
+    const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
+    const int side = es[0], flip = es[1];
+    const int pt = P.basis->v2s[s - 1][flip][side_plane_coords(s, i, j, k, NP)];
+    const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
+    const double* F = lf + (size_t)side * 5 * NPT + pt;
+    if (P.lifting == 2) {
+      double surf[3][5], tr[3][5];
+      for (int v = 0; v < 5; ++v) {
+        const double fl = sj * lh * F[v * NPT];
+        for (int d = 0; d < 3; ++d) {
+          surf[d][v] = fl * nvec[d * NPT];
+          g[d][v] += surf[d][v];
+          tr[d][v] = vol[d][v] + P.etaBR2 * surf[d][v];
+        }
+      }
+      for (int d = 0; d < 3; ++d) to_grad_prim(P, u, tr[d]);
+      double* T = traces + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 15 * NPT + pt;
+      for (int d = 0; d < 3; ++d)
+        for (int v = 0; v < 5; ++v) T[(size_t)(5 * d + v) * NPT] = tr[d][v];
+    } else {
+      for (int v = 0; v < 5; ++v) {
+        const double fl = F[v * NPT] * lh;
+        for (int d = 0; d < 3; ++d) g[d][v] += fl * nvec[d * NPT];
+      }
+    }
+  }
+  if (P.lifting != 2) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) g[d][v] *= sj;
+  }
+  double* G = P.grad + 15 * ((size_t)e * NP3 + n);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    to_grad_prim(P, u, g[d]);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) G[5 * d + v] = g[d][v];
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Volume kernel: split-form volume integral (volint.f90:173-218 with EvalAdvFluxAverage3D
+// flux_average.f90:198-269), viscous volume integral (volint.f90:228-271), surface integral
+// (surfint.f90:177-184, :253-259), Jacobian (dg.f90:446), source (equation.f90:992-1071), and
+// optionally the fused LSERK stage (timedisc.f90:452-477).  One thread per volume node,
+// EPB elements per block; smem holds U, the auxiliaries and the metrics of the block's elements.
+// ------------------------------------------------------------------------------------------------
+template <int NP>
+__host__ __device__ constexpr int vol_epb() { return (256 / (NP * NP * NP)) > 0 ? (256 / (NP * NP * NP)) : 1; }
+
+template <int NP>
+__host__ __device__ constexpr size_t vol_smem_bytes() {
+  return sizeof(double) * (size_t)(3 * NP * NP + vol_epb<NP>() * 20 * NP * NP * NP);
+}
+
+template <int NP, int VF, bool VISC>
+__global__ void __launch_bounds__(vol_epb<NP>() * NP * NP * NP)
+volume_kernel(KParams P) {
+  if (halted(P)) return;
+  constexpr int NP3 = NP * NP * NP, N = NP - 1, NPT = NP * NP, EPB = vol_epb<NP>();
+  extern __shared__ double smem[];
+  double* sDvs = smem;                // NP*NP
+  double* sDhat = sDvs + NPT;         // NP*NP
+  double* sE = sDhat + NPT + NPT;     // per element: U[5][NP3], A[6][NP3], M[9][NP3]
+  const int eb = threadIdx.x / NP3, n = threadIdx.x - eb * NP3;
+  const int e = blockIdx.x * EPB + eb;
+  const bool valid = e < P.nElems;
+  for (int z = threadIdx.x; z < NPT; z += blockDim.x) {
+    sDvs[z] = P.basis->Dvs[z];
+    sDhat[z] = P.basis->Dhat[z];
+  }
+  double* sU = sE + (size_t)eb * 20 * NP3;
+  double* sA = sU + 5 * NP3;
+  double* sM = sA + 6 * NP3;
+  const int i = n % NP, j = (n / NP) % NP, k = n / NPT;
+  double u[5];
+  if (valid) {
+    const double* Ug = P.U + 5 * ((size_t)e * NP3 + n);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) { u[v] = Ug[v]; sU[v * NP3 + n] = u[v]; }
+    Aux a = eval_aux(P, u);
+    sA[0 * NP3 + n] = a.srho; sA[1 * NP3 + n] = a.v1; sA[2 * NP3 + n] = a.v2;
+    sA[3 * NP3 + n] = a.v3; sA[4 * NP3 + n] = a.p; sA[5 * NP3 + n] = a.v2s;
+    const double* Mg = P.metrics + (size_t)e * 9 * NP3;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) sM[c * NP3 + n] = Mg[c * NP3 + n];
+  }
+  __syncthreads();
+  double ut[5] = {0., 0., 0., 0., 0.};
+  if (valid) {
+    double UL[5], mL[3];
+    Aux aL;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) UL[v] = u[v];
+    aL.srho = sA[n]; aL.v1 = sA[NP3 + n]; aL.v2 = sA[2 * NP3 + n]; aL.v3 = sA[3 * NP3 + n];
+    aL.p = sA[4 * NP3 + n]; aL.v2s = sA[5 * NP3 + n];
+#pragma unroll
+    for (int dir = 0; dir < 3; ++dir) {
+      const int me = (dir == 0) ? i : (dir == 1 ? j : k);
+      const int stride = (dir == 0) ? 1 : (dir == 1 ? NP : NPT);
+      const int base = n - me * stride;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) mL[d] = sM[(3 * dir + d) * NP3 + n];
+#pragma unroll 1
+      for (int l = 0; l < NP; ++l) {
+        if (l == me) continue;
+        const int nl = base + l * stride;
+        double UR[5], mR[3], F[5];
+        Aux aR;
+#pragma unroll
+        for (int v = 0; v < 5; ++v) UR[v] = sU[v * NP3 + nl];
+        aR.srho = sA[nl]; aR.v1 = sA[NP3 + nl]; aR.v2 = sA[2 * NP3 + nl]; aR.v3 = sA[3 * NP3 + nl];
+        aR.p = sA[4 * NP3 + nl]; aR.v2s = sA[5 * NP3 + nl];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) mR[d] = sM[(3 * dir + d) * NP3 + nl];
+        volume_flux_vec<VF>(P, UL, UR, aL, aR, mL, mR, F);
+        const double dv = sDvs[me * NP + l];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) ut[v] += dv * F[v];
+      }
+    }
+  }
+  if constexpr (VISC) {
+    // contravariant viscous fluxes f~,g~,h~ (components 1..4) of every node into the A/M area
+    double m[9];
+    if (valid) {
+#pragma unroll
+      for (int c = 0; c < 9; ++c) m[c] = sM[c * NP3 + n];
+    }
+    __syncthreads();
+    double* sT = sA;  // [12][NP3]
+    if (valid) {
+      const double* G = P.grad + 15 * ((size_t)e * NP3 + n);
+      double gg[15];
+#pragma unroll
+      for (int c = 0; c < 15; ++c) gg[c] = G[c];
+      double f[4], g[4], h[4];
+      diff_flux_3d(P, u, gg, gg + 5, gg + 10, f, g, h);
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        sT[(0 + v) * NP3 + n] = f[v] * m[0] + g[v] * m[1] + h[v] * m[2];
+        sT[(4 + v) * NP3 + n] = f[v] * m[3] + g[v] * m[4] + h[v] * m[5];
+        sT[(8 + v) * NP3 + n] = f[v] * m[6] + g[v] * m[7] + h[v] * m[8];
+      }
+    }
+    __syncthreads();
+    if (valid) {
+#pragma unroll
+      for (int l = 0; l < NP; ++l) {
+        const double di = sDhat[i * NP + l], dj = sDhat[j * NP + l], dk = sDhat[k * NP + l];
+        const int ni = l + NP * (j + NP * k), nj = i + NP * (l + NP * k), nk = i + NP * (j + NP * l);
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          ut[1 + v] += di * sT[(0 + v) * NP3 + ni] + dj * sT[(4 + v) * NP3 + nj] + dk * sT[(8 + v) * NP3 + nk];
+      }
+    }
+  }
+  if (!valid) return;
+  // surface integral at the boundary nodes (LGL)
+  int sides[3];
+  const int ns = boundary_sides(i, j, k, N, sides);
+  const double lh = P.basis->LhatM0;
+  for (int z = 0; z < ns; ++z) {
+    const int s = sides[z];
+    const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
+    const int side = es[0], flip = es[1];
+    const int pt = P.basis->v2s[s - 1][flip][side_plane_coords(s, i, j, k, NP)];
+    const double* F = P.flux + (size_t)side * 5 * NPT + pt;
+    const double sg = (flip == 0) ? lh : -lh;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) ut[v] += sg * F[v * NPT];
+  }
+  // Ut = -Ut*sJ  (+ source)
+  const double sj = P.sJ[(size_t)e * NP3 + n];
+  const double tStage = P.dtDev ? (P.dtDev[1] + P.rkC * P.dtDev[0]) : P.t;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) ut[v] = ut[v] * (-sj);
+  if (P.source) {  // CalcSource CASE(4), equation.f90:1000-1024
+    const double* x = P.xGP + 3 * ((size_t)e * NP3 + n);
+    double arg = P.srcOmega * (x[0] + x[1] + x[2] - tStage);
+    double c = cos(arg), sn = sin(arg), s2 = 2. * sn * c;
+    ut[0] += P.srcTmp[0] * c;
+    double m = P.srcTmp[1] * c + P.srcTmp[2] * s2;
+    ut[1] += m; ut[2] += m; ut[3] += m;
+    ut[4] += P.srcTmp[3] * c + P.srcTmp[4] * s2 + P.srcTmp[5] * sn;
+  }
+  const size_t o = 5 * ((size_t)e * NP3 + n);
+  if (P.stage == 0) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) P.Ut[o + v] = ut[v];
+  } else {
+    // LSERK-2reg stage: Ut_tmp = Ut - A*Ut_tmp (stage 1: Ut_tmp = Ut); U = U + b*dt*Ut_tmp
+    const double dt = P.dtDev ? P.dtDev[0] : P.dt;
+    const double bdt = P.rkB * dt;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      double tmp = (P.stage == 1) ? ut[v] : ut[v] - P.UtTmp[o + v] * P.rkA;
+      P.UtTmp[o + v] = tmp;
+      P.U[o + v] = u[v] + tmp * bdt;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------------
+// CALCTIMESTEP (navierstokes/calctimestep.f90:39-170): per-element max eigenvalues, global min dt,
+// error code of the first bad element (last bad node in it).  dtBits holds the double bits of
+// the minimum (atomicMin on the bit pattern of non-negative doubles); errKey = elem*8 + errType.
+// ------------------------------------------------------------------------------------------------
+template <int NP, bool VISC>
+__global__ void __launch_bounds__(512) timestep_kernel(KParams P, unsigned long long* dtBits, int* errKey) {
+  if (halted(P)) return;
+  constexpr int NP3 = NP * NP * NP;
+  constexpr int EPB = (256 / NP3) > 0 ? (256 / NP3) : 1;
+  constexpr int RSTART = (NP3 > 256) ? 256 : (NP3 > 128) ? 128 : (NP3 > 64) ? 64 : (NP3 > 32) ? 32 : (NP3 > 16) ? 16 : (NP3 > 8) ? 8 : 4;
+  __shared__ double s_l[EPB][6][NP3];
+  __shared__ int s_err[EPB];
+  const int eb = threadIdx.x / NP3, n = threadIdx.x - eb * NP3;
+  const int e = blockIdx.x * EPB + eb;
+  const bool valid = e < P.nElems;
+  if (n == 0) s_err[eb] = -1;
+  __syncthreads();
+  double lam[6] = {1e-12, 1e-12, 1e-12, 1e-12, 1e-12, 1e-12};
+  int code = 0;
+  if (valid) {
+    const double* U = P.U + 5 * ((size_t)e * NP3 + n);
+    double u[5];
+    for (int v = 0; v < 5; ++v) u[v] = U[v];
+    if (isnan(u[0])) code = 1;
+    double sRho = 1. / u[0];
+    double vv[3] = {u[1] * sRho, u[2] * sRho, u[3] * sRho};
+    double p = P.kappaM1 * (u[4] - 0.5 * u[0] * (vv[0] * vv[0] + vv[1] * vv[1] + vv[2] * vv[2]));
+    if (p <= 0.) code = 2;
+    double c = sqrt(P.kappa * p * sRho);
+    const double* M = P.metrics + (size_t)e * 9 * NP3 + n;
+    const double sj = P.sJ[(size_t)e * NP3 + n];
+    double mu = 0.;
+    if (VISC) mu = sRho * P.KappasPrMax * visc_mu(P, p, sRho);
+    for (int d = 0; d < 3; ++d) {
+      double m0 = M[(3 * d + 0) * NP3], m1 = M[(3 * d + 1) * NP3], m2 = M[(3 * d + 2) * NP3];
+      lam[d] = sj * (fabs(m0 * vv[0] + m1 * vv[1] + m2 * vv[2]) + c * sqrt(m0 * m0 + m1 * m1 + m2 * m2));
+      if (VISC) {
+        double a = m0 * sj, b = m1 * sj, cc = m2 * sj;
+        lam[3 + d] = mu * (a * a + b * b + cc * cc);
+      }
+    }
+  }
+  // per-element max: tree reduction in shared memory
+  if (code != 0) atomicMax(&s_err[eb], n * 8 + code);
+  for (int d = 0; d < 6; ++d) s_l[eb][d][n] = lam[d];
+  __syncthreads();
+  for (int stride = RSTART; stride > 0; stride >>= 1) {
+    if (n < stride && n + stride < NP3)
+      for (int d = 0; d < 6; ++d) s_l[eb][d][n] = fmax(s_l[eb][d][n], s_l[eb][d][n + stride]);
+    __syncthreads();
+  }
+  for (int d = 0; d < 6; ++d) lam[d] = s_l[eb][d][0];
+  if (n != 0 || !valid) return;
+  int err = (s_err[eb] >= 0) ? (s_err[eb] & 7) : 0;
+  double dtE = P.CFLScale * 2. / (lam[0] + lam[1] + lam[2]);
+  if (isnan(dtE)) err = 3;
+  if (VISC) {
+    double dtV = P.DFLScale * 4. / (lam[3] + lam[4] + lam[5]);
+    if (isnan(dtV)) err = 4;
+    dtE = fmin(dtE, dtV);
+  }
+  if (err != 0) {
+    atomicMin(errKey, e * 8 + err);
+  } else {
+    atomicMin(dtBits, (unsigned long long)__double_as_longlong(dtE));
+  }
+}
+
+}  // namespace fluxo

@@ -1,0 +1,32 @@
+// Host-side launchers of the templated kernels (one translation unit per volume flux
+// family so that the instantiations compile in parallel).
+#pragma once
+#include <cstddef>
+#include <cuda_runtime.h>
+#include "common.cuh"
+
+namespace fluxo {
+
+struct LaunchError {
+  cudaError_t err;
+};
+
+// Volume kernel: NP in 2..9, VF in {0,1,2,5,10,32}.  Returns cudaErrorInvalidValue for
+// unsupported combinations.
+cudaError_t launch_volume(int NP, int VF, bool visc, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf0(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf1(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf2(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf5(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf10(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf32(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P);
+
+cudaError_t launch_face_flux(int RS, bool visc, int NP, int nSides, cudaStream_t s, const KParams& P);
+cudaError_t launch_lift_flux(int NP, int nSides, cudaStream_t s, const KParams& P);
+cudaError_t launch_gradient(int NP, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_timestep(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P,
+                            unsigned long long* dtBits, int* errKey);
+bool riemann_supported(int RS);
+bool volume_flux_supported(int VF);
+
+}  // namespace fluxo

@@ -1,0 +1,109 @@
+// Launchers of the face, lifting and time-step kernels and the volume-flux dispatcher.
+#include "kernels.cuh"
+#include "launch.h"
+
+namespace fluxo {
+
+cudaError_t launch_volume(int NP, int VF, bool visc, int nElems, cudaStream_t s, const KParams& P) {
+  switch (VF) {
+    case 0: return launch_volume_vf0(NP, visc, nElems, s, P);
+    case 1: return launch_volume_vf1(NP, visc, nElems, s, P);
+    case 2: return launch_volume_vf2(NP, visc, nElems, s, P);
+    case 5: return launch_volume_vf5(NP, visc, nElems, s, P);
+    case 10: return launch_volume_vf10(NP, visc, nElems, s, P);
+    case 32: return launch_volume_vf32(NP, visc, nElems, s, P);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+bool volume_flux_supported(int VF) {
+  return VF == 0 || VF == 1 || VF == 2 || VF == 5 || VF == 10 || VF == 32;
+}
+
+bool riemann_supported(int RS) {
+  switch (RS) {
+    case 0: case 1: case 22: case 4: case 44: case 33: case 5: case 9: case 32: case 6: case 13: case 14: case 16:
+      return true;
+    default:
+      return false;
+  }
+}
+
+template <int RS, bool VISC>
+static cudaError_t face_t(int NP, int nSides, cudaStream_t s, const KParams& P) {
+  const int npts = NP * NP;
+  const int spb = (128 / npts) > 0 ? (128 / npts) : 1;
+  const int grid = (nSides + spb - 1) / spb;
+  face_flux_kernel<RS, VISC><<<grid, spb * npts, 0, s>>>(P, NP);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_face_flux(int RS, bool visc, int NP, int nSides, cudaStream_t s, const KParams& P) {
+#define FLUXO_RS_CASE(K) \
+  case K: return visc ? face_t<K, true>(NP, nSides, s, P) : face_t<K, false>(NP, nSides, s, P);
+  switch (RS) {
+    FLUXO_RS_CASE(0) FLUXO_RS_CASE(1) FLUXO_RS_CASE(22) FLUXO_RS_CASE(4) FLUXO_RS_CASE(44)
+    FLUXO_RS_CASE(33) FLUXO_RS_CASE(5) FLUXO_RS_CASE(9) FLUXO_RS_CASE(32) FLUXO_RS_CASE(6)
+    FLUXO_RS_CASE(13) FLUXO_RS_CASE(14) FLUXO_RS_CASE(16)
+    default: return cudaErrorInvalidValue;
+  }
+#undef FLUXO_RS_CASE
+}
+
+cudaError_t launch_lift_flux(int NP, int nSides, cudaStream_t s, const KParams& P) {
+  const size_t n = (size_t)nSides * NP * NP;
+  const int grid = (int)((n + 255) / 256);
+  lift_flux_kernel<<<grid, 256, 0, s>>>(P, NP, P.lflux);
+  return cudaGetLastError();
+}
+
+template <int NP>
+static cudaError_t grad_t(int nElems, cudaStream_t s, const KParams& P) {
+  constexpr int NP3 = NP * NP * NP;
+  constexpr int EPB = (256 / NP3) > 0 ? (256 / NP3) : 1;
+  const size_t smem = sizeof(double) * (NP * NP + EPB * 5 * NP3);
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(gradient_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  gradient_kernel<NP><<<(nElems + EPB - 1) / EPB, EPB * NP3, smem, s>>>(P, P.lflux, P.gtrace);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gradient(int NP, int nElems, cudaStream_t s, const KParams& P) {
+  switch (NP) {
+    case 2: return grad_t<2>(nElems, s, P);
+    case 3: return grad_t<3>(nElems, s, P);
+    case 4: return grad_t<4>(nElems, s, P);
+    case 5: return grad_t<5>(nElems, s, P);
+    case 6: return grad_t<6>(nElems, s, P);
+    case 7: return grad_t<7>(nElems, s, P);
+    case 8: return grad_t<8>(nElems, s, P);
+    case 9: return grad_t<9>(nElems, s, P);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int NP, bool VISC>
+static cudaError_t dt_t(int nElems, cudaStream_t s, const KParams& P, unsigned long long* dtBits, int* errKey) {
+  constexpr int NP3 = NP * NP * NP;
+  constexpr int EPB = (256 / NP3) > 0 ? (256 / NP3) : 1;
+  timestep_kernel<NP, VISC><<<(nElems + EPB - 1) / EPB, EPB * NP3, 0, s>>>(P, dtBits, errKey);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_timestep(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P,
+                            unsigned long long* dtBits, int* errKey) {
+#define FLUXO_DT_CASE(K) \
+  case K: return visc ? dt_t<K, true>(nElems, s, P, dtBits, errKey) : dt_t<K, false>(nElems, s, P, dtBits, errKey);
+  switch (NP) {
+    FLUXO_DT_CASE(2) FLUXO_DT_CASE(3) FLUXO_DT_CASE(4) FLUXO_DT_CASE(5)
+    FLUXO_DT_CASE(6) FLUXO_DT_CASE(7) FLUXO_DT_CASE(8) FLUXO_DT_CASE(9)
+    default: return cudaErrorInvalidValue;
+  }
+#undef FLUXO_DT_CASE
+}
+
+}  // namespace fluxo

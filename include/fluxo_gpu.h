@@ -1,0 +1,161 @@
+/*
+ * fluxo_gpu.h — C ABI of the B200 (sm_100a, FP64) DGSEM right-hand side and
+ * LSERK time step.  It is the drop-in boundary for the reference's
+ * DGTimeDerivative / TimeStep / CALCTIMESTEP path: a Fortran host binds these
+ * entry points with ISO_C_BINDING and keeps its own
+ * parameter.ini parsing, mesh reading, analysis and output.
+ *
+ * Conventions
+ *  - Every entry point returns an int status: FLUXO_OK (0) or a negative
+ *    FLUXO_E* code.  The library never calls exit(); fluxo_gpu_last_error()
+ *    returns the message of the last failure on a handle.
+ *  - Host arrays use the reference's Fortran layouts, first index fastest:
+ *      U, Ut          (nVar,0:N,0:N,0:N,nElems)      src/dg/dg_vars.f90:75-80
+ *      Metrics_fTilde (3,0:N,0:N,0:N,nElems) (also g,h)  src/mesh/mesh.f90:251-256
+ *      sJ             (0:N,0:N,0:N,nElems)
+ *      NormVec, TangVec1, TangVec2 (3,0:N,0:N,1:nSides); SurfElem (0:N,0:N,1:nSides)
+ *      SideToElem     (5,1:nSides)  ElemToSide (2,6,nElems)   1-based ids, -1 = none
+ *  - Only conforming meshes whose sides are all inner sides (periodic boxes):
+ *    nBCSides = 0, no mortars, no MPI sides (the same single-process side
+ *    ranges as src/mesh/mesh.f90:171-183 with firstInnerSide = 1).
+ *  - One handle owns one CUDA stream; calls on a handle must be serialised by
+ *    the caller.  Distinct handles may be used from distinct host threads.
+ */
+#ifndef FLUXO_GPU_H
+#define FLUXO_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  FLUXO_OK = 0,
+  FLUXO_EINVAL_CFG = -1,  /* unsupported or inconsistent configuration / arguments */
+  FLUXO_ENOMEM_HBM = -2,  /* device allocation failed (or HBM budget refused) */
+  FLUXO_ECUDA = -3,       /* CUDA runtime error (message in last_error) */
+  FLUXO_ENAN_STATE = -4,  /* CALCTIMESTEP found an invalid state, see errType */
+  FLUXO_ETIMEOUT = -5,    /* a bounded device wait expired */
+  FLUXO_ENOTREADY = -6    /* mesh or state not set */
+};
+
+enum { FLUXO_EQN_EULER = 0, FLUXO_EQN_NAVIERSTOKES = 1 };
+
+/* Runtime configuration: the parameter.ini keys of the reference's hot path
+ * (src/equation/navierstokes/equation.f90:162-470, src/timedisc/timedisc.f90:74-137,
+ * src/dg/br2/br2.f90:91-149) plus the compile-time switches the reference fixes
+ * with CMake (PARABOLIC, PP_Lifting, PP_Lifting_Var, PP_VISC), which are runtime
+ * choices here.  LGL nodes and the split (flux-differencing) form are fixed. */
+typedef struct fluxo_cfg {
+  int struct_size;   /* sizeof(fluxo_cfg) */
+  int N;             /* N: polynomial degree, 1..7 (one thread per volume node) */
+  int eqn;           /* FLUXO_EQN_EULER (PARABOLIC=0) or FLUXO_EQN_NAVIERSTOKES */
+  int riemann;       /* Riemann: 0,1,22,4,44,33,5,9,32,6,13,14,16 */
+  int volume_flux;   /* VolumeFlux: 0,1,2,5,10,32 */
+  int lifting;       /* 1 = BR1 (br1.f90), 2 = BR2 (br2.f90) */
+  int lifting_var;   /* PP_Lifting_Var: 1 cons_var, 2 prim_var, 3 entropy_var */
+  int visc;          /* PP_VISC: 0 constant mu0, 1 Sutherland, 2 power law */
+  double kappa, R, Pr, mu0, Ts, Tref, ExpoSuth, ExpoPow, etaBR2;
+  int time_disc;     /* TimeDiscMethod: 0 carpenterrk4-5, 1 standardrk3-3 */
+  double cfl_scale;  /* CFLScale (unscaled, as read from parameter.ini) */
+  double dfl_scale;  /* DFLScale (unscaled) */
+  int ini_exact_func;   /* IniExactFunc: only 4 adds a source term (CalcSource) */
+  double ini_frequency, ini_amplitude;
+  int device;        /* CUDA device ordinal */
+} fluxo_cfg;
+
+typedef struct fluxo_handle fluxo_handle;
+
+/* InitEquation + InitDGbasis + InitTimeDisc equivalent.
+ * Replaces: src/equation/navierstokes/equation.f90:162 InitEquation,
+ *           src/dg/dg.f90:61 InitDG / :181 InitDGbasis,
+ *           src/timedisc/timedisc.f90:74 InitTimeDisc (coefficients, FillCFL_DFL :697). */
+int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out);
+
+/* Copies the geometry of InitMesh/CalcMetrics to the device.
+ * Replaces the module state read by the RHS: src/mesh/mesh_vars.f90:40-104
+ * (SideToElem, ElemToSide, Metrics_*Tilde, sJ, NormVec, TangVec1/2, SurfElem,
+ * Elem_xGP).  Elem_xGP may be NULL unless a source term is active. */
+int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* SideToElem,
+                       const int* ElemToSide, const double* Metrics_fTilde,
+                       const double* Metrics_gTilde, const double* Metrics_hTilde,
+                       const double* sJ, const double* NormVec, const double* TangVec1,
+                       const double* TangVec2, const double* SurfElem, const double* Elem_xGP);
+
+/* MOD_DG_Vars::U host <-> device (src/dg/dg_vars.f90:75).  The device copy is
+ * authoritative between set_state and get_state. */
+int fluxo_gpu_set_state(fluxo_handle* h, const double* U);
+int fluxo_gpu_get_state(fluxo_handle* h, double* U);
+/* MOD_DG_Vars::Ut after the last fluxo_gpu_dg_time_derivative (dg_vars.f90:80). */
+int fluxo_gpu_get_ut(fluxo_handle* h, double* Ut);
+/* Primitive-variable gradients gradPx/y/z (nVar,0:N,0:N,0:N,nElems) of the last RHS
+ * (src/dg/br1/br1_vars.f90 gradPx..); Navier-Stokes only. */
+int fluxo_gpu_get_gradients(fluxo_handle* h, double* gradPx, double* gradPy, double* gradPz);
+
+/* DGTimeDerivative_weakForm(tIn): device U -> device Ut.
+ * Replaces: src/dg/dg.f90:282-452. */
+int fluxo_gpu_dg_time_derivative(fluxo_handle* h, double t);
+
+/* CALCTIMESTEP(errType): minimum over elements of the convective (and viscous)
+ * time step; errType 1 NaN density, 2 p<=0, 3 NaN dt_conv, 4 NaN dt_visc.
+ * Replaces: src/equation/navierstokes/calctimestep.f90:39-170. */
+int fluxo_gpu_calc_timestep(fluxo_handle* h, double* dt, int* errType);
+
+/* One full low-storage RK step from t with step dt (U updated in place).
+ * Replaces: src/timedisc/timedisc.f90:424-480 TimeStepByLSERKW2 (TimeStep pointer). */
+int fluxo_gpu_timestep(fluxo_handle* h, double t, double dt);
+
+/* The TimeDisc loop (src/timedisc/timedisc.f90:274-359) without output: per step
+ * CALCTIMESTEP on the device, dt clipped to tEnd, one LSERK step, until
+ * t >= tEnd or maxIter steps (maxIter < 0: no limit).  The host does not
+ * synchronise between steps.  Returns the final time, the steps taken and the
+ * errType that stopped the loop (0 = none). */
+int fluxo_gpu_time_disc(fluxo_handle* h, double t, double tEnd, int maxIter, double* tOut,
+                        int* nIter, int* errType);
+
+/* Device pointers and stream for zero-copy callers (e.g. torch tensors):
+ * U, Ut are device buffers of nVar*(N+1)^3*nElems doubles in the host layout. */
+int fluxo_gpu_device_buffers(fluxo_handle* h, double** dU, double** dUt, void** stream);
+/* Number of kernels this handle launched so far. */
+int fluxo_gpu_launch_count(fluxo_handle* h, uint64_t* n);
+
+/* Per-kernel timing with CUDA events on the handle's stream (off by default).
+ * kind: 0 lifting surface flux, 1 gradient, 2 face flux, 3 volume, 4 time step.
+ * fluxo_gpu_get_profile synchronises, returns the summed milliseconds and launch count of
+ * that kind since profiling was enabled, and resets them. */
+int fluxo_gpu_set_profiling(fluxo_handle* h, int enable);
+int fluxo_gpu_get_profile(fluxo_handle* h, int kind, double* total_ms, uint64_t* count);
+
+/* FP64 FMA throughput of the device (a register-resident DFMA loop over all SMs), in TFLOP/s
+ * counting an FMA as 2 flops: the denominator of the FP64 roofline. */
+int fluxo_gpu_fp64_peak(int device, double* tflops);
+
+int fluxo_gpu_destroy(fluxo_handle* h);
+/* Copies the last error message of the handle (or of the last failed create if h is NULL). */
+int fluxo_gpu_last_error(fluxo_handle* h, char* buf, size_t len);
+
+/* ------------------------------------------------------------------------------------------
+ * Host-side setup (no GPU needed).  The reference builds these arrays in InitMesh /
+ * CalcMetrics from an HDF5 (HOPR) mesh; here they are generated for a periodic box
+ * of nx*ny*nz hexahedra whose NGeo node coordinates are deformed by
+ * X_d += amp * prod_e sin(2*pi*(x_e-c_e)/L_e).  Outputs use the layouts above.
+ * Replaces: src/mesh/mesh.f90:89-296 InitMesh (with meshdeform :238-245),
+ *           src/mesh/metrics.f90:78-484 CalcMetrics / CalcSurfMetrics (curl form).
+ * ------------------------------------------------------------------------------------------ */
+int fluxo_host_box_sizes(const int* nElemsXYZ, int* nElems, int* nSides);
+int fluxo_host_box_mesh(int N, const int* nElemsXYZ, const double* xmin, const double* xmax, int NGeo,
+                        double deform_amp, int* SideToElem, int* ElemToSide, double* Metrics_fTilde,
+                        double* Metrics_gTilde, double* Metrics_hTilde, double* sJ, double* NormVec,
+                        double* TangVec1, double* TangVec2, double* SurfElem, double* Elem_xGP);
+/* FillIni(IniExactFunc, U) on the given node coordinates (src/equation/navierstokes/equation.f90:575-950):
+ * IniExactFunc 1 (constant refstate, prim given), 2 (density sine wave), 4 (manufactured), 7 (Taylor-Green). */
+int fluxo_host_exact_func(int func, double t, size_t nPoints, const double* x, double kappa,
+                          const double* adv_vel, double ini_amplitude, const double* ini_wavenumber,
+                          double ini_frequency, const double* ref_state_prim, double* U);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLUXO_GPU_H */

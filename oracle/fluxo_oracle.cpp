@@ -1336,10 +1336,13 @@ void ProlongToFace(Case& C, const std::vector<real>& Uvol, std::vector<real>& Um
 void VolIntSplitForm(Case& C) {
   int n = C.np, N = C.N;
   size_t nv = (size_t)n * n * n;
+#pragma omp parallel
+  {
   std::vector<real> aux(6 * nv), ft((size_t)5 * n * nv), gt((size_t)5 * n * nv), ht((size_t)5 * n * nv);
   auto F4 = [&](std::vector<real>& A, int v, int l, int i, int j, int k) -> real& {
     return A[v + 5 * ((size_t)l + n * ((size_t)i + n * ((size_t)j + (size_t)n * k)))];
   };
+#pragma omp for schedule(static)
   for (int e = 0; e < C.nElems; ++e) {
     for (size_t z = 0; z < nv; ++z) EvalUaux(C, &C.U[5 * (nv * e + z)], &aux[6 * z]);
     auto Up = [&](int i, int j, int k) { return &C.U[C.vol(0, i, j, k, e)]; };
@@ -1387,13 +1390,17 @@ void VolIntSplitForm(Case& C) {
                                            C.Dvolsurf_T[l + n * j] * F4(gt, v, l, i, j, k) +
                                            C.Dvolsurf_T[l + n * k] * F4(ht, v, l, i, j, k);
   }
+  }
 }
 
 // VolInt_visc + EvalDiffFluxTilde3D, dg/volint.f90:228-271, navierstokes/flux.f90:523-635
 void VolIntVisc(Case& C) {
   int n = C.np;
   size_t nv = (size_t)n * n * n;
+#pragma omp parallel
+  {
   std::vector<real> ft(5 * nv), gt(5 * nv), ht(5 * nv);
+#pragma omp for schedule(static)
   for (int e = 0; e < C.nElems; ++e) {
     for (size_t z = 0; z < nv; ++z) {
       size_t o = nv * e + z;
@@ -1417,6 +1424,7 @@ void VolIntVisc(Case& C) {
                                            C.Dhat_T[l + n * i] * ft[5 * (l + n * (j + n * k)) + v] +
                                            C.Dhat_T[l + n * j] * gt[5 * (i + n * (l + n * k)) + v] +
                                            C.Dhat_T[l + n * k] * ht[5 * (i + n * (j + n * l)) + v];
+  }
   }
 }
 
@@ -1445,7 +1453,10 @@ void Lifting(Case& C) {
         }
       }
   // Lifting_VolInt: br1_volint.f90:45-98 (BR1) / br2_volint.f90:45-103 (BR2 includes sJ)
+#pragma omp parallel
+  {
   std::vector<real> Fl(5 * nv);
+#pragma omp for schedule(static)
   for (int e = 0; e < C.nElems; ++e) {
     for (size_t z = 0; z < nv; ++z) LiftingVar(C, &C.U[5 * (nv * e + z)], &Fl[5 * z]);
     for (int k = 0; k < n; ++k)
@@ -1477,6 +1488,7 @@ void Lifting(Case& C) {
             C.gz[5 * o + v] = C.gz[5 * o + v] + az;
           }
         }
+  }
   }
   if (!br2) {
     // BR1_SurfInt (br1_surfint.f90:52-131), then Jacobian, ConvertToGradPrim, prolong
@@ -1569,7 +1581,10 @@ void Lifting(Case& C) {
 // FillFlux, dg/fillflux.f90:41-110 with Riemann (riemann.f90:104-169)
 void FillFlux(Case& C) {
   int n = C.np, npts = n * n;
+#pragma omp parallel
+  {
   std::vector<real> ULL(5 * npts), URR(5 * npts), F(5 * npts);
+#pragma omp for schedule(static)
   for (int sid = 0; sid < C.nSides; ++sid) {
     for (int z = 0; z < npts; ++z) {  // RotateState, riemann.f90:218-231
       size_t fi = (size_t)npts * sid + z;
@@ -1619,6 +1634,7 @@ void FillFlux(Case& C) {
       }
     }
   }
+  }
 }
 
 // SurfInt (LGL), dg/surfint.f90:48-264
@@ -1648,16 +1664,27 @@ void SurfInt(Case& C) {
   }
 }
 
+uint64_t g_phase[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+struct PhaseCount {  // operation count of one phase of the RHS (counting build)
+  int k;
+  uint64_t start;
+  explicit PhaseCount(int k_) : k(k_), start(g_oracle_flops) {}
+  ~PhaseCount() { g_phase[k] += g_oracle_flops - start; }
+};
+
+// Phases: 0 volume split form, 1 lifting, 2 viscous volume integral, 3 face fluxes,
+//         4 surface integral, 5 Jacobian + source
 void DGTimeDerivative(Case& C, double t) {
   std::fill(C.Ut.begin(), C.Ut.end(), real(0.));  // VNullify
   ProlongToFace(C, C.U, C.Umaster, C.Uslave);
-  VolIntSplitForm(C);
+  { PhaseCount pc(0); VolIntSplitForm(C); }
   if (C.parabolic) {
-    Lifting(C);
-    VolIntVisc(C);
+    { PhaseCount pc(1); Lifting(C); }
+    { PhaseCount pc(2); VolIntVisc(C); }
   }
-  FillFlux(C);
-  SurfInt(C);
+  { PhaseCount pc(3); FillFlux(C); }
+  { PhaseCount pc(4); SurfInt(C); }
+  PhaseCount pc(5);
   size_t nd = (size_t)C.np * C.np * C.np * C.nElems;
   for (size_t z = 0; z < nd; ++z)  // V2D_M_V1D(Ut,-sJ), vector.f90:144-166
     for (int v = 0; v < 5; ++v) C.Ut[5 * z + v] = C.Ut[5 * z + v] * (-C.sJ[z]);
@@ -1969,7 +1996,11 @@ void orc_basis(int N, double* xGP, double* wGP, double* wBary, double* D, double
 }
 
 uint64_t orc_flops(void) { return g_oracle_flops; }
-void orc_reset_flops(void) { g_oracle_flops = 0; }
+uint64_t orc_phase_flops(int k) { return (k >= 0 && k < 8) ? g_phase[k] : 0; }
+void orc_reset_flops(void) {
+  g_oracle_flops = 0;
+  for (int k = 0; k < 8; ++k) g_phase[k] = 0;
+}
 
 void orc_volume_flux(void* h, const double* UL, const double* UR, const double* mL, const double* mR, double* F) {
   Case* C = (Case*)h;

@@ -73,6 +73,9 @@ void orc_basis(int N, double* xGP, double* wGP, double* wBary, double* D,
                double* Dvolsurf, double* Dhat, double* Lminus, double* Lplus);
 /* Operation counter (only meaningful in the counting build). */
 uint64_t orc_flops(void);
+/* Per-phase counts: 0 split-form volume, 1 lifting, 2 viscous volume, 3 face fluxes,
+   4 surface integral, 5 Jacobian + source. */
+uint64_t orc_phase_flops(int phase);
 void orc_reset_flops(void);
 /* Two-point volume flux and Riemann solver at single points (unit tests). */
 void orc_volume_flux(void* h, const double* UL, const double* UR, const double* mL,

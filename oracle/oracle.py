@@ -99,6 +99,8 @@ def _lib(counting=False):
     lib.orc_exact_func.argtypes = [ctypes.c_void_p, i, d, i, ctypes.c_void_p, ctypes.c_void_p]
     lib.orc_basis.argtypes = [i] + [ctypes.c_void_p] * 8
     lib.orc_flops.restype = ctypes.c_uint64
+    lib.orc_phase_flops.restype = ctypes.c_uint64
+    lib.orc_phase_flops.argtypes = [i]
     lib.orc_volume_flux.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 5
     lib.orc_riemann_point.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 6
     lib.orc_ln_mean.restype = d
@@ -253,13 +255,18 @@ def basis(N):
     return out
 
 
+PHASES = ("volume_split_form", "lifting", "volume_viscous", "face_flux", "surface_integral", "jacobian_source")
+
+
 def count_flops(**kw):
-    """FP64 operation count of one DGTimeDerivative (counting build)."""
+    """FP64 operation count of one DGTimeDerivative (counting build): total and per phase,
+    both per DOF.  Counting rules in oracle/counted.h."""
     lib = _lib(counting=True)
     c = OracleCase(counting=True, **kw)
     lib.orc_reset_flops()
     c.dg_time_derivative(0.0)
-    return int(lib.orc_flops()), c.nElems * c.np ** 3
+    nd = c.nElems * c.np ** 3
+    return int(lib.orc_flops()) / nd, {k: int(lib.orc_phase_flops(i)) / nd for i, k in enumerate(PHASES)}
 
 
 def ln_mean(a, b):
