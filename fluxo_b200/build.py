@@ -41,15 +41,18 @@ def _headers():
     return hs
 
 
-def build(verbose=False, jobs=None, extra_flags=()):
-    os.makedirs(BUILD, exist_ok=True)
+def build(verbose=False, jobs=None, extra_flags=(), build_dir=None, lib_path=None):
+    """Compiles (incrementally) and links the library; extra_flags go to nvcc."""
+    BUILD_ = build_dir or BUILD
+    LIB_ = lib_path or LIB
+    os.makedirs(BUILD_, exist_ok=True)
     nvcc = _nvcc()
     hdrs = _headers()
     cmds = []
     objs = []
     for src in CU_SOURCES + CPP_SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src + ".o")
+        o = os.path.join(BUILD_, src + ".o")
         objs.append(o)
         if not _stale(o, [s] + hdrs):
             continue
@@ -70,12 +73,12 @@ def build(verbose=False, jobs=None, extra_flags=()):
                 print(r.stdout + r.stderr)
             if r.returncode != 0:
                 raise RuntimeError("compile failed: %s\n%s%s" % (" ".join(cmd), r.stdout, r.stderr))
-    if cmds or not os.path.exists(LIB):
-        link = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-Xcompiler", "-fopenmp", "-lgomp", "-lcudart"]
+    if cmds or not os.path.exists(LIB_):
+        link = [nvcc] + ARCH + ["-shared", "-o", LIB_] + objs + ["-Xcompiler", "-fopenmp", "-lgomp", "-lcudart"]
         r = subprocess.run(link, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stdout + r.stderr)
-    return LIB
+    return LIB_
 
 
 if __name__ == "__main__":

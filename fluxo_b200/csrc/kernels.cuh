@@ -8,6 +8,7 @@
 #pragma once
 #include "common.cuh"
 #include "physics_ns.cuh"
+#include "volume_pairs.cuh"
 
 namespace fluxo {
 
@@ -255,95 +256,164 @@ __global__ void __launch_bounds__(512) gradient_kernel(KParams P, const double* 
 // Volume kernel: split-form volume integral (volint.f90:173-218 with EvalAdvFluxAverage3D
 // flux_average.f90:198-269), viscous volume integral (volint.f90:228-271), surface integral
 // (surfint.f90:177-184, :253-259), Jacobian (dg.f90:446), source (equation.f90:992-1071), and
-// optionally the fused LSERK stage (timedisc.f90:452-477).  One thread per volume node,
-// EPB elements per block; smem holds U, the auxiliaries and the metrics of the block's elements.
+// optionally the fused LSERK stage (timedisc.f90:452-477).
+//
+// One thread per volume node, EPB elements per block.  Each node's record (volume_pairs.cuh) and
+// the metrics sit in shared memory.  For each direction the threads of one line evaluate every
+// pair of the line exactly once (the reference's symmetric reuse, flux_average.f90:232-243):
+// in round d thread p takes the pair (p, p+d mod NP); its own contribution stays in registers,
+// the partner's goes to a shared accumulator, and no two threads of a round touch the same
+// accumulator.  Lines are contiguous in the thread index in every direction, so for NP = 2, 4, 8 a
+// line lives in one warp and rounds need only a warp barrier.
 // ------------------------------------------------------------------------------------------------
 template <int NP>
 __host__ __device__ constexpr int vol_epb() { return (256 / (NP * NP * NP)) > 0 ? (256 / (NP * NP * NP)) : 1; }
 
+// Padded slot of node n in the shared record/accumulator arrays: one spare slot every 16 nodes
+// spreads the eta- and zeta-lines (node strides NP and NP^2) over the shared-memory banks.
+__host__ __device__ constexpr int vol_slot(int n) { return n + (n >> 4); }
+
 template <int NP>
+__host__ __device__ constexpr int vol_slots() { return vol_slot(NP * NP * NP - 1) + 1; }
+
+template <int NP, int VF>
 __host__ __device__ constexpr size_t vol_smem_bytes() {
-  return sizeof(double) * (size_t)(3 * NP * NP + vol_epb<NP>() * 20 * NP * NP * NP);
+  return sizeof(double) * (size_t)(2 * NP * NP + vol_epb<NP>() * (VolRec<VF>::RS + 5) * vol_slots<NP>());
+}
+
+template <int NP>
+__device__ __forceinline__ void line_sync() {
+  if constexpr (32 % NP == 0) __syncwarp();
+  else __syncthreads();
 }
 
 template <int NP, int VF, bool VISC>
-__global__ void __launch_bounds__(vol_epb<NP>() * NP * NP * NP)
+#ifndef FLUXO_VOL_MINB
+#define FLUXO_VOL_MINB 2  // resident blocks per SM the register allocation must allow
+#endif
+__global__ void __launch_bounds__(vol_epb<NP>() * NP * NP * NP, FLUXO_VOL_MINB)
 volume_kernel(KParams P) {
   if (halted(P)) return;
   constexpr int NP3 = NP * NP * NP, N = NP - 1, NPT = NP * NP, EPB = vol_epb<NP>();
+  constexpr int RS = VolRec<VF>::RS, NQ = VolRec<VF>::NQ;
   extern __shared__ double smem[];
-  double* sDvs = smem;                // NP*NP
-  double* sDhat = sDvs + NPT;         // NP*NP
-  double* sE = sDhat + NPT + NPT;     // per element: U[5][NP3], A[6][NP3], M[9][NP3]
-  const int eb = threadIdx.x / NP3, n = threadIdx.x - eb * NP3;
+  double* sDvs = smem;         // Dvolsurf(i,l) at [i*NP+l]
+  double* sDhat = sDvs + NPT;  // D_hat(i,l)
+  const int eb = threadIdx.x / NP3, t = threadIdx.x - eb * NP3;
   const int e = blockIdx.x * EPB + eb;
   const bool valid = e < P.nElems;
+  constexpr int NS = vol_slots<NP>();
+  double* rec = sDhat + NPT + (size_t)eb * (RS + 5) * NS;  // [slot][RS]
+  double* acc = rec + (size_t)RS * NS;                     // [slot][5]
   for (int z = threadIdx.x; z < NPT; z += blockDim.x) {
     sDvs[z] = P.basis->Dvs[z];
     sDhat[z] = P.basis->Dhat[z];
   }
-  double* sU = sE + (size_t)eb * 20 * NP3;
-  double* sA = sU + 5 * NP3;
-  double* sM = sA + 6 * NP3;
-  const int i = n % NP, j = (n / NP) % NP, k = n / NPT;
   double u[5];
   if (valid) {
-    const double* Ug = P.U + 5 * ((size_t)e * NP3 + n);
+    const double* Ug = P.U + 5 * ((size_t)e * NP3 + t);
 #pragma unroll
-    for (int v = 0; v < 5; ++v) { u[v] = Ug[v]; sU[v * NP3 + n] = u[v]; }
-    Aux a = eval_aux(P, u);
-    sA[0 * NP3 + n] = a.srho; sA[1 * NP3 + n] = a.v1; sA[2 * NP3 + n] = a.v2;
-    sA[3 * NP3 + n] = a.v3; sA[4 * NP3 + n] = a.p; sA[5 * NP3 + n] = a.v2s;
-    const double* Mg = P.metrics + (size_t)e * 9 * NP3;
+    for (int v = 0; v < 5; ++v) u[v] = Ug[v];
+    double* r = rec + vol_slot(t) * RS;
+    make_record<VF>(P, u, r);
+    const double* Mg = P.metrics + (size_t)e * 9 * NP3 + t;
 #pragma unroll
-    for (int c = 0; c < 9; ++c) sM[c * NP3 + n] = Mg[c * NP3 + n];
+    for (int c = 0; c < 9; ++c) r[NQ + c] = Mg[c * NP3];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) acc[vol_slot(t) * 5 + v] = 0.;
   }
   __syncthreads();
-  double ut[5] = {0., 0., 0., 0., 0.};
-  if (valid) {
-    double UL[5], mL[3];
-    Aux aL;
-#pragma unroll
-    for (int v = 0; v < 5; ++v) UL[v] = u[v];
-    aL.srho = sA[n]; aL.v1 = sA[NP3 + n]; aL.v2 = sA[2 * NP3 + n]; aL.v3 = sA[3 * NP3 + n];
-    aL.p = sA[4 * NP3 + n]; aL.v2s = sA[5 * NP3 + n];
-#pragma unroll
-    for (int dir = 0; dir < 3; ++dir) {
-      const int me = (dir == 0) ? i : (dir == 1 ? j : k);
-      const int stride = (dir == 0) ? 1 : (dir == 1 ? NP : NPT);
-      const int base = n - me * stride;
-#pragma unroll
-      for (int d = 0; d < 3; ++d) mL[d] = sM[(3 * dir + d) * NP3 + n];
+  // split-form volume integral, line by line
+  {
+    const int p = t % NP, Ln = t / NP, la = Ln % NP, lb = Ln / NP;
 #pragma unroll 1
-      for (int l = 0; l < NP; ++l) {
-        if (l == me) continue;
-        const int nl = base + l * stride;
-        double UR[5], mR[3], F[5];
-        Aux aR;
+    for (int dir = 0; dir < 3; ++dir) {
+      const int stride = dir == 0 ? 1 : (dir == 1 ? NP : NPT);
+      const int base = dir == 0 ? NP * (la + NP * lb) : (dir == 1 ? la + NPT * lb : la + NP * lb);
+      const int own = base + p * stride, os = vol_slot(own);
+      double ro[NQ], mo[3], racc[5] = {0., 0., 0., 0., 0.};
+      if (valid) {
 #pragma unroll
-        for (int v = 0; v < 5; ++v) UR[v] = sU[v * NP3 + nl];
-        aR.srho = sA[nl]; aR.v1 = sA[NP3 + nl]; aR.v2 = sA[2 * NP3 + nl]; aR.v3 = sA[3 * NP3 + nl];
-        aR.p = sA[4 * NP3 + nl]; aR.v2s = sA[5 * NP3 + nl];
+        for (int z = 0; z < NQ; ++z) ro[z] = rec[os * RS + z];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) mR[d] = sM[(3 * dir + d) * NP3 + nl];
-        volume_flux_vec<VF>(P, UL, UR, aL, aR, mL, mR, F);
-        const double dv = sDvs[me * NP + l];
-#pragma unroll
-        for (int v = 0; v < 5; ++v) ut[v] += dv * F[v];
+        for (int c = 0; c < 3; ++c) mo[c] = rec[os * RS + NQ + 3 * dir + c];
       }
+      if constexpr (32 % NP == 0) {
+        // the line's threads are NP consecutive lanes of one warp: the partner's share of each
+        // pair flux travels by warp shuffle to the partner's lane, so the rounds share no state
+        const int lane = threadIdx.x & 31, lbase = lane - p;
+#pragma unroll
+        for (int d = 1; d <= NP / 2; ++d) {
+          const bool active = valid && (2 * d < NP || p < d);
+          int q = p + d;
+          if (q >= NP) q -= NP;
+          double F[5] = {0., 0., 0., 0., 0.};
+          if (active) {
+            const int nq = vol_slot(base + q * stride);
+            double rp[NQ], mp[3];
+#pragma unroll
+            for (int z = 0; z < NQ; ++z) rp[z] = rec[nq * RS + z];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) mp[c] = rec[nq * RS + NQ + 3 * dir + c];
+            pair_flux<VF>(P, ro, rp, mo, mp, F);
+          }
+          const double dOwn = sDvs[p * NP + q], dPart = sDvs[q * NP + p];
+          int src = p - d;
+          if (src < 0) src += NP;
+          const bool receive = valid && (2 * d < NP || p >= d);
+#pragma unroll
+          for (int v = 0; v < 5; ++v) {
+            racc[v] += active ? dOwn * F[v] : 0.;
+            const double got = __shfl_sync(0xffffffffu, dPart * F[v], lbase + src);
+            racc[v] += receive ? got : 0.;
+          }
+        }
+      } else {
+#pragma unroll 1
+        for (int d = 1; d <= NP / 2; ++d) {
+          const bool active = valid && (2 * d < NP || p < d);
+          if (active) {
+            int q = p + d;
+            if (q >= NP) q -= NP;
+            const int nq = vol_slot(base + q * stride);
+            double rp[NQ], mp[3], F[5];
+#pragma unroll
+            for (int z = 0; z < NQ; ++z) rp[z] = rec[nq * RS + z];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) mp[c] = rec[nq * RS + NQ + 3 * dir + c];
+            pair_flux<VF>(P, ro, rp, mo, mp, F);
+            const double dOwn = sDvs[p * NP + q], dPart = sDvs[q * NP + p];
+#pragma unroll
+            for (int v = 0; v < 5; ++v) {
+              racc[v] += dOwn * F[v];
+              acc[nq * 5 + v] += dPart * F[v];
+            }
+          }
+          __syncthreads();
+        }
+      }
+      if (valid) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) acc[os * 5 + v] += racc[v];
+      }
+      __syncthreads();
     }
   }
+  double ut[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) ut[v] = valid ? acc[vol_slot(t) * 5 + v] : 0.;
+  const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
   if constexpr (VISC) {
-    // contravariant viscous fluxes f~,g~,h~ (components 1..4) of every node into the A/M area
+    // contravariant viscous fluxes f~,g~,h~ (components 1..4) of every node, into the record area
     double m[9];
     if (valid) {
 #pragma unroll
-      for (int c = 0; c < 9; ++c) m[c] = sM[c * NP3 + n];
+      for (int c = 0; c < 9; ++c) m[c] = rec[vol_slot(t) * RS + NQ + c];
     }
     __syncthreads();
-    double* sT = sA;  // [12][NP3]
+    double* sT = rec;  // [12][NP3]
     if (valid) {
-      const double* G = P.grad + 15 * ((size_t)e * NP3 + n);
+      const double* G = P.grad + 15 * ((size_t)e * NP3 + t);
       double gg[15];
 #pragma unroll
       for (int c = 0; c < 15; ++c) gg[c] = G[c];
@@ -351,9 +421,9 @@ volume_kernel(KParams P) {
       diff_flux_3d(P, u, gg, gg + 5, gg + 10, f, g, h);
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
-        sT[(0 + v) * NP3 + n] = f[v] * m[0] + g[v] * m[1] + h[v] * m[2];
-        sT[(4 + v) * NP3 + n] = f[v] * m[3] + g[v] * m[4] + h[v] * m[5];
-        sT[(8 + v) * NP3 + n] = f[v] * m[6] + g[v] * m[7] + h[v] * m[8];
+        sT[(0 + v) * NP3 + t] = f[v] * m[0] + g[v] * m[1] + h[v] * m[2];
+        sT[(4 + v) * NP3 + t] = f[v] * m[3] + g[v] * m[4] + h[v] * m[5];
+        sT[(8 + v) * NP3 + t] = f[v] * m[6] + g[v] * m[7] + h[v] * m[8];
       }
     }
     __syncthreads();
@@ -384,20 +454,20 @@ volume_kernel(KParams P) {
     for (int v = 0; v < 5; ++v) ut[v] += sg * F[v * NPT];
   }
   // Ut = -Ut*sJ  (+ source)
-  const double sj = P.sJ[(size_t)e * NP3 + n];
+  const double sj = P.sJ[(size_t)e * NP3 + t];
   const double tStage = P.dtDev ? (P.dtDev[1] + P.rkC * P.dtDev[0]) : P.t;
 #pragma unroll
   for (int v = 0; v < 5; ++v) ut[v] = ut[v] * (-sj);
   if (P.source) {  // CalcSource CASE(4), equation.f90:1000-1024
-    const double* x = P.xGP + 3 * ((size_t)e * NP3 + n);
+    const double* x = P.xGP + 3 * ((size_t)e * NP3 + t);
     double arg = P.srcOmega * (x[0] + x[1] + x[2] - tStage);
     double c = cos(arg), sn = sin(arg), s2 = 2. * sn * c;
     ut[0] += P.srcTmp[0] * c;
-    double m = P.srcTmp[1] * c + P.srcTmp[2] * s2;
-    ut[1] += m; ut[2] += m; ut[3] += m;
+    double mm = P.srcTmp[1] * c + P.srcTmp[2] * s2;
+    ut[1] += mm; ut[2] += mm; ut[3] += mm;
     ut[4] += P.srcTmp[3] * c + P.srcTmp[4] * s2 + P.srcTmp[5] * sn;
   }
-  const size_t o = 5 * ((size_t)e * NP3 + n);
+  const size_t o = 5 * ((size_t)e * NP3 + t);
   if (P.stage == 0) {
 #pragma unroll
     for (int v = 0; v < 5; ++v) P.Ut[o + v] = ut[v];

@@ -406,7 +406,8 @@ __device__ __forceinline__ void lifting_var(const KParams& P, const double* U, d
     double u = U[1] * srho, v = U[2] * srho, w = U[3] * srho;
     double v2s2 = 0.5 * (u * u + v * v + w * w);
     double rho_sp = U[0] / (P.kappaM1 * (U[4] - U[0] * v2s2));
-    double s = -log(rho_sp * pow(U[0], P.kappaM1));
+    // s = -log(rho_sp * rho^(kappa-1)), written with two logarithms instead of log + pow
+    double s = -(log(rho_sp) + P.kappaM1 * log(U[0]));
     V[0] = (P.kappa - s) * P.sKappaM1 - rho_sp * v2s2;
     V[1] = rho_sp * u; V[2] = rho_sp * v; V[3] = rho_sp * w;
     V[4] = -rho_sp;

@@ -11,7 +11,7 @@ namespace fluxo {
 template <int NP, bool VISC>
 static cudaError_t vol_launch_t(int nElems, cudaStream_t s, const KParams& P) {
   constexpr int EPB = vol_epb<NP>();
-  constexpr size_t smem = vol_smem_bytes<NP>();
+  constexpr size_t smem = vol_smem_bytes<NP, VF_ID>();
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(volume_kernel<NP, VF_ID, VISC>,
