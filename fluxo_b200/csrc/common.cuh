@@ -42,7 +42,8 @@ struct KParams {
   double* U;
   double* Ut;
   double* UtTmp;
-  double* grad;
+  double* grad;           // volume gradients [elem][node][3][var], written only when non-null
+  double* utvisc;         // viscous volume integral [elem][4][node] (momentum and energy)
   // geometry
   const double* metrics;
   const double* sJ;
@@ -73,5 +74,11 @@ struct KParams {
 };
 
 __device__ __forceinline__ bool halted(const KParams& P) { return P.haltFlag && *P.haltFlag != 0; }
+
+// Asks the memory system to bring the line holding p into L2 (no register result, no fault on the
+// caller's side: only addresses inside live allocations are passed).
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
 
 }  // namespace fluxo

@@ -76,7 +76,7 @@ struct fluxo_handle {
   cudaStream_t stream = nullptr;
   BasisTables hb{};
   BasisTables* dBasis = nullptr;
-  double *dU = nullptr, *dUt = nullptr, *dUtTmp = nullptr, *dGrad = nullptr;
+  double *dU = nullptr, *dUt = nullptr, *dUtTmp = nullptr, *dGrad = nullptr, *dUtVisc = nullptr;
   double *dMetrics = nullptr, *dsJ = nullptr, *dFaceGeo = nullptr, *dXGP = nullptr;
   double *dFlux = nullptr, *dLFlux = nullptr, *dGTrace = nullptr;
   int *dS2E = nullptr, *dE2S = nullptr;
@@ -161,7 +161,7 @@ KParams base_params(fluxo_handle* h) {
   KParams P{};
   const fluxo_cfg& c = h->cfg;
   P.nElems = h->nElems; P.nSides = h->nSides;
-  P.U = h->dU; P.Ut = h->dUt; P.UtTmp = h->dUtTmp; P.grad = h->dGrad;
+  P.U = h->dU; P.Ut = h->dUt; P.UtTmp = h->dUtTmp; P.grad = nullptr; P.utvisc = h->dUtVisc;
   P.metrics = h->dMetrics; P.sJ = h->dsJ; P.facegeo = h->dFaceGeo; P.xGP = h->dXGP;
   P.s2e = h->dS2E; P.e2s = h->dE2S;
   P.flux = h->dFlux; P.lflux = h->dLFlux; P.gtrace = h->dGTrace;
@@ -405,8 +405,10 @@ int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* S2E, 
       (r = dalloc(h, &h->dS2E, s2e.size())) || (r = dalloc(h, &h->dE2S, e2s.size())))
     return r;
   if (h->visc) {
-    if ((r = dalloc(h, &h->dGrad, 3 * nU)) || (r = dalloc(h, &h->dLFlux, nF))) return r;
-    if (h->cfg.lifting == 2 && (r = dalloc(h, &h->dGTrace, (size_t)2 * 15 * NPT * nSides))) return r;
+    if ((r = dalloc(h, &h->dGrad, 3 * nU)) || (r = dalloc(h, &h->dLFlux, nF)) ||
+        (r = dalloc(h, &h->dUtVisc, (size_t)4 * NP3 * nElems)) ||
+        (r = dalloc(h, &h->dGTrace, (size_t)2 * 15 * NPT * nSides)))
+      return r;
   }
   cudaStream_t s = h->stream;
   FLUXO_CUDA(h, cudaMemcpyAsync(h->dMetrics, met.data(), met.size() * 8, cudaMemcpyHostToDevice, s));
@@ -479,6 +481,7 @@ int fluxo_gpu_dg_time_derivative(fluxo_handle* h, double t) {
   KParams P = base_params(h);
   P.stage = 0;
   P.t = t;
+  P.grad = h->dGrad;  // keep the volume gradients of this RHS for fluxo_gpu_get_gradients
   if ((r = rhs(h, P))) return r;
   FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
   FLUXO_CUDA(h, cudaGetLastError());
@@ -630,7 +633,7 @@ int fluxo_gpu_destroy(fluxo_handle* h) {
   }
   cudaSetDevice(h->cfg.device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  void* ptrs[] = {h->dBasis, h->dU, h->dUt, h->dUtTmp, h->dGrad, h->dMetrics, h->dsJ, h->dFaceGeo, h->dXGP,
+  void* ptrs[] = {h->dBasis, h->dU, h->dUt, h->dUtTmp, h->dGrad, h->dUtVisc, h->dMetrics, h->dsJ, h->dFaceGeo, h->dXGP,
                   h->dFlux, h->dLFlux, h->dGTrace, h->dS2E, h->dE2S, h->dTD, h->dDtBits, h->dErrKey};
   for (void* p : ptrs)
     if (p) cudaFree(p);

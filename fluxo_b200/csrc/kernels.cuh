@@ -92,18 +92,14 @@ __global__ void face_flux_kernel(KParams P, int NP) {
   if constexpr (VISC) {  // riemann.f90:155-168: + 1/2 n.(F_v(L) + F_v(R))
     const double* U0 = P.U + 5 * ((size_t)eM * NP * NP * NP + nM);
     const double* U1 = P.U + 5 * ((size_t)eS * NP * NP * NP + nS);
-    const double* gM = P.grad + 15 * ((size_t)eM * NP * NP * NP + nM);
-    const double* gS = P.grad + 15 * ((size_t)eS * NP * NP * NP + nS);
     double uL[5], uR[5], gl[15], gr[15];
 #pragma unroll
     for (int v = 0; v < 5; ++v) { uL[v] = U0[v]; uR[v] = U1[v]; }
-    if (P.lifting == 2) {  // BR2 face traces: side buffers written by the gradient kernel
-      const double* tM = P.gtrace + ((size_t)side * 2 + 0) * 15 * npts + pt;
-      const double* tS = P.gtrace + ((size_t)side * 2 + 1) * 15 * npts + pt;
-      for (int c = 0; c < 15; ++c) { gl[c] = tM[(size_t)c * npts]; gr[c] = tS[(size_t)c * npts]; }
-    } else {
-      for (int c = 0; c < 15; ++c) { gl[c] = gM[c]; gr[c] = gS[c]; }
-    }
+    // gradient traces gradP_master / gradP_slave, side-major buffers written by the lifting kernel
+    const double* tM = P.gtrace + ((size_t)side * 2 + 0) * 15 * npts + pt;
+    const double* tS = P.gtrace + ((size_t)side * 2 + 1) * 15 * npts + pt;
+#pragma unroll
+    for (int c = 0; c < 15; ++c) { gl[c] = tM[(size_t)c * npts]; gr[c] = tS[(size_t)c * npts]; }
     double kL[4], gL[4], jL[4], kR[4], gR[4], jR[4];
     diff_flux_3d(P, uL, gl, gl + 5, gl + 10, kL, gL, jL);
     diff_flux_3d(P, uR, gr, gr + 5, gr + 10, kR, gR, jR);
@@ -139,117 +135,6 @@ static __global__ void lift_flux_kernel(KParams P, int NP, double* lf) {
   double se = P.facegeo[(size_t)side * 10 * npts + 9 * npts + pt];
   double* o = lf + (size_t)side * 5 * npts + pt;
   for (int v = 0; v < 5; ++v) o[v * npts] = 0.5 * (VS[v] - VM[v]) * se;
-}
-
-// ------------------------------------------------------------------------------------------------
-// Gradient kernel: BR1/BR2 lifting volume integral (br1_volint.f90:45-98 / br2_volint.f90),
-// surface integral (br1_surfint.f90:52-131 / br2_surfint.f90:53-148), Jacobian and
-// ConvertToGradPrimVec (equation_vars.f90:571-647).  One thread per volume node.
-// BR2 additionally writes the face traces gradP_master/slave = vol + etaBR2 * own-side surface term
-// into side buffers [side][master|slave][15][pt].
-// ------------------------------------------------------------------------------------------------
-template <int NP>
-__global__ void __launch_bounds__(512) gradient_kernel(KParams P, const double* lf, double* traces) {
-  if (halted(P)) return;
-  constexpr int NP3 = NP * NP * NP, N = NP - 1, NPT = NP * NP;
-  constexpr int EPB = (256 / NP3) > 0 ? (256 / NP3) : 1;
-  extern __shared__ double smem[];
-  double* sD = smem;                 // NP*NP
-  double* sV = sD + NP * NP;         // EPB * 5 * NP3
-  const int eb = threadIdx.x / NP3, n = threadIdx.x - eb * NP3;
-  const int e = blockIdx.x * EPB + eb;
-  const bool valid = e < P.nElems;
-  for (int z = threadIdx.x; z < NP * NP; z += blockDim.x) sD[z] = P.basis->D[(z / NP) * NP + (z % NP)];
-  const int i = n % NP, j = (n / NP) % NP, k = n / NPT;
-  double u[5];
-  double* myV = sV + (size_t)eb * 5 * NP3;
-  if (valid) {
-    const double* Ug = P.U + 5 * ((size_t)e * NP3 + n);
-    for (int v = 0; v < 5; ++v) u[v] = Ug[v];
-    double V[5];
-    lifting_var(P, u, V);
-    for (int v = 0; v < 5; ++v) myV[v * NP3 + n] = V[v];
-  }
-  __syncthreads();
-  if (!valid) return;
-  double gxi[5], geta[5], gzeta[5];
-#pragma unroll
-  for (int v = 0; v < 5; ++v) { gxi[v] = 0.; geta[v] = 0.; gzeta[v] = 0.; }
-#pragma unroll
-  for (int l = 0; l < NP; ++l) {
-    const double di = sD[i * NP + l], dj = sD[j * NP + l], dk = sD[k * NP + l];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      gxi[v] += di * myV[v * NP3 + l + NP * (j + NP * k)];
-      geta[v] += dj * myV[v * NP3 + i + NP * (l + NP * k)];
-      gzeta[v] += dk * myV[v * NP3 + i + NP * (j + NP * l)];
-    }
-  }
-  const double* M = P.metrics + (size_t)e * 9 * NP3 + n;
-  double m[9];
-#pragma unroll
-  for (int c = 0; c < 9; ++c) m[c] = M[c * NP3];
-  const double sj = P.sJ[(size_t)e * NP3 + n];
-  double g[3][5];
-#pragma unroll
-  for (int v = 0; v < 5; ++v)
-#pragma unroll
-    for (int d = 0; d < 3; ++d) g[d][v] = m[0 + d] * gxi[v] + m[3 + d] * geta[v] + m[6 + d] * gzeta[v];
-  if (P.lifting == 2) {
-#pragma unroll
-    for (int v = 0; v < 5; ++v)
-#pragma unroll
-      for (int d = 0; d < 3; ++d) g[d][v] *= sj;
-  }
-  int sides[3];
-  const int ns = boundary_sides(i, j, k, N, sides);
-  const double lh = P.basis->LhatM0;
-  double vol[3][5];
-  if (P.lifting == 2 && ns > 0) {
-    for (int d = 0; d < 3; ++d)
-      for (int v = 0; v < 5; ++v) vol[d][v] = g[d][v];
-  }
-  for (int z = 0; z < ns; ++z) {
-    const int s = sides[z];
-    const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
-    const int side = es[0], flip = es[1];
-    const int pt = P.basis->v2s[s - 1][flip][side_plane_coords(s, i, j, k, NP)];
-    const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
-    const double* F = lf + (size_t)side * 5 * NPT + pt;
-    if (P.lifting == 2) {
-      double surf[3][5], tr[3][5];
-      for (int v = 0; v < 5; ++v) {
-        const double fl = sj * lh * F[v * NPT];
-        for (int d = 0; d < 3; ++d) {
-          surf[d][v] = fl * nvec[d * NPT];
-          g[d][v] += surf[d][v];
-          tr[d][v] = vol[d][v] + P.etaBR2 * surf[d][v];
-        }
-      }
-      for (int d = 0; d < 3; ++d) to_grad_prim(P, u, tr[d]);
-      double* T = traces + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 15 * NPT + pt;
-      for (int d = 0; d < 3; ++d)
-        for (int v = 0; v < 5; ++v) T[(size_t)(5 * d + v) * NPT] = tr[d][v];
-    } else {
-      for (int v = 0; v < 5; ++v) {
-        const double fl = F[v * NPT] * lh;
-        for (int d = 0; d < 3; ++d) g[d][v] += fl * nvec[d * NPT];
-      }
-    }
-  }
-  if (P.lifting != 2) {
-#pragma unroll
-    for (int v = 0; v < 5; ++v)
-#pragma unroll
-      for (int d = 0; d < 3; ++d) g[d][v] *= sj;
-  }
-  double* G = P.grad + 15 * ((size_t)e * NP3 + n);
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    to_grad_prim(P, u, g[d]);
-#pragma unroll
-    for (int v = 0; v < 5; ++v) G[5 * d + v] = g[d][v];
-  }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -314,6 +199,13 @@ volume_kernel(KParams P) {
     const double* Ug = P.U + 5 * ((size_t)e * NP3 + t);
 #pragma unroll
     for (int v = 0; v < 5; ++v) u[v] = Ug[v];
+    // the epilogue's operands are needed only after the pair loops: start their way to L2 now
+    prefetch_l2(P.sJ + (size_t)e * NP3 + t);
+    if (P.stage > 1) prefetch_l2(P.UtTmp + 5 * ((size_t)e * NP3 + t));
+    if constexpr (VISC) {
+#pragma unroll
+      for (int v = 0; v < 4; ++v) prefetch_l2(P.utvisc + (size_t)e * 4 * NP3 + v * NP3 + t);
+    }
     double* r = rec + vol_slot(t) * RS;
     make_record<VF>(P, u, r);
     const double* Mg = P.metrics + (size_t)e * 9 * NP3 + t;
@@ -403,42 +295,12 @@ volume_kernel(KParams P) {
 #pragma unroll
   for (int v = 0; v < 5; ++v) ut[v] = valid ? acc[vol_slot(t) * 5 + v] : 0.;
   const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
-  if constexpr (VISC) {
-    // contravariant viscous fluxes f~,g~,h~ (components 1..4) of every node, into the record area
-    double m[9];
-    if (valid) {
-#pragma unroll
-      for (int c = 0; c < 9; ++c) m[c] = rec[vol_slot(t) * RS + NQ + c];
-    }
-    __syncthreads();
-    double* sT = rec;  // [12][NP3]
-    if (valid) {
-      const double* G = P.grad + 15 * ((size_t)e * NP3 + t);
-      double gg[15];
-#pragma unroll
-      for (int c = 0; c < 15; ++c) gg[c] = G[c];
-      double f[4], g[4], h[4];
-      diff_flux_3d(P, u, gg, gg + 5, gg + 10, f, g, h);
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        sT[(0 + v) * NP3 + t] = f[v] * m[0] + g[v] * m[1] + h[v] * m[2];
-        sT[(4 + v) * NP3 + t] = f[v] * m[3] + g[v] * m[4] + h[v] * m[5];
-        sT[(8 + v) * NP3 + t] = f[v] * m[6] + g[v] * m[7] + h[v] * m[8];
-      }
-    }
-    __syncthreads();
-    if (valid) {
-#pragma unroll
-      for (int l = 0; l < NP; ++l) {
-        const double di = sDhat[i * NP + l], dj = sDhat[j * NP + l], dk = sDhat[k * NP + l];
-        const int ni = l + NP * (j + NP * k), nj = i + NP * (l + NP * k), nk = i + NP * (j + NP * l);
-#pragma unroll
-        for (int v = 0; v < 4; ++v)
-          ut[1 + v] += di * sT[(0 + v) * NP3 + ni] + dj * sT[(4 + v) * NP3 + nj] + dk * sT[(8 + v) * NP3 + nk];
-      }
-    }
-  }
   if (!valid) return;
+  if constexpr (VISC) {  // viscous volume integral (volint.f90:228-271), computed by the lifting kernel
+    const double* V = P.utvisc + (size_t)e * 4 * NP3 + t;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) ut[1 + v] += V[v * NP3];
+  }
   // surface integral at the boundary nodes (LGL)
   int sides[3];
   const int ns = boundary_sides(i, j, k, N, sides);

@@ -24,6 +24,7 @@ cudaError_t launch_volume_vf32(int NP, bool visc, int nElems, cudaStream_t s, co
 cudaError_t launch_face_flux(int RS, bool visc, int NP, int nSides, cudaStream_t s, const KParams& P);
 cudaError_t launch_lift_flux(int NP, int nSides, cudaStream_t s, const KParams& P);
 cudaError_t launch_gradient(int NP, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_lift_visc(int NP, int lift, int lv, int nElems, cudaStream_t s, const KParams& P);
 cudaError_t launch_timestep(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P,
                             unsigned long long* dtBits, int* errKey);
 bool riemann_supported(int RS);

@@ -57,33 +57,8 @@ cudaError_t launch_lift_flux(int NP, int nSides, cudaStream_t s, const KParams& 
   return cudaGetLastError();
 }
 
-template <int NP>
-static cudaError_t grad_t(int nElems, cudaStream_t s, const KParams& P) {
-  constexpr int NP3 = NP * NP * NP;
-  constexpr int EPB = (256 / NP3) > 0 ? (256 / NP3) : 1;
-  const size_t smem = sizeof(double) * (NP * NP + EPB * 5 * NP3);
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(gradient_kernel<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
-  gradient_kernel<NP><<<(nElems + EPB - 1) / EPB, EPB * NP3, smem, s>>>(P, P.lflux, P.gtrace);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_gradient(int NP, int nElems, cudaStream_t s, const KParams& P) {
-  switch (NP) {
-    case 2: return grad_t<2>(nElems, s, P);
-    case 3: return grad_t<3>(nElems, s, P);
-    case 4: return grad_t<4>(nElems, s, P);
-    case 5: return grad_t<5>(nElems, s, P);
-    case 6: return grad_t<6>(nElems, s, P);
-    case 7: return grad_t<7>(nElems, s, P);
-    case 8: return grad_t<8>(nElems, s, P);
-    case 9: return grad_t<9>(nElems, s, P);
-    default: return cudaErrorInvalidValue;
-  }
+  return launch_lift_visc(NP, P.lifting, P.lifting_var, nElems, s, P);
 }
 
 template <int NP, bool VISC>

@@ -1,0 +1,245 @@
+// Lifting + viscous volume kernel of the Navier-Stokes right-hand side (LGL nodes).
+//
+// Per element (one thread per volume node) it computes
+//   1. the BR1/BR2 gradients of the lifting variable: strong-form volume derivative
+//      (br1_volint.f90:45-98, br2_volint.f90:45-103), surface integral of the lifting flux
+//      (br1_surfint.f90:52-131, br2_surfint.f90:53-148), Jacobian, conversion to gradients of the
+//      primitive variables (equation_vars.f90:571-647);
+//   2. the face traces gradP_master/slave the face kernel needs (BR1: the volume gradient at the
+//      boundary node, ProlongToFace; BR2: volume part + etaBR2 * own-side surface part), written
+//      side-major so the face kernel reads them coalesced;
+//   3. the viscous volume integral sum_l D_hat(i,l) (f~,g~,h~)(l) of the contravariant viscous
+//      fluxes (volint.f90:228-271 with EvalDiffFluxTilde3D flux.f90:523-635), written as 4 values per
+//      node for the volume kernel.
+// The derivative sums are line-blocked: one thread loads a whole line of one variable into registers
+// and produces all N+1 outputs, so a shared-memory load serves N+1 multiply-adds.
+#pragma once
+#include "common.cuh"
+#include "physics_ns.cuh"
+
+namespace fluxo {
+
+template <int NP>
+__host__ __device__ constexpr int lv_epb() { return (256 / (NP * NP * NP)) > 0 ? (256 / (NP * NP * NP)) : 1; }
+template <int NP>
+__host__ __device__ constexpr int lv_slots() { return (NP * NP * NP - 1) + ((NP * NP * NP - 1) >> 4) + 1; }
+template <int NP>
+__host__ __device__ constexpr size_t lv_smem_bytes() {
+  return sizeof(double) * (size_t)(2 * NP * NP + lv_epb<NP>() * 20 * lv_slots<NP>());
+}
+
+__device__ __forceinline__ int lv_slot(int n) { return n + (n >> 4); }
+
+// node index of position x on line (a,b) of direction dir
+template <int NP>
+__device__ __forceinline__ int line_node(int dir, int a, int b, int x) {
+  return dir == 0 ? x + NP * (a + NP * b) : (dir == 1 ? a + NP * (x + NP * b) : a + NP * (b + NP * x));
+}
+
+template <int LV>
+__device__ __forceinline__ void lifting_var_t(const KParams& P, const double* U, double* V) {
+  if constexpr (LV == 1) {
+    for (int v = 0; v < 5; ++v) V[v] = U[v];
+  } else if constexpr (LV == 2) {
+    const double s = 1. / U[0];
+    V[0] = U[0]; V[1] = U[1] * s; V[2] = U[2] * s; V[3] = U[3] * s;
+    V[4] = P.kappaM1 * (U[4] - 0.5 * (U[1] * V[1] + U[2] * V[2] + U[3] * V[3]));
+  } else {  // ConsToEntropyVec (equation_vars.f90:397-429)
+    const double srho = 1. / U[0];
+    const double u = U[1] * srho, v = U[2] * srho, w = U[3] * srho;
+    const double v2s2 = 0.5 * (u * u + v * v + w * w);
+    const double rho_sp = U[0] / (P.kappaM1 * (U[4] - U[0] * v2s2));
+    const double s = -(log(rho_sp) + P.kappaM1 * log(U[0]));  // -log(rho_sp * rho^(kappa-1))
+    V[0] = (P.kappa - s) * P.sKappaM1 - rho_sp * v2s2;
+    V[1] = rho_sp * u; V[2] = rho_sp * v; V[3] = rho_sp * w;
+    V[4] = -rho_sp;
+  }
+}
+
+template <int NP, int LIFT, int LV>
+#ifndef FLUXO_LV_MINB
+#define FLUXO_LV_MINB 2  // resident blocks per SM the register allocation must allow
+#endif
+__global__ void __launch_bounds__(lv_epb<NP>() * NP * NP * NP, FLUXO_LV_MINB)
+lift_visc_kernel(KParams P) {
+  if (halted(P)) return;
+  constexpr int NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1, EPB = lv_epb<NP>(), NS = lv_slots<NP>();
+  extern __shared__ double smem[];
+  double* sD = smem;           // D(i,l) at [i*NP+l]
+  double* sDhat = sD + NPT;    // D_hat(i,l)
+  const int eb = threadIdx.x / NP3, t = threadIdx.x - eb * NP3;
+  const int e = blockIdx.x * EPB + eb;
+  const bool valid = e < P.nElems;
+  double* sV = sDhat + NPT + (size_t)eb * 20 * NS;  // [5][NS] lifting variable; later [4][NS] divergence
+  double* sW = sV + 5 * NS;                          // [15][NS] xi/eta/zeta derivatives; later [12][NS] fluxes
+  for (int z = threadIdx.x; z < NPT; z += blockDim.x) {
+    sD[z] = P.basis->D[z];
+    sDhat[z] = P.basis->Dhat[z];
+  }
+  double u[5];
+  if (valid) {
+    const double* Ug = P.U + 5 * ((size_t)e * NP3 + t);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) u[v] = Ug[v];
+    // metrics and Jacobian are read after the derivative phase: start them towards L2 now
+#pragma unroll
+    for (int c = 0; c < 9; ++c) prefetch_l2(P.metrics + (size_t)e * 9 * NP3 + c * NP3 + t);
+    prefetch_l2(P.sJ + (size_t)e * NP3 + t);
+    double V[5];
+    lifting_var_t<LV>(P, u, V);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) sV[v * NS + lv_slot(t)] = V[v];
+  }
+  __syncthreads();
+  // derivatives of the lifting variable along xi, eta, zeta: tasks (dir, var, line)
+  if (valid) {
+    for (int task = t; task < 15 * NPT; task += NP3) {
+      const int dir = task / (5 * NPT), rem = task - dir * 5 * NPT, v = rem / NPT, L = rem - v * NPT;
+      const int a = L % NP, b = L / NP;
+      double x[NP];
+#pragma unroll
+      for (int l = 0; l < NP; ++l) x[l] = sV[v * NS + lv_slot(line_node<NP>(dir, a, b, l))];
+#pragma unroll
+      for (int o = 0; o < NP; ++o) {
+        double s = 0.;
+#pragma unroll
+        for (int l = 0; l < NP; ++l) s += sD[o * NP + l] * x[l];
+        sW[(dir * 5 + v) * NS + lv_slot(line_node<NP>(dir, a, b, o))] = s;
+      }
+    }
+  }
+  __syncthreads();
+  double ft[12];
+  if (valid) {
+    const double* M = P.metrics + (size_t)e * 9 * NP3 + t;
+    double m[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) m[c] = M[c * NP3];
+    const double sj = P.sJ[(size_t)e * NP3 + t];
+    double g[3][5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const double gx = sW[(0 + v) * NS + lv_slot(t)], ge = sW[(5 + v) * NS + lv_slot(t)],
+                   gz = sW[(10 + v) * NS + lv_slot(t)];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) g[d][v] = m[0 + d] * gx + m[3 + d] * ge + m[6 + d] * gz;
+    }
+    double gv[3][5];  // BR2: volume part of the gradient, the base of every face trace
+    if constexpr (LIFT == 2) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          g[d][v] *= sj;
+          gv[d][v] = g[d][v];
+        }
+    }
+    const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
+    int sides[3];
+    const int ns = boundary_sides(i, j, k, N, sides);
+    const double lh = P.basis->LhatM0;
+    int tside[3], tms[3], tpt[3];
+    for (int z = 0; z < ns; ++z) {
+      const int s = sides[z];
+      const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
+      const int side = es[0], flip = es[1];
+      const int pt = P.basis->v2s[s - 1][flip][side_plane_coords(s, i, j, k, NP)];
+      tside[z] = side; tms[z] = flip == 0 ? 0 : 1; tpt[z] = pt;
+      const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
+      const double* F = P.lflux + (size_t)side * 5 * NPT + pt;
+      const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
+      if constexpr (LIFT == 2) {
+        double tr[3][5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const double fl = sj * lh * F[v * NPT];
+          const double sx = fl * n0, sy = fl * n1, sz = fl * n2;
+          tr[0][v] = gv[0][v] + P.etaBR2 * sx;
+          tr[1][v] = gv[1][v] + P.etaBR2 * sy;
+          tr[2][v] = gv[2][v] + P.etaBR2 * sz;
+          g[0][v] += sx; g[1][v] += sy; g[2][v] += sz;  // volume gradient gets the plain surface term
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) to_grad_prim(P, u, tr[d]);
+        double* T = P.gtrace + ((size_t)side * 2 + tms[z]) * 15 * NPT + pt;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+          for (int v = 0; v < 5; ++v) T[(size_t)(5 * d + v) * NPT] = tr[d][v];
+      } else {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const double fl = F[v * NPT] * lh;
+          g[0][v] += fl * n0; g[1][v] += fl * n1; g[2][v] += fl * n2;
+        }
+      }
+    }
+    if constexpr (LIFT == 1) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) g[d][v] *= sj;
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) to_grad_prim(P, u, g[d]);
+    if constexpr (LIFT == 1) {  // BR1 traces: the volume gradient at the boundary node
+      for (int z = 0; z < ns; ++z) {
+        double* T = P.gtrace + ((size_t)tside[z] * 2 + tms[z]) * 15 * NPT + tpt[z];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+          for (int v = 0; v < 5; ++v) T[(size_t)(5 * d + v) * NPT] = g[d][v];
+      }
+    }
+    if (P.grad) {  // volume gradients kept for analysis (DGTimeDerivative calls only)
+      double* G = P.grad + 15 * ((size_t)e * NP3 + t);
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int v = 0; v < 5; ++v) G[5 * d + v] = g[d][v];
+    }
+    double f[4], gg[4], h[4];
+    diff_flux_3d(P, u, g[0], g[1], g[2], f, gg, h);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      ft[0 + v] = f[v] * m[0] + gg[v] * m[1] + h[v] * m[2];
+      ft[4 + v] = f[v] * m[3] + gg[v] * m[4] + h[v] * m[5];
+      ft[8 + v] = f[v] * m[6] + gg[v] * m[7] + h[v] * m[8];
+    }
+  }
+  __syncthreads();  // every thread is done with the derivatives in sW
+  if (valid) {
+#pragma unroll
+    for (int c = 0; c < 12; ++c) sW[c * NS + lv_slot(t)] = ft[c];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) sV[v * NS + lv_slot(t)] = 0.;
+  }
+  __syncthreads();
+  // viscous volume integral: sum_l D_hat(o,l) f~(l) along each direction, tasks (var, line)
+#pragma unroll 1
+  for (int dir = 0; dir < 3; ++dir) {
+    if (valid) {
+      for (int task = t; task < 4 * NPT; task += NP3) {
+        const int v = task / NPT, L = task - v * NPT, a = L % NP, b = L / NP;
+        double x[NP];
+#pragma unroll
+        for (int l = 0; l < NP; ++l) x[l] = sW[(dir * 4 + v) * NS + lv_slot(line_node<NP>(dir, a, b, l))];
+#pragma unroll
+        for (int o = 0; o < NP; ++o) {
+          double s = 0.;
+#pragma unroll
+          for (int l = 0; l < NP; ++l) s += sDhat[o * NP + l] * x[l];
+          sV[v * NS + lv_slot(line_node<NP>(dir, a, b, o))] += s;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (valid) {
+    double* O = P.utvisc + (size_t)e * 4 * NP3 + t;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) O[v * NP3] = sV[v * NS + lv_slot(t)];
+  }
+}
+
+}  // namespace fluxo
