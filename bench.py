@@ -43,6 +43,11 @@ FALG_RK_STAGE_PER_DOF = 20.0  # Ut_tmp = Ut - A*Ut_tmp; U += b*dt*Ut_tmp (2+2 fl
 VOLUME_KERNEL_FALG = (FALG_PER_DOF["volume_split_form"] + FALG_PER_DOF["volume_viscous"] +
                       FALG_PER_DOF["surface_integral"] + FALG_PER_DOF["jacobian_source"] + FALG_RK_STAGE_PER_DOF)
 
+# DRAM bytes (read + write) of one volume-kernel launch per DOF, from an ncu capture of the same
+# kernel on the 16^3 case (dram__bytes_read.sum + dram__bytes_write.sum = 579 MB for 2.1 M DOFs);
+# the traffic grows in proportion to the elements, so it is scaled to the launch's DOF count.
+VOLUME_KERNEL_DRAM_BYTES_PER_DOF = 276.0
+
 METRIC = "PID ns/DOF/RHS, NS Taylor-Green N=7 32^3 curved, BR1 + EC-KEP + ES (Riemann 44), LSERK4-5"
 
 
@@ -294,7 +299,9 @@ def run_fluxo(args):
     vol_avg_ms = vol_ms / max(vol_n, 1)
     achieved = VOLUME_KERNEL_FALG * nd / (vol_avg_ms * 1e-3) / 1e12
     roofline = {"bound": "fp64", "kernel": "volume_kernel<8,5,true>", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": VOLUME_KERNEL_DRAM_BYTES_PER_DOF * nd,
+                "traffic_note": "bytes per launch, ncu on 16^3 scaled by DOFs",
                 "flops_per_dof_launch": VOLUME_KERNEL_FALG, "launch_ms": vol_avg_ms,
                 "peak_source": "measured in this job: DFMA loop (fluxo_gpu_fp64_peak); MEASURED_PEAKS.json has no FP64"}
     line = {"metric": METRIC, "value": value, "unit": "ns/DOF/RHS", "n_gpus": world, "steps": args.steps,
