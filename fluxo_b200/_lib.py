@@ -60,8 +60,11 @@ EXPORTS = [
     "fluxo_gpu_get_gradients", "fluxo_gpu_dg_time_derivative", "fluxo_gpu_calc_timestep", "fluxo_gpu_timestep",
     "fluxo_gpu_time_disc", "fluxo_gpu_device_buffers", "fluxo_gpu_launch_count", "fluxo_gpu_destroy",
     "fluxo_gpu_last_error", "fluxo_gpu_set_profiling", "fluxo_gpu_get_profile", "fluxo_gpu_fp64_peak",
-    "fluxo_host_box_sizes", "fluxo_host_box_mesh", "fluxo_host_exact_func",
+    "fluxo_host_box_sizes", "fluxo_host_box_mesh", "fluxo_host_exact_func", "fluxo_gpu_dg_time_derivative_noalloc",
 ]
+
+# FLUXO_NOALLOC_SCRATCH_BYTES of fluxo_gpu.h: the static scratch of fluxo_gpu_dg_time_derivative_noalloc
+NOALLOC_SCRATCH_BYTES = 8 * 1024 * 1024
 
 _lib = None
 
@@ -95,6 +98,7 @@ def load():
     lib.fluxo_host_box_sizes.argtypes = [vp, P(i), P(i)]
     lib.fluxo_host_box_mesh.argtypes = [i, vp, vp, vp, i, d] + [vp] * 11
     lib.fluxo_host_exact_func.argtypes = [i, d, ctypes.c_size_t, vp, d, vp, d, vp, d, vp, vp]
+    lib.fluxo_gpu_dg_time_derivative_noalloc.argtypes = [P(FluxoCfg), i, i] + [vp] * 8
     for name in EXPORTS:
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib

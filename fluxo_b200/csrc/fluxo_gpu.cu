@@ -273,6 +273,11 @@ int check_ready(fluxo_handle* h) {
 
 }  // namespace
 
+namespace fluxo {
+void basis_tables_for(int N, BasisTables& B) { build_basis_tables(N, B); }
+int record_unbound_error(int code, const std::string& msg) { return fail(nullptr, code, msg); }
+}  // namespace fluxo
+
 extern "C" {
 
 int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {

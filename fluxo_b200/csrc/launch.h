@@ -2,6 +2,7 @@
 // family so that the instantiations compile in parallel).
 #pragma once
 #include <cstddef>
+#include <string>
 #include <cuda_runtime.h>
 #include "common.cuh"
 
@@ -29,5 +30,10 @@ cudaError_t launch_timestep(int NP, bool visc, int nElems, cudaStream_t s, const
                             unsigned long long* dtBits, int* errKey);
 bool riemann_supported(int RS);
 bool volume_flux_supported(int VF);
+
+// Host helpers of fluxo_gpu.cu for entry points without a handle: the per-N operator tables, and
+// the message that fluxo_gpu_last_error(NULL, ...) returns (returns `code`).
+void basis_tables_for(int N, BasisTables& B);
+int record_unbound_error(int code, const std::string& msg);
 
 }  // namespace fluxo

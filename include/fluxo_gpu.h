@@ -132,6 +132,29 @@ int fluxo_gpu_get_profile(fluxo_handle* h, int kind, double* total_ms, uint64_t*
  * counting an FMA as 2 flops: the denominator of the FP64 roofline. */
 int fluxo_gpu_fp64_peak(int device, double* tflops);
 
+/* Euler DGTimeDerivative (stage 0: Ut written) on caller-owned device arrays, allocating nothing.
+ * No counterpart in the reference: it is for callers that own all device memory and must not
+ * allocate while they run (e.g. a host code that reserves one arena of HBM at start-up and
+ * evaluates the right-hand side on its own vectors), which therefore cannot create a handle;
+ * cudaMalloc would fail once the arena holds the memory, and cudaFree synchronises the device.
+ * Same kernels and results as fluxo_gpu_dg_time_derivative for eqn = FLUXO_EQN_EULER (no source
+ * term).  Arrays are device memory of cfg->device in the device layouts of fluxo_gpu_set_mesh:
+ *   dU, dUt  (nVar,0:N,0:N,0:N,nElems) as U;  dsJ (0:N,0:N,0:N,nElems)
+ *   dMetrics [elem][9][node]: Metrics_f/g/hTilde (x,y,z) each, node = i+(N+1)(j+(N+1)k) fastest
+ *   dFaceGeo [side][10][pt]: NormVec, TangVec1, TangVec2 (x,y,z), SurfElem; pt = p+(N+1)q fastest
+ *   dS2E [side][5]: SideToElem with 0-based element ids;  dE2S [elem][6][2]: 0-based side id, flip.
+ * The face fluxes and operator tables live in one static device array of
+ * FLUXO_NOALLOC_SCRATCH_BYTES shared by all calls on a device: it needs
+ * 21504 + nSides*5*(N+1)^2*8 bytes (N=7: about 3270 sides; N=3: about 13070 sides), larger
+ * meshes return FLUXO_EINVAL_CFG.  Calls whose GPU work overlaps (other streams or host threads)
+ * race on that array; the call runs on `stream` (NULL: the legacy default stream) and
+ * synchronises it before returning.  Errors: fluxo_gpu_last_error(NULL, ...). */
+#define FLUXO_NOALLOC_SCRATCH_BYTES (8u * 1024u * 1024u)
+int fluxo_gpu_dg_time_derivative_noalloc(const fluxo_cfg* cfg, int nElems, int nSides, const double* dU,
+                                         double* dUt, const double* dMetrics, const double* dsJ,
+                                         const double* dFaceGeo, const int* dS2E, const int* dE2S,
+                                         void* stream);
+
 int fluxo_gpu_destroy(fluxo_handle* h);
 /* Copies the last error message of the handle (or of the last failed create if h is NULL). */
 int fluxo_gpu_last_error(fluxo_handle* h, char* buf, size_t len);
