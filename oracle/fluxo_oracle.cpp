@@ -327,10 +327,20 @@ void SideToVol(int N, int l, int p, int q, int flip, int s, int* ijk) {  // mapp
 // ----------------------------------------------------------------------------------------------
 // Case data
 // ----------------------------------------------------------------------------------------------
+const int NVMAX = 9;  // nVar: 5 (Navier-Stokes), 9 (MHD with GLM)
+
 struct Case {
   orc_params P;
   int N, np, nVar, nElems, nSides, nDOFElem;
   bool parabolic;
+  // MHD (equation/mhd/equation.f90:134-285): eqn 2 ideal, eqn 3 with resistivity/viscosity
+  bool mhd = false;
+  int nAux = 6;                 // auxiliary variables of the split form (NS 6, MHD 8)
+  int noncons = 0;              // NONCONS: 0 off, 1 Powell, 2 Brackbill, 3 Janhunen
+  bool ncGLM = false;           // PP_NC_GLM
+  double mu_0 = 1., smu_0 = 1., s2mu_0 = 0.5, kappaM2 = 0., eta = 0., etasmu_0 = 0., muMHD = 0.;
+  double GLM_scale = 0.5, GLM_scr = 0., GLM_ch = 0., GLM_dtch1 = 0.;
+  bool GLM_init = false;
   // basis (double), dg/dg.f90:181-252
   std::vector<double> xGP, wGP, wBary, D, D_T, Dhat, Dhat_T, Dvolsurf, Dvolsurf_T, Lminus, Lplus;
   double L_HatMinus0, L_HatPlus0;
@@ -871,6 +881,29 @@ void DiffFlux3D(const Case& C, const real* U, const real* gX, const real* gY, co
   h[4] = v1 * h[1] + v2 * h[2] + v3 * h[3] - lambda * cvTz;
 }
 
+#include "fluxo_oracle_mhd.h"
+
+// Equation-system dispatch (the reference selects the module at compile time).
+inline void Uaux(const Case& C, const real* U, real* a) {
+  if (C.mhd) MHD_Uaux(C, U, a);
+  else EvalUaux(C, U, a);
+}
+inline void LiftVar(const Case& C, const real* U, real* V) {
+  if (!C.mhd) { LiftingVar(C, U, V); return; }
+  if (C.P.lifting_var == 1) { for (int v = 0; v < 9; ++v) V[v] = U[v]; }
+  else if (C.P.lifting_var == 2) MHD_ConsToPrim(C, U, V);
+  else MHD_ConsToEntropy(C, U, V);
+}
+inline void GradPrim(const Case& C, const real* U, real* g) {
+  if (C.mhd) MHD_ConvertToGradPrim(C, U, g);
+  else ConvertToGradPrim(C, U, g);
+}
+inline void DiffFlux(const Case& C, const real* U, const real* gX, const real* gY, const real* gZ, real* f, real* g,
+                     real* h) {
+  if (C.mhd) MHD_DiffFlux3D(C, U, gX, gY, gZ, f, g, h);
+  else DiffFlux3D(C, U, gX, gY, gZ, f, g, h);
+}
+
 // ----------------------------------------------------------------------------------------------
 // Exact functions, navierstokes/equation.f90:575-950
 // ----------------------------------------------------------------------------------------------
@@ -881,6 +914,7 @@ void PrimToCons(const Case& C, const double* prim, double* cons) {  // equation_
 }
 
 void ExactFunc(const Case& C, int func, double t, const double* x, double* resu) {
+  if (C.mhd) { MHD_ExactFunc(C, func, t, x, resu); return; }
   const orc_params& P = C.P;
   double prim[5];
   switch (func) {
@@ -925,6 +959,12 @@ void ExactFunc(const Case& C, int func, double t, const double* x, double* resu)
 
 // CalcSource, navierstokes/equation.f90:992-1071 (CASE 4 only; other cases disable the source)
 void CalcSource(Case& C, double t) {
+  if (C.mhd) {  // GLM damping, mhd/equation.f90:1698-1706 (the default case has no other source)
+    if (AlmostEqual(C.GLM_scr, 0.)) return;
+    size_t nd = (size_t)C.np * C.np * C.np * C.nElems;
+    for (size_t z = 0; z < nd; ++z) C.Ut[9 * z + 8] = C.Ut[9 * z + 8] - C.GLM_scr * C.GLM_ch * C.U[9 * z + 8];
+    return;
+  }
   if (!C.doCalcSource) return;
   const orc_params& P = C.P;
   double Omega = PI * P.ini_frequency;
@@ -1258,7 +1298,14 @@ void InitEquationAndTime(Case& C) {
   C.kappaP1 = C.kappa + 1.; C.sKappaP1 = 1. / C.kappaP1; C.R = P.R; C.s23 = 2. / 3.;
   C.Pr = P.Pr; C.KappasPr = C.kappa / C.Pr;
   C.mu0 = P.mu0; C.etaBR2 = P.etaBR2;
-  if (P.visc == 1) {  // equation.f90:226-233
+  if (C.mhd) {  // mhd/equation.f90:178-209 (mu is the constant MHD viscosity, PP_VISC unused)
+    C.kappaM2 = C.kappa - 2.;
+    C.mu_0 = P.mu_0; C.smu_0 = 1. / C.mu_0; C.s2mu_0 = 0.5 * C.smu_0;
+    C.eta = C.parabolic ? P.eta : 0.; C.etasmu_0 = C.eta * C.smu_0;
+    C.muMHD = C.parabolic ? P.mu0 : 0.;
+    C.GLM_scale = P.glm_scale; C.GLM_scr = P.glm_scr; C.GLM_ch = P.glm_ch;
+    C.noncons = P.noncons; C.ncGLM = (P.noncons != 0 && P.nc_glm != 0);
+  } else if (P.visc == 1) {  // equation.f90:226-233
     C.Ts = P.Ts; C.sTref = 1. / P.Tref; C.ExpoSuth = P.ExpoSuth;
     C.Ts = C.Ts * C.sTref;
     C.cSuth = std::pow(C.Ts, C.ExpoSuth) * (1 + C.Ts) / (2 * C.Ts * C.Ts);
@@ -1338,54 +1385,72 @@ void VolIntSplitForm(Case& C) {
   size_t nv = (size_t)n * n * n;
 #pragma omp parallel
   {
-  std::vector<real> aux(6 * nv), ft((size_t)5 * n * nv), gt((size_t)5 * n * nv), ht((size_t)5 * n * nv);
+  const int NV = C.nVar, NA = C.nAux;
+  std::vector<real> aux(NA * nv), ft((size_t)NV * n * nv), gt((size_t)NV * n * nv), ht((size_t)NV * n * nv);
+  std::vector<real> mf(3 * nv), mg(3 * nv), mh(3 * nv);  // the element's metrics (copies)
   auto F4 = [&](std::vector<real>& A, int v, int l, int i, int j, int k) -> real& {
-    return A[v + 5 * ((size_t)l + n * ((size_t)i + n * ((size_t)j + (size_t)n * k)))];
+    return A[v + NV * ((size_t)l + n * ((size_t)i + n * ((size_t)j + (size_t)n * k)))];
   };
 #pragma omp for schedule(static)
   for (int e = 0; e < C.nElems; ++e) {
-    for (size_t z = 0; z < nv; ++z) EvalUaux(C, &C.U[5 * (nv * e + z)], &aux[6 * z]);
+    for (size_t z = 0; z < nv; ++z) Uaux(C, &C.U[NV * (nv * e + z)], &aux[NA * z]);
+    for (size_t z = 0; z < 3 * nv; ++z) {
+      mf[z] = C.Mf[3 * nv * e + z]; mg[z] = C.Mg[3 * nv * e + z]; mh[z] = C.Mh[3 * nv * e + z];
+    }
     auto Up = [&](int i, int j, int k) { return &C.U[C.vol(0, i, j, k, e)]; };
-    auto Ap = [&](int i, int j, int k) { return &aux[6 * (i + n * (j + n * k))]; };
-    auto Mfp = [&](int i, int j, int k) { return &C.Mf[3 * C.nod(i, j, k, e)]; };
-    auto Mgp = [&](int i, int j, int k) { return &C.Mg[3 * C.nod(i, j, k, e)]; };
-    auto Mhp = [&](int i, int j, int k) { return &C.Mh[3 * C.nod(i, j, k, e)]; };
-    real mL[3], mR[3], F[5];
+    auto Ap = [&](int i, int j, int k) { return &aux[NA * (i + n * (j + n * k))]; };
+    auto Mfp = [&](int i, int j, int k) { return &mf[3 * (i + n * (j + n * k))]; };
+    auto Mgp = [&](int i, int j, int k) { return &mg[3 * (i + n * (j + n * k))]; };
+    auto Mhp = [&](int i, int j, int k) { return &mh[3 * (i + n * (j + n * k))]; };
+    auto Flux = [&](const real* UL, const real* UR, const real* aL, const real* aR, const real* mL, const real* mR,
+                    real* F) {
+      if (C.mhd) MHD_VolumeFluxVec(C, C.P.volume_flux, UL, UR, aL, aR, mL, mR, F);
+      else VolumeFluxVec(C, UL, UR, aL, aR, mL, mR, F);
+    };
+    real F[NVMAX];
     for (int k = 0; k < n; ++k)
       for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i) {
-          for (int v = 0; v < 5; ++v) F4(ft, v, i, i, j, k) = 0.;
+          for (int v = 0; v < NV; ++v) F4(ft, v, i, i, j, k) = 0.;
           for (int l = i + 1; l <= N; ++l) {
-            for (int d = 0; d < 3; ++d) { mL[d] = Mfp(i, j, k)[d]; mR[d] = Mfp(l, j, k)[d]; }
-            VolumeFluxVec(C, Up(i, j, k), Up(l, j, k), Ap(i, j, k), Ap(l, j, k), mL, mR, F);
-            for (int v = 0; v < 5; ++v) { F4(ft, v, l, i, j, k) = F[v]; F4(ft, v, i, l, j, k) = F[v]; }
+            Flux(Up(i, j, k), Up(l, j, k), Ap(i, j, k), Ap(l, j, k), Mfp(i, j, k), Mfp(l, j, k), F);
+            for (int v = 0; v < NV; ++v) { F4(ft, v, l, i, j, k) = F[v]; F4(ft, v, i, l, j, k) = F[v]; }
           }
         }
     for (int k = 0; k < n; ++k)
       for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i) {
-          for (int v = 0; v < 5; ++v) F4(gt, v, j, i, j, k) = 0.;
+          for (int v = 0; v < NV; ++v) F4(gt, v, j, i, j, k) = 0.;
           for (int l = j + 1; l <= N; ++l) {
-            for (int d = 0; d < 3; ++d) { mL[d] = Mgp(i, j, k)[d]; mR[d] = Mgp(i, l, k)[d]; }
-            VolumeFluxVec(C, Up(i, j, k), Up(i, l, k), Ap(i, j, k), Ap(i, l, k), mL, mR, F);
-            for (int v = 0; v < 5; ++v) { F4(gt, v, l, i, j, k) = F[v]; F4(gt, v, j, i, l, k) = F[v]; }
+            Flux(Up(i, j, k), Up(i, l, k), Ap(i, j, k), Ap(i, l, k), Mgp(i, j, k), Mgp(i, l, k), F);
+            for (int v = 0; v < NV; ++v) { F4(gt, v, l, i, j, k) = F[v]; F4(gt, v, j, i, l, k) = F[v]; }
           }
         }
     for (int k = 0; k < n; ++k)
       for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i) {
-          for (int v = 0; v < 5; ++v) F4(ht, v, k, i, j, k) = 0.;
+          for (int v = 0; v < NV; ++v) F4(ht, v, k, i, j, k) = 0.;
           for (int l = k + 1; l <= N; ++l) {
-            for (int d = 0; d < 3; ++d) { mL[d] = Mhp(i, j, k)[d]; mR[d] = Mhp(i, j, l)[d]; }
-            VolumeFluxVec(C, Up(i, j, k), Up(i, j, l), Ap(i, j, k), Ap(i, j, l), mL, mR, F);
-            for (int v = 0; v < 5; ++v) { F4(ht, v, l, i, j, k) = F[v]; F4(ht, v, k, i, j, l) = F[v]; }
+            Flux(Up(i, j, k), Up(i, j, l), Ap(i, j, k), Ap(i, j, l), Mhp(i, j, k), Mhp(i, j, l), F);
+            for (int v = 0; v < NV; ++v) { F4(ht, v, l, i, j, k) = F[v]; F4(ht, v, k, i, j, l) = F[v]; }
           }
         }
+    if (C.mhd && C.noncons) {  // AddNonConsFluxTilde3D, mhd/flux_average.f90:268-366
+      for (int k = 0; k < n; ++k)
+        for (int j = 0; j < n; ++j)
+          for (int i = 0; i < n; ++i) {
+            const real* Ui = Up(i, j, k);
+            const real* ai = Ap(i, j, k);
+            for (int l = 0; l < n; ++l) MHD_NonConsPair(C, Ui, ai, Up(l, j, k), Mfp(i, j, k), Mfp(l, j, k), &F4(ft, 0, l, i, j, k));
+            for (int l = 0; l < n; ++l) MHD_NonConsPair(C, Ui, ai, Up(i, l, k), Mgp(i, j, k), Mgp(i, l, k), &F4(gt, 0, l, i, j, k));
+            for (int l = 0; l < n; ++l) MHD_NonConsPair(C, Ui, ai, Up(i, j, l), Mhp(i, j, k), Mhp(i, j, l), &F4(ht, 0, l, i, j, k));
+          }
+    }
     for (int k = 0; k < n; ++k)
       for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i)
           for (int l = 0; l < n; ++l)
-            for (int v = 0; v < 5; ++v)
+            for (int v = 0; v < NV; ++v)
               C.Ut[C.vol(v, i, j, k, e)] = C.Ut[C.vol(v, i, j, k, e)] + C.Dvolsurf_T[l + n * i] * F4(ft, v, l, i, j, k) +
                                            C.Dvolsurf_T[l + n * j] * F4(gt, v, l, i, j, k) +
                                            C.Dvolsurf_T[l + n * k] * F4(ht, v, l, i, j, k);
@@ -1399,31 +1464,32 @@ void VolIntVisc(Case& C) {
   size_t nv = (size_t)n * n * n;
 #pragma omp parallel
   {
-  std::vector<real> ft(5 * nv), gt(5 * nv), ht(5 * nv);
+  const int NV = C.nVar;
+  std::vector<real> ft(NV * nv), gt(NV * nv), ht(NV * nv);
 #pragma omp for schedule(static)
   for (int e = 0; e < C.nElems; ++e) {
     for (size_t z = 0; z < nv; ++z) {
       size_t o = nv * e + z;
-      real f[5], g[5], h[5];
-      DiffFlux3D(C, &C.U[5 * o], &C.gx[5 * o], &C.gy[5 * o], &C.gz[5 * o], f, g, h);
+      real f[NVMAX], g[NVMAX], h[NVMAX];
+      DiffFlux(C, &C.U[NV * o], &C.gx[NV * o], &C.gy[NV * o], &C.gz[NV * o], f, g, h);
       const double* mf = &C.Mf[3 * o];
       const double* mg = &C.Mg[3 * o];
       const double* mh = &C.Mh[3 * o];
-      for (int v = 0; v < 5; ++v) {
-        ft[5 * z + v] = f[v] * mf[0] + g[v] * mf[1] + h[v] * mf[2];
-        gt[5 * z + v] = f[v] * mg[0] + g[v] * mg[1] + h[v] * mg[2];
-        ht[5 * z + v] = f[v] * mh[0] + g[v] * mh[1] + h[v] * mh[2];
+      for (int v = 0; v < NV; ++v) {
+        ft[NV * z + v] = f[v] * mf[0] + g[v] * mf[1] + h[v] * mf[2];
+        gt[NV * z + v] = f[v] * mg[0] + g[v] * mg[1] + h[v] * mg[2];
+        ht[NV * z + v] = f[v] * mh[0] + g[v] * mh[1] + h[v] * mh[2];
       }
     }
     for (int k = 0; k < n; ++k)
       for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i)
           for (int l = 0; l < n; ++l)
-            for (int v = 0; v < 5; ++v)
+            for (int v = 0; v < NV; ++v)
               C.Ut[C.vol(v, i, j, k, e)] = C.Ut[C.vol(v, i, j, k, e)] +
-                                           C.Dhat_T[l + n * i] * ft[5 * (l + n * (j + n * k)) + v] +
-                                           C.Dhat_T[l + n * j] * gt[5 * (i + n * (l + n * k)) + v] +
-                                           C.Dhat_T[l + n * k] * ht[5 * (i + n * (j + n * l)) + v];
+                                           C.Dhat_T[l + n * i] * ft[NV * (l + n * (j + n * k)) + v] +
+                                           C.Dhat_T[l + n * j] * gt[NV * (i + n * (l + n * k)) + v] +
+                                           C.Dhat_T[l + n * k] * ht[NV * (i + n * (j + n * l)) + v];
   }
   }
 }
@@ -1437,15 +1503,16 @@ void Lifting(Case& C) {
   std::fill(C.gy.begin(), C.gy.end(), 0.);
   std::fill(C.gz.begin(), C.gz.end(), 0.);
   bool br2 = (C.P.lifting == 2);
+  const int NV = C.nVar;
   // Lifting_FillFlux (br1_fillflux.f90:49-91) with EvalLiftingSurfFlux (flux.f90:677-716)
   for (int sid = 0; sid < C.nSides; ++sid)
     for (int q = 0; q < n; ++q)
       for (int p = 0; p < n; ++p) {
-        real Fm[5], Fs[5];
-        LiftingVar(C, &C.Umaster[C.fac(0, p, q, sid)], Fm);
-        LiftingVar(C, &C.Uslave[C.fac(0, p, q, sid)], Fs);
+        real Fm[NVMAX], Fs[NVMAX];
+        LiftVar(C, &C.Umaster[C.fac(0, p, q, sid)], Fm);
+        LiftVar(C, &C.Uslave[C.fac(0, p, q, sid)], Fs);
         size_t fi = (size_t)p + n * ((size_t)q + (size_t)n * sid);
-        for (int v = 0; v < 5; ++v) {
+        for (int v = 0; v < NV; ++v) {
           real Fl = 0.5 * (Fs[v] - Fm[v]) * C.SurfElem[fi];
           C.FX[C.fac(v, p, q, sid)] = Fl * C.NormVec[3 * fi + 0];
           C.FY[C.fac(v, p, q, sid)] = Fl * C.NormVec[3 * fi + 1];
@@ -1455,37 +1522,37 @@ void Lifting(Case& C) {
   // Lifting_VolInt: br1_volint.f90:45-98 (BR1) / br2_volint.f90:45-103 (BR2 includes sJ)
 #pragma omp parallel
   {
-  std::vector<real> Fl(5 * nv);
+  std::vector<real> Fl(NV * nv);
 #pragma omp for schedule(static)
   for (int e = 0; e < C.nElems; ++e) {
-    for (size_t z = 0; z < nv; ++z) LiftingVar(C, &C.U[5 * (nv * e + z)], &Fl[5 * z]);
+    for (size_t z = 0; z < nv; ++z) LiftVar(C, &C.U[NV * (nv * e + z)], &Fl[NV * z]);
     for (int k = 0; k < n; ++k)
       for (int j = 0; j < n; ++j)
         for (int i = 0; i < n; ++i) {
-          real gxi[5], geta[5], gzeta[5];
-          for (int v = 0; v < 5; ++v) {
-            gxi[v] = C.D_T[0 + n * i] * Fl[5 * (0 + n * (j + n * k)) + v];
-            geta[v] = C.D_T[0 + n * j] * Fl[5 * (i + n * (0 + n * k)) + v];
-            gzeta[v] = C.D_T[0 + n * k] * Fl[5 * (i + n * (j + n * 0)) + v];
+          real gxi[NVMAX], geta[NVMAX], gzeta[NVMAX];
+          for (int v = 0; v < NV; ++v) {
+            gxi[v] = C.D_T[0 + n * i] * Fl[NV * (0 + n * (j + n * k)) + v];
+            geta[v] = C.D_T[0 + n * j] * Fl[NV * (i + n * (0 + n * k)) + v];
+            gzeta[v] = C.D_T[0 + n * k] * Fl[NV * (i + n * (j + n * 0)) + v];
           }
           for (int l = 1; l < n; ++l)
-            for (int v = 0; v < 5; ++v) {
-              gxi[v] = gxi[v] + C.D_T[l + n * i] * Fl[5 * (l + n * (j + n * k)) + v];
-              geta[v] = geta[v] + C.D_T[l + n * j] * Fl[5 * (i + n * (l + n * k)) + v];
-              gzeta[v] = gzeta[v] + C.D_T[l + n * k] * Fl[5 * (i + n * (j + n * l)) + v];
+            for (int v = 0; v < NV; ++v) {
+              gxi[v] = gxi[v] + C.D_T[l + n * i] * Fl[NV * (l + n * (j + n * k)) + v];
+              geta[v] = geta[v] + C.D_T[l + n * j] * Fl[NV * (i + n * (l + n * k)) + v];
+              gzeta[v] = gzeta[v] + C.D_T[l + n * k] * Fl[NV * (i + n * (j + n * l)) + v];
             }
           size_t o = C.nod(i, j, k, e);
           const double* mf = &C.Mf[3 * o];
           const double* mg = &C.Mg[3 * o];
           const double* mh = &C.Mh[3 * o];
-          for (int v = 0; v < 5; ++v) {
+          for (int v = 0; v < NV; ++v) {
             real ax = mf[0] * gxi[v] + mg[0] * geta[v] + mh[0] * gzeta[v];
             real ay = mf[1] * gxi[v] + mg[1] * geta[v] + mh[1] * gzeta[v];
             real az = mf[2] * gxi[v] + mg[2] * geta[v] + mh[2] * gzeta[v];
             if (br2) { ax = ax * C.sJ[o]; ay = ay * C.sJ[o]; az = az * C.sJ[o]; }
-            C.gx[5 * o + v] = C.gx[5 * o + v] + ax;
-            C.gy[5 * o + v] = C.gy[5 * o + v] + ay;
-            C.gz[5 * o + v] = C.gz[5 * o + v] + az;
+            C.gx[NV * o + v] = C.gx[NV * o + v] + ax;
+            C.gy[NV * o + v] = C.gy[NV * o + v] + ay;
+            C.gz[NV * o + v] = C.gz[NV * o + v] + az;
           }
         }
   }
@@ -1505,7 +1572,7 @@ void Lifting(Case& C) {
           int ls = C.SideToElem[2 + 5 * sid];
           for (int q = 0; q < n; ++q)
             for (int p = 0; p < n; ++p)
-              for (int v = 0; v < 5; ++v) {
+              for (int v = 0; v < NV; ++v) {
                 size_t idx = C.vol(v, C.s2v(0, p, q, 0, ls, 0), C.s2v(0, p, q, 0, ls, 1), C.s2v(0, p, q, 0, ls, 2), e - 1);
                 g[idx] = g[idx] + F[C.fac(v, p, q, sid)] * C.L_HatMinus0;
               }
@@ -1515,16 +1582,16 @@ void Lifting(Case& C) {
           int nls = C.SideToElem[3 + 5 * sid], fl = C.SideToElem[4 + 5 * sid];
           for (int q = 0; q < n; ++q)
             for (int p = 0; p < n; ++p)
-              for (int v = 0; v < 5; ++v) {
+              for (int v = 0; v < NV; ++v) {
                 size_t idx = C.vol(v, C.s2v(0, p, q, fl, nls, 0), C.s2v(0, p, q, fl, nls, 1),
                                    C.s2v(0, p, q, fl, nls, 2), nb - 1);
                 g[idx] = g[idx] + F[C.fac(v, p, q, sid)] * C.L_HatMinus0;
               }
         }
       }
-      for (size_t z = 0; z < nt / 5; ++z)
-        for (int v = 0; v < 5; ++v) g[5 * z + v] = g[5 * z + v] * C.sJ[z];
-      for (size_t z = 0; z < nt / 5; ++z) ConvertToGradPrim(C, &C.U[5 * z], &g[5 * z]);
+      for (size_t z = 0; z < nt / NV; ++z)
+        for (int v = 0; v < NV; ++v) g[NV * z + v] = g[NV * z + v] * C.sJ[z];
+      for (size_t z = 0; z < nt / NV; ++z) GradPrim(C, &C.U[NV * z], &g[NV * z]);
       ProlongToFace(C, g, *GM[d], *GS[d]);
     }
   } else {
@@ -1547,9 +1614,9 @@ void Lifting(Case& C) {
           for (int q = 0; q < n; ++q)
             for (int p = 0; p < n; ++p) {
               size_t o = C.nod(C.s2v(0, p, q, 0, ls, 0), C.s2v(0, p, q, 0, ls, 1), C.s2v(0, p, q, 0, ls, 2), e - 1);
-              for (int v = 0; v < 5; ++v) {
+              for (int v = 0; v < NV; ++v) {
                 real Floc = C.sJ[o] * C.L_HatMinus0 * F[C.fac(v, p, q, sid)];
-                g[5 * o + v] = g[5 * o + v] + Floc;
+                g[NV * o + v] = g[NV * o + v] + Floc;
                 gm[C.fac(v, p, q, sid)] = gm[C.fac(v, p, q, sid)] + C.etaBR2 * Floc;
               }
             }
@@ -1560,19 +1627,19 @@ void Lifting(Case& C) {
           for (int q = 0; q < n; ++q)
             for (int p = 0; p < n; ++p) {
               size_t o = C.nod(C.s2v(0, p, q, fl, nls, 0), C.s2v(0, p, q, fl, nls, 1), C.s2v(0, p, q, fl, nls, 2), nb - 1);
-              for (int v = 0; v < 5; ++v) {
+              for (int v = 0; v < NV; ++v) {
                 real Floc = C.sJ[o] * C.L_HatMinus0 * F[C.fac(v, p, q, sid)];
-                g[5 * o + v] = g[5 * o + v] + Floc;
+                g[NV * o + v] = g[NV * o + v] + Floc;
                 gs[C.fac(v, p, q, sid)] = gs[C.fac(v, p, q, sid)] + C.etaBR2 * Floc;
               }
             }
         }
       }
-      for (size_t z = 0; z < nt / 5; ++z) ConvertToGradPrim(C, &C.U[5 * z], &g[5 * z]);
+      for (size_t z = 0; z < nt / NV; ++z) GradPrim(C, &C.U[NV * z], &g[NV * z]);
       size_t nf = (size_t)n * n * C.nSides;
       for (size_t z = 0; z < nf; ++z) {
-        ConvertToGradPrim(C, &C.Umaster[5 * z], &gm[5 * z]);
-        ConvertToGradPrim(C, &C.Uslave[5 * z], &gs[5 * z]);
+        GradPrim(C, &C.Umaster[NV * z], &gm[NV * z]);
+        GradPrim(C, &C.Uslave[NV * z], &gs[NV * z]);
       }
     }
   }
@@ -1583,54 +1650,76 @@ void FillFlux(Case& C) {
   int n = C.np, npts = n * n;
 #pragma omp parallel
   {
-  std::vector<real> ULL(5 * npts), URR(5 * npts), F(5 * npts);
+  const int NV = C.nVar;
+  std::vector<real> ULL(NV * npts), URR(NV * npts), F(NV * npts), FS(NV * npts);
+  // RotateState (navierstokes/riemann.f90:218-231, mhd/riemann.f90:185-200: also B)
+  auto rotate = [&](const real* U, const double* nv, const double* t1, const double* t2, real* R) {
+    for (int v = 0; v < NV; ++v) R[v] = U[v];
+    R[1] = U[1] * nv[0] + U[2] * nv[1] + U[3] * nv[2];
+    R[2] = U[1] * t1[0] + U[2] * t1[1] + U[3] * t1[2];
+    R[3] = U[1] * t2[0] + U[2] * t2[1] + U[3] * t2[2];
+    if (C.mhd) {
+      R[5] = U[5] * nv[0] + U[6] * nv[1] + U[7] * nv[2];
+      R[6] = U[5] * t1[0] + U[6] * t1[1] + U[7] * t1[2];
+      R[7] = U[5] * t2[0] + U[6] * t2[1] + U[7] * t2[2];
+    }
+  };
 #pragma omp for schedule(static)
   for (int sid = 0; sid < C.nSides; ++sid) {
-    for (int z = 0; z < npts; ++z) {  // RotateState, riemann.f90:218-231
+    for (int z = 0; z < npts; ++z) {
       size_t fi = (size_t)npts * sid + z;
       const double* nv = &C.NormVec[3 * fi];
       const double* t1 = &C.TangVec1[3 * fi];
       const double* t2 = &C.TangVec2[3 * fi];
-      const real* UL = &C.Umaster[5 * fi];
-      const real* UR = &C.Uslave[5 * fi];
-      ULL[5 * z + 0] = UL[0];
-      ULL[5 * z + 1] = UL[1] * nv[0] + UL[2] * nv[1] + UL[3] * nv[2];
-      ULL[5 * z + 2] = UL[1] * t1[0] + UL[2] * t1[1] + UL[3] * t1[2];
-      ULL[5 * z + 3] = UL[1] * t2[0] + UL[2] * t2[1] + UL[3] * t2[2];
-      ULL[5 * z + 4] = UL[4];
-      URR[5 * z + 0] = UR[0];
-      URR[5 * z + 1] = UR[1] * nv[0] + UR[2] * nv[1] + UR[3] * nv[2];
-      URR[5 * z + 2] = UR[1] * t1[0] + UR[2] * t1[1] + UR[3] * t1[2];
-      URR[5 * z + 3] = UR[1] * t2[0] + UR[2] * t2[1] + UR[3] * t2[2];
-      URR[5 * z + 4] = UR[4];
+      rotate(&C.Umaster[NV * fi], nv, t1, t2, &ULL[NV * z]);
+      rotate(&C.Uslave[NV * fi], nv, t1, t2, &URR[NV * z]);
     }
-    SolveRiemann(C, npts, ULL.data(), URR.data(), F.data());
-    for (int z = 0; z < npts; ++z) {  // RotateFluxBack :235-246
+    if (C.mhd) {
+      for (int z = 0; z < npts; ++z) MHD_Riemann(C, &ULL[NV * z], &URR[NV * z], &F[NV * z]);
+    } else {
+      SolveRiemann(C, npts, ULL.data(), URR.data(), F.data());
+    }
+    for (int z = 0; z < npts; ++z) {  // RotateFluxBack :235-246 (mhd/riemann.f90:204-217: also B)
       size_t fi = (size_t)npts * sid + z;
       const double* nv = &C.NormVec[3 * fi];
       const double* t1 = &C.TangVec1[3 * fi];
       const double* t2 = &C.TangVec2[3 * fi];
-      real f2 = F[5 * z + 1], f3 = F[5 * z + 2], f4 = F[5 * z + 3];
-      F[5 * z + 1] = nv[0] * f2 + t1[0] * f3 + t2[0] * f4;
-      F[5 * z + 2] = nv[1] * f2 + t1[1] * f3 + t2[1] * f4;
-      F[5 * z + 3] = nv[2] * f2 + t1[2] * f3 + t2[2] * f4;
+      real f2 = F[NV * z + 1], f3 = F[NV * z + 2], f4 = F[NV * z + 3];
+      F[NV * z + 1] = nv[0] * f2 + t1[0] * f3 + t2[0] * f4;
+      F[NV * z + 2] = nv[1] * f2 + t1[1] * f3 + t2[1] * f4;
+      F[NV * z + 3] = nv[2] * f2 + t1[2] * f3 + t2[2] * f4;
+      if (C.mhd) {
+        real f6 = F[NV * z + 5], f7 = F[NV * z + 6], f8 = F[NV * z + 7];
+        F[NV * z + 5] = nv[0] * f6 + t1[0] * f7 + t2[0] * f8;
+        F[NV * z + 6] = nv[1] * f6 + t1[1] * f7 + t2[1] * f8;
+        F[NV * z + 7] = nv[2] * f6 + t1[2] * f7 + t2[2] * f8;
+      }
     }
-    if (C.parabolic) {  // riemann.f90:155-168
+    if (C.parabolic) {  // riemann.f90:155-168 (mhd/riemann.f90:120-141)
       for (int z = 0; z < npts; ++z) {
         size_t fi = (size_t)npts * sid + z;
-        real kL[5], gL[5], jL[5], kR[5], gR[5], jR[5];
-        DiffFlux3D(C, &C.Umaster[5 * fi], &C.gxm[5 * fi], &C.gym[5 * fi], &C.gzm[5 * fi], kL, gL, jL);
-        DiffFlux3D(C, &C.Uslave[5 * fi], &C.gxs[5 * fi], &C.gys[5 * fi], &C.gzs[5 * fi], kR, gR, jR);
+        real kL[NVMAX], gL[NVMAX], jL[NVMAX], kR[NVMAX], gR[NVMAX], jR[NVMAX];
+        DiffFlux(C, &C.Umaster[NV * fi], &C.gxm[NV * fi], &C.gym[NV * fi], &C.gzm[NV * fi], kL, gL, jL);
+        DiffFlux(C, &C.Uslave[NV * fi], &C.gxs[NV * fi], &C.gys[NV * fi], &C.gzs[NV * fi], kR, gR, jR);
         const double* nv = &C.NormVec[3 * fi];
-        for (int v = 1; v < 5; ++v)
-          F[5 * z + v] = F[5 * z + v] + 0.5 * (nv[0] * (kL[v] + kR[v]) + nv[1] * (gL[v] + gR[v]) + nv[2] * (jL[v] + jR[v]));
+        for (int v = 1; v < NV; ++v)
+          F[NV * z + v] = F[NV * z + v] + 0.5 * (nv[0] * (kL[v] + kR[v]) + nv[1] * (gL[v] + gR[v]) + nv[2] * (jL[v] + jR[v]));
+      }
+    }
+    for (size_t z = 0; z < F.size(); ++z) FS[z] = F[z];  // Flux_slave = Flux_master (fillflux.f90:91)
+    if (C.mhd && C.noncons) {  // AddNonConsFlux on both sides, fillflux.f90:92-100
+      for (int z = 0; z < npts; ++z) {
+        size_t fi = (size_t)npts * sid + z;
+        const double* nv = &C.NormVec[3 * fi];
+        MHD_NonConsSurf(C, &C.Umaster[NV * fi], &C.Uslave[NV * fi], nv, &F[NV * z]);
+        MHD_NonConsSurf(C, &C.Uslave[NV * fi], &C.Umaster[NV * fi], nv, &FS[NV * z]);
       }
     }
     for (int z = 0; z < npts; ++z) {
       size_t fi = (size_t)npts * sid + z;
-      for (int v = 0; v < 5; ++v) {
-        C.Fmaster[5 * fi + v] = F[5 * z + v] * C.SurfElem[fi];
-        C.Fslave[5 * fi + v] = F[5 * z + v] * C.SurfElem[fi];
+      for (int v = 0; v < NV; ++v) {
+        C.Fmaster[NV * fi + v] = F[NV * z + v] * C.SurfElem[fi];
+        C.Fslave[NV * fi + v] = FS[NV * z + v] * C.SurfElem[fi];
       }
     }
   }
@@ -1646,7 +1735,7 @@ void SurfInt(Case& C) {
       int ls = C.SideToElem[2 + 5 * sid];
       for (int q = 0; q < n; ++q)
         for (int p = 0; p < n; ++p)
-          for (int v = 0; v < 5; ++v) {
+          for (int v = 0; v < C.nVar; ++v) {
             size_t idx = C.vol(v, C.s2v(0, p, q, 0, ls, 0), C.s2v(0, p, q, 0, ls, 1), C.s2v(0, p, q, 0, ls, 2), e - 1);
             C.Ut[idx] = C.Ut[idx] + C.Fmaster[C.fac(v, p, q, sid)] * C.L_HatMinus0;
           }
@@ -1656,7 +1745,7 @@ void SurfInt(Case& C) {
       int nls = C.SideToElem[3 + 5 * sid], fl = C.SideToElem[4 + 5 * sid];
       for (int q = 0; q < n; ++q)
         for (int p = 0; p < n; ++p)
-          for (int v = 0; v < 5; ++v) {
+          for (int v = 0; v < C.nVar; ++v) {
             size_t idx = C.vol(v, C.s2v(0, p, q, fl, nls, 0), C.s2v(0, p, q, fl, nls, 1), C.s2v(0, p, q, fl, nls, 2), nb - 1);
             C.Ut[idx] = C.Ut[idx] - C.Fslave[C.fac(v, p, q, sid)] * C.L_HatMinus0;
           }
@@ -1687,12 +1776,13 @@ void DGTimeDerivative(Case& C, double t) {
   PhaseCount pc(5);
   size_t nd = (size_t)C.np * C.np * C.np * C.nElems;
   for (size_t z = 0; z < nd; ++z)  // V2D_M_V1D(Ut,-sJ), vector.f90:144-166
-    for (int v = 0; v < 5; ++v) C.Ut[5 * z + v] = C.Ut[5 * z + v] * (-C.sJ[z]);
+    for (int v = 0; v < C.nVar; ++v) C.Ut[C.nVar * z + v] = C.Ut[C.nVar * z + v] * (-C.sJ[z]);
   CalcSource(C, t);
 }
 
 // CALCTIMESTEP, navierstokes/calctimestep.f90:39-170
 double CalcTimeStep(Case& C, int* errType) {
+  if (C.mhd) return MHD_CalcTimeStep(C, errType);
   *errType = 0;
   int n = C.np;
   double KappasPr_max = std::max(4. / 3., C.KappasPr);
@@ -1774,9 +1864,11 @@ void* orc_create(const orc_params* p) {
     C->P = *p;
     C->N = p->N;
     C->np = p->N + 1;
-    C->nVar = 5;
+    C->mhd = (p->eqn == 2 || p->eqn == 3);
+    C->nVar = C->mhd ? 9 : 5;
+    C->nAux = C->mhd ? 8 : 6;
     C->nDOFElem = C->np * C->np * C->np;
-    C->parabolic = (p->eqn == 1);
+    C->parabolic = (p->eqn == 1 || p->eqn == 3);
     InitEquationAndTime(*C);
     InitBasis(*C);
     BuildMesh(*C);
@@ -1794,9 +1886,10 @@ void* orc_create(const orc_params* p) {
     // FillIni(IniExactFunc, U), equation.f90:545-568
     size_t nd = (size_t)C->nDOFElem * C->nElems;
     for (size_t z = 0; z < nd; ++z) {
-      double r[5];
+      double r[NVMAX];
+      if (p->ini_exact_func == 0) break;  // state set by the caller (orc_set_U)
       ExactFunc(*C, p->ini_exact_func, 0., &C->Elem_xGP[3 * z], r);
-      for (int v = 0; v < 5; ++v) C->U[5 * z + v] = r[v];
+      for (int v = 0; v < C->nVar; ++v) C->U[C->nVar * z + v] = r[v];
     }
     return C;
   } catch (const std::exception& ex) {
@@ -1904,35 +1997,59 @@ void orc_analyze(void* h, double t, double* L2, double* Linf, double* entropy, d
     std::vector<double> xA(na), wA(na), V(na * n);
     LGLNodesWeights(NA, xA.data(), wA.data());
     InitVdm(N, NA, C->wBary.data(), C->xGP.data(), xA.data(), V.data());
-    double l2[5] = {0, 0, 0, 0, 0}, li[5] = {-1e10, -1e10, -1e10, -1e10, -1e10};
-    std::vector<double> XA(3 * na * na * na), JN(nv), JA(na * na * na), Uin(5 * nv), UA(5 * na * na * na);
+    const int NV = C->nVar;
+    double l2[NVMAX], li[NVMAX];
+    for (int v = 0; v < NVMAX; ++v) { l2[v] = 0.; li[v] = -1e10; }
+    std::vector<double> XA(3 * na * na * na), JN(nv), JA(na * na * na), Uin(NV * nv), UA(NV * na * na * na);
     for (int e = 0; e < C->nElems; ++e) {
       ChangeBasis3D(3, N, NA, V.data(), &C->Elem_xGP[3 * nv * e], XA.data());
       for (size_t z = 0; z < nv; ++z) JN[z] = 1. / C->sJ[nv * e + z];
       ChangeBasis3D(1, N, NA, V.data(), JN.data(), JA.data());
-      for (size_t z = 0; z < 5 * nv; ++z) Uin[z] = val(C->U[5 * nv * e + z]);
-      ChangeBasis3D(5, N, NA, V.data(), Uin.data(), UA.data());
+      for (size_t z = 0; z < NV * nv; ++z) Uin[z] = val(C->U[NV * nv * e + z]);
+      ChangeBasis3D(NV, N, NA, V.data(), Uin.data(), UA.data());
       for (int m = 0; m < na; ++m)
         for (int l = 0; l < na; ++l)
           for (int k = 0; k < na; ++k) {
             size_t z = k + na * (l + (size_t)na * m);
-            double ue[5];
+            double ue[NVMAX];
             ExactFunc(*C, C->P.ini_exact_func, t, &XA[3 * z], ue);
             double w = wA[k] * wA[l] * wA[m] * JA[z];
-            for (int v = 0; v < 5; ++v) {
-              double d = UA[5 * z + v] - ue[v];
+            for (int v = 0; v < NV; ++v) {
+              double d = UA[NV * z + v] - ue[v];
               li[v] = std::max(li[v], std::fabs(d));
               l2[v] += d * d * w;
             }
           }
     }
-    for (int v = 0; v < 5; ++v) {
+    for (int v = 0; v < NV; ++v) {
       if (L2) L2[v] = std::sqrt(l2[v] / Vol);
       if (Linf) Linf[v] = li[v];
     }
   }
   // CalcEntropy, navierstokes/analyze_equation.f90:549-599
   double S = 0., dS = 0., Ek = 0., En = 0.;
+  if (C->mhd) {  // CalcEntropy, mhd/analyze_equation.f90:421-470
+    for (int e = 0; e < C->nElems; ++e)
+      for (size_t z = 0; z < nv; ++z) {
+        size_t o = nv * e + z;
+        double w = wVol[z] / C->sJ[o];
+        real U[9], prim[9], W[9];
+        for (int v = 0; v < 9; ++v) U[v] = C->U[9 * o + v];
+        MHD_ConsToPrim(*C, U, prim);
+        S += val(-prim[0] * (log(prim[4]) - C->kappa * log(prim[0]))) * w;
+        MHD_ConsToEntropy(*C, U, W);
+        double loc = 0.;
+        for (int v = 0; v < 9; ++v) loc += val(W[v]) * val(C->Ut[9 * o + v]);
+        dS += loc * w;
+        double u = val(prim[1]), vv = val(prim[2]), ww = val(prim[3]);
+        Ek += 0.5 * val(U[0]) * (u * u + vv * vv + ww * ww) * w;
+      }
+    if (entropy) *entropy = S * C->sKappaM1;
+    if (dSdU_Ut) *dSdU_Ut = dS;
+    if (ekin) *ekin = Ek / Vol;
+    if (enstrophy) *enstrophy = 0.;
+    return;
+  }
   for (int e = 0; e < C->nElems; ++e)
     for (size_t z = 0; z < nv; ++z) {
       size_t o = nv * e + z;
@@ -1976,7 +2093,7 @@ void orc_analyze(void* h, double t, double* L2, double* Linf, double* entropy, d
 
 void orc_exact_func(void* h, int func, double t, int n, const double* x, double* U) {
   Case* C = (Case*)h;
-  for (int i = 0; i < n; ++i) ExactFunc(*C, func, t, x + 3 * i, U + 5 * i);
+  for (int i = 0; i < n; ++i) ExactFunc(*C, func, t, x + 3 * i, U + C->nVar * i);
 }
 
 void orc_basis(int N, double* xGP, double* wGP, double* wBary, double* D, double* Dvolsurf, double* Dhat,
@@ -2004,35 +2121,44 @@ void orc_reset_flops(void) {
 
 void orc_volume_flux(void* h, const double* UL, const double* UR, const double* mL, const double* mR, double* F) {
   Case* C = (Case*)h;
-  real uL[5], uR[5], aL[6], aR[6], ml[3], mr[3], f[5];
-  for (int v = 0; v < 5; ++v) { uL[v] = UL[v]; uR[v] = UR[v]; }
+  const int NV = C->nVar;
+  real uL[NVMAX], uR[NVMAX], aL[8], aR[8], ml[3], mr[3], f[NVMAX];
+  for (int v = 0; v < NV; ++v) { uL[v] = UL[v]; uR[v] = UR[v]; }
   for (int d = 0; d < 3; ++d) { ml[d] = mL[d]; mr[d] = mR[d]; }
-  EvalUaux(*C, uL, aL);
-  EvalUaux(*C, uR, aR);
-  VolumeFluxVec(*C, uL, uR, aL, aR, ml, mr, f);
-  for (int v = 0; v < 5; ++v) F[v] = val(f[v]);
+  Uaux(*C, uL, aL);
+  Uaux(*C, uR, aR);
+  if (C->mhd) MHD_VolumeFluxVec(*C, C->P.volume_flux, uL, uR, aL, aR, ml, mr, f);
+  else VolumeFluxVec(*C, uL, uR, aL, aR, ml, mr, f);
+  for (int v = 0; v < NV; ++v) F[v] = val(f[v]);
 }
 
 void orc_riemann_point(void* h, const double* UL, const double* UR, const double* nv, const double* t1,
                        const double* t2, double* F) {
   Case* C = (Case*)h;
-  real LL[5], RR[5], f[5];
-  LL[0] = UL[0]; LL[4] = UL[4];
-  RR[0] = UR[0]; RR[4] = UR[4];
-  LL[1] = UL[1] * nv[0] + UL[2] * nv[1] + UL[3] * nv[2];
-  LL[2] = UL[1] * t1[0] + UL[2] * t1[1] + UL[3] * t1[2];
-  LL[3] = UL[1] * t2[0] + UL[2] * t2[1] + UL[3] * t2[2];
-  RR[1] = UR[1] * nv[0] + UR[2] * nv[1] + UR[3] * nv[2];
-  RR[2] = UR[1] * t1[0] + UR[2] * t1[1] + UR[3] * t1[2];
-  RR[3] = UR[1] * t2[0] + UR[2] * t2[1] + UR[3] * t2[2];
-  SolveRiemann(*C, 1, LL, RR, f);
-  real f2 = f[1], f3 = f[2], f4 = f[3];
-  F[0] = val(f[0]);
-  F[1] = val(nv[0] * f2 + t1[0] * f3 + t2[0] * f4);
-  F[2] = val(nv[1] * f2 + t1[1] * f3 + t2[1] * f4);
-  F[3] = val(nv[2] * f2 + t1[2] * f3 + t2[2] * f4);
-  F[4] = val(f[4]);
+  const int NV = C->nVar;
+  real LL[NVMAX], RR[NVMAX], f[NVMAX];
+  for (int v = 0; v < NV; ++v) { LL[v] = UL[v]; RR[v] = UR[v]; }
+  for (int b = 1; b <= (C->mhd ? 5 : 1); b += 4) {  // momentum (and B for MHD)
+    LL[b] = UL[b] * nv[0] + UL[b + 1] * nv[1] + UL[b + 2] * nv[2];
+    LL[b + 1] = UL[b] * t1[0] + UL[b + 1] * t1[1] + UL[b + 2] * t1[2];
+    LL[b + 2] = UL[b] * t2[0] + UL[b + 1] * t2[1] + UL[b + 2] * t2[2];
+    RR[b] = UR[b] * nv[0] + UR[b + 1] * nv[1] + UR[b + 2] * nv[2];
+    RR[b + 1] = UR[b] * t1[0] + UR[b + 1] * t1[1] + UR[b + 2] * t1[2];
+    RR[b + 2] = UR[b] * t2[0] + UR[b + 1] * t2[1] + UR[b + 2] * t2[2];
+  }
+  if (C->mhd) MHD_Riemann(*C, LL, RR, f);
+  else SolveRiemann(*C, 1, LL, RR, f);
+  for (int v = 0; v < NV; ++v) F[v] = val(f[v]);
+  for (int b = 1; b <= (C->mhd ? 5 : 1); b += 4) {
+    real f2 = f[b], f3 = f[b + 1], f4 = f[b + 2];
+    F[b] = val(nv[0] * f2 + t1[0] * f3 + t2[0] * f4);
+    F[b + 1] = val(nv[1] * f2 + t1[1] * f3 + t2[1] * f4);
+    F[b + 2] = val(nv[2] * f2 + t1[2] * f3 + t2[2] * f4);
+  }
 }
+
+void orc_set_glm_ch(void* h, double ch) { ((Case*)h)->GLM_ch = ch; }
+double orc_get_glm_ch(void* h) { return ((Case*)h)->GLM_ch; }
 
 double orc_ln_mean(double aL, double aR) { return val(LN_MEAN(real(aL), real(aR))); }
 

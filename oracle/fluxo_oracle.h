@@ -23,7 +23,7 @@ typedef struct orc_params {
   double xmin[3], xmax[3];
   int NGeo;               /* geometry degree of the node coordinates */
   double deform_amp;      /* X_d += amp*prod_e sin(2*pi*(x_e-c_e)/L_e) */
-  int eqn;                /* 0 Euler (PARABOLIC=0), 1 Navier-Stokes */
+  int eqn;                /* 0 Euler (PARABOLIC=0), 1 Navier-Stokes, 2 ideal MHD + GLM, 3 MHD + GLM with PARABOLIC */
   int lifting;            /* 1 BR1, 2 BR2 */
   int lifting_var;        /* 1 cons_var, 2 prim_var, 3 entropy_var */
   int visc;               /* PP_VISC: 0 constant, 1 Sutherland, 2 power law */
@@ -38,6 +38,16 @@ typedef struct orc_params {
   double ref_state[5];    /* RefState (primitive) used by IniExactFunc=1 */
   double cfl_scale, dfl_scale;  /* CFLScale, DFLScale (unscaled input values) */
   int time_disc;          /* 0 carpenterrk4-5, 1 standardrk3-3, 2 niegemannrk4-14 */
+  /* MHD (eqn 2: ideal, eqn 3: with eta / mu, PARABOLIC), equation/mhd/equation.f90:134-285 */
+  double mu_0;            /* mu_0 (magnetic permeability) */
+  double eta;             /* eta (resistivity); the viscosity mu is mu0 above */
+  double glm_scale, glm_scr;  /* GLM_scale, GLM_scr */
+  double glm_ch;          /* GLM_ch before the first CALCTIMESTEP */
+  int noncons;            /* NONCONS: 0 off, 1 Powell, 2 Brackbill, 3 Janhunen */
+  int nc_glm;             /* PP_NC_GLM */
+  double mhd_ref_state[2][8];  /* RefState 1 and 2 (rho,u,v,w,p,B1,B2,B3) */
+  double ini_center[3];   /* IniCenter */
+  double ini_halfwidth;   /* IniHalfwidth */
 } orc_params;
 
 void* orc_create(const orc_params* p);
@@ -83,6 +93,9 @@ void orc_volume_flux(void* h, const double* UL, const double* UR, const double* 
 void orc_riemann_point(void* h, const double* UL, const double* UR, const double* nv,
                        const double* t1, const double* t2, double* F);
 double orc_ln_mean(double aL, double aR);
+/* MHD: the GLM cleaning speed GLM_ch (set by CALCTIMESTEP, or explicitly). */
+void orc_set_glm_ch(void* h, double ch);
+double orc_get_glm_ch(void* h);
 
 #ifdef __cplusplus
 }

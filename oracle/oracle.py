@@ -48,6 +48,16 @@ class OrcParams(ctypes.Structure):
         ("cfl_scale", ctypes.c_double),
         ("dfl_scale", ctypes.c_double),
         ("time_disc", ctypes.c_int),
+        ("mu_0", ctypes.c_double),
+        ("eta", ctypes.c_double),
+        ("glm_scale", ctypes.c_double),
+        ("glm_scr", ctypes.c_double),
+        ("glm_ch", ctypes.c_double),
+        ("noncons", ctypes.c_int),
+        ("nc_glm", ctypes.c_int),
+        ("mhd_ref_state", (ctypes.c_double * 8) * 2),
+        ("ini_center", ctypes.c_double * 3),
+        ("ini_halfwidth", ctypes.c_double),
     ]
 
 
@@ -58,6 +68,9 @@ DEFAULTS = dict(
     etaBR2=2.0, ini_exact_func=2, adv_vel=(1.0, 1.0, 1.0), ini_amplitude=0.1,
     ini_wavenumber=(1.0, 1.0, 1.0), ini_frequency=1.0, ref_state=(1.0, 0.3, 0.0, 0.0, 0.71428571),
     cfl_scale=0.9, dfl_scale=0.4, time_disc=0,
+    mu_0=1.0, eta=0.0, glm_scale=0.5, glm_scr=0.0, glm_ch=0.0, noncons=1, nc_glm=0,
+    mhd_ref_state=((1.0, 0.0, 0.0, 0.0, 1.0, 1.0, 0.0, 0.0), (1.0, 0.0, 0.0, 0.0, 1.0, 1.0, 0.0, 0.0)),
+    ini_center=(0.0, 0.0, 0.0), ini_halfwidth=0.1,
 )
 
 
@@ -105,6 +118,9 @@ def _lib(counting=False):
     lib.orc_riemann_point.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 6
     lib.orc_ln_mean.restype = d
     lib.orc_ln_mean.argtypes = [d, d]
+    lib.orc_set_glm_ch.argtypes = [ctypes.c_void_p, d]
+    lib.orc_get_glm_ch.restype = d
+    lib.orc_get_glm_ch.argtypes = [ctypes.c_void_p]
     _LIBS[name] = lib
     return lib
 
@@ -124,7 +140,11 @@ def make_params(**kw):
         f = getattr(p, k)
         if isinstance(f, ctypes.Array):
             for n, x in enumerate(v):
-                f[n] = x
+                if isinstance(f[n], ctypes.Array):
+                    for m, y in enumerate(x):
+                        f[n][m] = y
+                else:
+                    f[n] = x
         else:
             setattr(p, k, v)
     return p
@@ -230,14 +250,22 @@ class OracleCase:
         self.lib.orc_exact_func(self.h, func, t, x.shape[0], _ptr(x), _ptr(U))
         return U
 
+    @property
+    def glm_ch(self):
+        return self.lib.orc_get_glm_ch(self.h)
+
+    @glm_ch.setter
+    def glm_ch(self, ch):
+        self.lib.orc_set_glm_ch(self.h, float(ch))
+
     def volume_flux(self, UL, UR, mL, mR):
-        F = np.zeros(5)
+        F = np.zeros(self.nVar)
         a = [np.ascontiguousarray(v, dtype=np.float64) for v in (UL, UR, mL, mR)]
         self.lib.orc_volume_flux(self.h, *[_ptr(v) for v in a], _ptr(F))
         return F
 
     def riemann(self, UL, UR, nv, t1, t2):
-        F = np.zeros(5)
+        F = np.zeros(self.nVar)
         a = [np.ascontiguousarray(v, dtype=np.float64) for v in (UL, UR, nv, t1, t2)]
         self.lib.orc_riemann_point(self.h, *[_ptr(v) for v in a], _ptr(F))
         return F
