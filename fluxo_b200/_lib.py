@@ -52,6 +52,12 @@ class FluxoCfg(ctypes.Structure):
         ("ini_frequency", ctypes.c_double),
         ("ini_amplitude", ctypes.c_double),
         ("device", ctypes.c_int),
+        ("mu_0", ctypes.c_double),
+        ("eta", ctypes.c_double),
+        ("glm_scale", ctypes.c_double),
+        ("glm_scr", ctypes.c_double),
+        ("noncons", ctypes.c_int),
+        ("nc_glm", ctypes.c_int),
     ]
 
 
@@ -61,6 +67,7 @@ EXPORTS = [
     "fluxo_gpu_time_disc", "fluxo_gpu_device_buffers", "fluxo_gpu_launch_count", "fluxo_gpu_destroy",
     "fluxo_gpu_last_error", "fluxo_gpu_set_profiling", "fluxo_gpu_get_profile", "fluxo_gpu_fp64_peak",
     "fluxo_host_box_sizes", "fluxo_host_box_mesh", "fluxo_host_exact_func", "fluxo_gpu_dg_time_derivative_noalloc",
+    "fluxo_gpu_set_glm_ch", "fluxo_gpu_get_glm_ch",
 ]
 
 # FLUXO_NOALLOC_SCRATCH_BYTES of fluxo_gpu.h: the static scratch of fluxo_gpu_dg_time_derivative_noalloc
@@ -99,6 +106,8 @@ def load():
     lib.fluxo_host_box_mesh.argtypes = [i, vp, vp, vp, i, d] + [vp] * 11
     lib.fluxo_host_exact_func.argtypes = [i, d, ctypes.c_size_t, vp, d, vp, d, vp, d, vp, vp]
     lib.fluxo_gpu_dg_time_derivative_noalloc.argtypes = [P(FluxoCfg), i, i] + [vp] * 8
+    lib.fluxo_gpu_set_glm_ch.argtypes = [vp, d]
+    lib.fluxo_gpu_get_glm_ch.argtypes = [vp, P(d)]
     for name in EXPORTS:
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib

@@ -71,9 +71,17 @@ struct KParams {
   int stage;              // 1-based stage; 0 = plain DGTimeDerivative (write Ut)
   const int* haltFlag;    // device flag: nonzero -> kernels return at once
   double CFLScale, DFLScale, KappasPrMax;
+  // MHD with GLM (equation/mhd/equation.f90:134-285); the state has 9 variables
+  double smu_0, s2mu_0, kappaM2, etasmu_0, muMHD, glmScr;
+  int noncons;            // NONCONS: 0 off, 1 Powell, 2 Brackbill, 3 Janhunen
+  int ncGLM;              // PP_NC_GLM
+  int parabolic;          // resistive / viscous MHD (lifting + viscous fluxes)
+  double glmCh;           // GLM_ch of this RHS (host value) ...
+  const double* chDev;    // ... or from device memory (time_disc loop)
 };
 
 __device__ __forceinline__ bool halted(const KParams& P) { return P.haltFlag && *P.haltFlag != 0; }
+__device__ __forceinline__ double glm_ch(const KParams& P) { return P.chDev ? *P.chDev : P.glmCh; }
 
 // Asks the memory system to bring the line holding p into L2 (no register result, no fault on the
 // caller's side: only addresses inside live allocations are passed).

@@ -31,7 +31,13 @@ struct TDState {
   int errKey;                  // elem*8+errType of the first bad element, INT_MAX if none
   int iter, maxIter, last, done, err;
   int halt;                    // kernels return at once when nonzero
+  int glm;                     // MHD: GLM_ch follows every CALCTIMESTEP
+  double ch, glmScale, glmDtch1;  // GLM_ch of the current step, GLM_scale, GLM_dtch1
 };
+
+__global__ void td_glm_kernel(TDState* s, int glm, double ch, double scale, double dtch1) {
+  s->glm = glm; s->ch = ch; s->glmScale = scale; s->glmDtch1 = dtch1;
+}
 
 __global__ void td_begin_kernel(TDState* s, double t, double tEnd, int maxIter) {
   s->t = t; s->tEnd = tEnd; s->dt = 0.; s->iter = 0; s->maxIter = maxIter;
@@ -47,6 +53,7 @@ __global__ void td_finalize_kernel(TDState* s) {
   if (s->halt) return;
   if (s->errKey != INT_MAX) { s->err = s->errKey & 7; s->halt = 1; return; }
   double dt = __longlong_as_double((long long)s->dtBits);
+  if (s->glm) s->ch = s->glmScale * (s->glmDtch1 / dt);  // mhd/calctimestep.f90:176, before clipping
   s->last = 0;
   if (s->tEnd - s->t <= dt * (1. + 1.e-4)) { dt = s->tEnd - s->t; s->last = 1; }
   s->dt = dt;
@@ -72,6 +79,9 @@ __global__ void dt_reset_kernel(unsigned long long* bits, int* key) {
 struct fluxo_handle {
   fluxo_cfg cfg{};
   int N = 0, NP = 0, nElems = 0, nSides = 0;
+  int nVar = 5;                     // 5 (Euler / Navier-Stokes), 9 (MHD + GLM)
+  bool mhd = false;
+  double glmCh = 0., glmDtch1 = 0.;  // MHD: GLM_ch, GLM_dtch1 (from the metrics at set_mesh)
   bool visc = false, meshSet = false, stateSet = false, haveXGP = false;
   cudaStream_t stream = nullptr;
   BasisTables hb{};
@@ -185,6 +195,18 @@ KParams base_params(fluxo_handle* h) {
   }
   P.CFLScale = h->CFLScale; P.DFLScale = h->DFLScale;
   P.KappasPrMax = std::max(4. / 3., P.KappasPr);
+  if (h->mhd) {  // mhd/equation.f90:170-209; calctimestep.f90:81-84
+    P.kappaM2 = c.kappa - 2.;
+    P.smu_0 = 1. / c.mu_0; P.s2mu_0 = 0.5 * P.smu_0;
+    P.etasmu_0 = h->visc ? c.eta * P.smu_0 : 0.;
+    P.muMHD = h->visc ? c.mu0 : 0.;
+    P.KappasPrMax = P.muMHD * std::max(4. / 3., P.KappasPr);
+    P.glmScr = c.glm_scr;
+    P.source = (std::fabs(c.glm_scr) > 0.) ? 1 : 0;  // GLM damping in the volume kernel
+    P.glmCh = h->glmCh; P.chDev = nullptr;
+    P.noncons = c.noncons; P.ncGLM = c.nc_glm; P.parabolic = h->visc ? 1 : 0;
+    P.mu0 = 0.; P.visc = 0;
+  }
   return P;
 }
 
@@ -211,6 +233,31 @@ struct ProfScope {
 // One DGTimeDerivative; stage 0 writes Ut, stage >= 1 applies the fused LSERK stage update.
 int rhs(fluxo_handle* h, KParams P) {
   cudaStream_t s = h->stream;
+  if (h->mhd) {
+    if (h->visc) {
+      {
+        ProfScope ps(h, 0);
+        FLUXO_CUDA(h, launch_mhd_lift_flux(h->NP, h->nSides, s, P));
+      }
+      {
+        ProfScope ps(h, 1);
+        FLUXO_CUDA(h, launch_mhd_lift_visc(h->NP, h->cfg.lifting, h->nElems, s, P));
+      }
+      h->launches += 2;
+    }
+    {
+      ProfScope ps(h, 2);
+      FLUXO_CUDA(h, launch_mhd_face(h->cfg.riemann, h->visc, h->NP, h->nSides, s, P));
+    }
+    {
+      ProfScope ps(h, 3);
+      const int vf = h->cfg.volume_flux;
+      FLUXO_CUDA(h, (vf == 10 || vf == 12) ? launch_mhd_volume_ec(h->NP, vf, h->nElems, s, P)
+                                           : launch_mhd_volume_std(h->NP, vf, h->nElems, s, P));
+    }
+    h->launches += 2;
+    return FLUXO_OK;
+  }
   if (h->visc) {
     {
       ProfScope ps(h, 0);
@@ -250,9 +297,11 @@ __global__ void fp64_fma_kernel(double* out, int iters, double a, double b) {
 }
 
 // One LSERK-2reg step (timedisc.f90:424-480): host dt (dtDev == null) or device dt.
-int rk_step(fluxo_handle* h, double t, double dt, const double* dtDev, const int* halt) {
+int rk_step(fluxo_handle* h, double t, double dt, const double* dtDev, const int* halt,
+            const double* chDev = nullptr) {
   KParams P = base_params(h);
   P.dtDev = dtDev; P.haltFlag = halt; P.dt = dt;
+  P.chDev = chDev;
   for (int st = 1; st <= h->nStages; ++st) {
     P.stage = st;
     P.rkA = h->RKA[st]; P.rkB = h->RKb[st]; P.rkC = h->RKc[st];
@@ -285,11 +334,23 @@ int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {
   *out = nullptr;
   if (cfg->struct_size != (int)sizeof(fluxo_cfg)) return fail(nullptr, FLUXO_EINVAL_CFG, "fluxo_cfg size mismatch");
   if (cfg->N < 1 || cfg->N > 7) return fail(nullptr, FLUXO_EINVAL_CFG, "N must be in 1..7");
-  if (cfg->eqn != FLUXO_EQN_EULER && cfg->eqn != FLUXO_EQN_NAVIERSTOKES)
+  if (cfg->eqn < FLUXO_EQN_EULER || cfg->eqn > FLUXO_EQN_MHD_PARABOLIC)
     return fail(nullptr, FLUXO_EINVAL_CFG, "unknown equation system");
-  if (!riemann_supported(cfg->riemann)) return fail(nullptr, FLUXO_EINVAL_CFG, "Riemann solver not implemented");
-  if (!volume_flux_supported(cfg->volume_flux)) return fail(nullptr, FLUXO_EINVAL_CFG, "volume flux not implemented");
-  if (cfg->eqn == FLUXO_EQN_NAVIERSTOKES) {
+  const bool mhd = (cfg->eqn == FLUXO_EQN_MHD || cfg->eqn == FLUXO_EQN_MHD_PARABOLIC);
+  const bool parabolic = (cfg->eqn == FLUXO_EQN_NAVIERSTOKES || cfg->eqn == FLUXO_EQN_MHD_PARABOLIC);
+  if (mhd) {
+    if (!mhd_riemann_supported(cfg->riemann)) return fail(nullptr, FLUXO_EINVAL_CFG, "MHD Riemann solver not implemented");
+    if (!mhd_volume_flux_supported(cfg->volume_flux))
+      return fail(nullptr, FLUXO_EINVAL_CFG, "MHD volume flux not implemented");
+    if (cfg->noncons < 0 || cfg->noncons > 3) return fail(nullptr, FLUXO_EINVAL_CFG, "noncons must be 0..3");
+    if (!(cfg->mu_0 > 0.)) return fail(nullptr, FLUXO_EINVAL_CFG, "mu_0 must be > 0");
+    if (cfg->ini_exact_func == 4) return fail(nullptr, FLUXO_EINVAL_CFG, "MHD source terms are not implemented");
+  } else {
+    if (!riemann_supported(cfg->riemann)) return fail(nullptr, FLUXO_EINVAL_CFG, "Riemann solver not implemented");
+    if (!volume_flux_supported(cfg->volume_flux))
+      return fail(nullptr, FLUXO_EINVAL_CFG, "volume flux not implemented");
+  }
+  if (parabolic) {
     if (cfg->lifting != 1 && cfg->lifting != 2) return fail(nullptr, FLUXO_EINVAL_CFG, "lifting must be BR1 or BR2");
     if (cfg->lifting_var < 1 || cfg->lifting_var > 3) return fail(nullptr, FLUXO_EINVAL_CFG, "lifting_var must be 1..3");
     if (cfg->visc < 0 || cfg->visc > 2) return fail(nullptr, FLUXO_EINVAL_CFG, "visc must be 0..2");
@@ -298,7 +359,9 @@ int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {
   fluxo_handle* h = new fluxo_handle();
   h->cfg = *cfg;
   h->N = cfg->N; h->NP = cfg->N + 1;
-  h->visc = (cfg->eqn == FLUXO_EQN_NAVIERSTOKES);
+  h->visc = parabolic;
+  h->mhd = mhd;
+  h->nVar = mhd ? 9 : 5;
   // time discretisation coefficients and CFL/DFL scaling (timedisc_vars.f90:204-235, timedisc.f90:697-741)
   double cflAlpha[15], relDFL;
   if (cfg->time_disc == 0) {
@@ -402,18 +465,34 @@ int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* S2E, 
       geo[((size_t)s * 10 + 9) * NPT + p] = SurfElem[src];
     }
   h->nElems = nElems; h->nSides = nSides;
-  const size_t nU = (size_t)5 * NP3 * nElems, nF = (size_t)5 * NPT * nSides;
+  const int NV = h->nVar;
+  const size_t nU = (size_t)NV * NP3 * nElems, nF = (size_t)NV * NPT * nSides;
+  const size_t nFlux = (size_t)(h->mhd ? 13 : 5) * NPT * nSides;  // MHD: + non-conservative weights
   int r = FLUXO_OK;
   if ((r = dalloc(h, &h->dU, nU)) || (r = dalloc(h, &h->dUt, nU)) || (r = dalloc(h, &h->dUtTmp, nU)) ||
       (r = dalloc(h, &h->dMetrics, met.size())) || (r = dalloc(h, &h->dsJ, (size_t)NP3 * nElems)) ||
-      (r = dalloc(h, &h->dFaceGeo, geo.size())) || (r = dalloc(h, &h->dFlux, nF)) ||
+      (r = dalloc(h, &h->dFaceGeo, geo.size())) || (r = dalloc(h, &h->dFlux, nFlux)) ||
       (r = dalloc(h, &h->dS2E, s2e.size())) || (r = dalloc(h, &h->dE2S, e2s.size())))
     return r;
   if (h->visc) {
     if ((r = dalloc(h, &h->dGrad, 3 * nU)) || (r = dalloc(h, &h->dLFlux, nF)) ||
-        (r = dalloc(h, &h->dUtVisc, (size_t)4 * NP3 * nElems)) ||
-        (r = dalloc(h, &h->dGTrace, (size_t)2 * 15 * NPT * nSides)))
+        (r = dalloc(h, &h->dUtVisc, (size_t)(h->mhd ? 7 : 4) * NP3 * nElems)) ||
+        (r = dalloc(h, &h->dGTrace, (size_t)2 * 3 * NV * NPT * nSides)))
       return r;
+  }
+  if (h->mhd) {  // InitTimeStep_GLM, mhd/calctimestep.f90:187-223
+    double dtch1 = 1.7976931348623157e308;
+    for (int e = 0; e < nElems; ++e) {
+      double ml[3] = {0., 0., 0.};
+      for (int n = 0; n < NP3; ++n) {
+        const size_t o = (size_t)e * NP3 + n;
+        const double* M[3] = {Mf + 3 * o, Mg + 3 * o, Mh + 3 * o};
+        for (int d = 0; d < 3; ++d)
+          ml[d] = std::max(ml[d], sJ[o] * std::sqrt(M[d][0] * M[d][0] + M[d][1] * M[d][1] + M[d][2] * M[d][2]));
+      }
+      dtch1 = std::min(dtch1, h->CFLScale * 2. / (ml[0] + ml[1] + ml[2]));
+    }
+    h->glmDtch1 = dtch1;
   }
   cudaStream_t s = h->stream;
   FLUXO_CUDA(h, cudaMemcpyAsync(h->dMetrics, met.data(), met.size() * 8, cudaMemcpyHostToDevice, s));
@@ -438,7 +517,7 @@ int fluxo_gpu_set_state(fluxo_handle* h, const double* U) {
   if (!h || !U) return FLUXO_EINVAL_CFG;
   if (!h->meshSet) return fail(h, FLUXO_ENOTREADY, "mesh not set");
   FLUXO_CUDA(h, cudaSetDevice(h->cfg.device));
-  const size_t nU = (size_t)5 * h->NP * h->NP * h->NP * h->nElems;
+  const size_t nU = (size_t)h->nVar * h->NP * h->NP * h->NP * h->nElems;
   FLUXO_CUDA(h, cudaMemcpyAsync(h->dU, U, nU * 8, cudaMemcpyHostToDevice, h->stream));
   FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
   h->stateSet = true;
@@ -448,7 +527,7 @@ int fluxo_gpu_set_state(fluxo_handle* h, const double* U) {
 int fluxo_gpu_get_state(fluxo_handle* h, double* U) {
   int r = check_ready(h);
   if (r) return r;
-  const size_t nU = (size_t)5 * h->NP * h->NP * h->NP * h->nElems;
+  const size_t nU = (size_t)h->nVar * h->NP * h->NP * h->NP * h->nElems;
   FLUXO_CUDA(h, cudaMemcpyAsync(U, h->dU, nU * 8, cudaMemcpyDeviceToHost, h->stream));
   FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
   return FLUXO_OK;
@@ -457,7 +536,7 @@ int fluxo_gpu_get_state(fluxo_handle* h, double* U) {
 int fluxo_gpu_get_ut(fluxo_handle* h, double* Ut) {
   int r = check_ready(h);
   if (r) return r;
-  const size_t nU = (size_t)5 * h->NP * h->NP * h->NP * h->nElems;
+  const size_t nU = (size_t)h->nVar * h->NP * h->NP * h->NP * h->nElems;
   FLUXO_CUDA(h, cudaMemcpyAsync(Ut, h->dUt, nU * 8, cudaMemcpyDeviceToHost, h->stream));
   FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
   return FLUXO_OK;
@@ -466,16 +545,17 @@ int fluxo_gpu_get_ut(fluxo_handle* h, double* Ut) {
 int fluxo_gpu_get_gradients(fluxo_handle* h, double* gx, double* gy, double* gz) {
   int r = check_ready(h);
   if (r) return r;
-  if (!h->visc) return fail(h, FLUXO_EINVAL_CFG, "gradients exist for Navier-Stokes only");
+  if (!h->visc) return fail(h, FLUXO_EINVAL_CFG, "gradients exist for the parabolic equations only");
   const size_t nD = (size_t)h->NP * h->NP * h->NP * h->nElems;
-  std::vector<double> g(15 * nD);
+  const int NV = h->nVar;
+  std::vector<double> g(3 * NV * nD);
   FLUXO_CUDA(h, cudaMemcpyAsync(g.data(), h->dGrad, g.size() * 8, cudaMemcpyDeviceToHost, h->stream));
   FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
   for (size_t z = 0; z < nD; ++z)
-    for (int v = 0; v < 5; ++v) {
-      if (gx) gx[5 * z + v] = g[15 * z + v];
-      if (gy) gy[5 * z + v] = g[15 * z + 5 + v];
-      if (gz) gz[5 * z + v] = g[15 * z + 10 + v];
+    for (int v = 0; v < NV; ++v) {
+      if (gx) gx[NV * z + v] = g[3 * NV * z + v];
+      if (gy) gy[NV * z + v] = g[3 * NV * z + NV + v];
+      if (gz) gz[NV * z + v] = g[3 * NV * z + 2 * NV + v];
     }
   return FLUXO_OK;
 }
@@ -499,7 +579,8 @@ int fluxo_gpu_calc_timestep(fluxo_handle* h, double* dt, int* errType) {
   KParams P = base_params(h);
   dt_reset_kernel<<<1, 1, 0, h->stream>>>(h->dDtBits, h->dErrKey);
   FLUXO_CUDA(h, cudaGetLastError());
-  FLUXO_CUDA(h, launch_timestep(h->NP, h->visc, h->nElems, h->stream, P, h->dDtBits, h->dErrKey));
+  if (h->mhd) FLUXO_CUDA(h, launch_mhd_timestep(h->NP, h->visc, h->nElems, h->stream, P, h->dDtBits, h->dErrKey));
+  else FLUXO_CUDA(h, launch_timestep(h->NP, h->visc, h->nElems, h->stream, P, h->dDtBits, h->dErrKey));
   h->launches += 2;
   unsigned long long bits = 0;
   int key = 0;
@@ -509,6 +590,7 @@ int fluxo_gpu_calc_timestep(fluxo_handle* h, double* dt, int* errType) {
   double d;
   std::memcpy(&d, &bits, 8);
   if (dt) *dt = d;
+  if (h->mhd && key == INT_MAX) h->glmCh = h->cfg.glm_scale * (h->glmDtch1 / d);  // mhd/calctimestep.f90:176
   int err = (key == INT_MAX) ? 0 : (key & 7);
   if (errType) *errType = err;
   return err ? FLUXO_ENAN_STATE : FLUXO_OK;
@@ -529,8 +611,9 @@ int fluxo_gpu_time_disc(fluxo_handle* h, double t, double tEnd, int maxIter, dou
   cudaStream_t s = h->stream;
   TDState* td = h->dTD;
   td_begin_kernel<<<1, 1, 0, s>>>(td, t, tEnd, maxIter);
+  td_glm_kernel<<<1, 1, 0, s>>>(td, h->mhd ? 1 : 0, h->glmCh, h->cfg.glm_scale, h->glmDtch1);
   FLUXO_CUDA(h, cudaGetLastError());
-  h->launches += 1;
+  h->launches += 2;
   const int chunk = 16;
   for (;;) {
     for (int c = 0; c < chunk; ++c) {
@@ -538,11 +621,12 @@ int fluxo_gpu_time_disc(fluxo_handle* h, double t, double tEnd, int maxIter, dou
       P.haltFlag = &td->halt;
       {
         ProfScope ps(h, 4);
-        FLUXO_CUDA(h, launch_timestep(h->NP, h->visc, h->nElems, s, P, &td->dtBits, &td->errKey));
+        if (h->mhd) FLUXO_CUDA(h, launch_mhd_timestep(h->NP, h->visc, h->nElems, s, P, &td->dtBits, &td->errKey));
+        else FLUXO_CUDA(h, launch_timestep(h->NP, h->visc, h->nElems, s, P, &td->dtBits, &td->errKey));
       }
       td_finalize_kernel<<<1, 1, 0, s>>>(td);
       FLUXO_CUDA(h, cudaGetLastError());
-      if ((r = rk_step(h, 0., 0., &td->dt, &td->halt))) return r;
+      if ((r = rk_step(h, 0., 0., &td->dt, &td->halt, h->mhd ? &td->ch : nullptr))) return r;
       td_advance_kernel<<<1, 1, 0, s>>>(td);
       FLUXO_CUDA(h, cudaGetLastError());
       h->launches += 3;
@@ -552,12 +636,27 @@ int fluxo_gpu_time_disc(fluxo_handle* h, double t, double tEnd, int maxIter, dou
     FLUXO_CUDA(h, cudaMemcpyAsync(&hs, td, sizeof(TDState), cudaMemcpyDeviceToHost, s));
     FLUXO_CUDA(h, cudaStreamSynchronize(s));
     if (hs.halt) {
+      if (h->mhd) h->glmCh = hs.ch;
       if (tOut) *tOut = hs.t;
       if (nIter) *nIter = hs.iter;
       if (errType) *errType = hs.err;
       return hs.err ? FLUXO_ENAN_STATE : FLUXO_OK;
     }
   }
+}
+
+int fluxo_gpu_set_glm_ch(fluxo_handle* h, double ch) {
+  if (!h) return FLUXO_EINVAL_CFG;
+  if (!h->mhd) return fail(h, FLUXO_EINVAL_CFG, "GLM_ch exists for MHD only");
+  h->glmCh = ch;
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_get_glm_ch(fluxo_handle* h, double* ch) {
+  if (!h || !ch) return FLUXO_EINVAL_CFG;
+  if (!h->mhd) return fail(h, FLUXO_EINVAL_CFG, "GLM_ch exists for MHD only");
+  *ch = h->glmCh;
+  return FLUXO_OK;
 }
 
 int fluxo_gpu_device_buffers(fluxo_handle* h, double** dU, double** dUt, void** stream) {

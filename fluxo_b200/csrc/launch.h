@@ -31,6 +31,19 @@ cudaError_t launch_timestep(int NP, bool visc, int nElems, cudaStream_t s, const
 bool riemann_supported(int RS);
 bool volume_flux_supported(int VF);
 
+// MHD + GLM (9 variables): face (Riemann 0,1,4,10-15), lifting flux, lifting + viscous, volume
+// (VF 0,1 standard; 10,12 entropy conserving), time step.  Non-conservative terms and the
+// parabolic part are runtime flags of KParams.
+bool mhd_riemann_supported(int RS);
+bool mhd_volume_flux_supported(int VF);
+cudaError_t launch_mhd_face(int RS, bool visc, int NP, int nSides, cudaStream_t s, const KParams& P);
+cudaError_t launch_mhd_lift_flux(int NP, int nSides, cudaStream_t s, const KParams& P);
+cudaError_t launch_mhd_lift_visc(int NP, int lift, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_mhd_volume_ec(int NP, int VF, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_mhd_volume_std(int NP, int VF, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_mhd_timestep(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P,
+                                unsigned long long* dtBits, int* errKey);
+
 // Host helpers of fluxo_gpu.cu for entry points without a handle: the per-N operator tables, and
 // the message that fluxo_gpu_last_error(NULL, ...) returns (returns `code`).
 void basis_tables_for(int N, BasisTables& B);

@@ -28,7 +28,8 @@ def make_cfg(**fields):
     cfg.struct_size = ctypes.sizeof(_lib.FluxoCfg)
     defaults = dict(N=3, eqn=0, riemann=1, volume_flux=0, lifting=1, lifting_var=3, visc=0, kappa=1.4, R=287.058,
                     Pr=0.72, mu0=0.0, Ts=110.4, Tref=280.0, ExpoSuth=1.5, ExpoPow=0.0, etaBR2=2.0, time_disc=0,
-                    cfl_scale=0.9, dfl_scale=0.4, ini_exact_func=1, ini_frequency=1.0, ini_amplitude=0.1, device=0)
+                    cfl_scale=0.9, dfl_scale=0.4, ini_exact_func=1, ini_frequency=1.0, ini_amplitude=0.1, device=0,
+                    mu_0=1.0, eta=0.0, glm_scale=0.5, glm_scr=0.0, noncons=1, nc_glm=0)
     defaults.update(fields)
     for k, v in defaults.items():
         setattr(cfg, k, v)
@@ -86,6 +87,7 @@ class DGOperator:
         _lib.check(r, None)
         self.h = h
         self.N = self.cfg.N
+        self.nVar = 9 if self.cfg.eqn in (2, 3) else 5
         self.nElems = self.nSides = 0
 
     def close(self):
@@ -113,7 +115,18 @@ class DGOperator:
     @property
     def shape(self):
         n = self.N + 1
-        return (self.nElems, n, n, n, 5)
+        return (self.nElems, n, n, n, self.nVar)
+
+    @property
+    def glm_ch(self):
+        """MHD: GLM_ch of the next right-hand side (set by calc_timestep / time_disc)."""
+        ch = ctypes.c_double()
+        self._check(self.lib.fluxo_gpu_get_glm_ch(self.h, ctypes.byref(ch)))
+        return ch.value
+
+    @glm_ch.setter
+    def glm_ch(self, ch):
+        self._check(self.lib.fluxo_gpu_set_glm_ch(self.h, float(ch)))
 
     def set_state(self, U):
         U = _c(U)

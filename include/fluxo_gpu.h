@@ -41,7 +41,7 @@ enum {
   FLUXO_ENOTREADY = -6    /* mesh or state not set */
 };
 
-enum { FLUXO_EQN_EULER = 0, FLUXO_EQN_NAVIERSTOKES = 1 };
+enum { FLUXO_EQN_EULER = 0, FLUXO_EQN_NAVIERSTOKES = 1, FLUXO_EQN_MHD = 2, FLUXO_EQN_MHD_PARABOLIC = 3 };
 
 /* Runtime configuration: the parameter.ini keys of the reference's hot path
  * (src/equation/navierstokes/equation.f90:162-470, src/timedisc/timedisc.f90:74-137,
@@ -64,6 +64,15 @@ typedef struct fluxo_cfg {
   int ini_exact_func;   /* IniExactFunc: only 4 adds a source term (CalcSource) */
   double ini_frequency, ini_amplitude;
   int device;        /* CUDA device ordinal */
+  /* MHD with GLM cleaning, eqn = FLUXO_EQN_MHD / FLUXO_EQN_MHD_PARABOLIC
+   * (src/equation/mhd/equation.f90:134-285; nVar = 9: rho, rho*v, E, B, psi).  The MHD viscosity
+   * mu is mu0 above (constant); riemann 0,1,4,10-15; volume_flux 0,1,10,12. */
+  double mu_0;       /* mu_0, magnetic permeability */
+  double eta;        /* eta, resistivity (PARABOLIC) */
+  double glm_scale;  /* GLM_scale: GLM_ch = GLM_scale * GLM_dtch1 / dt (calctimestep.f90:176) */
+  double glm_scr;    /* GLM_scr: damping Ut(9) -= GLM_scr*GLM_ch*U(9) (equation.f90:1698-1706) */
+  int noncons;       /* NONCONS: 0 off, 1 Powell, 2 Brackbill, 3 Janhunen (CMake FLUXO_EQN_NONCONS_TYPE) */
+  int nc_glm;        /* PP_NC_GLM: non-conservative GLM terms (CMake FLUXO_EQN_NONCONS_GLM) */
 } fluxo_cfg;
 
 typedef struct fluxo_handle fluxo_handle;
@@ -114,6 +123,12 @@ int fluxo_gpu_timestep(fluxo_handle* h, double t, double dt);
  * errType that stopped the loop (0 = none). */
 int fluxo_gpu_time_disc(fluxo_handle* h, double t, double tEnd, int maxIter, double* tOut,
                         int* nIter, int* errType);
+
+/* MHD: MOD_Equation_Vars::GLM_ch, the GLM cleaning speed used by the RHS.  CALCTIMESTEP
+ * (fluxo_gpu_calc_timestep, and every step of fluxo_gpu_time_disc) sets it to
+ * GLM_scale*GLM_dtch1/dt (src/equation/mhd/calctimestep.f90:175-177, InitTimeStep_GLM :187-223). */
+int fluxo_gpu_set_glm_ch(fluxo_handle* h, double ch);
+int fluxo_gpu_get_glm_ch(fluxo_handle* h, double* ch);
 
 /* Device pointers and stream for zero-copy callers (e.g. torch tensors):
  * U, Ut are device buffers of nVar*(N+1)^3*nElems doubles in the host layout. */
