@@ -341,6 +341,8 @@ struct Case {
   double mu_0 = 1., smu_0 = 1., s2mu_0 = 0.5, kappaM2 = 0., eta = 0., etasmu_0 = 0., muMHD = 0.;
   double GLM_scale = 0.5, GLM_scr = 0., GLM_ch = 0., GLM_dtch1 = 0.;
   bool GLM_init = false;
+  // NFVSE shock capturing (shockcapturing/nfvse_vars.f90): blending coefficients, sub-cell metrics
+  std::vector<double> alpha, alphaMaster, alphaSlave, scNv, scT1, scT2, scNorm;
   // basis (double), dg/dg.f90:181-252
   std::vector<double> xGP, wGP, wBary, D, D_T, Dhat, Dhat_T, Dvolsurf, Dvolsurf_T, Lminus, Lplus;
   double L_HatMinus0, L_HatPlus0;
@@ -1753,6 +1755,8 @@ void SurfInt(Case& C) {
   }
 }
 
+#include "fluxo_oracle_nfvse.h"
+
 uint64_t g_phase[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 struct PhaseCount {  // operation count of one phase of the RHS (counting build)
   int k;
@@ -1766,7 +1770,9 @@ struct PhaseCount {  // operation count of one phase of the RHS (counting build)
 void DGTimeDerivative(Case& C, double t) {
   std::fill(C.Ut.begin(), C.Ut.end(), real(0.));  // VNullify
   ProlongToFace(C, C.U, C.Umaster, C.Uslave);
+  if (C.P.nfvse) CalcBlendingCoefficient(C);  // dg.f90:358-361
   { PhaseCount pc(0); VolIntSplitForm(C); }
+  if (C.P.nfvse) { PhaseCount pc(6); VolIntNFVSE(C); }  // dg.f90:380-383
   if (C.parabolic) {
     { PhaseCount pc(1); Lifting(C); }
     { PhaseCount pc(2); VolIntVisc(C); }
@@ -1873,6 +1879,13 @@ void* orc_create(const orc_params* p) {
     InitBasis(*C);
     BuildMesh(*C);
     CalcMetrics(*C);
+    if (p->nfvse) {  // InitNFVSE, nfvse.f90:106-260
+      if (p->N < 2) throw std::runtime_error("NFVSE needs N >= 2 (shockcapturing.f90)");
+      C->alpha.assign(C->nElems, 0.);
+      C->alphaMaster.assign(C->nSides, 0.);
+      C->alphaSlave.assign(C->nSides, 0.);
+      ComputeSubcellMetrics(*C);
+    }
     size_t nt = (size_t)C->nVar * C->nDOFElem * C->nElems;
     size_t nf = (size_t)C->nVar * C->np * C->np * C->nSides;
     C->U.assign(nt, 0.); C->Ut.assign(nt, 0.); C->UtTmp.assign(nt, 0.);
@@ -2155,6 +2168,11 @@ void orc_riemann_point(void* h, const double* UL, const double* UR, const double
     F[b + 1] = val(nv[1] * f2 + t1[1] * f3 + t2[1] * f4);
     F[b + 2] = val(nv[2] * f2 + t1[2] * f3 + t2[2] * f4);
   }
+}
+
+void orc_get_alpha(void* h, double* alpha) {
+  Case* C = (Case*)h;
+  for (size_t e = 0; e < C->alpha.size(); ++e) alpha[e] = C->alpha[e];
 }
 
 void orc_set_glm_ch(void* h, double ch) { ((Case*)h)->GLM_ch = ch; }

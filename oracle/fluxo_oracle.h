@@ -48,6 +48,15 @@ typedef struct orc_params {
   double mhd_ref_state[2][8];  /* RefState 1 and 2 (rho,u,v,w,p,B1,B2,B3) */
   double ini_center[3];   /* IniCenter */
   double ini_halfwidth;   /* IniHalfwidth */
+  /* NFVSE shock capturing (shockcapturing/nfvse.f90:63-260), SubFVMethod = 1 */
+  int nfvse;              /* SHOCK_NFVSE on/off */
+  int compute_alpha;      /* ComputeAlpha: 1 Persson-Peraire indicator, 3 fixed ShockBlendCoef */
+  double shock_blend_coef;
+  int modal_threshold;    /* ModalThreshold 1 or 2 */
+  double alpha_max, alpha_min, space_prop_factor;
+  int space_prop_sweeps;
+  double time_rel_factor;
+  int indicator_quantity; /* ShockIndicatorQuantity: 1 Density, 2 Pressure, 3 DensityTimesPressure, 4 KinEnergy */
 } orc_params;
 
 void* orc_create(const orc_params* p);
@@ -93,6 +102,8 @@ void orc_volume_flux(void* h, const double* UL, const double* UR, const double* 
 void orc_riemann_point(void* h, const double* UL, const double* UR, const double* nv,
                        const double* t1, const double* t2, double* F);
 double orc_ln_mean(double aL, double aR);
+/* NFVSE: blending coefficient alpha(nElems) of the last right-hand side. */
+void orc_get_alpha(void* h, double* alpha);
 /* MHD: the GLM cleaning speed GLM_ch (set by CALCTIMESTEP, or explicitly). */
 void orc_set_glm_ch(void* h, double ch);
 double orc_get_glm_ch(void* h);

@@ -1,0 +1,234 @@
+// ORACLE — test infrastructure only (part of fluxo_oracle.cpp, included inside its namespace).
+// CPU restatement of the reference's NFVSE shock capturing (shockcapturing/nfvse.f90,
+// nfvse_mpi.f90, indicators/indicators.f90): Persson-Peraire indicator, blending coefficient,
+// its space propagation, the first-order subcell finite-volume volume integral on the LGL
+// subcells (SubFVMethod = 1) and its blending with the split-form volume integral.
+
+// Sub-cell metrics, nfvse.f90:261-378: for direction d, subcell face f = -1..N and transverse
+// point (a,b): normal, tangents and the norm of the (unnormalised) face metric
+inline size_t SubcellIdx(const Case& C, int e, int d, int f, int a, int b) {
+  const int n = C.np;
+  return ((((size_t)e * 3 + d) * (n + 1) + (f + 1)) * n + b) * n + a;
+}
+
+void ComputeSubcellMetrics(Case& C) {
+  const int n = C.np, N = C.N;
+  const size_t cnt = (size_t)C.nElems * 3 * (n + 1) * n * n;
+  C.scNv.assign(3 * cnt, 0.); C.scT1.assign(3 * cnt, 0.); C.scT2.assign(3 * cnt, 0.); C.scNorm.assign(cnt, 0.);
+  for (int e = 0; e < C.nElems; ++e)
+    for (int d = 0; d < 3; ++d) {
+      // metric of the normal (Ja^d) and of the first tangent (Ja^(d+1)) at line position x, point (a,b)
+      const std::vector<double>& Mn = (d == 0) ? C.Mf : (d == 1 ? C.Mg : C.Mh);
+      const std::vector<double>& Mt = (d == 0) ? C.Mg : (d == 1 ? C.Mh : C.Mf);
+      auto node = [&](int x, int a, int b) -> size_t {  // (a,b) = (j,k) for xi, (i,k) for eta, (i,j) for zeta
+        if (d == 0) return C.nod(x, a, b, e);
+        if (d == 1) return C.nod(a, x, b, e);
+        return C.nod(a, b, x, e);
+      };
+      for (int f = -1; f <= N; ++f)
+        for (int b = 0; b < n; ++b)
+          for (int a = 0; a < n; ++a) {
+            double nv[3], t1[3];
+            for (int c = 0; c < 3; ++c) { nv[c] = Mn[3 * node(0, a, b) + c]; t1[c] = Mt[3 * node(0, a, b) + c]; }
+            for (int m = 0; m <= N; ++m)
+              for (int l = 0; l <= f; ++l)
+                for (int c = 0; c < 3; ++c) {
+                  nv[c] = nv[c] + C.wGP[l] * C.D[l + n * m] * Mn[3 * node(m, a, b) + c];
+                  t1[c] = t1[c] + C.wGP[l] * C.D[l + n * m] * Mt[3 * node(m, a, b) + c];
+                }
+            const double norm = std::sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+            for (int c = 0; c < 3; ++c) nv[c] = nv[c] / norm;
+            const double tn = t1[0] * nv[0] + t1[1] * nv[1] + t1[2] * nv[2];
+            for (int c = 0; c < 3; ++c) t1[c] = t1[c] - tn * nv[c];
+            const double tl = std::sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+            for (int c = 0; c < 3; ++c) t1[c] = t1[c] / tl;
+            const double t2[3] = {nv[1] * t1[2] - nv[2] * t1[1], nv[2] * t1[0] - nv[0] * t1[2],
+                                  nv[0] * t1[1] - nv[1] * t1[0]};
+            const size_t s = SubcellIdx(C, e, d, f, a, b);
+            for (int c = 0; c < 3; ++c) { C.scNv[3 * s + c] = nv[c]; C.scT1[3 * s + c] = t1[c]; C.scT2[3 * s + c] = t2[c]; }
+            C.scNorm[s] = norm;
+          }
+    }
+}
+
+// indicator quantity (SetIndicatorFunction, navierstokes/equation_vars.f90:735-790, mhd/equation_vars.f90:764-808)
+inline double IndicatorQuantity(const Case& C, const double* U) {
+  const int q = C.P.indicator_quantity;
+  const double ke = (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / U[0];
+  double p = C.kappaM1 * (U[4] - 0.5 * ke);
+  if (C.mhd) p = C.kappaM1 * (U[4] - 0.5 * ke - C.s2mu_0 * (U[5] * U[5] + U[6] * U[6] + U[7] * U[7] + U[8] * U[8]));
+  switch (q) {
+    case 1: return U[0];
+    case 2: return p;
+    case 4: return C.mhd ? 0.5 * ke + C.s2mu_0 * (U[5] * U[5] + U[6] * U[6] + U[7] * U[7]) : ke;
+    default: return U[0] * p;
+  }
+}
+
+// CalcBlendingCoefficient (nfvse.f90:1537-1620) with PerssonPeraire_Compute (indicators.f90:108-173)
+// and ProlongBlendingCoeffToFaces (nfvse_mpi.f90:31-58)
+void CalcBlendingCoefficient(Case& C) {
+  const int n = C.np, N = C.N;
+  const size_t nv = (size_t)n * n * n;
+  const orc_params& P = C.P;
+  if (P.compute_alpha == 1) {
+    std::vector<double> Uind(nv), Umod(nv), Vdm(n * n), sVdm(n * n);
+    LegendreVdm(N, C.xGP.data(), Vdm.data(), sVdm.data());
+    const double sharpness = std::log((1.0 - 1.e-4) / 1.e-4);
+    const double threshold = (P.modal_threshold == 2) ? 0.5 * std::pow(10.0, -1.8 * std::pow((double)N, 0.25))
+                                                      : 0.5 * std::pow(10.0, -1.8 * std::pow(N + 1., 0.25));
+    for (int e = 0; e < C.nElems; ++e) {
+      for (size_t z = 0; z < nv; ++z) {
+        double U[NVMAX];
+        for (int v = 0; v < C.nVar; ++v) U[v] = val(C.U[C.nVar * (nv * e + z) + v]);
+        Uind[z] = IndicatorQuantity(C, U);
+      }
+      ChangeBasis3D(1, N, N, sVdm.data(), Uind.data(), Umod.data());
+      double LU = 0., LUM1 = 0., LUM2 = 0.;
+      for (int k = 0; k < n; ++k)
+        for (int j = 0; j < n; ++j)
+          for (int i = 0; i < n; ++i) {
+            const double m2 = Umod[i + n * (j + n * k)] * Umod[i + n * (j + n * k)];
+            LU += m2;
+            if (i < N && j < N && k < N) LUM1 += m2;
+            if (i < N - 1 && j < N - 1 && k < N - 1) LUM2 += m2;
+          }
+      double eta = std::max((LU - LUM1) / LU, (LUM1 - LUM2) / LUM1);
+      if (eta < REALTOL) eta = REALTOL;
+      C.alpha[e] = std::max(P.time_rel_factor * C.alpha[e],
+                            1.0 / (1.0 + std::exp(-sharpness * (eta - threshold) / threshold)));
+    }
+  } else if (P.compute_alpha == 3) {
+    for (int e = 0; e < C.nElems; ++e) C.alpha[e] = P.shock_blend_coef;
+  } else {
+    throw std::runtime_error("ComputeAlpha not implemented in oracle");
+  }
+  for (int e = 0; e < C.nElems; ++e) {
+    if (C.alpha[e] < P.alpha_min) C.alpha[e] = 0.0;
+    else if (C.alpha[e] >= P.alpha_max) C.alpha[e] = P.alpha_max;
+  }
+  if (P.space_prop_sweeps > 0) {  // ProlongBlendingCoeffToFaces
+    for (int s = 0; s < C.nSides; ++s) {
+      C.alphaMaster[s] = C.alpha[C.SideToElem[5 * s] - 1];
+      C.alphaSlave[s] = C.alpha[C.SideToElem[5 * s + 1] - 1];
+    }
+  }
+}
+
+// PropagateBlendingCoeff, nfvse_mpi.f90:62-131 (conforming inner sides)
+void PropagateBlendingCoeff(Case& C) {
+  for (int s = 0; s < C.nSides; ++s) {
+    const double m = C.P.space_prop_factor * std::max(C.alphaMaster[s], C.alphaSlave[s]);
+    const int e = C.SideToElem[5 * s] - 1, nb = C.SideToElem[5 * s + 1] - 1;
+    if (C.alpha[e] < m) C.alpha[e] = m;
+    if (C.alpha[nb] < m) C.alpha[nb] = m;
+  }
+}
+
+// Rotated Riemann flux of one subcell face plane (AdvRiemann, riemann.f90), npts points
+void SubcellRiemann(const Case& C, int npts, const real* UL, const real* UR, const double* nv, const double* t1,
+                    const double* t2, real* F) {
+  const int NV = C.nVar;
+  std::vector<real> L((size_t)NV * npts), R((size_t)NV * npts);
+  for (int z = 0; z < npts; ++z) {
+    const real* a = UL + NV * z;
+    const real* b = UR + NV * z;
+    for (int v = 0; v < NV; ++v) { L[NV * z + v] = a[v]; R[NV * z + v] = b[v]; }
+    for (int o = 1; o <= (C.mhd ? 5 : 1); o += 4) {
+      L[NV * z + o] = a[o] * nv[3 * z] + a[o + 1] * nv[3 * z + 1] + a[o + 2] * nv[3 * z + 2];
+      L[NV * z + o + 1] = a[o] * t1[3 * z] + a[o + 1] * t1[3 * z + 1] + a[o + 2] * t1[3 * z + 2];
+      L[NV * z + o + 2] = a[o] * t2[3 * z] + a[o + 1] * t2[3 * z + 1] + a[o + 2] * t2[3 * z + 2];
+      R[NV * z + o] = b[o] * nv[3 * z] + b[o + 1] * nv[3 * z + 1] + b[o + 2] * nv[3 * z + 2];
+      R[NV * z + o + 1] = b[o] * t1[3 * z] + b[o + 1] * t1[3 * z + 1] + b[o + 2] * t1[3 * z + 2];
+      R[NV * z + o + 2] = b[o] * t2[3 * z] + b[o + 1] * t2[3 * z + 1] + b[o + 2] * t2[3 * z + 2];
+    }
+  }
+  if (C.mhd) {
+    for (int z = 0; z < npts; ++z) MHD_Riemann(C, &L[NV * z], &R[NV * z], F + NV * z);
+  } else {
+    SolveRiemann(C, npts, L.data(), R.data(), F);
+  }
+  for (int z = 0; z < npts; ++z)
+    for (int o = 1; o <= (C.mhd ? 5 : 1); o += 4) {
+      real f2 = F[NV * z + o], f3 = F[NV * z + o + 1], f4 = F[NV * z + o + 2];
+      for (int c = 0; c < 3; ++c)
+        F[NV * z + o + c] = nv[3 * z + c] * f2 + t1[3 * z + c] * f3 + t2[3 * z + c] * f4;
+    }
+}
+
+// VolInt_NFVSE (nfvse.f90:475-565) with Compute_FVFluxes_1st_Order (:566-673) and
+// Compute_FVFluxes_1D (:1389-1447): Ut = (1-alpha) Ut + alpha F_FV on the blended elements
+void VolIntNFVSE(Case& C) {
+  const int n = C.np, N = C.N, NV = C.nVar, npt = n * n;
+  if (C.P.space_prop_sweeps > 0) {
+    PropagateBlendingCoeff(C);
+    for (int sw = 2; sw <= C.P.space_prop_sweeps; ++sw) {
+      for (int s = 0; s < C.nSides; ++s) {
+        C.alphaMaster[s] = C.alpha[C.SideToElem[5 * s] - 1];
+        C.alphaSlave[s] = C.alpha[C.SideToElem[5 * s + 1] - 1];
+      }
+      PropagateBlendingCoeff(C);
+    }
+  }
+  std::vector<double> sW(n);
+  for (int i = 0; i < n; ++i) sW[i] = 1.0 / C.wGP[i];
+  // per direction: left flux FL(x) and right flux FR(x) of subcell face x = -1..N at (a,b)
+  std::vector<real> FL((size_t)3 * (n + 1) * npt * NV), FR((size_t)3 * (n + 1) * npt * NV);
+  std::vector<real> UL((size_t)npt * NV), UR((size_t)npt * NV), F((size_t)npt * NV), G((size_t)npt * NV);
+  std::vector<double> nvb(3 * npt), t1b(3 * npt), t2b(3 * npt);
+  auto fi = [&](int d, int x, int p) { return ((size_t)(d * (n + 1) + (x + 1)) * npt + p) * NV; };
+  for (int e = 0; e < C.nElems; ++e) {
+    if (AlmostEqual(C.alpha[e], 0.0)) continue;
+    std::fill(FL.begin(), FL.end(), real(0.));
+    std::fill(FR.begin(), FR.end(), real(0.));
+    for (int d = 0; d < 3; ++d) {
+      auto node = [&](int x, int a, int b) -> size_t {
+        if (d == 0) return C.nod(x, a, b, e);
+        if (d == 1) return C.nod(a, x, b, e);
+        return C.nod(a, b, x, e);
+      };
+      for (int x = 0; x < N; ++x) {
+        for (int b = 0; b < n; ++b)
+          for (int a = 0; a < n; ++a) {
+            const int p = a + n * b;
+            for (int v = 0; v < NV; ++v) {
+              UL[NV * p + v] = C.U[NV * node(x, a, b) + v];
+              UR[NV * p + v] = C.U[NV * node(x + 1, a, b) + v];
+            }
+            const size_t s = SubcellIdx(C, e, d, x, a, b);
+            for (int c = 0; c < 3; ++c) {
+              nvb[3 * p + c] = C.scNv[3 * s + c]; t1b[3 * p + c] = C.scT1[3 * s + c]; t2b[3 * p + c] = C.scT2[3 * s + c];
+            }
+          }
+        SubcellRiemann(C, npt, UL.data(), UR.data(), nvb.data(), t1b.data(), t2b.data(), F.data());
+        for (size_t z = 0; z < F.size(); ++z) G[z] = F[z];  // FR_ = F_ before the non-conservative terms
+        if (C.mhd && C.noncons) {
+          for (int p = 0; p < npt; ++p) {
+            MHD_NonConsSurf(C, &UR[NV * p], &UL[NV * p], &nvb[3 * p], &F[NV * p]);  // left flux of node x+1
+            MHD_NonConsSurf(C, &UL[NV * p], &UR[NV * p], &nvb[3 * p], &G[NV * p]);  // right flux of node x
+          }
+        }
+        for (int b = 0; b < n; ++b)
+          for (int a = 0; a < n; ++a) {
+            const int p = a + n * b;
+            const double nrm = C.scNorm[SubcellIdx(C, e, d, x, a, b)];
+            for (int v = 0; v < NV; ++v) {
+              FL[fi(d, x, p) + v] = F[NV * p + v] * nrm;
+              FR[fi(d, x, p) + v] = (C.mhd && C.noncons) ? G[NV * p + v] * nrm : F[NV * p + v] * nrm;
+            }
+          }
+      }
+    }
+    const double al = C.alpha[e];
+    for (int k = 0; k < n; ++k)
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i)
+          for (int v = 0; v < NV; ++v) {
+            real ffv = sW[i] * (FR[fi(0, i, j + n * k) + v] - FL[fi(0, i - 1, j + n * k) + v]) +
+                       sW[j] * (FR[fi(1, j, i + n * k) + v] - FL[fi(1, j - 1, i + n * k) + v]) +
+                       sW[k] * (FR[fi(2, k, i + n * j) + v] - FL[fi(2, k - 1, i + n * j) + v]);
+            real& ut = C.Ut[C.vol(v, i, j, k, e)];
+            ut = (1. - al) * ut + al * ffv;
+          }
+  }
+}

@@ -58,6 +58,16 @@ class OrcParams(ctypes.Structure):
         ("mhd_ref_state", (ctypes.c_double * 8) * 2),
         ("ini_center", ctypes.c_double * 3),
         ("ini_halfwidth", ctypes.c_double),
+        ("nfvse", ctypes.c_int),
+        ("compute_alpha", ctypes.c_int),
+        ("shock_blend_coef", ctypes.c_double),
+        ("modal_threshold", ctypes.c_int),
+        ("alpha_max", ctypes.c_double),
+        ("alpha_min", ctypes.c_double),
+        ("space_prop_factor", ctypes.c_double),
+        ("space_prop_sweeps", ctypes.c_int),
+        ("time_rel_factor", ctypes.c_double),
+        ("indicator_quantity", ctypes.c_int),
     ]
 
 
@@ -71,6 +81,8 @@ DEFAULTS = dict(
     mu_0=1.0, eta=0.0, glm_scale=0.5, glm_scr=0.0, glm_ch=0.0, noncons=1, nc_glm=0,
     mhd_ref_state=((1.0, 0.0, 0.0, 0.0, 1.0, 1.0, 0.0, 0.0), (1.0, 0.0, 0.0, 0.0, 1.0, 1.0, 0.0, 0.0)),
     ini_center=(0.0, 0.0, 0.0), ini_halfwidth=0.1,
+    nfvse=0, compute_alpha=1, shock_blend_coef=0.0, modal_threshold=1, alpha_max=0.5, alpha_min=0.01,
+    space_prop_factor=0.5, space_prop_sweeps=1, time_rel_factor=0.0, indicator_quantity=3,
 )
 
 
@@ -118,6 +130,7 @@ def _lib(counting=False):
     lib.orc_riemann_point.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 6
     lib.orc_ln_mean.restype = d
     lib.orc_ln_mean.argtypes = [d, d]
+    lib.orc_get_alpha.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     lib.orc_set_glm_ch.argtypes = [ctypes.c_void_p, d]
     lib.orc_get_glm_ch.restype = d
     lib.orc_get_glm_ch.argtypes = [ctypes.c_void_p]
@@ -250,6 +263,12 @@ class OracleCase:
         self.lib.orc_exact_func(self.h, func, t, x.shape[0], _ptr(x), _ptr(U))
         return U
 
+    def alpha(self):
+        """NFVSE blending coefficient per element after the last right-hand side."""
+        a = np.zeros(self.nElems)
+        self.lib.orc_get_alpha(self.h, _ptr(a))
+        return a
+
     @property
     def glm_ch(self):
         return self.lib.orc_get_glm_ch(self.h)
@@ -283,7 +302,8 @@ def basis(N):
     return out
 
 
-PHASES = ("volume_split_form", "lifting", "volume_viscous", "face_flux", "surface_integral", "jacobian_source")
+PHASES = ("volume_split_form", "lifting", "volume_viscous", "face_flux", "surface_integral", "jacobian_source",
+          "nfvse")
 
 
 def count_flops(**kw):
