@@ -58,6 +58,16 @@ class FluxoCfg(ctypes.Structure):
         ("glm_scr", ctypes.c_double),
         ("noncons", ctypes.c_int),
         ("nc_glm", ctypes.c_int),
+        ("nfvse", ctypes.c_int),
+        ("compute_alpha", ctypes.c_int),
+        ("shock_blend_coef", ctypes.c_double),
+        ("modal_threshold", ctypes.c_int),
+        ("alpha_max", ctypes.c_double),
+        ("alpha_min", ctypes.c_double),
+        ("space_prop_factor", ctypes.c_double),
+        ("space_prop_sweeps", ctypes.c_int),
+        ("time_rel_factor", ctypes.c_double),
+        ("indicator_quantity", ctypes.c_int),
     ]
 
 
@@ -67,7 +77,7 @@ EXPORTS = [
     "fluxo_gpu_time_disc", "fluxo_gpu_device_buffers", "fluxo_gpu_launch_count", "fluxo_gpu_destroy",
     "fluxo_gpu_last_error", "fluxo_gpu_set_profiling", "fluxo_gpu_get_profile", "fluxo_gpu_fp64_peak",
     "fluxo_host_box_sizes", "fluxo_host_box_mesh", "fluxo_host_exact_func", "fluxo_gpu_dg_time_derivative_noalloc",
-    "fluxo_gpu_set_glm_ch", "fluxo_gpu_get_glm_ch",
+    "fluxo_gpu_set_glm_ch", "fluxo_gpu_get_glm_ch", "fluxo_gpu_get_alpha",
 ]
 
 # FLUXO_NOALLOC_SCRATCH_BYTES of fluxo_gpu.h: the static scratch of fluxo_gpu_dg_time_derivative_noalloc
@@ -108,6 +118,7 @@ def load():
     lib.fluxo_gpu_dg_time_derivative_noalloc.argtypes = [P(FluxoCfg), i, i] + [vp] * 8
     lib.fluxo_gpu_set_glm_ch.argtypes = [vp, d]
     lib.fluxo_gpu_get_glm_ch.argtypes = [vp, P(d)]
+    lib.fluxo_gpu_get_alpha.argtypes = [vp, vp]
     for name in EXPORTS:
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib

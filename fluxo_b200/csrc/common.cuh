@@ -78,6 +78,17 @@ struct KParams {
   int parabolic;          // resistive / viscous MHD (lifting + viscous fluxes)
   double glmCh;           // GLM_ch of this RHS (host value) ...
   const double* chDev;    // ... or from device memory (time_disc loop)
+  // NFVSE shock capturing (shockcapturing/nfvse.f90): blending of the volume integral with the
+  // first-order subcell finite-volume one on the elements whose alpha > 2*EPSILON
+  int nfvse;
+  double* alpha;          // [elem] blending coefficient after propagation (kept for TimeRelFactor)
+  double* alphaRaw;       // [elem] before propagation
+  int* blendList;         // [elem] blended elements of this RHS, count in *blendCount
+  int* blendCount;
+  double* fv;             // [elem][var][node] alpha * F_FV of the blended elements
+  const double* sVdm;     // nodal -> modal Legendre coefficients [m][i]
+  int computeAlpha, indicatorQuantity, propSweeps;
+  double threshold, sharpness, alphaMax, alphaMin, propFactor, timeRelFactor, shockBlendCoef;
 };
 
 __device__ __forceinline__ bool halted(const KParams& P) { return P.haltFlag && *P.haltFlag != 0; }

@@ -82,6 +82,10 @@ struct fluxo_handle {
   int nVar = 5;                     // 5 (Euler / Navier-Stokes), 9 (MHD + GLM)
   bool mhd = false;
   double glmCh = 0., glmDtch1 = 0.;  // MHD: GLM_ch, GLM_dtch1 (from the metrics at set_mesh)
+  // NFVSE: blending coefficients, list of blended elements, alpha * F_FV, modal transform
+  double *dAlpha = nullptr, *dAlphaRaw = nullptr, *dAlphaTmp = nullptr, *dFV = nullptr, *dSVdm = nullptr;
+  int *dBlendList = nullptr, *dBlendCount = nullptr;
+  int nSMs = 148;
   bool visc = false, meshSet = false, stateSet = false, haveXGP = false;
   cudaStream_t stream = nullptr;
   BasisTables hb{};
@@ -99,7 +103,7 @@ struct fluxo_handle {
   uint64_t launches = 0;
   std::string lastError;
   bool profiling = false;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof[5];
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof[6];
 };
 
 namespace {
@@ -207,6 +211,17 @@ KParams base_params(fluxo_handle* h) {
     P.noncons = c.noncons; P.ncGLM = c.nc_glm; P.parabolic = h->visc ? 1 : 0;
     P.mu0 = 0.; P.visc = 0;
   }
+  if (c.nfvse) {  // InitNFVSE, nfvse.f90:106-260; sharpness nfvse_vars.f90:74
+    P.nfvse = 1;
+    P.alpha = h->dAlpha; P.alphaRaw = h->dAlphaRaw; P.blendList = h->dBlendList; P.blendCount = h->dBlendCount;
+    P.fv = h->dFV; P.sVdm = h->dSVdm;
+    P.computeAlpha = c.compute_alpha; P.indicatorQuantity = c.indicator_quantity; P.propSweeps = c.space_prop_sweeps;
+    P.threshold = (c.modal_threshold == 2) ? 0.5 * std::pow(10.0, -1.8 * std::pow((double)h->N, 0.25))
+                                           : 0.5 * std::pow(10.0, -1.8 * std::pow(h->N + 1., 0.25));
+    P.sharpness = std::log((1.0 - 1.e-4) / 1.e-4);
+    P.alphaMax = c.alpha_max; P.alphaMin = c.alpha_min; P.propFactor = c.space_prop_factor;
+    P.timeRelFactor = c.time_rel_factor; P.shockBlendCoef = c.shock_blend_coef;
+  }
   return P;
 }
 
@@ -234,6 +249,12 @@ struct ProfScope {
 int rhs(fluxo_handle* h, KParams P) {
   cudaStream_t s = h->stream;
   if (h->mhd) {
+    if (h->cfg.nfvse) {  // CalcBlendingCoefficient (dg.f90:358-361) and VolInt_NFVSE's FV part (:380-383)
+      ProfScope ps(h, 5);
+      FLUXO_CUDA(h, launch_nfvse_alpha(h->NP, true, h->nElems, s, P, h->dAlphaTmp));
+      FLUXO_CUDA(h, launch_nfvse_fv(h->cfg.riemann, h->NP, h->nElems, h->nSMs, s, P));
+      h->launches += 3 + (h->cfg.space_prop_sweeps > 1 ? 2 * (h->cfg.space_prop_sweeps - 1) : 0);
+    }
     if (h->visc) {
       {
         ProfScope ps(h, 0);
@@ -350,6 +371,15 @@ int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {
     if (!volume_flux_supported(cfg->volume_flux))
       return fail(nullptr, FLUXO_EINVAL_CFG, "volume flux not implemented");
   }
+  if (cfg->nfvse) {  // InitShockCapturing / InitNFVSE checks (shockcapturing.f90:82-112, nfvse.f90:120-170)
+    if (!mhd) return fail(nullptr, FLUXO_EINVAL_CFG, "NFVSE is implemented for the MHD equations");
+    if (cfg->N < 2) return fail(nullptr, FLUXO_EINVAL_CFG, "NFVSE needs N >= 2");
+    if (cfg->compute_alpha != 1 && cfg->compute_alpha != 3)
+      return fail(nullptr, FLUXO_EINVAL_CFG, "ComputeAlpha must be 1 (indicator) or 3 (fixed)");
+    if (cfg->indicator_quantity < 1 || cfg->indicator_quantity > 4)
+      return fail(nullptr, FLUXO_EINVAL_CFG, "ShockIndicatorQuantity must be 1..4");
+    if (cfg->space_prop_sweeps < 0) return fail(nullptr, FLUXO_EINVAL_CFG, "SpacePropSweeps must be >= 0");
+  }
   if (parabolic) {
     if (cfg->lifting != 1 && cfg->lifting != 2) return fail(nullptr, FLUXO_EINVAL_CFG, "lifting must be BR1 or BR2");
     if (cfg->lifting_var < 1 || cfg->lifting_var > 3) return fail(nullptr, FLUXO_EINVAL_CFG, "lifting_var must be 1..3");
@@ -402,10 +432,20 @@ int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {
     return fail(nullptr, FLUXO_ECUDA, m);
   }
   build_basis_tables(h->N, h->hb);
-  if (dalloc(h, &h->dBasis, 1) || dalloc(h, &h->dTD, 1) || dalloc(h, &h->dDtBits, 1) || dalloc(h, &h->dErrKey, 1)) {
+  cudaDeviceGetAttribute(&h->nSMs, cudaDevAttrMultiProcessorCount, cfg->device);
+  if (dalloc(h, &h->dBasis, 1) || dalloc(h, &h->dTD, 1) || dalloc(h, &h->dDtBits, 1) || dalloc(h, &h->dErrKey, 1) ||
+      (cfg->nfvse && (dalloc(h, &h->dSVdm, (size_t)h->NP * h->NP) || dalloc(h, &h->dBlendCount, 1)))) {
     std::string m = h->lastError;
     fluxo_gpu_destroy(h);
     return fail(nullptr, FLUXO_ENOMEM_HBM, m);
+  }
+  if (cfg->nfvse) {  // sVdm_Leg of BuildLegendreVdm (basis.f90:196-251), indicators.f90:176-197
+    std::vector<double> sv = host::legendre_modal(h->N);
+    e = cudaMemcpy(h->dSVdm, sv.data(), sv.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      fluxo_gpu_destroy(h);
+      return fail(nullptr, FLUXO_ECUDA, cudaGetErrorString(e));
+    }
   }
   e = cudaMemcpy(h->dBasis, &h->hb, sizeof(BasisTables), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) {
@@ -493,6 +533,13 @@ int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* S2E, 
       dtch1 = std::min(dtch1, h->CFLScale * 2. / (ml[0] + ml[1] + ml[2]));
     }
     h->glmDtch1 = dtch1;
+  }
+  if (h->cfg.nfvse) {
+    if ((r = dalloc(h, &h->dAlpha, (size_t)nElems)) || (r = dalloc(h, &h->dAlphaRaw, (size_t)nElems)) ||
+        (r = dalloc(h, &h->dAlphaTmp, (size_t)nElems)) || (r = dalloc(h, &h->dBlendList, (size_t)nElems)) ||
+        (r = dalloc(h, &h->dFV, nU)))
+      return r;
+    FLUXO_CUDA(h, cudaMemsetAsync(h->dAlpha, 0, (size_t)nElems * sizeof(double), h->stream));
   }
   cudaStream_t s = h->stream;
   FLUXO_CUDA(h, cudaMemcpyAsync(h->dMetrics, met.data(), met.size() * 8, cudaMemcpyHostToDevice, s));
@@ -659,6 +706,16 @@ int fluxo_gpu_get_glm_ch(fluxo_handle* h, double* ch) {
   return FLUXO_OK;
 }
 
+int fluxo_gpu_get_alpha(fluxo_handle* h, double* alpha) {
+  int r = check_ready(h);
+  if (r) return r;
+  if (!alpha) return FLUXO_EINVAL_CFG;
+  if (!h->cfg.nfvse) return fail(h, FLUXO_EINVAL_CFG, "NFVSE is off");
+  FLUXO_CUDA(h, cudaMemcpyAsync(alpha, h->dAlpha, (size_t)h->nElems * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
+  return FLUXO_OK;
+}
+
 int fluxo_gpu_device_buffers(fluxo_handle* h, double** dU, double** dUt, void** stream) {
   if (!h) return FLUXO_EINVAL_CFG;
   if (dU) *dU = h->dU;
@@ -681,7 +738,7 @@ int fluxo_gpu_set_profiling(fluxo_handle* h, int enable) {
 }
 
 int fluxo_gpu_get_profile(fluxo_handle* h, int kind, double* total_ms, uint64_t* count) {
-  if (!h || kind < 0 || kind > 4) return FLUXO_EINVAL_CFG;
+  if (!h || kind < 0 || kind > 5) return FLUXO_EINVAL_CFG;
   FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
   double tot = 0.;
   for (auto& pr : h->prof[kind]) {
@@ -731,14 +788,15 @@ int fluxo_gpu_fp64_peak(int device, double* tflops) {
 
 int fluxo_gpu_destroy(fluxo_handle* h) {
   if (!h) return FLUXO_OK;
-  for (int k = 0; k < 5; ++k) {
+  for (int k = 0; k < 6; ++k) {
     for (auto& pr : h->prof[k]) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
     h->prof[k].clear();
   }
   cudaSetDevice(h->cfg.device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   void* ptrs[] = {h->dBasis, h->dU, h->dUt, h->dUtTmp, h->dGrad, h->dUtVisc, h->dMetrics, h->dsJ, h->dFaceGeo, h->dXGP,
-                  h->dFlux, h->dLFlux, h->dGTrace, h->dS2E, h->dE2S, h->dTD, h->dDtBits, h->dErrKey};
+                  h->dFlux, h->dLFlux, h->dGTrace, h->dS2E, h->dE2S, h->dTD, h->dDtBits, h->dErrKey,
+                  h->dAlpha, h->dAlphaRaw, h->dAlphaTmp, h->dFV, h->dSVdm, h->dBlendList, h->dBlendCount};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);

@@ -145,6 +145,26 @@ inline std::vector<double> modal_projection(const std::vector<double>& xin, cons
   return V;
 }
 
+// Nodal -> modal transform onto the orthonormal Legendre polynomials sqrt(m+1/2) P_m on the LGL
+// nodes of degree N (sVdm_Leg of BuildLegendreVdm, basis.f90:196-251): c_m = sum_i S[m*(N+1)+i] u_i,
+// the L2 projection with 3N/2+2 Gauss points.
+inline std::vector<double> legendre_modal(int N) {
+  std::vector<double> x, w, xg, wg;
+  lgl(N, x, w);
+  gauss(3 * N / 2 + 1, xg, wg);
+  std::vector<double> Vg = interp_matrix(x, xg);  // L_i(x_g) at [g*(N+1)+i]
+  const int n = N + 1;
+  std::vector<double> S((size_t)n * n, 0.);
+  for (int m = 0; m < n; ++m)
+    for (size_t g = 0; g < xg.size(); ++g) {
+      double P, dP;
+      legendre(m, xg[g], P, dP);
+      const double f = std::sqrt(m + 0.5) * P * wg[g];
+      for (int i = 0; i < n; ++i) S[(size_t)m * n + i] += f * Vg[g * n + i];
+    }
+  return S;
+}
+
 struct LGLBasis {
   int N;
   std::vector<double> x, w, D, Dhat, Dvs;

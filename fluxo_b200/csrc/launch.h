@@ -44,6 +44,11 @@ cudaError_t launch_mhd_volume_std(int NP, int VF, int nElems, cudaStream_t s, co
 cudaError_t launch_mhd_timestep(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P,
                                 unsigned long long* dtBits, int* errKey);
 
+// NFVSE shock capturing: blending coefficient (indicator + propagation + list of blended elements;
+// `scratch` holds nElems doubles for sweeps > 1) and the subcell FV volume integral of MHD.
+cudaError_t launch_nfvse_alpha(int NP, bool mhd, int nElems, cudaStream_t s, const KParams& P, double* scratch);
+cudaError_t launch_nfvse_fv(int RS, int NP, int nElems, int nSMs, cudaStream_t s, const KParams& P);
+
 // Host helpers of fluxo_gpu.cu for entry points without a handle: the per-N operator tables, and
 // the message that fluxo_gpu_last_error(NULL, ...) returns (returns `code`).
 void basis_tables_for(int N, BasisTables& B);

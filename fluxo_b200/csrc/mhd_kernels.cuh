@@ -430,6 +430,14 @@ __global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, FLUXO_MHD_VOL_MINB) 
     if (NC == 1 || NC == 3) { ut[5] += h * v0; ut[6] += h * v1; ut[7] += h * v2; }
     if (NCGLM) { ut[4] += u[8] * ncGLM; ut[8] += ncGLM; }
   }
+  if (P.nfvse) {  // VolInt_NFVSE (nfvse.f90:475-565): blend with alpha * F_FV of the FV kernel
+    const double a = P.alpha[e];
+    if (a > 4.440892098500626e-16) {
+      const double* FV = P.fv + (size_t)e * NV * NP3 + t;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) ut[v] = (1. - a) * ut[v] + FV[v * NP3];
+    }
+  }
   if (P.parabolic) {  // viscous / resistive volume integral of variables 2..8 (lifting kernel)
     const double* V = P.utvisc + (size_t)e * 7 * NP3 + t;
 #pragma unroll

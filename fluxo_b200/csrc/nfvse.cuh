@@ -1,0 +1,261 @@
+// NFVSE shock capturing (shockcapturing/nfvse.f90, nfvse_mpi.f90, indicators/indicators.f90) on
+// the sm_100a path, LGL nodes, first-order subcell finite volumes (SubFVMethod = 1):
+//   alpha_kernel      Persson-Peraire indicator of rho*p (or rho, p, kinetic energy) from its modal
+//                     Legendre coefficients, alpha = 1/(1+exp(-s (eta-T)/T)), clipping;
+//   propagate_kernel  alpha_e = max(alpha_e, SpacePropFactor * max over its sides of the two
+//                     element values) and the list of blended elements (alpha > 2*EPSILON);
+//   fv_kernel_mhd     per blended element: first-order subcell FV volume integral with sub-cell
+//                     metrics built from the element's metrics on the fly (nfvse.f90:261-378),
+//                     the Riemann solver of the face kernel and the non-conservative terms,
+//                     written as alpha * F_FV for the volume kernel to blend with.
+#pragma once
+#include "common.cuh"
+#include "kernels.cuh"
+#include "mhd_kernels.cuh"
+#include "physics_mhd.cuh"
+
+namespace fluxo {
+namespace nfvse {
+
+constexpr double kTiny = 2. * 2.220446049250313e-16;  // ALMOSTEQUAL(alpha, 0), basis.f90:673-690
+
+// indicator quantity (SetIndicatorFunction, navierstokes/equation_vars.f90:735-790, mhd/equation_vars.f90:764-808)
+template <int NV>
+__device__ __forceinline__ double indicator_quantity(const KParams& P, const double* U) {
+  const double ke = (U[1] * U[1] + U[2] * U[2] + U[3] * U[3]) / U[0];
+  double p;
+  if constexpr (NV == 9)
+    p = P.kappaM1 * (U[4] - 0.5 * ke - P.s2mu_0 * (U[5] * U[5] + U[6] * U[6] + U[7] * U[7] + U[8] * U[8]));
+  else
+    p = P.kappaM1 * (U[4] - 0.5 * ke);
+  switch (P.indicatorQuantity) {
+    case 1: return U[0];
+    case 2: return p;
+    case 4:
+      if constexpr (NV == 9) return 0.5 * ke + P.s2mu_0 * (U[5] * U[5] + U[6] * U[6] + U[7] * U[7]);
+      else return ke;
+    default: return U[0] * p;
+  }
+}
+
+// CalcBlendingCoefficient (nfvse.f90:1537-1620) with PerssonPeraire_Compute (indicators.f90:108-173);
+// EPB elements per block, one thread per node; the modal energies are summed by one thread per
+// element in node order, so the result does not depend on thread scheduling
+template <int NP, int NV>
+__global__ void __launch_bounds__(512) alpha_kernel(KParams P) {
+  if (halted(P)) return;
+  constexpr int NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1;
+  constexpr int EPB = (256 / NP3) > 0 ? (256 / NP3) : 1;
+  __shared__ double sV[NPT];
+  __shared__ double sA[EPB][NP3], sB[EPB][NP3];
+  const int eb = threadIdx.x / NP3, t = threadIdx.x - eb * NP3;
+  const int e = blockIdx.x * EPB + eb;
+  const bool valid = e < P.nElems;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *P.blendCount = 0;  // the list kernels run after this one
+  for (int z = threadIdx.x; z < NPT; z += blockDim.x) sV[z] = P.sVdm[z];
+  const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
+  if (valid) {
+    double U[NV];
+    const double* Ug = P.U + NV * ((size_t)e * NP3 + t);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) U[v] = Ug[v];
+    sA[eb][t] = indicator_quantity<NV>(P, U);
+  }
+  __syncthreads();
+  // modal coefficients Umod(m1,m2,m3) = sum sVdm(m1,i) sVdm(m2,j) sVdm(m3,k) Uind(i,j,k), one index at a time
+  if (valid) {
+    double s = 0.;
+    for (int l = 0; l < NP; ++l) s += sV[i * NP + l] * sA[eb][l + NP * (j + NP * k)];
+    sB[eb][t] = s;
+  }
+  __syncthreads();
+  if (valid) {
+    double s = 0.;
+    for (int l = 0; l < NP; ++l) s += sV[j * NP + l] * sB[eb][i + NP * (l + NP * k)];
+    sA[eb][t] = s;
+  }
+  __syncthreads();
+  if (valid) {
+    double s = 0.;
+    for (int l = 0; l < NP; ++l) s += sV[k * NP + l] * sA[eb][i + NP * (j + NP * l)];
+    sB[eb][t] = s * s;
+  }
+  __syncthreads();
+  if (!valid || t != 0) return;
+  double a;
+  if (P.computeAlpha == 1) {
+    double LU = 0., LUM1 = 0., LUM2 = 0.;
+    for (int z = 0; z < NP3; ++z) {
+      const int zi = z % NP, zj = (z / NP) % NP, zk = z / NPT;
+      const double m2 = sB[eb][z];
+      LU += m2;
+      if (zi < N && zj < N && zk < N) LUM1 += m2;
+      if (zi < N - 1 && zj < N - 1 && zk < N - 1) LUM2 += m2;
+    }
+    double eta = fmax((LU - LUM1) / LU, (LUM1 - LUM2) / LUM1);
+    if (eta < 2.220446049250313e-16) eta = 2.220446049250313e-16;
+    a = fmax(P.timeRelFactor * P.alpha[e], 1.0 / (1.0 + exp(-P.sharpness * (eta - P.threshold) / P.threshold)));
+  } else {
+    a = P.shockBlendCoef;
+  }
+  if (a < P.alphaMin) a = 0.0;
+  else if (a >= P.alphaMax) a = P.alphaMax;
+  P.alphaRaw[e] = a;
+}
+
+// PropagateBlendingCoeff (nfvse_mpi.f90:62-131) for one sweep from `src` into alpha; the last
+// sweep also lists the blended elements
+__global__ void propagate_kernel(KParams P, const double* src, bool last) {
+  if (halted(P)) return;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= P.nElems) return;
+  double a = src[e];
+  for (int ls = 0; ls < 6; ++ls) {
+    const int s = P.e2s[2 * (6 * e + ls)];
+    const double m = P.propFactor * fmax(src[P.s2e[5 * s]], src[P.s2e[5 * s + 1]]);
+    if (a < m) a = m;
+  }
+  P.alpha[e] = a;
+  if (last && a > kTiny) P.blendList[atomicAdd(P.blendCount, 1)] = e;
+}
+
+// no propagation (SpacePropSweeps = 0): alpha = raw value, list the blended elements
+__global__ void list_kernel(KParams P) {
+  if (halted(P)) return;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= P.nElems) return;
+  const double a = P.alphaRaw[e];
+  P.alpha[e] = a;
+  if (a > kTiny) P.blendList[atomicAdd(P.blendCount, 1)] = e;
+}
+
+template <int NP>
+__host__ __device__ constexpr size_t fv_smem_bytes() {
+  return sizeof(double) * (size_t)(NP * NP + 2 * NP + 27 * NP * NP * NP);
+}
+
+// First-order subcell FV volume integral (Compute_FVFluxes_1st_Order nfvse.f90:566-673,
+// Compute_FVFluxes_1D :1389-1447) of the MHD equations on the listed elements: one element per
+// block iteration, one thread per node.  Per direction each node evaluates the flux on its right
+// subcell face (x, x+1), keeps its own share (with its own non-conservative part) and hands the
+// right neighbour's share over in shared memory.  F_FV(x) = (FR(x) - FL(x-1)) / w_x.
+template <int NP, int RS>
+__global__ void __launch_bounds__(NP * NP * NP) fv_kernel_mhd(KParams P) {
+  if (halted(P)) return;
+  constexpr int NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1, NV = 9;
+  extern __shared__ double smem[];
+  double* sD = smem;          // D(l,m) at [l*NP+m]
+  double* sW = sD + NPT;      // wGP
+  double* sIW = sW + NP;      // 1/wGP
+  double* sU = sIW + NP;      // [node][9] state
+  double* sM = sU + 9 * NP3;  // [9][node] metrics
+  double* sA = sM + 9 * NP3;  // [node][9] left-face flux handed over by the left neighbour
+  const int t = threadIdx.x;
+  for (int z = t; z < NPT; z += blockDim.x) sD[z] = P.basis->D[z];
+  if (t < NP) { sW[t] = P.basis->wGP[t]; sIW[t] = 1.0 / P.basis->wGP[t]; }
+  const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
+  const double ch = glm_ch(P);
+  const int count = *P.blendCount;
+  for (int li = blockIdx.x; li < count; li += gridDim.x) {
+    const int e = P.blendList[li];
+    __syncthreads();  // the previous element is done with the shared arrays
+    {
+      const double* Ug = P.U + NV * ((size_t)e * NP3 + t);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) sU[NV * t + v] = Ug[v];
+      const double* Mg = P.metrics + (size_t)e * 9 * NP3 + t;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) sM[c * NP3 + t] = Mg[c * NP3];
+    }
+    __syncthreads();
+    double ffv[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) ffv[v] = 0.;
+#pragma unroll 1
+    for (int dir = 0; dir < 3; ++dir) {
+      const int x = dir == 0 ? i : (dir == 1 ? j : k);
+      const int stride = dir == 0 ? 1 : (dir == 1 ? NP : NPT);
+      const int n0 = t - x * stride;  // node at position 0 of this node's line
+      if (x < N) {
+        // sub-cell metrics of face x (nfvse.f90:261-378): nv from Ja^dir, t1 from Ja^(dir+1)
+        const double* Mn = sM + (3 * dir) * NP3;
+        const double* Mt = sM + (3 * ((dir + 1) % 3)) * NP3;
+        double nv[3], t1[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { nv[c] = Mn[c * NP3 + n0]; t1[c] = Mt[c * NP3 + n0]; }
+        for (int m = 0; m < NP; ++m)
+          for (int l = 0; l <= x; ++l) {
+            const double wd = sW[l] * sD[l * NP + m];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              nv[c] += wd * Mn[c * NP3 + n0 + m * stride];
+              t1[c] += wd * Mt[c * NP3 + n0 + m * stride];
+            }
+          }
+        const double norm = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) nv[c] = nv[c] / norm;
+        const double tn = t1[0] * nv[0] + t1[1] * nv[1] + t1[2] * nv[2];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) t1[c] = t1[c] - tn * nv[c];
+        const double tl = sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) t1[c] = t1[c] / tl;
+        const double t2[3] = {nv[1] * t1[2] - nv[2] * t1[1], nv[2] * t1[0] - nv[0] * t1[2],
+                              nv[0] * t1[1] - nv[1] * t1[0]};
+        const double* uL = sU + NV * t;
+        const double* uR = sU + NV * (t + stride);
+        double L[NV], R[NV], F[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) { L[v] = uL[v]; R[v] = uR[v]; }
+#pragma unroll
+        for (int b = 1; b <= 5; b += 4) {  // RotateState, mhd/riemann.f90:185-200
+          L[b] = uL[b] * nv[0] + uL[b + 1] * nv[1] + uL[b + 2] * nv[2];
+          L[b + 1] = uL[b] * t1[0] + uL[b + 1] * t1[1] + uL[b + 2] * t1[2];
+          L[b + 2] = uL[b] * t2[0] + uL[b + 1] * t2[1] + uL[b + 2] * t2[2];
+          R[b] = uR[b] * nv[0] + uR[b + 1] * nv[1] + uR[b + 2] * nv[2];
+          R[b + 1] = uR[b] * t1[0] + uR[b + 1] * t1[1] + uR[b + 2] * t1[2];
+          R[b + 2] = uR[b] * t2[0] + uR[b + 1] * t2[1] + uR[b + 2] * t2[2];
+        }
+        mhd::riemann<RS>(P, ch, L, R, F);
+#pragma unroll
+        for (int b = 1; b <= 5; b += 4) {  // RotateFluxBack, mhd/riemann.f90:204-217
+          const double f2 = F[b], f3 = F[b + 1], f4 = F[b + 2];
+          F[b] = nv[0] * f2 + t1[0] * f3 + t2[0] * f4;
+          F[b + 1] = nv[1] * f2 + t1[1] * f3 + t2[1] * f4;
+          F[b + 2] = nv[2] * f2 + t1[2] * f3 + t2[2] * f4;
+        }
+        double FR[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) FR[v] = F[v];
+        if (P.noncons != 0) {  // AddNonConsFlux on both nodes of the face (Compute_FVFluxes_1D :1420-1436)
+          const bool ncg = P.ncGLM != 0;
+          const double Bn = 0.5 * ((uL[5] + uR[5]) * nv[0] + (uL[6] + uR[6]) * nv[1] + (uL[7] + uR[7]) * nv[2]);
+          const double ps = 0.5 * (uL[8] + uR[8]);
+          const double nq[3] = {ps * nv[0], ps * nv[1], ps * nv[2]};
+          mhd::add_noncons_surface(P.noncons, ncg, uR, Bn, nq, F);
+          mhd::add_noncons_surface(P.noncons, ncg, uL, Bn, nq, FR);
+        }
+        double* A = sA + NV * (t + stride);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          A[v] = F[v] * norm;
+          ffv[v] += sIW[x] * (FR[v] * norm);
+        }
+      }
+      __syncthreads();
+      if (x > 0) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) ffv[v] -= sIW[x] * sA[NV * t + v];
+      }
+      __syncthreads();
+    }
+    const double a = P.alpha[e];
+    double* O = P.fv + (size_t)e * NV * NP3 + t;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) O[v * NP3] = a * ffv[v];
+  }
+}
+
+}  // namespace nfvse
+}  // namespace fluxo

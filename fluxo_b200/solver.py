@@ -29,7 +29,10 @@ def make_cfg(**fields):
     defaults = dict(N=3, eqn=0, riemann=1, volume_flux=0, lifting=1, lifting_var=3, visc=0, kappa=1.4, R=287.058,
                     Pr=0.72, mu0=0.0, Ts=110.4, Tref=280.0, ExpoSuth=1.5, ExpoPow=0.0, etaBR2=2.0, time_disc=0,
                     cfl_scale=0.9, dfl_scale=0.4, ini_exact_func=1, ini_frequency=1.0, ini_amplitude=0.1, device=0,
-                    mu_0=1.0, eta=0.0, glm_scale=0.5, glm_scr=0.0, noncons=1, nc_glm=0)
+                    mu_0=1.0, eta=0.0, glm_scale=0.5, glm_scr=0.0, noncons=1, nc_glm=0,
+                    nfvse=0, compute_alpha=1, shock_blend_coef=0.0, modal_threshold=1, alpha_max=0.5,
+                    alpha_min=0.01, space_prop_factor=0.5, space_prop_sweeps=1, time_rel_factor=0.0,
+                    indicator_quantity=3)
     defaults.update(fields)
     for k, v in defaults.items():
         setattr(cfg, k, v)
@@ -127,6 +130,12 @@ class DGOperator:
     @glm_ch.setter
     def glm_ch(self, ch):
         self._check(self.lib.fluxo_gpu_set_glm_ch(self.h, float(ch)))
+
+    def alpha(self):
+        """NFVSE blending coefficients of the last right-hand side (one per element)."""
+        a = np.empty(self.nElems)
+        self._check(self.lib.fluxo_gpu_get_alpha(self.h, _ptr(a)))
+        return a
 
     def set_state(self, U):
         U = _c(U)

@@ -73,6 +73,17 @@ typedef struct fluxo_cfg {
   double glm_scr;    /* GLM_scr: damping Ut(9) -= GLM_scr*GLM_ch*U(9) (equation.f90:1698-1706) */
   int noncons;       /* NONCONS: 0 off, 1 Powell, 2 Brackbill, 3 Janhunen (CMake FLUXO_EQN_NONCONS_TYPE) */
   int nc_glm;        /* PP_NC_GLM: non-conservative GLM terms (CMake FLUXO_EQN_NONCONS_GLM) */
+  /* NFVSE shock capturing (CMake FLUXO_SHOCKCAP_NFVSE; src/shockcapturing/nfvse.f90:63-260), MHD,
+   * N >= 2, SubFVMethod = 1 (first-order subcell finite volumes). */
+  int nfvse;               /* 0 off, 1 on */
+  int compute_alpha;       /* ComputeAlpha: 1 Persson-Peraire indicator, 3 fixed ShockBlendCoef */
+  double shock_blend_coef; /* ShockBlendCoef */
+  int modal_threshold;     /* ModalThreshold: 1 T = 0.5*10^(-1.8 (N+1)^0.25), 2 T = 0.5*10^(-1.8 N^0.25) */
+  double alpha_max, alpha_min, space_prop_factor; /* alpha_max, alpha_min, SpacePropFactor */
+  int space_prop_sweeps;   /* SpacePropSweeps */
+  double time_rel_factor;  /* TimeRelFactor */
+  int indicator_quantity;  /* ShockIndicatorQuantity: 1 Density, 2 Pressure, 3 DensityTimesPressure,
+                              4 KinPlusMagEnergy */
 } fluxo_cfg;
 
 typedef struct fluxo_handle fluxo_handle;
@@ -130,6 +141,10 @@ int fluxo_gpu_time_disc(fluxo_handle* h, double t, double tEnd, int maxIter, dou
 int fluxo_gpu_set_glm_ch(fluxo_handle* h, double ch);
 int fluxo_gpu_get_glm_ch(fluxo_handle* h, double* ch);
 
+/* NFVSE: MOD_NFVSE_Vars::alpha(nElems), the blending coefficients of the last right-hand side
+ * (src/shockcapturing/nfvse_vars.f90). */
+int fluxo_gpu_get_alpha(fluxo_handle* h, double* alpha);
+
 /* Device pointers and stream for zero-copy callers (e.g. torch tensors):
  * U, Ut are device buffers of nVar*(N+1)^3*nElems doubles in the host layout. */
 int fluxo_gpu_device_buffers(fluxo_handle* h, double** dU, double** dUt, void** stream);
@@ -137,7 +152,8 @@ int fluxo_gpu_device_buffers(fluxo_handle* h, double** dU, double** dUt, void** 
 int fluxo_gpu_launch_count(fluxo_handle* h, uint64_t* n);
 
 /* Per-kernel timing with CUDA events on the handle's stream (off by default).
- * kind: 0 lifting surface flux, 1 gradient, 2 face flux, 3 volume, 4 time step.
+ * kind: 0 lifting surface flux, 1 gradient, 2 face flux, 3 volume, 4 time step, 5 NFVSE
+ * (indicator, propagation and subcell finite volumes).
  * fluxo_gpu_get_profile synchronises, returns the summed milliseconds and launch count of
  * that kind since profiling was enabled, and resets them. */
 int fluxo_gpu_set_profiling(fluxo_handle* h, int enable);

@@ -1,0 +1,93 @@
+"""Parity of the sm_100a NFVSE shock capturing (MHD) against the CPU oracle, through the C ABI:
+the blending coefficients (Persson-Peraire indicator, clipping, space propagation) and Ut of the
+blended split-form / first-order subcell FV right-hand side, and a few device-resident time steps.
+Tolerances: alpha to 1e-12 absolute, Ut relative L2 <= 1e-12 (FP64, different summation order)."""
+import numpy as np
+import pytest
+
+import fluxo_b200 as fb
+from oracle.oracle import OracleCase
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+REF = ((1.2, 0.1, 0.0, 0.1, 0.9, 1.0, 1.0, 1.0), (1.1, 0.2, -0.1, 0.2, 0.6, 1.0, 1.0, 1.0))
+NFVSE_KEYS = ("nfvse", "compute_alpha", "shock_blend_coef", "modal_threshold", "alpha_max", "alpha_min",
+              "space_prop_factor", "space_prop_sweeps", "time_rel_factor", "indicator_quantity")
+
+
+def rel_l2(a, b):
+    return np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300)
+
+
+def nfvse_pair(noise=0.02, seed=0, ch=0.7, **kw):
+    base = dict(eqn=2, N=3, nElems=(3, 3, 2), xmin=(-1, -1, -1), xmax=(1, 1, 1), NGeo=2, deform_amp=0.1,
+                kappa=5 / 3, mhd_ref_state=REF, ini_exact_func=201, ini_center=(0.1, 0.05, 0.0),
+                ini_halfwidth=0.4, ini_amplitude=0.02, glm_ch=ch, nfvse=1, volume_flux=10, riemann=14)
+    base.update(kw)
+    c = OracleCase(**base)
+    U = c.get_U()
+    if noise:
+        rng = np.random.default_rng(seed)
+        U = U * (1 + noise * rng.standard_normal(U.shape))
+        U[..., 8] = 0.05 * rng.standard_normal(U[..., 8].shape)
+        c.set_U(U)
+    p = c.params
+    fields = dict(N=p.N, eqn=p.eqn, riemann=p.riemann, volume_flux=p.volume_flux, lifting=p.lifting,
+                  lifting_var=p.lifting_var, kappa=p.kappa, Pr=p.Pr, mu0=p.mu0, time_disc=p.time_disc,
+                  cfl_scale=p.cfl_scale, dfl_scale=p.dfl_scale, ini_exact_func=1, mu_0=p.mu_0, eta=p.eta,
+                  glm_scale=p.glm_scale, glm_scr=p.glm_scr, noncons=p.noncons, nc_glm=p.nc_glm)
+    fields.update({k: getattr(p, k) for k in NFVSE_KEYS})
+    op = fb.DGOperator(**fields)
+    op.set_mesh(c.mesh())
+    op.set_state(U)
+    op.glm_ch = ch
+    return c, op
+
+
+FIXED = [
+    dict(N=3, volume_flux=10, riemann=14, noncons=1, nc_glm=0),
+    dict(N=4, volume_flux=10, riemann=10, noncons=1, nc_glm=1),
+    dict(N=2, volume_flux=12, riemann=15, noncons=2, nc_glm=0),
+    dict(N=3, volume_flux=0, riemann=1, noncons=3, nc_glm=0),
+    dict(N=5, volume_flux=1, riemann=4, noncons=0, nc_glm=0),
+    dict(N=7, volume_flux=12, riemann=13, noncons=1, nc_glm=1, nElems=(1, 2, 1)),
+]
+
+
+@pytest.mark.parametrize("case", FIXED, ids=lambda c: "N%d_vf%d_rs%d_nc%d" % (
+    c["N"], c["volume_flux"], c["riemann"], c["noncons"]))
+def test_nfvse_fixed_alpha_parity(gpu_lib, case):
+    c, op = nfvse_pair(compute_alpha=3, shock_blend_coef=0.3, **case)
+    ref = c.dg_time_derivative(0.0)
+    op.dg_time_derivative(0.0)
+    assert np.abs(op.alpha() - c.alpha()).max() <= 1e-12
+    assert rel_l2(op.get_ut(), ref) <= TOL
+
+
+@pytest.mark.parametrize("sweeps,width", [(0, 0.02), (1, 0.02), (2, 0.02), (0, 0.1), (1, 0.15)])
+def test_nfvse_indicator_parity(gpu_lib, sweeps, width):
+    """Sharp (alpha clipped at alpha_max) and smoother blasts (alpha between alpha_min and alpha_max)."""
+    c, op = nfvse_pair(noise=0.0, N=4, nElems=(4, 4, 3), space_prop_sweeps=sweeps, ini_amplitude=width)
+    ref = c.dg_time_derivative(0.0)
+    op.dg_time_derivative(0.0)
+    a_ref = c.alpha()
+    assert a_ref.max() > 0.0 and (a_ref == 0.0).any()  # a mix of blended and pure DG elements
+    assert np.abs(op.alpha() - a_ref).max() <= 1e-12
+    assert rel_l2(op.get_ut(), ref) <= TOL
+
+
+def test_nfvse_resistive_parity(gpu_lib):
+    c, op = nfvse_pair(noise=0.0, eqn=3, eta=0.02, mu0=0.01, N=3, nElems=(4, 3, 3))
+    ref = c.dg_time_derivative(0.0)
+    op.dg_time_derivative(0.0)
+    assert np.abs(op.alpha() - c.alpha()).max() <= 1e-12
+    assert rel_l2(op.get_ut(), ref) <= TOL
+
+
+def test_nfvse_time_disc_parity(gpu_lib):
+    c, op = nfvse_pair(noise=0.0, N=3, nElems=(4, 3, 3), time_rel_factor=0.5)
+    t_ref, n_ref = c.run(0.0, 1.0, max_iter=6)
+    t, n, err = op.time_disc(0.0, 1.0, max_iter=6)
+    assert err == 0 and n == n_ref == 6
+    assert t == pytest.approx(t_ref, rel=1e-12)
+    assert rel_l2(op.get_state(), c.get_U()) <= 1e-11
