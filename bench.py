@@ -50,6 +50,29 @@ VOLUME_KERNEL_DRAM_BYTES_PER_DOF = 276.0
 
 METRIC = "PID ns/DOF/RHS, NS Taylor-Green N=7 32^3 curved, BR1 + EC-KEP + ES (Riemann 44), LSERK4-5"
 
+# The resistive-MHD configuration (--workload mhd): F_alg per DOF of one RHS by phase, from the
+# oracle's counting build on the configuration's initial state (4^3 elements, N=4); the NFVSE
+# phase is zero there because the smooth initial data blends no element.
+MHD_FALG_PER_DOF = {
+    "volume_split_form": 1912.0,
+    "lifting": 787.6,
+    "volume_viscous": 510.0,
+    "face_flux": 850.692,
+    "surface_integral": 21.6,
+    "jacobian_source": 9.0,
+}
+MHD_VOLUME_KERNEL_FALG = (MHD_FALG_PER_DOF["volume_split_form"] + MHD_FALG_PER_DOF["surface_integral"] +
+                          MHD_FALG_PER_DOF["jacobian_source"] + 36.0)  # + LSERK stage, 4 flops x 9 variables
+MHD_METRIC = ("PID ns/DOF/RHS, resistive MHD+GLM Orszag-Tang N=4 24^3 curved, Derigs EC + 9-wave ES "
+              "(Riemann 14), Powell, BR1, NFVSE, LSERK4-5")
+
+
+def mhd_workload(elems=24, N=4):
+    return dict(N=N, elems=(elems,) * 3, xmin=(0.0,) * 3, xmax=(2 * np.pi,) * 3, NGeo=2, deform_amp=0.05,
+                eqn=3, lifting=1, lifting_var=3, riemann=14, volume_flux=10, kappa=5.0 / 3.0, eta=1e-3, mu0=0.0,
+                noncons=1, nc_glm=0, glm_scale=0.5, nfvse=1, compute_alpha=1, alpha_max=0.5, alpha_min=0.01,
+                space_prop_sweeps=1, cfl_scale=0.9, dfl_scale=0.4, time_disc=0)
+
 
 def workload(elems=32, N=7):
     return dict(N=N, elems=(elems,) * 3, xmin=(-np.pi,) * 3, xmax=(np.pi,) * 3, NGeo=2, deform_amp=0.05,
@@ -227,17 +250,29 @@ def run_fluxo(args):
     world, rank, local = dist_setup(args.gpus)
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    w = workload(elems=args.elems, N=args.N)
+    mhd = args.workload == "mhd"
     t0 = time.time()
-    mesh = fb.box_mesh(w["N"], w["elems"], w["xmin"], w["xmax"], NGeo=w["NGeo"], deform_amp=w["deform_amp"])
-    op = fb.DGOperator(N=w["N"], eqn=1, riemann=w["riemann"], volume_flux=w["volume_flux"], lifting=1,
-                       lifting_var=3, visc=0, mu0=w["mu0"], Pr=w["Pr"], kappa=w["kappa"],
-                       cfl_scale=w["cfl_scale"], dfl_scale=w["dfl_scale"], time_disc=0, device=local)
-    op.set_mesh(mesh)
-    U0 = fb.exact_func(7, 0.0, mesh["Elem_xGP"], kappa=w["kappa"])
+    if mhd:
+        from fluxo_b200.workloads import mhd_orszag_tang_state
+
+        w = mhd_workload(elems=args.elems or 24, N=args.N or 4)
+        mesh = fb.box_mesh(w["N"], w["elems"], w["xmin"], w["xmax"], NGeo=w["NGeo"], deform_amp=w["deform_amp"])
+        fields = {k: v for k, v in w.items() if k not in ("elems", "xmin", "xmax", "NGeo", "deform_amp")}
+        op = fb.DGOperator(device=local, **fields)
+        op.set_mesh(mesh)
+        U0 = mhd_orszag_tang_state(mesh["Elem_xGP"], kappa=w["kappa"])
+    else:
+        w = workload(elems=args.elems or 32, N=args.N or 7)
+        mesh = fb.box_mesh(w["N"], w["elems"], w["xmin"], w["xmax"], NGeo=w["NGeo"], deform_amp=w["deform_amp"])
+        op = fb.DGOperator(N=w["N"], eqn=1, riemann=w["riemann"], volume_flux=w["volume_flux"], lifting=1,
+                           lifting_var=3, visc=0, mu0=w["mu0"], Pr=w["Pr"], kappa=w["kappa"],
+                           cfl_scale=w["cfl_scale"], dfl_scale=w["dfl_scale"], time_disc=0, device=local)
+        op.set_mesh(mesh)
+        U0 = fb.exact_func(7, 0.0, mesh["Elem_xGP"], kappa=w["kappa"])
     del mesh
     op.set_state(U0)
     setup_s = time.time() - t0
+    nvar = 9 if mhd else 5
     nd = op.nElems * (w["N"] + 1) ** 3
     _, _, stream_ptr = op.device_buffers()
     stream = torch.cuda.ExternalStream(stream_ptr, device=dev)
@@ -263,8 +298,9 @@ def run_fluxo(args):
     ms = ev0.elapsed_time(ev1)
     launches = op.launch_count() - n0
     vol_ms, vol_n = profile(op, 3)
-    kinds = {k: profile(op, i) for i, k in enumerate(("lift_flux", "gradient", "face_flux", "volume", "timestep"))
-             if i != 3}
+    kinds = {k: profile(op, i)
+             for i, k in enumerate(("lift_flux", "gradient", "face_flux", "volume", "timestep", "nfvse"))
+             if i != 3 and (i != 5 or mhd)}
     kinds["volume"] = (vol_ms, vol_n)
     set_profiling(op, False)
     ms_max = max_over_ranks(ms, world, dev)
@@ -274,7 +310,7 @@ def run_fluxo(args):
     # ---- end-to-end through the public API with pinned host buffers ----
     e2e = None
     if not args.no_e2e:
-        hostU = torch.empty(nd * 5, dtype=torch.float64, pin_memory=True)
+        hostU = torch.empty(nd * nvar, dtype=torch.float64, pin_memory=True)
         get_state_ptr(op, hostU.data_ptr())
         e2e_steps = max(2, min(args.steps, 5))
         barrier(world)
@@ -290,29 +326,42 @@ def run_fluxo(args):
         barrier(world)
         ems = max_over_ranks(e0.elapsed_time(e1), world, dev)
         e2e = {"value": ems * 1e6 / (world * nd * 5 * e2e_steps), "unit": "ns/DOF/RHS",
-               "h2d_bytes_per_step": nd * 5 * 8, "d2h_bytes_per_step": nd * 5 * 8, "steps": e2e_steps,
+               "h2d_bytes_per_step": nd * nvar * 8, "d2h_bytes_per_step": nd * nvar * 8, "steps": e2e_steps,
                "path": "fluxo_gpu_set_state + fluxo_gpu_time_disc(1 step) + fluxo_gpu_get_state, pinned host"}
 
     if rank != 0:
         op.close()
         return
     vol_avg_ms = vol_ms / max(vol_n, 1)
-    achieved = VOLUME_KERNEL_FALG * nd / (vol_avg_ms * 1e-3) / 1e12
-    roofline = {"bound": "fp64", "kernel": "volume_kernel<8,5,true>", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": VOLUME_KERNEL_DRAM_BYTES_PER_DOF * nd,
-                "traffic_note": "bytes per launch, ncu on 16^3 scaled by DOFs",
-                "flops_per_dof_launch": VOLUME_KERNEL_FALG, "launch_ms": vol_avg_ms,
+    vol_falg = MHD_VOLUME_KERNEL_FALG if mhd else VOLUME_KERNEL_FALG
+    achieved = vol_falg * nd / (vol_avg_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp64", "kernel": "mhd::volume_kernel<5,10>" if mhd else "volume_kernel<8,5,true>",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None if mhd else VOLUME_KERNEL_DRAM_BYTES_PER_DOF * nd,
+                "traffic_note": None if mhd else "bytes per launch, ncu on 16^3 scaled by DOFs",
+                "flops_per_dof_launch": vol_falg, "launch_ms": vol_avg_ms,
                 "peak_source": "measured in this job: DFMA loop (fluxo_gpu_fp64_peak); MEASURED_PEAKS.json has no FP64"}
-    line = {"metric": METRIC, "value": value, "unit": "ns/DOF/RHS", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_dict(w, world, args.steps), "roofline": roofline, "e2e": e2e,
+    falg_rhs = sum((MHD_FALG_PER_DOF if mhd else FALG_PER_DOF).values())
+    if mhd:
+        alpha = op.alpha()
+        config = {"workload": "mhd_glm_resistive_orszag_tang_N%d_%dx%dx%d_curved" % ((w["N"],) + w["elems"]),
+                  "N": w["N"], "elements": list(w["elems"]), "dofs_per_gpu": nd, "riemann": 14, "volume_flux": 10,
+                  "noncons": "powell", "lifting": "br1_entropy_var", "eta": w["eta"],
+                  "nfvse": "indicator, alpha_max 0.5, alpha_min 0.01, 1 sweep",
+                  "blended_elements_last_rhs": int((alpha > 0).sum()), "time_disc": "carpenterrk4-5",
+                  "rhs_per_step": 5, "parallelism": "replicas x%d" % world,
+                  "l2": "inputs larger than L2 (state %d MB)" % (nd * 72 // 10 ** 6), "steps": args.steps}
+    else:
+        config = config_dict(w, world, args.steps)
+    line = {"metric": MHD_METRIC if mhd else METRIC, "value": value, "unit": "ns/DOF/RHS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config, "roofline": roofline, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clk.summary(),
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kinds.items()},
-            "rhs_roofline_frac": (sum(FALG_PER_DOF.values()) * nd * rhs / (ms * 1e-3) / 1e12) / peak,
+            "rhs_roofline_frac": (falg_rhs * nd * rhs / (ms * 1e-3) / 1e12) / peak,
             "setup_s": setup_s}
-    if world == 1 and not args.no_cpu:
+    if world == 1 and not args.no_cpu and not mhd:
         line["cpu_baseline"] = cpu_baseline_subprocess(os.cpu_count() or 1, seconds=args.cpu_seconds)
     print(json.dumps(line))
     op.close()
@@ -324,8 +373,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fluxo", choices=("fluxo", "reference"))
-    ap.add_argument("--elems", type=int, default=32)
-    ap.add_argument("--N", type=int, default=7)
+    ap.add_argument("--workload", default="tgv", choices=("tgv", "mhd"),
+                    help="tgv: the headline Navier-Stokes configuration; mhd: the resistive-MHD configuration")
+    ap.add_argument("--elems", type=int, default=0, help="elements per direction (0: the configuration's)")
+    ap.add_argument("--N", type=int, default=0, help="polynomial degree (0: the configuration's)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)

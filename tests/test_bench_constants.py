@@ -14,3 +14,28 @@ def test_falg_constants_match_oracle_count():
         assert abs(phases[k] - v) < 1e-9, k
     assert abs(total - sum(bench.FALG_PER_DOF.values())) < 1e-9
     assert np.isclose(bench.VOLUME_KERNEL_FALG, 1124.5 + 384.0 + 7.5 + 5.0 + 20.0)
+
+
+def test_mhd_falg_constants_match_oracle_count():
+    """The resistive-MHD configuration's counts, on its initial state (4^3 elements, N=4)."""
+    from oracle.oracle import PHASES, OracleCase, _lib
+    from fluxo_b200.workloads import mhd_orszag_tang_state
+
+    w = bench.mhd_workload(elems=4)
+    kw = dict(N=w["N"], nElems=w["elems"], xmin=w["xmin"], xmax=w["xmax"], NGeo=w["NGeo"], deform_amp=w["deform_amp"],
+              eqn=3, kappa=w["kappa"], eta=w["eta"], mu0=0.0, lifting=1, lifting_var=3, volume_flux=10, riemann=14,
+              noncons=1, nc_glm=0, nfvse=1, ini_exact_func=0, glm_scale=0.5, cfl_scale=0.9, dfl_scale=0.4)
+    ref = OracleCase(**kw)
+    ref.set_U(mhd_orszag_tang_state(ref.mesh()["Elem_xGP"], kappa=w["kappa"]))
+    ref.calc_timestep()  # sets GLM_ch as in a time step
+    c = OracleCase(counting=True, **kw)
+    c.set_U(ref.get_U())
+    c.glm_ch = ref.glm_ch
+    lib = _lib(counting=True)
+    lib.orc_reset_flops()
+    c.dg_time_derivative(0.0)
+    nd = c.nElems * c.np ** 3
+    phases = {k: lib.orc_phase_flops(i) / nd for i, k in enumerate(PHASES)}
+    assert phases["nfvse"] == 0.0
+    for k, v in bench.MHD_FALG_PER_DOF.items():
+        assert abs(phases[k] - v) < 1e-9, k

@@ -84,6 +84,44 @@ def test_nfvse_resistive_parity(gpu_lib):
     assert rel_l2(op.get_ut(), ref) <= TOL
 
 
+@pytest.mark.parametrize("riemann,tol", [(10, 1e-12), (14, 1e-10)])
+def test_resistive_mhd_orszag_tang_config_parity(gpu_lib, riemann, tol):
+    """The resistive-MHD benchmark configuration (GLM, Powell terms, BR1 entropy variables, Derigs EC
+    volume flux, NFVSE from the indicator) on a 3^3 curved box at N=4: GPU and oracle agree on Ut and
+    after five device-resident time steps.  With the configuration's 9-wave surface flux (Riemann 14)
+    the tolerance is 1e-10: its eigenvectors are ill-conditioned where the averaged B is almost
+    normal to a face (this initial B lies in the x-y plane), and in the oracle alone a relative
+    perturbation of 1e-16 of U moves Ut by 4e-11.  With the ES-LLF flux (Riemann 10) it is 1e-12."""
+    from fluxo_b200.workloads import mhd_orszag_tang_state
+
+    TOL = tol
+    kw = dict(eqn=3, N=4, nElems=(3, 3, 3), xmin=(0, 0, 0), xmax=(2 * np.pi,) * 3, NGeo=2, deform_amp=0.05,
+              kappa=5 / 3, eta=1e-3, mu0=0.0, lifting=1, lifting_var=3, volume_flux=10, riemann=riemann, noncons=1,
+              nc_glm=0, nfvse=1, ini_exact_func=0, glm_scale=0.5, cfl_scale=0.9, dfl_scale=0.4)
+    c = OracleCase(**kw)
+    m = c.mesh()
+    U = mhd_orszag_tang_state(m["Elem_xGP"])
+    c.set_U(U)
+    p = c.params
+    fields = dict(N=4, eqn=3, riemann=riemann, volume_flux=10, lifting=1, lifting_var=3, kappa=p.kappa, Pr=p.Pr,
+                  mu0=0.0, eta=1e-3, glm_scale=0.5, noncons=1, nc_glm=0, ini_exact_func=1, cfl_scale=0.9,
+                  dfl_scale=0.4)
+    fields.update({k: getattr(p, k) for k in NFVSE_KEYS})
+    op = fb.DGOperator(**fields)
+    op.set_mesh(m)
+    op.set_state(U)
+    d_ref, _ = c.calc_timestep()
+    d, _ = op.calc_timestep()
+    assert abs(d - d_ref) <= 1e-13 * d_ref
+    ref = c.dg_time_derivative(0.0)
+    op.dg_time_derivative(0.0)
+    assert rel_l2(op.get_ut(), ref) <= TOL
+    t_ref, _ = c.run(0.0, 1.0, max_iter=5)
+    t, n, err = op.time_disc(0.0, 1.0, max_iter=5)
+    assert err == 0 and n == 5 and t == pytest.approx(t_ref, rel=1e-12)
+    assert rel_l2(op.get_state(), c.get_U()) <= 1e-11
+
+
 def test_nfvse_time_disc_parity(gpu_lib):
     c, op = nfvse_pair(noise=0.0, N=3, nElems=(4, 3, 3), time_rel_factor=0.5)
     t_ref, n_ref = c.run(0.0, 1.0, max_iter=6)
