@@ -67,6 +67,17 @@ MHD_METRIC = ("PID ns/DOF/RHS, resistive MHD+GLM Orszag-Tang N=4 24^3 curved, De
               "(Riemann 14), Powell, BR1, NFVSE, LSERK4-5")
 
 
+# The batched configuration (--workload batch): F_alg per DOF of one RHS for each (equation, N) of the
+# mix (Euler: EC flux + LLF; Navier-Stokes: EC-KEP + Riemann 44, BR1), from the oracle's counting
+# build on a 2^3 instance with the mix's initial data (fourier_state, seed SEED).
+BATCH_FALG_PER_DOF = {
+    (0, 3): 684.7734375, (0, 4): 830.796, (0, 5): 985.3472222222222, (0, 7): 1306.18359375,
+    (1, 3): 1632.5859375, (1, 4): 1738.812, (1, 5): 1882.201388888889, (1, 7): 2219.6220703125,
+}
+BATCH_METRIC = ("aggregate DOF-updates/s (DOFs x RHS evaluations per second), 64 uneven Euler/NS periodic-box "
+                "instances (4^3..16^3 elements, N in {3,4,5,7}) batched, vs one at a time")
+
+
 def mhd_workload(elems=24, N=4):
     return dict(N=N, elems=(elems,) * 3, xmin=(0.0,) * 3, xmax=(2 * np.pi,) * 3, NGeo=2, deform_amp=0.05,
                 eqn=3, lifting=1, lifting_var=3, riemann=14, volume_flux=10, kappa=5.0 / 3.0, eta=1e-3, mu0=0.0,
@@ -367,14 +378,146 @@ def run_fluxo(args):
     op.close()
 
 
+def batch_falg(specs):
+    """Algorithmic FP64 operations of one RHS plus its LSERK stage update, summed over instances."""
+    return sum((BATCH_FALG_PER_DOF[(s["eqn"], s["N"])] + FALG_RK_STAGE_PER_DOF) * s["elems"] ** 3 * (s["N"] + 1) ** 3
+               for s in specs)
+
+
+def batch_launches_per_step(specs):
+    """Kernels in one replay of the batch's step graph: per group reset, CALCTIMESTEP, dt, time update,
+    and per stage face + volume (+ lifting flux + gradients for Navier-Stokes)."""
+    groups = {(s["eqn"], s["N"]) for s in specs}
+    return sum(4 + 5 * (4 if eqn == 1 else 2) for eqn, _ in groups)
+
+
+def run_batch(args):
+    """The batched configuration: the instances advance together (fluxo_batch_run, one graph replay
+    per step) and, for comparison, one at a time (fluxo_gpu_time_disc per instance)."""
+    import torch
+
+    import fluxo_b200 as fb
+    from fluxo_b200.batch import Batch
+    from fluxo_b200.solver import fp64_peak
+    from fluxo_b200.workloads import batch_instance_specs, build_instance, instance_fields
+
+    world, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    t0 = time.time()
+    specs = batch_instance_specs(args.instances)
+    cache, insts = {}, []
+    for s in specs:
+        mesh, U = build_instance(s, cache)
+        insts.append((s, mesh, U, fb.make_cfg(device=local, **instance_fields(s))))
+    dofs = [s["elems"] ** 3 * (s["N"] + 1) ** 3 for s in specs]
+    nd = sum(dofs)
+    setup_s = time.time() - t0
+    peak = fp64_peak(local)
+
+    # ---- batched: all instances in one batch, one graph replay per step ----
+    b = Batch(device=local)
+    ids = [b.add(mesh, U, 0.0, 1e30, cfg=cfg) for (s, mesh, U, cfg) in insts]
+    b.run(args.warmup)
+    stream = torch.cuda.ExternalStream(b.stream(), device=dev)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        b.run(args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    barrier(world)
+    ms = ev0.elapsed_time(ev1)
+    for iid in ids:
+        _, n, done, err = b.status(iid)
+        assert n == args.warmup + args.steps and not done and err == 0, (iid, n, done, err)
+    ms_max = max_over_ranks(ms, world, dev)
+    value = world * nd * 5 * args.steps / (ms_max * 1e-3)
+    groups, placed, nbytes = b.info()
+
+    # ---- end to end through the public API: host state in and out every step ----
+    e2e = None
+    if not args.no_e2e:
+        host = [torch.empty(d * 5, dtype=torch.float64, pin_memory=True) for d in dofs]
+        for iid, h in zip(ids, host):
+            b.lib.fluxo_batch_get_state(b.b, iid, h.data_ptr())
+        e2e_steps = max(2, min(args.steps, 5))
+        barrier(world)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            for iid, h in zip(ids, host):
+                b._check(b.lib.fluxo_batch_set_state(b.b, iid, h.data_ptr()))
+            b.run(1)
+            for iid, h in zip(ids, host):
+                b._check(b.lib.fluxo_batch_get_state(b.b, iid, h.data_ptr()))
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier(world)
+        ems = max_over_ranks(e0.elapsed_time(e1), world, dev)
+        e2e = {"value": world * nd * 5 * e2e_steps / (ems * 1e-3), "unit": "DOF-updates/s",
+               "h2d_bytes_per_step": nd * 5 * 8, "d2h_bytes_per_step": nd * 5 * 8, "steps": e2e_steps,
+               "path": "fluxo_batch_set_state (all instances) + fluxo_batch_run(1) + fluxo_batch_get_state, pinned host"}
+    b.close()
+
+    # ---- one at a time: each instance alone through fluxo_gpu_time_disc, device time summed ----
+    seq_ms = 0.0
+    if not args.no_sequential:
+        for (s, mesh, U, cfg) in insts:
+            op = fb.DGOperator(cfg=cfg)
+            op.set_mesh(mesh)
+            op.set_state(U)
+            t, n, err = op.time_disc(0.0, 1e30, args.warmup)
+            st = torch.cuda.ExternalStream(op.device_buffers()[2], device=dev)
+            torch.cuda.synchronize(dev)
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(st)
+            t, n, err = op.time_disc(t, 1e30, args.steps)
+            a1.record(st)
+            torch.cuda.synchronize(dev)
+            assert err == 0 and n == args.steps
+            seq_ms += a0.elapsed_time(a1)
+            op.close()
+        seq_ms = max_over_ranks(seq_ms, world, dev)
+    if rank != 0:
+        return
+    achieved = batch_falg(specs) * 5 * args.steps / (ms * 1e-3) / 1e12
+    seq = None
+    if seq_ms > 0:
+        seq = {"value": world * nd * 5 * args.steps / (seq_ms * 1e-3), "unit": "DOF-updates/s",
+               "ms_per_step": seq_ms / args.steps, "path": "fluxo_gpu_time_disc per instance, one after another"}
+    ne = [s["elems"] ** 3 for s in specs]
+    config = {"workload": "batched_%d_uneven_euler_ns_instances" % len(specs), "instances": len(specs),
+              "elements": "per instance %d..%d (%d total)" % (min(ne), max(ne), sum(ne)),
+              "N": sorted({s["N"] for s in specs}), "navier_stokes_instances": sum(s["eqn"] for s in specs),
+              "dofs_per_gpu": nd, "groups": groups, "device_bytes": nbytes, "time_disc": "carpenterrk4-5",
+              "rhs_per_step": 5, "parallelism": "replicas x%d" % world,
+              "l2": "inputs larger than L2 (state %d MB)" % (nd * 40 // 10 ** 6), "steps": args.steps}
+    line = {"metric": BATCH_METRIC, "value": value, "unit": "DOF-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+            "roofline": {"bound": "fp64", "kernel": "batched step (all groups, all kernels)", "achieved": achieved,
+                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None},
+            "one_at_a_time": seq, "batched_over_one_at_a_time": (value / seq["value"]) if seq else None,
+            "e2e": e2e, "gpu_launches": batch_launches_per_step(specs) * args.steps, "clocks": clk.summary(),
+            "setup_s": setup_s}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fluxo", choices=("fluxo", "reference"))
-    ap.add_argument("--workload", default="tgv", choices=("tgv", "mhd"),
-                    help="tgv: the headline Navier-Stokes configuration; mhd: the resistive-MHD configuration")
+    ap.add_argument("--workload", default="tgv", choices=("tgv", "mhd", "batch"),
+                    help="tgv: the headline Navier-Stokes configuration; mhd: the resistive-MHD configuration; "
+                         "batch: uneven Euler/NS instances batched vs one at a time")
+    ap.add_argument("--instances", type=int, default=64, help="batch: number of instances")
+    ap.add_argument("--no-sequential", action="store_true", help="batch: skip the one-at-a-time comparison")
     ap.add_argument("--elems", type=int, default=0, help="elements per direction (0: the configuration's)")
     ap.add_argument("--N", type=int, default=0, help="polynomial degree (0: the configuration's)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -383,6 +526,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch":
+        run_batch(args)
     else:
         run_fluxo(args)
     if int(os.environ.get("WORLD_SIZE", "1")) > 1:

@@ -78,6 +78,11 @@ EXPORTS = [
     "fluxo_gpu_last_error", "fluxo_gpu_set_profiling", "fluxo_gpu_get_profile", "fluxo_gpu_fp64_peak",
     "fluxo_host_box_sizes", "fluxo_host_box_mesh", "fluxo_host_exact_func", "fluxo_gpu_dg_time_derivative_noalloc",
     "fluxo_gpu_set_glm_ch", "fluxo_gpu_get_glm_ch", "fluxo_gpu_get_alpha",
+    "fluxo_batch_create", "fluxo_batch_add", "fluxo_batch_run", "fluxo_batch_status", "fluxo_batch_get_state",
+    "fluxo_batch_set_state",
+    "fluxo_batch_remove", "fluxo_batch_info", "fluxo_batch_stream", "fluxo_batch_instance_bytes",
+    "fluxo_batch_last_error",
+    "fluxo_batch_destroy",
 ]
 
 # FLUXO_NOALLOC_SCRATCH_BYTES of fluxo_gpu.h: the static scratch of fluxo_gpu_dg_time_derivative_noalloc
@@ -119,6 +124,19 @@ def load():
     lib.fluxo_gpu_set_glm_ch.argtypes = [vp, d]
     lib.fluxo_gpu_get_glm_ch.argtypes = [vp, P(d)]
     lib.fluxo_gpu_get_alpha.argtypes = [vp, vp]
+    sz = ctypes.c_size_t
+    lib.fluxo_batch_create.argtypes = [i, P(vp)]
+    lib.fluxo_batch_add.argtypes = [vp, P(FluxoCfg), i, i] + [vp] * 11 + [d, d, i, P(i)]
+    lib.fluxo_batch_run.argtypes = [vp, i, P(i)]
+    lib.fluxo_batch_status.argtypes = [vp, i, P(d), P(i), P(i), P(i)]
+    lib.fluxo_batch_get_state.argtypes = [vp, i, vp]
+    lib.fluxo_batch_set_state.argtypes = [vp, i, vp]
+    lib.fluxo_batch_remove.argtypes = [vp, i]
+    lib.fluxo_batch_info.argtypes = [vp, P(i), P(i), P(sz)]
+    lib.fluxo_batch_stream.argtypes = [vp, P(vp)]
+    lib.fluxo_batch_instance_bytes.argtypes = [P(FluxoCfg), i, i, P(sz)]
+    lib.fluxo_batch_last_error.argtypes = [vp, ctypes.c_char_p, sz]
+    lib.fluxo_batch_destroy.argtypes = [vp]
     for name in EXPORTS:
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib

@@ -89,9 +89,33 @@ struct KParams {
   const double* sVdm;     // nodal -> modal Legendre coefficients [m][i]
   int computeAlpha, indicatorQuantity, propSweeps;
   double threshold, sharpness, alphaMax, alphaMin, propFactor, timeRelFactor, shockBlendCoef;
+  // batched solves: the elements of many independent instances in one launch; each instance has
+  // its own time step (null for a single solve)
+  const int* elemInst;               // [elem] index of the element's instance in the arrays below
+  const double* instDt;              // [instance] dt of the current step (0 once finished)
+  unsigned long long* instDtBits;    // [instance] CALCTIMESTEP minimum (bits of a double)
+  int* instErrKey;                   // [instance] elem*8+errType of the first bad element
 };
 
 __device__ __forceinline__ bool halted(const KParams& P) { return P.haltFlag && *P.haltFlag != 0; }
+
+// dt of the LSERK stage update of element e (host value, device time loop, or per instance)
+__device__ __forceinline__ double stage_dt(const KParams& P, int e) {
+  if (P.elemInst) return P.instDt[P.elemInst[e]];
+  return P.dtDev ? P.dtDev[0] : P.dt;
+}
+
+// global minimum of CALCTIMESTEP (one solve) or the minimum of the element's instance (batch)
+__device__ __forceinline__ void reduce_timestep(const KParams& P, int e, double dtE, int err,
+                                                unsigned long long* dtBits, int* errKey) {
+  if (P.elemInst) {
+    const int inst = P.elemInst[e];
+    dtBits = P.instDtBits + inst;
+    errKey = P.instErrKey + inst;
+  }
+  if (err != 0) atomicMin(errKey, e * 8 + err);
+  else atomicMin(dtBits, (unsigned long long)__double_as_longlong(dtE));
+}
 __device__ __forceinline__ double glm_ch(const KParams& P) { return P.chDev ? *P.chDev : P.glmCh; }
 
 // Asks the memory system to bring the line holding p into L2 (no register result, no fault on the

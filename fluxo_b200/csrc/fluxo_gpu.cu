@@ -180,15 +180,7 @@ KParams base_params(fluxo_handle* h) {
   P.s2e = h->dS2E; P.e2s = h->dE2S;
   P.flux = h->dFlux; P.lflux = h->dLFlux; P.gtrace = h->dGTrace;
   P.basis = h->dBasis;
-  P.kappa = c.kappa; P.kappaM1 = c.kappa - 1.; P.sKappaM1 = 1. / (c.kappa - 1.); P.kappaP1 = c.kappa + 1.;
-  P.R = c.R; P.s23 = 2. / 3.; P.KappasPr = c.kappa / c.Pr; P.mu0 = c.mu0;
-  P.visc = c.visc; P.lifting_var = c.lifting_var; P.lifting = c.lifting; P.etaBR2 = c.etaBR2;
-  if (c.visc == 1) {  // equation.f90:226-233 (Sutherland constants)
-    P.sTref = 1. / c.Tref; P.ExpoSuth = c.ExpoSuth; P.Ts = c.Ts * P.sTref;
-    P.cSuth = std::pow(P.Ts, P.ExpoSuth) * (1 + P.Ts) / (2 * P.Ts * P.Ts);
-  } else if (c.visc == 2) {  // equation.f90:236-241 (power law)
-    P.ExpoPow = c.ExpoPow; P.mu0 = c.mu0 / std::pow(c.Tref, c.ExpoPow);
-  }
+  fill_ns_physics(P, c);
   P.source = (c.ini_exact_func == 4 && h->haveXGP) ? 1 : 0;
   if (P.source) {  // CalcSource CASE(4) constants, equation.f90:1000-1012
     double Omega = M_PI * c.ini_frequency, A = c.ini_amplitude, km1 = c.kappa - 1.;
@@ -198,7 +190,6 @@ KParams base_params(fluxo_handle* h) {
     for (int z = 0; z < 6; ++z) P.srcTmp[z] = tmp[z] * A * Omega;
   }
   P.CFLScale = h->CFLScale; P.DFLScale = h->DFLScale;
-  P.KappasPrMax = std::max(4. / 3., P.KappasPr);
   if (h->mhd) {  // mhd/equation.f90:170-209; calctimestep.f90:81-84
     P.kappaM2 = c.kappa - 2.;
     P.smu_0 = 1. / c.mu_0; P.s2mu_0 = 0.5 * P.smu_0;
@@ -345,6 +336,59 @@ int check_ready(fluxo_handle* h) {
 
 namespace fluxo {
 void basis_tables_for(int N, BasisTables& B) { build_basis_tables(N, B); }
+
+// Equation constants of the Euler / Navier-Stokes kernels (navierstokes/equation.f90:162-260)
+void fill_ns_physics(KParams& P, const fluxo_cfg& c) {
+  P.kappa = c.kappa; P.kappaM1 = c.kappa - 1.; P.sKappaM1 = 1. / (c.kappa - 1.); P.kappaP1 = c.kappa + 1.;
+  P.R = c.R; P.s23 = 2. / 3.; P.KappasPr = c.kappa / c.Pr; P.mu0 = c.mu0;
+  P.visc = c.visc; P.lifting_var = c.lifting_var; P.lifting = c.lifting; P.etaBR2 = c.etaBR2;
+  if (c.visc == 1) {  // equation.f90:226-233 (Sutherland constants)
+    P.sTref = 1. / c.Tref; P.ExpoSuth = c.ExpoSuth; P.Ts = c.Ts * P.sTref;
+    P.cSuth = std::pow(P.Ts, P.ExpoSuth) * (1 + P.Ts) / (2 * P.Ts * P.Ts);
+  } else if (c.visc == 2) {  // equation.f90:236-241 (power law)
+    P.ExpoPow = c.ExpoPow; P.mu0 = c.mu0 / std::pow(c.Tref, c.ExpoPow);
+  }
+  P.KappasPrMax = std::max(4. / 3., P.KappasPr);
+}
+
+// LSERK coefficients (index 1..nStages) and the scaled CFL/DFL numbers of a configuration
+// (timedisc_vars.f90:168-235, FillCFL_DFL timedisc.f90:697-741); false for an unknown time_disc
+bool time_disc_setup(const fluxo_cfg& c, double* RKA, double* RKb, double* RKc, int* nStages, double* CFLScale,
+                     double* DFLScale) {
+  double cflAlpha[15], relDFL;
+  if (c.time_disc == 0) {
+    const double a[15] = {4.7497, 3.4144, 2.8451, 2.4739, 2.2027, 1.9912, 1.8225, 1.6830,
+                          1.5682, 1.4692, 1.3849, 1.3106, 1.2454, 1.1880, 1.1362};
+    std::copy(a, a + 15, cflAlpha);
+    relDFL = 1.853;
+    *nStages = 5;
+    const double A[6] = {0., 0., 567301805773.0 / 1357537059087.0, 2404267990393.0 / 2016746695238.0,
+                         3550918686646.0 / 2091501179385.0, 1275806237668.0 / 842570457699.0};
+    const double B[6] = {0., 1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+                         1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+                         2277821191437.0 / 14882151754819.0};
+    const double C[6] = {0., 0., 1432997174477.0 / 9575080441755.0, 2526269341429.0 / 6820363962896.0,
+                         2006345519317.0 / 3224310063776.0, 2802321613138.0 / 2924317926251.0};
+    std::copy(A, A + 6, RKA); std::copy(B, B + 6, RKb); std::copy(C, C + 6, RKc);
+  } else if (c.time_disc == 1) {
+    const double a[15] = {3.1871, 2.2444, 1.7797, 1.5075, 1.3230, 1.1857, 1.0800, 0.9945,
+                          0.9247, 0.8651, 0.8134, 0.7695, 0.7301, 0.6952, 0.6649};
+    std::copy(a, a + 15, cflAlpha);
+    relDFL = 1.;
+    *nStages = 3;
+    const double A[4] = {0., 0., 5. / 9., 153. / 128.}, B[4] = {0., 1. / 3., 15. / 16., 8. / 15.},
+                 C[4] = {0., 0., 1. / 3., 0.75};
+    std::copy(A, A + 4, RKA); std::copy(B, B + 4, RKb); std::copy(C, C + 4, RKc);
+  } else {
+    return false;
+  }
+  const int N = c.N;
+  const double dflAlpha[10] = {4.50, 1.95, 1.18, 0.79, 0.56, 0.42, 0.32, 0.25, 0.20, 0.17};
+  *CFLScale = c.cfl_scale * cflAlpha[std::min(15, N) - 1] / (2. * N + 1.);
+  *DFLScale = c.dfl_scale * dflAlpha[std::min(10, N) - 1] * relDFL / ((2. * N + 1.) * (2. * N + 1.));
+  return true;
+}
+
 int record_unbound_error(int code, const std::string& msg) { return fail(nullptr, code, msg); }
 }  // namespace fluxo
 
@@ -392,38 +436,10 @@ int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {
   h->visc = parabolic;
   h->mhd = mhd;
   h->nVar = mhd ? 9 : 5;
-  // time discretisation coefficients and CFL/DFL scaling (timedisc_vars.f90:204-235, timedisc.f90:697-741)
-  double cflAlpha[15], relDFL;
-  if (cfg->time_disc == 0) {
-    const double a[15] = {4.7497, 3.4144, 2.8451, 2.4739, 2.2027, 1.9912, 1.8225, 1.6830,
-                          1.5682, 1.4692, 1.3849, 1.3106, 1.2454, 1.1880, 1.1362};
-    std::copy(a, a + 15, cflAlpha);
-    relDFL = 1.853;
-    h->nStages = 5;
-    const double A[6] = {0., 0., 567301805773.0 / 1357537059087.0, 2404267990393.0 / 2016746695238.0,
-                         3550918686646.0 / 2091501179385.0, 1275806237668.0 / 842570457699.0};
-    const double B[6] = {0., 1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
-                         1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
-                         2277821191437.0 / 14882151754819.0};
-    const double C[6] = {0., 0., 1432997174477.0 / 9575080441755.0, 2526269341429.0 / 6820363962896.0,
-                         2006345519317.0 / 3224310063776.0, 2802321613138.0 / 2924317926251.0};
-    std::copy(A, A + 6, h->RKA); std::copy(B, B + 6, h->RKb); std::copy(C, C + 6, h->RKc);
-  } else if (cfg->time_disc == 1) {
-    const double a[15] = {3.1871, 2.2444, 1.7797, 1.5075, 1.3230, 1.1857, 1.0800, 0.9945,
-                          0.9247, 0.8651, 0.8134, 0.7695, 0.7301, 0.6952, 0.6649};
-    std::copy(a, a + 15, cflAlpha);
-    relDFL = 1.;
-    h->nStages = 3;
-    const double A[4] = {0., 0., 5. / 9., 153. / 128.}, B[4] = {0., 1. / 3., 15. / 16., 8. / 15.},
-                 C[4] = {0., 0., 1. / 3., 0.75};
-    std::copy(A, A + 4, h->RKA); std::copy(B, B + 4, h->RKb); std::copy(C, C + 4, h->RKc);
-  } else {
+  if (!time_disc_setup(*cfg, h->RKA, h->RKb, h->RKc, &h->nStages, &h->CFLScale, &h->DFLScale)) {
     delete h;
     return fail(nullptr, FLUXO_EINVAL_CFG, "time_disc must be 0 (carpenterrk4-5) or 1 (standardrk3-3)");
   }
-  const double dflAlpha[10] = {4.50, 1.95, 1.18, 0.79, 0.56, 0.42, 0.32, 0.25, 0.20, 0.17};
-  h->CFLScale = cfg->cfl_scale * cflAlpha[std::min(15, h->N) - 1] / (2. * h->N + 1.);
-  h->DFLScale = cfg->dfl_scale * dflAlpha[std::min(10, h->N) - 1] * relDFL / ((2. * h->N + 1.) * (2. * h->N + 1.));
   cudaError_t e = cudaSetDevice(cfg->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
@@ -467,43 +483,13 @@ int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* S2E, 
   if (h->cfg.ini_exact_func == 4 && !Elem_xGP) return fail(h, FLUXO_EINVAL_CFG, "source term needs Elem_xGP");
   FLUXO_CUDA(h, cudaSetDevice(h->cfg.device));
   const int NP = h->NP, NP3 = NP * NP * NP, NPT = NP * NP;
-  // connectivity: 1-based -> 0-based, checked
-  std::vector<int> s2e((size_t)5 * nSides), e2s((size_t)12 * nElems);
-  for (int s = 0; s < nSides; ++s) {
-    const int* a = S2E + 5 * (size_t)s;
-    if (a[0] < 1 || a[0] > nElems || a[1] < 1 || a[1] > nElems || a[2] < 1 || a[2] > 6 || a[3] < 1 || a[3] > 6 ||
-        a[4] < 1 || a[4] > 4)
-      return fail(h, FLUXO_EINVAL_CFG, "set_mesh: SideToElem entry out of range (only inner sides are supported)");
-    s2e[5 * (size_t)s + 0] = a[0] - 1; s2e[5 * (size_t)s + 1] = a[1] - 1;
-    s2e[5 * (size_t)s + 2] = a[2]; s2e[5 * (size_t)s + 3] = a[3]; s2e[5 * (size_t)s + 4] = a[4];
-  }
-  for (int e = 0; e < nElems; ++e)
-    for (int ls = 0; ls < 6; ++ls) {
-      const int sid = E2S[2 * (6 * (size_t)e + ls)], fl = E2S[2 * (6 * (size_t)e + ls) + 1];
-      if (sid < 1 || sid > nSides || fl < 0 || fl > 4) return fail(h, FLUXO_EINVAL_CFG, "set_mesh: ElemToSide out of range");
-      e2s[2 * (6 * (size_t)e + ls)] = sid - 1;
-      e2s[2 * (6 * (size_t)e + ls) + 1] = fl;
-    }
-  // repack geometry: metrics [elem][9][node], face geometry [side][10][pt]
-  std::vector<double> met((size_t)9 * NP3 * nElems), geo((size_t)10 * NPT * nSides);
-  for (int e = 0; e < nElems; ++e)
-    for (int n = 0; n < NP3; ++n)
-      for (int d = 0; d < 3; ++d) {
-        const size_t src = 3 * ((size_t)e * NP3 + n) + d;
-        met[((size_t)e * 9 + d) * NP3 + n] = Mf[src];
-        met[((size_t)e * 9 + 3 + d) * NP3 + n] = Mg[src];
-        met[((size_t)e * 9 + 6 + d) * NP3 + n] = Mh[src];
-      }
-  for (int s = 0; s < nSides; ++s)
-    for (int p = 0; p < NPT; ++p) {
-      const size_t src = (size_t)s * NPT + p;
-      for (int d = 0; d < 3; ++d) {
-        geo[((size_t)s * 10 + d) * NPT + p] = NormVec[3 * src + d];
-        geo[((size_t)s * 10 + 3 + d) * NPT + p] = TangVec1[3 * src + d];
-        geo[((size_t)s * 10 + 6 + d) * NPT + p] = TangVec2[3 * src + d];
-      }
-      geo[((size_t)s * 10 + 9) * NPT + p] = SurfElem[src];
-    }
+  // connectivity 1-based -> 0-based (checked), metrics [elem][9][node], face geometry [side][10][pt]
+  std::vector<int> s2e, e2s;
+  std::vector<double> met, geo;
+  std::string rerr;
+  if (!host::repack_mesh(h->N, nElems, nSides, S2E, E2S, Mf, Mg, Mh, NormVec, TangVec1, TangVec2, SurfElem, s2e, e2s,
+                         met, geo, rerr))
+    return fail(h, FLUXO_EINVAL_CFG, "set_mesh: " + rerr);
   h->nElems = nElems; h->nSides = nSides;
   const int NV = h->nVar;
   const size_t nU = (size_t)NV * NP3 * nElems, nF = (size_t)NV * NPT * nSides;

@@ -276,6 +276,56 @@ void box_geometry(int N, const int* ne, const double* xmin, const double* xmax, 
   }
 }
 
+bool repack_mesh(int N, int nElems, int nSides, const int* S2E, const int* E2S, const double* Mf, const double* Mg,
+                 const double* Mh, const double* NormVec, const double* TangVec1, const double* TangVec2,
+                 const double* SurfElem, std::vector<int>& s2e, std::vector<int>& e2s, std::vector<double>& met,
+                 std::vector<double>& geo, std::string& err) {
+  const int NP = N + 1, NP3 = NP * NP * NP, NPT = NP * NP;
+  s2e.assign((size_t)5 * nSides, 0);
+  e2s.assign((size_t)12 * nElems, 0);
+  for (int s = 0; s < nSides; ++s) {
+    const int* a = S2E + 5 * (size_t)s;
+    if (a[0] < 1 || a[0] > nElems || a[1] < 1 || a[1] > nElems || a[2] < 1 || a[2] > 6 || a[3] < 1 || a[3] > 6 ||
+        a[4] < 1 || a[4] > 4) {
+      err = "SideToElem entry out of range (only inner sides are supported)";
+      return false;
+    }
+    s2e[5 * (size_t)s + 0] = a[0] - 1; s2e[5 * (size_t)s + 1] = a[1] - 1;
+    s2e[5 * (size_t)s + 2] = a[2]; s2e[5 * (size_t)s + 3] = a[3]; s2e[5 * (size_t)s + 4] = a[4];
+  }
+  for (int e = 0; e < nElems; ++e)
+    for (int ls = 0; ls < 6; ++ls) {
+      const int sid = E2S[2 * (6 * (size_t)e + ls)], fl = E2S[2 * (6 * (size_t)e + ls) + 1];
+      if (sid < 1 || sid > nSides || fl < 0 || fl > 4) {
+        err = "ElemToSide out of range";
+        return false;
+      }
+      e2s[2 * (6 * (size_t)e + ls)] = sid - 1;
+      e2s[2 * (6 * (size_t)e + ls) + 1] = fl;
+    }
+  met.assign((size_t)9 * NP3 * nElems, 0.);
+  geo.assign((size_t)10 * NPT * nSides, 0.);
+  for (int e = 0; e < nElems; ++e)
+    for (int n = 0; n < NP3; ++n)
+      for (int d = 0; d < 3; ++d) {
+        const size_t src = 3 * ((size_t)e * NP3 + n) + d;
+        met[((size_t)e * 9 + d) * NP3 + n] = Mf[src];
+        met[((size_t)e * 9 + 3 + d) * NP3 + n] = Mg[src];
+        met[((size_t)e * 9 + 6 + d) * NP3 + n] = Mh[src];
+      }
+  for (int s = 0; s < nSides; ++s)
+    for (int p = 0; p < NPT; ++p) {
+      const size_t src = (size_t)s * NPT + p;
+      for (int d = 0; d < 3; ++d) {
+        geo[((size_t)s * 10 + d) * NPT + p] = NormVec[3 * src + d];
+        geo[((size_t)s * 10 + 3 + d) * NPT + p] = TangVec1[3 * src + d];
+        geo[((size_t)s * 10 + 6 + d) * NPT + p] = TangVec2[3 * src + d];
+      }
+      geo[((size_t)s * 10 + 9) * NPT + p] = SurfElem[src];
+    }
+  return true;
+}
+
 }  // namespace host
 }  // namespace fluxo
 

@@ -335,7 +335,7 @@ volume_kernel(KParams P) {
     for (int v = 0; v < 5; ++v) P.Ut[o + v] = ut[v];
   } else {
     // LSERK-2reg stage: Ut_tmp = Ut - A*Ut_tmp (stage 1: Ut_tmp = Ut); U = U + b*dt*Ut_tmp
-    const double dt = P.dtDev ? P.dtDev[0] : P.dt;
+    const double dt = stage_dt(P, e);
     const double bdt = P.rkB * dt;
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -408,11 +408,7 @@ __global__ void __launch_bounds__(512) timestep_kernel(KParams P, unsigned long 
     if (isnan(dtV)) err = 4;
     dtE = fmin(dtE, dtV);
   }
-  if (err != 0) {
-    atomicMin(errKey, e * 8 + err);
-  } else {
-    atomicMin(dtBits, (unsigned long long)__double_as_longlong(dtE));
-  }
+  reduce_timestep(P, e, dtE, err, dtBits, errKey);
 }
 
 }  // namespace fluxo

@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 #include "common.cuh"
 
+struct fluxo_cfg;  // include/fluxo_gpu.h
+
 namespace fluxo {
 
 struct LaunchError {
@@ -53,5 +55,10 @@ cudaError_t launch_nfvse_fv(int RS, int NP, int nElems, int nSMs, cudaStream_t s
 // the message that fluxo_gpu_last_error(NULL, ...) returns (returns `code`).
 void basis_tables_for(int N, BasisTables& B);
 int record_unbound_error(int code, const std::string& msg);
+// Equation constants of the Euler / Navier-Stokes kernels, and the LSERK tables with the scaled
+// CFL / DFL numbers of a configuration (false for an unknown time_disc).
+void fill_ns_physics(KParams& P, const fluxo_cfg& c);
+bool time_disc_setup(const fluxo_cfg& c, double* RKA, double* RKb, double* RKc, int* nStages, double* CFLScale,
+                     double* DFLScale);
 
 }  // namespace fluxo

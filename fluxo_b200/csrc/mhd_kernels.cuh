@@ -473,7 +473,7 @@ __global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, FLUXO_MHD_VOL_MINB) 
 #pragma unroll
     for (int v = 0; v < NV; ++v) P.Ut[o + v] = ut[v];
   } else {
-    const double dt = P.dtDev ? P.dtDev[0] : P.dt;
+    const double dt = stage_dt(P, e);
     const double bdt = P.rkB * dt;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
@@ -545,8 +545,7 @@ __global__ void __launch_bounds__(512) timestep_kernel(KParams P, unsigned long 
   double dtE = P.CFLScale * 2. / (lam[0] + lam[1] + lam[2]);
   if (isnan(dtE)) err = 3;
   if (VISC && lam[3] > 0.) dtE = fmin(dtE, P.DFLScale * 4. / lam[3]);
-  if (err != 0) atomicMin(errKey, e * 8 + err);
-  else atomicMin(dtBits, (unsigned long long)__double_as_longlong(dtE));
+  reduce_timestep(P, e, dtE, err, dtBits, errKey);
 }
 
 }  // namespace mhd

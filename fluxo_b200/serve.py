@@ -1,0 +1,163 @@
+"""Served request stream: continuous batching of independent solves on one GPU.
+
+No counterpart in the reference (one solve per program).  Requests (a periodic-box Euler or
+Navier-Stokes solve: mesh arrays, initial state, end time) arrive over time; the server keeps
+their state on the device inside one ``Batch`` and advances all admitted requests together, one
+graph replay per time step.  A request is admitted when its device bytes fit the HBM budget next to
+the requests already running (first come, first served: a request that does not fit holds the ones
+behind it), and leaves the batch as soon as it reaches its end time, which frees its bytes for
+the next ones.  Each result is what the same solve gives alone (``DGOperator.time_disc``).
+"""
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Request:
+    """One solve: kernel configuration (a ``FluxoCfg``), reference-layout mesh arrays, initial U."""
+    rid: int
+    cfg: object
+    mesh: dict
+    U: np.ndarray
+    t_end: float
+    arrival: float = 0.0            # seconds after the start of the stream
+    dofs: int = 0
+    nbytes: int = 0
+
+
+@dataclass
+class Result:
+    rid: int
+    U: np.ndarray
+    t: float
+    steps: int
+    err: int
+    arrival: float
+    admitted: float
+    finished: float
+    dofs: int
+
+    @property
+    def time_to_solution(self):
+        return self.finished - self.arrival
+
+
+@dataclass
+class ServeStats:
+    results: list = field(default_factory=list)
+    wall: float = 0.0
+    rebuilds: int = 0
+    max_running: int = 0
+    max_bytes: int = 0
+
+    def dof_updates(self):
+        """DOFs x RHS evaluations of all finished requests (5 stages per LSERK4-5 step)."""
+        return sum(r.dofs * r.steps * 5 for r in self.results)
+
+    def summary(self):
+        tts = np.array([r.time_to_solution for r in self.results]) if self.results else np.zeros(1)
+        return {"requests": len(self.results), "wall_s": self.wall,
+                "dof_updates_per_s": self.dof_updates() / self.wall if self.wall > 0 else None,
+                "p50_s": float(np.percentile(tts, 50)), "p99_s": float(np.percentile(tts, 99)),
+                "mean_s": float(tts.mean()), "max_running": self.max_running, "max_device_bytes": self.max_bytes,
+                "failed": sum(1 for r in self.results if r.err)}
+
+
+class Server:
+    """Continuous batching over a ``Batch``: admission by HBM budget, eviction on completion.
+
+    ``batch`` is a ``fluxo_b200.batch.Batch`` (or an object with its methods); ``instance_bytes``
+    gives a request's device bytes; ``steps_per_poll`` time steps run between two admission rounds.
+    """
+
+    def __init__(self, batch, hbm_budget, instance_bytes, steps_per_poll=2, clock=time.perf_counter):
+        self.batch = batch
+        self.budget = int(hbm_budget)
+        self.instance_bytes = instance_bytes
+        self.steps_per_poll = int(steps_per_poll)
+        self.clock = clock
+        self.queue = deque()
+        self.running = {}           # batch id -> (request, admitted time)
+        self.used = 0
+
+    def submit(self, req):
+        if not req.nbytes:
+            nE = req.mesh["ElemToSide"].shape[0]
+            req.nbytes = self.instance_bytes(req.cfg, nE, req.mesh["SideToElem"].shape[0])
+            req.dofs = nE * (req.cfg.N + 1) ** 3
+        if req.nbytes > self.budget:
+            raise ValueError("request %d needs %d device bytes, more than the budget %d" %
+                             (req.rid, req.nbytes, self.budget))
+        self.queue.append(req)
+
+    def admit(self, now):
+        """Adds queued requests in arrival order while they fit the budget; returns how many."""
+        n = 0
+        while self.queue and self.used + self.queue[0].nbytes <= self.budget:
+            req = self.queue.popleft()
+            iid = self.batch.add(req.mesh, req.U, 0.0, req.t_end, cfg=req.cfg)
+            self.running[iid] = (req, now)
+            self.used += req.nbytes
+            n += 1
+        return n
+
+    def harvest(self, now, stats):
+        """Moves finished requests out of the batch (their result to the host)."""
+        for iid in list(self.running):
+            t, steps, done, err = self.batch.status(iid)
+            if not done:
+                continue
+            req, admitted = self.running.pop(iid)
+            U = self.batch.get_state(iid)
+            self.batch.remove(iid)
+            self.used -= req.nbytes
+            stats.results.append(Result(req.rid, U, t, steps, err, req.arrival, admitted, self.clock() - self._t0,
+                                        req.dofs))
+
+    def serve(self, requests, stats=None):
+        """Runs a stream to the end: each request becomes visible at its arrival time (seconds after
+        the call), all of them finish.  Returns ServeStats with per-request results."""
+        stats = stats or ServeStats()
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        self._t0 = self.clock()
+        while pending or self.queue or self.running:
+            now = self.clock() - self._t0
+            while pending and pending[0].arrival <= now:
+                self.submit(pending.popleft())
+            if self.admit(now):
+                stats.rebuilds += 1
+            stats.max_running = max(stats.max_running, len(self.running))
+            stats.max_bytes = max(stats.max_bytes, self.used)
+            if self.running:
+                self.batch.run(self.steps_per_poll)
+                self.harvest(self.clock() - self._t0, stats)
+            elif pending:
+                time.sleep(max(0.0, pending[0].arrival - (self.clock() - self._t0)))
+        stats.wall = self.clock() - self._t0
+        return stats
+
+
+def serve_one_at_a_time(requests, make_operator, clock=time.perf_counter):
+    """The plain path on the same stream: one solve at a time in arrival order (first come, first
+    served), each through its own operator (``DGOperator``: set_mesh, set_state, time_disc)."""
+    stats = ServeStats()
+    t0 = clock()
+    for req in sorted(requests, key=lambda r: r.arrival):
+        now = clock() - t0
+        if req.arrival > now:
+            time.sleep(req.arrival - now)
+        start = clock() - t0
+        op = make_operator(req.cfg)
+        op.set_mesh(req.mesh)
+        op.set_state(req.U)
+        t, steps, err = op.time_disc(0.0, req.t_end)
+        U = op.get_state()
+        op.close()
+        nE = req.mesh["ElemToSide"].shape[0]
+        stats.results.append(Result(req.rid, U, t, steps, err, req.arrival, start, clock() - t0,
+                                    nE * (req.cfg.N + 1) ** 3))
+    stats.wall = clock() - t0
+    return stats

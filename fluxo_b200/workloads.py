@@ -6,12 +6,22 @@
   amplitude 1e-3 at every node.  It is not one of the reference's ExactFunc cases (the closest are
   IniExactFunc 311/312/322 in equation/mhd/equation.f90:1248-1276), so it is fed identically to the
   oracle and the GPU.
-* ``fourier_instances``: the batched / served configurations' instances, periodic boxes with smooth
-  random-Fourier perturbations (|k| <= 4, amplitude 0.05) of density and velocity on rho = 1, p = 1.
+* ``batch_instance_specs`` / ``build_instance``: the batched configuration's instances, periodic
+  boxes [0,2]^3 with elements per direction from {4,6,8,12,16} and N from {3,4,5,7} drawn from one
+  seeded RNG, Euler or Navier-Stokes, and ``fourier_state`` initial data: smooth random-Fourier
+  perturbations (|k| <= 4, amplitude 0.05) of density and velocity on rho = 1, p = 1.
 """
 import numpy as np
 
 SEED = 20261203
+
+BOX_MIN, BOX_MAX = (0.0, 0.0, 0.0), (2.0, 2.0, 2.0)
+BATCH_ELEMS = (4, 6, 8, 12, 16)
+BATCH_N = (3, 4, 5, 7)
+# kernel configuration of the two equation systems in the batched / served mixes
+EULER_FIELDS = dict(eqn=0, riemann=1, volume_flux=10, kappa=1.4, cfl_scale=0.9, time_disc=0, ini_exact_func=0)
+NS_FIELDS = dict(eqn=1, riemann=44, volume_flux=5, lifting=1, lifting_var=3, visc=0, mu0=1.0 / 1600.0, Pr=0.72,
+                 kappa=1.4, cfl_scale=0.9, dfl_scale=0.4, time_disc=0, ini_exact_func=0)
 
 
 def mhd_prim_to_cons(prim, kappa, mu_0=1.0):
@@ -64,3 +74,55 @@ def fourier_state(xGP, xmin, xmax, rng, kmax=4, amplitude=0.05, kappa=1.4, nmode
     U[..., 1:4] = prim[..., 1:4] * prim[..., :1]
     U[..., 4] = prim[..., 4] / (kappa - 1.0) + 0.5 * prim[..., 0] * np.sum(prim[..., 1:4] ** 2, axis=-1)
     return U
+
+
+def batch_instance_specs(n=64, seed=SEED):
+    """The batched configuration: n instances drawn from one RNG (elements per direction, N,
+    equation system, and the seed of each instance's initial data)."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n):
+        e = int(rng.choice(BATCH_ELEMS))
+        N = int(rng.choice(BATCH_N))
+        eqn = int(rng.integers(0, 2))
+        specs.append(dict(index=i, elems=e, N=N, eqn=eqn, seed=int(rng.integers(0, 2 ** 31 - 1))))
+    return specs
+
+
+def instance_fields(spec):
+    """fluxo_cfg fields of an instance spec."""
+    f = dict(NS_FIELDS if spec["eqn"] == 1 else EULER_FIELDS)
+    f["N"] = spec["N"]
+    return f
+
+
+def build_instance(spec, mesh_cache=None):
+    """(mesh arrays, initial state) of an instance spec; meshes of equal (N, elements) are shared."""
+    from .solver import box_mesh
+
+    key = (spec["N"], spec["elems"])
+    mesh = None if mesh_cache is None else mesh_cache.get(key)
+    if mesh is None:
+        mesh = box_mesh(spec["N"], (spec["elems"],) * 3, BOX_MIN, BOX_MAX)
+        if mesh_cache is not None:
+            mesh_cache[key] = mesh
+    U = fourier_state(mesh["Elem_xGP"], BOX_MIN, BOX_MAX, np.random.default_rng(spec["seed"]))
+    return mesh, U
+
+
+def serve_request_specs(rate, duration, seed=SEED, elems=(4, 24), N=(3, 7), t_end=(0.05, 1.0)):
+    """The served configuration's request stream: Poisson arrivals at `rate` per second over
+    `duration` seconds; each request an Euler or Navier-Stokes periodic box with elements per
+    direction uniform in elems[0]..elems[1], N uniform in N[0]..N[1], end time log-uniform in
+    t_end, and its own seed for the ``fourier_state`` initial data."""
+    rng = np.random.default_rng(seed)
+    specs, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration:
+            break
+        specs.append(dict(index=len(specs), arrival=t, elems=int(rng.integers(elems[0], elems[1] + 1)),
+                          N=int(rng.integers(N[0], N[1] + 1)), eqn=int(rng.integers(0, 2)),
+                          t_end=float(np.exp(rng.uniform(np.log(t_end[0]), np.log(t_end[1])))),
+                          seed=int(rng.integers(0, 2 ** 31 - 1))))
+    return specs

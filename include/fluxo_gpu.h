@@ -191,6 +191,42 @@ int fluxo_gpu_destroy(fluxo_handle* h);
 int fluxo_gpu_last_error(fluxo_handle* h, char* buf, size_t len);
 
 /* ------------------------------------------------------------------------------------------
+ * Batched solves.  No counterpart in the reference, which runs one mesh per program
+ * (src/fluxo.f90: InitMesh .. TimeDisc): many independent Euler / Navier-Stokes instances
+ * (own mesh, N, fluxes, end time) advance together, each exactly as fluxo_gpu_time_disc would
+ * advance it alone (same kernels, same per-instance CALCTIMESTEP and dt clipping).
+ * Instances with the same kernel configuration (everything in fluxo_cfg except ini_* and device)
+ * share one launch per kernel; one step of all instances is one CUDA graph replay.
+ *   add:       takes the arrays of fluxo_gpu_set_mesh (no Elem_xGP: no source terms) and the
+ *              initial U; the instance joins at the next run.  maxIter < 0: no limit.
+ *   run:       up to nSteps steps of every unfinished instance; returns how many are unfinished.
+ *   status:    time, steps taken, finished flag and errType (as fluxo_gpu_time_disc).
+ *   get_state: the instance's U (host layout of fluxo_gpu_get_state); set_state overwrites it.
+ *   remove:    frees the instance's slot at the next run.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct fluxo_batch fluxo_batch;
+int fluxo_batch_create(int device, fluxo_batch** out);
+int fluxo_batch_add(fluxo_batch* b, const fluxo_cfg* cfg, int nElems, int nSides, const int* SideToElem,
+                    const int* ElemToSide, const double* Metrics_fTilde, const double* Metrics_gTilde,
+                    const double* Metrics_hTilde, const double* sJ, const double* NormVec,
+                    const double* TangVec1, const double* TangVec2, const double* SurfElem, const double* U,
+                    double t, double tEnd, int maxIter, int* id);
+int fluxo_batch_run(fluxo_batch* b, int nSteps, int* nRunning);
+int fluxo_batch_status(fluxo_batch* b, int id, double* t, int* nIter, int* done, int* errType);
+int fluxo_batch_get_state(fluxo_batch* b, int id, double* U);
+/* Overwrites the instance's U (its time and step count stay). */
+int fluxo_batch_set_state(fluxo_batch* b, int id, const double* U);
+int fluxo_batch_remove(fluxo_batch* b, int id);
+/* Groups with elements, placed instances and the device bytes they occupy. */
+int fluxo_batch_info(fluxo_batch* b, int* nGroups, int* nInstances, size_t* deviceBytes);
+/* The stream all of the batch's GPU work runs on (for events around fluxo_batch_run). */
+int fluxo_batch_stream(fluxo_batch* b, void** stream);
+/* Device bytes one instance of this configuration and mesh size occupies (admission control). */
+int fluxo_batch_instance_bytes(const fluxo_cfg* cfg, int nElems, int nSides, size_t* bytes);
+int fluxo_batch_last_error(fluxo_batch* b, char* buf, size_t len);
+int fluxo_batch_destroy(fluxo_batch* b);
+
+/* ------------------------------------------------------------------------------------------
  * Host-side setup (no GPU needed).  The reference builds these arrays in InitMesh /
  * CalcMetrics from an HDF5 (HOPR) mesh; here they are generated for a periodic box
  * of nx*ny*nz hexahedra whose NGeo node coordinates are deformed by

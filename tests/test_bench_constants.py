@@ -39,3 +39,18 @@ def test_mhd_falg_constants_match_oracle_count():
     assert phases["nfvse"] == 0.0
     for k, v in bench.MHD_FALG_PER_DOF.items():
         assert abs(phases[k] - v) < 1e-9, k
+
+
+def test_batch_falg_constants_match_oracle_count():
+    """The batched configuration's per-(equation, N) counts, on a 2^3 instance with the mix's data."""
+    from oracle.oracle import OracleCase, _lib
+    from fluxo_b200.workloads import BOX_MAX, BOX_MIN, SEED, fourier_state, instance_fields
+
+    for (eqn, N), v in bench.BATCH_FALG_PER_DOF.items():
+        c = OracleCase(counting=True, nElems=(2, 2, 2), xmin=BOX_MIN, xmax=BOX_MAX, NGeo=1, deform_amp=0.0,
+                       **instance_fields(dict(N=N, eqn=eqn)))
+        c.set_U(fourier_state(c.mesh()["Elem_xGP"], BOX_MIN, BOX_MAX, np.random.default_rng(SEED)))
+        lib = _lib(counting=True)
+        lib.orc_reset_flops()
+        c.dg_time_derivative(0.0)
+        assert abs(lib.orc_flops() / (c.nElems * c.np ** 3) - v) < 1e-9, (eqn, N)

@@ -1,0 +1,108 @@
+"""Host logic of the served request stream (fluxo_b200.serve) on a fake batch, no GPU:
+admission by HBM budget in arrival order, eviction on completion, result bookkeeping."""
+import numpy as np
+import pytest
+
+from fluxo_b200.serve import Request, Server, ServeStats
+
+
+class FakeCfg:
+    def __init__(self, N):
+        self.N = N
+
+
+class FakeBatch:
+    """Each instance takes ceil(t_end / dt) steps; records the admission order."""
+
+    def __init__(self, dt=0.1):
+        self.dt = dt
+        self.inst = {}
+        self.next = 1
+        self.order = []
+        self.live_bytes = []
+
+    def add(self, mesh, U, t, t_end, cfg=None):
+        iid = self.next
+        self.next += 1
+        self.inst[iid] = dict(U=U.copy(), t=t, t_end=t_end, steps=0, done=False)
+        self.order.append(int(U.ravel()[0]))
+        return iid
+
+    def run(self, k):
+        for s in self.inst.values():
+            for _ in range(k):
+                if s["done"]:
+                    break
+                s["t"] = min(s["t"] + self.dt, s["t_end"])
+                s["steps"] += 1
+                s["U"] += 1.0
+                s["done"] = s["t"] >= s["t_end"]
+        return sum(not s["done"] for s in self.inst.values())
+
+    def status(self, iid):
+        s = self.inst[iid]
+        return s["t"], s["steps"], s["done"], 0
+
+    def get_state(self, iid):
+        return self.inst[iid]["U"].copy()
+
+    def remove(self, iid):
+        del self.inst[iid]
+
+
+def mesh(nE):
+    return {"ElemToSide": np.zeros((nE, 6, 2), np.int32), "SideToElem": np.zeros((3 * nE, 5), np.int32)}
+
+
+def fake_bytes(cfg, nE, nS):
+    return 1000 * nE
+
+
+def make_requests(n, seed=0):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(n):
+        nE = int(rng.integers(1, 9))
+        reqs.append(Request(rid=i, cfg=FakeCfg(3), mesh=mesh(nE), U=np.full(4, float(i)),
+                            t_end=float(rng.uniform(0.1, 1.0)), arrival=float(i) * 1e-7))
+    return reqs
+
+
+class CountingServer(Server):
+    def admit(self, now):
+        n = super().admit(now)
+        assert self.used <= self.budget
+        return n
+
+
+def test_admission_respects_budget_and_order():
+    fb = FakeBatch()
+    srv = CountingServer(fb, hbm_budget=12000, instance_bytes=fake_bytes, steps_per_poll=1)
+    reqs = make_requests(40)
+    stats = srv.serve(reqs)
+    assert len(stats.results) == 40
+    assert fb.order == list(range(40))                 # first come, first served
+    assert stats.max_bytes <= 12000 and stats.max_running >= 2
+    assert not fb.inst and srv.used == 0               # every request left the batch
+    for r in stats.results:
+        req = reqs[r.rid]
+        steps = int(np.ceil(req.t_end / 0.1 - 1e-12))
+        assert r.steps == steps and r.t == pytest.approx(req.t_end)
+        assert np.array_equal(r.U, req.U + steps)      # the result is the request's own state
+        assert r.finished >= r.admitted >= r.arrival - 1e-9
+        assert r.dofs == req.mesh["ElemToSide"].shape[0] * 64
+    s = stats.summary()
+    assert s["requests"] == 40 and s["p99_s"] >= s["p50_s"] >= 0 and s["failed"] == 0
+
+
+def test_request_larger_than_budget_is_refused():
+    srv = Server(FakeBatch(), hbm_budget=5000, instance_bytes=fake_bytes)
+    with pytest.raises(ValueError):
+        srv.submit(Request(rid=0, cfg=FakeCfg(3), mesh=mesh(6), U=np.zeros(4), t_end=1.0))
+
+
+def test_stats_throughput_counts_rhs_evaluations():
+    st = ServeStats()
+    srv = Server(FakeBatch(dt=0.25), hbm_budget=10 ** 9, instance_bytes=fake_bytes)
+    stats = srv.serve([Request(rid=0, cfg=FakeCfg(3), mesh=mesh(2), U=np.zeros(4), t_end=1.0)], st)
+    assert stats.dof_updates() == 2 * 64 * 4 * 5
