@@ -4,7 +4,9 @@ Workload (the configuration the reference's PID metric is quoted on here): compr
 Navier-Stokes Taylor-Green vortex, FP64, N=7, 32^3 hexahedra on [-pi,pi]^3 with interior nodes
 deformed by 0.05*sin(x)sin(y)sin(z) (NGeo=2, curved metrics), Re=1600 (mu0=1/1600), Ma=0.1,
 Pr=0.72, BR1 lifting of the entropy variables, EC-KEP split-form volume flux (VolumeFlux=5),
-entropy-stable matrix-dissipation surface flux (Riemann=44), Carpenter LSERK4-5, CFL 0.9, DFL 0.4.
+entropy-stable matrix-dissipation surface flux (Riemann=44), Carpenter LSERK4-5, CFLscale 0.5, DFLscale 0.5
+(the reference's own TGV setup, ini/navstokes/tgv/parameter.ini; at CFLscale 0.9 the scheme is unstable
+on this case: a 1e-14 perturbation of the initial state grows to 1e-2 in 60 steps).
 Synthetic data: the mesh and the initial state are generated in-code (no mesh file, no dataset).
 
 One step = CALCTIMESTEP + one 5-stage LSERK step (5 right-hand sides).  The metric is the
@@ -68,27 +70,30 @@ MHD_METRIC = ("PID ns/DOF/RHS, resistive MHD+GLM Orszag-Tang N=4 24^3 curved, De
 
 
 # The batched configuration (--workload batch): F_alg per DOF of one RHS for each (equation, N) of the
-# mix (Euler: EC flux + LLF; Navier-Stokes: EC-KEP + Riemann 44, BR1), from the oracle's counting
+# mix (EC-KEP volume flux + Riemann 44 for both; Navier-Stokes with BR1), from the oracle's counting
 # build on a 2^3 instance with the mix's initial data (fourier_state, seed SEED).
 BATCH_FALG_PER_DOF = {
-    (0, 3): 684.7734375, (0, 4): 830.796, (0, 5): 985.3472222222222, (0, 7): 1306.18359375,
+    (0, 3): 783.5859375, (0, 4): 877.212, (0, 5): 992.2013888888889, (0, 7): 1249.1220703125,
     (1, 3): 1632.5859375, (1, 4): 1738.812, (1, 5): 1882.201388888889, (1, 7): 2219.6220703125,
 }
 BATCH_METRIC = ("aggregate DOF-updates/s (DOFs x RHS evaluations per second), 64 uneven Euler/NS periodic-box "
                 "instances (4^3..16^3 elements, N in {3,4,5,7}) batched, vs one at a time")
+SERVE_METRIC = ("served DOF-updates/s with p50/p99 time-to-solution, Poisson stream of Euler/NS periodic-box "
+                "solves (4^3..24^3 elements, N 3..7, end time log-uniform [0.05,1]), continuous batching vs one "
+                "at a time")
 
 
 def mhd_workload(elems=24, N=4):
     return dict(N=N, elems=(elems,) * 3, xmin=(0.0,) * 3, xmax=(2 * np.pi,) * 3, NGeo=2, deform_amp=0.05,
                 eqn=3, lifting=1, lifting_var=3, riemann=14, volume_flux=10, kappa=5.0 / 3.0, eta=1e-3, mu0=0.0,
                 noncons=1, nc_glm=0, glm_scale=0.5, nfvse=1, compute_alpha=1, alpha_max=0.5, alpha_min=0.01,
-                space_prop_sweeps=1, cfl_scale=0.9, dfl_scale=0.4, time_disc=0)
+                space_prop_sweeps=1, cfl_scale=0.5, dfl_scale=0.5, time_disc=0)  # as ini/mhd/orszagtang
 
 
 def workload(elems=32, N=7):
     return dict(N=N, elems=(elems,) * 3, xmin=(-np.pi,) * 3, xmax=(np.pi,) * 3, NGeo=2, deform_amp=0.05,
                 eqn=1, lifting=1, lifting_var=3, visc=0, riemann=44, volume_flux=5, mu0=1.0 / 1600.0, Pr=0.72,
-                kappa=1.4, ini_exact_func=7, cfl_scale=0.9, dfl_scale=0.4, time_disc=0)
+                kappa=1.4, ini_exact_func=7, cfl_scale=0.5, dfl_scale=0.5, time_disc=0)
 
 
 def config_dict(w, n_gpus, steps):
@@ -190,7 +195,8 @@ def cpu_baseline(threads, seconds=15.0):
     w = workload(elems=4)
     c = OracleCase(N=w["N"], nElems=w["elems"], xmin=w["xmin"], xmax=w["xmax"], NGeo=w["NGeo"],
                    deform_amp=w["deform_amp"], eqn=1, lifting=1, lifting_var=3, mu0=w["mu0"], riemann=44,
-                   volume_flux=5, ini_exact_func=7, cfl_scale=0.9, dfl_scale=0.4)
+                   volume_flux=5, ini_exact_func=7, cfl_scale=w["cfl_scale"],
+                   dfl_scale=w["dfl_scale"])
     U0 = c.get_U()
     t_sim, n = c.run(0.0, 1e9, max_iter=1)  # warm-up
     if n != 1:
@@ -372,10 +378,20 @@ def run_fluxo(args):
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kinds.items()},
             "rhs_roofline_frac": (falg_rhs * nd * rhs / (ms * 1e-3) / 1e12) / peak,
             "setup_s": setup_s}
+    if not mhd:
+        line["volume_shape"] = shape_dict(w["N"], w["volume_flux"], True)
     if world == 1 and not args.no_cpu and not mhd:
         line["cpu_baseline"] = cpu_baseline_subprocess(os.cpu_count() or 1, seconds=args.cpu_seconds)
     print(json.dumps(line))
     op.close()
+
+
+def shape_dict(N, volume_flux, visc):
+    """The volume kernel's launch shape the autotuner chose (index -1: not tuned)."""
+    from fluxo_b200.solver import volume_shape
+
+    count, index, epb, lpw = volume_shape(N, volume_flux, visc)
+    return {"candidates": count, "chosen": index, "elements_per_block": epb, "lines_per_warp": lpw}
 
 
 def batch_falg(specs):
@@ -503,7 +519,94 @@ def run_batch(args):
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None},
             "one_at_a_time": seq, "batched_over_one_at_a_time": (value / seq["value"]) if seq else None,
             "e2e": e2e, "gpu_launches": batch_launches_per_step(specs) * args.steps, "clocks": clk.summary(),
-            "setup_s": setup_s}
+            "setup_s": setup_s,
+            "volume_shapes": {"%s_N%d" % ("ns" if eqn else "euler", N): shape_dict(N, 5, eqn == 1)
+                              for eqn, N in sorted({(s["eqn"], s["N"]) for s in specs})}}
+    print(json.dumps(line))
+
+
+def run_serve(args):
+    """The served configuration: a Poisson stream of solve requests, continuous batching under an HBM
+    budget (fluxo_b200.serve.Server) vs the plain path serving them one at a time, first come first
+    served.  Both arms see the same requests at the same arrival times (wall clock from the start of
+    the arm); time-to-solution = completion on the host - arrival."""
+    import torch
+
+    import fluxo_b200 as fb
+    from fluxo_b200.batch import Batch, instance_bytes
+    from fluxo_b200.serve import Request, Server, serve_one_at_a_time
+    from fluxo_b200.workloads import SEED, build_instance, instance_fields, serve_request_specs
+
+    world, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    t0 = time.time()
+    specs = serve_request_specs(args.rate, args.duration, seed=SEED + rank)
+    cache, reqs = {}, []
+    for s in specs:
+        mesh, U = build_instance(s, cache)
+        reqs.append(Request(rid=s["index"], cfg=fb.make_cfg(device=local, **instance_fields(s)), mesh=mesh, U=U,
+                            t_end=s["t_end"], arrival=s["arrival"]))
+    del cache
+    setup_s = time.time() - t0
+    budget = int(args.hbm_budget_gb * 1e9)
+
+    # warm-up: a short stream of the first requests (library, context and graph paths), untimed
+    warm = [Request(rid=r.rid, cfg=r.cfg, mesh=r.mesh, U=r.U, t_end=r.t_end * 0.05, arrival=0.0) for r in reqs[:3]]
+    b = Batch(device=local)
+    Server(b, budget, instance_bytes).serve(warm)
+    b.close()
+    serve_one_at_a_time(warm[:1], lambda cfg: fb.DGOperator(cfg=cfg))
+
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    b = Batch(device=local)
+    srv = Server(b, budget, instance_bytes, steps_per_poll=args.poll_steps)
+    with ClockSampler(local) as clk:
+        served = srv.serve(reqs)
+        torch.cuda.synchronize(dev)
+    b.close()
+    barrier(world)
+    plain = None
+    if not args.no_sequential:
+        plain = serve_one_at_a_time(reqs, lambda cfg: fb.DGOperator(cfg=cfg))
+        torch.cuda.synchronize(dev)
+    barrier(world)
+    s_sum = served.summary()
+    work = served.dof_updates()
+    wall = max_over_ranks(served.wall, world, dev)
+    value = world * work / wall
+    p_sum = plain.summary() if plain else None
+    if plain:
+        p_sum["dof_updates_per_s"] = world * plain.dof_updates() / max_over_ranks(plain.wall, world, dev)
+    if rank != 0:
+        return
+    assert s_sum["requests"] == len(reqs), (s_sum["requests"], len(reqs))
+    failed = [(r.rid, r.err, r.steps, r.t) for r in served.results if r.err]
+    if failed:  # CALCTIMESTEP stopped these solves (errType); the plain path must stop them alike
+        print("stopped requests (rid, errType, steps, t):", failed, file=sys.stderr)
+        print("their specs:", [specs[f[0]] for f in failed], file=sys.stderr)
+    dofs = [r.dofs for r in reqs]
+    config = {"workload": "served_stream_poisson_%greq_per_s_%gs" % (args.rate, args.duration),
+              "requests": len(reqs), "rate_per_s": args.rate, "duration_s": args.duration,
+              "elements": "per direction 4..24", "N": "3..7", "t_end": "log-uniform [0.05, 1]",
+              "dofs_per_request": "%d..%d" % (min(dofs), max(dofs)), "hbm_budget_bytes": budget,
+              "max_running": s_sum["max_running"], "max_device_bytes": s_sum["max_device_bytes"],
+              "graph_rebuilds": served.rebuilds, "steps_per_poll": args.poll_steps,
+              "stopped_by_calctimestep": len(failed),
+              "parallelism": "replicas x%d (own stream per rank)" % world}
+    line = {"metric": SERVE_METRIC, "value": value, "unit": "DOF-updates/s", "n_gpus": world, "steps": len(reqs),
+            "warmup": len(warm), "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
+            "p50_s": s_sum["p50_s"], "p99_s": s_sum["p99_s"], "mean_s": s_sum["mean_s"], "wall_s": wall,
+            "one_at_a_time": p_sum,
+            "served_over_one_at_a_time": (value / p_sum["dof_updates_per_s"]) if p_sum else None,
+            "e2e": {"value": value, "unit": "DOF-updates/s",
+                    "h2d_bytes_per_step": int(np.mean([r.U.nbytes for r in reqs])),
+                    "d2h_bytes_per_step": int(np.mean([r.U.nbytes for r in reqs])),
+                    "note": "a step is one request: its mesh and state go to the device at admission, its "
+                            "state comes back at completion, all inside the served wall time"},
+            "clocks": clk.summary(), "setup_s": setup_s}
     print(json.dumps(line))
 
 
@@ -513,11 +616,16 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fluxo", choices=("fluxo", "reference"))
-    ap.add_argument("--workload", default="tgv", choices=("tgv", "mhd", "batch"),
+    ap.add_argument("--workload", default="tgv", choices=("tgv", "mhd", "batch", "serve"),
                     help="tgv: the headline Navier-Stokes configuration; mhd: the resistive-MHD configuration; "
-                         "batch: uneven Euler/NS instances batched vs one at a time")
+                         "batch: uneven Euler/NS instances batched vs one at a time; serve: Poisson request "
+                         "stream, continuous batching vs one at a time")
     ap.add_argument("--instances", type=int, default=64, help="batch: number of instances")
-    ap.add_argument("--no-sequential", action="store_true", help="batch: skip the one-at-a-time comparison")
+    ap.add_argument("--no-sequential", action="store_true", help="batch/serve: skip the one-at-a-time comparison")
+    ap.add_argument("--rate", type=float, default=20.0, help="serve: requests per second")
+    ap.add_argument("--duration", type=float, default=3.0, help="serve: seconds of arrivals")
+    ap.add_argument("--hbm-budget-gb", type=float, default=64.0, help="serve: device bytes for admitted requests")
+    ap.add_argument("--poll-steps", type=int, default=2, help="serve: time steps between admission rounds")
     ap.add_argument("--elems", type=int, default=0, help="elements per direction (0: the configuration's)")
     ap.add_argument("--N", type=int, default=0, help="polynomial degree (0: the configuration's)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -528,6 +636,8 @@ def main():
         run_reference(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_fluxo(args)
     if int(os.environ.get("WORLD_SIZE", "1")) > 1:

@@ -77,7 +77,8 @@ EXPORTS = [
     "fluxo_gpu_time_disc", "fluxo_gpu_device_buffers", "fluxo_gpu_launch_count", "fluxo_gpu_destroy",
     "fluxo_gpu_last_error", "fluxo_gpu_set_profiling", "fluxo_gpu_get_profile", "fluxo_gpu_fp64_peak",
     "fluxo_host_box_sizes", "fluxo_host_box_mesh", "fluxo_host_exact_func", "fluxo_gpu_dg_time_derivative_noalloc",
-    "fluxo_gpu_set_glm_ch", "fluxo_gpu_get_glm_ch", "fluxo_gpu_get_alpha",
+    "fluxo_gpu_set_glm_ch", "fluxo_gpu_get_glm_ch", "fluxo_gpu_get_alpha", "fluxo_gpu_volume_shape",
+    "fluxo_gpu_set_volume_shape",
     "fluxo_batch_create", "fluxo_batch_add", "fluxo_batch_run", "fluxo_batch_status", "fluxo_batch_get_state",
     "fluxo_batch_set_state",
     "fluxo_batch_remove", "fluxo_batch_info", "fluxo_batch_stream", "fluxo_batch_instance_bytes",
@@ -124,6 +125,8 @@ def load():
     lib.fluxo_gpu_set_glm_ch.argtypes = [vp, d]
     lib.fluxo_gpu_get_glm_ch.argtypes = [vp, P(d)]
     lib.fluxo_gpu_get_alpha.argtypes = [vp, vp]
+    lib.fluxo_gpu_volume_shape.argtypes = [i, i, i, P(i), P(i), P(i), P(i)]
+    lib.fluxo_gpu_set_volume_shape.argtypes = [i, i, i, i]
     sz = ctypes.c_size_t
     lib.fluxo_batch_create.argtypes = [i, P(vp)]
     lib.fluxo_batch_add.argtypes = [vp, P(FluxoCfg), i, i] + [vp] * 11 + [d, d, i, P(i)]

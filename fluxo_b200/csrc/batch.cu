@@ -399,6 +399,10 @@ int commit(fluxo_batch* b) {
     BATCH_CUDA(b, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     b->joins.push_back(ev);
   }
+  // launch shapes of the volume kernels, tuned on the group's own arrays before the capture
+  for (const Group& g : b->groups)
+    if (g.nElems > 0 && volume_shape(g.NP, g.key.volume_flux, g.visc) < 0)
+      BATCH_CUDA(b, tune_volume(g.NP, g.key.volume_flux, g.visc, g.nElems, s, group_params(b, g)));
   if (nInst > 0) {
     BATCH_CUDA(b, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = enqueue_step(b);

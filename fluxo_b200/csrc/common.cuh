@@ -15,6 +15,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "side_index.h"
+
 #define FLUXO_NPMAX 9  // N <= 8
 
 namespace fluxo {

@@ -17,6 +17,7 @@
 #include "host_basis.h"
 #include "host_setup.h"
 #include "launch.h"
+#include "vol_shapes.h"
 
 using namespace fluxo;
 
@@ -284,6 +285,10 @@ int rhs(fluxo_handle* h, KParams P) {
   {
     ProfScope ps(h, 2);
     FLUXO_CUDA(h, launch_face_flux(h->cfg.riemann, h->visc, h->NP, h->nSides, s, P));
+  }
+  if (volume_shape(h->NP, h->cfg.volume_flux, h->visc) < 0) {  // first RHS of this (N, flux, visc)
+    FLUXO_CUDA(h, tune_volume(h->NP, h->cfg.volume_flux, h->visc, h->nElems, s, P));
+    if (volume_shape_count(h->NP) > 1) h->launches += 4 * volume_shape_count(h->NP);
   }
   {
     ProfScope ps(h, 3);
@@ -737,6 +742,25 @@ int fluxo_gpu_get_profile(fluxo_handle* h, int kind, double* total_ms, uint64_t*
   if (total_ms) *total_ms = tot;
   if (count) *count = h->prof[kind].size();
   h->prof[kind].clear();
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_volume_shape(int N, int volume_flux, int visc, int* count, int* index, int* epb, int* lpw) {
+  const int NP = N + 1;
+  if (N < 1 || N > 8 || !volume_flux_supported(volume_flux))
+    return fail(nullptr, FLUXO_EINVAL_CFG, "volume_shape: unsupported N or volume flux");
+  const int c = volume_shape_count(NP), i = volume_shape(NP, volume_flux, visc != 0);
+  if (count) *count = c;
+  if (index) *index = i;
+  const int k = i < 0 ? 0 : i;
+  if (epb) *epb = kVolShapes[NP][k].epb;
+  if (lpw) *lpw = kVolShapes[NP][k].lpw;
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_set_volume_shape(int N, int volume_flux, int visc, int index) {
+  if (N < 1 || N > 8 || !volume_flux_supported(volume_flux) || !pin_volume_shape(N + 1, volume_flux, visc != 0, index))
+    return fail(nullptr, FLUXO_EINVAL_CFG, "set_volume_shape: unsupported N, volume flux or shape index");
   return FLUXO_OK;
 }
 

@@ -12,13 +12,6 @@
 
 namespace fluxo {
 
-__device__ __forceinline__ int side_plane_coords(int s, int i, int j, int k, int NP) {
-  // in-plane volume coordinates of a node on local side s (see BasisTables::v2s)
-  if (s == XI_MINUS || s == XI_PLUS) return j + NP * k;
-  if (s == ETA_MINUS || s == ETA_PLUS) return i + NP * k;
-  return i + NP * j;
-}
-
 // Up to three local sides touched by volume node (i,j,k); returns the count.
 __device__ __forceinline__ int boundary_sides(int i, int j, int k, int N, int* s) {
   int c = 0;
@@ -52,8 +45,9 @@ __global__ void face_flux_kernel(KParams P, int NP) {
     const int* se5 = P.s2e + 5 * side;
     eM = se5[0]; eS = se5[1];
     int lsM = se5[2], lsS = se5[3], fl = se5[4];
-    nM = P.basis->s2v[lsM - 1][0][pt];
-    nS = P.basis->s2v[lsS - 1][fl][pt];
+    const int p = pt % NP, q = pt / NP;
+    nM = side_node(NP - 1, p, q, 0, lsM);
+    nS = side_node(NP - 1, p, q, fl, lsS);
     const double* UM = P.U + 5 * ((size_t)eM * NP * NP * NP + nM);
     const double* US = P.U + 5 * ((size_t)eS * NP * NP * NP + nS);
     const double* g = P.facegeo + (size_t)side * 10 * npts + pt;
@@ -124,8 +118,9 @@ static __global__ void lift_flux_kernel(KParams P, int NP, double* lf) {
   if (idx >= (size_t)P.nSides * npts) return;
   const int side = (int)(idx / npts), pt = (int)(idx - (size_t)side * npts);
   const int* se5 = P.s2e + 5 * side;
-  int nM = P.basis->s2v[se5[2] - 1][0][pt];
-  int nS = P.basis->s2v[se5[3] - 1][se5[4]][pt];
+  const int p = pt % NP, q = pt / NP;
+  const int nM = side_node(NP - 1, p, q, 0, se5[2]);
+  const int nS = side_node(NP - 1, p, q, se5[4], se5[3]);
   const double* UM = P.U + 5 * ((size_t)se5[0] * NP * NP * NP + nM);
   const double* US = P.U + 5 * ((size_t)se5[1] * NP * NP * NP + nS);
   double uM[5], uS[5], VM[5], VS[5];
@@ -148,11 +143,30 @@ static __global__ void lift_flux_kernel(KParams P, int NP, double* lf) {
 // pair of the line exactly once (the reference's symmetric reuse, flux_average.f90:232-243):
 // in round d thread p takes the pair (p, p+d mod NP); its own contribution stays in registers,
 // the partner's goes to a shared accumulator, and no two threads of a round touch the same
-// accumulator.  Lines are contiguous in the thread index in every direction, so for NP = 2, 4, 8 a
-// line lives in one warp and rounds need only a warp barrier.
+// accumulator.
+//
+// The partner's share of each pair flux travels by warp shuffle to the partner's lane, so a line must
+// live in one warp.  Launch shape (template parameters, chosen per N by the launcher's autotuner):
+// EPB elements per block and the line-to-warp schedule of the pair phase,
+//   LPW = 0: thread t of an element takes node t's line position in every direction (lines are
+//            contiguous in the thread index; needs NP | 32);
+//   LPW > 0: LPW lines per warp, line slot s on lanes [s*G, s*G+NP) with G = 32/LPW, the other lanes
+//            idle; the block then has more threads than nodes and the node phases use the first
+//            EPB*NP^3 threads.
+// Every schedule adds the same terms in the same order, so the launch shape does not change a bit of
+// the result.
 // ------------------------------------------------------------------------------------------------
 template <int NP>
 __host__ __device__ constexpr int vol_epb() { return (256 / (NP * NP * NP)) > 0 ? (256 / (NP * NP * NP)) : 1; }
+
+template <int NP, int EPB, int LPW, int MINB_ = 0>
+struct VolShape {
+  static constexpr int NP3 = NP * NP * NP, NPT = NP * NP;
+  static constexpr int WPE = LPW > 0 ? (NPT + LPW - 1) / LPW : 0;  // warps per element (LPW > 0)
+  static constexpr int THREADS = LPW > 0 ? EPB * WPE * 32 : EPB * NP3;
+  // resident blocks per SM the register allocation must allow
+  static constexpr int MINB = MINB_ > 0 ? MINB_ : (THREADS > 512 ? 1 : 2);
+};
 
 // Padded slot of node n in the shared record/accumulator arrays: one spare slot every 16 nodes
 // spreads the eta- and zeta-lines (node strides NP and NP^2) over the shared-memory banks.
@@ -161,32 +175,26 @@ __host__ __device__ constexpr int vol_slot(int n) { return n + (n >> 4); }
 template <int NP>
 __host__ __device__ constexpr int vol_slots() { return vol_slot(NP * NP * NP - 1) + 1; }
 
-template <int NP, int VF>
+template <int NP, int VF, int EPB = vol_epb<NP>()>
 __host__ __device__ constexpr size_t vol_smem_bytes() {
-  return sizeof(double) * (size_t)(2 * NP * NP + vol_epb<NP>() * (VolRec<VF>::RS + 5) * vol_slots<NP>());
+  return sizeof(double) * (size_t)(2 * NP * NP + EPB * (VolRec<VF>::RS + 5) * vol_slots<NP>());
 }
 
-template <int NP>
-__device__ __forceinline__ void line_sync() {
-  if constexpr (32 % NP == 0) __syncwarp();
-  else __syncthreads();
-}
-
-template <int NP, int VF, bool VISC>
-#ifndef FLUXO_VOL_MINB
-#define FLUXO_VOL_MINB 2  // resident blocks per SM the register allocation must allow
-#endif
-__global__ void __launch_bounds__(vol_epb<NP>() * NP * NP * NP, FLUXO_VOL_MINB)
+template <int NP, int VF, bool VISC, int EPB, int LPW, int MINB, int OWNSM>
+__global__ void __launch_bounds__(VolShape<NP, EPB, LPW>::THREADS, VolShape<NP, EPB, LPW, MINB>::MINB)
 volume_kernel(KParams P) {
   if (halted(P)) return;
-  constexpr int NP3 = NP * NP * NP, N = NP - 1, NPT = NP * NP, EPB = vol_epb<NP>();
+  constexpr int NP3 = NP * NP * NP, N = NP - 1, NPT = NP * NP;
   constexpr int RS = VolRec<VF>::RS, NQ = VolRec<VF>::NQ;
+  static_assert(LPW > 0 ? (32 / LPW >= NP) : (32 % NP == 0), "a line must fit its lanes of one warp");
   extern __shared__ double smem[];
   double* sDvs = smem;         // Dvolsurf(i,l) at [i*NP+l]
   double* sDhat = sDvs + NPT;  // D_hat(i,l)
-  const int eb = threadIdx.x / NP3, t = threadIdx.x - eb * NP3;
+  // node phases: thread -> (element slot eb, node t); with PACK the threads past EPB*NP3 idle
+  const bool nodeThread = threadIdx.x < EPB * NP3;
+  const int eb = nodeThread ? threadIdx.x / NP3 : 0, t = nodeThread ? threadIdx.x - eb * NP3 : 0;
   const int e = blockIdx.x * EPB + eb;
-  const bool valid = e < P.nElems;
+  const bool valid = nodeThread && e < P.nElems;
   constexpr int NS = vol_slots<NP>();
   double* rec = sDhat + NPT + (size_t)eb * (RS + 5) * NS;  // [slot][RS]
   double* acc = rec + (size_t)RS * NS;                     // [slot][5]
@@ -217,76 +225,71 @@ volume_kernel(KParams P) {
   __syncthreads();
   // split-form volume integral, line by line
   {
-    const int p = t % NP, Ln = t / NP, la = Ln % NP, lb = Ln / NP;
+    // this thread's (element slot pe, line Ln, position p) in the pair phase; lv: it holds a position
+    // of a line of an existing element (idle lanes keep in-range indexes and only join the shuffles)
+    int pe, p, Ln, lbase;
+    bool lv;
+    const int lane = threadIdx.x & 31;
+    if constexpr (LPW == 0) {
+      pe = eb; p = t % NP; Ln = t / NP; lv = valid; lbase = lane - p;
+    } else {
+      constexpr int G = 32 / LPW, WPE = VolShape<NP, EPB, LPW>::WPE;
+      const int wi = threadIdx.x >> 5, slot = lane / G;
+      pe = wi / WPE;
+      p = lane - slot * G;
+      Ln = (wi - pe * WPE) * LPW + slot;
+      lv = slot < LPW && p < NP && Ln < NPT && (int)blockIdx.x * EPB + pe < P.nElems;
+      lbase = slot * G;
+      if (!lv) { p = 0; Ln = 0; }
+    }
+    const int la = Ln % NP, lb = Ln / NP;
+    double* prec = sDhat + NPT + (size_t)pe * (RS + 5) * NS;
+    double* pacc = prec + (size_t)RS * NS;
 #pragma unroll 1
     for (int dir = 0; dir < 3; ++dir) {
       const int stride = dir == 0 ? 1 : (dir == 1 ? NP : NPT);
       const int base = dir == 0 ? NP * (la + NP * lb) : (dir == 1 ? la + NPT * lb : la + NP * lb);
       const int own = base + p * stride, os = vol_slot(own);
+      // own record: held in registers for all rounds, or (OWNSM) read from shared memory in every
+      // round, which frees 2*(NQ+3) registers
       double ro[NQ], mo[3], racc[5] = {0., 0., 0., 0., 0.};
-      if (valid) {
+      if (!OWNSM && lv) {
 #pragma unroll
-        for (int z = 0; z < NQ; ++z) ro[z] = rec[os * RS + z];
+        for (int z = 0; z < NQ; ++z) ro[z] = prec[os * RS + z];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) mo[c] = rec[os * RS + NQ + 3 * dir + c];
+        for (int c = 0; c < 3; ++c) mo[c] = prec[os * RS + NQ + 3 * dir + c];
       }
-      if constexpr (32 % NP == 0) {
-        // the line's threads are NP consecutive lanes of one warp: the partner's share of each
-        // pair flux travels by warp shuffle to the partner's lane, so the rounds share no state
-        const int lane = threadIdx.x & 31, lbase = lane - p;
+      const double* rOwn = OWNSM ? prec + os * RS : ro;
+      const double* mOwn = OWNSM ? prec + os * RS + NQ + 3 * dir : mo;
 #pragma unroll
-        for (int d = 1; d <= NP / 2; ++d) {
-          const bool active = valid && (2 * d < NP || p < d);
-          int q = p + d;
-          if (q >= NP) q -= NP;
-          double F[5] = {0., 0., 0., 0., 0.};
-          if (active) {
-            const int nq = vol_slot(base + q * stride);
-            double rp[NQ], mp[3];
+      for (int d = 1; d <= NP / 2; ++d) {
+        const bool active = lv && (2 * d < NP || p < d);
+        int q = p + d;
+        if (q >= NP) q -= NP;
+        double F[5] = {0., 0., 0., 0., 0.};
+        if (active) {
+          const int nq = vol_slot(base + q * stride);
+          double rp[NQ], mp[3];
 #pragma unroll
-            for (int z = 0; z < NQ; ++z) rp[z] = rec[nq * RS + z];
+          for (int z = 0; z < NQ; ++z) rp[z] = prec[nq * RS + z];
 #pragma unroll
-            for (int c = 0; c < 3; ++c) mp[c] = rec[nq * RS + NQ + 3 * dir + c];
-            pair_flux<VF>(P, ro, rp, mo, mp, F);
-          }
-          const double dOwn = sDvs[p * NP + q], dPart = sDvs[q * NP + p];
-          int src = p - d;
-          if (src < 0) src += NP;
-          const bool receive = valid && (2 * d < NP || p >= d);
-#pragma unroll
-          for (int v = 0; v < 5; ++v) {
-            racc[v] += active ? dOwn * F[v] : 0.;
-            const double got = __shfl_sync(0xffffffffu, dPart * F[v], lbase + src);
-            racc[v] += receive ? got : 0.;
-          }
+          for (int c = 0; c < 3; ++c) mp[c] = prec[nq * RS + NQ + 3 * dir + c];
+          pair_flux<VF>(P, rOwn, rp, mOwn, mp, F);
         }
-      } else {
-#pragma unroll 1
-        for (int d = 1; d <= NP / 2; ++d) {
-          const bool active = valid && (2 * d < NP || p < d);
-          if (active) {
-            int q = p + d;
-            if (q >= NP) q -= NP;
-            const int nq = vol_slot(base + q * stride);
-            double rp[NQ], mp[3], F[5];
+        const double dOwn = sDvs[p * NP + q], dPart = sDvs[q * NP + p];
+        int src = p - d;
+        if (src < 0) src += NP;
+        const bool receive = lv && (2 * d < NP || p >= d);
 #pragma unroll
-            for (int z = 0; z < NQ; ++z) rp[z] = rec[nq * RS + z];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) mp[c] = rec[nq * RS + NQ + 3 * dir + c];
-            pair_flux<VF>(P, ro, rp, mo, mp, F);
-            const double dOwn = sDvs[p * NP + q], dPart = sDvs[q * NP + p];
-#pragma unroll
-            for (int v = 0; v < 5; ++v) {
-              racc[v] += dOwn * F[v];
-              acc[nq * 5 + v] += dPart * F[v];
-            }
-          }
-          __syncthreads();
+        for (int v = 0; v < 5; ++v) {
+          racc[v] += active ? dOwn * F[v] : 0.;
+          const double got = __shfl_sync(0xffffffffu, dPart * F[v], (lbase + src) & 31);
+          racc[v] += receive ? got : 0.;
         }
       }
-      if (valid) {
+      if (lv) {
 #pragma unroll
-        for (int v = 0; v < 5; ++v) acc[os * 5 + v] += racc[v];
+        for (int v = 0; v < 5; ++v) pacc[os * 5 + v] += racc[v];
       }
       __syncthreads();
     }
@@ -309,7 +312,7 @@ volume_kernel(KParams P) {
     const int s = sides[z];
     const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
     const int side = es[0], flip = es[1];
-    const int pt = P.basis->v2s[s - 1][flip][side_plane_coords(s, i, j, k, NP)];
+    const int pt = node_side_point(N, s, flip, i, j, k);
     const double* F = P.flux + (size_t)side * 5 * NPT + pt;
     const double sg = (flip == 0) ? lh : -lh;
 #pragma unroll

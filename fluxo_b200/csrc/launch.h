@@ -14,15 +14,27 @@ struct LaunchError {
   cudaError_t err;
 };
 
-// Volume kernel: NP in 2..9, VF in {0,1,2,5,10,32}.  Returns cudaErrorInvalidValue for
+// Volume kernel: NP in 2..9, VF in {0,1,2,5,10,32}, in the launch shape the autotuner chose for
+// (NP, VF, visc) (vol_shapes.h; shape 0 until tuned or pinned).  Returns cudaErrorInvalidValue for
 // unsupported combinations.
 cudaError_t launch_volume(int NP, int VF, bool visc, int nElems, cudaStream_t s, const KParams& P);
-cudaError_t launch_volume_vf0(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P);
-cudaError_t launch_volume_vf1(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P);
-cudaError_t launch_volume_vf2(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P);
-cudaError_t launch_volume_vf5(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P);
-cudaError_t launch_volume_vf10(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P);
-cudaError_t launch_volume_vf32(int NP, bool visc, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_shape(int NP, int VF, bool visc, int shape, int nElems, cudaStream_t s,
+                                const KParams& P);
+cudaError_t launch_volume_vf0(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf1(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf2(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf5(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf10(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf32(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
+// Autotuner of the volume kernel's launch shape: times every candidate shape of (NP, VF, visc) on the
+// given data (stage-0 launches, which write only Ut) and keeps the fastest for the process; a no-op
+// once (NP, VF, visc) is tuned or pinned, or when it has one candidate.  Not callable during stream
+// capture (it synchronises the stream).
+cudaError_t tune_volume(int NP, int VF, bool visc, int nElems, cudaStream_t s, const KParams& P);
+// Chosen shape (-1: not tuned), pin (shape < 0: back to untuned), candidate count.
+int volume_shape(int NP, int VF, bool visc);
+bool pin_volume_shape(int NP, int VF, bool visc, int shape);
+int volume_shape_count(int NP);
 
 cudaError_t launch_face_flux(int RS, bool visc, int NP, int nSides, cudaStream_t s, const KParams& P);
 cudaError_t launch_lift_flux(int NP, int nSides, cudaStream_t s, const KParams& P);

@@ -1,19 +1,95 @@
-// Launchers of the face, lifting and time-step kernels and the volume-flux dispatcher.
+// Launchers of the face, lifting and time-step kernels, the volume-flux dispatcher and the volume
+// kernel's launch-shape autotuner.
+#include <mutex>
+
 #include "kernels.cuh"
 #include "launch.h"
+#include "vol_shapes.h"
 
 namespace fluxo {
 
-cudaError_t launch_volume(int NP, int VF, bool visc, int nElems, cudaStream_t s, const KParams& P) {
+cudaError_t launch_volume_shape(int NP, int VF, bool visc, int shape, int nElems, cudaStream_t s,
+                                const KParams& P) {
   switch (VF) {
-    case 0: return launch_volume_vf0(NP, visc, nElems, s, P);
-    case 1: return launch_volume_vf1(NP, visc, nElems, s, P);
-    case 2: return launch_volume_vf2(NP, visc, nElems, s, P);
-    case 5: return launch_volume_vf5(NP, visc, nElems, s, P);
-    case 10: return launch_volume_vf10(NP, visc, nElems, s, P);
-    case 32: return launch_volume_vf32(NP, visc, nElems, s, P);
+    case 0: return launch_volume_vf0(NP, visc, shape, nElems, s, P);
+    case 1: return launch_volume_vf1(NP, visc, shape, nElems, s, P);
+    case 2: return launch_volume_vf2(NP, visc, shape, nElems, s, P);
+    case 5: return launch_volume_vf5(NP, visc, shape, nElems, s, P);
+    case 10: return launch_volume_vf10(NP, visc, shape, nElems, s, P);
+    case 32: return launch_volume_vf32(NP, visc, shape, nElems, s, P);
     default: return cudaErrorInvalidValue;
   }
+}
+
+namespace {
+// chosen launch shape per (NP, VF, visc); -1 = not tuned
+std::mutex g_shape_mutex;
+int g_shape[10][33][2];
+bool g_shape_init = false;
+
+int* shape_slot(int NP, int VF, bool visc) {
+  if (NP < 2 || NP > 9 || VF < 0 || VF > 32) return nullptr;
+  if (!g_shape_init) {
+    for (auto& a : g_shape)
+      for (auto& b : a) b[0] = b[1] = -1;
+    g_shape_init = true;
+  }
+  return &g_shape[NP][VF][visc ? 1 : 0];
+}
+}  // namespace
+
+int volume_shape_count(int NP) { return vol_shape_count(NP); }
+
+int volume_shape(int NP, int VF, bool visc) {
+  std::lock_guard<std::mutex> lk(g_shape_mutex);
+  int* p = shape_slot(NP, VF, visc);
+  return p ? *p : -1;
+}
+
+bool pin_volume_shape(int NP, int VF, bool visc, int shape) {
+  std::lock_guard<std::mutex> lk(g_shape_mutex);
+  int* p = shape_slot(NP, VF, visc);
+  if (!p || shape >= vol_shape_count(NP)) return false;
+  *p = shape < 0 ? -1 : shape;
+  return true;
+}
+
+cudaError_t launch_volume(int NP, int VF, bool visc, int nElems, cudaStream_t s, const KParams& P) {
+  const int sh = volume_shape(NP, VF, visc);
+  return launch_volume_shape(NP, VF, visc, sh < 0 ? 0 : sh, nElems, s, P);
+}
+
+cudaError_t tune_volume(int NP, int VF, bool visc, int nElems, cudaStream_t s, const KParams& P) {
+  const int C = vol_shape_count(NP);
+  if (volume_shape(NP, VF, visc) >= 0) return cudaSuccess;
+  if (C <= 1) {
+    pin_volume_shape(NP, VF, visc, 0);
+    return cudaSuccess;
+  }
+  KParams Q = P;
+  Q.stage = 0;           // writes Ut only: the state and the RK register stay untouched
+  Q.haltFlag = nullptr;  // every launch does its full work
+  Q.grad = nullptr;
+  cudaEvent_t a, b;
+  cudaError_t e;
+  if ((e = cudaEventCreate(&a)) != cudaSuccess) return e;
+  if ((e = cudaEventCreate(&b)) != cudaSuccess) { cudaEventDestroy(a); return e; }
+  int best = 0;
+  float bestMs = 0.f;
+  for (int i = 0; i < C && e == cudaSuccess; ++i) {
+    if ((e = launch_volume_shape(NP, VF, visc, i, nElems, s, Q)) != cudaSuccess) break;  // warm-up
+    if ((e = cudaEventRecord(a, s)) != cudaSuccess) break;
+    for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = launch_volume_shape(NP, VF, visc, i, nElems, s, Q);
+    if (e != cudaSuccess) break;
+    if ((e = cudaEventRecord(b, s)) != cudaSuccess || (e = cudaEventSynchronize(b)) != cudaSuccess) break;
+    float ms = 0.f;
+    if ((e = cudaEventElapsedTime(&ms, a, b)) != cudaSuccess) break;
+    if (i == 0 || ms < bestMs) { bestMs = ms; best = i; }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (e == cudaSuccess) pin_volume_shape(NP, VF, visc, best);
+  return e;
 }
 
 bool volume_flux_supported(int VF) {

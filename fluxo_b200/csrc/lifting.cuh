@@ -23,9 +23,11 @@ template <int NP>
 __host__ __device__ constexpr int lv_epb() { return (256 / (NP * NP * NP)) > 0 ? (256 / (NP * NP * NP)) : 1; }
 template <int NP>
 __host__ __device__ constexpr int lv_slots() { return (NP * NP * NP - 1) + ((NP * NP * NP - 1) >> 4) + 1; }
+// per element: 5 lifting variables + 15 derivatives, later 12 contravariant fluxes + 12 directional
+// divergences
 template <int NP>
 __host__ __device__ constexpr size_t lv_smem_bytes() {
-  return sizeof(double) * (size_t)(2 * NP * NP + lv_epb<NP>() * 20 * lv_slots<NP>());
+  return sizeof(double) * (size_t)(2 * NP * NP + lv_epb<NP>() * 24 * lv_slots<NP>());
 }
 
 __device__ __forceinline__ int lv_slot(int n) { return n + (n >> 4); }
@@ -70,8 +72,10 @@ lift_visc_kernel(KParams P) {
   const int eb = threadIdx.x / NP3, t = threadIdx.x - eb * NP3;
   const int e = blockIdx.x * EPB + eb;
   const bool valid = e < P.nElems;
-  double* sV = sDhat + NPT + (size_t)eb * 20 * NS;  // [5][NS] lifting variable; later [4][NS] divergence
-  double* sW = sV + 5 * NS;                          // [15][NS] xi/eta/zeta derivatives; later [12][NS] fluxes
+  // per element 24 arrays of NS: [0,5) lifting variable, [5,20) xi/eta/zeta derivatives; later
+  // [5,17) contravariant fluxes and the 12 directional divergences in [0,5) and [17,24)
+  double* sV = sDhat + NPT + (size_t)eb * 24 * NS;
+  double* sW = sV + 5 * NS;
   for (int z = threadIdx.x; z < NPT; z += blockDim.x) {
     sD[z] = P.basis->D[z];
     sDhat[z] = P.basis->Dhat[z];
@@ -109,20 +113,24 @@ lift_visc_kernel(KParams P) {
     }
   }
   __syncthreads();
-  double ft[12];
+  // Each thread reads only its own node's derivatives and overwrites the same node's slots with its
+  // contravariant fluxes, so no barrier separates the two.  The metrics are read twice (gradient
+  // transform, flux transform) rather than held across the gradient work: fewer live registers.
   if (valid) {
     const double* M = P.metrics + (size_t)e * 9 * NP3 + t;
-    double m[9];
-#pragma unroll
-    for (int c = 0; c < 9; ++c) m[c] = M[c * NP3];
     const double sj = P.sJ[(size_t)e * NP3 + t];
     double g[3][5];
+    {
+      double m[9];
 #pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      const double gx = sW[(0 + v) * NS + lv_slot(t)], ge = sW[(5 + v) * NS + lv_slot(t)],
-                   gz = sW[(10 + v) * NS + lv_slot(t)];
+      for (int c = 0; c < 9; ++c) m[c] = M[c * NP3];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) g[d][v] = m[0 + d] * gx + m[3 + d] * ge + m[6 + d] * gz;
+      for (int v = 0; v < 5; ++v) {
+        const double gx = sW[(0 + v) * NS + lv_slot(t)], ge = sW[(5 + v) * NS + lv_slot(t)],
+                     gz = sW[(10 + v) * NS + lv_slot(t)];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) g[d][v] = m[0 + d] * gx + m[3 + d] * ge + m[6 + d] * gz;
+      }
     }
     double gv[3][5];  // BR2: volume part of the gradient, the base of every face trace
     if constexpr (LIFT == 2) {
@@ -138,13 +146,11 @@ lift_visc_kernel(KParams P) {
     int sides[3];
     const int ns = boundary_sides(i, j, k, N, sides);
     const double lh = P.basis->LhatM0;
-    int tside[3], tms[3], tpt[3];
     for (int z = 0; z < ns; ++z) {
       const int s = sides[z];
       const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
       const int side = es[0], flip = es[1];
-      const int pt = P.basis->v2s[s - 1][flip][side_plane_coords(s, i, j, k, NP)];
-      tside[z] = side; tms[z] = flip == 0 ? 0 : 1; tpt[z] = pt;
+      const int pt = node_side_point(N, s, flip, i, j, k);
       const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
       const double* F = P.lflux + (size_t)side * 5 * NPT + pt;
       const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
@@ -161,7 +167,7 @@ lift_visc_kernel(KParams P) {
         }
 #pragma unroll
         for (int d = 0; d < 3; ++d) to_grad_prim(P, u, tr[d]);
-        double* T = P.gtrace + ((size_t)side * 2 + tms[z]) * 15 * NPT + pt;
+        double* T = P.gtrace + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 15 * NPT + pt;
 #pragma unroll
         for (int d = 0; d < 3; ++d)
 #pragma unroll
@@ -184,7 +190,10 @@ lift_visc_kernel(KParams P) {
     for (int d = 0; d < 3; ++d) to_grad_prim(P, u, g[d]);
     if constexpr (LIFT == 1) {  // BR1 traces: the volume gradient at the boundary node
       for (int z = 0; z < ns; ++z) {
-        double* T = P.gtrace + ((size_t)tside[z] * 2 + tms[z]) * 15 * NPT + tpt[z];
+        const int s = sides[z];
+        const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
+        const int side = es[0], flip = es[1];
+        double* T = P.gtrace + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 15 * NPT + node_side_point(N, s, flip, i, j, k);
 #pragma unroll
         for (int d = 0; d < 3; ++d)
 #pragma unroll
@@ -200,45 +209,47 @@ lift_visc_kernel(KParams P) {
     }
     double f[4], gg[4], h[4];
     diff_flux_3d(P, u, g[0], g[1], g[2], f, gg, h);
+    const int st = lv_slot(t);
 #pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      ft[0 + v] = f[v] * m[0] + gg[v] * m[1] + h[v] * m[2];
-      ft[4 + v] = f[v] * m[3] + gg[v] * m[4] + h[v] * m[5];
-      ft[8 + v] = f[v] * m[6] + gg[v] * m[7] + h[v] * m[8];
+    for (int dir = 0; dir < 3; ++dir) {
+      const double m0 = M[(3 * dir + 0) * NP3], m1 = M[(3 * dir + 1) * NP3], m2 = M[(3 * dir + 2) * NP3];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) sW[(4 * dir + v) * NS + st] = f[v] * m0 + gg[v] * m1 + h[v] * m2;
     }
-  }
-  __syncthreads();  // every thread is done with the derivatives in sW
-  if (valid) {
-#pragma unroll
-    for (int c = 0; c < 12; ++c) sW[c * NS + lv_slot(t)] = ft[c];
-#pragma unroll
-    for (int v = 0; v < 4; ++v) sV[v * NS + lv_slot(t)] = 0.;
   }
   __syncthreads();
-  // viscous volume integral: sum_l D_hat(o,l) f~(l) along each direction, tasks (var, line)
-#pragma unroll 1
-  for (int dir = 0; dir < 3; ++dir) {
-    if (valid) {
-      for (int task = t; task < 4 * NPT; task += NP3) {
-        const int v = task / NPT, L = task - v * NPT, a = L % NP, b = L / NP;
-        double x[NP];
+  // viscous volume integral: sum_l D_hat(o,l) f~(l) along each direction, tasks (dir, var, line) of
+  // all three directions at once, each (dir, var) into its own array (array dv -> sV index
+  // dv < 5 ? dv : dv + 12, around the fluxes in [5,17))
+  if (valid) {
+    for (int task = t; task < 12 * NPT; task += NP3) {
+      const int dv = task / NPT, L = task - dv * NPT, a = L % NP, b = L / NP, dir = dv >> 2;
+      double x[NP];
 #pragma unroll
-        for (int l = 0; l < NP; ++l) x[l] = sW[(dir * 4 + v) * NS + lv_slot(line_node<NP>(dir, a, b, l))];
+      for (int l = 0; l < NP; ++l) x[l] = sW[dv * NS + lv_slot(line_node<NP>(dir, a, b, l))];
+      double* out = sV + (dv < 5 ? dv : dv + 12) * NS;
+      // D_hat is read through a volatile view: otherwise its NP^2 entries are hoisted out of the
+      // task loop into registers, which spills
+      const volatile double* vDhat = sDhat;
 #pragma unroll
-        for (int o = 0; o < NP; ++o) {
-          double s = 0.;
+      for (int o = 0; o < NP; ++o) {
+        double s = 0.;
 #pragma unroll
-          for (int l = 0; l < NP; ++l) s += sDhat[o * NP + l] * x[l];
-          sV[v * NS + lv_slot(line_node<NP>(dir, a, b, o))] += s;
-        }
+        for (int l = 0; l < NP; ++l) s += vDhat[o * NP + l] * x[l];
+        out[lv_slot(line_node<NP>(dir, a, b, o))] = s;
       }
     }
-    __syncthreads();
   }
+  __syncthreads();
   if (valid) {
     double* O = P.utvisc + (size_t)e * 4 * NP3 + t;
+    const int st = lv_slot(t);
+    // divergence arrays of (dir, v): dv = 4 dir + v at sV index dv < 5 ? dv : dv + 12
 #pragma unroll
-    for (int v = 0; v < 4; ++v) O[v * NP3] = sV[v * NS + lv_slot(t)];
+    for (int v = 0; v < 4; ++v) {
+      const int d1 = 4 + v, d2 = 8 + v;
+      O[v * NP3] = (sV[v * NS + st] + sV[(d1 < 5 ? d1 : d1 + 12) * NS + st]) + sV[(d2 + 12) * NS + st];
+    }
   }
 }
 

@@ -31,8 +31,8 @@ __global__ void face_kernel(KParams P, int NP) {
   const int side = (int)(idx / npts), pt = (int)(idx - (size_t)side * npts);
   const int* se5 = P.s2e + 5 * side;
   const int eM = se5[0], eS = se5[1];
-  const int nM = P.basis->s2v[se5[2] - 1][0][pt];
-  const int nS = P.basis->s2v[se5[3] - 1][se5[4]][pt];
+  const int nM = side_node(NP - 1, pt % NP, pt / NP, 0, se5[2]);
+  const int nS = side_node(NP - 1, pt % NP, pt / NP, se5[4], se5[3]);
   const size_t NP3 = (size_t)NP * NP * NP;
   const double* UM = P.U + NV * ((size_t)eM * NP3 + nM);
   const double* US = P.U + NV * ((size_t)eS * NP3 + nS);
@@ -98,8 +98,8 @@ __global__ void lift_flux_kernel(KParams P, int NP) {
   if (idx >= (size_t)P.nSides * npts) return;
   const int side = (int)(idx / npts), pt = (int)(idx - (size_t)side * npts);
   const int* se5 = P.s2e + 5 * side;
-  const int nM = P.basis->s2v[se5[2] - 1][0][pt];
-  const int nS = P.basis->s2v[se5[3] - 1][se5[4]][pt];
+  const int nM = side_node(NP - 1, pt % NP, pt / NP, 0, se5[2]);
+  const int nS = side_node(NP - 1, pt % NP, pt / NP, se5[4], se5[3]);
   const size_t NP3 = (size_t)NP * NP * NP;
   const double* UM = P.U + NV * ((size_t)se5[0] * NP3 + nM);
   const double* US = P.U + NV * ((size_t)se5[1] * NP3 + nS);
@@ -451,7 +451,7 @@ __global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, FLUXO_MHD_VOL_MINB) 
     const int s = sides[z];
     const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
     const int side = es[0], flip = es[1];
-    const int pt = P.basis->v2s[s - 1][flip][side_plane_coords(s, i, j, k, NP)];
+    const int pt = node_side_point(N, s, flip, i, j, k);
     const double* Fs = P.flux + (size_t)side * NF * NPT + pt;
     double F[NV];
 #pragma unroll

@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, FLUXO_MHD_LV_MINB) l
       const int s = sides[z];
       const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
       const int side = es[0], flip = es[1];
-      const int pt = P.basis->v2s[s - 1][flip][side_plane_coords(s, i, j, k, NP)];
+      const int pt = node_side_point(N, s, flip, i, j, k);
       tside[z] = side; tms[z] = flip == 0 ? 0 : 1; tpt[z] = pt;
       const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
       const double* F = P.lflux + (size_t)side * NV * NPT + pt;

@@ -273,3 +273,16 @@ def fp64_peak(device=0):
     t = ctypes.c_double()
     _lib.check(_lib.load().fluxo_gpu_fp64_peak(int(device), ctypes.byref(t)))
     return t.value
+
+
+def volume_shape(N, volume_flux, visc=False):
+    """(candidate count, chosen index or -1, elements per block, lines per warp) of the volume kernel."""
+    c, i, e, l = (ctypes.c_int() for _ in range(4))
+    _lib.check(_lib.load().fluxo_gpu_volume_shape(int(N), int(volume_flux), int(bool(visc)), ctypes.byref(c),
+                                                  ctypes.byref(i), ctypes.byref(e), ctypes.byref(l)))
+    return c.value, i.value, e.value, l.value
+
+
+def set_volume_shape(N, volume_flux, visc, index):
+    """Pins the volume kernel's launch shape of (N, volume_flux, visc); index < 0 re-enables tuning."""
+    _lib.check(_lib.load().fluxo_gpu_set_volume_shape(int(N), int(volume_flux), int(bool(visc)), int(index)))

@@ -18,10 +18,14 @@ SEED = 20261203
 BOX_MIN, BOX_MAX = (0.0, 0.0, 0.0), (2.0, 2.0, 2.0)
 BATCH_ELEMS = (4, 6, 8, 12, 16)
 BATCH_N = (3, 4, 5, 7)
-# kernel configuration of the two equation systems in the batched / served mixes
-EULER_FIELDS = dict(eqn=0, riemann=1, volume_flux=10, kappa=1.4, cfl_scale=0.9, time_disc=0, ini_exact_func=0)
+# kernel configuration of the two equation systems in the batched / served mixes: the EC-KEP
+# split form with the matrix-dissipation entropy-stable surface flux for both, CFLscale 0.5.  With
+# CFLscale 0.9 the reference algorithm (the oracle) is unstable on these boxes at N = 6, 7: a 1e-14
+# perturbation of the initial state ends in a negative density within ~30 steps, while at 0.5 it
+# stays at 1e-14 (and with the LLF surface flux it stops some N = 6, 7 requests as well).
+EULER_FIELDS = dict(eqn=0, riemann=44, volume_flux=5, kappa=1.4, cfl_scale=0.5, time_disc=0, ini_exact_func=0)
 NS_FIELDS = dict(eqn=1, riemann=44, volume_flux=5, lifting=1, lifting_var=3, visc=0, mu0=1.0 / 1600.0, Pr=0.72,
-                 kappa=1.4, cfl_scale=0.9, dfl_scale=0.4, time_disc=0, ini_exact_func=0)
+                 kappa=1.4, cfl_scale=0.5, dfl_scale=0.4, time_disc=0, ini_exact_func=0)
 
 
 def mhd_prim_to_cons(prim, kappa, mu_0=1.0):

@@ -159,6 +159,15 @@ int fluxo_gpu_launch_count(fluxo_handle* h, uint64_t* n);
 int fluxo_gpu_set_profiling(fluxo_handle* h, int enable);
 int fluxo_gpu_get_profile(fluxo_handle* h, int kind, double* total_ms, uint64_t* count);
 
+/* Launch shape of the Euler / Navier-Stokes volume kernel (no counterpart in the reference): for each
+ * (N, volume_flux, visc) a few candidate shapes (elements per block, lines per warp; 0 = lines
+ * contiguous in the thread index) give identical results; the first right-hand side of a handle, or
+ * the first run of a batch group, times them on its own data and keeps the fastest for the process.
+ * fluxo_gpu_volume_shape reports the candidates, the chosen index (-1: not tuned yet) and its shape;
+ * fluxo_gpu_set_volume_shape pins one (index < 0: tune again at the next use). */
+int fluxo_gpu_volume_shape(int N, int volume_flux, int visc, int* count, int* index, int* epb, int* lpw);
+int fluxo_gpu_set_volume_shape(int N, int volume_flux, int visc, int index);
+
 /* FP64 FMA throughput of the device (a register-resident DFMA loop over all SMs), in TFLOP/s
  * counting an FMA as 2 flops: the denominator of the FP64 roofline. */
 int fluxo_gpu_fp64_peak(int device, double* tflops);

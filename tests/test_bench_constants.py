@@ -24,7 +24,8 @@ def test_mhd_falg_constants_match_oracle_count():
     w = bench.mhd_workload(elems=4)
     kw = dict(N=w["N"], nElems=w["elems"], xmin=w["xmin"], xmax=w["xmax"], NGeo=w["NGeo"], deform_amp=w["deform_amp"],
               eqn=3, kappa=w["kappa"], eta=w["eta"], mu0=0.0, lifting=1, lifting_var=3, volume_flux=10, riemann=14,
-              noncons=1, nc_glm=0, nfvse=1, ini_exact_func=0, glm_scale=0.5, cfl_scale=0.9, dfl_scale=0.4)
+              noncons=1, nc_glm=0, nfvse=1, ini_exact_func=0, glm_scale=0.5, cfl_scale=w["cfl_scale"],
+              dfl_scale=w["dfl_scale"])
     ref = OracleCase(**kw)
     ref.set_U(mhd_orszag_tang_state(ref.mesh()["Elem_xGP"], kappa=w["kappa"]))
     ref.calc_timestep()  # sets GLM_ch as in a time step
