@@ -480,7 +480,7 @@ def run_batch(args):
     b.close()
 
     # ---- one at a time: each instance alone through fluxo_gpu_time_disc, device time summed ----
-    seq_ms = 0.0
+    seq_ms, inst_ms = 0.0, []
     if not args.no_sequential:
         for (s, mesh, U, cfg) in insts:
             op = fb.DGOperator(cfg=cfg)
@@ -495,9 +495,32 @@ def run_batch(args):
             a1.record(st)
             torch.cuda.synchronize(dev)
             assert err == 0 and n == args.steps
-            seq_ms += a0.elapsed_time(a1)
+            inst_ms.append(a0.elapsed_time(a1))
             op.close()
-        seq_ms = max_over_ranks(seq_ms, world, dev)
+        seq_ms = max_over_ranks(sum(inst_ms), world, dev)
+    # where batching pays: the instances of at most 8^3 elements, batched on their own vs alone
+    small = None
+    if inst_ms:
+        sel = [k for k, s in enumerate(specs) if s["elems"] <= 8]
+        bs = Batch(device=local)
+        for k in sel:
+            s, mesh, U, cfg = insts[k]
+            bs.add(mesh, U, 0.0, 1e30, cfg=cfg)
+        bs.run(args.warmup)
+        sst = torch.cuda.ExternalStream(bs.stream(), device=dev)
+        torch.cuda.synchronize(dev)
+        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b0.record(sst)
+        bs.run(args.steps)
+        b1.record(sst)
+        torch.cuda.synchronize(dev)
+        bs.close()
+        nds = sum(dofs[k] for k in sel)
+        alone = sum(inst_ms[k] for k in sel)
+        small = {"instances": len(sel), "dofs": nds, "batched_ms_per_step": b0.elapsed_time(b1) / args.steps,
+                 "one_at_a_time_ms_per_step": alone / args.steps,
+                 "batched_over_one_at_a_time": alone / b0.elapsed_time(b1),
+                 "note": "instances of at most 8^3 elements: too small to fill the GPU alone"}
     if rank != 0:
         return
     achieved = batch_falg(specs) * 5 * args.steps / (ms * 1e-3) / 1e12
@@ -518,6 +541,7 @@ def run_batch(args):
             "roofline": {"bound": "fp64", "kernel": "batched step (all groups, all kernels)", "achieved": achieved,
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None},
             "one_at_a_time": seq, "batched_over_one_at_a_time": (value / seq["value"]) if seq else None,
+            "small_instances": small,
             "e2e": e2e, "gpu_launches": batch_launches_per_step(specs) * args.steps, "clocks": clk.summary(),
             "setup_s": setup_s,
             "volume_shapes": {"%s_N%d" % ("ns" if eqn else "euler", N): shape_dict(N, 5, eqn == 1)
