@@ -159,7 +159,7 @@ cudaError_t balloc(fluxo_batch* b, T** p, size_t n) {
 size_t instance_bytes(const fluxo_cfg& c, int ne, int ns) {
   const size_t NP = c.N + 1, NP3 = NP * NP * NP, NPT = NP * NP;
   size_t d = 3 * 5 * NP3 * ne + 9 * NP3 * ne + NP3 * ne + 10 * NPT * ns + 5 * NPT * ns;
-  if (c.eqn == FLUXO_EQN_NAVIERSTOKES) d += 5 * NPT * ns + 4 * NP3 * ne + 30 * NPT * ns;
+  if (c.eqn == FLUXO_EQN_NAVIERSTOKES) d += 5 * NPT * ns + 4 * NP3 * ne + 8 * NPT * ns;
   return 8 * d + 4 * (5 * (size_t)ns + 12 * (size_t)ne + ne) + sizeof(InstState) + 8 + 8 + 4;
 }
 
@@ -318,7 +318,7 @@ int commit(fluxo_batch* b) {
       if (g.visc) {
         BATCH_CUDA(b, balloc(b, &g.lflux, (size_t)5 * NPT * ns));
         BATCH_CUDA(b, balloc(b, &g.utvisc, (size_t)4 * NP3 * ne));
-        BATCH_CUDA(b, balloc(b, &g.gtrace, (size_t)2 * 15 * NPT * ns));
+        BATCH_CUDA(b, balloc(b, &g.gtrace, (size_t)2 * 4 * NPT * ns));  // n.F_v of both sides
       }
       std::vector<int> s2e((size_t)5 * ns), e2s((size_t)12 * ne), einst(ne);
       int eo = 0, so = 0;

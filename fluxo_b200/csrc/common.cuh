@@ -56,7 +56,8 @@ struct KParams {
   // face buffers
   double* flux;
   double* lflux;
-  double* gtrace;         // BR2 face gradient traces [side][master|slave][15][pt]
+  double* gtrace;         // face traces of the viscous flux: n.F_v(U, gradP trace) of the master / slave
+                          // side [side][master|slave][4][pt] (Navier-Stokes; MHD: gradient traces)
   const BasisTables* basis;
   // physics constants (navierstokes/equation.f90:162-260)
   double kappa, kappaM1, sKappaM1, kappaP1, R, s23, KappasPr, mu0, Ts, sTref, ExpoSuth, cSuth, ExpoPow;

@@ -83,24 +83,12 @@ __global__ void face_flux_kernel(KParams P, int NP) {
   F[1] = nv[0] * f2 + t1[0] * f3 + t2[0] * f4;
   F[2] = nv[1] * f2 + t1[1] * f3 + t2[1] * f4;
   F[3] = nv[2] * f2 + t1[2] * f3 + t2[2] * f4;
-  if constexpr (VISC) {  // riemann.f90:155-168: + 1/2 n.(F_v(L) + F_v(R))
-    const double* U0 = P.U + 5 * ((size_t)eM * NP * NP * NP + nM);
-    const double* U1 = P.U + 5 * ((size_t)eS * NP * NP * NP + nS);
-    double uL[5], uR[5], gl[15], gr[15];
+  if constexpr (VISC) {  // riemann.f90:155-168: + 1/2 (n.F_v(L) + n.F_v(R))
+    // each side's n.F_v(U, gradP trace) was formed by the lifting kernel of its element
+    const double* tM = P.gtrace + ((size_t)side * 2 + 0) * 4 * npts + pt;
+    const double* tS = P.gtrace + ((size_t)side * 2 + 1) * 4 * npts + pt;
 #pragma unroll
-    for (int v = 0; v < 5; ++v) { uL[v] = U0[v]; uR[v] = U1[v]; }
-    // gradient traces gradP_master / gradP_slave, side-major buffers written by the lifting kernel
-    const double* tM = P.gtrace + ((size_t)side * 2 + 0) * 15 * npts + pt;
-    const double* tS = P.gtrace + ((size_t)side * 2 + 1) * 15 * npts + pt;
-#pragma unroll
-    for (int c = 0; c < 15; ++c) { gl[c] = tM[(size_t)c * npts]; gr[c] = tS[(size_t)c * npts]; }
-    double kL[4], gL[4], jL[4], kR[4], gR[4], jR[4];
-    diff_flux_3d(P, uL, gl, gl + 5, gl + 10, kL, gL, jL);
-    diff_flux_3d(P, uR, gr, gr + 5, gr + 10, kR, gR, jR);
-#pragma unroll
-    for (int v = 1; v < 5; ++v)
-      F[v] = F[v] + 0.5 * (nv[0] * (kL[v - 1] + kR[v - 1]) + nv[1] * (gL[v - 1] + gR[v - 1]) +
-                           nv[2] * (jL[v - 1] + jR[v - 1]));
+    for (int v = 1; v < 5; ++v) F[v] = F[v] + 0.5 * (tM[(v - 1) * npts] + tS[(v - 1) * npts]);
   }
   double* out = P.flux + (size_t)side * 5 * npts + pt;
 #pragma unroll

@@ -5,9 +5,11 @@
 //      (br1_volint.f90:45-98, br2_volint.f90:45-103), surface integral of the lifting flux
 //      (br1_surfint.f90:52-131, br2_surfint.f90:53-148), Jacobian, conversion to gradients of the
 //      primitive variables (equation_vars.f90:571-647);
-//   2. the face traces gradP_master/slave the face kernel needs (BR1: the volume gradient at the
-//      boundary node, ProlongToFace; BR2: volume part + etaBR2 * own-side surface part), written
-//      side-major so the face kernel reads them coalesced;
+//   2. each side's share n.F_v(U, gradP trace) of the viscous face flux 1/2 n.(F_v(L) + F_v(R))
+//      (riemann.f90:155-168), from the face trace of the gradient (BR1: the volume gradient at the
+//      boundary node, ProlongToFace; BR2: volume part + etaBR2 * own-side surface part): 4 values
+//      per side and face point instead of the 15 gradient components, written side-major so the
+//      face kernel reads them coalesced;
 //   3. the viscous volume integral sum_l D_hat(i,l) (f~,g~,h~)(l) of the contravariant viscous
 //      fluxes (volint.f90:228-271 with EvalDiffFluxTilde3D flux.f90:523-635), written as 4 values per
 //      node for the volume kernel.
@@ -167,11 +169,12 @@ lift_visc_kernel(KParams P) {
         }
 #pragma unroll
         for (int d = 0; d < 3; ++d) to_grad_prim(P, u, tr[d]);
-        double* T = P.gtrace + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 15 * NPT + pt;
+        // this side's share of the viscous face flux: n.F_v(U, trace) (riemann.f90:155-168)
+        double kf[4], kg[4], kh[4];
+        diff_flux_3d(P, u, tr[0], tr[1], tr[2], kf, kg, kh);
+        double* T = P.gtrace + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 4 * NPT + pt;
 #pragma unroll
-        for (int d = 0; d < 3; ++d)
-#pragma unroll
-          for (int v = 0; v < 5; ++v) T[(size_t)(5 * d + v) * NPT] = tr[d][v];
+        for (int v = 0; v < 4; ++v) T[(size_t)v * NPT] = n0 * kf[v] + n1 * kg[v] + n2 * kh[v];
       } else {
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
@@ -188,18 +191,6 @@ lift_visc_kernel(KParams P) {
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) to_grad_prim(P, u, g[d]);
-    if constexpr (LIFT == 1) {  // BR1 traces: the volume gradient at the boundary node
-      for (int z = 0; z < ns; ++z) {
-        const int s = sides[z];
-        const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
-        const int side = es[0], flip = es[1];
-        double* T = P.gtrace + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 15 * NPT + node_side_point(N, s, flip, i, j, k);
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
-#pragma unroll
-          for (int v = 0; v < 5; ++v) T[(size_t)(5 * d + v) * NPT] = g[d][v];
-      }
-    }
     if (P.grad) {  // volume gradients kept for analysis (DGTimeDerivative calls only)
       double* G = P.grad + 15 * ((size_t)e * NP3 + t);
 #pragma unroll
@@ -209,6 +200,21 @@ lift_visc_kernel(KParams P) {
     }
     double f[4], gg[4], h[4];
     diff_flux_3d(P, u, g[0], g[1], g[2], f, gg, h);
+    if constexpr (LIFT == 1) {
+      // BR1: the face trace of the gradient is the volume gradient at the boundary node, so this
+      // side's share of the viscous face flux is n.F_v of the node (riemann.f90:155-168)
+      for (int z = 0; z < ns; ++z) {
+        const int s = sides[z];
+        const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
+        const int side = es[0], flip = es[1];
+        const int pt = node_side_point(N, s, flip, i, j, k);
+        const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
+        const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
+        double* T = P.gtrace + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 4 * NPT + pt;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) T[(size_t)v * NPT] = n0 * f[v] + n1 * gg[v] + n2 * h[v];
+      }
+    }
     const int st = lv_slot(t);
 #pragma unroll
     for (int dir = 0; dir < 3; ++dir) {
