@@ -190,8 +190,10 @@ volume_kernel(KParams P) {
     sDvs[z] = P.basis->Dvs[z];
     sDhat[z] = P.basis->Dhat[z];
   }
+  __shared__ int sE2S[EPB][12];  // the element's ElemToSide (side, flip per local side)
   double u[5];
   if (valid) {
+    for (int z = t; z < 12; z += NP3) sE2S[eb][z] = P.e2s[12 * (size_t)e + z];  // NP3 = 8 for N = 1
     const double* Ug = P.U + 5 * ((size_t)e * NP3 + t);
 #pragma unroll
     for (int v = 0; v < 5; ++v) u[v] = Ug[v];
@@ -285,7 +287,6 @@ volume_kernel(KParams P) {
   double ut[5];
 #pragma unroll
   for (int v = 0; v < 5; ++v) ut[v] = valid ? acc[vol_slot(t) * 5 + v] : 0.;
-  const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
   if (!valid) return;
   if constexpr (VISC) {  // viscous volume integral (volint.f90:228-271), computed by the lifting kernel
     const double* V = P.utvisc + (size_t)e * 4 * NP3 + t;
@@ -293,13 +294,12 @@ volume_kernel(KParams P) {
     for (int v = 0; v < 4; ++v) ut[1 + v] += V[v * NP3];
   }
   // surface integral at the boundary nodes (LGL)
+  const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
   int sides[3];
   const int ns = boundary_sides(i, j, k, N, sides);
   const double lh = P.basis->LhatM0;
   for (int z = 0; z < ns; ++z) {
-    const int s = sides[z];
-    const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
-    const int side = es[0], flip = es[1];
+    const int s = sides[z], side = sE2S[eb][2 * (s - 1)], flip = sE2S[eb][2 * (s - 1) + 1];
     const int pt = node_side_point(N, s, flip, i, j, k);
     const double* F = P.flux + (size_t)side * 5 * NPT + pt;
     const double sg = (flip == 0) ? lh : -lh;

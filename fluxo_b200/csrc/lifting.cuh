@@ -78,12 +78,14 @@ lift_visc_kernel(KParams P) {
   // [5,17) contravariant fluxes and the 12 directional divergences in [0,5) and [17,24)
   double* sV = sDhat + NPT + (size_t)eb * 24 * NS;
   double* sW = sV + 5 * NS;
+  __shared__ int sE2S[EPB][12];  // the element's ElemToSide (side, flip per local side)
   for (int z = threadIdx.x; z < NPT; z += blockDim.x) {
     sD[z] = P.basis->D[z];
     sDhat[z] = P.basis->Dhat[z];
   }
   double u[5];
   if (valid) {
+    for (int z = t; z < 12; z += NP3) sE2S[eb][z] = P.e2s[12 * (size_t)e + z];  // NP3 = 8 for N = 1
     const double* Ug = P.U + 5 * ((size_t)e * NP3 + t);
 #pragma unroll
     for (int v = 0; v < 5; ++v) u[v] = Ug[v];
@@ -149,9 +151,7 @@ lift_visc_kernel(KParams P) {
     const int ns = boundary_sides(i, j, k, N, sides);
     const double lh = P.basis->LhatM0;
     for (int z = 0; z < ns; ++z) {
-      const int s = sides[z];
-      const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
-      const int side = es[0], flip = es[1];
+      const int s = sides[z], side = sE2S[eb][2 * (s - 1)], flip = sE2S[eb][2 * (s - 1) + 1];
       const int pt = node_side_point(N, s, flip, i, j, k);
       const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
       const double* F = P.lflux + (size_t)side * 5 * NPT + pt;
@@ -204,9 +204,7 @@ lift_visc_kernel(KParams P) {
       // BR1: the face trace of the gradient is the volume gradient at the boundary node, so this
       // side's share of the viscous face flux is n.F_v of the node (riemann.f90:155-168)
       for (int z = 0; z < ns; ++z) {
-        const int s = sides[z];
-        const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
-        const int side = es[0], flip = es[1];
+        const int s = sides[z], side = sE2S[eb][2 * (s - 1)], flip = sE2S[eb][2 * (s - 1) + 1];
         const int pt = node_side_point(N, s, flip, i, j, k);
         const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
         const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
