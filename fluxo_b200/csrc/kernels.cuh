@@ -141,8 +141,10 @@ static __global__ void lift_flux_kernel(KParams P, int NP, double* lf) {
 //   LPW > 0: LPW lines per warp, line slot s on lanes [s*G, s*G+NP) with G = 32/LPW, the other lanes
 //            idle; the block then has more threads than nodes and the node phases use the first
 //            EPB*NP^3 threads.
-// Every schedule adds the same terms in the same order, so the launch shape does not change a bit of
-// the result.
+// Every schedule adds the same terms in the same order; the shapes are separate instantiations,
+// though, and the compiler may fuse a different product of an a*b + c*d into a multiply-add in each,
+// so shapes agree to roundoff (one process uses one shape per N, flux and viscosity, so batched and
+// single solves stay bit-identical).
 // ------------------------------------------------------------------------------------------------
 template <int NP>
 __host__ __device__ constexpr int vol_epb() { return (256 / (NP * NP * NP)) > 0 ? (256 / (NP * NP * NP)) : 1; }
@@ -208,7 +210,7 @@ volume_kernel(KParams P) {
     make_record<VF>(P, u, r);
     const double* Mg = P.metrics + (size_t)e * 9 * NP3 + t;
 #pragma unroll
-    for (int c = 0; c < 9; ++c) r[NQ + c] = Mg[c * NP3];
+    for (int c = 0; c < 9; ++c) r[VolRec<VF>::MO + c] = Mg[c * NP3];
 #pragma unroll
     for (int v = 0; v < 5; ++v) acc[vol_slot(t) * 5 + v] = 0.;
   }
@@ -244,13 +246,11 @@ volume_kernel(KParams P) {
       // round, which frees 2*(NQ+3) registers
       double ro[NQ], mo[3], racc[5] = {0., 0., 0., 0., 0.};
       if (!OWNSM && lv) {
-#pragma unroll
-        for (int z = 0; z < NQ; ++z) ro[z] = prec[os * RS + z];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) mo[c] = prec[os * RS + NQ + 3 * dir + c];
+        load_rec<VF>(prec + os * RS, ro);
+        load_metric<VF>(prec + os * RS, dir, mo);
       }
       const double* rOwn = OWNSM ? prec + os * RS : ro;
-      const double* mOwn = OWNSM ? prec + os * RS + NQ + 3 * dir : mo;
+      const double* mOwn = OWNSM ? prec + os * RS + VolRec<VF>::MO + 3 * dir : mo;
 #pragma unroll
       for (int d = 1; d <= NP / 2; ++d) {
         const bool active = lv && (2 * d < NP || p < d);
@@ -260,21 +260,20 @@ volume_kernel(KParams P) {
         if (active) {
           const int nq = vol_slot(base + q * stride);
           double rp[NQ], mp[3];
-#pragma unroll
-          for (int z = 0; z < NQ; ++z) rp[z] = prec[nq * RS + z];
-#pragma unroll
-          for (int c = 0; c < 3; ++c) mp[c] = prec[nq * RS + NQ + 3 * dir + c];
+          load_rec<VF>(prec + nq * RS, rp);
+          load_metric<VF>(prec + nq * RS, dir, mp);
           pair_flux<VF>(P, rOwn, rp, mOwn, mp, F);
         }
         const double dOwn = sDvs[p * NP + q], dPart = sDvs[q * NP + p];
         int src = p - d;
         if (src < 0) src += NP;
-        const bool receive = lv && (2 * d < NP || p >= d);
+        // An inactive lane has F = 0, so its own share and the share it sends are zeros; a lane that
+        // receives nothing in the last round (2d = NP, p < d) gets the zero of an inactive sender.
+        // Hence no selects: the sums are the same (up to the sign of an exact zero).
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          racc[v] += active ? dOwn * F[v] : 0.;
-          const double got = __shfl_sync(0xffffffffu, dPart * F[v], (lbase + src) & 31);
-          racc[v] += receive ? got : 0.;
+          racc[v] = fma(dOwn, F[v], racc[v]);
+          racc[v] += __shfl_sync(0xffffffffu, dPart * F[v], (lbase + src) & 31);
         }
       }
       if (lv) {

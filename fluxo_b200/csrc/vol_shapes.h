@@ -4,9 +4,9 @@
 //   minb  resident blocks per SM the register allocation must allow (0: 2 up to 512 threads, else 1);
 //   ownsm 1: a thread reads its own node's record from shared memory in every round instead of
 //         holding it in registers (fewer registers, more shared-memory loads).
-// Entry 0 of each list is the shape used before tuning.  All shapes of one N give identical results
-// (same terms in the same order); they differ in occupancy, idle lanes, register spills and
-// shared-memory traffic.
+// Entry 0 of each list is the shape used before tuning.  All shapes of one N add the same terms in
+// the same order (they agree to roundoff: the compiler's multiply-add fusion may differ between
+// instantiations); they differ in occupancy, idle lanes, register spills and shared-memory traffic.
 #pragma once
 
 namespace fluxo {

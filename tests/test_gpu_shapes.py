@@ -1,5 +1,6 @@
-"""Launch shapes of the volume kernel (vol_shapes.h): every candidate of an N gives the same bits,
-the autotuner picks one of them, and the result matches the oracle."""
+"""Launch shapes of the volume kernel (vol_shapes.h): every candidate of an N matches the oracle and
+the other candidates to roundoff (the shapes are separate instantiations whose multiply-add fusion
+may differ), the autotuner picks one of them, and a process keeps using it (same bits on re-use)."""
 import numpy as np
 import pytest
 
@@ -33,13 +34,14 @@ def test_every_shape_same_bits(gpu_lib, N, eqn, vf):
         assert volume_shape(N, vf, eqn == 1)[1] == i
         op.dg_time_derivative(0.0)
         outs.append(op.get_ut())
-    for o in outs[1:]:
-        assert np.array_equal(o, outs[0])
-    err = np.linalg.norm(outs[0] - ref) / np.linalg.norm(ref)
-    assert err <= 1e-12
+    for o in outs:
+        assert np.linalg.norm(o - ref) / np.linalg.norm(ref) <= 1e-12
+        assert np.linalg.norm(o - outs[0]) / np.linalg.norm(outs[0]) <= 1e-14
     set_volume_shape(N, vf, eqn == 1, -1)   # the next RHS tunes again
     op.dg_time_derivative(0.0)
     cnt, chosen, epb, lpw = volume_shape(N, vf, eqn == 1)
     assert 0 <= chosen < cnt and epb >= 1
-    assert np.array_equal(op.get_ut(), outs[0])
+    assert np.array_equal(op.get_ut(), outs[chosen])
+    op.dg_time_derivative(0.0)             # the tuned shape stays: same bits
+    assert np.array_equal(op.get_ut(), outs[chosen])
     op.close()
