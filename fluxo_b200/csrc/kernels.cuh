@@ -210,7 +210,7 @@ volume_kernel(KParams P) {
     make_record<VF>(P, u, r);
     const double* Mg = P.metrics + (size_t)e * 9 * NP3 + t;
 #pragma unroll
-    for (int c = 0; c < 9; ++c) r[VolRec<VF>::MO + c] = Mg[c * NP3];
+    for (int c = 0; c < 9; ++c) r[VolRec<VF>::MO + c] = (VF == 0 ? 1.0 : 0.5) * Mg[c * NP3];  // half metrics
 #pragma unroll
     for (int v = 0; v < 5; ++v) acc[vol_slot(t) * 5 + v] = 0.;
   }

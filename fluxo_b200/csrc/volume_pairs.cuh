@@ -37,7 +37,8 @@ template <> struct VolRec<0> { static constexpr int NQ = 9, MO = 9, RS = 19; };
 template <> struct VolRec<1> { static constexpr int NQ = 9, MO = 9, RS = 19; };
 // Kennedy-Gruber (2): rho, u, v, w, p, e = E/rho
 template <> struct VolRec<2> { static constexpr int NQ = 6, MO = 6, RS = 15; };
-// EC-KEP (5): rho, u, v, w, beta = rho/(2p), |v|^2, log rho, log beta
+// EC-KEP (5): rho, u/2, v/2, w/2, beta = rho/(2p), |v|^2/2, log rho, log beta (the halves make the
+// pair averages plain sums; halving is exact, so the averages are bit-identical)
 template <> struct VolRec<5> { static constexpr int NQ = 8, MO = 8, RS = 17; };
 // Ismail-Roe (10): z1 = sqrt(rho/p), u, v, w, z5 = z1 p, log z1, log z5
 template <> struct VolRec<10> { static constexpr int NQ = 7, MO = 7, RS = 17; };
@@ -71,7 +72,7 @@ __device__ __forceinline__ void make_record(const KParams& P, const double* U, d
     r[0] = U[0]; r[1] = u; r[2] = v; r[3] = w; r[4] = p; r[5] = srho * U[4];
   } else if constexpr (VF == 5) {
     const double beta = 0.5 * U[0] / p;
-    r[0] = U[0]; r[1] = u; r[2] = v; r[3] = w; r[4] = beta; r[5] = v2;
+    r[0] = U[0]; r[1] = 0.5 * u; r[2] = 0.5 * v; r[3] = 0.5 * w; r[4] = beta; r[5] = 0.5 * v2;
     r[6] = log(U[0]); r[7] = log(beta);
   } else if constexpr (VF == 10) {
     const double z1 = sqrt(U[0] / p);
@@ -96,7 +97,8 @@ __device__ __forceinline__ void pair_flux(const KParams& P, const double* L, con
     F[3] = 0.5 * (L[3] * qL + R[3] * qR + mL[2] * L[8] + mR[2] * R[8]);
     F[4] = 0.5 * ((L[4] + L[8]) * qL + (R[4] + R[8]) * qR);
   } else {
-    const double m1 = 0.5 * (mL[0] + mR[0]), m2 = 0.5 * (mL[1] + mR[1]), m3 = 0.5 * (mL[2] + mR[2]);
+    // the records of these fluxes hold half metrics: the dealiased metric 1/2 (Ja_L + Ja_R) is a sum
+    const double m1 = mL[0] + mR[0], m2 = mL[1] + mR[1], m3 = mL[2] + mR[2];
     if constexpr (VF == 1) {  // StandardDGFluxDealiasedMetricVec :446-494
       const double qL = L[5] * m1 + L[6] * m2 + L[7] * m3;
       const double qR = R[5] * m1 + R[6] * m2 + R[7] * m3;
@@ -126,13 +128,13 @@ __device__ __forceinline__ void pair_flux(const KParams& P, const double* L, con
       const double rhoHat = nr * sb * nb * inv;      // LN(rho)
       const double p1 = 0.5 * sr * dr * nb * inv;    // 0.5*rho_mean/beta_mean
       const double sbHat = db * dr * sb * inv;       // 1/LN(beta)
-      const double uH = 0.5 * (L[1] + R[1]), vH = 0.5 * (L[2] + R[2]), wH = 0.5 * (L[3] + R[3]);
+      const double uH = L[1] + R[1], vH = L[2] + R[2], wH = L[3] + R[3];  // records hold u/2, v/2, w/2
       const double q = uH * m1 + vH * m2 + wH * m3;
       F[0] = rhoHat * q;
       F[1] = F[0] * uH + m1 * p1;
       F[2] = F[0] * vH + m2 * p1;
       F[3] = F[0] * wH + m3 * p1;
-      F[4] = F[0] * 0.5 * (P.sKappaM1 * sbHat - 0.5 * (L[5] + R[5])) + uH * F[1] + vH * F[2] + wH * F[3];
+      F[4] = F[0] * 0.5 * (P.sKappaM1 * sbHat - (L[5] + R[5])) + uH * F[1] + vH * F[2] + wH * F[3];
     } else if constexpr (VF == 10) {  // TwoPointEntropyConservingFluxVec :574-673
       double n1, d1, n5, d5;
       ln_mean_nd(L[0], R[0], L[5], R[5], n1, d1);
