@@ -258,11 +258,9 @@ volume_kernel(KParams P) {
         if (q >= NP) q -= NP;
         double F[5] = {0., 0., 0., 0., 0.};
         if (active) {
-          const int nq = vol_slot(base + q * stride);
-          double rp[NQ], mp[3];
-          load_rec<VF>(prec + nq * RS, rp);
-          load_metric<VF>(prec + nq * RS, dir, mp);
-          pair_flux<VF>(P, rOwn, rp, mOwn, mp, F);
+          // the partner's record is read in place (the log-mean logarithms only when needed)
+          const double* rq = prec + vol_slot(base + q * stride) * RS;
+          pair_flux<VF>(P, rOwn, rq, mOwn, rq + VolRec<VF>::MO + 3 * dir, F);
         }
         const double dOwn = sDvs[p * NP + q], dPart = sDvs[q * NP + p];
         int src = p - d;

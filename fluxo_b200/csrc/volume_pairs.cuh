@@ -26,6 +26,23 @@ __device__ __forceinline__ void ln_mean_nd(double a, double b, double la, double
   den = series ? qs : (lb - la);
 }
 
+// log mean of (a, b) = (L[i], R[i]) as num/den; the logarithms log a = L[il], log b = R[il] are read
+// only off the series branch (R usually points into shared memory: in smooth flows nearly every
+// pair takes the series branch, so its two logarithm loads are skipped)
+__device__ __forceinline__ void ln_mean_nd(const double* L, const double* R, int i, int il, double& num,
+                                           double& den) {
+  const double a = L[i], b = R[i];
+  const double d = b - a, s = b + a;
+  const double d2 = d * d, s2 = s * s;
+  if (d2 < 1.0e-4 * s2) {
+    num = 0.5 * s * (s2 * s2 * s2);
+    den = s2 * (s2 * (s2 + d2 * (1. / 3.)) + d2 * d2 * (1. / 5.)) + d2 * d2 * d2 * (1. / 7.);
+  } else {
+    num = d;
+    den = R[il] - L[il];
+  }
+}
+
 // Record of a node in shared memory: NQ flux quantities at [0, NQ), the metric terms Ja^1..Ja^3
 // (x,y,z each) at [MO, MO+9), RS doubles per node.  The odd stride RS spreads the records of the
 // nodes of a line over the shared-memory banks (padded 16-byte-aligned records read with 16-byte
@@ -121,8 +138,8 @@ __device__ __forceinline__ void pair_flux(const KParams& P, const double* L, con
       F[4] = F[0] * eH + p1 * q;
     } else if constexpr (VF == 5) {  // EntropyAndEnergyConservingFluxVec :1277-1356
       double nr, dr, nb, db;
-      ln_mean_nd(L[0], R[0], L[6], R[6], nr, dr);
-      ln_mean_nd(L[4], R[4], L[7], R[7], nb, db);
+      ln_mean_nd(L, R, 0, 6, nr, dr);
+      ln_mean_nd(L, R, 4, 7, nb, db);
       const double sr = L[0] + R[0], sb = L[4] + R[4];
       const double inv = 1. / (dr * sb * nb);
       const double rhoHat = nr * sb * nb * inv;      // LN(rho)
@@ -137,8 +154,8 @@ __device__ __forceinline__ void pair_flux(const KParams& P, const double* L, con
       F[4] = F[0] * 0.5 * (P.sKappaM1 * sbHat - (L[5] + R[5])) + uH * F[1] + vH * F[2] + wH * F[3];
     } else if constexpr (VF == 10) {  // TwoPointEntropyConservingFluxVec :574-673
       double n1, d1, n5, d5;
-      ln_mean_nd(L[0], R[0], L[5], R[5], n1, d1);
-      ln_mean_nd(L[4], R[4], L[6], R[6], n5, d5);
+      ln_mean_nd(L, R, 0, 5, n1, d1);
+      ln_mean_nd(L, R, 4, 6, n5, d5);
       const double z1M = 0.5 * (L[0] + R[0]);
       const double inv = 1. / (d5 * z1M * n1);
       const double z5LN = n5 * z1M * n1 * inv;
@@ -157,8 +174,8 @@ __device__ __forceinline__ void pair_flux(const KParams& P, const double* L, con
       F[4] = 0.5 * (q * P.kappaP1 * P.sKappaM1 * ratio + uH * F[1] + vH * F[2] + wH * F[3]);
     } else if constexpr (VF == 32) {  // RanochaFluxVec :1876-1929
       double nr, dr, ns, ds;
-      ln_mean_nd(L[0], R[0], L[6], R[6], nr, dr);
-      ln_mean_nd(L[5], R[5], L[7], R[7], ns, ds);
+      ln_mean_nd(L, R, 0, 6, nr, dr);
+      ln_mean_nd(L, R, 5, 7, ns, ds);
       const double inv = 1. / (dr * ns);
       const double rhoLN = nr * ns * inv;
       const double srspM = ds * dr * inv;  // 1/LN(rho/p)
