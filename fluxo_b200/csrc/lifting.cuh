@@ -40,6 +40,35 @@ __device__ __forceinline__ int line_node(int dir, int a, int b, int x) {
   return dir == 0 ? x + NP * (a + NP * b) : (dir == 1 ? a + NP * (x + NP * b) : a + NP * (b + NP * x));
 }
 
+// sum_l row[l] x[l] for a row of an (N+1)^2 operator in shared memory, in the order l = 0..N.  For
+// even N+1 the row is read with 16-byte loads (half the load instructions; every lane reads the same
+// address, a broadcast).  FRESH: the row is re-read on every call, so the compiler cannot hoist the
+// whole operator out of a loop into registers (which spills).
+template <int NP, bool FRESH>
+__device__ __forceinline__ double row_dot(const double* row, const double* x) {
+  double s = 0.;
+  if constexpr (NP % 2 == 0) {
+#pragma unroll
+    for (int l = 0; l < NP; l += 2) {
+      double a, b;
+      if constexpr (FRESH) {
+        const unsigned addr = static_cast<unsigned>(__cvta_generic_to_shared(row + l));
+        asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(a), "=d"(b) : "r"(addr));
+      } else {
+        const double2 r2 = *reinterpret_cast<const double2*>(row + l);
+        a = r2.x; b = r2.y;
+      }
+      s += a * x[l];
+      s += b * x[l + 1];
+    }
+  } else {
+    const volatile double* vrow = row;
+#pragma unroll
+    for (int l = 0; l < NP; ++l) s += (FRESH ? vrow[l] : row[l]) * x[l];
+  }
+  return s;
+}
+
 template <int LV>
 __device__ __forceinline__ void lifting_var_t(const KParams& P, const double* U, double* V) {
   if constexpr (LV == 1) {
@@ -108,12 +137,7 @@ lift_visc_kernel(KParams P) {
 #pragma unroll
       for (int l = 0; l < NP; ++l) x[l] = sV[v * NS + lv_slot(line_node<NP>(dir, a, b, l))];
 #pragma unroll
-      for (int o = 0; o < NP; ++o) {
-        double s = 0.;
-#pragma unroll
-        for (int l = 0; l < NP; ++l) s += sD[o * NP + l] * x[l];
-        sW[(dir * 5 + v) * NS + lv_slot(line_node<NP>(dir, a, b, o))] = s;
-      }
+      for (int o = 0; o < NP; ++o) sW[(dir * 5 + v) * NS + lv_slot(line_node<NP>(dir, a, b, o))] = row_dot<NP, true>(sD + o * NP, x);
     }
   }
   __syncthreads();
@@ -232,16 +256,9 @@ lift_visc_kernel(KParams P) {
 #pragma unroll
       for (int l = 0; l < NP; ++l) x[l] = sW[dv * NS + lv_slot(line_node<NP>(dir, a, b, l))];
       double* out = sV + (dv < 5 ? dv : dv + 12) * NS;
-      // D_hat is read through a volatile view: otherwise its NP^2 entries are hoisted out of the
-      // task loop into registers, which spills
-      const volatile double* vDhat = sDhat;
+      // D_hat re-read per row: hoisting its NP^2 entries out of the task loop spills
 #pragma unroll
-      for (int o = 0; o < NP; ++o) {
-        double s = 0.;
-#pragma unroll
-        for (int l = 0; l < NP; ++l) s += vDhat[o * NP + l] * x[l];
-        out[lv_slot(line_node<NP>(dir, a, b, o))] = s;
-      }
+      for (int o = 0; o < NP; ++o) out[lv_slot(line_node<NP>(dir, a, b, o))] = row_dot<NP, true>(sDhat + o * NP, x);
     }
   }
   __syncthreads();
