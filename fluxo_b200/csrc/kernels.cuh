@@ -162,12 +162,22 @@ struct VolShape {
 // spreads the eta- and zeta-lines (node strides NP and NP^2) over the shared-memory banks.
 __host__ __device__ constexpr int vol_slot(int n) { return n + (n >> 4); }
 
+// The Euler / Navier-Stokes kernel's padding: for N+1 = 8 two spare slots every 16 nodes and two
+// more every 64 make the line accesses of all three directions (own and partner records, the
+// accumulators) free of bank conflicts, one spare slot every 16 nodes leaves 2/3 more wavefronts.
+template <int NP>
+__host__ __device__ constexpr int vol_pad(int n) {
+  return NP == 8 ? n + 2 * (n >> 4) + 2 * (n >> 6) : vol_slot(n);
+}
+
 template <int NP>
 __host__ __device__ constexpr int vol_slots() { return vol_slot(NP * NP * NP - 1) + 1; }
+template <int NP>
+__host__ __device__ constexpr int vol_pad_slots() { return vol_pad<NP>(NP * NP * NP - 1) + 1; }
 
 template <int NP, int VF, int EPB = vol_epb<NP>()>
 __host__ __device__ constexpr size_t vol_smem_bytes() {
-  return sizeof(double) * (size_t)(2 * NP * NP + EPB * (VolRec<VF>::RS + 5) * vol_slots<NP>());
+  return sizeof(double) * (size_t)(2 * NP * NP + EPB * (VolRec<VF>::RS + 5) * vol_pad_slots<NP>());
 }
 
 template <int NP, int VF, bool VISC, int EPB, int LPW, int MINB, int OWNSM>
@@ -185,7 +195,7 @@ volume_kernel(KParams P) {
   const int eb = nodeThread ? threadIdx.x / NP3 : 0, t = nodeThread ? threadIdx.x - eb * NP3 : 0;
   const int e = blockIdx.x * EPB + eb;
   const bool valid = nodeThread && e < P.nElems;
-  constexpr int NS = vol_slots<NP>();
+  constexpr int NS = vol_pad_slots<NP>();
   double* rec = sDhat + NPT + (size_t)eb * (RS + 5) * NS;  // [slot][RS]
   double* acc = rec + (size_t)RS * NS;                     // [slot][5]
   for (int z = threadIdx.x; z < NPT; z += blockDim.x) {
@@ -206,13 +216,13 @@ volume_kernel(KParams P) {
 #pragma unroll
       for (int v = 0; v < 4; ++v) prefetch_l2(P.utvisc + (size_t)e * 4 * NP3 + v * NP3 + t);
     }
-    double* r = rec + vol_slot(t) * RS;
+    double* r = rec + vol_pad<NP>(t) * RS;
     make_record<VF>(P, u, r);
     const double* Mg = P.metrics + (size_t)e * 9 * NP3 + t;
 #pragma unroll
     for (int c = 0; c < 9; ++c) r[VolRec<VF>::MO + c] = (VF == 0 ? 1.0 : 0.5) * Mg[c * NP3];  // half metrics
 #pragma unroll
-    for (int v = 0; v < 5; ++v) acc[vol_slot(t) * 5 + v] = 0.;
+    for (int v = 0; v < 5; ++v) acc[vol_pad<NP>(t) * 5 + v] = 0.;
   }
   __syncthreads();
   // split-form volume integral, line by line
@@ -241,7 +251,7 @@ volume_kernel(KParams P) {
     for (int dir = 0; dir < 3; ++dir) {
       const int stride = dir == 0 ? 1 : (dir == 1 ? NP : NPT);
       const int base = dir == 0 ? NP * (la + NP * lb) : (dir == 1 ? la + NPT * lb : la + NP * lb);
-      const int own = base + p * stride, os = vol_slot(own);
+      const int own = base + p * stride, os = vol_pad<NP>(own);
       // own record: held in registers for all rounds, or (OWNSM) read from shared memory in every
       // round, which frees 2*(NQ+3) registers
       double ro[NQ], mo[3], racc[5] = {0., 0., 0., 0., 0.};
@@ -259,7 +269,7 @@ volume_kernel(KParams P) {
         double F[5] = {0., 0., 0., 0., 0.};
         if (active) {
           // the partner's record is read in place (the log-mean logarithms only when needed)
-          const double* rq = prec + vol_slot(base + q * stride) * RS;
+          const double* rq = prec + vol_pad<NP>(base + q * stride) * RS;
           pair_flux<VF>(P, rOwn, rq, mOwn, rq + VolRec<VF>::MO + 3 * dir, F);
         }
         const double dOwn = sDvs[p * NP + q], dPart = sDvs[q * NP + p];
@@ -283,7 +293,7 @@ volume_kernel(KParams P) {
   }
   double ut[5];
 #pragma unroll
-  for (int v = 0; v < 5; ++v) ut[v] = valid ? acc[vol_slot(t) * 5 + v] : 0.;
+  for (int v = 0; v < 5; ++v) ut[v] = valid ? acc[vol_pad<NP>(t) * 5 + v] : 0.;
   if (!valid) return;
   if constexpr (VISC) {  // viscous volume integral (volint.f90:228-271), computed by the lifting kernel
     const double* V = P.utvisc + (size_t)e * 4 * NP3 + t;
