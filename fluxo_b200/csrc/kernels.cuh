@@ -129,9 +129,9 @@ static __global__ void lift_flux_kernel(KParams P, int NP, double* lf) {
 // One thread per volume node, EPB elements per block.  Each node's record (volume_pairs.cuh) and
 // the metrics sit in shared memory.  For each direction the threads of one line evaluate every
 // pair of the line exactly once (the reference's symmetric reuse, flux_average.f90:232-243):
-// in round d thread p takes the pair (p, p+d mod NP); its own contribution stays in registers,
-// the partner's goes to a shared accumulator, and no two threads of a round touch the same
-// accumulator.
+// in round d thread p takes the pair (p, p+d mod NP); its own contribution stays in registers and
+// the partner's share is shuffled to the partner's lane; after the rounds of a direction each node
+// adds its sum to its shared accumulator.
 //
 // The partner's share of each pair flux travels by warp shuffle to the partner's lane, so a line must
 // live in one warp.  Launch shape (template parameters, chosen per N by the launcher's autotuner):
