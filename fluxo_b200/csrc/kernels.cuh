@@ -162,22 +162,31 @@ struct VolShape {
 // spreads the eta- and zeta-lines (node strides NP and NP^2) over the shared-memory banks.
 __host__ __device__ constexpr int vol_slot(int n) { return n + (n >> 4); }
 
-// The Euler / Navier-Stokes kernel's padding: for N+1 = 8 two spare slots every 16 nodes and two
-// more every 64 make the line accesses of all three directions (own and partner records, the
-// accumulators) free of bank conflicts, one spare slot every 16 nodes leaves 2/3 more wavefronts.
-template <int NP>
+// The Euler / Navier-Stokes kernel's node padding per (N+1, lines per warp): chosen with a lane-by-
+// lane model of the pair rounds (own and partner records and accumulators of all three directions)
+// so that a warp's 8-byte accesses need the minimum number of shared wavefronts (one spare slot
+// every 16 nodes needs 1.6-2x as many): N+1 = 8 contiguous, 4 contiguous, 5/6/7 with 4 lines per
+// warp and 3 with 8 lines per warp are conflict-free (7: 1.04, 3: 1.08); the other schedules keep
+// the 16-node padding.
+template <int NP, int LPW = 0>
 __host__ __device__ constexpr int vol_pad(int n) {
-  return NP == 8 ? n + 2 * (n >> 4) + 2 * (n >> 6) : vol_slot(n);
+  return (NP == 8 && LPW == 0)   ? n + 2 * (n >> 4) + 2 * (n >> 6)
+         : (NP == 4 && LPW == 0) ? n + 4 * (n >> 4)
+         : (NP == 5 && LPW == 4) ? n + n / 5 + 5 * (n / 25)
+         : (NP == 6 && LPW == 4) ? n + 2 * (n / 36)
+         : (NP == 7 && LPW == 4) ? n + n / 49
+         : (NP == 3 && LPW == 8) ? n + 2 * (n >> 4)
+                                 : vol_slot(n);
 }
 
 template <int NP>
 __host__ __device__ constexpr int vol_slots() { return vol_slot(NP * NP * NP - 1) + 1; }
-template <int NP>
-__host__ __device__ constexpr int vol_pad_slots() { return vol_pad<NP>(NP * NP * NP - 1) + 1; }
+template <int NP, int LPW = 0>
+__host__ __device__ constexpr int vol_pad_slots() { return vol_pad<NP, LPW>(NP * NP * NP - 1) + 1; }
 
-template <int NP, int VF, int EPB = vol_epb<NP>()>
+template <int NP, int VF, int EPB = vol_epb<NP>(), int LPW = 0>
 __host__ __device__ constexpr size_t vol_smem_bytes() {
-  return sizeof(double) * (size_t)(2 * NP * NP + EPB * (VolRec<VF>::RS + 5) * vol_pad_slots<NP>());
+  return sizeof(double) * (size_t)(2 * NP * NP + EPB * (VolRec<VF>::RS + 5) * vol_pad_slots<NP, LPW>());
 }
 
 template <int NP, int VF, bool VISC, int EPB, int LPW, int MINB, int OWNSM>
@@ -195,7 +204,7 @@ volume_kernel(KParams P) {
   const int eb = nodeThread ? threadIdx.x / NP3 : 0, t = nodeThread ? threadIdx.x - eb * NP3 : 0;
   const int e = blockIdx.x * EPB + eb;
   const bool valid = nodeThread && e < P.nElems;
-  constexpr int NS = vol_pad_slots<NP>();
+  constexpr int NS = vol_pad_slots<NP, LPW>();
   double* rec = sDhat + NPT + (size_t)eb * (RS + 5) * NS;  // [slot][RS]
   double* acc = rec + (size_t)RS * NS;                     // [slot][5]
   for (int z = threadIdx.x; z < NPT; z += blockDim.x) {
@@ -216,13 +225,13 @@ volume_kernel(KParams P) {
 #pragma unroll
       for (int v = 0; v < 4; ++v) prefetch_l2(P.utvisc + (size_t)e * 4 * NP3 + v * NP3 + t);
     }
-    double* r = rec + vol_pad<NP>(t) * RS;
+    double* r = rec + vol_pad<NP, LPW>(t) * RS;
     make_record<VF>(P, u, r);
     const double* Mg = P.metrics + (size_t)e * 9 * NP3 + t;
 #pragma unroll
     for (int c = 0; c < 9; ++c) r[VolRec<VF>::MO + c] = (VF == 0 ? 1.0 : 0.5) * Mg[c * NP3];  // half metrics
 #pragma unroll
-    for (int v = 0; v < 5; ++v) acc[vol_pad<NP>(t) * 5 + v] = 0.;
+    for (int v = 0; v < 5; ++v) acc[vol_pad<NP, LPW>(t) * 5 + v] = 0.;
   }
   __syncthreads();
   // split-form volume integral, line by line
@@ -251,7 +260,7 @@ volume_kernel(KParams P) {
     for (int dir = 0; dir < 3; ++dir) {
       const int stride = dir == 0 ? 1 : (dir == 1 ? NP : NPT);
       const int base = dir == 0 ? NP * (la + NP * lb) : (dir == 1 ? la + NPT * lb : la + NP * lb);
-      const int own = base + p * stride, os = vol_pad<NP>(own);
+      const int own = base + p * stride, os = vol_pad<NP, LPW>(own);
       // own record: held in registers for all rounds, or (OWNSM) read from shared memory in every
       // round, which frees 2*(NQ+3) registers
       double ro[NQ], mo[3], racc[5] = {0., 0., 0., 0., 0.};
@@ -269,7 +278,7 @@ volume_kernel(KParams P) {
         double F[5] = {0., 0., 0., 0., 0.};
         if (active) {
           // the partner's record is read in place (the log-mean logarithms only when needed)
-          const double* rq = prec + vol_pad<NP>(base + q * stride) * RS;
+          const double* rq = prec + vol_pad<NP, LPW>(base + q * stride) * RS;
           pair_flux<VF>(P, rOwn, rq, mOwn, rq + VolRec<VF>::MO + 3 * dir, F);
         }
         const double dOwn = sDvs[p * NP + q], dPart = sDvs[q * NP + p];
@@ -293,7 +302,7 @@ volume_kernel(KParams P) {
   }
   double ut[5];
 #pragma unroll
-  for (int v = 0; v < 5; ++v) ut[v] = valid ? acc[vol_pad<NP>(t) * 5 + v] : 0.;
+  for (int v = 0; v < 5; ++v) ut[v] = valid ? acc[vol_pad<NP, LPW>(t) * 5 + v] : 0.;
   if (!valid) return;
   if constexpr (VISC) {  // viscous volume integral (volint.f90:228-271), computed by the lifting kernel
     const double* V = P.utvisc + (size_t)e * 4 * NP3 + t;

@@ -14,7 +14,7 @@ template <int NP, bool VISC, int I>
 static cudaError_t vol_shape_launch(int nElems, cudaStream_t s, const KParams& P) {
   constexpr VolShapeId sh = kVolShapes[NP][I];
   constexpr int EPB = sh.epb, LPW = sh.lpw, MINB = sh.minb, OWNSM = sh.ownsm;
-  constexpr size_t smem = vol_smem_bytes<NP, VF_ID, EPB>();
+  constexpr size_t smem = vol_smem_bytes<NP, VF_ID, EPB, LPW>();
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(volume_kernel<NP, VF_ID, VISC, EPB, LPW, MINB, OWNSM>,

@@ -22,10 +22,10 @@ constexpr VolShapeId kVolShapes[10][kVolShapeMax] = {
     {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}},    // NP 0 (unused)
     {{0, 0, 0, 0}, {0, 0, 0, 0}, {0, 0, 0, 0}},    // NP 1 (unused)
     {{32, 0, 0, 0}, {16, 0, 0, 0}, {0, 0, 0, 0}},  // NP 2: 256 / 128 threads
-    {{8, 10, 0, 0}, {8, 8, 0, 0}, {4, 10, 0, 0}},  // NP 3: 256 / 512 / 128 threads
+    {{8, 10, 0, 0}, {8, 8, 0, 0}, {4, 8, 0, 0}},   // NP 3: 256 / 512 / 256 threads
     {{4, 0, 0, 0}, {8, 0, 0, 0}, {2, 0, 0, 0}},    // NP 4: 256 / 512 / 128 threads
-    {{2, 6, 0, 0}, {2, 4, 0, 0}, {1, 6, 0, 0}},    // NP 5: 320 / 448 / 160 threads
-    {{1, 5, 0, 0}, {1, 4, 0, 0}, {2, 5, 0, 1}},    // NP 6: 256 / 288 / 512 threads
+    {{2, 6, 0, 0}, {2, 4, 0, 0}, {1, 4, 0, 0}},    // NP 5: 320 / 448 / 224 threads
+    {{1, 5, 0, 0}, {1, 4, 0, 0}, {1, 4, 0, 1}},    // NP 6: 256 / 288 / 288 threads
     {{1, 4, 0, 0}, {1, 4, 1, 0}, {1, 4, 0, 1}},    // NP 7: 416 threads; 1-block registers; own record in smem
     {{1, 0, 0, 0}, {1, 0, 1, 0}, {1, 0, 0, 1}},    // NP 8: 512 threads; 1-block registers; own record in smem
     {{1, 3, 0, 1}, {0, 0, 0, 0}, {0, 0, 0, 0}},    // NP 9: 864 threads
