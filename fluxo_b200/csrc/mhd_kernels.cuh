@@ -194,8 +194,8 @@ __device__ __forceinline__ void pair_flux_mhd(const KParams& P, double ch, const
       F[8] = 0.5 * ch * (qbL + qbR);
     } else if constexpr (VF == 10) {  // EntropyAndKinEnergyConservingFluxVec_Derigs :761-848
       double nr, dr, nb, db;
-      ln_mean_nd(L[0], R[0], L[12], R[12], nr, dr);
-      ln_mean_nd(L[1], R[1], L[13], R[13], nb, db);
+      ln_mean_nd(L, R, 0, 12, nr, dr);
+      ln_mean_nd(L, R, 1, 13, nb, db);
       const double sr = L[0] + R[0], sb = L[1] + R[1];
       const double inv = 1. / (dr * nb * sb);
       const double rhoLN = nr * nb * sb * inv;    // LN(rho)
@@ -223,8 +223,8 @@ __device__ __forceinline__ void pair_flux_mhd(const KParams& P, double ch, const
              smu0 * (sB - 0.25 * b2v + 0.5 * (L[11] + R[11]) * Bm + F[8] * psiA - (ch * 0.5) * pB);
     } else if constexpr (VF == 12) {  // EntropyAndKinEnergyConservingFluxVec_FloGor :970-1074
       double nr, dr, ne, de;
-      ln_mean_nd(L[0], R[0], L[10], R[10], nr, dr);
-      ln_mean_nd(L[2], R[2], L[11], R[11], ne, de);
+      ln_mean_nd(L, R, 0, 10, nr, dr);
+      ln_mean_nd(L, R, 2, 11, ne, de);
       const double inv = 1. / (dr * ne);
       const double rhoLN = nr * ne * inv;
       const double ieT = L[2] * R[2] * de * dr * inv;  // e_L e_R / LN(e)
@@ -272,23 +272,35 @@ __host__ __device__ constexpr size_t vol_smem_bytes() {
   return sizeof(double) * (size_t)(NP * NP + NP + epb<NP>() * (Rec<VF>::RS + NACC) * vol_slots<NP>());
 }
 
-#ifndef FLUXO_MHD_VOL_MINB
-#define FLUXO_MHD_VOL_MINB 1
-#endif
+// Pair-phase schedule: lines contiguous in the thread index when N+1 divides 32, otherwise
+// floor(32/(N+1)) lines packed whole into each warp (the rounds are warp shuffles either way; see the
+// Euler / Navier-Stokes volume kernel)
+template <int NP>
+__host__ __device__ constexpr int vol_lpw() { return 32 % NP == 0 ? 0 : 32 / NP; }
+template <int NP>
+__host__ __device__ constexpr int vol_threads() { return VolShape<NP, epb<NP>(), vol_lpw<NP>()>::THREADS; }
+
+// resident blocks per SM the register allocation must allow: 2 for blocks of up to 320 threads
+// (at most 102 registers: more resident warps than the unconstrained ~160), else 1
+template <int NP>
+__host__ __device__ constexpr int vol_minb() { return vol_threads<NP>() <= 320 ? 2 : 1; }
+
 template <int NP, int VF>
-__global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, FLUXO_MHD_VOL_MINB) volume_kernel(KParams P) {
+__global__ void __launch_bounds__(vol_threads<NP>(), vol_minb<NP>()) volume_kernel(KParams P) {
   if (halted(P)) return;
   const int NC = P.noncons;
   const bool NCGLM = NC != 0 && P.ncGLM != 0;
-  constexpr int NP3 = NP * NP * NP, N = NP - 1, NPT = NP * NP, EPB = epb<NP>();
+  constexpr int NP3 = NP * NP * NP, N = NP - 1, NPT = NP * NP, EPB = epb<NP>(), LPW = vol_lpw<NP>();
   constexpr int RS = Rec<VF>::RS, NQ = Rec<VF>::NQ, IB = Rec<VF>::B, IPSI = Rec<VF>::PSI, IV = Rec<VF>::V;
   constexpr int NS = vol_slots<NP>();
   extern __shared__ double smem[];
   double* sDvs = smem;        // Dvolsurf(i,l) at [i*NP+l]
   double* sRow = sDvs + NPT;  // sum_l Dvolsurf(i,l)
-  const int eb = threadIdx.x / NP3, t = threadIdx.x - eb * NP3;
+  // node phases: thread -> (element slot eb, node t); with packed lines the threads past EPB*NP3 idle
+  const bool nodeThread = threadIdx.x < EPB * NP3;
+  const int eb = nodeThread ? threadIdx.x / NP3 : 0, t = nodeThread ? threadIdx.x - eb * NP3 : 0;
   const int e = blockIdx.x * EPB + eb;
-  const bool valid = e < P.nElems;
+  const bool valid = nodeThread && e < P.nElems;
   double* rec = sRow + NP + (size_t)eb * (RS + NACC) * NS;  // [slot][RS]
   double* acc = rec + (size_t)RS * NS;                       // [slot][NACC]
   for (int z = threadIdx.x; z < NPT; z += blockDim.x) sDvs[z] = P.basis->Dvs[z];
@@ -314,7 +326,26 @@ __global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, FLUXO_MHD_VOL_MINB) 
   }
   __syncthreads();
   {
-    const int p = t % NP, Ln = t / NP, la = Ln % NP, lb = Ln / NP;
+    // this thread's (element slot pe, line Ln, position p) in the pair phase; lv: it holds a position
+    // of a line of an existing element (idle lanes keep in-range indexes and only join the shuffles)
+    int pe, p, Ln, lbase;
+    bool lv;
+    const int lane = threadIdx.x & 31;
+    if constexpr (LPW == 0) {
+      pe = eb; p = t % NP; Ln = t / NP; lv = valid; lbase = lane - p;
+    } else {
+      constexpr int G = 32 / LPW, WPE = VolShape<NP, EPB, LPW>::WPE;
+      const int wi = threadIdx.x >> 5, slot = lane / G;
+      pe = wi / WPE;
+      p = lane - slot * G;
+      Ln = (wi - pe * WPE) * LPW + slot;
+      lv = slot < LPW && p < NP && Ln < NPT && (int)blockIdx.x * EPB + pe < P.nElems;
+      lbase = slot * G;
+      if (!lv) { p = 0; Ln = 0; }
+    }
+    const int la = Ln % NP, lb = Ln / NP;
+    double* prec = sRow + NP + (size_t)pe * (RS + NACC) * NS;
+    double* pacc = prec + (size_t)RS * NS;
 #pragma unroll 1
     for (int dir = 0; dir < 3; ++dir) {
       const int stride = dir == 0 ? 1 : (dir == 1 ? NP : NPT);
@@ -323,73 +354,43 @@ __global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, FLUXO_MHD_VOL_MINB) 
       double ro[NQ], mo[3], racc[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) racc[v] = 0.;
-      if (valid) {
+      if (lv) {
 #pragma unroll
-        for (int z = 0; z < NQ; ++z) ro[z] = rec[os * RS + z];
+        for (int z = 0; z < NQ; ++z) ro[z] = prec[os * RS + z];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) mo[c] = rec[os * RS + NQ + 3 * dir + c];
+        for (int c = 0; c < 3; ++c) mo[c] = prec[os * RS + NQ + 3 * dir + c];
       }
-      if constexpr (32 % NP == 0) {
-        const int lane = threadIdx.x & 31, lbase = lane - p;
 #pragma unroll
-        for (int d = 1; d <= NP / 2; ++d) {
-          const bool active = valid && (2 * d < NP || p < d);
-          int q = p + d;
-          if (q >= NP) q -= NP;
-          double F[NV];
+      for (int d = 1; d <= NP / 2; ++d) {
+        const bool active = lv && (2 * d < NP || p < d);
+        int q = p + d;
+        if (q >= NP) q -= NP;
+        double F[NV];
 #pragma unroll
-          for (int v = 0; v < NV; ++v) F[v] = 0.;
-          if (active) {
-            const int nq = vol_slot(base + q * stride);
-            double rp[NQ], mp[3];
-#pragma unroll
-            for (int z = 0; z < NQ; ++z) rp[z] = rec[nq * RS + z];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) mp[c] = rec[nq * RS + NQ + 3 * dir + c];
-            pair_flux_mhd<VF>(P, ch, ro, rp, mo, mp, F);
-          }
-          const double dOwn = sDvs[p * NP + q], dPart = sDvs[q * NP + p];
-          int src = p - d;
-          if (src < 0) src += NP;
-          const bool receive = valid && (2 * d < NP || p >= d);
-#pragma unroll
-          for (int v = 0; v < NV; ++v) {
-            racc[v] += active ? dOwn * F[v] : 0.;
-            const double got = __shfl_sync(0xffffffffu, dPart * F[v], lbase + src);
-            racc[v] += receive ? got : 0.;
-          }
+        for (int v = 0; v < NV; ++v) F[v] = 0.;
+        if (active) {
+          // the partner's record is read in place (the log-mean logarithms only when needed)
+          const double* rq = prec + vol_slot(base + q * stride) * RS;
+          pair_flux_mhd<VF>(P, ch, ro, rq, mo, rq + NQ + 3 * dir, F);
         }
-      } else {
-#pragma unroll 1
-        for (int d = 1; d <= NP / 2; ++d) {
-          const bool active = valid && (2 * d < NP || p < d);
-          if (active) {
-            int q = p + d;
-            if (q >= NP) q -= NP;
-            const int nq = vol_slot(base + q * stride);
-            double rp[NQ], mp[3], F[NV];
+        const double dOwn = sDvs[p * NP + q], dPart = sDvs[q * NP + p];
+        int src = p - d;
+        if (src < 0) src += NP;
+        const bool receive = lv && (2 * d < NP || p >= d);
 #pragma unroll
-            for (int z = 0; z < NQ; ++z) rp[z] = rec[nq * RS + z];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) mp[c] = rec[nq * RS + NQ + 3 * dir + c];
-            pair_flux_mhd<VF>(P, ch, ro, rp, mo, mp, F);
-            const double dOwn = sDvs[p * NP + q], dPart = sDvs[q * NP + p];
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-              racc[v] += dOwn * F[v];
-              acc[nq * NACC + v] += dPart * F[v];
-            }
-          }
-          __syncthreads();
+        for (int v = 0; v < NV; ++v) {
+          racc[v] += active ? dOwn * F[v] : 0.;
+          const double got = __shfl_sync(0xffffffffu, dPart * F[v], (lbase + src) & 31);
+          racc[v] += receive ? got : 0.;
         }
       }
       double ncMHD = 0., ncGLM = 0.;  // this direction's non-conservative line sums of node `own`
       {
-        if (valid && NC != 0) {
+        if (lv && NC != 0) {
           double sB0 = 0., sB1 = 0., sB2 = 0., sBh = 0., sPsi = 0.;
 #pragma unroll
           for (int l = 0; l < NP; ++l) {
-            const double* rl = rec + vol_slot(base + l * stride) * RS;
+            const double* rl = prec + vol_slot(base + l * stride) * RS;
             const double dl = sDvs[p * NP + l];
             const double b0 = rl[IB], b1 = rl[IB + 1], b2 = rl[IB + 2];
             const double* ml = rl + NQ + 3 * dir;
@@ -405,11 +406,11 @@ __global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, FLUXO_MHD_VOL_MINB) 
           }
         }
       }
-      if (valid) {
+      if (lv) {
 #pragma unroll
-        for (int v = 0; v < NV; ++v) acc[os * NACC + v] += racc[v];
-        acc[os * NACC + NV] += ncMHD;
-        acc[os * NACC + NV + 1] += ncGLM;
+        for (int v = 0; v < NV; ++v) pacc[os * NACC + v] += racc[v];
+        pacc[os * NACC + NV] += ncMHD;
+        pacc[os * NACC + NV + 1] += ncGLM;
       }
       __syncthreads();
     }

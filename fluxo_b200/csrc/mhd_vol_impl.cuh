@@ -13,7 +13,7 @@ cudaError_t volume_np(int nElems, cudaStream_t s, const KParams& P) {
   auto k = mhd::volume_kernel<NP, VF>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  k<<<(nElems + EPB - 1) / EPB, EPB * NP * NP * NP, smem, s>>>(P);
+  k<<<(nElems + EPB - 1) / EPB, mhd::vol_threads<NP>(), smem, s>>>(P);
   return cudaGetLastError();
 }
 
