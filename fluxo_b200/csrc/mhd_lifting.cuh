@@ -21,11 +21,13 @@ __host__ __device__ constexpr size_t lv_smem_bytes() {
   return sizeof(double) * (size_t)(2 * NP * NP + epb<NP>() * 36 * lv_slots<NP>());
 }
 
-#ifndef FLUXO_MHD_LV_MINB
-#define FLUXO_MHD_LV_MINB 1
-#endif
+// resident blocks per SM the register allocation must allow: 2 for BR1 blocks of up to 320 threads
+// (more resident warps than the ~150 registers it would take unconstrained), else 1
 template <int NP, int LIFT>
-__global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, FLUXO_MHD_LV_MINB) lift_visc_kernel(KParams P) {
+__host__ __device__ constexpr int lv_minb() { return (LIFT == 1 && epb<NP>() * NP * NP * NP <= 320) ? 2 : 1; }
+
+template <int NP, int LIFT>
+__global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, lv_minb<NP, LIFT>()) lift_visc_kernel(KParams P) {
   if (halted(P)) return;
   constexpr int NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1, EPB = epb<NP>(), NS = lv_slots<NP>();
   extern __shared__ double smem[];
