@@ -57,7 +57,7 @@ struct KParams {
   double* flux;
   double* lflux;
   double* gtrace;         // face traces of the viscous flux: n.F_v(U, gradP trace) of the master / slave
-                          // side [side][master|slave][4][pt] (Navier-Stokes; MHD: gradient traces)
+                          // side [side][master|slave][4 (Navier-Stokes) or 7 (MHD)][pt]
   const BasisTables* basis;
   // physics constants (navierstokes/equation.f90:162-260)
   double kappa, kappaM1, sKappaM1, kappaP1, R, s23, KappasPr, mu0, Ts, sTref, ExpoSuth, cSuth, ExpoPow;

@@ -508,9 +508,8 @@ int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* S2E, 
   if (h->visc) {
     if ((r = dalloc(h, &h->dGrad, 3 * nU)) || (r = dalloc(h, &h->dLFlux, nF)) ||
         (r = dalloc(h, &h->dUtVisc, (size_t)(h->mhd ? 7 : 4) * NP3 * nElems)) ||
-        // face traces per side and point: MHD the 27 gradient components of both sides,
-        // Navier-Stokes the 4 components of n.F_v of both sides
-        (r = dalloc(h, &h->dGTrace, (size_t)2 * (h->mhd ? 3 * NV : 4) * NPT * nSides)))
+        // face traces per side and point: n.F_v of both sides (MHD 7 components, Navier-Stokes 4)
+        (r = dalloc(h, &h->dGTrace, (size_t)2 * (h->mhd ? 7 : 4) * NPT * nSides)))
       return r;
   }
   if (h->mhd) {  // InitTimeStep_GLM, mhd/calctimestep.f90:187-223

@@ -63,19 +63,11 @@ __global__ void face_kernel(KParams P, int NP) {
     F[b + 1] = nv[1] * f2 + t1[1] * f3 + t2[1] * f4;
     F[b + 2] = nv[2] * f2 + t1[2] * f3 + t2[2] * f4;
   }
-  if constexpr (VISC) {
-    const double* tM = P.gtrace + ((size_t)side * 2 + 0) * 27 * npts + pt;
-    const double* tS = P.gtrace + ((size_t)side * 2 + 1) * 27 * npts + pt;
-    double gl[27], gr[27];
+  if constexpr (VISC) {  // + 1/2 (n.F_v(L) + n.F_v(R)); each side's share from its lifting kernel
+    const double* tM = P.gtrace + ((size_t)side * 2 + 0) * 7 * npts + pt;
+    const double* tS = P.gtrace + ((size_t)side * 2 + 1) * 7 * npts + pt;
 #pragma unroll
-    for (int c = 0; c < 27; ++c) { gl[c] = tM[(size_t)c * npts]; gr[c] = tS[(size_t)c * npts]; }
-    double kL[7], gL[7], jL[7], kR[7], gR[7], jR[7];
-    visc_flux_3d(P, uL, gl, gl + 9, gl + 18, kL, gL, jL);
-    visc_flux_3d(P, uR, gr, gr + 9, gr + 18, kR, gR, jR);
-#pragma unroll
-    for (int v = 1; v < 8; ++v)
-      F[v] = F[v] + 0.5 * (nv[0] * (kL[v - 1] + kR[v - 1]) + nv[1] * (gL[v - 1] + gR[v - 1]) +
-                           nv[2] * (jL[v - 1] + jR[v - 1]));
+    for (int v = 1; v < 8; ++v) F[v] = F[v] + 0.5 * (tM[(v - 1) * npts] + tS[(v - 1) * npts]);
   }
   double* out = P.flux + (size_t)side * NF * npts + pt;
 #pragma unroll

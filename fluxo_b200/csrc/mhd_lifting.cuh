@@ -3,7 +3,8 @@
 //   1. BR1/BR2 gradients of the lifting variable (strong-form volume derivative br1_volint.f90:45-98 /
 //      br2_volint.f90:45-103, surface lifting br1_surfint.f90:52-131 / br2_surfint.f90:53-148,
 //      Jacobian, ConvertToGradPrim mhd/equation_vars.f90:547-628);
-//   2. the face traces gradP_master/slave, side-major ([side][master|slave][27][pt]);
+//   2. each side's share n.F_v(U, gradP trace) of the viscous / resistive face flux (7 components,
+//      side-major [side][master|slave][7][pt]) from the face trace of the gradient;
 //   3. the viscous / resistive volume integral sum_l D_hat(i,l) (f~,g~,h~)(l) of variables 2..8
 //      (volint.f90:228-271 with EvalDiffFluxTilde3D mhd/flux.f90:579-712), 7 values per node.
 #pragma once
@@ -101,13 +102,11 @@ __global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, lv_minb<NP, LIFT>())
     int sides[3];
     const int ns = boundary_sides(i, j, k, N, sides);
     const double lh = P.basis->LhatM0;
-    int tside[3], tms[3], tpt[3];
     for (int z = 0; z < ns; ++z) {
       const int s = sides[z];
       const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
       const int side = es[0], flip = es[1];
       const int pt = node_side_point(N, s, flip, i, j, k);
-      tside[z] = side; tms[z] = flip == 0 ? 0 : 1; tpt[z] = pt;
       const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
       const double* F = P.lflux + (size_t)side * NV * NPT + pt;
       const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
@@ -124,11 +123,12 @@ __global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, lv_minb<NP, LIFT>())
         }
 #pragma unroll
         for (int d = 0; d < 3; ++d) to_grad_prim_rt(P, u, tr[d]);
-        double* T = P.gtrace + ((size_t)side * 2 + tms[z]) * 27 * NPT + pt;
+        // this side's share of the viscous / resistive face flux: n.F_v(U, trace) (7 components)
+        double kf[7], kg[7], kh[7];
+        visc_flux_3d(P, u, tr[0], tr[1], tr[2], kf, kg, kh);
+        double* T = P.gtrace + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 7 * NPT + pt;
 #pragma unroll
-        for (int d = 0; d < 3; ++d)
-#pragma unroll
-          for (int v = 0; v < NV; ++v) T[(size_t)(9 * d + v) * NPT] = tr[d][v];
+        for (int v = 0; v < 7; ++v) T[(size_t)v * NPT] = n0 * kf[v] + n1 * kg[v] + n2 * kh[v];
       } else {
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
@@ -145,15 +145,6 @@ __global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, lv_minb<NP, LIFT>())
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) to_grad_prim_rt(P, u, g[d]);
-    if constexpr (LIFT == 1) {
-      for (int z = 0; z < ns; ++z) {
-        double* T = P.gtrace + ((size_t)tside[z] * 2 + tms[z]) * 27 * NPT + tpt[z];
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
-#pragma unroll
-          for (int v = 0; v < NV; ++v) T[(size_t)(9 * d + v) * NPT] = g[d][v];
-      }
-    }
     if (P.grad) {
       double* G = P.grad + 27 * ((size_t)e * NP3 + t);
 #pragma unroll
@@ -163,6 +154,21 @@ __global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, lv_minb<NP, LIFT>())
     }
     double f[7], gg[7], h[7];
     visc_flux_3d(P, u, g[0], g[1], g[2], f, gg, h);
+    if constexpr (LIFT == 1) {
+      // BR1: the face trace of the gradient is the volume gradient at the boundary node, so this
+      // side's share of the viscous / resistive face flux is n.F_v of the node
+      for (int z = 0; z < ns; ++z) {
+        const int s = sides[z];
+        const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
+        const int side = es[0], flip = es[1];
+        const int pt = node_side_point(N, s, flip, i, j, k);
+        const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
+        const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
+        double* T = P.gtrace + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 7 * NPT + pt;
+#pragma unroll
+        for (int v = 0; v < 7; ++v) T[(size_t)v * NPT] = n0 * f[v] + n1 * gg[v] + n2 * h[v];
+      }
+    }
 #pragma unroll
     for (int v = 0; v < 7; ++v) {
       ft[0 + v] = f[v] * m[0] + gg[v] * m[1] + h[v] * m[2];
