@@ -106,28 +106,37 @@ def config_dict(w, n_gpus, steps):
 
 # ------------------------------------------------------------------------------------------------
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms; the summary keeps the samples whose
+    timestamps fall in the timed region (the sampler is started, and its first sample awaited, before
+    the region begins; when the region is shorter than the period the nearest sample stands in)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
         self.index = index
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.p = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                       "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
                                       stderr=subprocess.DEVNULL)
+            deadline = time.time() + 3.0
+            while time.time() < deadline and os.path.getsize(self.f.name) == 0:
+                time.sleep(0.02)
         except OSError:
             self.p = None
+        self.t0 = time.time()
         return self
 
     def __exit__(self, *a):
+        self.t1 = time.time()
         if self.p is not None:
+            time.sleep(0.15)  # one more sample after the region
             self.p.terminate()
             try:
                 self.p.wait(timeout=5)
@@ -135,23 +144,36 @@ class ClockSampler:
                 self.p.kill()
 
     def summary(self):
+        import datetime
+
         self.f.flush()
         self.f.seek(0)
-        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        rows = []
+        for line in self.f.read().strip().splitlines():
+            r = [x.strip() for x in line.split(",")]
+            try:
+                ts = datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, r))
+            except (ValueError, IndexError):
+                continue
         os.unlink(self.f.name)
+        inside = [r for ts, r in rows if self.t0 is not None and self.t0 <= ts <= self.t1]
+        if not inside and rows and self.t0 is not None:
+            mid = 0.5 * (self.t0 + self.t1)
+            inside = [min(rows, key=lambda x: abs(x[0] - mid))[1]]
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
+        for r in inside:
             try:
-                sm.append(float(r[1]))
-                mx = float(r[2])
+                sm.append(float(r[2]))
+                mx = float(r[3])
                 for k, nm in enumerate(names):
-                    if r[5 + k].strip().lower() == "active":
+                    if r[6 + k].lower() == "active":
                         reasons.add(nm)
             except (ValueError, IndexError):
                 continue
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "timed_s": (self.t1 - self.t0) if self.t0 is not None else None}
 
 
 def dist_setup(n_gpus):
@@ -637,7 +659,7 @@ def run_serve(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fluxo", choices=("fluxo", "reference"))
     ap.add_argument("--workload", default="tgv", choices=("tgv", "mhd", "batch", "serve"),
