@@ -60,9 +60,10 @@ struct KParams {
                           // side [side][master|slave][4 (Navier-Stokes) or 7 (MHD)][pt]
   const BasisTables* basis;
   // physics constants (navierstokes/equation.f90:162-260)
-  double kappa, kappaM1, sKappaM1, kappaP1, R, s23, KappasPr, mu0, Ts, sTref, ExpoSuth, cSuth, ExpoPow;
+  double kappa, kappaM1, sKappaM1, kappaP1, sKappa, R, s23, KappasPr, mu0, Ts, sTref, ExpoSuth, cSuth, ExpoPow;
   double etaBR2;
   int visc, lifting_var, lifting;
+  int volumeFlux;         // VolumeFlux id (the Roe solver's baseline flux depends on it)
   // source term (IniExactFunc 4)
   int source;
   double srcOmega, srcTmp[6];

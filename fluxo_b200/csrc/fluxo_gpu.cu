@@ -345,6 +345,7 @@ void basis_tables_for(int N, BasisTables& B) { build_basis_tables(N, B); }
 // Equation constants of the Euler / Navier-Stokes kernels (navierstokes/equation.f90:162-260)
 void fill_ns_physics(KParams& P, const fluxo_cfg& c) {
   P.kappa = c.kappa; P.kappaM1 = c.kappa - 1.; P.sKappaM1 = 1. / (c.kappa - 1.); P.kappaP1 = c.kappa + 1.;
+  P.sKappa = 1. / c.kappa; P.volumeFlux = c.volume_flux;
   P.R = c.R; P.s23 = 2. / 3.; P.KappasPr = c.kappa / c.Pr; P.mu0 = c.mu0;
   P.visc = c.visc; P.lifting_var = c.lifting_var; P.lifting = c.lifting; P.etaBR2 = c.etaBR2;
   if (c.visc == 1) {  // equation.f90:226-233 (Sutherland constants)

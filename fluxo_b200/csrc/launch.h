@@ -23,7 +23,13 @@ cudaError_t launch_volume_shape(int NP, int VF, bool visc, int shape, int nElems
 cudaError_t launch_volume_vf0(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
 cudaError_t launch_volume_vf1(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
 cudaError_t launch_volume_vf2(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf3(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf4(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
 cudaError_t launch_volume_vf5(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf6(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf7(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf8(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_volume_vf9(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
 cudaError_t launch_volume_vf10(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
 cudaError_t launch_volume_vf32(int NP, bool visc, int shape, int nElems, cudaStream_t s, const KParams& P);
 // Autotuner of the volume kernel's launch shape: times every candidate shape of (NP, VF, visc) on the

@@ -14,7 +14,13 @@ cudaError_t launch_volume_shape(int NP, int VF, bool visc, int shape, int nElems
     case 0: return launch_volume_vf0(NP, visc, shape, nElems, s, P);
     case 1: return launch_volume_vf1(NP, visc, shape, nElems, s, P);
     case 2: return launch_volume_vf2(NP, visc, shape, nElems, s, P);
+    case 3: return launch_volume_vf3(NP, visc, shape, nElems, s, P);
+    case 4: return launch_volume_vf4(NP, visc, shape, nElems, s, P);
     case 5: return launch_volume_vf5(NP, visc, shape, nElems, s, P);
+    case 6: return launch_volume_vf6(NP, visc, shape, nElems, s, P);
+    case 7: return launch_volume_vf7(NP, visc, shape, nElems, s, P);
+    case 8: return launch_volume_vf8(NP, visc, shape, nElems, s, P);
+    case 9: return launch_volume_vf9(NP, visc, shape, nElems, s, P);
     case 10: return launch_volume_vf10(NP, visc, shape, nElems, s, P);
     case 32: return launch_volume_vf32(NP, visc, shape, nElems, s, P);
     default: return cudaErrorInvalidValue;
@@ -93,12 +99,14 @@ cudaError_t tune_volume(int NP, int VF, bool visc, int nElems, cudaStream_t s, c
 }
 
 bool volume_flux_supported(int VF) {
-  return VF == 0 || VF == 1 || VF == 2 || VF == 5 || VF == 10 || VF == 32;
+  return (VF >= 0 && VF <= 10) || VF == 32;
 }
 
 bool riemann_supported(int RS) {
   switch (RS) {
-    case 0: case 1: case 22: case 4: case 44: case 33: case 5: case 9: case 32: case 6: case 13: case 14: case 16:
+    case 0: case 1: case 2: case 3: case 4: case 5: case 6: case 7: case 8: case 9: case 10: case 11: case 12:
+    case 13: case 14: case 15: case 16: case 17: case 18: case 19: case 20: case 21: case 22: case 23: case 24:
+    case 32: case 33: case 44:
       return true;
     default:
       return false;
@@ -118,9 +126,11 @@ cudaError_t launch_face_flux(int RS, bool visc, int NP, int nSides, cudaStream_t
 #define FLUXO_RS_CASE(K) \
   case K: return visc ? face_t<K, true>(NP, nSides, s, P) : face_t<K, false>(NP, nSides, s, P);
   switch (RS) {
-    FLUXO_RS_CASE(0) FLUXO_RS_CASE(1) FLUXO_RS_CASE(22) FLUXO_RS_CASE(4) FLUXO_RS_CASE(44)
-    FLUXO_RS_CASE(33) FLUXO_RS_CASE(5) FLUXO_RS_CASE(9) FLUXO_RS_CASE(32) FLUXO_RS_CASE(6)
-    FLUXO_RS_CASE(13) FLUXO_RS_CASE(14) FLUXO_RS_CASE(16)
+    FLUXO_RS_CASE(0) FLUXO_RS_CASE(1) FLUXO_RS_CASE(2) FLUXO_RS_CASE(3) FLUXO_RS_CASE(4) FLUXO_RS_CASE(5)
+    FLUXO_RS_CASE(6) FLUXO_RS_CASE(7) FLUXO_RS_CASE(8) FLUXO_RS_CASE(9) FLUXO_RS_CASE(10) FLUXO_RS_CASE(11)
+    FLUXO_RS_CASE(12) FLUXO_RS_CASE(13) FLUXO_RS_CASE(14) FLUXO_RS_CASE(15) FLUXO_RS_CASE(16) FLUXO_RS_CASE(17)
+    FLUXO_RS_CASE(18) FLUXO_RS_CASE(19) FLUXO_RS_CASE(20) FLUXO_RS_CASE(21) FLUXO_RS_CASE(22) FLUXO_RS_CASE(23)
+    FLUXO_RS_CASE(24) FLUXO_RS_CASE(32) FLUXO_RS_CASE(33) FLUXO_RS_CASE(44)
     default: return cudaErrorInvalidValue;
   }
 #undef FLUXO_RS_CASE

@@ -15,107 +15,12 @@ __device__ __forceinline__ double ln_mean(double aL, double aR) {
   return (aR - aL) / log(xi);
 }
 
-// auxiliary variables of EvalUaux (flux_average.f90:305-332): 1/rho, v1, v2, v3, p, |v|^2
-struct Aux { double srho, v1, v2, v3, p, v2s; };
-
-__device__ __forceinline__ Aux eval_aux(const KParams& P, const double* U) {
-  Aux a;
-  a.srho = 1. / U[0];
-  a.v1 = U[1] * a.srho; a.v2 = U[2] * a.srho; a.v3 = U[3] * a.srho;
-  a.v2s = a.v1 * a.v1 + a.v2 * a.v2 + a.v3 * a.v3;
-  a.p = P.kappaM1 * (U[4] - 0.5 * U[0] * a.v2s);
-  return a;
-}
-
-// Metric-transformed two-point volume fluxes (VolumeFluxAverageVec, flux_average.f90).
-template <int VF>
-__device__ __forceinline__ void volume_flux_vec(const KParams& P, const double* UL, const double* UR, const Aux& aL,
-                                                const Aux& aR, const double* mL, const double* mR, double* F) {
-  if constexpr (VF == 0) {  // StandardDGFluxVec :394-439
-    double qL = aL.v1 * mL[0] + aL.v2 * mL[1] + aL.v3 * mL[2];
-    double qR = aR.v1 * mR[0] + aR.v2 * mR[1] + aR.v3 * mR[2];
-    F[0] = 0.5 * (UL[0] * qL + UR[0] * qR);
-    F[1] = 0.5 * (UL[1] * qL + UR[1] * qR + mL[0] * aL.p + mR[0] * aR.p);
-    F[2] = 0.5 * (UL[2] * qL + UR[2] * qR + mL[1] * aL.p + mR[1] * aR.p);
-    F[3] = 0.5 * (UL[3] * qL + UR[3] * qR + mL[2] * aL.p + mR[2] * aR.p);
-    F[4] = 0.5 * ((UL[4] + aL.p) * qL + (UR[4] + aR.p) * qR);
-  } else {
-    const double m1 = 0.5 * (mL[0] + mR[0]), m2 = 0.5 * (mL[1] + mR[1]), m3 = 0.5 * (mL[2] + mR[2]);
-    if constexpr (VF == 1) {  // StandardDGFluxDealiasedMetricVec :446-494
-      double qL = aL.v1 * m1 + aL.v2 * m2 + aL.v3 * m3;
-      double qR = aR.v1 * m1 + aR.v2 * m2 + aR.v3 * m3;
-      double ps = aL.p + aR.p;
-      F[0] = 0.5 * (UL[0] * qL + UR[0] * qR);
-      F[1] = 0.5 * (UL[1] * qL + UR[1] * qR + m1 * ps);
-      F[2] = 0.5 * (UL[2] * qL + UR[2] * qR + m2 * ps);
-      F[3] = 0.5 * (UL[3] * qL + UR[3] * qR + m3 * ps);
-      F[4] = 0.5 * ((UL[4] + aL.p) * qL + (UR[4] + aR.p) * qR);
-    } else if constexpr (VF == 2) {  // KennedyAndGruberFluxVec1 :731-803
-      double rhoHat = 0.5 * (UL[0] + UR[0]);
-      double uH = 0.5 * (aL.v1 + aR.v1), vH = 0.5 * (aL.v2 + aR.v2), wH = 0.5 * (aL.v3 + aR.v3);
-      double p1 = 0.5 * (aL.p + aR.p);
-      double eH = 0.5 * (aL.srho * UL[4] + aR.srho * UR[4]);
-      double q = uH * m1 + vH * m2 + wH * m3;
-      F[0] = rhoHat * q;
-      F[1] = F[0] * uH + m1 * p1;
-      F[2] = F[0] * vH + m2 * p1;
-      F[3] = F[0] * wH + m3 * p1;
-      F[4] = F[0] * eH + p1 * q;
-    } else if constexpr (VF == 5) {  // EntropyAndEnergyConservingFluxVec :1277-1356
-      double bL = 0.5 * UL[0] / aL.p, bR = 0.5 * UR[0] / aR.p;
-      double rhoM = 0.5 * (UL[0] + UR[0]);
-      double rhoHat = ln_mean(UL[0], UR[0]);
-      double bM = 0.5 * (bL + bR);
-      double bHat = ln_mean(bL, bR);
-      double uH = 0.5 * (aL.v1 + aR.v1), vH = 0.5 * (aL.v2 + aR.v2), wH = 0.5 * (aL.v3 + aR.v3);
-      double p1 = 0.5 * rhoM / bM;
-      double q = uH * m1 + vH * m2 + wH * m3;
-      F[0] = rhoHat * q;
-      F[1] = F[0] * uH + m1 * p1;
-      F[2] = F[0] * vH + m2 * p1;
-      F[3] = F[0] * wH + m3 * p1;
-      F[4] = F[0] * 0.5 * (P.sKappaM1 / bHat - 0.5 * (aL.v2s + aR.v2s)) + uH * F[1] + vH * F[2] + wH * F[3];
-    } else if constexpr (VF == 10) {  // TwoPointEntropyConservingFluxVec :574-673
-      double z1L = sqrt(UL[0] / aL.p), z1R = sqrt(UR[0] / aR.p);
-      double z1M = 0.5 * (z1L + z1R);
-      double z1LN = ln_mean(z1L, z1R);
-      double z2M = 0.5 * (z1L * aL.v1 + z1R * aR.v1);
-      double z3M = 0.5 * (z1L * aL.v2 + z1R * aR.v2);
-      double z4M = 0.5 * (z1L * aL.v3 + z1R * aR.v3);
-      double z5L = z1L * aL.p, z5R = z1R * aR.p;
-      double z5M = 0.5 * (z5L + z5R);
-      double z5LN = ln_mean(z5L, z5R);
-      double rhoHat = z1M * z5LN;
-      double sz1M = 1. / z1M;
-      double uH = z2M * sz1M, vH = z3M * sz1M, wH = z4M * sz1M;
-      double p1 = z5M * sz1M;
-      double q = uH * m1 + vH * m2 + wH * m3;
-      F[0] = rhoHat * q;
-      F[1] = F[0] * uH + m1 * p1;
-      F[2] = F[0] * vH + m2 * p1;
-      F[3] = F[0] * wH + m3 * p1;
-      F[4] = 0.5 * (q * P.kappaP1 * P.sKappaM1 * (z5LN / z1LN) + uH * F[1] + vH * F[2] + wH * F[3]);
-    } else if constexpr (VF == 32) {  // RanochaFluxVec :1876-1929
-      double rhoLN = ln_mean(UL[0], UR[0]);
-      double va1 = 0.5 * (aL.v1 + aR.v1), va2 = 0.5 * (aL.v2 + aR.v2), va3 = 0.5 * (aL.v3 + aR.v3);
-      double v2zip = 0.5 * (aL.v1 * aR.v1 + aL.v2 * aR.v2 + aL.v3 * aR.v3);
-      double pavg = 0.5 * (aL.p + aR.p);
-      double vmL = aL.v1 * m1 + aL.v2 * m2 + aL.v3 * m3;
-      double vmR = aR.v1 * m1 + aR.v2 * m2 + aR.v3 * m3;
-      double rspM = ln_mean(UL[0] / aL.p, UR[0] / aR.p);
-      F[0] = rhoLN * 0.5 * (vmL + vmR);
-      F[1] = F[0] * va1 + m1 * pavg;
-      F[2] = F[0] * va2 + m2 * pavg;
-      F[3] = F[0] * va3 + m3 * pavg;
-      F[4] = F[0] * (v2zip + 1. / rspM * P.sKappaM1) + 0.5 * (aL.p * vmR + aR.p * vmL);
-    }
-  }
-}
-
 // Roe-type mean values returned by the 1D two-point fluxes (VolumeFluxAverage interface).
 struct Hat { double u, v, w, a, H, p1, rho; };
 
-// 1D two-point fluxes on rotated states (flux_average.f90): 10 Ismail-Roe, 5 EC-KEP, 32 Ranocha, 2 K&G.
+// 1D two-point fluxes on rotated states (flux_average.f90), numbered like VolumeFlux: 2 and 8
+// Kennedy-Gruber, 3 Ducros, 4 Morinishi, 5 EC-KEP, 6 approximate EC-KEP, 7 EC-KEP with pressure
+// average, 9 Gassner-Winters-Walch, 10 Ismail-Roe, 32 Ranocha.
 template <int W>
 __device__ __forceinline__ void volume_flux_1d(const KParams& P, const double* UL, const double* UR, double* F,
                                                Hat& h) {
@@ -179,6 +84,87 @@ __device__ __forceinline__ void volume_flux_1d(const KParams& P, const double* U
     F[2] = F[0] * h.v;
     F[3] = F[0] * h.w;
     F[4] = F[0] * (v2zip + 1. / rspM * P.sKappaM1) + 0.5 * (pL * uR + pR * uL);
+  } else if constexpr (W == 3) {  // DucrosFlux :937-979
+    h.rho = 0.5 * (UL[0] + UR[0]);
+    h.u = 0.5 * (uL + uR); h.v = 0.5 * (vL + vR); h.w = 0.5 * (wL + wR);
+    h.p1 = 0.5 * P.kappaM1 *
+           (UL[4] + UR[4] - 0.5 * (UL[1] * uL + UL[2] * vL + UL[3] * wL + UR[1] * uR + UR[2] * vR + UR[3] * wR));
+    h.a = sqrt(P.kappa * h.p1 / h.rho);
+    h.H = P.kappa * h.p1 / (h.rho * P.kappaM1) + 0.5 * (h.u * h.u + h.v * h.v + h.w * h.w);
+    const double qLR = 0.5 * h.u;
+    F[0] = h.rho * (qLR + qLR);
+    F[1] = qLR * (UL[1] + UR[1]) + h.p1;
+    F[2] = qLR * (UL[2] + UR[2]);
+    F[3] = qLR * (UL[3] + UR[3]);
+    F[4] = qLR * ((UL[4] + UR[4]) + (h.p1 + h.p1));
+  } else if constexpr (W == 4) {  // MorinishiFlux :1066-1113
+    const double vel2L = uL * uL + vL * vL + wL * wL, vel2R = uR * uR + vR * vR + wR * wR;
+    const double pL = P.kappaM1 * (UL[4] - 0.5 * UL[0] * vel2L), pR = P.kappaM1 * (UR[4] - 0.5 * UR[0] * vel2R);
+    h.rho = 0.5 * (UL[0] + UR[0]);
+    h.u = 0.5 * (uL + uR); h.v = 0.5 * (vL + vR); h.w = 0.5 * (wL + wR);
+    h.p1 = 0.5 * (pL + pR);
+    h.a = sqrt(P.kappa * h.p1 / h.rho);
+    h.H = P.kappa * h.p1 / (h.rho * P.kappaM1) + 0.5 * (h.u * h.u + h.v * h.v + h.w * h.w);
+    const double rq2L = 0.5 * UL[0] * uL, rq2R = 0.5 * UR[0] * uR;
+    F[0] = rq2L + rq2R;
+    F[1] = F[0] * h.u + h.p1;
+    F[2] = F[0] * h.v;
+    F[3] = F[0] * h.w;
+    F[4] = 0.5 * (P.kappa * P.sKappaM1 * (pL * uL + pR * uR) - (rq2L * vel2L + rq2R * vel2R)) +
+           rq2L * (uL * h.u + vL * h.v + wL * h.w) + rq2R * (uR * h.u + vR * h.v + wR * h.w);
+  } else if constexpr (W == 6 || W == 7) {
+    // EntropyAndEnergyConservingFlux2 :1365-1419 (6) and ggFlux :1513-1567 (7); a = H = 0
+    const double v2s2L = 0.5 * (uL * uL + vL * vL + wL * wL), v2s2R = 0.5 * (uR * uR + vR * vR + wR * wR);
+    const double pL = P.kappaM1 * (UL[4] - UL[0] * v2s2L), pR = P.kappaM1 * (UR[4] - UR[0] * v2s2R);
+    const double bL = 0.5 * UL[0] / pL, bR = 0.5 * UR[0] / pR;
+    h.a = 0.; h.H = 0.;
+    h.rho = ln_mean(UL[0], UR[0]);
+    h.u = 0.5 * (uL + uR); h.v = 0.5 * (vL + vR); h.w = 0.5 * (wL + wR);
+    double rhoF, sb;  // density of the mass flux, 1/beta of the energy flux
+    if constexpr (W == 6) {
+      const double rhoM = 0.5 * (UL[0] + UR[0]);
+      sb = 2. / (bL + bR);
+      h.p1 = 0.5 * rhoM * sb;
+      rhoF = rhoM;
+    } else {
+      sb = 1. / ln_mean(bL, bR);
+      h.p1 = 0.5 * (pL + pR);
+      rhoF = h.rho;
+    }
+    F[0] = rhoF * h.u;
+    F[1] = F[0] * h.u + h.p1;
+    F[2] = F[0] * h.v;
+    F[3] = F[0] * h.w;
+    F[4] = F[0] * 0.5 * (P.sKappaM1 * sb - (v2s2L + v2s2R)) + h.u * F[1] + h.v * F[2] + h.w * F[3];
+  } else if constexpr (W == 8) {  // KennedyAndGruberFlux2 :810-850
+    const double pL = P.kappaM1 * (UL[4] - 0.5 * (UL[1] * uL + UL[2] * vL + UL[3] * wL));
+    const double pR = P.kappaM1 * (UR[4] - 0.5 * (UR[1] * uR + UR[2] * vR + UR[3] * wR));
+    h.rho = 0.5 * (UL[0] + UR[0]);
+    h.u = 0.5 * (uL + uR); h.v = 0.5 * (vL + vR); h.w = 0.5 * (wL + wR);
+    h.p1 = 0.5 * (pL + pR);
+    h.a = sqrt(P.kappa * h.p1 / h.rho);
+    h.H = 0.5 * ((UL[4] + pL) * sRL + (UR[4] + pR) * sRR);
+    F[0] = h.rho * h.u;
+    F[1] = F[0] * h.u + h.p1;
+    F[2] = F[0] * h.v;
+    F[3] = F[0] * h.w;
+    F[4] = F[0] * h.H;
+  } else if constexpr (W == 9) {  // GassnerWintersWalchFlux :1661-1716 (a = 0)
+    const double pL = P.kappaM1 * (UL[4] - 0.5 * (UL[1] * uL + UL[2] * vL + UL[3] * wL));
+    const double pR = P.kappaM1 * (UR[4] - 0.5 * (UR[1] * uR + UR[2] * vR + UR[3] * wR));
+    const double w1L = sqrt(UL[0]), w1R = sqrt(UR[0]);
+    h.rho = 0.5 * (w1L + w1R);
+    h.u = 0.5 * (w1L * uL + w1R * uR);
+    h.v = 0.5 * (w1L * vL + w1R * vR);
+    h.w = 0.5 * (w1L * wL + w1R * wR);
+    h.H = 0.5 * (w1L * (sRL * (UL[4] + pL)) + w1R * (sRR * (UR[4] + pR)));
+    h.p1 = P.kappaM1 * P.sKappa * (h.rho * h.H - 0.5 * (h.u * h.u + h.v * h.v + h.w * h.w));
+    h.a = 0.;
+    F[0] = h.u * h.rho;
+    F[1] = h.u * h.u + h.p1;
+    F[2] = h.u * h.v;
+    F[3] = h.u * h.w;
+    F[4] = h.u * h.H;
   } else {  // W == 2: KennedyAndGruberFlux1 :680-721
     h.rho = 0.5 * (UL[0] + UR[0]);
     h.u = 0.5 * (uL + uR); h.v = 0.5 * (vL + vR); h.w = 0.5 * (wL + wR);
@@ -222,8 +208,21 @@ __device__ __forceinline__ void primitive_pv(const KParams& P, const double* U, 
   p = P.kappaM1 * (U[4] - 0.5 * (U[1] * v[0] + U[2] * v[1] + U[3] * v[2]));
 }
 
+// Point flux of the Riemann solvers that use RiemannSolver_VolumeFluxAverage (0: not such a
+// solver), navierstokes/equation.f90:291-406
+template <int RS>
+__host__ __device__ constexpr int riemann_point_flux() {
+  return RS == 5 ? 10 : RS == 6 ? 2 : RS == 7 ? 3 : RS == 8 ? 4 : RS == 9 ? 5 : RS == 10 ? 6 : RS == 11 ? 7
+       : RS == 12 ? 8 : RS == 20 ? 9 : RS == 32 ? 32 : 0;
+}
+// ... and of those using RiemannSolver_VolumeFluxAverage_LLF
+template <int RS>
+__host__ __device__ constexpr int riemann_llf_point_flux() {
+  return RS == 14 ? 2 : RS == 15 ? 3 : RS == 17 ? 7 : RS == 18 ? 8 : RS == 19 ? 4 : RS == 21 ? 9 : 0;
+}
+
 // Riemann solvers on rotated states (navierstokes/riemann.f90).  lmm is the maximum wave speed
-// over the side, used by the LLF-dissipation variants 13/14/16.
+// over the side, used by the LLF-dissipation variants 13-19 and 21.
 template <int RS>
 __device__ __forceinline__ void riemann_rotated(const KParams& P, const double* L, const double* R, double lmm,
                                                 double* F) {
@@ -295,16 +294,135 @@ __device__ __forceinline__ void riemann_rotated(const KParams& P, const double* 
     for (int r = 0; r < 5; ++r)
       F[r] = Fc[r] - 0.5 * (Rh[r][0] * diss[0] + Rh[r][1] * diss[1] + Rh[r][2] * diss[2] + Rh[r][3] * diss[3] +
                             Rh[r][4] * diss[4]);
-  } else if constexpr (RS == 5 || RS == 9 || RS == 32 || RS == 6) {
+  } else if constexpr (riemann_point_flux<RS>() > 0) {
     // RiemannSolver_VolumeFluxAverage :980-1005
-    constexpr int W = (RS == 5) ? 10 : (RS == 9 ? 5 : (RS == 32 ? 32 : 2));
     Hat h;
-    volume_flux_1d<W>(P, L, R, F, h);
-  } else if constexpr (RS == 14) {  // RiemannSolver_VolumeFluxAverage_LLF with K&G :1117-1148
+    volume_flux_1d<riemann_point_flux<RS>()>(P, L, R, F, h);
+  } else if constexpr (riemann_llf_point_flux<RS>() > 0) {  // RiemannSolver_VolumeFluxAverage_LLF :1117-1151
     double Fc[5];
     Hat h;
-    volume_flux_1d<2>(P, L, R, Fc, h);
+    volume_flux_1d<riemann_llf_point_flux<RS>()>(P, L, R, Fc, h);
     for (int v = 0; v < 5; ++v) F[v] = Fc[v] - 0.5 * lmm * (R[v] - L[v]);
+  } else if constexpr (RS == 2) {  // RiemannSolverByHLLC :552-615
+    double FL[5], FR[5];
+    euler_flux_1d(P, L, FL);
+    euler_flux_1d(P, R, FR);
+    double vL[3], vR[3], pL, pR;
+    primitive_pv(P, L, vL, pL);
+    primitive_pv(P, R, vR, pR);
+    const double sRL = 1. / L[0], sRR = 1. / R[0];
+    const double ssl = vL[0] - sqrt(P.kappa * pL * sRL);
+    const double ssr = vR[0] + sqrt(P.kappa * pR * sRR);
+    if (ssl >= 0.) {
+      for (int v = 0; v < 5; ++v) F[v] = FL[v];
+    } else if (ssr <= 0.) {
+      for (int v = 0; v < 5; ++v) F[v] = FR[v];
+    } else {
+      const double smuL = ssl - vL[0], smuR = ssr - vR[0];
+      const double sStar = (pR - pL + L[1] * smuL - R[1] * smuR) / (L[0] * smuL - R[0] * smuR);
+      const bool left = (ssl <= 0.) && (sStar >= 0.);
+      const double* U = left ? L : R;
+      const double* FF = left ? FL : FR;
+      const double ss = left ? ssl : ssr, smu = left ? smuL : smuR, sr = left ? sRL : sRR, p = left ? pL : pR;
+      const double vn = left ? vL[0] : vR[0];
+      const double fac = U[0] * smu / (ss - sStar);
+      const double Us[5] = {fac, fac * sStar, fac * (U[2] * sr), fac * (U[3] * sr),
+                            fac * (U[4] * sr + (sStar - vn) * (sStar + p * sr / smu))};
+      for (int v = 0; v < 5; ++v) F[v] = FF[v] + ss * (Us[v] - U[v]);
+    }
+  } else if constexpr (RS == 23 || RS == 24) {  // RiemannSolverByHLLE :393-462, ...HLLEM :466-547
+    double FL[5], FR[5];
+    euler_flux_1d(P, L, FL);
+    euler_flux_1d(P, R, FR);
+    double vL[3], vR[3], pL, pR;
+    primitive_pv(P, L, vL, pL);
+    primitive_pv(P, R, vR, pR);
+    const double beta = sqrt(0.5 * P.kappaM1 / P.kappa);
+    const double sRL = 1. / L[0], sRR = 1. / R[0];
+    const double aL = sqrt(P.kappa * pL * sRL), aR = sqrt(P.kappa * pR * sRR);
+    const double HL = (L[4] + pL) * sRL, HR = (R[4] + pR) * sRR;
+    const double sqL = sqrt(L[0]), sqR = sqrt(R[0]);
+    const double ssq = 1. / (sqL + sqR);
+    double rv[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) rv[d] = (sqR * vR[d] + sqL * vL[d]) * ssq;
+    const double rH = (sqR * HR + sqL * HL) * ssq;
+    const double absVel = rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2];
+    const double rc = sqrt(P.kappaM1 * (rH - 0.5 * absVel));
+    const double ssl = fmin(fmin(rv[0] - rc, vL[0] - beta * aL), 0.);
+    const double ssr = fmax(fmax(rv[0] + rc, vR[0] + beta * aR), 0.);
+    if (ssl >= 0. && ssr > 0.) {
+      for (int v = 0; v < 5; ++v) F[v] = FL[v];
+    } else if (ssr <= 0. && ssl < 0.) {
+      for (int v = 0; v < 5; ++v) F[v] = FR[v];
+    } else if constexpr (RS == 23) {
+      for (int v = 0; v < 5; ++v) F[v] = (ssr * FL[v] - ssl * FR[v] + ssl * ssr * (R[v] - L[v])) / (ssr - ssl);
+    } else {  // HLLEM: anti-diffusion along the Roe-mean entropy and shear waves
+      const double rd = sqrt(L[0] * R[0]);
+      const double delta = rc / (rc + fabs(0.5 * (ssl + ssr)));
+      const double al2 = (R[0] - L[0]) - (pR - pL) / (rc * rc);
+      const double al3 = rd * (vR[1] - vL[1]), al4 = rd * (vR[2] - vL[2]);
+      const double r2[5] = {1., rv[0], rv[1], rv[2], 0.5 * absVel};
+      const double r3[5] = {0., 0., 1., 0., rv[1]};
+      const double r4[5] = {0., 0., 0., 1., rv[2]};
+      for (int v = 0; v < 5; ++v)
+        F[v] = (ssr * FL[v] - ssl * FR[v] +
+                ssl * ssr * (R[v] - L[v] - delta * (r2[v] * al2 + r3[v] * al3 + r4[v] * al4))) /
+               (ssr - ssl);
+    }
+  } else if constexpr (RS == 3) {  // RiemannSolverByRoe :742-869 (baseline flux by the volume flux id)
+    double FL[5], FR[5];
+    euler_flux_1d(P, L, FL);
+    euler_flux_1d(P, R, FR);
+    const double sRL = 1. / L[0], sRR = 1. / R[0];
+    const double vL[3] = {L[1] * sRL, L[2] * sRL, L[3] * sRL};
+    const double vR[3] = {R[1] * sRR, R[2] * sRR, R[3] * sRR};
+    const double HL = (L[4] + P.kappaM1 * (L[4] - 0.5 * (L[1] * vL[0] + L[2] * vL[1] + L[3] * vL[2]))) * sRL;
+    const double HR = (R[4] + P.kappaM1 * (R[4] - 0.5 * (R[1] * vR[0] + R[2] * vR[1] + R[3] * vR[2]))) * sRR;
+    const double sqL = sqrt(L[0]), sqR = sqrt(R[0]);
+    const double ssq = 1. / (sqL + sqR);
+    double rv[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) rv[d] = (sqR * vR[d] + sqL * vL[d]) * ssq;
+    const double rH = (sqR * HR + sqL * HL) * ssq;
+    const double v2 = rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2];
+    const double rc = sqrt(P.kappaM1 * (rH - 0.5 * v2));
+    double a1 = rv[0] - rc, a5 = rv[0] + rc;
+    const double a2 = rv[0];
+    const double r1[5] = {1., a1, rv[1], rv[2], rH - rv[0] * rc};
+    const double r2[5] = {1., rv[0], rv[1], rv[2], 0.5 * v2};
+    const double r5[5] = {1., a5, rv[1], rv[2], rH + rv[0] * rc};
+    double dU[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) dU[v] = R[v] - L[v];
+    const double dU6 = dU[4] - (dU[2] - rv[1] * dU[0]) * rv[1] - (dU[3] - rv[2] * dU[0]) * rv[2];
+    const double al3 = dU[2] - rv[1] * dU[0];
+    const double al4 = dU[3] - rv[2] * dU[0];
+    const double al2 = P.kappaM1 / (rc * rc) * (dU[0] * (rH - rv[0] * rv[0]) - dU6 + rv[0] * dU[1]);
+    const double al1 = 0.5 / rc * (dU[0] * (rv[0] + rc) - dU[1] - rc * al2);
+    const double al5 = dU[0] - al1 - al2;
+    double Fc[5];
+    Hat h;
+    if (P.volumeFlux == 2 || P.volumeFlux == 4) {
+      // Kennedy-Gruber baseline (volume flux 4 is paired with the Pirozzoli variant here) with the
+      // acoustic speeds replaced by their maximum (consistent kinetic energy dissipation)
+      if (P.volumeFlux == 2) volume_flux_1d<2>(P, L, R, Fc, h);
+      else volume_flux_1d<8>(P, L, R, Fc, h);
+      a1 = fmax(fabs(rv[0] - rc), fabs(rv[0] + rc));
+      a5 = a1;
+    } else if (P.volumeFlux == 3) {
+      volume_flux_1d<3>(P, L, R, Fc, h);
+    } else {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) Fc[v] = 0.5 * (FL[v] + FR[v]);
+    }
+    const double g1 = al1 * fabs(a1), g2 = al2 * fabs(a2), g3 = al3 * fabs(a2), g4 = al4 * fabs(a2),
+                 g5 = al5 * fabs(a5);
+    F[0] = Fc[0] - 0.5 * (g1 * r1[0] + g2 * r2[0] + g5 * r5[0]);
+    F[1] = Fc[1] - 0.5 * (g1 * r1[1] + g2 * r2[1] + g5 * r5[1]);
+    F[2] = Fc[2] - 0.5 * (g1 * r1[2] + g2 * r2[2] + g3 + g5 * r5[2]);
+    F[3] = Fc[3] - 0.5 * (g1 * r1[3] + g2 * r2[3] + g4 + g5 * r5[3]);
+    F[4] = Fc[4] - 0.5 * (g1 * r1[4] + g2 * r2[4] + g3 * rv[1] + g4 * rv[2] + g5 * r5[4]);
   } else if constexpr (RS == 13) {  // RiemannSolver_EC_LLF :1011-1110
     double Fc[5];
     Hat h;
@@ -351,7 +469,9 @@ __device__ __forceinline__ void riemann_rotated(const KParams& P, const double* 
 }
 
 template <int RS>
-__host__ __device__ constexpr bool riemann_needs_side_max() { return RS == 13 || RS == 14 || RS == 16; }
+__host__ __device__ constexpr bool riemann_needs_side_max() {
+  return RS == 13 || RS == 16 || riemann_llf_point_flux<RS>() > 0;
+}
 
 // viscosity law (equation_vars.f90:672-692; flux.f90:470-480)
 __device__ __forceinline__ double visc_mu(const KParams& P, double p, double srho) {

@@ -54,9 +54,21 @@ template <> struct VolRec<0> { static constexpr int NQ = 9, MO = 9, RS = 19; };
 template <> struct VolRec<1> { static constexpr int NQ = 9, MO = 9, RS = 19; };
 // Kennedy-Gruber (2): rho, u, v, w, p, e = E/rho
 template <> struct VolRec<2> { static constexpr int NQ = 6, MO = 6, RS = 15; };
+// Ducros (3): halves of rho, u, v, w, p, rho u, rho v, rho w, rho E (every average is arithmetic)
+template <> struct VolRec<3> { static constexpr int NQ = 9, MO = 9, RS = 19; };
+// Morinishi (4): rho, u, v, w, p, |v|^2
+template <> struct VolRec<4> { static constexpr int NQ = 6, MO = 6, RS = 15; };
 // EC-KEP (5): rho, u/2, v/2, w/2, beta = rho/(2p), |v|^2/2, log rho, log beta (the halves make the
 // pair averages plain sums; halving is exact, so the averages are bit-identical)
 template <> struct VolRec<5> { static constexpr int NQ = 8, MO = 8, RS = 17; };
+// approximate EC-KEP (6): rho/2, u/2, v/2, w/2, beta, |v|^2/2
+template <> struct VolRec<6> { static constexpr int NQ = 6, MO = 6, RS = 15; };
+// EC-KEP with pressure average (7): rho/2, u/2, v/2, w/2, p/2, beta, |v|^2/2, log beta
+template <> struct VolRec<7> { static constexpr int NQ = 8, MO = 8, RS = 17; };
+// Kennedy-Gruber, Pirozzoli form (8): halves of rho, u, v, w, p, H = (rho E + p)/rho
+template <> struct VolRec<8> { static constexpr int NQ = 6, MO = 6, RS = 15; };
+// Gassner-Winters-Walch (9): halves of sqrt(rho) times (1, u, v, w, H)
+template <> struct VolRec<9> { static constexpr int NQ = 5, MO = 5, RS = 15; };
 // Ismail-Roe (10): z1 = sqrt(rho/p), u, v, w, z5 = z1 p, log z1, log z5
 template <> struct VolRec<10> { static constexpr int NQ = 7, MO = 7, RS = 17; };
 // Ranocha (32): rho, u, v, w, p, rho/p, log rho, log(rho/p)
@@ -87,6 +99,24 @@ __device__ __forceinline__ void make_record(const KParams& P, const double* U, d
     r[5] = u; r[6] = v; r[7] = w; r[8] = p;
   } else if constexpr (VF == 2) {
     r[0] = U[0]; r[1] = u; r[2] = v; r[3] = w; r[4] = p; r[5] = srho * U[4];
+  } else if constexpr (VF == 3) {
+    r[0] = 0.5 * U[0]; r[1] = 0.5 * u; r[2] = 0.5 * v; r[3] = 0.5 * w; r[4] = 0.5 * p;
+    r[5] = 0.5 * U[1]; r[6] = 0.5 * U[2]; r[7] = 0.5 * U[3]; r[8] = 0.5 * U[4];
+  } else if constexpr (VF == 4) {
+    r[0] = U[0]; r[1] = u; r[2] = v; r[3] = w; r[4] = p; r[5] = v2;
+  } else if constexpr (VF == 6) {
+    r[0] = 0.5 * U[0]; r[1] = 0.5 * u; r[2] = 0.5 * v; r[3] = 0.5 * w; r[4] = 0.5 * U[0] / p; r[5] = 0.5 * v2;
+  } else if constexpr (VF == 7) {
+    const double beta = 0.5 * U[0] / p;
+    r[0] = 0.5 * U[0]; r[1] = 0.5 * u; r[2] = 0.5 * v; r[3] = 0.5 * w; r[4] = 0.5 * p; r[5] = beta;
+    r[6] = 0.5 * v2; r[7] = log(beta);
+  } else if constexpr (VF == 8) {
+    r[0] = 0.5 * U[0]; r[1] = 0.5 * u; r[2] = 0.5 * v; r[3] = 0.5 * w; r[4] = 0.5 * p;
+    r[5] = 0.5 * ((U[4] + p) * srho);
+  } else if constexpr (VF == 9) {
+    const double w1 = sqrt(U[0]);
+    r[0] = 0.5 * w1; r[1] = 0.5 * (w1 * u); r[2] = 0.5 * (w1 * v); r[3] = 0.5 * (w1 * w);
+    r[4] = 0.5 * (w1 * srho * (U[4] + p));
   } else if constexpr (VF == 5) {
     const double beta = 0.5 * U[0] / p;
     r[0] = U[0]; r[1] = 0.5 * u; r[2] = 0.5 * v; r[3] = 0.5 * w; r[4] = beta; r[5] = 0.5 * v2;
@@ -136,6 +166,69 @@ __device__ __forceinline__ void pair_flux(const KParams& P, const double* L, con
       F[2] = F[0] * vH + m2 * p1;
       F[3] = F[0] * wH + m3 * p1;
       F[4] = F[0] * eH + p1 * q;
+    } else if constexpr (VF == 3) {  // DucrosFluxVec :986-1059 (records hold halves)
+      const double q = (L[1] + R[1]) * m1 + (L[2] + R[2]) * m2 + (L[3] + R[3]) * m3;
+      const double p1 = L[4] + R[4];
+      F[0] = (L[0] + R[0]) * q;
+      F[1] = (L[5] + R[5]) * q + m1 * p1;
+      F[2] = (L[6] + R[6]) * q + m2 * p1;
+      F[3] = (L[7] + R[7]) * q + m3 * p1;
+      F[4] = ((L[8] + R[8]) + p1) * q;
+    } else if constexpr (VF == 4) {  // MorinishiFluxVec :1121-1205
+      const double uH = 0.5 * (L[1] + R[1]), vH = 0.5 * (L[2] + R[2]), wH = 0.5 * (L[3] + R[3]);
+      const double p1 = 0.5 * (L[4] + R[4]);
+      const double qL = L[1] * m1 + L[2] * m2 + L[3] * m3;
+      const double qR = R[1] * m1 + R[2] * m2 + R[3] * m3;
+      const double rq2L = 0.5 * L[0] * qL, rq2R = 0.5 * R[0] * qR;
+      F[0] = rq2L + rq2R;
+      F[1] = F[0] * uH + m1 * p1;
+      F[2] = F[0] * vH + m2 * p1;
+      F[3] = F[0] * wH + m3 * p1;
+      F[4] = 0.5 * (P.kappa * P.sKappaM1 * (L[4] * qL + R[4] * qR) - (rq2L * L[5] + rq2R * R[5])) +
+             rq2L * (L[1] * uH + L[2] * vH + L[3] * wH) + rq2R * (R[1] * uH + R[2] * vH + R[3] * wH);
+    } else if constexpr (VF == 6) {  // EntropyAndEnergyConservingFluxVec2 :1427-1504 (halves)
+      const double rhoM = L[0] + R[0];
+      const double sbM = 2. / (L[4] + R[4]);
+      const double uH = L[1] + R[1], vH = L[2] + R[2], wH = L[3] + R[3];
+      const double p1 = 0.5 * rhoM * sbM;
+      const double q = uH * m1 + vH * m2 + wH * m3;
+      F[0] = rhoM * q;
+      F[1] = F[0] * uH + m1 * p1;
+      F[2] = F[0] * vH + m2 * p1;
+      F[3] = F[0] * wH + m3 * p1;
+      F[4] = F[0] * 0.5 * (P.sKappaM1 * sbM - (L[5] + R[5])) + uH * F[1] + vH * F[2] + wH * F[3];
+    } else if constexpr (VF == 7) {  // ggFluxVec :1575-1653 (halves)
+      double nb, db;
+      ln_mean_nd(L, R, 5, 7, nb, db);
+      const double rhoM = L[0] + R[0];
+      const double uH = L[1] + R[1], vH = L[2] + R[2], wH = L[3] + R[3];
+      const double p1 = L[4] + R[4];
+      const double q = uH * m1 + vH * m2 + wH * m3;
+      F[0] = rhoM * q;
+      F[1] = F[0] * uH + m1 * p1;
+      F[2] = F[0] * vH + m2 * p1;
+      F[3] = F[0] * wH + m3 * p1;
+      F[4] = F[0] * 0.5 * (P.sKappaM1 * db / nb - (L[6] + R[6])) + uH * F[1] + vH * F[2] + wH * F[3];
+    } else if constexpr (VF == 8) {  // KennedyAndGruberFluxVec2 :857-929 (halves)
+      const double uH = L[1] + R[1], vH = L[2] + R[2], wH = L[3] + R[3];
+      const double p1 = L[4] + R[4];
+      const double q = uH * m1 + vH * m2 + wH * m3;
+      F[0] = (L[0] + R[0]) * q;
+      F[1] = F[0] * uH + m1 * p1;
+      F[2] = F[0] * vH + m2 * p1;
+      F[3] = F[0] * wH + m3 * p1;
+      F[4] = F[0] * (L[5] + R[5]);
+    } else if constexpr (VF == 9) {  // GassnerWintersWalchFluxVec :1724-1799 (halves)
+      const double rhoH = L[0] + R[0];
+      const double uH = L[1] + R[1], vH = L[2] + R[2], wH = L[3] + R[3];
+      const double HH = L[4] + R[4];
+      const double p1 = P.kappaM1 * P.sKappa * (rhoH * HH - 0.5 * (uH * uH + vH * vH + wH * wH));
+      const double q = uH * m1 + vH * m2 + wH * m3;
+      F[0] = rhoH * q;
+      F[1] = q * uH + m1 * p1;
+      F[2] = q * vH + m2 * p1;
+      F[3] = q * wH + m3 * p1;
+      F[4] = q * HH;
     } else if constexpr (VF == 5) {  // EntropyAndEnergyConservingFluxVec :1277-1356
       double nr, dr, nb, db;
       ln_mean_nd(L, R, 0, 6, nr, dr);

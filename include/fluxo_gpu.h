@@ -52,8 +52,8 @@ typedef struct fluxo_cfg {
   int struct_size;   /* sizeof(fluxo_cfg) */
   int N;             /* N: polynomial degree, 1..7 (one thread per volume node) */
   int eqn;           /* FLUXO_EQN_EULER (PARABOLIC=0) or FLUXO_EQN_NAVIERSTOKES */
-  int riemann;       /* Riemann: 0,1,22,4,44,33,5,9,32,6,13,14,16 */
-  int volume_flux;   /* VolumeFlux: 0,1,2,5,10,32 */
+  int riemann;       /* Riemann: 0-24, 32, 33, 44 */
+  int volume_flux;   /* VolumeFlux: 0-10, 32 */
   int lifting;       /* 1 = BR1 (br1.f90), 2 = BR2 (br2.f90) */
   int lifting_var;   /* PP_Lifting_Var: 1 cons_var, 2 prim_var, 3 entropy_var */
   int visc;          /* PP_VISC: 0 constant mu0, 1 Sutherland, 2 power law */

@@ -495,6 +495,91 @@ void VolumeFluxVec(const Case& C, const real* UL, const real* UR, const real* aL
       F[4] = F[0] * (v2ZIP + 1. / rspM * C.sKappaM1) + 0.5 * (aL[4] * vmR + aR[4] * vmL);
       return;
     }
+    case 3: {  // DucrosFluxVec :986-1059
+      real rhoHat = 0.5 * (UL[0] + UR[0]);
+      real uHat = 0.5 * (aL[1] + aR[1]), vHat = 0.5 * (aL[2] + aR[2]), wHat = 0.5 * (aL[3] + aR[3]);
+      real rhouHat = 0.5 * (UL[1] + UR[1]), rhovHat = 0.5 * (UL[2] + UR[2]), rhowHat = 0.5 * (UL[3] + UR[3]);
+      real rhoeHat = 0.5 * (UL[4] + UR[4]);
+      real p1Hat = 0.5 * (aL[4] + aR[4]);
+      real qHat = uHat * m1 + vHat * m2 + wHat * m3;
+      F[0] = rhoHat * qHat;
+      F[1] = rhouHat * qHat + m1 * p1Hat;
+      F[2] = rhovHat * qHat + m2 * p1Hat;
+      F[3] = rhowHat * qHat + m3 * p1Hat;
+      F[4] = (rhoeHat + p1Hat) * qHat;
+      return;
+    }
+    case 4: {  // MorinishiFluxVec :1121-1205
+      real uHat = 0.5 * (aL[1] + aR[1]), vHat = 0.5 * (aL[2] + aR[2]), wHat = 0.5 * (aL[3] + aR[3]);
+      real p1Hat = 0.5 * (aL[4] + aR[4]);
+      real qL = aL[1] * m1 + aL[2] * m2 + aL[3] * m3;
+      real qR = aR[1] * m1 + aR[2] * m2 + aR[3] * m3;
+      real rq2L = 0.5 * UL[0] * qL, rq2R = 0.5 * UR[0] * qR;
+      F[0] = rq2L + rq2R;
+      F[1] = F[0] * uHat + m1 * p1Hat;
+      F[2] = F[0] * vHat + m2 * p1Hat;
+      F[3] = F[0] * wHat + m3 * p1Hat;
+      F[4] = 0.5 * (C.kappa * C.sKappaM1 * (aL[4] * qL + aR[4] * qR) - (rq2L * aL[5] + rq2R * aR[5])) +
+             rq2L * (aL[1] * uHat + aL[2] * vHat + aL[3] * wHat) + rq2R * (aR[1] * uHat + aR[2] * vHat + aR[3] * wHat);
+      return;
+    }
+    case 6: {  // EntropyAndEnergyConservingFluxVec2 :1427-1504
+      real betaL = 0.5 * UL[0] / aL[4], betaR = 0.5 * UR[0] / aR[4];
+      real rhoM = 0.5 * (UL[0] + UR[0]);
+      real sbetaM = 2. / (betaL + betaR);
+      real uHat = 0.5 * (aL[1] + aR[1]), vHat = 0.5 * (aL[2] + aR[2]), wHat = 0.5 * (aL[3] + aR[3]);
+      real p1Hat = 0.5 * rhoM * sbetaM;
+      real qHat = uHat * m1 + vHat * m2 + wHat * m3;
+      F[0] = rhoM * qHat;
+      F[1] = F[0] * uHat + m1 * p1Hat;
+      F[2] = F[0] * vHat + m2 * p1Hat;
+      F[3] = F[0] * wHat + m3 * p1Hat;
+      F[4] = F[0] * 0.5 * (C.sKappaM1 * sbetaM - 0.5 * (aL[5] + aR[5])) + uHat * F[1] + vHat * F[2] + wHat * F[3];
+      return;
+    }
+    case 7: {  // ggFluxVec :1575-1653 (its log mean of rho is computed but unused there; left out)
+      real betaL = 0.5 * UL[0] / aL[4], betaR = 0.5 * UR[0] / aR[4];
+      real rhoM = 0.5 * (UL[0] + UR[0]);
+      real betaHat = LN_MEAN(betaL, betaR);
+      real uHat = 0.5 * (aL[1] + aR[1]), vHat = 0.5 * (aL[2] + aR[2]), wHat = 0.5 * (aL[3] + aR[3]);
+      real p1Hat = 0.5 * (aL[4] + aR[4]);
+      real qHat = uHat * m1 + vHat * m2 + wHat * m3;
+      F[0] = rhoM * qHat;
+      F[1] = F[0] * uHat + m1 * p1Hat;
+      F[2] = F[0] * vHat + m2 * p1Hat;
+      F[3] = F[0] * wHat + m3 * p1Hat;
+      F[4] = F[0] * 0.5 * (C.sKappaM1 / betaHat - 0.5 * (aL[5] + aR[5])) + uHat * F[1] + vHat * F[2] + wHat * F[3];
+      return;
+    }
+    case 8: {  // KennedyAndGruberFluxVec2 :857-929
+      real rhoHat = 0.5 * (UL[0] + UR[0]);
+      real uHat = 0.5 * (aL[1] + aR[1]), vHat = 0.5 * (aL[2] + aR[2]), wHat = 0.5 * (aL[3] + aR[3]);
+      real p1Hat = 0.5 * (aL[4] + aR[4]);
+      real HHat = 0.5 * ((UL[4] + aL[4]) * aL[0] + (UR[4] + aR[4]) * aR[0]);
+      real qHat = uHat * m1 + vHat * m2 + wHat * m3;
+      F[0] = rhoHat * qHat;
+      F[1] = F[0] * uHat + m1 * p1Hat;
+      F[2] = F[0] * vHat + m2 * p1Hat;
+      F[3] = F[0] * wHat + m3 * p1Hat;
+      F[4] = F[0] * HHat;
+      return;
+    }
+    case 9: {  // GassnerWintersWalchFluxVec :1724-1799
+      real sqL = sqrt(UL[0]), sqR = sqrt(UR[0]);
+      real rhoHat = 0.5 * (sqL + sqR);
+      real uHat = 0.5 * (sqL * aL[1] + sqR * aR[1]);
+      real vHat = 0.5 * (sqL * aL[2] + sqR * aR[2]);
+      real wHat = 0.5 * (sqL * aL[3] + sqR * aR[3]);
+      real HHat = 0.5 * (sqL * aL[0] * (UL[4] + aL[4]) + sqR * aR[0] * (UR[4] + aR[4]));
+      real p1Hat = C.kappaM1 * C.sKappa * (rhoHat * HHat - 0.5 * (uHat * uHat + vHat * vHat + wHat * wHat));
+      real qHat = uHat * m1 + vHat * m2 + wHat * m3;
+      F[0] = rhoHat * qHat;
+      F[1] = qHat * uHat + m1 * p1Hat;
+      F[2] = qHat * vHat + m2 * p1Hat;
+      F[3] = qHat * wHat + m3 * p1Hat;
+      F[4] = qHat * HHat;
+      return;
+    }
     default: throw std::runtime_error("volume flux not implemented");
   }
 }
@@ -583,6 +668,105 @@ void VolumeFluxAverage(const Case& C, int which, const real* UL, const real* UR,
       F[2] = F[0] * h.v;
       F[3] = F[0] * h.w;
       F[4] = F[0] * eHat + h.p1 * h.u;
+      return;
+    }
+    case 3: {  // DucrosFlux :937-979
+      h.rho = 0.5 * (UL[0] + UR[0]);
+      h.u = 0.5 * (uL + uR); h.v = 0.5 * (vL + vR); h.w = 0.5 * (wL + wR);
+      h.p1 = 0.5 * C.kappaM1 *
+             (UL[4] + UR[4] - 0.5 * (UL[1] * uL + UL[2] * vL + UL[3] * wL + UR[1] * uR + UR[2] * vR + UR[3] * wR));
+      h.a = sqrt(C.kappa * h.p1 / h.rho);
+      h.H = C.kappa * h.p1 / (h.rho * C.kappaM1) + 0.5 * (h.u * h.u + h.v * h.v + h.w * h.w);
+      real qLR = 0.5 * h.u;
+      F[0] = h.rho * (qLR + qLR);
+      F[1] = qLR * (UL[1] + UR[1]) + h.p1;
+      F[2] = qLR * (UL[2] + UR[2]);
+      F[3] = qLR * (UL[3] + UR[3]);
+      F[4] = qLR * ((UL[4] + UR[4]) + (h.p1 + h.p1));
+      return;
+    }
+    case 4: {  // MorinishiFlux :1066-1113
+      real vel2L = uL * uL + vL * vL + wL * wL, vel2R = uR * uR + vR * vR + wR * wR;
+      real pL = C.kappaM1 * (UL[4] - 0.5 * UL[0] * vel2L), pR = C.kappaM1 * (UR[4] - 0.5 * UR[0] * vel2R);
+      h.rho = 0.5 * (UL[0] + UR[0]);
+      h.u = 0.5 * (uL + uR); h.v = 0.5 * (vL + vR); h.w = 0.5 * (wL + wR);
+      h.p1 = 0.5 * (pL + pR);
+      h.a = sqrt(C.kappa * h.p1 / h.rho);
+      h.H = C.kappa * h.p1 / (h.rho * C.kappaM1) + 0.5 * (h.u * h.u + h.v * h.v + h.w * h.w);
+      real rq2L = 0.5 * UL[0] * uL, rq2R = 0.5 * UR[0] * uR;
+      F[0] = rq2L + rq2R;
+      F[1] = F[0] * h.u + h.p1;
+      F[2] = F[0] * h.v;
+      F[3] = F[0] * h.w;
+      F[4] = 0.5 * (C.kappa * C.sKappaM1 * (pL * uL + pR * uR) - (rq2L * vel2L + rq2R * vel2R)) +
+             rq2L * (uL * h.u + vL * h.v + wL * h.w) + rq2R * (uR * h.u + vR * h.v + wR * h.w);
+      return;
+    }
+    case 6: {  // EntropyAndEnergyConservingFlux2 :1365-1419 (a, H = 0)
+      real v2s2L = 0.5 * (uL * uL + vL * vL + wL * wL), v2s2R = 0.5 * (uR * uR + vR * vR + wR * wR);
+      real pL = C.kappaM1 * (UL[4] - UL[0] * v2s2L), pR = C.kappaM1 * (UR[4] - UR[0] * v2s2R);
+      real betaL = 0.5 * UL[0] / pL, betaR = 0.5 * UR[0] / pR;
+      real rhoM = 0.5 * (UL[0] + UR[0]);
+      real sbetaM = 2. / (betaL + betaR);
+      h.a = 0.; h.H = 0.;
+      h.rho = LN_MEAN(UL[0], UR[0]);
+      h.u = 0.5 * (uL + uR); h.v = 0.5 * (vL + vR); h.w = 0.5 * (wL + wR);
+      h.p1 = 0.5 * rhoM * sbetaM;
+      F[0] = rhoM * h.u;
+      F[1] = F[0] * h.u + h.p1;
+      F[2] = F[0] * h.v;
+      F[3] = F[0] * h.w;
+      F[4] = F[0] * 0.5 * (C.sKappaM1 * sbetaM - (v2s2L + v2s2R)) + h.u * F[1] + h.v * F[2] + h.w * F[3];
+      return;
+    }
+    case 7: {  // ggFlux :1513-1567 (a, H = 0)
+      real v2s2L = 0.5 * (uL * uL + vL * vL + wL * wL), v2s2R = 0.5 * (uR * uR + vR * vR + wR * wR);
+      real pL = C.kappaM1 * (UL[4] - UL[0] * v2s2L), pR = C.kappaM1 * (UR[4] - UR[0] * v2s2R);
+      real betaL = 0.5 * UL[0] / pL, betaR = 0.5 * UR[0] / pR;
+      h.a = 0.; h.H = 0.;
+      h.rho = LN_MEAN(UL[0], UR[0]);
+      real betaHat = LN_MEAN(betaL, betaR);
+      h.u = 0.5 * (uL + uR); h.v = 0.5 * (vL + vR); h.w = 0.5 * (wL + wR);
+      h.p1 = 0.5 * (pL + pR);
+      F[0] = h.rho * h.u;
+      F[1] = F[0] * h.u + h.p1;
+      F[2] = F[0] * h.v;
+      F[3] = F[0] * h.w;
+      F[4] = F[0] * 0.5 * (C.sKappaM1 / betaHat - (v2s2L + v2s2R)) + h.u * F[1] + h.v * F[2] + h.w * F[3];
+      return;
+    }
+    case 8: {  // KennedyAndGruberFlux2 :810-850
+      real pL = C.kappaM1 * (UL[4] - 0.5 * (UL[1] * uL + UL[2] * vL + UL[3] * wL));
+      real pR = C.kappaM1 * (UR[4] - 0.5 * (UR[1] * uR + UR[2] * vR + UR[3] * wR));
+      h.rho = 0.5 * (UL[0] + UR[0]);
+      h.u = 0.5 * (uL + uR); h.v = 0.5 * (vL + vR); h.w = 0.5 * (wL + wR);
+      h.p1 = 0.5 * (pL + pR);
+      h.a = sqrt(C.kappa * h.p1 / h.rho);
+      h.H = 0.5 * ((UL[4] + pL) * sRL + (UR[4] + pR) * sRR);
+      F[0] = h.rho * h.u;
+      F[1] = F[0] * h.u + h.p1;
+      F[2] = F[0] * h.v;
+      F[3] = F[0] * h.w;
+      F[4] = F[0] * h.H;
+      return;
+    }
+    case 9: {  // GassnerWintersWalchFlux :1661-1716 (a = 0; Hat values are the averaged Roe variables)
+      real pL = C.kappaM1 * (UL[4] - 0.5 * (UL[1] * uL + UL[2] * vL + UL[3] * wL));
+      real pR = C.kappaM1 * (UR[4] - 0.5 * (UR[1] * uR + UR[2] * vR + UR[3] * wR));
+      real hL = sRL * (UL[4] + pL), hR = sRR * (UR[4] + pR);
+      real w1L = sqrt(UL[0]), w1R = sqrt(UR[0]);
+      h.rho = 0.5 * (w1L + w1R);
+      h.u = 0.5 * (w1L * uL + w1R * uR);
+      h.v = 0.5 * (w1L * vL + w1R * vR);
+      h.w = 0.5 * (w1L * wL + w1R * wR);
+      h.H = 0.5 * (w1L * hL + w1R * hR);
+      h.p1 = C.kappaM1 * C.sKappa * (h.rho * h.H - 0.5 * (h.u * h.u + h.v * h.v + h.w * h.w));
+      h.a = 0.;
+      F[0] = h.u * h.rho;
+      F[1] = h.u * h.u + h.p1;
+      F[2] = h.u * h.v;
+      F[3] = h.u * h.w;
+      F[4] = h.u * h.H;
       return;
     }
     default: throw std::runtime_error("two-point flux for Riemann solver not implemented");
@@ -710,15 +894,163 @@ void SolveRiemann(const Case& C, int npts, const real* ULL, const real* URR, rea
       }
       return;
     }
-    case 5: case 9: case 32: case 6: {  // RiemannSolver_VolumeFluxAverage :980-1005
-      int which = (rs == 5) ? 10 : (rs == 9 ? 5 : (rs == 32 ? 32 : 2));
+    case 2:  // RiemannSolverByHLLC :552-615
+      for (int i = 0; i < npts; ++i) {
+        const real* L = ULL + nv * i;
+        const real* R = URR + nv * i;
+        real FL[5], FR[5];
+        EulerFlux1D(C, L, FL);
+        EulerFlux1D(C, R, FR);
+        real sRL = 1. / L[0], sRR = 1. / R[0];
+        real vL[3] = {L[1] * sRL, L[2] * sRL, L[3] * sRL};
+        real vR[3] = {R[1] * sRR, R[2] * sRR, R[3] * sRR};
+        real pL = C.kappaM1 * (L[4] - 0.5 * (L[1] * vL[0] + L[2] * vL[1] + L[3] * vL[2]));
+        real pR = C.kappaM1 * (R[4] - 0.5 * (R[1] * vR[0] + R[2] * vR[1] + R[3] * vR[2]));
+        real ssl = vL[0] - sqrt(C.kappa * pL * sRL);
+        real ssr = vR[0] + sqrt(C.kappa * pR * sRR);
+        real* Fo = F + nv * i;
+        if (ssl >= 0.) {
+          for (int v = 0; v < 5; ++v) Fo[v] = FL[v];
+        } else if (ssr <= 0.) {
+          for (int v = 0; v < 5; ++v) Fo[v] = FR[v];
+        } else {
+          real smuL = ssl - vL[0], smuR = ssr - vR[0];
+          real sStar = (pR - pL + L[1] * smuL - R[1] * smuR) / (L[0] * smuL - R[0] * smuR);
+          const bool left = (ssl <= 0.) && (sStar >= 0.);
+          const real* U = left ? L : R;
+          const real* FF = left ? FL : FR;
+          real ss = left ? ssl : ssr, smu = left ? smuL : smuR, sr = left ? sRL : sRR, p = left ? pL : pR;
+          real vn = left ? vL[0] : vR[0];
+          real fac = U[0] * smu / (ss - sStar);
+          real Ustar[5] = {fac * 1., fac * sStar, fac * (U[2] * sr), fac * (U[3] * sr),
+                           fac * (U[4] * sr + (sStar - vn) * (sStar + p * sr / smu))};
+          for (int v = 0; v < 5; ++v) Fo[v] = FF[v] + ss * (Ustar[v] - U[v]);
+        }
+      }
+      return;
+    case 23: case 24:  // RiemannSolverByHLLE :393-462, RiemannSolverByHLLEM :466-547
+      for (int i = 0; i < npts; ++i) {
+        const real* L = ULL + nv * i;
+        const real* R = URR + nv * i;
+        real FL[5], FR[5];
+        EulerFlux1D(C, L, FL);
+        EulerFlux1D(C, R, FR);
+        real beta = sqrt(0.5 * C.kappaM1 / C.kappa);
+        real sRL = 1. / L[0], sRR = 1. / R[0];
+        real vL[3] = {L[1] * sRL, L[2] * sRL, L[3] * sRL};
+        real vR[3] = {R[1] * sRR, R[2] * sRR, R[3] * sRR};
+        real pL = C.kappaM1 * (L[4] - 0.5 * (L[1] * vL[0] + L[2] * vL[1] + L[3] * vL[2]));
+        real pR = C.kappaM1 * (R[4] - 0.5 * (R[1] * vR[0] + R[2] * vR[1] + R[3] * vR[2]));
+        real aL = sqrt(C.kappa * pL * sRL), aR = sqrt(C.kappa * pR * sRR);
+        real HL = (L[4] + pL) * sRL, HR = (R[4] + pR) * sRR;
+        real sqL = sqrt(L[0]), sqR = sqrt(R[0]);
+        real ssq = 1. / (sqL + sqR);
+        real rv[3];
+        for (int d = 0; d < 3; ++d) rv[d] = (sqR * vR[d] + sqL * vL[d]) * ssq;
+        real rH = (sqR * HR + sqL * HL) * ssq;
+        real absVel = rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2];
+        real rc = sqrt(C.kappaM1 * (rH - 0.5 * absVel));
+        real ssl = fmin(fmin(rv[0] - rc, vL[0] - beta * aL), real(0.));
+        real ssr = fmax(fmax(rv[0] + rc, vR[0] + beta * aR), real(0.));
+        real* Fo = F + nv * i;
+        if (ssl >= 0. && ssr > 0.) {
+          for (int v = 0; v < 5; ++v) Fo[v] = FL[v];
+        } else if (ssr <= 0. && ssl < 0.) {
+          for (int v = 0; v < 5; ++v) Fo[v] = FR[v];
+        } else if (rs == 23) {
+          for (int v = 0; v < 5; ++v) Fo[v] = (ssr * FL[v] - ssl * FR[v] + ssl * ssr * (R[v] - L[v])) / (ssr - ssl);
+        } else {  // HLLEM: anti-diffusion along the Roe-mean entropy and shear waves
+          real rd = sqrt(L[0] * R[0]);
+          real delta = rc / (rc + fabs(0.5 * (ssl + ssr)));
+          real al2 = (R[0] - L[0]) - (pR - pL) / (rc * rc);
+          real al3 = rd * (vR[1] - vL[1]), al4 = rd * (vR[2] - vL[2]);
+          real r2[5] = {1., rv[0], rv[1], rv[2], 0.5 * absVel};
+          real r3[5] = {0., 0., 1., 0., rv[1]};
+          real r4[5] = {0., 0., 0., 1., rv[2]};
+          for (int v = 0; v < 5; ++v)
+            Fo[v] = (ssr * FL[v] - ssl * FR[v] +
+                     ssl * ssr * (R[v] - L[v] - delta * (r2[v] * al2 + r3[v] * al3 + r4[v] * al4))) /
+                    (ssr - ssl);
+        }
+      }
+      return;
+    case 3:  // RiemannSolverByRoe :742-869 (baseline flux chosen by the volume flux id)
+      for (int i = 0; i < npts; ++i) {
+        const real* L = ULL + nv * i;
+        const real* R = URR + nv * i;
+        real FL[5], FR[5];
+        EulerFlux1D(C, L, FL);
+        EulerFlux1D(C, R, FR);
+        real sRL = 1. / L[0], sRR = 1. / R[0];
+        real vL[3] = {L[1] * sRL, L[2] * sRL, L[3] * sRL};
+        real vR[3] = {R[1] * sRR, R[2] * sRR, R[3] * sRR};
+        real HL = (L[4] + C.kappaM1 * (L[4] - 0.5 * (L[1] * vL[0] + L[2] * vL[1] + L[3] * vL[2]))) * sRL;
+        real HR = (R[4] + C.kappaM1 * (R[4] - 0.5 * (R[1] * vR[0] + R[2] * vR[1] + R[3] * vR[2]))) * sRR;
+        real sqL = sqrt(L[0]), sqR = sqrt(R[0]);
+        real ssq = 1. / (sqL + sqR);
+        real rv[3];
+        for (int d = 0; d < 3; ++d) rv[d] = (sqR * vR[d] + sqL * vL[d]) * ssq;
+        real rH = (sqR * HR + sqL * HL) * ssq;
+        real rc = sqrt(C.kappaM1 * (rH - 0.5 * (rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2])));
+        real a1 = rv[0] - rc, a2 = rv[0], a5 = rv[0] + rc;
+        real r1[5] = {1., a1, rv[1], rv[2], rH - rv[0] * rc};
+        real r2[5] = {1., rv[0], rv[1], rv[2], 0.5 * (rv[0] * rv[0] + rv[1] * rv[1] + rv[2] * rv[2])};
+        real r3[5] = {0., 0., 1., 0., rv[1]};
+        real r4[5] = {0., 0., 0., 1., rv[2]};
+        real r5[5] = {1., a5, rv[1], rv[2], rH + rv[0] * rc};
+        real dU[6];
+        for (int v = 0; v < 5; ++v) dU[v] = R[v] - L[v];
+        dU[5] = dU[4] - (dU[2] - rv[1] * dU[0]) * rv[1] - (dU[3] - rv[2] * dU[0]) * rv[2];
+        real al3 = dU[2] - rv[1] * dU[0];
+        real al4 = dU[3] - rv[2] * dU[0];
+        real al2 = C.kappaM1 / (rc * rc) * (dU[0] * (rH - rv[0] * rv[0]) - dU[5] + rv[0] * dU[1]);
+        real al1 = 0.5 / rc * (dU[0] * (rv[0] + rc) - dU[1] - rc * al2);
+        real al5 = dU[0] - al1 - al2;
+        real Fc[5];
+        Hat h;
+        switch (C.P.volume_flux) {
+          case 2:
+            VolumeFluxAverage(C, 2, L, R, Fc, h);
+            a1 = fmax(fabs(rv[0] - rc), fabs(rv[0] + rc));
+            a5 = fmax(fabs(rv[0] - rc), fabs(rv[0] + rc));
+            break;
+          case 3: VolumeFluxAverage(C, 3, L, R, Fc, h); break;
+          case 4:  // the reference pairs volume flux 4 with the Pirozzoli Kennedy-Gruber flux here
+            VolumeFluxAverage(C, 8, L, R, Fc, h);
+            a1 = fmax(fabs(rv[0] - rc), fabs(rv[0] + rc));
+            a5 = fmax(fabs(rv[0] - rc), fabs(rv[0] + rc));
+            break;
+          default:
+            for (int v = 0; v < 5; ++v) Fc[v] = 0.5 * (FL[v] + FR[v]);
+        }
+        real g1 = al1 * fabs(a1), g2 = al2 * fabs(a2), g3 = al3 * fabs(a2), g4 = al4 * fabs(a2), g5 = al5 * fabs(a5);
+        for (int v = 0; v < 5; ++v)
+          F[nv * i + v] = Fc[v] - 0.5 * (g1 * r1[v] + g2 * r2[v] + g3 * r3[v] + g4 * r4[v] + g5 * r5[v]);
+      }
+      return;
+    case 5: case 9: case 32: case 6: case 7: case 8: case 10: case 11: case 12: case 20: {
+      // RiemannSolver_VolumeFluxAverage :980-1005 with the point flux of equation.f90:291-406
+      int which = 0;
+      switch (rs) {
+        case 5: which = 10; break;
+        case 9: which = 5; break;
+        case 32: which = 32; break;
+        case 6: which = 2; break;
+        case 7: which = 3; break;
+        case 8: which = 4; break;
+        case 10: which = 6; break;
+        case 11: which = 7; break;
+        case 12: which = 8; break;
+        default: which = 9; break;  // 20
+      }
       for (int i = 0; i < npts; ++i) {
         Hat h;
         VolumeFluxAverage(C, which, ULL + nv * i, URR + nv * i, F + nv * i, h);
       }
       return;
     }
-    case 13: case 14: case 16: {  // LLF-dissipation variants :1011-1209 (lambda max over the side)
+    case 13: case 14: case 16: case 15: case 17: case 18: case 19: case 21: {
+      // LLF-dissipation variants :1011-1209 (lambda max over the side)
       real lmm = 0.;
       for (int i = 0; i < npts; ++i) lmm = fmax(lmm, lambdaMaxPair(C, ULL + nv * i, URR + nv * i));
       for (int i = 0; i < npts; ++i) {
@@ -726,8 +1058,9 @@ void SolveRiemann(const Case& C, int npts, const real* ULL, const real* URR, rea
         const real* R = URR + nv * i;
         real Fc[5];
         Hat h;
-        if (rs == 14) {  // RiemannSolver_VolumeFluxAverage_LLF with Kennedy-Gruber :1117-1148
-          VolumeFluxAverage(C, 2, L, R, Fc, h);
+        if (rs != 13 && rs != 16) {  // RiemannSolver_VolumeFluxAverage_LLF :1117-1151
+          const int which = rs == 14 ? 2 : rs == 15 ? 3 : rs == 17 ? 7 : rs == 18 ? 8 : rs == 19 ? 4 : 9;
+          VolumeFluxAverage(C, which, L, R, Fc, h);
           for (int v = 0; v < 5; ++v) F[nv * i + v] = Fc[v] - 0.5 * lmm * (R[v] - L[v]);
         } else if (rs == 13) {  // RiemannSolver_EC_LLF :1011-1110
           VolumeFluxAverage(C, 10, L, R, Fc, h);

@@ -64,8 +64,31 @@ def test_euler_ut_parity(gpu_lib, case):
     assert rel_l2(op.get_ut(), ref) <= TOL
 
 
+# every remaining Riemann solver and volume flux of navierstokes/equation.f90:291-466 (Roe with each
+# of its baseline fluxes; the point-flux and LLF variants with their own volume flux)
+OPTION_CASES = [
+    dict(N=3, riemann=2, volume_flux=3), dict(N=4, riemann=23, volume_flux=4), dict(N=2, riemann=24, volume_flux=6),
+    dict(N=3, riemann=3, volume_flux=0), dict(N=3, riemann=3, volume_flux=2), dict(N=5, riemann=3, volume_flux=3),
+    dict(N=3, riemann=3, volume_flux=4), dict(N=3, riemann=7, volume_flux=3), dict(N=6, riemann=8, volume_flux=4),
+    dict(N=3, riemann=10, volume_flux=6), dict(N=4, riemann=11, volume_flux=7), dict(N=3, riemann=12, volume_flux=8),
+    dict(N=7, riemann=20, volume_flux=9), dict(N=3, riemann=15, volume_flux=3), dict(N=3, riemann=17, volume_flux=7),
+    dict(N=6, riemann=18, volume_flux=8), dict(N=3, riemann=19, volume_flux=4), dict(N=1, riemann=21, volume_flux=9),
+]
+
+
+@pytest.mark.parametrize("case", OPTION_CASES, ids=lambda c: "N%d_rs%d_vf%d" % (c["N"], c["riemann"], c["volume_flux"]))
+def test_every_riemann_and_volume_flux(gpu_lib, case):
+    c, op = pair(ini_exact_func=2, ini_amplitude=0.3, adv_vel=(0.3, -0.2, 0.5), nElems=(2, 2, 2), NGeo=2,
+                 deform_amp=0.1, **CUBE, **case)
+    ref = c.dg_time_derivative(0.1)
+    op.dg_time_derivative(0.1)
+    assert rel_l2(op.get_ut(), ref) <= TOL
+
+
 NS_CASES = [
     dict(N=3, lifting=1, lifting_var=3, visc=0, riemann=44, volume_flux=5),
+    dict(N=4, lifting=1, lifting_var=3, visc=0, riemann=17, volume_flux=7),
+    dict(N=3, lifting=2, lifting_var=1, visc=0, riemann=3, volume_flux=3),
     dict(N=4, lifting=1, lifting_var=1, visc=0, riemann=1, volume_flux=10),
     dict(N=2, lifting=1, lifting_var=2, visc=1, riemann=22, volume_flux=2),
     dict(N=5, lifting=2, lifting_var=3, visc=0, riemann=4, volume_flux=32),
@@ -75,7 +98,8 @@ NS_CASES = [
 
 
 @pytest.mark.parametrize("case", NS_CASES,
-                         ids=lambda c: "N%d_br%d_lv%d_visc%d" % (c["N"], c["lifting"], c["lifting_var"], c["visc"]))
+                         ids=lambda c: "N%d_br%d_lv%d_visc%d_rs%d" % (c["N"], c["lifting"], c["lifting_var"], c["visc"],
+                                                                     c["riemann"]))
 def test_navier_stokes_parity(gpu_lib, case):
     extra = dict(R=1.0, Tref=1.0, Ts=0.4, ExpoPow=0.7) if case["visc"] else {}
     c, op = pair(eqn=1, mu0=0.02, ini_exact_func=7, nElems=(2, 3, 2), NGeo=2, deform_amp=0.05,
