@@ -411,6 +411,8 @@ int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {
   const bool parabolic = (cfg->eqn == FLUXO_EQN_NAVIERSTOKES || cfg->eqn == FLUXO_EQN_MHD_PARABOLIC);
   if (mhd) {
     if (!mhd_riemann_supported(cfg->riemann)) return fail(nullptr, FLUXO_EINVAL_CFG, "MHD Riemann solver not implemented");
+    if (cfg->riemann == 5 && std::fabs(cfg->mu_0 - 1.) > 1.0e-12)  // mhd/equation.f90:343-346
+      return fail(nullptr, FLUXO_EINVAL_CFG, "HLLD solver only for mu_0=1 implemented");
     if (!mhd_volume_flux_supported(cfg->volume_flux))
       return fail(nullptr, FLUXO_EINVAL_CFG, "MHD volume flux not implemented");
     if (cfg->noncons < 0 || cfg->noncons > 3) return fail(nullptr, FLUXO_EINVAL_CFG, "noncons must be 0..3");

@@ -5,7 +5,7 @@
 namespace fluxo {
 
 bool mhd_riemann_supported(int RS) {
-  return RS == 0 || RS == 1 || RS == 4 || RS == 10 || RS == 11 || RS == 12 || RS == 13 || RS == 14 || RS == 15;
+  return (RS >= 0 && RS <= 5) || (RS >= 10 && RS <= 15);
 }
 bool mhd_volume_flux_supported(int VF) { return VF == 0 || VF == 1 || VF == 10 || VF == 12; }
 
@@ -46,7 +46,10 @@ cudaError_t launch_mhd_face(int RS, bool visc, int NP, int nSides, cudaStream_t 
   switch (RS) {
     case 0: return face_rs<0>(visc, NP, nSides, s, P);
     case 1: return face_rs<1>(visc, NP, nSides, s, P);
+    case 2: return face_rs<2>(visc, NP, nSides, s, P);
+    case 3: return face_rs<3>(visc, NP, nSides, s, P);
     case 4: return face_rs<4>(visc, NP, nSides, s, P);
+    case 5: return face_rs<5>(visc, NP, nSides, s, P);
     case 10: return face_rs<10>(visc, NP, nSides, s, P);
     case 11: return face_rs<11>(visc, NP, nSides, s, P);
     case 12: return face_rs<12>(visc, NP, nSides, s, P);

@@ -72,7 +72,10 @@ cudaError_t launch_nfvse_fv(int RS, int NP, int nElems, int nSMs, cudaStream_t s
   switch (RS) {
     case 0: return fv_rs<0>(NP, grid, s, P);
     case 1: return fv_rs<1>(NP, grid, s, P);
+    case 2: return fv_rs<2>(NP, grid, s, P);
+    case 3: return fv_rs<3>(NP, grid, s, P);
     case 4: return fv_rs<4>(NP, grid, s, P);
+    case 5: return fv_rs<5>(NP, grid, s, P);
     case 10: return fv_rs<10>(NP, grid, s, P);
     case 11: return fv_rs<11>(NP, grid, s, P);
     case 12: return fv_rs<12>(NP, grid, s, P);

@@ -382,7 +382,253 @@ __device__ __forceinline__ void es_9wave(const KParams& P, double ch, const doub
 
 template <int RS>
 __host__ __device__ constexpr bool riemann_supported() {
-  return RS == 0 || RS == 1 || RS == 4 || RS == 10 || RS == 11 || RS == 12 || RS == 13 || RS == 14 || RS == 15;
+  return (RS >= 0 && RS <= 5) || (RS >= 10 && RS <= 15);
+}
+
+// PrimToCons, mhd/equation_vars.f90:258-278
+__device__ __forceinline__ void prim_to_cons(const KParams& P, const double* Q, double* U) {
+  U[0] = Q[0];
+  U[1] = Q[1] * Q[0]; U[2] = Q[2] * Q[0]; U[3] = Q[3] * Q[0];
+  U[4] = P.sKappaM1 * Q[4] + 0.5 * (U[1] * Q[1] + U[2] * Q[2] + U[3] * Q[3]) +
+         P.s2mu_0 * (Q[5] * Q[5] + Q[6] * Q[6] + Q[7] * Q[7] + Q[8] * Q[8]);
+#pragma unroll
+  for (int v = 5; v < 9; ++v) U[v] = Q[v];
+}
+
+// RiemannSolverByHLLC, mhd/riemann.f90:371-501 with the HLL state of EvalHLLState :733-757
+__device__ __forceinline__ void hllc(const KParams& P, double ch, const double* UL, const double* UR, double* F) {
+  double QL[9], QR[9], RoeVelx, cfRoe;
+  cons_to_prim(P, UL, QL);
+  cons_to_prim(P, UR, QR);
+  const double cfL = fastest_wave_1d(P, QL);
+  fastest_wave_1d_roe(P, UL, UR, QL, QR, RoeVelx, cfRoe);
+  const double SL = fmin(QL[1] - cfL, RoeVelx - cfRoe);
+  if (SL > 0.0) { flux_1d(P, ch, UL, F); return; }
+  const double SR = fmax(RoeVelx + cfRoe, QR[1] + fastest_wave_1d(P, QR));
+  if (SR < 0.0) { flux_1d(P, ch, UR, F); return; }
+  double FL[9], FR[9], UH[9];
+  flux_1d(P, ch, UL, FL);
+  flux_1d(P, ch, UR, FR);
+#pragma unroll
+  for (int v = 0; v < 9; ++v) UH[v] = (SR * UR[v] - SL * UL[v] - FR[v] + FL[v]) / (SR - SL);
+  const double ptotL = QL[4] + P.s2mu_0 * (QL[5] * QL[5] + QL[6] * QL[6] + QL[7] * QL[7]);
+  const double sRhoH = 1. / UH[0];
+  const double SM = UH[1] * sRhoH;
+  const double Bx = UH[5], By = UH[6], Bz = UH[7];
+  const double pS = ptotL + QL[0] * (QL[1] - SL) * (QL[1] - SM) - P.s2mu_0 * (QL[5] * QL[5] - Bx * Bx);
+  const double ES = pS * SM + P.smu_0 * (-Bx * (UH[5] * UH[1] + UH[6] * UH[2] + UH[7] * UH[3]) * sRhoH +
+                                         UH[8] * (ch * Bx - 0.5 * UH[8] * SM));
+  const bool left = (SL <= 0.0) && (0.0 < SM);
+  const double* U = left ? UL : UR;
+  const double* Q = left ? QL : QR;
+  const double* FF = left ? FL : FR;
+  const double S = left ? SL : SR;
+  const double sd = 1. / (S - SM);
+  double Us[9];
+  Us[0] = Q[0] * (S - Q[1]) * sd;
+  Us[1] = Us[0] * SM;
+  Us[2] = (U[2] * S - FF[2] - P.smu_0 * Bx * By) * sd;
+  Us[3] = (U[3] * S - FF[3] - P.smu_0 * Bx * Bz) * sd;
+  Us[4] = (ES + U[4] * S - FF[4]) * sd;
+  Us[5] = Bx; Us[6] = By; Us[7] = Bz;
+  Us[8] = U[8];
+#pragma unroll
+  for (int v = 0; v < 9; ++v) F[v] = FF[v] + S * (Us[v] - U[v]);
+}
+
+// RiemannSolverByHLLD, mhd/riemann.f90:511-729 (mu_0 = 1, checked at set-up; B_n made continuous)
+__device__ __forceinline__ void hlld(const KParams& P, double ch, const double* ULin, const double* URin, double* F) {
+  constexpr double eps = 1.0e-8, small = 1.0e-12;
+  double QL[9], QR[9], UL[9], UR[9];
+  cons_to_prim(P, ULin, QL);
+  cons_to_prim(P, URin, QR);
+  const double Bn = 0.5 * (QL[5] + QR[5]);
+  QL[5] = Bn; QR[5] = Bn;
+  prim_to_cons(P, QL, UL);
+  prim_to_cons(P, QR, UR);
+  const double FW = fmax(fastest_wave_1d(P, QL), fastest_wave_1d(P, QR));
+  const double SL = fmin(QL[1], QR[1]) - FW;
+  if (SL > 0.0) { flux_1d(P, ch, UL, F); return; }
+  const double SR = fmax(QL[1], QR[1]) + FW;
+  if (SR < 0.0) { flux_1d(P, ch, UR, F); return; }
+  double FL[9], FR[9];
+  flux_1d(P, ch, UL, FL);
+  flux_1d(P, ch, UR, FR);
+  const double rhoL = QL[0], rhoR = QR[0], unL = QL[1], unR = QR[1];
+  const double ptotL = QL[4] + 0.5 * (QL[5] * QL[5] + QL[6] * QL[6] + QL[7] * QL[7]);
+  const double ptotR = QR[4] + 0.5 * (QR[5] * QR[5] + QR[6] * QR[6] + QR[7] * QR[7]);
+  const double SM = (rhoR * unR * (SR - unR) - rhoL * unL * (SL - unL) - ptotR + ptotL) /
+                    (rhoR * (SR - unR) - rhoL * (SL - unL));
+  const double sSL = 1. / (SL - SM), sSR = 1. / (SR - SM);
+  const double rhoLS = rhoL * (SL - unL) * sSL, rhoRS = rhoR * (SR - unR) * sSR;
+  const double sqLS = sqrt(rhoLS), sqRS = sqrt(rhoRS);
+  const double SLS = SM - fabs(Bn) / sqLS, SRS = SM + fabs(Bn) / sqRS;
+  const double ptotS = ptotL + rhoL * (SL - unL) * (SM - unL);
+  // tangential velocity and field of the * states
+  double utL1 = QL[2], utL2 = QL[3], BtL1 = QL[6], BtL2 = QL[7];
+  double utR1 = QR[2], utR2 = QR[3], BtR1 = QR[6], BtR2 = QR[7];
+  double temp = rhoL * (SL - unL) * (SL - SM) - Bn * Bn;
+  if (!(fabs(temp) < eps)) {
+    const double st = 1. / temp;
+    const double a = Bn * (SM - unL) * st, b = (rhoL * (SL - unL) * (SL - unL) - Bn * Bn) * st;
+    utL1 = utL1 - a * BtL1; utL2 = utL2 - a * BtL2;
+    BtL1 = b * BtL1; BtL2 = b * BtL2;
+  }
+  double uBS = SM * Bn + utL1 * BtL1 + utL2 * BtL2;
+  double uB = QL[1] * QL[5] + QL[2] * QL[6] + QL[3] * QL[7];
+  const double eLS = (UL[4] * (SL - unL) + ptotS * SM - ptotL * unL + Bn * (uB - uBS)) * sSL;
+  temp = rhoR * (SR - unR) * (SR - SM) - Bn * Bn;
+  if (!(fabs(temp) < eps)) {
+    const double st = 1. / temp;
+    const double a = Bn * (SM - unR) * st, b = (rhoR * (SR - unR) * (SR - unR) - Bn * Bn) * st;
+    utR1 = utR1 - a * BtR1; utR2 = utR2 - a * BtR2;
+    BtR1 = b * BtR1; BtR2 = b * BtR2;
+  }
+  uBS = SM * Bn + utR1 * BtR1 + utR2 * BtR2;
+  uB = QR[1] * QR[5] + QR[2] * QR[6] + QR[3] * QR[7];
+  const double eRS = (UR[4] * (SR - unR) - ptotR * unR + ptotS * SM + Bn * (uB - uBS)) * sSR;
+  const double ULS[9] = {rhoLS, rhoLS * SM, rhoLS * utL1, rhoLS * utL2, eLS, Bn, BtL1, BtL2, UL[8]};
+  const double URS[9] = {rhoRS, rhoRS * SM, rhoRS * utR1, rhoRS * utR2, eRS, Bn, BtR1, BtR2, UR[8]};
+  if (0.0 <= SLS) {
+#pragma unroll
+    for (int v = 0; v < 9; ++v) F[v] = FL[v] + SL * (ULS[v] - UL[v]);
+    return;
+  }
+  if (0.0 > SRS) {
+#pragma unroll
+    for (int v = 0; v < 9; ++v) F[v] = FR[v] + SR * (URS[v] - UR[v]);
+    return;
+  }
+  double ULSS[9], URSS[9];
+#pragma unroll
+  for (int v = 0; v < 9; ++v) { ULSS[v] = ULS[v]; URSS[v] = URS[v]; }
+  if (!(fabs(Bn) < small)) {
+    const double sgn = Bn < 0.0 ? -1.0 : 1.0;
+    const double st = 1. / (sqLS + sqRS);
+    const double ut1 = (sqLS * utL1 + sqRS * utR1 + sgn * (BtR1 - BtL1)) * st;
+    const double ut2 = (sqLS * utL2 + sqRS * utR2 + sgn * (BtR2 - BtL2)) * st;
+    const double bt1 = (sqLS * BtR1 + sqRS * BtL1 + sgn * (utR1 - utL1) * sqLS * sqRS) * st;
+    const double bt2 = (sqLS * BtR2 + sqRS * BtL2 + sgn * (utR2 - utL2) * sqLS * sqRS) * st;
+    const double uBSS = ut1 * bt1 + ut2 * bt2;
+    ULSS[4] = eLS - sgn * sqLS * ((utL1 * BtL1 + utL2 * BtL2) - uBSS);
+    URSS[4] = eRS + sgn * sqRS * ((utR1 * BtR1 + utR2 * BtR2) - uBSS);
+    ULSS[1] = rhoLS * SM; ULSS[2] = rhoLS * ut1; ULSS[3] = rhoLS * ut2;
+    URSS[1] = rhoRS * SM; URSS[2] = rhoRS * ut1; URSS[3] = rhoRS * ut2;
+    ULSS[6] = bt1; ULSS[7] = bt2; URSS[6] = bt1; URSS[7] = bt2;
+  }
+  if (0.0 <= SM) {
+#pragma unroll
+    for (int v = 0; v < 9; ++v) F[v] = FL[v] + SLS * ULSS[v] - (SLS - SL) * ULS[v] - SL * UL[v];
+  } else {
+#pragma unroll
+    for (int v = 0; v < 9; ++v) F[v] = FR[v] + SRS * URSS[v] - (SRS - SR) * URS[v] - SR * UR[v];
+  }
+}
+
+// RiemannSolverByRoe, mhd/riemann.f90:764-1024: Cargo & Gallice Roe matrix, the dissipation
+// sum_i eta_i |lambda_i| r_i over the 7 waves (entropy fix on the waves 1, 3, 6, 7 as in the reference)
+__device__ __forceinline__ void roe(const KParams& P, double ch, const double* UL, const double* UR, double* F) {
+  constexpr double efix = 1.0e-6, sefix = 1.0e6;
+  double QL[9], QR[9];
+  cons_to_prim(P, UL, QL);
+  cons_to_prim(P, UR, QR);
+  const double sqL = sqrt(QL[0]), sqR = sqrt(QR[0]);
+  const double sS = 1. / (sqL + sqR);
+  const double RL = sqL * sS, RR = sqR * sS;
+  const double ptL = QL[4] + P.s2mu_0 * (QL[5] * QL[5] + QL[6] * QL[6] + QL[7] * QL[7]);
+  const double ptR = QR[4] + P.s2mu_0 * (QR[5] * QR[5] + QR[6] * QR[6] + QR[7] * QR[7]);
+  const double rhoRoe = sqL * sqR, sRhoRoe = 1. / rhoRoe;
+  const double sqRoe = sqrt(rhoRoe), ssqRoe = 1. / sqRoe;
+  double v[3], B[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) { v[d] = RL * QL[1 + d] + RR * QR[1 + d]; B[d] = RL * QR[5 + d] + RR * QL[5 + d]; }
+  const double v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+  const double B2 = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
+  const double H = RL * ((UL[4] + ptL) / QL[0]) + RR * ((UR[4] + ptR) / QR[0]);
+  const double dB0 = QL[5] - QR[5], dB1 = QL[6] - QR[6], dB2 = QL[7] - QR[7];
+  const double XX = 0.5 * (dB0 * dB0 + dB1 * dB1 + dB2 * dB2) * (sS * sS);
+  const double va2 = B2 * P.smu_0 * sRhoRoe;
+  const double c2 = (2. - P.kappa) * XX + P.kappaM1 * (H - 0.5 * v2 - va2);
+  const double sc2 = 1. / c2, c = sqrt(c2);
+  const double ca2 = B[0] * B[0] * P.smu_0 * sRhoRoe, ca = sqrt(ca2);
+  const double astar = sqrt((c2 + va2) * (c2 + va2) - 4. * c2 * ca2);
+  const double cf2 = 0.5 * (c2 + va2 + astar), cf = sqrt(cf2);
+  const double cs2 = 0.5 * (c2 + va2 - astar), cs = sqrt(cs2);
+  flux_1d(P, ch, UL, F);
+  double FR[9];
+  flux_1d(P, ch, UR, FR);
+#pragma unroll
+  for (int z = 0; z < 9; ++z) F[z] = F[z] + FR[z];
+  const double sBx = copysign(1.0, B[0]);
+  const double Bt = sqrt(B[1] * B[1] + B[2] * B[2]);
+  double by, bz;
+  if (Bt > 1.0e-9) { by = B[1] / Bt; bz = B[2] / Bt; } else { by = sqrt(0.5); bz = by; }
+  double af, as;
+  if (cf2 == cs2) { af = 1.; as = 0.; }
+  else if (c2 <= cs2) { af = 0.; as = 1.; }
+  else if (cf2 <= c2) { af = 1.; as = 0.; }
+  else {
+    const double s = 1. / (cf2 - cs2);
+    af = sqrt(fmax(0., (c2 - cs2) * s));
+    as = sqrt(fmax(0., (cf2 - c2) * s));
+  }
+  const double drho = QR[0] - QL[0];
+  const double dv0 = QR[1] - QL[1], dv1 = QR[2] - QL[2], dv2 = QR[3] - QL[3];
+  const double dBy = QR[6] - QL[6], dBz = QR[7] - QL[7];
+  const double dp = P.kappaM1 * ((0.5 * v2 - XX) * drho -
+                                 (v[0] * (UR[1] - UL[1]) + v[1] * (UR[2] - UL[2]) + v[2] * (UR[3] - UL[3])) +
+                                 (UR[4] - UL[4]) - P.smu_0 * (B[0] * (QR[5] - QL[5]) + B[1] * dBy + B[2] * dBz));
+  // |lambda| with the entropy fix of the reference on the waves u-c_f, u-c_s, u+c_a, u+c_f
+  auto fixed = [&](double l) { return fabs(l) < 0.5 * efix ? fabs(l * l * sefix + 0.25 * efix) : fabs(l); };
+  const double l1 = fixed(v[0] - cf), l2 = fabs(v[0] - ca), l3 = fixed(v[0] - cs), l4 = fabs(v[0]);
+  const double l5 = fabs(v[0] + cs), l6 = fixed(v[0] + ca), l7 = fixed(v[0] + cf);
+  // fast waves
+  double bv = by * v[1] + bz * v[2], bdv = by * dv1 + bz * dv2, bdB = by * dBy + bz * dBz;
+  const double ascs = as * cs * sBx, asc = as * c * ssqRoe;
+  const double fc = af * (XX * drho + dp);
+  double g = 0.5 * sc2 * (fc + rhoRoe * (ascs * bdv - af * cf * dv0 + asc * bdB)) * l1;  // eta_1 |lambda_1|
+  double h = 0.5 * sc2 * (fc - rhoRoe * (ascs * bdv - af * cf * dv0 - asc * bdB)) * l7;  // eta_7 |lambda_7|
+  F[0] -= af * (g + h);
+  F[1] -= af * ((v[0] - cf) * g + (v[0] + cf) * h);
+  F[2] -= (af * v[1] + ascs * by) * g + (af * v[1] - ascs * by) * h;
+  F[3] -= (af * v[2] + ascs * bz) * g + (af * v[2] - ascs * bz) * h;
+  F[4] -= (af * (H - va2 - v[0] * cf) + ascs * bv + asc * Bt) * g +
+          (af * (H - va2 + v[0] * cf) - ascs * bv + asc * Bt) * h;
+  F[6] -= asc * by * (g + h);
+  F[7] -= asc * bz * (g + h);
+  // slow waves
+  const double afcf = af * cf * sBx, afc = af * c * ssqRoe;
+  const double sc = as * (XX * drho + dp);
+  g = 0.5 * sc2 * (sc - rhoRoe * (afcf * bdv + as * cs * dv0 + afc * bdB)) * l3;
+  h = 0.5 * sc2 * (sc + rhoRoe * (afcf * bdv + as * cs * dv0 - afc * bdB)) * l5;
+  F[0] -= as * (g + h);
+  F[1] -= as * ((v[0] - cs) * g + (v[0] + cs) * h);
+  F[2] -= (as * v[1] - afcf * by) * g + (as * v[1] + afcf * by) * h;
+  F[3] -= (as * v[2] - afcf * bz) * g + (as * v[2] + afcf * bz) * h;
+  F[4] -= (as * (H - va2 - v[0] * cs) - afcf * bv - afc * Bt) * g +
+          (as * (H - va2 + v[0] * cs) + afcf * bv - afc * Bt) * h;
+  F[6] += afc * by * (g + h);
+  F[7] += afc * bz * (g + h);
+  // Alfven waves
+  bv = bz * v[1] - by * v[2];
+  bdv = bz * dv1 - by * dv2;
+  bdB = bz * dBy - by * dBz;
+  g = 0.5 * (-bdv - sBx * ssqRoe * bdB) * l2;
+  h = 0.5 * (bdv - sBx * ssqRoe * bdB) * l6;
+  F[2] -= -rhoRoe * bz * (g - h);
+  F[3] -= rhoRoe * by * (g - h);
+  F[4] -= -rhoRoe * bv * (g - h);
+  F[6] -= -sBx * sqRoe * bz * (g + h);
+  F[7] -= sBx * sqRoe * by * (g + h);
+  // entropy wave
+  g = sc2 * ((c2 - XX) * drho - dp) * l4;
+  F[0] -= g;
+  F[1] -= v[0] * g;
+  F[2] -= v[1] * g;
+  F[3] -= v[2] * g;
+  F[4] -= (0.5 * v2 + P.kappaM2 * P.sKappaM1 * XX) * g;
+#pragma unroll
+  for (int z = 0; z < 9; ++z) F[z] = 0.5 * F[z];
 }
 
 // SolveRiemannProblem in the rotated frame, mhd/equation.f90:311-391
@@ -414,6 +660,12 @@ __device__ __forceinline__ void riemann(const KParams& P, double ch, const doubl
     flux_1d(P, ch, UR, FR);
 #pragma unroll
     for (int v = 0; v < 9; ++v) F[v] = (SR * FL[v] - SL * FR[v] + SL * SR * (UR[v] - UL[v])) / (SR - SL);
+  } else if constexpr (RS == 2) {
+    hllc(P, ch, UL, UR, F);
+  } else if constexpr (RS == 3) {
+    roe(P, ch, UL, UR, F);
+  } else if constexpr (RS == 5) {
+    hlld(P, ch, UL, UR, F);
   } else if constexpr (RS == 10) {
     es_llf<false>(P, ch, UL, UR, F);
   } else if constexpr (RS == 11) {

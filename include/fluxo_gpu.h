@@ -66,7 +66,7 @@ typedef struct fluxo_cfg {
   int device;        /* CUDA device ordinal */
   /* MHD with GLM cleaning, eqn = FLUXO_EQN_MHD / FLUXO_EQN_MHD_PARABOLIC
    * (src/equation/mhd/equation.f90:134-285; nVar = 9: rho, rho*v, E, B, psi).  The MHD viscosity
-   * mu is mu0 above (constant); riemann 0,1,4,10-15; volume_flux 0,1,10,12. */
+   * mu is mu0 above (constant); riemann 0-5 (5 = HLLD needs mu_0 = 1), 10-15; volume_flux 0,1,10,12. */
   double mu_0;       /* mu_0, magnetic permeability */
   double eta;        /* eta, resistivity (PARABOLIC) */
   double glm_scale;  /* GLM_scale: GLM_ch = GLM_scale * GLM_dtch1 / dt (calctimestep.f90:176) */

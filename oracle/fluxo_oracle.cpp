@@ -1640,6 +1640,8 @@ void InitEquationAndTime(Case& C) {
     C.muMHD = C.parabolic ? P.mu0 : 0.;
     C.GLM_scale = P.glm_scale; C.GLM_scr = P.glm_scr; C.GLM_ch = P.glm_ch;
     C.noncons = P.noncons; C.ncGLM = (P.noncons != 0 && P.nc_glm != 0);
+    if (P.riemann == 5 && std::fabs(C.mu_0 - 1.) > 1.0e-12)  // mhd/equation.f90:343-346
+      throw std::runtime_error("HLLD solver only for mu_0=1 implemented");
   } else if (P.visc == 1) {  // equation.f90:226-233
     C.Ts = P.Ts; C.sTref = 1. / P.Tref; C.ExpoSuth = P.ExpoSuth;
     C.Ts = C.Ts * C.sTref;

@@ -179,7 +179,8 @@ inline void MHD_ConsToPrim(const Case& C, const real* U, real* P) {
 }
 
 // PrimToCons, mhd/equation_vars.f90:258-278
-inline void MHD_PrimToCons(const Case& C, const double* P, double* U) {
+template <typename T>
+inline void MHD_PrimToCons(const Case& C, const T* P, T* U) {
   U[0] = P[0];
   U[1] = P[1] * P[0]; U[2] = P[2] * P[0]; U[3] = P[3] * P[0];
   U[4] = C.sKappaM1 * P[4] + 0.5 * (U[1] * P[1] + U[2] * P[2] + U[3] * P[3]) +
@@ -515,6 +516,220 @@ inline void MHD_EntropyStable9Wave(const Case& C, const real* UL, const real* UR
   }
 }
 
+// RiemannSolverByHLLC, mhd/riemann.f90:371-501 (with GLM), HLL state EvalHLLState :733-757
+inline void MHD_HLLC(const Case& C, const real* UL, const real* UR, real* F) {
+  real PL[9], PR[9];
+  MHD_ConsToPrim(C, UL, PL);
+  MHD_ConsToPrim(C, UR, PR);
+  real cfL = MHD_FastestWave1D(C, PL), RoeVelx, cfRoe;
+  MHD_FastestWave1D_Roe(C, UL, UR, PL, PR, RoeVelx, cfRoe);
+  real SL = fmin(PL[1] - cfL, RoeVelx - cfRoe);
+  if (SL > 0.0) { MHD_Flux1D(C, UL, F); return; }
+  real cfR = MHD_FastestWave1D(C, PR);
+  real SR = fmax(RoeVelx + cfRoe, PR[1] + cfR);
+  if (SR < 0.0) { MHD_Flux1D(C, UR, F); return; }
+  real FL[9], FR[9], UH[9];
+  MHD_Flux1D(C, UL, FL);
+  MHD_Flux1D(C, UR, FR);
+  for (int v = 0; v < 9; ++v) UH[v] = (SR * UR[v] - SL * UL[v] - FR[v] + FL[v]) / (SR - SL);
+  real ptotL = PL[4] + C.s2mu_0 * (PL[5] * PL[5] + PL[6] * PL[6] + PL[7] * PL[7]);
+  real sRhoH = 1. / UH[0];
+  real SM = UH[1] * sRhoH;
+  real Bx = UH[5], By = UH[6], Bz = UH[7];
+  real pS = ptotL + PL[0] * (PL[1] - SL) * (PL[1] - SM) - C.s2mu_0 * (PL[5] * PL[5] - Bx * Bx);
+  real ES = pS * SM + C.smu_0 * (-Bx * (UH[5] * UH[1] + UH[6] * UH[2] + UH[7] * UH[3]) * sRhoH +
+                                 UH[8] * (C.GLM_ch * Bx - 0.5 * UH[8] * SM));
+  const bool left = (SL <= 0.0) && (0.0 < SM);
+  const real* U = left ? UL : UR;
+  const real* P = left ? PL : PR;
+  const real* FF = left ? FL : FR;
+  real S = left ? SL : SR;
+  real s = 1. / (S - SM);
+  real Us[9];
+  Us[0] = P[0] * (S - P[1]) * s;
+  Us[1] = Us[0] * SM;
+  Us[2] = (U[2] * S - FF[2] - C.smu_0 * Bx * By) * s;
+  Us[3] = (U[3] * S - FF[3] - C.smu_0 * Bx * Bz) * s;
+  Us[4] = (ES + U[4] * S - FF[4]) * s;
+  Us[5] = Bx; Us[6] = By; Us[7] = Bz;
+  Us[8] = U[8];
+  for (int v = 0; v < 9; ++v) F[v] = FF[v] + S * (Us[v] - U[v]);
+}
+
+// RiemannSolverByHLLD, mhd/riemann.f90:511-729 (mu_0 = 1; B_n made continuous first)
+inline void MHD_HLLD(const Case& C, const real* ULin, const real* URin, real* F) {
+  const double eps = 1.0e-8, small = 1.0e-12;
+  real PL[9], PR[9], UL[9], UR[9];
+  MHD_ConsToPrim(C, ULin, PL);
+  MHD_ConsToPrim(C, URin, PR);
+  real Bn = 0.5 * (PL[5] + PR[5]);
+  PL[5] = Bn; PR[5] = Bn;
+  MHD_PrimToCons(C, PL, UL);
+  MHD_PrimToCons(C, PR, UR);
+  real FW = fmax(MHD_FastestWave1D(C, PL), MHD_FastestWave1D(C, PR));
+  real SL = fmin(PL[1], PR[1]) - FW;
+  if (SL > 0.0) { MHD_Flux1D(C, UL, F); return; }
+  real SR = fmax(PL[1], PR[1]) + FW;
+  if (SR < 0.0) { MHD_Flux1D(C, UR, F); return; }
+  real FL[9], FR[9];
+  MHD_Flux1D(C, UL, FL);
+  MHD_Flux1D(C, UR, FR);
+  real rhoL = PL[0], rhoR = PR[0], unL = PL[1], unR = PR[1];
+  real ptotL = PL[4] + 0.5 * (PL[5] * PL[5] + PL[6] * PL[6] + PL[7] * PL[7]);
+  real ptotR = PR[4] + 0.5 * (PR[5] * PR[5] + PR[6] * PR[6] + PR[7] * PR[7]);
+  real SM = (rhoR * unR * (SR - unR) - rhoL * unL * (SL - unL) - ptotR + ptotL) /
+            (rhoR * (SR - unR) - rhoL * (SL - unL));
+  real sSL = 1. / (SL - SM), sSR = 1. / (SR - SM);
+  real rhoLS = rhoL * (SL - unL) * sSL, rhoRS = rhoR * (SR - unR) * sSR;
+  real sqLS = sqrt(rhoLS), sqRS = sqrt(rhoRS);
+  real SLS = SM - fabs(Bn) / sqLS, SRS = SM + fabs(Bn) / sqRS;
+  real ptotS = ptotL + rhoL * (SL - unL) * (SM - unL);
+  // tangential velocity and field of the * states (index 0 = normal, zero)
+  real utLS[3] = {0., PL[2], PL[3]}, BtLS[3] = {0., PL[6], PL[7]};
+  real utRS[3] = {0., PR[2], PR[3]}, BtRS[3] = {0., PR[6], PR[7]};
+  real temp = rhoL * (SL - unL) * (SL - SM) - Bn * Bn;
+  if (!(fabs(temp) < eps)) {
+    real st = 1. / temp;
+    real a = Bn * (SM - unL) * st, b = (rhoL * (SL - unL) * (SL - unL) - Bn * Bn) * st;
+    for (int d = 1; d < 3; ++d) { utLS[d] = utLS[d] - a * BtLS[d]; BtLS[d] = b * BtLS[d]; }
+  }
+  real uBS = SM * Bn + utLS[1] * BtLS[1] + utLS[2] * BtLS[2];
+  real uB = PL[1] * PL[5] + PL[2] * PL[6] + PL[3] * PL[7];
+  real eLS = (UL[4] * (SL - unL) + ptotS * SM - ptotL * unL + Bn * (uB - uBS)) * sSL;
+  real ULS[9] = {rhoLS, rhoLS * SM, rhoLS * utLS[1], rhoLS * utLS[2], eLS, Bn, BtLS[1], BtLS[2], UL[8]};
+  temp = rhoR * (SR - unR) * (SR - SM) - Bn * Bn;
+  if (!(fabs(temp) < eps)) {
+    real st = 1. / temp;
+    real a = Bn * (SM - unR) * st, b = (rhoR * (SR - unR) * (SR - unR) - Bn * Bn) * st;
+    for (int d = 1; d < 3; ++d) { utRS[d] = utRS[d] - a * BtRS[d]; BtRS[d] = b * BtRS[d]; }
+  }
+  uBS = SM * Bn + utRS[1] * BtRS[1] + utRS[2] * BtRS[2];
+  uB = PR[1] * PR[5] + PR[2] * PR[6] + PR[3] * PR[7];
+  real eRS = (UR[4] * (SR - unR) - ptotR * unR + ptotS * SM + Bn * (uB - uBS)) * sSR;
+  real URS[9] = {rhoRS, rhoRS * SM, rhoRS * utRS[1], rhoRS * utRS[2], eRS, Bn, BtRS[1], BtRS[2], UR[8]};
+  real ULSS[9], URSS[9];
+  for (int v = 0; v < 9; ++v) { ULSS[v] = ULS[v]; URSS[v] = URS[v]; }
+  if (!(fabs(Bn) < small)) {
+    real sgn = Bn < 0.0 ? -1.0 : 1.0;
+    real st = 1. / (sqLS + sqRS);
+    real utSS[3], BtSS[3];
+    for (int d = 1; d < 3; ++d) {
+      utSS[d] = (sqLS * utLS[d] + sqRS * utRS[d] + sgn * (BtRS[d] - BtLS[d])) * st;
+      BtSS[d] = (sqLS * BtRS[d] + sqRS * BtLS[d] + sgn * (utRS[d] - utLS[d]) * sqLS * sqRS) * st;
+    }
+    uBS = utSS[1] * BtSS[1] + utSS[2] * BtSS[2];
+    real eLSS = eLS - sgn * sqLS * ((utLS[1] * BtLS[1] + utLS[2] * BtLS[2]) - uBS);
+    real eRSS = eRS + sgn * sqRS * ((utRS[1] * BtRS[1] + utRS[2] * BtRS[2]) - uBS);
+    real uSS[3] = {SM, utSS[1], utSS[2]}, BSS[3] = {Bn, BtSS[1], BtSS[2]};
+    for (int d = 0; d < 3; ++d) {
+      ULSS[1 + d] = rhoLS * uSS[d]; URSS[1 + d] = rhoRS * uSS[d];
+      ULSS[5 + d] = BSS[d]; URSS[5 + d] = BSS[d];
+    }
+    ULSS[4] = eLSS; URSS[4] = eRSS;
+  }
+  if (0.0 <= SLS) {
+    for (int v = 0; v < 9; ++v) F[v] = FL[v] + SL * (ULS[v] - UL[v]);
+  } else if (0.0 <= SM) {
+    for (int v = 0; v < 9; ++v) F[v] = FL[v] + SLS * ULSS[v] - (SLS - SL) * ULS[v] - SL * UL[v];
+  } else if (0.0 <= SRS) {
+    for (int v = 0; v < 9; ++v) F[v] = FR[v] + SRS * URSS[v] - (SRS - SR) * URS[v] - SR * UR[v];
+  } else {
+    for (int v = 0; v < 9; ++v) F[v] = FR[v] + SR * (URS[v] - UR[v]);
+  }
+}
+
+// RiemannSolverByRoe, mhd/riemann.f90:764-1024 (Cargo & Gallice Roe matrix, entropy fix on the
+// waves 1, 3, 6, 7 as in the reference)
+inline void MHD_Roe(const Case& C, const real* UL, const real* UR, real* F) {
+  const double efix = 1.0e-6, sefix = 1.0e6;
+  real PL[9], PR[9];
+  MHD_ConsToPrim(C, UL, PL);
+  MHD_ConsToPrim(C, UR, PR);
+  real sqL = sqrt(PL[0]), sqR = sqrt(PR[0]);
+  real sS = 1. / (sqL + sqR);
+  real RL = sqL * sS, RR = sqR * sS;
+  real ptL = PL[4] + C.s2mu_0 * (PL[5] * PL[5] + PL[6] * PL[6] + PL[7] * PL[7]);
+  real ptR = PR[4] + C.s2mu_0 * (PR[5] * PR[5] + PR[6] * PR[6] + PR[7] * PR[7]);
+  real rhoRoe = sqL * sqR;
+  real sRhoRoe = 1. / rhoRoe;
+  real sqRoe = sqrt(rhoRoe);
+  real ssqRoe = 1. / sqRoe;
+  real v[3], B[3];
+  for (int d = 0; d < 3; ++d) { v[d] = RL * PL[1 + d] + RR * PR[1 + d]; B[d] = RL * PR[5 + d] + RR * PL[5 + d]; }
+  real v2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+  real B2 = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
+  real HL = (UL[4] + ptL) / PL[0], HR = (UR[4] + ptR) / PR[0];
+  real H = RL * HL + RR * HR;
+  real dB0 = PL[5] - PR[5], dB1 = PL[6] - PR[6], dB2 = PL[7] - PR[7];
+  real XX = 0.5 * (dB0 * dB0 + dB1 * dB1 + dB2 * dB2) * (sS * sS);
+  real va2 = B2 * C.smu_0 * sRhoRoe;
+  real c2 = (2. - C.kappa) * XX + C.kappaM1 * (H - 0.5 * v2 - va2);
+  real sc2 = 1. / c2;
+  real c = sqrt(c2);
+  real ca2 = B[0] * B[0] * C.smu_0 * sRhoRoe;
+  real ca = sqrt(ca2);
+  real astar = sqrt((c2 + va2) * (c2 + va2) - 4. * c2 * ca2);
+  real cf2 = 0.5 * (c2 + va2 + astar), cf = sqrt(cf2);
+  real cs2 = 0.5 * (c2 + va2 - astar), cs = sqrt(cs2);
+  real FL[9], FR[9];
+  MHD_Flux1D(C, UL, FL);
+  MHD_Flux1D(C, UR, FR);
+  real sBx = std::signbit(val(B[0])) ? -1.0 : 1.0;
+  real Bt = sqrt(B[1] * B[1] + B[2] * B[2]);
+  real by, bz;
+  if (Bt > 1.0e-9) { by = B[1] / Bt; bz = B[2] / Bt; } else { by = sqrt(real(0.5)); bz = by; }
+  real af, as;
+  if (val(cf2) == val(cs2)) { af = 1.; as = 0.; }
+  else if (c2 <= cs2) { af = 0.; as = 1.; }
+  else if (cf2 <= c2) { af = 1.; as = 0.; }
+  else {
+    real s = 1. / (cf2 - cs2);
+    af = sqrt(fmax(real(0.), (c2 - cs2) * s));
+    as = sqrt(fmax(real(0.), (cf2 - c2) * s));
+  }
+  real drho = PR[0] - PL[0];
+  real dv[3] = {PR[1] - PL[1], PR[2] - PL[2], PR[3] - PL[3]};
+  real dB[3] = {PR[5] - PL[5], PR[6] - PL[6], PR[7] - PL[7]};
+  real dp = C.kappaM1 * ((0.5 * v2 - XX) * drho -
+                         (v[0] * (UR[1] - UL[1]) + v[1] * (UR[2] - UL[2]) + v[2] * (UR[3] - UL[3])) +
+                         (UR[4] - UL[4]) - C.smu_0 * (B[0] * dB[0] + B[1] * dB[1] + B[2] * dB[2]));
+  real lam[7] = {v[0] - cf, v[0] - ca, v[0] - cs, v[0], v[0] + cs, v[0] + ca, v[0] + cf};
+  real eta[7];
+  real bv = by * v[1] + bz * v[2], bdv = by * dv[1] + bz * dv[2], bdB = by * dB[1] + bz * dB[2];
+  real ascs = as * cs * sBx, asc = as * c * ssqRoe;
+  real EVr1[8] = {af, af * lam[0], af * v[1] + ascs * by, af * v[2] + ascs * bz,
+                  af * (H - va2 - v[0] * cf) + ascs * bv + asc * Bt, 0., asc * by, asc * bz};
+  real EVr7[8] = {af, af * lam[6], af * v[1] - ascs * by, af * v[2] - ascs * bz,
+                  af * (H - va2 + v[0] * cf) - ascs * bv + asc * Bt, 0., asc * by, asc * bz};
+  eta[0] = 0.5 * sc2 * (af * (XX * drho + dp) + rhoRoe * (ascs * bdv - af * cf * dv[0] + asc * bdB));
+  eta[6] = 0.5 * sc2 * (af * (XX * drho + dp) - rhoRoe * (ascs * bdv - af * cf * dv[0] - asc * bdB));
+  real afcf = af * cf * sBx, afc = af * c * ssqRoe;
+  real EVr3[8] = {as, as * lam[2], as * v[1] - afcf * by, as * v[2] - afcf * bz,
+                  as * (H - va2 - v[0] * cs) - afcf * bv - afc * Bt, 0., -afc * by, -afc * bz};
+  real EVr5[8] = {as, as * lam[4], as * v[1] + afcf * by, as * v[2] + afcf * bz,
+                  as * (H - va2 + v[0] * cs) + afcf * bv - afc * Bt, 0., -afc * by, -afc * bz};
+  eta[2] = 0.5 * sc2 * (as * (XX * drho + dp) - rhoRoe * (afcf * bdv + as * cs * dv[0] + afc * bdB));
+  eta[4] = 0.5 * sc2 * (as * (XX * drho + dp) + rhoRoe * (afcf * bdv + as * cs * dv[0] - afc * bdB));
+  bv = bz * v[1] - by * v[2];
+  bdv = bz * dv[1] - by * dv[2];
+  bdB = bz * dB[1] - by * dB[2];
+  real EVr2[8] = {0., 0., -rhoRoe * bz, rhoRoe * by, -rhoRoe * bv, 0., -sBx * sqRoe * bz, sBx * sqRoe * by};
+  real EVr6[8] = {0., 0., rhoRoe * bz, -rhoRoe * by, rhoRoe * bv, 0., -sBx * sqRoe * bz, sBx * sqRoe * by};
+  eta[1] = 0.5 * (-bdv - sBx * ssqRoe * bdB);
+  eta[5] = 0.5 * (bdv - sBx * ssqRoe * bdB);
+  real EVr4[8] = {1., v[0], v[1], v[2], 0.5 * v2 + C.kappaM2 * C.sKappaM1 * XX, 0., 0., 0.};
+  eta[3] = sc2 * ((c2 - XX) * drho - dp);
+  for (int z : {0, 6, 2, 5})
+    if (fabs(lam[z]) < 0.5 * efix) lam[z] = lam[z] * lam[z] * sefix + 0.25 * efix;
+  const real* EV7[7] = {EVr1, EVr2, EVr3, EVr4, EVr5, EVr6, EVr7};
+  for (int v9 = 0; v9 < 9; ++v9) F[v9] = FL[v9] + FR[v9];
+  for (int i = 0; i < 7; ++i) {
+    real g = eta[i] * fabs(lam[i]);
+    for (int r = 0; r < 8; ++r) F[r] = F[r] - g * EV7[i][r];
+  }
+  for (int v9 = 0; v9 < 9; ++v9) F[v9] = 0.5 * F[v9];
+}
+
 // SolveRiemannProblem (rotated frame) for the MHD solvers, mhd/equation.f90:311-391
 inline void MHD_Riemann(const Case& C, const real* UL, const real* UR, real* F) {
   switch (C.P.riemann) {
@@ -547,6 +762,9 @@ inline void MHD_Riemann(const Case& C, const real* UL, const real* UR, real* F) 
       for (int v = 0; v < 9; ++v) F[v] = (SR * FL[v] - SL * FR[v] + SL * SR * (UR[v] - UL[v])) / (SR - SL);
       return;
     }
+    case 2: MHD_HLLC(C, UL, UR, F); return;
+    case 3: MHD_Roe(C, UL, UR, F); return;
+    case 5: MHD_HLLD(C, UL, UR, F); return;
     case 10: MHD_EntropyStableLLF(C, UL, UR, false, F); return;
     case 11: MHD_DerigsFlux(C, UL, UR, F); return;
     case 12: MHD_FloGorFlux(C, UL, UR, F); return;

@@ -55,6 +55,9 @@ IDEAL = [
     dict(N=3, volume_flux=10, riemann=12, noncons=0, nc_glm=0),
     dict(N=7, volume_flux=10, riemann=14, noncons=1, nc_glm=0, nElems=(1, 2, 1)),
     dict(N=6, volume_flux=12, riemann=0, noncons=1, nc_glm=1, nElems=(2, 1, 1)),
+    dict(N=3, volume_flux=10, riemann=2, noncons=1, nc_glm=1),
+    dict(N=4, volume_flux=0, riemann=3, noncons=1, nc_glm=0),
+    dict(N=3, volume_flux=12, riemann=5, noncons=2, nc_glm=0),
 ]
 
 
@@ -72,10 +75,12 @@ PARA = [
     dict(N=4, lifting=1, lifting_var=1, volume_flux=10, riemann=10),
     dict(N=3, lifting=2, lifting_var=2, volume_flux=12, riemann=1),
     dict(N=2, lifting=2, lifting_var=3, volume_flux=0, riemann=4),
+    dict(N=3, lifting=1, lifting_var=3, volume_flux=10, riemann=5),
 ]
 
 
-@pytest.mark.parametrize("case", PARA, ids=lambda c: "N%d_br%d_lv%d" % (c["N"], c["lifting"], c["lifting_var"]))
+@pytest.mark.parametrize("case", PARA, ids=lambda c: "N%d_br%d_lv%d_rs%d" % (c["N"], c["lifting"], c["lifting_var"],
+                                                                           c["riemann"]))
 def test_mhd_resistive_parity(gpu_lib, case):
     c, op = mhd_pair(eqn=3, eta=0.02, mu0=0.01, noncons=1, **case)
     ref = c.dg_time_derivative(0.0)

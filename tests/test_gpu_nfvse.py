@@ -51,6 +51,8 @@ FIXED = [
     dict(N=3, volume_flux=0, riemann=1, noncons=3, nc_glm=0),
     dict(N=5, volume_flux=1, riemann=4, noncons=0, nc_glm=0),
     dict(N=7, volume_flux=12, riemann=13, noncons=1, nc_glm=1, nElems=(1, 2, 1)),
+    dict(N=3, volume_flux=10, riemann=5, noncons=1, nc_glm=0),
+    dict(N=4, volume_flux=10, riemann=3, noncons=1, nc_glm=1),
 ]
 
 

@@ -74,3 +74,57 @@ def test_mhd_glm_speed_from_timestep():
     cfl = 0.9 * 2.8451 / 7.0  # CFLScale * alpha(N=3) / (2N+1)
     dtch1 = cfl * 0.5 / 3.0
     assert c.glm_ch == pytest.approx(0.5 * dtch1 / dt, rel=1e-13)
+
+
+def _mhd_state(rng, B=True, psi=True):
+    rho, p = 1 + 0.3 * rng.random(), 0.8 + 0.4 * rng.random()
+    v = 0.4 * rng.standard_normal(3)
+    b = 0.6 * rng.standard_normal(3) if B else np.zeros(3)
+    s = 0.1 * rng.standard_normal() if psi else 0.0
+    E = p / (5 / 3 - 1) + 0.5 * rho * v @ v + 0.5 * (b @ b + s * s)
+    return np.array([rho, *(rho * v), E, *b, s])
+
+
+def _point_case(**kw):
+    return OracleCase(eqn=2, N=1, nElems=(1, 1, 1), volume_flux=10, kappa=5 / 3, glm_ch=0.7, ini_exact_func=1,
+                      mhd_ref_state=REF, **kw)
+
+
+@pytest.mark.parametrize("rs", [2, 3, 5])
+def test_mhd_hllc_roe_hlld_consistent(rs):
+    """F*(U, U) equals the Rusanov flux at U, i.e. the physical flux (GLM terms included)."""
+    rng = np.random.default_rng(40 + rs)
+    c = _point_case(riemann=rs)
+    r = _point_case(riemann=1)
+    for _ in range(5):
+        U = _mhd_state(rng)
+        Q, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+        args = (U, U, Q[:, 0], Q[:, 1], Q[:, 2])
+        assert np.allclose(c.riemann(*args), r.riemann(*args), rtol=1e-12, atol=1e-13)
+
+
+def test_mhd_roe_without_field_is_the_euler_roe_flux():
+    """With B = 0 and psi = 0 the Cargo-Gallice Roe matrix reduces to the Euler Roe solver."""
+    rng = np.random.default_rng(7)
+    m = _point_case(riemann=3)
+    e = OracleCase(eqn=0, N=1, nElems=(1, 1, 1), riemann=3, volume_flux=0, kappa=5 / 3)
+    for _ in range(5):
+        UL, UR = _mhd_state(rng, B=False, psi=False), _mhd_state(rng, B=False, psi=False)
+        Q, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+        Fm = m.riemann(UL, UR, Q[:, 0], Q[:, 1], Q[:, 2])
+        Fe = e.riemann(UL[:5], UR[:5], Q[:, 0], Q[:, 1], Q[:, 2])
+        assert np.allclose(Fm[:5], Fe, rtol=1e-12, atol=1e-13)
+        assert np.allclose(Fm[5:], 0, atol=1e-13)
+
+
+@pytest.mark.parametrize("eqn", [2, 3])
+@pytest.mark.parametrize("vf,rs", [(10, 2), (0, 3), (10, 5)])
+def test_mhd_freestream_hllc_roe_hlld(eqn, vf, rs):
+    c = OracleCase(eqn=eqn, ini_exact_func=1, volume_flux=vf, riemann=rs, noncons=1, nc_glm=1, **WARPED,
+                   **(PARA if eqn == 3 else {}))
+    assert np.abs(c.dg_time_derivative(0.0)).max() <= 1e-11
+
+
+def test_hlld_needs_unit_mu0():
+    with pytest.raises(Exception):
+        _point_case(riemann=5, mu_0=2.0)
