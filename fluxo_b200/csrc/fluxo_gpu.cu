@@ -656,7 +656,10 @@ int fluxo_gpu_time_disc(fluxo_handle* h, double t, double tEnd, int maxIter, dou
   td_glm_kernel<<<1, 1, 0, s>>>(td, h->mhd ? 1 : 0, h->glmCh, h->cfg.glm_scale, h->glmDtch1);
   FLUXO_CUDA(h, cudaGetLastError());
   h->launches += 2;
+  // steps are enqueued in chunks between halt checks; with maxIter > 0 no more than maxIter steps
+  // are enqueued in all (steps after a halt return at once but still count as launches)
   const int chunk = 16;
+  int enqueued = 0;
   for (;;) {
     for (int c = 0; c < chunk; ++c) {
       KParams P = base_params(h);
@@ -672,7 +675,7 @@ int fluxo_gpu_time_disc(fluxo_handle* h, double t, double tEnd, int maxIter, dou
       td_advance_kernel<<<1, 1, 0, s>>>(td);
       FLUXO_CUDA(h, cudaGetLastError());
       h->launches += 3;
-      if (maxIter > 0 && c + 1 >= maxIter) break;
+      if (maxIter > 0 && ++enqueued >= maxIter) break;
     }
     TDState hs;
     FLUXO_CUDA(h, cudaMemcpyAsync(&hs, td, sizeof(TDState), cudaMemcpyDeviceToHost, s));

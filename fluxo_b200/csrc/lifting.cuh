@@ -13,8 +13,12 @@
 //   3. the viscous volume integral sum_l D_hat(i,l) (f~,g~,h~)(l) of the contravariant viscous
 //      fluxes (volint.f90:228-271 with EvalDiffFluxTilde3D flux.f90:523-635), written as 4 values per
 //      node for the volume kernel.
-// The derivative sums are line-blocked: one thread loads a whole line of one variable into registers
-// and produces all N+1 outputs, so a shared-memory load serves N+1 multiply-adds.
+// Both operator applications are node-centric: every thread forms the derivatives (and later the
+// divergence) of its own node from the N+1 nodes of its three lines, so the gradient flows straight
+// from the derivative sums into the flux evaluation and the divergence straight into the global
+// store, with two block barriers in all and the same work on every thread.  Reads of a line are
+// broadcasts or consecutive doubles within a warp (no bank conflicts, no padding), and every
+// shared-memory address is a per-thread base plus a compile-time offset.
 #pragma once
 #include "common.cuh"
 #include "physics_ns.cuh"
@@ -23,13 +27,17 @@ namespace fluxo {
 
 template <int NP>
 __host__ __device__ constexpr int lv_epb() { return (256 / (NP * NP * NP)) > 0 ? (256 / (NP * NP * NP)) : 1; }
+// padded node slots of the MHD lifting kernel's line-blocked arrays
 template <int NP>
 __host__ __device__ constexpr int lv_slots() { return (NP * NP * NP - 1) + ((NP * NP * NP - 1) >> 4) + 1; }
-// per element: 5 lifting variables + 15 derivatives, later 12 contravariant fluxes + 12 directional
-// divergences
+// per element: the 5 lifting variables, then the 12 contravariant viscous fluxes (4 per direction)
+// row stride of the operator copies in shared memory: odd, so that the rows D(i,.) that the 8 lanes
+// of a line read at once fall into different banks
+template <int NP>
+__host__ __device__ constexpr int lv_row() { return NP | 1; }
 template <int NP>
 __host__ __device__ constexpr size_t lv_smem_bytes() {
-  return sizeof(double) * (size_t)(2 * NP * NP + lv_epb<NP>() * 24 * lv_slots<NP>());
+  return sizeof(double) * (size_t)(2 * NP * lv_row<NP>() + lv_epb<NP>() * 17 * NP * NP * NP);
 }
 
 __device__ __forceinline__ int lv_slot(int n) { return n + (n >> 4); }
@@ -38,35 +46,6 @@ __device__ __forceinline__ int lv_slot(int n) { return n + (n >> 4); }
 template <int NP>
 __device__ __forceinline__ int line_node(int dir, int a, int b, int x) {
   return dir == 0 ? x + NP * (a + NP * b) : (dir == 1 ? a + NP * (x + NP * b) : a + NP * (b + NP * x));
-}
-
-// sum_l row[l] x[l] for a row of an (N+1)^2 operator in shared memory, in the order l = 0..N.  For
-// even N+1 the row is read with 16-byte loads (half the load instructions; every lane reads the same
-// address, a broadcast).  FRESH: the row is re-read on every call, so the compiler cannot hoist the
-// whole operator out of a loop into registers (which spills).
-template <int NP, bool FRESH>
-__device__ __forceinline__ double row_dot(const double* row, const double* x) {
-  double s = 0.;
-  if constexpr (NP % 2 == 0) {
-#pragma unroll
-    for (int l = 0; l < NP; l += 2) {
-      double a, b;
-      if constexpr (FRESH) {
-        const unsigned addr = static_cast<unsigned>(__cvta_generic_to_shared(row + l));
-        asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(a), "=d"(b) : "r"(addr));
-      } else {
-        const double2 r2 = *reinterpret_cast<const double2*>(row + l);
-        a = r2.x; b = r2.y;
-      }
-      s += a * x[l];
-      s += b * x[l + 1];
-    }
-  } else {
-    const volatile double* vrow = row;
-#pragma unroll
-    for (int l = 0; l < NP; ++l) s += (FRESH ? vrow[l] : row[l]) * x[l];
-  }
-  return s;
 }
 
 template <int LV>
@@ -90,75 +69,70 @@ __device__ __forceinline__ void lifting_var_t(const KParams& P, const double* U,
 }
 
 template <int NP, int LIFT, int LV>
-#ifndef FLUXO_LV_MINB
-#define FLUXO_LV_MINB 2  // resident blocks per SM the register allocation must allow
-#endif
-__global__ void __launch_bounds__(lv_epb<NP>() * NP * NP * NP, FLUXO_LV_MINB)
-lift_visc_kernel(KParams P) {
+__global__ void __launch_bounds__(lv_epb<NP>() * NP * NP * NP, 2) lift_visc_kernel(KParams P) {
   if (halted(P)) return;
-  constexpr int NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1, EPB = lv_epb<NP>(), NS = lv_slots<NP>();
+  constexpr int NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1, EPB = lv_epb<NP>(), R = lv_row<NP>();
   extern __shared__ double smem[];
-  double* sD = smem;           // D(i,l) at [i*NP+l]
-  double* sDhat = sD + NPT;    // D_hat(i,l)
+  double* sD = smem;             // D(i,l) at [i*R+l]
+  double* sDhat = sD + NP * R;   // D_hat(i,l)
   const int eb = threadIdx.x / NP3, t = threadIdx.x - eb * NP3;
   const int e = blockIdx.x * EPB + eb;
   const bool valid = e < P.nElems;
-  // per element 24 arrays of NS: [0,5) lifting variable, [5,20) xi/eta/zeta derivatives; later
-  // [5,17) contravariant fluxes and the 12 directional divergences in [0,5) and [17,24)
-  double* sV = sDhat + NPT + (size_t)eb * 24 * NS;
-  double* sW = sV + 5 * NS;
+  double* sV = sDhat + NP * R + (size_t)eb * 17 * NP3;  // [5][node] lifting variable
+  double* sF = sV + 5 * NP3;                         // [12][node] contravariant fluxes, 4 per direction
   __shared__ int sE2S[EPB][12];  // the element's ElemToSide (side, flip per local side)
   for (int z = threadIdx.x; z < NPT; z += blockDim.x) {
-    sD[z] = P.basis->D[z];
-    sDhat[z] = P.basis->Dhat[z];
+    const int r = z / NP, c = z - r * NP;
+    sD[r * R + c] = P.basis->D[z];
+    sDhat[r * R + c] = P.basis->Dhat[z];
   }
+  const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
+  // first node of the own xi / eta / zeta line; the line's nodes follow at strides 1, NP, NP^2
+  const int bx = t - i, be = t - NP * j, bz = t - NPT * k;
   double u[5];
   if (valid) {
     for (int z = t; z < 12; z += NP3) sE2S[eb][z] = P.e2s[12 * (size_t)e + z];  // NP3 = 8 for N = 1
     const double* Ug = P.U + 5 * ((size_t)e * NP3 + t);
 #pragma unroll
     for (int v = 0; v < 5; ++v) u[v] = Ug[v];
-    // metrics and Jacobian are read after the derivative phase: start them towards L2 now
 #pragma unroll
     for (int c = 0; c < 9; ++c) prefetch_l2(P.metrics + (size_t)e * 9 * NP3 + c * NP3 + t);
     prefetch_l2(P.sJ + (size_t)e * NP3 + t);
     double V[5];
     lifting_var_t<LV>(P, u, V);
 #pragma unroll
-    for (int v = 0; v < 5; ++v) sV[v * NS + lv_slot(t)] = V[v];
+    for (int v = 0; v < 5; ++v) sV[v * NP3 + t] = V[v];
   }
   __syncthreads();
-  // derivatives of the lifting variable along xi, eta, zeta: tasks (dir, var, line)
-  if (valid) {
-    for (int task = t; task < 15 * NPT; task += NP3) {
-      const int dir = task / (5 * NPT), rem = task - dir * 5 * NPT, v = rem / NPT, L = rem - v * NPT;
-      const int a = L % NP, b = L / NP;
-      double x[NP];
-#pragma unroll
-      for (int l = 0; l < NP; ++l) x[l] = sV[v * NS + lv_slot(line_node<NP>(dir, a, b, l))];
-#pragma unroll
-      for (int o = 0; o < NP; ++o) sW[(dir * 5 + v) * NS + lv_slot(line_node<NP>(dir, a, b, o))] = row_dot<NP, true>(sD + o * NP, x);
-    }
-  }
-  __syncthreads();
-  // Each thread reads only its own node's derivatives and overwrites the same node's slots with its
-  // contravariant fluxes, so no barrier separates the two.  The metrics are read twice (gradient
-  // transform, flux transform) rather than held across the gradient work: fewer live registers.
   if (valid) {
     const double* M = P.metrics + (size_t)e * 9 * NP3 + t;
     const double sj = P.sJ[(size_t)e * NP3 + t];
     double g[3][5];
     {
+      // derivatives of the lifting variable along xi, eta, zeta at the own node, l = 0..N
+      double dx[5], de[5], dz[5];
+#pragma unroll
+      for (int v = 0; v < 5; ++v) { dx[v] = 0.; de[v] = 0.; dz[v] = 0.; }
+      const double* Di = sD + i * R;
+      const double* Dj = sD + j * R;
+      const double* Dk = sD + k * R;
+#pragma unroll
+      for (int l = 0; l < NP; ++l) {
+        const double a = Di[l], b = Dj[l], c = Dk[l];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          dx[v] += a * sV[v * NP3 + bx + l];
+          de[v] += b * sV[v * NP3 + be + NP * l];
+          dz[v] += c * sV[v * NP3 + bz + NPT * l];
+        }
+      }
       double m[9];
 #pragma unroll
       for (int c = 0; c < 9; ++c) m[c] = M[c * NP3];
 #pragma unroll
-      for (int v = 0; v < 5; ++v) {
-        const double gx = sW[(0 + v) * NS + lv_slot(t)], ge = sW[(5 + v) * NS + lv_slot(t)],
-                     gz = sW[(10 + v) * NS + lv_slot(t)];
+      for (int v = 0; v < 5; ++v)
 #pragma unroll
-        for (int d = 0; d < 3; ++d) g[d][v] = m[0 + d] * gx + m[3 + d] * ge + m[6 + d] * gz;
-      }
+        for (int d = 0; d < 3; ++d) g[d][v] = m[0 + d] * dx[v] + m[3 + d] * de[v] + m[6 + d] * dz[v];
     }
     double gv[3][5];  // BR2: volume part of the gradient, the base of every face trace
     if constexpr (LIFT == 2) {
@@ -170,7 +144,6 @@ lift_visc_kernel(KParams P) {
           gv[d][v] = g[d][v];
         }
     }
-    const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
     int sides[3];
     const int ns = boundary_sides(i, j, k, N, sides);
     const double lh = P.basis->LhatM0;
@@ -237,40 +210,35 @@ lift_visc_kernel(KParams P) {
         for (int v = 0; v < 4; ++v) T[(size_t)v * NPT] = n0 * f[v] + n1 * gg[v] + n2 * h[v];
       }
     }
-    const int st = lv_slot(t);
+    // contravariant fluxes (metrics re-read rather than held across the gradient work)
 #pragma unroll
     for (int dir = 0; dir < 3; ++dir) {
       const double m0 = M[(3 * dir + 0) * NP3], m1 = M[(3 * dir + 1) * NP3], m2 = M[(3 * dir + 2) * NP3];
 #pragma unroll
-      for (int v = 0; v < 4; ++v) sW[(4 * dir + v) * NS + st] = f[v] * m0 + gg[v] * m1 + h[v] * m2;
+      for (int v = 0; v < 4; ++v) sF[(4 * dir + v) * NP3 + t] = f[v] * m0 + gg[v] * m1 + h[v] * m2;
     }
   }
   __syncthreads();
-  // viscous volume integral: sum_l D_hat(o,l) f~(l) along each direction, tasks (dir, var, line) of
-  // all three directions at once, each (dir, var) into its own array (array dv -> sV index
-  // dv < 5 ? dv : dv + 12, around the fluxes in [5,17))
+  // viscous volume integral at the own node: sum_l D_hat(i,l) f~(l,j,k) + D_hat(j,l) g~(i,l,k) +
+  // D_hat(k,l) h~(i,j,l), l = 0..N
   if (valid) {
-    for (int task = t; task < 12 * NPT; task += NP3) {
-      const int dv = task / NPT, L = task - dv * NPT, a = L % NP, b = L / NP, dir = dv >> 2;
-      double x[NP];
+    double r[4] = {0., 0., 0., 0.};
+    const double* Hi = sDhat + i * R;
+    const double* Hj = sDhat + j * R;
+    const double* Hk = sDhat + k * R;
 #pragma unroll
-      for (int l = 0; l < NP; ++l) x[l] = sW[dv * NS + lv_slot(line_node<NP>(dir, a, b, l))];
-      double* out = sV + (dv < 5 ? dv : dv + 12) * NS;
-      // D_hat re-read per row: hoisting its NP^2 entries out of the task loop spills
+    for (int l = 0; l < NP; ++l) {
+      const double a = Hi[l], b = Hj[l], c = Hk[l];
 #pragma unroll
-      for (int o = 0; o < NP; ++o) out[lv_slot(line_node<NP>(dir, a, b, o))] = row_dot<NP, true>(sDhat + o * NP, x);
+      for (int v = 0; v < 4; ++v) {
+        r[v] += a * sF[v * NP3 + bx + l];
+        r[v] += b * sF[(4 + v) * NP3 + be + NP * l];
+        r[v] += c * sF[(8 + v) * NP3 + bz + NPT * l];
+      }
     }
-  }
-  __syncthreads();
-  if (valid) {
     double* O = P.utvisc + (size_t)e * 4 * NP3 + t;
-    const int st = lv_slot(t);
-    // divergence arrays of (dir, v): dv = 4 dir + v at sV index dv < 5 ? dv : dv + 12
 #pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const int d1 = 4 + v, d2 = 8 + v;
-      O[v * NP3] = (sV[v * NS + st] + sV[(d1 < 5 ? d1 : d1 + 12) * NS + st]) + sV[(d2 + 12) * NS + st];
-    }
+    for (int v = 0; v < 4; ++v) O[v * NP3] = r[v];
   }
 }
 
