@@ -68,8 +68,13 @@ __device__ __forceinline__ void lifting_var_t(const KParams& P, const double* U,
   }
 }
 
+// resident blocks per SM the register allocation must allow: 2, except BR2 for N+1 >= 7, whose
+// per-side traces need more than the 64 registers of two 512-thread blocks
+template <int NP, int LIFT>
+__host__ __device__ constexpr int lv_minb() { return (LIFT == 2 && NP >= 7) ? 1 : 2; }
+
 template <int NP, int LIFT, int LV>
-__global__ void __launch_bounds__(lv_epb<NP>() * NP * NP * NP, 2) lift_visc_kernel(KParams P) {
+__global__ void __launch_bounds__(lv_epb<NP>() * NP * NP * NP, lv_minb<NP, LIFT>()) lift_visc_kernel(KParams P) {
   if (halted(P)) return;
   constexpr int NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1, EPB = lv_epb<NP>(), R = lv_row<NP>();
   extern __shared__ double smem[];
@@ -134,47 +139,54 @@ __global__ void __launch_bounds__(lv_epb<NP>() * NP * NP * NP, 2) lift_visc_kern
 #pragma unroll
         for (int d = 0; d < 3; ++d) g[d][v] = m[0 + d] * dx[v] + m[3 + d] * de[v] + m[6 + d] * dz[v];
     }
-    double gv[3][5];  // BR2: volume part of the gradient, the base of every face trace
-    if constexpr (LIFT == 2) {
-#pragma unroll
-      for (int v = 0; v < 5; ++v)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          g[d][v] *= sj;
-          gv[d][v] = g[d][v];
-        }
-    }
     int sides[3];
     const int ns = boundary_sides(i, j, k, N, sides);
     const double lh = P.basis->LhatM0;
+    if constexpr (LIFT == 2) {
+      // g is the volume part of the gradient, the base of every face trace.  First pass: each side's
+      // trace (volume part + etaBR2 * own-side surface part) and its share n.F_v(U, trace) of the
+      // viscous face flux (riemann.f90:155-168); second pass: the plain surface terms into g.  Two
+      // passes (the face data read twice) keep only one gradient copy live beside the trace.
+#pragma unroll
+      for (int v = 0; v < 5; ++v)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) g[d][v] *= sj;
+#pragma unroll 1
+      for (int z = 0; z < ns; ++z) {
+        const int s = sides[z], side = sE2S[eb][2 * (s - 1)], flip = sE2S[eb][2 * (s - 1) + 1];
+        const int pt = node_side_point(N, s, flip, i, j, k);
+        const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
+        const double* F = P.lflux + (size_t)side * 5 * NPT + pt;
+        const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
+        double tr[3][5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const double fl = sj * lh * F[v * NPT];
+          tr[0][v] = g[0][v] + P.etaBR2 * (fl * n0);
+          tr[1][v] = g[1][v] + P.etaBR2 * (fl * n1);
+          tr[2][v] = g[2][v] + P.etaBR2 * (fl * n2);
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) to_grad_prim(P, u, tr[d]);
+        double kf[4], kg[4], kh[4];
+        diff_flux_3d(P, u, tr[0], tr[1], tr[2], kf, kg, kh);
+        double* T = P.gtrace + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 4 * NPT + pt;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) T[(size_t)v * NPT] = n0 * kf[v] + n1 * kg[v] + n2 * kh[v];
+      }
+    }
     for (int z = 0; z < ns; ++z) {
       const int s = sides[z], side = sE2S[eb][2 * (s - 1)], flip = sE2S[eb][2 * (s - 1) + 1];
       const int pt = node_side_point(N, s, flip, i, j, k);
       const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
       const double* F = P.lflux + (size_t)side * 5 * NPT + pt;
       const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
-      if constexpr (LIFT == 2) {
-        double tr[3][5];
 #pragma unroll
-        for (int v = 0; v < 5; ++v) {
+      for (int v = 0; v < 5; ++v) {
+        if constexpr (LIFT == 2) {  // volume gradient gets the plain surface term
           const double fl = sj * lh * F[v * NPT];
-          const double sx = fl * n0, sy = fl * n1, sz = fl * n2;
-          tr[0][v] = gv[0][v] + P.etaBR2 * sx;
-          tr[1][v] = gv[1][v] + P.etaBR2 * sy;
-          tr[2][v] = gv[2][v] + P.etaBR2 * sz;
-          g[0][v] += sx; g[1][v] += sy; g[2][v] += sz;  // volume gradient gets the plain surface term
-        }
-#pragma unroll
-        for (int d = 0; d < 3; ++d) to_grad_prim(P, u, tr[d]);
-        // this side's share of the viscous face flux: n.F_v(U, trace) (riemann.f90:155-168)
-        double kf[4], kg[4], kh[4];
-        diff_flux_3d(P, u, tr[0], tr[1], tr[2], kf, kg, kh);
-        double* T = P.gtrace + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 4 * NPT + pt;
-#pragma unroll
-        for (int v = 0; v < 4; ++v) T[(size_t)v * NPT] = n0 * kf[v] + n1 * kg[v] + n2 * kh[v];
-      } else {
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
+          g[0][v] += fl * n0; g[1][v] += fl * n1; g[2][v] += fl * n2;
+        } else {
           const double fl = F[v * NPT] * lh;
           g[0][v] += fl * n0; g[1][v] += fl * n1; g[2][v] += fl * n2;
         }

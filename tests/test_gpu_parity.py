@@ -94,6 +94,8 @@ NS_CASES = [
     dict(N=5, lifting=2, lifting_var=3, visc=0, riemann=4, volume_flux=32),
     dict(N=3, lifting=2, lifting_var=1, visc=2, riemann=1, volume_flux=5),
     dict(N=7, lifting=1, lifting_var=3, visc=0, riemann=44, volume_flux=5),
+    dict(N=7, lifting=2, lifting_var=3, visc=0, riemann=44, volume_flux=5),
+    dict(N=6, lifting=2, lifting_var=2, visc=1, riemann=1, volume_flux=5),
 ]
 
 
