@@ -88,53 +88,56 @@ __global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, lv_minb<NP, LIFT>())
 #pragma unroll
       for (int d = 0; d < 3; ++d) g[d][v] = m[0 + d] * gx + m[3 + d] * ge + m[6 + d] * gz;
     }
-    double gv[3][NV];
-    if constexpr (LIFT == 2) {
-#pragma unroll
-      for (int v = 0; v < NV; ++v)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          g[d][v] *= sj;
-          gv[d][v] = g[d][v];
-        }
-    }
     const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
     int sides[3];
     const int ns = boundary_sides(i, j, k, N, sides);
     const double lh = P.basis->LhatM0;
-    for (int z = 0; z < ns; ++z) {
-      const int s = sides[z];
-      const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
-      const int side = es[0], flip = es[1];
-      const int pt = node_side_point(N, s, flip, i, j, k);
-      const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
-      const double* F = P.lflux + (size_t)side * NV * NPT + pt;
-      const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
-      if constexpr (LIFT == 2) {
+    if constexpr (LIFT == 2) {
+      // g is the volume part of the gradient.  First pass: each side's trace (volume part + etaBR2 *
+      // own-side surface part) and its share n.F_v(U, trace) of the viscous / resistive face flux;
+      // second pass: the plain surface terms into g (one gradient copy live beside the trace)
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) g[d][v] *= sj;
+#pragma unroll 1
+      for (int z = 0; z < ns; ++z) {
+        const int s = sides[z];
+        const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
+        const int side = es[0], flip = es[1];
+        const int pt = node_side_point(N, s, flip, i, j, k);
+        const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
+        const double* F = P.lflux + (size_t)side * NV * NPT + pt;
+        const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
         double tr[3][NV];
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
           const double fl = sj * lh * F[v * NPT];
-          const double sx = fl * n0, sy = fl * n1, sz = fl * n2;
-          tr[0][v] = gv[0][v] + P.etaBR2 * sx;
-          tr[1][v] = gv[1][v] + P.etaBR2 * sy;
-          tr[2][v] = gv[2][v] + P.etaBR2 * sz;
-          g[0][v] += sx; g[1][v] += sy; g[2][v] += sz;
+          tr[0][v] = g[0][v] + P.etaBR2 * (fl * n0);
+          tr[1][v] = g[1][v] + P.etaBR2 * (fl * n1);
+          tr[2][v] = g[2][v] + P.etaBR2 * (fl * n2);
         }
 #pragma unroll
         for (int d = 0; d < 3; ++d) to_grad_prim_rt(P, u, tr[d]);
-        // this side's share of the viscous / resistive face flux: n.F_v(U, trace) (7 components)
         double kf[7], kg[7], kh[7];
         visc_flux_3d(P, u, tr[0], tr[1], tr[2], kf, kg, kh);
         double* T = P.gtrace + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 7 * NPT + pt;
 #pragma unroll
         for (int v = 0; v < 7; ++v) T[(size_t)v * NPT] = n0 * kf[v] + n1 * kg[v] + n2 * kh[v];
-      } else {
+      }
+    }
+    for (int z = 0; z < ns; ++z) {
+      const int s = sides[z];
+      const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
+      const int side = es[0];
+      const int pt = node_side_point(N, s, es[1], i, j, k);
+      const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
+      const double* F = P.lflux + (size_t)side * NV * NPT + pt;
+      const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          const double fl = F[v * NPT] * lh;
-          g[0][v] += fl * n0; g[1][v] += fl * n1; g[2][v] += fl * n2;
-        }
+      for (int v = 0; v < NV; ++v) {
+        const double fl = LIFT == 2 ? sj * lh * F[v * NPT] : F[v * NPT] * lh;
+        g[0][v] += fl * n0; g[1][v] += fl * n1; g[2][v] += fl * n2;
       }
     }
     if constexpr (LIFT == 1) {

@@ -76,6 +76,7 @@ PARA = [
     dict(N=3, lifting=2, lifting_var=2, volume_flux=12, riemann=1),
     dict(N=2, lifting=2, lifting_var=3, volume_flux=0, riemann=4),
     dict(N=3, lifting=1, lifting_var=3, volume_flux=10, riemann=5),
+    dict(N=7, lifting=2, lifting_var=3, volume_flux=10, riemann=14),
 ]
 
 
