@@ -68,6 +68,8 @@ class FluxoCfg(ctypes.Structure):
         ("space_prop_sweeps", ctypes.c_int),
         ("time_rel_factor", ctypes.c_double),
         ("indicator_quantity", ctypes.c_int),
+        ("sub_fv_method", ctypes.c_int),
+        ("recons_boundaries", ctypes.c_int),
     ]
 
 

@@ -31,10 +31,7 @@ struct BasisTables {
   double D[FLUXO_NPMAX * FLUXO_NPMAX];     // D(i,l) at [i*NP+l]
   double LhatM0;                           // L_HatMinus(0)
   double wGP[FLUXO_NPMAX];
-  // face point -> volume node for (locSide-1, flip): node index, pt = p + NP*q  (mappings.f90 S2V, l=0)
-  int s2v[6][5][FLUXO_NPMAX * FLUXO_NPMAX];
-  // in-plane volume coordinates (a,b) -> face point for (locSide-1, flip); XI: (j,k), ETA: (i,k), ZETA: (i,j)
-  int v2s[6][5][FLUXO_NPMAX * FLUXO_NPMAX];
+  double xGP[FLUXO_NPMAX];                 // LGL nodes
 };
 
 // Everything a kernel needs, passed by value.
@@ -92,6 +89,7 @@ struct KParams {
   double* fv;             // [elem][var][node] alpha * F_FV of the blended elements
   const double* sVdm;     // nodal -> modal Legendre coefficients [m][i]
   int computeAlpha, indicatorQuantity, propSweeps;
+  int subFV, reconsBoundaries;       // SubFVMethod (1 first order, 2 TVD), ReconsBoundaries (1..3)
   double threshold, sharpness, alphaMax, alphaMin, propFactor, timeRelFactor, shockBlendCoef;
   // batched solves: the elements of many independent instances in one launch; each instance has
   // its own time step (null for a single solve)

@@ -155,21 +155,7 @@ void build_basis_tables(int N, BasisTables& B) {
       B.D[i * NP + l] = b.D[(size_t)i * NP + l];
     }
   B.LhatM0 = b.LhatM0;
-  for (int i = 0; i < NP; ++i) B.wGP[i] = b.w[i];
-  for (int s = 1; s <= 6; ++s)
-    for (int f = 0; f <= 4; ++f)
-      for (int q = 0; q < NP; ++q)
-        for (int p = 0; p < NP; ++p) {
-          int ijk[3];
-          host::side_to_vol(N, 0, p, q, f, s, ijk);
-          const int pt = p + NP * q;
-          B.s2v[s - 1][f][pt] = ijk[0] + NP * (ijk[1] + NP * ijk[2]);
-          int a, bb;
-          if (s == XI_MINUS || s == XI_PLUS) { a = ijk[1]; bb = ijk[2]; }
-          else if (s == ETA_MINUS || s == ETA_PLUS) { a = ijk[0]; bb = ijk[2]; }
-          else { a = ijk[0]; bb = ijk[1]; }
-          B.v2s[s - 1][f][a + NP * bb] = pt;
-        }
+  for (int i = 0; i < NP; ++i) { B.wGP[i] = b.w[i]; B.xGP[i] = b.x[i]; }
 }
 
 KParams base_params(fluxo_handle* h) {
@@ -208,6 +194,7 @@ KParams base_params(fluxo_handle* h) {
     P.alpha = h->dAlpha; P.alphaRaw = h->dAlphaRaw; P.blendList = h->dBlendList; P.blendCount = h->dBlendCount;
     P.fv = h->dFV; P.sVdm = h->dSVdm;
     P.computeAlpha = c.compute_alpha; P.indicatorQuantity = c.indicator_quantity; P.propSweeps = c.space_prop_sweeps;
+    P.subFV = c.sub_fv_method; P.reconsBoundaries = c.recons_boundaries;
     P.threshold = (c.modal_threshold == 2) ? 0.5 * std::pow(10.0, -1.8 * std::pow((double)h->N, 0.25))
                                            : 0.5 * std::pow(10.0, -1.8 * std::pow(h->N + 1., 0.25));
     P.sharpness = std::log((1.0 - 1.e-4) / 1.e-4);
@@ -431,6 +418,10 @@ int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {
     if (cfg->indicator_quantity < 1 || cfg->indicator_quantity > 4)
       return fail(nullptr, FLUXO_EINVAL_CFG, "ShockIndicatorQuantity must be 1..4");
     if (cfg->space_prop_sweeps < 0) return fail(nullptr, FLUXO_EINVAL_CFG, "SpacePropSweeps must be >= 0");
+    if (cfg->sub_fv_method != 1 && cfg->sub_fv_method != 2)
+      return fail(nullptr, FLUXO_EINVAL_CFG, "SubFVMethod must be 1 (first order) or 2 (TVD)");
+    if (cfg->sub_fv_method == 2 && (cfg->recons_boundaries < 1 || cfg->recons_boundaries > 3))
+      return fail(nullptr, FLUXO_EINVAL_CFG, "ReconsBoundaries must be 1..3");
   }
   if (parabolic) {
     if (cfg->lifting != 1 && cfg->lifting != 2) return fail(nullptr, FLUXO_EINVAL_CFG, "lifting must be BR1 or BR2");

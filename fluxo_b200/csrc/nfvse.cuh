@@ -129,9 +129,100 @@ __global__ void list_kernel(KParams P) {
   if (a > kTiny) P.blendList[atomicAdd(P.blendCount, 1)] = e;
 }
 
+// minmod limiter (nfvse.f90:1514-1529)
+__device__ __forceinline__ double minmod(double a, double b) {
+  if (fabs(a) < fabs(b) && a * b > 0.0) return a;
+  if (fabs(b) < fabs(a) && a * b > 0.0) return b;
+  return 0.;
+}
+
+// The TVD reconstruction is evaluated without multiply-add contraction, each operation rounded as in
+// the reference's formula: the limiter's decisions (|a| < |b|, a*b > 0) are discontinuous, and for
+// data continuous across an element face its two slopes tie, so a last-bit difference would select
+// another branch.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+
+// ConsToPrim / PrimToCons of MHD (mhd/equation_vars.f90:229-278), uncontracted
+__device__ __forceinline__ void cons_to_prim_rn(const KParams& P, const double* U, double* Q) {
+  const double s = 1. / U[0];
+  Q[0] = U[0];
+  Q[1] = mul_rn(U[1], s); Q[2] = mul_rn(U[2], s); Q[3] = mul_rn(U[3], s);
+  const double mv = add_rn(add_rn(mul_rn(U[1], Q[1]), mul_rn(U[2], Q[2])), mul_rn(U[3], Q[3]));
+  const double b2 = add_rn(add_rn(add_rn(mul_rn(U[5], U[5]), mul_rn(U[6], U[6])), mul_rn(U[7], U[7])), mul_rn(U[8], U[8]));
+  Q[4] = mul_rn(P.kappaM1, sub_rn(sub_rn(U[4], mul_rn(0.5, mv)), mul_rn(P.s2mu_0, b2)));
+#pragma unroll
+  for (int v = 5; v < 9; ++v) Q[v] = U[v];
+}
+__device__ __forceinline__ void prim_to_cons_rn(const KParams& P, const double* Q, double* U) {
+  U[0] = Q[0];
+  U[1] = mul_rn(Q[1], Q[0]); U[2] = mul_rn(Q[2], Q[0]); U[3] = mul_rn(Q[3], Q[0]);
+  const double mv = add_rn(add_rn(mul_rn(U[1], Q[1]), mul_rn(U[2], Q[2])), mul_rn(U[3], Q[3]));
+  const double b2 = add_rn(add_rn(add_rn(mul_rn(Q[5], Q[5]), mul_rn(Q[6], Q[6])), mul_rn(Q[7], Q[7])), mul_rn(Q[8], Q[8]));
+  U[4] = add_rn(add_rn(mul_rn(P.sKappaM1, Q[4]), mul_rn(0.5, mv)), mul_rn(P.s2mu_0, b2));
+#pragma unroll
+  for (int v = 5; v < 9; ++v) U[v] = Q[v];
+}
+
+// Primitive state of the neighbour element's node that coincides with the boundary node `node` of
+// element e on the minus (plus = false) or plus side of direction dir (Get_externalU: U_slave on a
+// master side, U_master on a slave side, which are the neighbour's boundary nodes for LGL)
+template <int NP>
+__device__ __forceinline__ void ext_prim(const KParams& P, int e, int dir, bool plus, int node, double* pr) {
+  constexpr int N = NP - 1, NP3 = NP * NP * NP;
+  const int s = dir == 0 ? (plus ? XI_PLUS : XI_MINUS) : (dir == 1 ? (plus ? ETA_PLUS : ETA_MINUS)
+                                                                   : (plus ? ZETA_PLUS : ZETA_MINUS));
+  const int i = node % NP, j = (node / NP) % NP, k = node / (NP * NP);
+  const int* es = P.e2s + 2 * (6 * (size_t)e + (s - 1));
+  const int side = es[0], flip = es[1];
+  const int pt = node_side_point(N, s, flip, i, j, k), p = pt % NP, q = pt / NP;
+  const int* se5 = P.s2e + 5 * side;
+  const int nb = flip == 0 ? se5[1] : se5[0];
+  const int nn = flip == 0 ? side_node(N, p, q, se5[4], se5[3]) : side_node(N, p, q, 0, se5[2]);
+  cons_to_prim_rn(P, P.U + mhd::NV * ((size_t)nb * NP3 + nn), pr);
+}
+
+// TVD states of subcell face x of a line (ReconstructSolution_2nd_Order, nfvse.f90:1448-1510):
+// cL = cons(primR(x)), cR = cons(primL(x+1)); pr = the line's primitive records (stride st doubles)
+template <int NP>
+__device__ __forceinline__ void tvd_states(const KParams& P, const double* pr, int st, int x, const double* sdxR,
+                                           const double* sdxL, const double* rL, const double* rR,
+                                           const double* w, const double* extL, const double* extR, double* cL,
+                                           double* cR) {
+  constexpr int N = NP - 1, NV = mhd::NV;
+  const int rb = P.reconsBoundaries;
+  double pl[NV], prr[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    auto Q = [&](int m) { return pr[m * st + v]; };
+    // right face of the subcell of node x
+    if (x == 0) {
+      if (rb == 1) pl[v] = Q(0);
+      else if (rb == 2) pl[v] = add_rn(Q(0), mul_rn(mul_rn(sub_rn(Q(1), Q(0)), sdxL[1]), w[0]));
+      else pl[v] = add_rn(Q(0), mul_rn(minmod(mul_rn(sdxL[1], sub_rn(Q(1), Q(0))), mul_rn(sdxL[1], sub_rn(Q(1), extL[v]))), w[0]));
+    } else {
+      const double sg = minmod(mul_rn(sdxR[x], sub_rn(Q(x + 1), Q(x))), mul_rn(sdxL[x], sub_rn(Q(x), Q(x - 1))));
+      pl[v] = add_rn(Q(x), mul_rn(sg, rR[x]));
+    }
+    // left face of the subcell of node x+1
+    const int y = x + 1;
+    if (y == N) {
+      if (rb == 1) prr[v] = Q(N);
+      else if (rb == 2) prr[v] = sub_rn(Q(N), mul_rn(mul_rn(sub_rn(Q(N), Q(N - 1)), sdxL[1]), w[N]));
+      else prr[v] = sub_rn(Q(N), mul_rn(minmod(mul_rn(sdxL[1], sub_rn(Q(N), Q(N - 1))), mul_rn(sdxL[1], sub_rn(extR[v], Q(N - 1)))), w[0]));
+    } else {
+      const double sg = minmod(mul_rn(sdxR[y], sub_rn(Q(y + 1), Q(y))), mul_rn(sdxL[y], sub_rn(Q(y), Q(y - 1))));
+      prr[v] = add_rn(Q(y), mul_rn(sg, rL[y]));
+    }
+  }
+  prim_to_cons_rn(P, pl, cL);
+  prim_to_cons_rn(P, prr, cR);
+}
+
 template <int NP>
 __host__ __device__ constexpr size_t fv_smem_bytes() {
-  return sizeof(double) * (size_t)(NP * NP + 2 * NP + 27 * NP * NP * NP);
+  return sizeof(double) * (size_t)(NP * NP + 6 * NP + 36 * NP * NP * NP);
 }
 
 // First-order subcell FV volume integral (Compute_FVFluxes_1st_Order nfvse.f90:566-673,
@@ -150,9 +241,27 @@ __global__ void __launch_bounds__(NP * NP * NP) fv_kernel_mhd(KParams P) {
   double* sU = sIW + NP;      // [node][9] state
   double* sM = sU + 9 * NP3;  // [9][node] metrics
   double* sA = sM + 9 * NP3;  // [node][9] left-face flux handed over by the left neighbour
+  double* sPr = sA + 9 * NP3;  // [node][9] primitive variables (TVD reconstruction)
+  // TVD: node spacings and sub-cell offsets of InitNFVSE (nfvse.f90:218-238), index 1..N-1
+  double* sdxR = sPr + 9 * NP3;
+  double* sdxL = sdxR + NP;
+  double* rL = sdxL + NP;
+  double* rR = rL + NP;
   const int t = threadIdx.x;
   for (int z = t; z < NPT; z += blockDim.x) sD[z] = P.basis->D[z];
   if (t < NP) { sW[t] = P.basis->wGP[t]; sIW[t] = 1.0 / P.basis->wGP[t]; }
+  if (t == 0) {
+    const double* x = P.basis->xGP;
+    double sumWm1 = P.basis->wGP[0] - 1.;
+    for (int m = 1; m <= N - 1; ++m) {
+      sdxR[m] = 1.0 / (x[m + 1] - x[m]);
+      sdxL[m] = 1.0 / (x[m] - x[m - 1]);
+      rL[m] = sumWm1 - x[m];
+      sumWm1 = sumWm1 + P.basis->wGP[m];
+      rR[m] = sumWm1 - x[m];
+    }
+  }
+  const bool tvd = P.subFV == 2;
   const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
   const double ch = glm_ch(P);
   const int count = *P.blendCount;
@@ -166,6 +275,7 @@ __global__ void __launch_bounds__(NP * NP * NP) fv_kernel_mhd(KParams P) {
       const double* Mg = P.metrics + (size_t)e * 9 * NP3 + t;
 #pragma unroll
       for (int c = 0; c < 9; ++c) sM[c * NP3 + t] = Mg[c * NP3];
+      if (tvd) cons_to_prim_rn(P, sU + NV * t, sPr + NV * t);
     }
     __syncthreads();
     double ffv[NV];
@@ -205,17 +315,31 @@ __global__ void __launch_bounds__(NP * NP * NP) fv_kernel_mhd(KParams P) {
                               nv[0] * t1[1] - nv[1] * t1[0]};
         const double* uL = sU + NV * t;
         const double* uR = sU + NV * (t + stride);
+        // states of the subcell Riemann problem: the nodal values (first order) or the TVD
+        // reconstruction primR(x), primL(x+1) of the line (Compute_FVFluxes_TVD nfvse.f90:674-815)
+        double cL[NV], cR[NV];
+        if (tvd) {
+          double extL[NV], extR[NV];
+          if (P.reconsBoundaries == 3) {  // Get_externalU (nfvse.f90:1621-1683): the neighbours' nodes
+            if (x == 0) ext_prim<NP>(P, e, dir, false, t, extL);
+            if (x + 1 == N) ext_prim<NP>(P, e, dir, true, t + stride, extR);
+          }
+          tvd_states<NP>(P, sPr + NV * (t - x * stride), NV * stride, x, sdxR, sdxL, rL, rR, sW, extL, extR, cL, cR);
+        } else {
+#pragma unroll
+          for (int v = 0; v < NV; ++v) { cL[v] = uL[v]; cR[v] = uR[v]; }
+        }
         double L[NV], R[NV], F[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) { L[v] = uL[v]; R[v] = uR[v]; }
+        for (int v = 0; v < NV; ++v) { L[v] = cL[v]; R[v] = cR[v]; }
 #pragma unroll
         for (int b = 1; b <= 5; b += 4) {  // RotateState, mhd/riemann.f90:185-200
-          L[b] = uL[b] * nv[0] + uL[b + 1] * nv[1] + uL[b + 2] * nv[2];
-          L[b + 1] = uL[b] * t1[0] + uL[b + 1] * t1[1] + uL[b + 2] * t1[2];
-          L[b + 2] = uL[b] * t2[0] + uL[b + 1] * t2[1] + uL[b + 2] * t2[2];
-          R[b] = uR[b] * nv[0] + uR[b + 1] * nv[1] + uR[b + 2] * nv[2];
-          R[b + 1] = uR[b] * t1[0] + uR[b + 1] * t1[1] + uR[b + 2] * t1[2];
-          R[b + 2] = uR[b] * t2[0] + uR[b + 1] * t2[1] + uR[b + 2] * t2[2];
+          L[b] = cL[b] * nv[0] + cL[b + 1] * nv[1] + cL[b + 2] * nv[2];
+          L[b + 1] = cL[b] * t1[0] + cL[b + 1] * t1[1] + cL[b + 2] * t1[2];
+          L[b + 2] = cL[b] * t2[0] + cL[b + 1] * t2[1] + cL[b + 2] * t2[2];
+          R[b] = cR[b] * nv[0] + cR[b + 1] * nv[1] + cR[b + 2] * nv[2];
+          R[b + 1] = cR[b] * t1[0] + cR[b + 1] * t1[1] + cR[b + 2] * t1[2];
+          R[b + 2] = cR[b] * t2[0] + cR[b + 1] * t2[1] + cR[b + 2] * t2[2];
         }
         mhd::riemann<RS>(P, ch, L, R, F);
 #pragma unroll

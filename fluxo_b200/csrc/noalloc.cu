@@ -35,7 +35,7 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 constexpr size_t kTablesBytes = (sizeof(BasisTables) + 255) / 256 * 256;  // face fluxes start 256-aligned
-static_assert(kTablesBytes == 21504, "the scratch size formula in fluxo_gpu.h states 21504 bytes of tables");
+static_assert(kTablesBytes == 2304, "the scratch size formula in fluxo_gpu.h states 2304 bytes of tables");
 
 std::mutex g_mutex;
 void* g_scratch[kMaxDevices];       // device address of g_noalloc_scratch, looked up once per device

@@ -74,7 +74,7 @@ typedef struct fluxo_cfg {
   int noncons;       /* NONCONS: 0 off, 1 Powell, 2 Brackbill, 3 Janhunen (CMake FLUXO_EQN_NONCONS_TYPE) */
   int nc_glm;        /* PP_NC_GLM: non-conservative GLM terms (CMake FLUXO_EQN_NONCONS_GLM) */
   /* NFVSE shock capturing (CMake FLUXO_SHOCKCAP_NFVSE; src/shockcapturing/nfvse.f90:63-260), MHD,
-   * N >= 2, SubFVMethod = 1 (first-order subcell finite volumes). */
+   * N >= 2, SubFVMethod = 1 (first-order subcell finite volumes) or 2 (TVD). */
   int nfvse;               /* 0 off, 1 on */
   int compute_alpha;       /* ComputeAlpha: 1 Persson-Peraire indicator, 3 fixed ShockBlendCoef */
   double shock_blend_coef; /* ShockBlendCoef */
@@ -84,6 +84,9 @@ typedef struct fluxo_cfg {
   double time_rel_factor;  /* TimeRelFactor */
   int indicator_quantity;  /* ShockIndicatorQuantity: 1 Density, 2 Pressure, 3 DensityTimesPressure,
                               4 KinPlusMagEnergy */
+  int sub_fv_method;       /* SubFVMethod: 1 first-order subcell FV, 2 TVD (minmod reconstruction of the
+                              primitive variables, nfvse.f90:674-815, 1448-1529) */
+  int recons_boundaries;   /* ReconsBoundaries (SubFVMethod 2): 1 none, 2 central, 3 neighbour element */
 } fluxo_cfg;
 
 typedef struct fluxo_handle fluxo_handle;
@@ -185,7 +188,7 @@ int fluxo_gpu_fp64_peak(int device, double* tflops);
  *   dS2E [side][5]: SideToElem with 0-based element ids;  dE2S [elem][6][2]: 0-based side id, flip.
  * The face fluxes and operator tables live in one static device array of
  * FLUXO_NOALLOC_SCRATCH_BYTES shared by all calls on a device: it needs
- * 21504 + nSides*5*(N+1)^2*8 bytes (N=7: about 3270 sides; N=3: about 13070 sides), larger
+ * 2304 + nSides*5*(N+1)^2*8 bytes (N=7: about 3270 sides; N=3: about 13100 sides), larger
  * meshes return FLUXO_EINVAL_CFG.  Calls whose GPU work overlaps (other streams or host threads)
  * race on that array; the call runs on `stream` (NULL: the legacy default stream) and
  * synchronises it before returning.  Errors: fluxo_gpu_last_error(NULL, ...). */

@@ -48,7 +48,7 @@ typedef struct orc_params {
   double mhd_ref_state[2][8];  /* RefState 1 and 2 (rho,u,v,w,p,B1,B2,B3) */
   double ini_center[3];   /* IniCenter */
   double ini_halfwidth;   /* IniHalfwidth */
-  /* NFVSE shock capturing (shockcapturing/nfvse.f90:63-260), SubFVMethod = 1 */
+  /* NFVSE shock capturing (shockcapturing/nfvse.f90:63-260), SubFVMethod = 1, 2 */
   int nfvse;              /* SHOCK_NFVSE on/off */
   int compute_alpha;      /* ComputeAlpha: 1 Persson-Peraire indicator, 3 fixed ShockBlendCoef */
   double shock_blend_coef;
@@ -57,6 +57,8 @@ typedef struct orc_params {
   int space_prop_sweeps;
   double time_rel_factor;
   int indicator_quantity; /* ShockIndicatorQuantity: 1 Density, 2 Pressure, 3 DensityTimesPressure, 4 KinEnergy */
+  int sub_fv_method;      /* SubFVMethod: 1 first order, 2 TVD (minmod reconstruction of primitive variables) */
+  int recons_boundaries;  /* ReconsBoundaries (SubFVMethod 2): 1 none, 2 central, 3 neighbour element */
 } orc_params;
 
 void* orc_create(const orc_params* p);

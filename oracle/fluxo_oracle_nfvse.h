@@ -156,8 +156,82 @@ void SubcellRiemann(const Case& C, int npts, const real* UL, const real* UR, con
     }
 }
 
-// VolInt_NFVSE (nfvse.f90:475-565) with Compute_FVFluxes_1st_Order (:566-673) and
-// Compute_FVFluxes_1D (:1389-1447): Ut = (1-alpha) Ut + alpha F_FV on the blended elements
+inline void FV_ConsToPrim(const Case& C, const real* U, real* P) {
+  if (C.mhd) MHD_ConsToPrim(C, U, P);
+  else ConsToPrim(C, U, P);
+}
+inline void FV_PrimToCons(const Case& C, const real* P, real* U) {  // PrimToConsVec (both systems)
+  if (C.mhd) { MHD_PrimToCons(C, P, U); return; }
+  U[0] = P[0];
+  U[1] = P[1] * P[0]; U[2] = P[2] * P[0]; U[3] = P[3] * P[0];
+  U[4] = C.sKappaM1 * P[4] + 0.5 * (U[1] * P[1] + U[2] * P[2] + U[3] * P[3]);
+}
+// minmod limiter, nfvse.f90:1514-1529
+inline real MinMod(real a, real b) {
+  if (fabs(a) < fabs(b) && a * b > 0.0) return a;
+  if (fabs(b) < fabs(a) && a * b > 0.0) return b;
+  return real(0.);
+}
+
+// Second-order (TVD) reconstruction along one line, ReconstructSolution_2nd_Order nfvse.f90:1448-1510
+// with the node spacings and sub-cell offsets of InitNFVSE :218-238.  pr[x*NV+v]: primitive variables
+// of the line; ext[0|1]: the neighbour elements' boundary states beyond node 0 / node N (ReconsBoundaries
+// 3); outputs primR (right face of the subcell of node x, x = 0..N-1) and primL (left face, x = 1..N).
+void ReconstructLine(const Case& C, const real* pr, const real* extL, const real* extR, real* pR, real* pL) {
+  const int N = C.N, NV = C.nVar;
+  std::vector<double> sdxR(N), sdxL(N), rL(N), rR(N);
+  double sumWm1 = C.wGP[0] - 1.;
+  for (int i = 1; i <= N - 1; ++i) {
+    sdxR[i] = 1.0 / (C.xGP[i + 1] - C.xGP[i]);
+    sdxL[i] = 1.0 / (C.xGP[i] - C.xGP[i - 1]);
+    rL[i] = sumWm1 - C.xGP[i];
+    sumWm1 = sumWm1 + C.wGP[i];
+    rR[i] = sumWm1 - C.xGP[i];
+  }
+  const int rb = C.P.recons_boundaries;
+  for (int v = 0; v < NV; ++v) {
+    auto P = [&](int i) { return pr[i * NV + v]; };
+    // first node
+    if (rb == 1) pR[v] = P(0);
+    else if (rb == 2) pR[v] = P(0) + (P(1) - P(0)) * sdxL[1] * C.wGP[0];
+    else pR[v] = P(0) + MinMod(sdxL[1] * (P(1) - P(0)), sdxL[1] * (P(1) - extL[v])) * C.wGP[0];
+    for (int i = 1; i <= N - 1; ++i) {
+      real sigma = MinMod(sdxR[i] * (P(i + 1) - P(i)), sdxL[i] * (P(i) - P(i - 1)));
+      pR[i * NV + v] = P(i) + sigma * rR[i];
+      pL[i * NV + v] = P(i) + sigma * rL[i];
+    }
+    // last node
+    if (rb == 1) pL[N * NV + v] = P(N);
+    else if (rb == 2) pL[N * NV + v] = P(N) - (P(N) - P(N - 1)) * sdxL[1] * C.wGP[N];
+    else pL[N * NV + v] = P(N) - MinMod(sdxL[1] * (P(N) - P(N - 1)), sdxL[1] * (extR[v] - P(N - 1))) * C.wGP[0];
+  }
+}
+
+// External state of ReconsBoundaries 3 (Get_externalU, nfvse.f90:1621-1683): at the boundary node of
+// local side s of element e, the neighbour's face state (U_slave on a master side, U_master on a
+// slave side); returned as primitive variables at [(a + n*b)*NV], (a,b) the tangential node indexes
+void ExternalPrim(const Case& C, int e, int s, std::vector<real>& ext) {
+  const int n = C.np, N = C.N, NV = C.nVar;
+  ext.assign((size_t)n * n * NV, real(0.));
+  const int sideID = C.ElemToSide[2 * (6 * e + (s - 1))] - 1;
+  const int flipE = C.ElemToSide[2 * (6 * e + (s - 1)) + 1];
+  const bool master = flipE == 0;  // master sides have flip 0
+  static const int tan1[6] = {0, 0, 1, 0, 1, 0}, tan2[6] = {1, 2, 2, 2, 2, 1};  // TanDirs1/2 - 1
+  for (int q = 0; q <= N; ++q)
+    for (int p = 0; p <= N; ++p) {
+      int ijk[3];
+      SideToVol(N, 0, p, q, master ? 0 : flipE, s, ijk);
+      const real* Uf = master ? &C.Uslave[C.fac(0, p, q, sideID)] : &C.Umaster[C.fac(0, p, q, sideID)];
+      real pr[NVMAX];
+      FV_ConsToPrim(C, Uf, pr);
+      const int a = ijk[tan1[s - 1]], b = ijk[tan2[s - 1]];
+      for (int v = 0; v < NV; ++v) ext[(a + n * b) * NV + v] = pr[v];
+    }
+}
+
+// VolInt_NFVSE (nfvse.f90:475-565) with Compute_FVFluxes_1st_Order (:566-673) or
+// Compute_FVFluxes_TVD (:674-815) and Compute_FVFluxes_1D (:1389-1447): Ut = (1-alpha) Ut + alpha F_FV
+// on the blended elements
 void VolIntNFVSE(Case& C) {
   const int n = C.np, N = C.N, NV = C.nVar, npt = n * n;
   if (C.P.space_prop_sweeps > 0) {
@@ -175,6 +249,12 @@ void VolIntNFVSE(Case& C) {
   // per direction: left flux FL(x) and right flux FR(x) of subcell face x = -1..N at (a,b)
   std::vector<real> FL((size_t)3 * (n + 1) * npt * NV), FR((size_t)3 * (n + 1) * npt * NV);
   std::vector<real> UL((size_t)npt * NV), UR((size_t)npt * NV), F((size_t)npt * NV), G((size_t)npt * NV);
+  // TVD: reconstructed face states of the Riemann problems, per direction and line
+  const bool tvd = C.P.sub_fv_method == 2;
+  std::vector<real> RL((size_t)npt * NV), RR((size_t)npt * NV), pr((size_t)n * NV), pRl((size_t)n * NV),
+      pLl((size_t)n * NV), recR((size_t)3 * n * npt * NV), recL((size_t)3 * n * npt * NV);
+  std::vector<real> extL, extR;
+  static const int sideMinus[3] = {XI_MINUS, ETA_MINUS, ZETA_MINUS}, sidePlus[3] = {XI_PLUS, ETA_PLUS, ZETA_PLUS};
   std::vector<double> nvb(3 * npt), t1b(3 * npt), t2b(3 * npt);
   auto fi = [&](int d, int x, int p) { return ((size_t)(d * (n + 1) + (x + 1)) * npt + p) * NV; };
   for (int e = 0; e < C.nElems; ++e) {
@@ -187,6 +267,23 @@ void VolIntNFVSE(Case& C) {
         if (d == 1) return C.nod(a, x, b, e);
         return C.nod(a, b, x, e);
       };
+      if (tvd) {  // reconstruct every line of this direction: recR/recL[(x*npt + p)*NV + v]
+        if (C.P.recons_boundaries == 3) {
+          ExternalPrim(C, e, sideMinus[d], extL);
+          ExternalPrim(C, e, sidePlus[d], extR);
+        }
+        for (int b = 0; b < n; ++b)
+          for (int a = 0; a < n; ++a) {
+            for (int x = 0; x <= N; ++x) FV_ConsToPrim(C, &C.U[NV * node(x, a, b)], &pr[x * NV]);
+            const real* eL = C.P.recons_boundaries == 3 ? &extL[(a + n * b) * NV] : nullptr;
+            const real* eR = C.P.recons_boundaries == 3 ? &extR[(a + n * b) * NV] : nullptr;
+            ReconstructLine(C, pr.data(), eL, eR, pRl.data(), pLl.data());
+            for (int x = 0; x <= N; ++x) {
+              FV_PrimToCons(C, &pRl[x * NV], &recR[((size_t)x * npt + a + n * b) * NV]);
+              FV_PrimToCons(C, &pLl[x * NV], &recL[((size_t)x * npt + a + n * b) * NV]);
+            }
+          }
+      }
       for (int x = 0; x < N; ++x) {
         for (int b = 0; b < n; ++b)
           for (int a = 0; a < n; ++a) {
@@ -200,7 +297,15 @@ void VolIntNFVSE(Case& C) {
               nvb[3 * p + c] = C.scNv[3 * s + c]; t1b[3 * p + c] = C.scT1[3 * s + c]; t2b[3 * p + c] = C.scT2[3 * s + c];
             }
           }
-        SubcellRiemann(C, npt, UL.data(), UR.data(), nvb.data(), t1b.data(), t2b.data(), F.data());
+        if (tvd) {
+          for (int z = 0; z < npt * NV; ++z) {
+            RL[z] = recR[(size_t)x * npt * NV + z];
+            RR[z] = recL[(size_t)(x + 1) * npt * NV + z];
+          }
+          SubcellRiemann(C, npt, RL.data(), RR.data(), nvb.data(), t1b.data(), t2b.data(), F.data());
+        } else {
+          SubcellRiemann(C, npt, UL.data(), UR.data(), nvb.data(), t1b.data(), t2b.data(), F.data());
+        }
         for (size_t z = 0; z < F.size(); ++z) G[z] = F[z];  // FR_ = F_ before the non-conservative terms
         if (C.mhd && C.noncons) {
           for (int p = 0; p < npt; ++p) {

@@ -68,6 +68,8 @@ class OrcParams(ctypes.Structure):
         ("space_prop_sweeps", ctypes.c_int),
         ("time_rel_factor", ctypes.c_double),
         ("indicator_quantity", ctypes.c_int),
+        ("sub_fv_method", ctypes.c_int),
+        ("recons_boundaries", ctypes.c_int),
     ]
 
 
@@ -83,6 +85,7 @@ DEFAULTS = dict(
     ini_center=(0.0, 0.0, 0.0), ini_halfwidth=0.1,
     nfvse=0, compute_alpha=1, shock_blend_coef=0.0, modal_threshold=1, alpha_max=0.5, alpha_min=0.01,
     space_prop_factor=0.5, space_prop_sweeps=1, time_rel_factor=0.0, indicator_quantity=3,
+    sub_fv_method=1, recons_boundaries=1,
 )
 
 

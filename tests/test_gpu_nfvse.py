@@ -12,7 +12,8 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-12
 REF = ((1.2, 0.1, 0.0, 0.1, 0.9, 1.0, 1.0, 1.0), (1.1, 0.2, -0.1, 0.2, 0.6, 1.0, 1.0, 1.0))
 NFVSE_KEYS = ("nfvse", "compute_alpha", "shock_blend_coef", "modal_threshold", "alpha_max", "alpha_min",
-              "space_prop_factor", "space_prop_sweeps", "time_rel_factor", "indicator_quantity")
+              "space_prop_factor", "space_prop_sweeps", "time_rel_factor", "indicator_quantity", "sub_fv_method",
+              "recons_boundaries")
 
 
 def rel_l2(a, b):
@@ -131,3 +132,30 @@ def test_nfvse_time_disc_parity(gpu_lib):
     assert err == 0 and n == n_ref == 6
     assert t == pytest.approx(t_ref, rel=1e-12)
     assert rel_l2(op.get_state(), c.get_U()) <= 1e-11
+
+
+@pytest.mark.parametrize("rb,N,rs,tol", [(1, 3, 14, TOL), (2, 4, 10, TOL), (3, 3, 10, TOL), (3, 5, 1, TOL),
+                                         (2, 2, 4, TOL), (3, 3, 14, 1e-10)])
+def test_nfvse_tvd_parity(gpu_lib, rb, N, rs, tol):
+    """SubFVMethod 2: minmod-reconstructed primitive states at the subcell faces, all three boundary
+    reconstructions (3: the neighbour elements' nodes), fixed blending and the indicator.  With the
+    9-wave entropy-stable solver (Riemann 14) the reference algorithm itself moves by 4e-11 in Ut
+    between two legal roundings of the same formulas (the oracle built with and without multiply-add
+    contraction: 1.2e-11 for ReconsBoundaries 1, 3.8e-11 for 3), so that case is held to 1e-10."""
+    for ca in (3, 1):
+        c, op = nfvse_pair(N=N, riemann=rs, compute_alpha=ca, shock_blend_coef=0.4, sub_fv_method=2,
+                           recons_boundaries=rb, noise=0.05)
+        ref = c.dg_time_derivative(0.0)
+        op.dg_time_derivative(0.0)
+        assert np.abs(op.alpha() - c.alpha()).max() <= 1e-12
+        assert rel_l2(op.get_ut(), ref) <= tol
+
+
+def test_nfvse_tvd_continuous_data_ties(gpu_lib):
+    """Data continuous across element faces makes the two boundary slopes of ReconsBoundaries 3 tie
+    exactly; the uncontracted reconstruction takes the same limiter branch as the oracle."""
+    c, op = nfvse_pair(N=3, riemann=14, compute_alpha=3, shock_blend_coef=0.4, sub_fv_method=2,
+                       recons_boundaries=3, noise=0.0)
+    ref = c.dg_time_derivative(0.0)
+    op.dg_time_derivative(0.0)
+    assert rel_l2(op.get_ut(), ref) <= TOL

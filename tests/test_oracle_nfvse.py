@@ -83,3 +83,39 @@ def test_persson_peraire_indicator_and_propagation():
     for e in range(cp.nElems):
         nbs = {int(x) for s in e2s[e] for x in s2e[s] if x != e}
         assert a1[e] >= 0.5 * max(a0[n] for n in nbs) - 1e-15
+
+
+TVD = dict(FIXED, sub_fv_method=2)
+
+
+@pytest.mark.parametrize("rb", [1, 2, 3])
+def test_nfvse_tvd_freestream(rb):
+    """SubFVMethod 2 (minmod reconstruction of the primitive variables) keeps a constant state."""
+    c = OracleCase(ini_exact_func=1, volume_flux=10, riemann=14, recons_boundaries=rb, **WARPED, **MHD, **TVD)
+    assert np.abs(c.dg_time_derivative(0.0)).max() <= 1e-11
+    c = OracleCase(eqn=0, ini_exact_func=1, volume_flux=5, riemann=1, ref_state=(1.1, 0.3, -0.2, 0.1, 0.8),
+                   recons_boundaries=rb, **WARPED, **TVD)
+    assert np.abs(c.dg_time_derivative(0.0)).max() <= 1e-11
+
+
+def test_nfvse_tvd_is_conservative_and_differs_from_first_order():
+    """The blended scheme with the TVD subcell fluxes conserves mass, momentum and energy on a periodic
+    mesh (sum of w J Ut = 0), and each reconstruction at the element boundaries gives another Ut."""
+    from oracle.oracle import basis
+    out = []
+    for kw in (dict(FIXED), dict(TVD, recons_boundaries=1), dict(TVD, recons_boundaries=2),
+               dict(TVD, recons_boundaries=3)):
+        c = OracleCase(eqn=0, ini_exact_func=2, ini_amplitude=0.3, volume_flux=5, riemann=1,
+                       adv_vel=(0.3, -0.2, 0.5), **WARPED, **kw)
+        U = c.get_U()
+        c.set_U(U * (1 + 0.05 * np.random.default_rng(5).standard_normal(U.shape)))
+        Ut = c.dg_time_derivative(0.0)
+        w = basis(3)["wGP"]
+        W = w[None, None, None, :] * w[None, None, :, None] * w[None, :, None, None]
+        sJ = c.mesh()["sJ"].reshape(Ut.shape[:4])
+        total = np.einsum("ekji,ekjiv->v", W / sJ, Ut)
+        assert np.abs(total).max() <= 1e-12 * np.abs(Ut).max()
+        out.append(Ut)
+    for a in range(4):
+        for b in range(a + 1, 4):
+            assert np.abs(out[a] - out[b]).max() > 1e-6

@@ -60,7 +60,7 @@ def test_noalloc_rejects_oversized_mesh():
     c = OracleCase(**CASE)
     cfg = cfg_for(c.params)
     fake = ctypes.c_void_p(0x1000)  # never dereferenced: the call returns before touching memory
-    too_many = (_lib.NOALLOC_SCRATCH_BYTES - 21504) // (5 * 16 * 8) + 1
+    too_many = (_lib.NOALLOC_SCRATCH_BYTES - 2304) // (5 * 16 * 8) + 1
     r = lib.fluxo_gpu_dg_time_derivative_noalloc(ctypes.byref(cfg), 10, too_many, *([fake] * 7), None)
     assert r == -1
     msg = last_error(lib)
