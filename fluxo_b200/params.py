@@ -22,7 +22,7 @@ KEYS = {
     "parabolic": ("s", "T"),
     "riemann": ("i", 1),
     "volumeflux": ("i", 0),
-    "kappa": ("r", 1.4),
+    "kappa": ("r", None),  # 1.4 (Navier-Stokes), 5/3 (MHD)
     "r": ("r", 287.058),
     "pr": ("r", 0.72),
     "mu0": ("r", 0.0),
@@ -40,6 +40,33 @@ KEYS = {
     "iniwavenumber": ("ra", (1.0, 1.0, 1.0)),
     "inifrequency": ("r", 1.0),
     "refstate": ("ra", (1.0, 0.0, 0.0, 0.0, 0.71428571)),
+    # MHD with GLM (mhd/equation.f90:65-135); the equation system, NONCONS and NC_GLM are build
+    # options of the reference (CMake FLUXO_EQNSYSNAME, FLUXO_EQN_NONCONS_TYPE, FLUXO_EQN_NONCONS_GLM)
+    # and keys here
+    "inirefstate": ("i", 1),
+    "inicenter": ("ra", (0.0, 0.0, 0.0)),
+    "inihalfwidth": ("r", 0.1),
+    "mu_0": ("r", 1.0),
+    "eta": ("r", 0.0),
+    "mu": ("r", 0.0),
+    "glm_scale": ("r", 0.5),
+    "glm_scr": ("r", 0.0),
+    "noncons": ("i", 1),
+    "nc_glm": ("s", "F"),
+    # NFVSE shock capturing (shockcapturing.f90:55-75, nfvse.f90:63-102); "nfvse" stands for the
+    # reference's build option FLUXO_SHOCKCAP_NFVSE
+    "nfvse": ("s", "F"),
+    "computealpha": ("i", 1),
+    "shockblendcoef": ("r", 0.0),
+    "modalthreshold": ("i", 1),
+    "alpha_max": ("r", 0.5),
+    "alpha_min": ("r", 0.01),
+    "spacepropfactor": ("r", 0.5),
+    "spacepropsweeps": ("i", 1),
+    "timerelfactor": ("r", 0.0),
+    "shockindicatorquantity": ("s", "DensityTimesPressure"),
+    "subfvmethod": ("i", 1),
+    "reconsboundaries": ("i", 1),
     # time discretisation (timedisc.f90:53-70)
     "timediscmethod": ("s", "carpenterrk4-5"),
     "tend": ("r", None),
@@ -50,6 +77,7 @@ KEYS = {
 }
 
 _TIMEDISC = {"carpenterrk4-5": 0, "standardrk3-3": 1}
+_INDICATOR = {"density": 1, "pressure": 2, "densitytimespressure": 3, "kinplusmagenergy": 4}
 _LIFTVAR = {"cons_var": 1, "prim_var": 2, "entropy_var": 3}
 _VISC = {"constant": 0, "sutherland": 1, "powerlaw": 2}
 
@@ -89,6 +117,8 @@ def parse_ini(text):
             out[k] = _parse_value(KEYS[k][0], v)
         else:
             out[k] = v.strip()
+        if k == "refstate":  # a repeated option: IniRefState selects one (equation.f90 RefStatePrim)
+            out.setdefault("refstates", []).append(out[k])
     return out
 
 
@@ -105,21 +135,30 @@ def resolve(opts):
             raise KeyError("parameter.ini: mandatory option '%s' missing" % k)
         else:
             res[k] = dflt
+    mhd = str(res["equation"]).strip().lower() == "mhd"
+    if res["kappa"] is None:
+        res["kappa"] = 5.0 / 3.0 if mhd else 1.4
+    res["refstates"] = opts.get("refstates", [res["refstate"]])
     return res
+
+
+def _flag(v):
+    return str(v).strip().lower() in ("t", ".true.", "true", "1")
 
 
 def to_cfg_fields(res):
     """Maps resolved options onto the fields of ``fluxo_cfg``."""
-    parabolic = str(res["parabolic"]).strip().lower() in ("t", ".true.", "true", "1")
-    if str(res["equation"]).strip().lower() != "navierstokes":
-        raise ValueError("only the navierstokes equation system is implemented")
+    parabolic = _flag(res["parabolic"])
+    eqsys = str(res["equation"]).strip().lower()
+    if eqsys not in ("navierstokes", "mhd"):
+        raise ValueError("equation system %r not implemented (navierstokes, mhd)" % res["equation"])
     lifting = str(res["lifting"]).strip().lower()
     if lifting not in ("br1", "br2"):
         raise ValueError("lifting must be br1 or br2")
     tdm = str(res["timediscmethod"]).replace(" ", "").lower()
     if tdm not in _TIMEDISC:
         raise ValueError("TimeDiscMethod %r not implemented" % res["timediscmethod"])
-    return dict(
+    f = dict(
         N=res["n"], eqn=1 if parabolic else 0, riemann=res["riemann"], volume_flux=res["volumeflux"],
         lifting=1 if lifting == "br1" else 2, lifting_var=_LIFTVAR[str(res["liftingvar"]).lower()],
         visc=_VISC[str(res["viscosity"]).lower()], kappa=res["kappa"], R=res["r"], Pr=res["pr"], mu0=res["mu0"],
@@ -127,3 +166,16 @@ def to_cfg_fields(res):
         time_disc=_TIMEDISC[tdm], cfl_scale=res["cflscale"], dfl_scale=res["dflscale"],
         ini_exact_func=res["iniexactfunc"], ini_frequency=res["inifrequency"], ini_amplitude=res["iniamplitude"],
     )
+    if eqsys == "mhd":
+        ind = str(res["shockindicatorquantity"]).strip().lower()
+        if ind not in _INDICATOR:
+            raise ValueError("ShockIndicatorQuantity %r not implemented" % res["shockindicatorquantity"])
+        f.update(eqn=3 if parabolic else 2, mu0=res["mu"], mu_0=res["mu_0"], eta=res["eta"],
+                 glm_scale=res["glm_scale"], glm_scr=res["glm_scr"], noncons=res["noncons"],
+                 nc_glm=1 if _flag(res["nc_glm"]) else 0, nfvse=1 if _flag(res["nfvse"]) else 0,
+                 compute_alpha=res["computealpha"], shock_blend_coef=res["shockblendcoef"],
+                 modal_threshold=res["modalthreshold"], alpha_max=res["alpha_max"], alpha_min=res["alpha_min"],
+                 space_prop_factor=res["spacepropfactor"], space_prop_sweeps=res["spacepropsweeps"],
+                 time_rel_factor=res["timerelfactor"], indicator_quantity=_INDICATOR[ind],
+                 sub_fv_method=res["subfvmethod"], recons_boundaries=res["reconsboundaries"])
+    return f

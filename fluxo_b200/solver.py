@@ -204,9 +204,16 @@ class Fluxo:
         self.op = DGOperator(**fields)
         self.op.set_mesh(self.mesh)
         # InitDG: FillIni(IniExactFunc, U)
-        self.U0 = exact_func(o["iniexactfunc"], 0.0, self.mesh["Elem_xGP"], kappa=o["kappa"], adv_vel=o["advvel"],
-                             amplitude=o["iniamplitude"], wavenumber=o["iniwavenumber"], frequency=o["inifrequency"],
-                             ref_state=o["refstate"])
+        if fields["eqn"] in (2, 3):
+            from .workloads import mhd_exact_func
+            self.U0 = mhd_exact_func(o["iniexactfunc"], 0.0, self.mesh["Elem_xGP"], kappa=o["kappa"],
+                                     mu_0=o["mu_0"], ref_states=o["refstates"], ini_ref_state=o["inirefstate"],
+                                     center=o["inicenter"], halfwidth=o["inihalfwidth"],
+                                     amplitude=o["iniamplitude"], frequency=o["inifrequency"])
+        else:
+            self.U0 = exact_func(o["iniexactfunc"], 0.0, self.mesh["Elem_xGP"], kappa=o["kappa"],
+                                 adv_vel=o["advvel"], amplitude=o["iniamplitude"], wavenumber=o["iniwavenumber"],
+                                 frequency=o["inifrequency"], ref_state=o["refstate"])
         self.op.set_state(self.U0)
         self.t = 0.0
         self.nDOF = self.op.nElems * (o["n"] + 1) ** 3

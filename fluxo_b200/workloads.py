@@ -40,6 +40,52 @@ def mhd_prim_to_cons(prim, kappa, mu_0=1.0):
     return U
 
 
+def mhd_exact_func(func, t, x, kappa=5.0 / 3.0, mu_0=1.0, ref_states=((1.0, 0, 0, 0, 1.0, 1.0, 0, 0),),
+                   ini_ref_state=1, center=(0.0, 0.0, 0.0), halfwidth=0.1, amplitude=0.1, frequency=1.0):
+    """FillIni / ExactFunc of the MHD equations (mhd/equation.f90:540-1276) on points x (..., 3) ->
+    conservative U (..., 9): 1 constant RefState(IniRefState), 3 Alfven wave, 201 soft blast between
+    RefStates 1 and 2, 311 Orszag-Tang vortex, 312 its 3D perturbed form."""
+    x = np.asarray(x, dtype=np.float64)
+    prim = np.zeros(x.shape[:-1] + (9,))
+    refs = np.asarray(ref_states, dtype=np.float64)
+    if func == 1:
+        prim[..., :8] = refs[ini_ref_state - 1]
+    elif func == 3:  # :596-639
+        omega, r, e = 2.0 * np.pi * frequency, 2.0, 0.2
+        nx, ny = 1.0 / np.sqrt(r * r + 1.0), r / np.sqrt(r * r + 1.0)
+        va = omega / ny
+        phi = omega / ny * (nx * (x[..., 0] - 0.5 * r) + ny * (x[..., 1] - 0.5 * r)) - va * t
+        U = np.zeros(x.shape[:-1] + (9,))
+        U[..., 0] = 1.0
+        U[..., 1] = -e * ny * np.cos(phi)
+        U[..., 2] = e * nx * np.cos(phi)
+        U[..., 3] = e * np.sin(phi)
+        U[..., 4] = 1.0 / (kappa - 1.0) + 0.5 * np.sum(U[..., 1:4] ** 2, axis=-1)
+        U[..., 5] = nx - U[..., 1]
+        U[..., 6] = ny - U[..., 2]
+        U[..., 7] = -U[..., 3]
+        return U
+    elif func == 201:  # :1239-1246
+        rr = np.sqrt(np.sum((x - np.asarray(center)) ** 2, axis=-1))
+        a = np.exp(5.0 * (rr - halfwidth) / amplitude)
+        a = (a / (a + 1.0))[..., None]
+        prim[..., :8] = (1.0 - a) * refs[0] + a * refs[1]
+    elif func in (311, 312):  # :1248-1266
+        sx, sy = np.sin(2 * np.pi * x[..., 0]), np.sin(2 * np.pi * x[..., 1])
+        fz = 1.0 + 0.2 * np.sin(2 * np.pi * x[..., 2]) if func == 312 else 1.0
+        prim[..., 0] = 1.0
+        prim[..., 1] = -fz * sy
+        prim[..., 2] = fz * sx
+        if func == 312:
+            prim[..., 3] = 0.2 * np.sin(2 * np.pi * x[..., 2])
+        prim[..., 4] = 1.0 / kappa
+        prim[..., 5] = -sy / kappa
+        prim[..., 6] = np.sin(4 * np.pi * x[..., 0]) / kappa
+    else:
+        raise ValueError("MHD IniExactFunc %d not implemented" % func)
+    return mhd_prim_to_cons(prim, kappa, mu_0)
+
+
 def mhd_orszag_tang_state(xGP, kappa=5.0 / 3.0, seed=SEED, perturbation=1e-3, mu_0=1.0):
     """Conservative state (nElems, n, n, n, 9) of the resistive-MHD configuration at the nodes xGP
     (nElems, n, n, n, 3)."""

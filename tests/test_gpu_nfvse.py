@@ -159,3 +159,41 @@ def test_nfvse_tvd_continuous_data_ties(gpu_lib):
     ref = c.dg_time_derivative(0.0)
     op.dg_time_derivative(0.0)
     assert rel_l2(op.get_ut(), ref) <= TOL
+
+
+def test_product_setup_path_mhd_shock_capturing(gpu_lib):
+    """Fluxo() from a parameter.ini of resistive MHD with NFVSE (indicator, TVD subcell FV with the
+    neighbours' states at the element boundaries): own mesh and initial state, matches the oracle."""
+    ini = """
+    N = 3
+    Equation = mhd
+    BoxElems = (/3,2,2/)
+    BoxMin = (/-1.,-1.,-1./)
+    BoxMax = (/1.,1.,1./)
+    NGeo = 2
+    MeshDeformAmp = 0.1
+    RefState = (/1.2, 0.1, 0.0, 0.1, 0.9, 1.0, 1.0, 1.0/)
+    RefState = (/1.1, 0.2, -0.1, 0.2, 0.6, 1.0, 1.0, 1.0/)
+    IniExactFunc = 201
+    IniCenter = (/0.1,0.05,0./)
+    IniHalfwidth = 0.4
+    IniAmplitude = 0.02
+    Riemann = 10
+    VolumeFlux = 10
+    eta = 0.01
+    nfvse = T
+    ComputeAlpha = 1
+    SubFVMethod = 2
+    ReconsBoundaries = 3
+    CFLScale = 0.5
+    """
+    f = fb.Fluxo(ini)
+    f.op.glm_ch = 0.7
+    f.DGTimeDerivative(0.0)
+    c = OracleCase(eqn=3, N=3, nElems=(3, 2, 2), xmin=(-1, -1, -1), xmax=(1, 1, 1), NGeo=2, deform_amp=0.1,
+                   kappa=5 / 3, mhd_ref_state=REF, ini_exact_func=201, ini_center=(0.1, 0.05, 0.0),
+                   ini_halfwidth=0.4, ini_amplitude=0.02, glm_ch=0.7, nfvse=1, volume_flux=10, riemann=10,
+                   eta=0.01, sub_fv_method=2, recons_boundaries=3, cfl_scale=0.5)
+    ref = c.dg_time_derivative(0.0)
+    assert np.abs(f.op.alpha() - c.alpha()).max() <= 1e-12
+    assert rel_l2(f.Ut, ref) <= 1e-11

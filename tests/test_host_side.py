@@ -85,3 +85,45 @@ def test_parameter_ini():
     assert f["eqn"] == 1 and f["lifting_var"] == 3
     with pytest.raises(KeyError):
         resolve(parse_ini("Riemann = 1"))
+
+
+def test_parameter_ini_mhd_and_shock_capturing():
+    txt = """
+    N = 4
+    Equation = mhd
+    RefState = (/1., 0., 0., 0., 1., 1., 0., 0./)
+    RefState = (/1.2, 0.1, 0., 0., 0.9, 1., 0., 0./)
+    IniRefState = 2
+    Riemann = 14
+    VolumeFlux = 10
+    eta = 1.0d-3
+    GLM_scale = 0.4
+    nfvse = T
+    ComputeAlpha = 1
+    SubFVMethod = 2
+    ReconsBoundaries = 3
+    ShockIndicatorQuantity = Pressure
+    alpha_max = 0.6
+    CFLScale = 0.5
+    """
+    r = resolve(parse_ini(txt))
+    assert abs(r["kappa"] - 5 / 3) < 1e-15 and len(r["refstates"]) == 2
+    f = to_cfg_fields(r)
+    assert f["eqn"] == 3 and f["riemann"] == 14 and f["volume_flux"] == 10 and f["eta"] == 1e-3
+    assert f["nfvse"] == 1 and f["sub_fv_method"] == 2 and f["recons_boundaries"] == 3
+    assert f["indicator_quantity"] == 2 and f["alpha_max"] == 0.6 and f["glm_scale"] == 0.4
+    assert to_cfg_fields(resolve(parse_ini("N = 3\nCFLScale = 0.9")))["kappa"] == 1.4
+    with pytest.raises(ValueError):
+        to_cfg_fields(resolve(parse_ini(txt.replace("Pressure", "Entropy"))))
+
+
+@pytest.mark.parametrize("func", [1, 3, 201, 311, 312])
+def test_mhd_exact_func_matches_oracle(func):
+    from fluxo_b200.workloads import mhd_exact_func
+    ref = ((1.2, 0.1, 0.0, 0.1, 0.9, 1.0, 1.0, 1.0), (1.1, 0.2, -0.1, 0.2, 0.6, 1.0, 1.0, 1.0))
+    c = OracleCase(eqn=2, N=3, nElems=(2, 2, 2), xmin=(-1, -1, -1), xmax=(1, 1, 1), NGeo=2, deform_amp=0.05,
+                   kappa=5 / 3, mhd_ref_state=ref, ini_exact_func=func, ini_center=(0.1, 0.0, 0.0),
+                   ini_halfwidth=0.3, ini_amplitude=0.1)
+    U = mhd_exact_func(func, 0.0, c.mesh()["Elem_xGP"], kappa=5 / 3, ref_states=ref, ini_ref_state=1,
+                       center=(0.1, 0.0, 0.0), halfwidth=0.3, amplitude=0.1)
+    assert np.allclose(U, c.get_U(), rtol=1e-13, atol=1e-14)
