@@ -258,6 +258,12 @@ int rhs(fluxo_handle* h, KParams P) {
     h->launches += 2;
     return FLUXO_OK;
   }
+  if (h->cfg.nfvse) {  // CalcBlendingCoefficient (dg.f90:358-361) and VolInt_NFVSE's FV part (:380-383)
+    ProfScope ps(h, 5);
+    FLUXO_CUDA(h, launch_nfvse_alpha(h->NP, false, h->nElems, s, P, h->dAlphaTmp));
+    FLUXO_CUDA(h, launch_nfvse_fv_ns(h->cfg.riemann, h->NP, h->nElems, h->nSMs, s, P));
+    h->launches += 3 + (h->cfg.space_prop_sweeps > 1 ? 2 * (h->cfg.space_prop_sweeps - 1) : 0);
+  }
   if (h->visc) {
     {
       ProfScope ps(h, 0);
@@ -411,7 +417,6 @@ int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {
       return fail(nullptr, FLUXO_EINVAL_CFG, "volume flux not implemented");
   }
   if (cfg->nfvse) {  // InitShockCapturing / InitNFVSE checks (shockcapturing.f90:82-112, nfvse.f90:120-170)
-    if (!mhd) return fail(nullptr, FLUXO_EINVAL_CFG, "NFVSE is implemented for the MHD equations");
     if (cfg->N < 2) return fail(nullptr, FLUXO_EINVAL_CFG, "NFVSE needs N >= 2");
     if (cfg->compute_alpha != 1 && cfg->compute_alpha != 3)
       return fail(nullptr, FLUXO_EINVAL_CFG, "ComputeAlpha must be 1 (indicator) or 3 (fixed)");

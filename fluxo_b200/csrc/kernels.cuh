@@ -304,6 +304,14 @@ volume_kernel(KParams P) {
 #pragma unroll
   for (int v = 0; v < 5; ++v) ut[v] = valid ? acc[vol_pad<NP, LPW>(t) * 5 + v] : 0.;
   if (!valid) return;
+  if (P.nfvse) {  // VolInt_NFVSE (nfvse.f90:475-565): blend with alpha * F_FV of the subcell FV kernel
+    const double a = P.alpha[e];
+    if (a > 4.440892098500626e-16) {
+      const double* FV = P.fv + (size_t)e * 5 * NP3 + t;
+#pragma unroll
+      for (int v = 0; v < 5; ++v) ut[v] = (1. - a) * ut[v] + FV[v * NP3];
+    }
+  }
   if constexpr (VISC) {  // viscous volume integral (volint.f90:228-271), computed by the lifting kernel
     const double* V = P.utvisc + (size_t)e * 4 * NP3 + t;
 #pragma unroll

@@ -68,6 +68,7 @@ cudaError_t launch_mhd_timestep(int NP, bool visc, int nElems, cudaStream_t s, c
 // `scratch` holds nElems doubles for sweeps > 1) and the subcell FV volume integral of MHD.
 cudaError_t launch_nfvse_alpha(int NP, bool mhd, int nElems, cudaStream_t s, const KParams& P, double* scratch);
 cudaError_t launch_nfvse_fv(int RS, int NP, int nElems, int nSMs, cudaStream_t s, const KParams& P);
+cudaError_t launch_nfvse_fv_ns(int RS, int NP, int nElems, int nSMs, cudaStream_t s, const KParams& P);
 
 // Host helpers of fluxo_gpu.cu for entry points without a handle: the per-N operator tables, and
 // the message that fluxo_gpu_last_error(NULL, ...) returns (returns `code`).

@@ -4,7 +4,7 @@
 //                     Legendre coefficients, alpha = 1/(1+exp(-s (eta-T)/T)), clipping;
 //   propagate_kernel  alpha_e = max(alpha_e, SpacePropFactor * max over its sides of the two
 //                     element values) and the list of blended elements (alpha > 2*EPSILON);
-//   fv_kernel_mhd     per blended element: first-order subcell FV volume integral with sub-cell
+//   fv_kernel         per blended element: first-order or TVD subcell FV volume integral with sub-cell
 //                     metrics built from the element's metrics on the fly (nfvse.f90:261-378),
 //                     the Riemann solver of the face kernel and the non-conservative terms,
 //                     written as alpha * F_FV for the volume kernel to blend with.
@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(512) alpha_kernel(KParams P) {
 
 // PropagateBlendingCoeff (nfvse_mpi.f90:62-131) for one sweep from `src` into alpha; the last
 // sweep also lists the blended elements
-__global__ void propagate_kernel(KParams P, const double* src, bool last) {
+static __global__ void propagate_kernel(KParams P, const double* src, bool last) {
   if (halted(P)) return;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= P.nElems) return;
@@ -120,7 +120,7 @@ __global__ void propagate_kernel(KParams P, const double* src, bool last) {
 }
 
 // no propagation (SpacePropSweeps = 0): alpha = raw value, list the blended elements
-__global__ void list_kernel(KParams P) {
+static __global__ void list_kernel(KParams P) {
   if (halted(P)) return;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= P.nElems) return;
@@ -155,6 +155,26 @@ __device__ __forceinline__ void cons_to_prim_rn(const KParams& P, const double* 
 #pragma unroll
   for (int v = 5; v < 9; ++v) Q[v] = U[v];
 }
+// ConsToPrim / PrimToCons of Euler / Navier-Stokes (navierstokes/equation_vars.f90:243-290), uncontracted
+__device__ __forceinline__ void cons_to_prim_ns_rn(const KParams& P, const double* U, double* Q) {
+  const double s = 1. / U[0];
+  Q[0] = U[0];
+  Q[1] = mul_rn(U[1], s); Q[2] = mul_rn(U[2], s); Q[3] = mul_rn(U[3], s);
+  const double mv = add_rn(add_rn(mul_rn(U[1], Q[1]), mul_rn(U[2], Q[2])), mul_rn(U[3], Q[3]));
+  Q[4] = mul_rn(P.kappaM1, sub_rn(U[4], mul_rn(0.5, mv)));
+}
+__device__ __forceinline__ void prim_to_cons_ns_rn(const KParams& P, const double* Q, double* U) {
+  U[0] = Q[0];
+  U[1] = mul_rn(Q[1], Q[0]); U[2] = mul_rn(Q[2], Q[0]); U[3] = mul_rn(Q[3], Q[0]);
+  const double mv = add_rn(add_rn(mul_rn(U[1], Q[1]), mul_rn(U[2], Q[2])), mul_rn(U[3], Q[3]));
+  U[4] = add_rn(mul_rn(P.sKappaM1, Q[4]), mul_rn(0.5, mv));
+}
+template <int NV>
+__device__ __forceinline__ void c2p_rn(const KParams& P, const double* U, double* Q) {
+  if constexpr (NV == 9) cons_to_prim_rn(P, U, Q);
+  else cons_to_prim_ns_rn(P, U, Q);
+}
+
 __device__ __forceinline__ void prim_to_cons_rn(const KParams& P, const double* Q, double* U) {
   U[0] = Q[0];
   U[1] = mul_rn(Q[1], Q[0]); U[2] = mul_rn(Q[2], Q[0]); U[3] = mul_rn(Q[3], Q[0]);
@@ -168,7 +188,7 @@ __device__ __forceinline__ void prim_to_cons_rn(const KParams& P, const double* 
 // Primitive state of the neighbour element's node that coincides with the boundary node `node` of
 // element e on the minus (plus = false) or plus side of direction dir (Get_externalU: U_slave on a
 // master side, U_master on a slave side, which are the neighbour's boundary nodes for LGL)
-template <int NP>
+template <int NP, int NV>
 __device__ __forceinline__ void ext_prim(const KParams& P, int e, int dir, bool plus, int node, double* pr) {
   constexpr int N = NP - 1, NP3 = NP * NP * NP;
   const int s = dir == 0 ? (plus ? XI_PLUS : XI_MINUS) : (dir == 1 ? (plus ? ETA_PLUS : ETA_MINUS)
@@ -180,17 +200,17 @@ __device__ __forceinline__ void ext_prim(const KParams& P, int e, int dir, bool 
   const int* se5 = P.s2e + 5 * side;
   const int nb = flip == 0 ? se5[1] : se5[0];
   const int nn = flip == 0 ? side_node(N, p, q, se5[4], se5[3]) : side_node(N, p, q, 0, se5[2]);
-  cons_to_prim_rn(P, P.U + mhd::NV * ((size_t)nb * NP3 + nn), pr);
+  c2p_rn<NV>(P, P.U + NV * ((size_t)nb * NP3 + nn), pr);
 }
 
 // TVD states of subcell face x of a line (ReconstructSolution_2nd_Order, nfvse.f90:1448-1510):
 // cL = cons(primR(x)), cR = cons(primL(x+1)); pr = the line's primitive records (stride st doubles)
-template <int NP>
+template <int NP, int NV>
 __device__ __forceinline__ void tvd_states(const KParams& P, const double* pr, int st, int x, const double* sdxR,
                                            const double* sdxL, const double* rL, const double* rR,
                                            const double* w, const double* extL, const double* extR, double* cL,
                                            double* cR) {
-  constexpr int N = NP - 1, NV = mhd::NV;
+  constexpr int N = NP - 1;
   const int rb = P.reconsBoundaries;
   double pl[NV], prr[NV];
 #pragma unroll
@@ -216,8 +236,13 @@ __device__ __forceinline__ void tvd_states(const KParams& P, const double* pr, i
       prr[v] = add_rn(Q(y), mul_rn(sg, rL[y]));
     }
   }
-  prim_to_cons_rn(P, pl, cL);
-  prim_to_cons_rn(P, prr, cR);
+  if constexpr (NV == 9) {
+    prim_to_cons_rn(P, pl, cL);
+    prim_to_cons_rn(P, prr, cR);
+  } else {
+    prim_to_cons_ns_rn(P, pl, cL);
+    prim_to_cons_ns_rn(P, prr, cR);
+  }
 }
 
 template <int NP>
@@ -230,10 +255,14 @@ __host__ __device__ constexpr size_t fv_smem_bytes() {
 // block iteration, one thread per node.  Per direction each node evaluates the flux on its right
 // subcell face (x, x+1), keeps its own share (with its own non-conservative part) and hands the
 // right neighbour's share over in shared memory.  F_FV(x) = (FR(x) - FL(x-1)) / w_x.
-template <int NP, int RS>
-__global__ void __launch_bounds__(NP * NP * NP) fv_kernel_mhd(KParams P) {
+template <int NP, int RS, bool MHD>
+__global__ void __launch_bounds__(NP * NP * NP) fv_kernel(KParams P) {
   if (halted(P)) return;
-  constexpr int NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1, NV = 9;
+  constexpr int NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1, NV = MHD ? 9 : 5;
+  // LLF-dissipation solvers of Euler / Navier-Stokes: the largest wave speed over each subcell face
+  // plane (AdvRiemann on the plane's points), per direction and face
+  constexpr bool planeMax = !MHD && riemann_needs_side_max<RS>();
+  __shared__ unsigned long long sLam[3][NP];
   extern __shared__ double smem[];
   double* sD = smem;          // D(l,m) at [l*NP+m]
   double* sW = sD + NPT;      // wGP
@@ -263,7 +292,7 @@ __global__ void __launch_bounds__(NP * NP * NP) fv_kernel_mhd(KParams P) {
   }
   const bool tvd = P.subFV == 2;
   const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
-  const double ch = glm_ch(P);
+  const double ch = MHD ? glm_ch(P) : 0.;
   const int count = *P.blendCount;
   for (int li = blockIdx.x; li < count; li += gridDim.x) {
     const int e = P.blendList[li];
@@ -275,7 +304,8 @@ __global__ void __launch_bounds__(NP * NP * NP) fv_kernel_mhd(KParams P) {
       const double* Mg = P.metrics + (size_t)e * 9 * NP3 + t;
 #pragma unroll
       for (int c = 0; c < 9; ++c) sM[c * NP3 + t] = Mg[c * NP3];
-      if (tvd) cons_to_prim_rn(P, sU + NV * t, sPr + NV * t);
+      if (tvd) c2p_rn<NV>(P, sU + NV * t, sPr + NV * t);
+      if (planeMax && t < 3 * NP) sLam[t / NP][t % NP] = 0ull;
     }
     __syncthreads();
     double ffv[NV];
@@ -286,11 +316,13 @@ __global__ void __launch_bounds__(NP * NP * NP) fv_kernel_mhd(KParams P) {
       const int x = dir == 0 ? i : (dir == 1 ? j : k);
       const int stride = dir == 0 ? 1 : (dir == 1 ? NP : NPT);
       const int n0 = t - x * stride;  // node at position 0 of this node's line
+      double nv[3], t1[3], t2[3], norm = 0., L[NV], R[NV];
+      const double* uL = sU + NV * t;
+      const double* uR = sU + NV * (t + (x < N ? stride : 0));
       if (x < N) {
         // sub-cell metrics of face x (nfvse.f90:261-378): nv from Ja^dir, t1 from Ja^(dir+1)
         const double* Mn = sM + (3 * dir) * NP3;
         const double* Mt = sM + (3 * ((dir + 1) % 3)) * NP3;
-        double nv[3], t1[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) { nv[c] = Mn[c * NP3 + n0]; t1[c] = Mt[c * NP3 + n0]; }
         for (int m = 0; m < NP; ++m)
@@ -302,7 +334,7 @@ __global__ void __launch_bounds__(NP * NP * NP) fv_kernel_mhd(KParams P) {
               t1[c] += wd * Mt[c * NP3 + n0 + m * stride];
             }
           }
-        const double norm = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+        norm = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
 #pragma unroll
         for (int c = 0; c < 3; ++c) nv[c] = nv[c] / norm;
         const double tn = t1[0] * nv[0] + t1[1] * nv[1] + t1[2] * nv[2];
@@ -311,29 +343,28 @@ __global__ void __launch_bounds__(NP * NP * NP) fv_kernel_mhd(KParams P) {
         const double tl = sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
 #pragma unroll
         for (int c = 0; c < 3; ++c) t1[c] = t1[c] / tl;
-        const double t2[3] = {nv[1] * t1[2] - nv[2] * t1[1], nv[2] * t1[0] - nv[0] * t1[2],
-                              nv[0] * t1[1] - nv[1] * t1[0]};
-        const double* uL = sU + NV * t;
-        const double* uR = sU + NV * (t + stride);
+        t2[0] = nv[1] * t1[2] - nv[2] * t1[1];
+        t2[1] = nv[2] * t1[0] - nv[0] * t1[2];
+        t2[2] = nv[0] * t1[1] - nv[1] * t1[0];
         // states of the subcell Riemann problem: the nodal values (first order) or the TVD
         // reconstruction primR(x), primL(x+1) of the line (Compute_FVFluxes_TVD nfvse.f90:674-815)
         double cL[NV], cR[NV];
         if (tvd) {
           double extL[NV], extR[NV];
           if (P.reconsBoundaries == 3) {  // Get_externalU (nfvse.f90:1621-1683): the neighbours' nodes
-            if (x == 0) ext_prim<NP>(P, e, dir, false, t, extL);
-            if (x + 1 == N) ext_prim<NP>(P, e, dir, true, t + stride, extR);
+            if (x == 0) ext_prim<NP, NV>(P, e, dir, false, t, extL);
+            if (x + 1 == N) ext_prim<NP, NV>(P, e, dir, true, t + stride, extR);
           }
-          tvd_states<NP>(P, sPr + NV * (t - x * stride), NV * stride, x, sdxR, sdxL, rL, rR, sW, extL, extR, cL, cR);
+          tvd_states<NP, NV>(P, sPr + NV * (t - x * stride), NV * stride, x, sdxR, sdxL, rL, rR, sW, extL, extR, cL,
+                             cR);
         } else {
 #pragma unroll
           for (int v = 0; v < NV; ++v) { cL[v] = uL[v]; cR[v] = uR[v]; }
         }
-        double L[NV], R[NV], F[NV];
 #pragma unroll
         for (int v = 0; v < NV; ++v) { L[v] = cL[v]; R[v] = cR[v]; }
 #pragma unroll
-        for (int b = 1; b <= 5; b += 4) {  // RotateState, mhd/riemann.f90:185-200
+        for (int b = 1; b <= (MHD ? 5 : 1); b += 4) {  // RotateState, riemann.f90:218-231 (MHD :185-200)
           L[b] = cL[b] * nv[0] + cL[b + 1] * nv[1] + cL[b + 2] * nv[2];
           L[b + 1] = cL[b] * t1[0] + cL[b + 1] * t1[1] + cL[b + 2] * t1[2];
           L[b + 2] = cL[b] * t2[0] + cL[b + 1] * t2[1] + cL[b + 2] * t2[2];
@@ -341,9 +372,19 @@ __global__ void __launch_bounds__(NP * NP * NP) fv_kernel_mhd(KParams P) {
           R[b + 1] = cR[b] * t1[0] + cR[b + 1] * t1[1] + cR[b + 2] * t1[2];
           R[b + 2] = cR[b] * t2[0] + cR[b + 1] * t2[1] + cR[b + 2] * t2[2];
         }
-        mhd::riemann<RS>(P, ch, L, R, F);
+      }
+      double lmm = 0.;
+      if constexpr (planeMax) {
+        if (x < N) atomicMax(&sLam[dir][x], (unsigned long long)__double_as_longlong(lambda_max_pair(P, L, R)));
+        __syncthreads();
+        if (x < N) lmm = __longlong_as_double((long long)sLam[dir][x]);
+      }
+      if (x < N) {
+        double F[NV];
+        if constexpr (MHD) mhd::riemann<RS>(P, ch, L, R, F);
+        else riemann_rotated<RS>(P, L, R, lmm, F);
 #pragma unroll
-        for (int b = 1; b <= 5; b += 4) {  // RotateFluxBack, mhd/riemann.f90:204-217
+        for (int b = 1; b <= (MHD ? 5 : 1); b += 4) {  // RotateFluxBack, riemann.f90:235-246 (MHD :204-217)
           const double f2 = F[b], f3 = F[b + 1], f4 = F[b + 2];
           F[b] = nv[0] * f2 + t1[0] * f3 + t2[0] * f4;
           F[b + 1] = nv[1] * f2 + t1[1] * f3 + t2[1] * f4;
@@ -352,13 +393,15 @@ __global__ void __launch_bounds__(NP * NP * NP) fv_kernel_mhd(KParams P) {
         double FR[NV];
 #pragma unroll
         for (int v = 0; v < NV; ++v) FR[v] = F[v];
-        if (P.noncons != 0) {  // AddNonConsFlux on both nodes of the face (Compute_FVFluxes_1D :1420-1436)
-          const bool ncg = P.ncGLM != 0;
-          const double Bn = 0.5 * ((uL[5] + uR[5]) * nv[0] + (uL[6] + uR[6]) * nv[1] + (uL[7] + uR[7]) * nv[2]);
-          const double ps = 0.5 * (uL[8] + uR[8]);
-          const double nq[3] = {ps * nv[0], ps * nv[1], ps * nv[2]};
-          mhd::add_noncons_surface(P.noncons, ncg, uR, Bn, nq, F);
-          mhd::add_noncons_surface(P.noncons, ncg, uL, Bn, nq, FR);
+        if constexpr (MHD) {
+          if (P.noncons != 0) {  // AddNonConsFlux on both nodes of the face (Compute_FVFluxes_1D :1420-1436)
+            const bool ncg = P.ncGLM != 0;
+            const double Bn = 0.5 * ((uL[5] + uR[5]) * nv[0] + (uL[6] + uR[6]) * nv[1] + (uL[7] + uR[7]) * nv[2]);
+            const double ps = 0.5 * (uL[8] + uR[8]);
+            const double nq[3] = {ps * nv[0], ps * nv[1], ps * nv[2]};
+            mhd::add_noncons_surface(P.noncons, ncg, uR, Bn, nq, F);
+            mhd::add_noncons_surface(P.noncons, ncg, uL, Bn, nq, FR);
+          }
         }
         double* A = sA + NV * (t + stride);
 #pragma unroll

@@ -1,8 +1,9 @@
-// Host launchers of the NFVSE kernels (indicator, propagation, subcell FV of MHD).
+// Host launchers of the NFVSE kernels (indicator, propagation, subcell FV of MHD; the Euler /
+// Navier-Stokes subcell FV launcher is in nfvse_ns.cu).
 #include <algorithm>
 
 #include "launch.h"
-#include "nfvse.cuh"
+#include "nfvse_fv.cuh"
 
 namespace fluxo {
 
@@ -14,28 +15,6 @@ cudaError_t alpha_np(int nElems, cudaStream_t s, const KParams& P) {
   return cudaGetLastError();
 }
 
-template <int NP, int RS>
-cudaError_t fv_np(int grid, cudaStream_t s, const KParams& P) {
-  constexpr size_t smem = nfvse::fv_smem_bytes<NP>();
-  auto k = nfvse::fv_kernel_mhd<NP, RS>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  k<<<grid, NP * NP * NP, smem, s>>>(P);
-  return cudaGetLastError();
-}
-
-template <int RS>
-cudaError_t fv_rs(int NP, int grid, cudaStream_t s, const KParams& P) {
-  switch (NP) {
-    case 3: return fv_np<3, RS>(grid, s, P);
-    case 4: return fv_np<4, RS>(grid, s, P);
-    case 5: return fv_np<5, RS>(grid, s, P);
-    case 6: return fv_np<6, RS>(grid, s, P);
-    case 7: return fv_np<7, RS>(grid, s, P);
-    case 8: return fv_np<8, RS>(grid, s, P);
-    default: return cudaErrorInvalidValue;
-  }
-}
 }  // namespace
 
 cudaError_t launch_nfvse_alpha(int NP, bool mhd, int nElems, cudaStream_t s, const KParams& P, double* scratch) {
@@ -70,18 +49,18 @@ cudaError_t launch_nfvse_alpha(int NP, bool mhd, int nElems, cudaStream_t s, con
 cudaError_t launch_nfvse_fv(int RS, int NP, int nElems, int nSMs, cudaStream_t s, const KParams& P) {
   const int grid = std::min(nElems, 8 * nSMs);
   switch (RS) {
-    case 0: return fv_rs<0>(NP, grid, s, P);
-    case 1: return fv_rs<1>(NP, grid, s, P);
-    case 2: return fv_rs<2>(NP, grid, s, P);
-    case 3: return fv_rs<3>(NP, grid, s, P);
-    case 4: return fv_rs<4>(NP, grid, s, P);
-    case 5: return fv_rs<5>(NP, grid, s, P);
-    case 10: return fv_rs<10>(NP, grid, s, P);
-    case 11: return fv_rs<11>(NP, grid, s, P);
-    case 12: return fv_rs<12>(NP, grid, s, P);
-    case 13: return fv_rs<13>(NP, grid, s, P);
-    case 14: return fv_rs<14>(NP, grid, s, P);
-    case 15: return fv_rs<15>(NP, grid, s, P);
+    case 0: return nfvse::fv_rs<true, 0>(NP, grid, s, P);
+    case 1: return nfvse::fv_rs<true, 1>(NP, grid, s, P);
+    case 2: return nfvse::fv_rs<true, 2>(NP, grid, s, P);
+    case 3: return nfvse::fv_rs<true, 3>(NP, grid, s, P);
+    case 4: return nfvse::fv_rs<true, 4>(NP, grid, s, P);
+    case 5: return nfvse::fv_rs<true, 5>(NP, grid, s, P);
+    case 10: return nfvse::fv_rs<true, 10>(NP, grid, s, P);
+    case 11: return nfvse::fv_rs<true, 11>(NP, grid, s, P);
+    case 12: return nfvse::fv_rs<true, 12>(NP, grid, s, P);
+    case 13: return nfvse::fv_rs<true, 13>(NP, grid, s, P);
+    case 14: return nfvse::fv_rs<true, 14>(NP, grid, s, P);
+    case 15: return nfvse::fv_rs<true, 15>(NP, grid, s, P);
     default: return cudaErrorInvalidValue;
   }
 }

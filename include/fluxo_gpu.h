@@ -73,8 +73,8 @@ typedef struct fluxo_cfg {
   double glm_scr;    /* GLM_scr: damping Ut(9) -= GLM_scr*GLM_ch*U(9) (equation.f90:1698-1706) */
   int noncons;       /* NONCONS: 0 off, 1 Powell, 2 Brackbill, 3 Janhunen (CMake FLUXO_EQN_NONCONS_TYPE) */
   int nc_glm;        /* PP_NC_GLM: non-conservative GLM terms (CMake FLUXO_EQN_NONCONS_GLM) */
-  /* NFVSE shock capturing (CMake FLUXO_SHOCKCAP_NFVSE; src/shockcapturing/nfvse.f90:63-260), MHD,
-   * N >= 2, SubFVMethod = 1 (first-order subcell finite volumes) or 2 (TVD). */
+  /* NFVSE shock capturing (CMake FLUXO_SHOCKCAP_NFVSE; src/shockcapturing/nfvse.f90:63-260), Euler,
+   * Navier-Stokes and MHD, N >= 2, SubFVMethod = 1 (first-order subcell finite volumes) or 2 (TVD). */
   int nfvse;               /* 0 off, 1 on */
   int compute_alpha;       /* ComputeAlpha: 1 Persson-Peraire indicator, 3 fixed ShockBlendCoef */
   double shock_blend_coef; /* ShockBlendCoef */

@@ -197,3 +197,43 @@ def test_product_setup_path_mhd_shock_capturing(gpu_lib):
     ref = c.dg_time_derivative(0.0)
     assert np.abs(f.op.alpha() - c.alpha()).max() <= 1e-12
     assert rel_l2(f.Ut, ref) <= 1e-11
+
+
+NS_NFVSE = [
+    dict(eqn=0, N=3, riemann=1, volume_flux=5, sub_fv_method=1),
+    dict(eqn=0, N=4, riemann=44, volume_flux=5, sub_fv_method=2, recons_boundaries=3),
+    dict(eqn=0, N=3, riemann=14, volume_flux=2, sub_fv_method=1),
+    dict(eqn=0, N=3, riemann=16, volume_flux=5, sub_fv_method=2, recons_boundaries=2),
+    dict(eqn=0, N=5, riemann=2, volume_flux=10, sub_fv_method=2, recons_boundaries=1),
+    dict(eqn=1, N=3, riemann=44, volume_flux=5, sub_fv_method=2, recons_boundaries=3, mu0=0.01),
+]
+
+
+@pytest.mark.parametrize("case", NS_NFVSE, ids=lambda c: "eqn%d_N%d_rs%d_fv%d" % (c["eqn"], c["N"], c["riemann"],
+                                                                                 c["sub_fv_method"]))
+def test_nfvse_euler_navier_stokes_parity(gpu_lib, case):
+    """NFVSE on the Euler / Navier-Stokes system: indicator and fixed blending, first-order and TVD
+    subcell fluxes with every kind of Riemann solver (14/16: wave-speed maximum over the subcell face
+    plane)."""
+    for ca in (3, 1):
+        kw = dict(nElems=(3, 2, 2), xmin=(-1, -1, -1), xmax=(1, 1, 1), NGeo=2, deform_amp=0.1, ini_exact_func=2,
+                  ini_amplitude=0.3, adv_vel=(0.3, -0.2, 0.5), nfvse=1, compute_alpha=ca, shock_blend_coef=0.4,
+                  alpha_min=0.001, **case)
+        c = OracleCase(**kw)
+        U = c.get_U()
+        U = U * (1 + 0.03 * np.random.default_rng(4).standard_normal(U.shape))
+        c.set_U(U)
+        p = c.params
+        fields = dict(N=p.N, eqn=p.eqn, riemann=p.riemann, volume_flux=p.volume_flux, lifting=p.lifting,
+                      lifting_var=p.lifting_var, visc=p.visc, kappa=p.kappa, Pr=p.Pr, mu0=p.mu0,
+                      time_disc=p.time_disc, cfl_scale=p.cfl_scale, dfl_scale=p.dfl_scale, ini_exact_func=1)
+        fields.update({k: getattr(p, k) for k in NFVSE_KEYS})
+        op = fb.DGOperator(**fields)
+        op.set_mesh(c.mesh())
+        op.set_state(U)
+        ref = c.dg_time_derivative(0.0)
+        op.dg_time_derivative(0.0)
+        assert np.abs(op.alpha() - c.alpha()).max() <= 1e-12
+        if ca == 1:
+            assert (c.alpha() > 0).any()
+        assert rel_l2(op.get_ut(), ref) <= TOL
