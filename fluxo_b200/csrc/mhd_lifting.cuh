@@ -1,5 +1,6 @@
 // Lifting + viscous / resistive volume kernel of the MHD right-hand side (9 variables, LGL nodes).
-// Same structure as the Navier-Stokes kernel (lifting.cuh): per element, one thread per node,
+// Same node-centric structure as the Navier-Stokes kernel (lifting.cuh): per element, one thread per
+// node, two block barriers,
 //   1. BR1/BR2 gradients of the lifting variable (strong-form volume derivative br1_volint.f90:45-98 /
 //      br2_volint.f90:45-103, surface lifting br1_surfint.f90:52-131 / br2_surfint.f90:53-148,
 //      Jacobian, ConvertToGradPrim mhd/equation_vars.f90:547-628);
@@ -17,9 +18,11 @@
 namespace fluxo {
 namespace mhd {
 
+// operators at an odd row stride, then per element the 9 lifting variables and the 21 contravariant
+// viscous / resistive fluxes (7 per direction), node-major
 template <int NP>
 __host__ __device__ constexpr size_t lv_smem_bytes() {
-  return sizeof(double) * (size_t)(2 * NP * NP + epb<NP>() * 36 * lv_slots<NP>());
+  return sizeof(double) * (size_t)(2 * NP * lv_row<NP>() + epb<NP>() * 30 * NP * NP * NP);
 }
 
 // resident blocks per SM the register allocation must allow: 2 for BR1 blocks of up to 320 threads
@@ -30,19 +33,23 @@ __host__ __device__ constexpr int lv_minb() { return (LIFT == 1 && epb<NP>() * N
 template <int NP, int LIFT>
 __global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, lv_minb<NP, LIFT>()) lift_visc_kernel(KParams P) {
   if (halted(P)) return;
-  constexpr int NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1, EPB = epb<NP>(), NS = lv_slots<NP>();
+  constexpr int NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1, EPB = epb<NP>(), R = lv_row<NP>();
   extern __shared__ double smem[];
-  double* sD = smem;
-  double* sDhat = sD + NPT;
+  double* sD = smem;             // D(i,l) at [i*R+l]
+  double* sDhat = sD + NP * R;   // D_hat(i,l)
   const int eb = threadIdx.x / NP3, t = threadIdx.x - eb * NP3;
   const int e = blockIdx.x * EPB + eb;
   const bool valid = e < P.nElems;
-  double* sV = sDhat + NPT + (size_t)eb * 36 * NS;  // [9][NS] lifting variable; later [7][NS] sums
-  double* sW = sV + 9 * NS;                          // [27][NS] derivatives; later [21][NS] fluxes
+  double* sV = sDhat + NP * R + (size_t)eb * 30 * NP3;  // [9][node] lifting variable
+  double* sF = sV + 9 * NP3;                            // [21][node] contravariant fluxes, 7 per direction
   for (int z = threadIdx.x; z < NPT; z += blockDim.x) {
-    sD[z] = P.basis->D[z];
-    sDhat[z] = P.basis->Dhat[z];
+    const int r = z / NP, c = z - r * NP;
+    sD[r * R + c] = P.basis->D[z];
+    sDhat[r * R + c] = P.basis->Dhat[z];
   }
+  const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
+  // first node of the own xi / eta / zeta line; the line's nodes follow at strides 1, NP, NP^2
+  const int bx = t - i, be = t - NP * j, bz = t - NPT * k;
   double u[NV];
   if (valid) {
     const double* Ug = P.U + NV * ((size_t)e * NP3 + t);
@@ -54,24 +61,7 @@ __global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, lv_minb<NP, LIFT>())
     double V[NV];
     lifting_var_rt(P, u, V);
 #pragma unroll
-    for (int v = 0; v < NV; ++v) sV[v * NS + lv_slot(t)] = V[v];
-  }
-  __syncthreads();
-  if (valid) {  // line-blocked derivatives: tasks (dir, var, line)
-    for (int task = t; task < 27 * NPT; task += NP3) {
-      const int dir = task / (9 * NPT), rem = task - dir * 9 * NPT, v = rem / NPT, L = rem - v * NPT;
-      const int a = L % NP, b = L / NP;
-      double x[NP];
-#pragma unroll
-      for (int l = 0; l < NP; ++l) x[l] = sV[v * NS + lv_slot(line_node<NP>(dir, a, b, l))];
-#pragma unroll
-      for (int o = 0; o < NP; ++o) {
-        double s = 0.;
-#pragma unroll
-        for (int l = 0; l < NP; ++l) s += sD[o * NP + l] * x[l];
-        sW[(dir * 9 + v) * NS + lv_slot(line_node<NP>(dir, a, b, o))] = s;
-      }
-    }
+    for (int v = 0; v < NV; ++v) sV[v * NP3 + t] = V[v];
   }
   __syncthreads();
   double ft[21];
@@ -82,13 +72,29 @@ __global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, lv_minb<NP, LIFT>())
     for (int c = 0; c < 9; ++c) m[c] = M[c * NP3];
     const double sj = P.sJ[(size_t)e * NP3 + t];
     double g[3][NV];
+    {
+      // derivatives of the lifting variable along xi, eta, zeta at the own node, l = 0..N
+      double dx[NV], de[NV], dz[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      const double gx = sW[v * NS + lv_slot(t)], ge = sW[(9 + v) * NS + lv_slot(t)], gz = sW[(18 + v) * NS + lv_slot(t)];
+      for (int v = 0; v < NV; ++v) { dx[v] = 0.; de[v] = 0.; dz[v] = 0.; }
+      const double* Di = sD + i * R;
+      const double* Dj = sD + j * R;
+      const double* Dk = sD + k * R;
 #pragma unroll
-      for (int d = 0; d < 3; ++d) g[d][v] = m[0 + d] * gx + m[3 + d] * ge + m[6 + d] * gz;
+      for (int l = 0; l < NP; ++l) {
+        const double a = Di[l], b = Dj[l], c = Dk[l];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          dx[v] += a * sV[v * NP3 + bx + l];
+          de[v] += b * sV[v * NP3 + be + NP * l];
+          dz[v] += c * sV[v * NP3 + bz + NPT * l];
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) g[d][v] = m[0 + d] * dx[v] + m[3 + d] * de[v] + m[6 + d] * dz[v];
     }
-    const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
     int sides[3];
     const int ns = boundary_sides(i, j, k, N, sides);
     const double lh = P.basis->LhatM0;
@@ -178,38 +184,31 @@ __global__ void __launch_bounds__(epb<NP>() * NP * NP * NP, lv_minb<NP, LIFT>())
       ft[7 + v] = f[v] * m[3] + gg[v] * m[4] + h[v] * m[5];
       ft[14 + v] = f[v] * m[6] + gg[v] * m[7] + h[v] * m[8];
     }
+    // contravariant fluxes of the own node
+#pragma unroll
+    for (int c = 0; c < 21; ++c) sF[c * NP3 + t] = ft[c];
   }
   __syncthreads();
+  // viscous / resistive volume integral at the own node: sum_l D_hat(i,l) f~(l,j,k) + D_hat(j,l) g~(i,l,k)
+  // + D_hat(k,l) h~(i,j,l), l = 0..N
   if (valid) {
+    double r[7] = {0., 0., 0., 0., 0., 0., 0.};
+    const double* Hi = sDhat + i * R;
+    const double* Hj = sDhat + j * R;
+    const double* Hk = sDhat + k * R;
 #pragma unroll
-    for (int c = 0; c < 21; ++c) sW[c * NS + lv_slot(t)] = ft[c];
+    for (int l = 0; l < NP; ++l) {
+      const double a = Hi[l], b = Hj[l], c = Hk[l];
 #pragma unroll
-    for (int v = 0; v < 7; ++v) sV[v * NS + lv_slot(t)] = 0.;
-  }
-  __syncthreads();
-#pragma unroll 1
-  for (int dir = 0; dir < 3; ++dir) {
-    if (valid) {
-      for (int task = t; task < 7 * NPT; task += NP3) {
-        const int v = task / NPT, L = task - v * NPT, a = L % NP, b = L / NP;
-        double x[NP];
-#pragma unroll
-        for (int l = 0; l < NP; ++l) x[l] = sW[(dir * 7 + v) * NS + lv_slot(line_node<NP>(dir, a, b, l))];
-#pragma unroll
-        for (int o = 0; o < NP; ++o) {
-          double s = 0.;
-#pragma unroll
-          for (int l = 0; l < NP; ++l) s += sDhat[o * NP + l] * x[l];
-          sV[v * NS + lv_slot(line_node<NP>(dir, a, b, o))] += s;
-        }
+      for (int v = 0; v < 7; ++v) {
+        r[v] += a * sF[v * NP3 + bx + l];
+        r[v] += b * sF[(7 + v) * NP3 + be + NP * l];
+        r[v] += c * sF[(14 + v) * NP3 + bz + NPT * l];
       }
     }
-    __syncthreads();
-  }
-  if (valid) {
     double* O = P.utvisc + (size_t)e * 7 * NP3 + t;
 #pragma unroll
-    for (int v = 0; v < 7; ++v) O[v * NP3] = sV[v * NS + lv_slot(t)];
+    for (int v = 0; v < 7; ++v) O[v * NP3] = r[v];
   }
 }
 
