@@ -259,9 +259,18 @@ __device__ __forceinline__ void pair_flux_mhd(const KParams& P, double ch, const
 template <int NP>
 __host__ __device__ constexpr int epb() { return (256 / (NP * NP * NP)) > 0 ? (256 / (NP * NP * NP)) : 1; }
 
+// node slot of the records and accumulators: for N+1 = 5 (6 lines of 5 lanes per warp, 23-double
+// records) four spare slots after every 25 nodes, from a lane-by-lane model of the own, partner and
+// line-sum loads (1.12x the minimum shared wavefronts against 1.24x for one spare slot every 16
+// nodes); other N+1 keep the 16-node padding
+template <int NP>
+__host__ __device__ constexpr int mpad(int n) { return NP == 5 ? n + 4 * (n / 25) : vol_slot(n); }
+template <int NP>
+__host__ __device__ constexpr int mpad_slots() { return mpad<NP>(NP * NP * NP - 1) + 1; }
+
 template <int NP, int VF>
 __host__ __device__ constexpr size_t vol_smem_bytes() {
-  return sizeof(double) * (size_t)(NP * NP + NP + epb<NP>() * (Rec<VF>::RS + NACC) * vol_slots<NP>());
+  return sizeof(double) * (size_t)(NP * NP + NP + epb<NP>() * (Rec<VF>::RS + NACC) * mpad_slots<NP>());
 }
 
 // Pair-phase schedule: lines contiguous in the thread index when N+1 divides 32, otherwise
@@ -269,6 +278,7 @@ __host__ __device__ constexpr size_t vol_smem_bytes() {
 // Euler / Navier-Stokes volume kernel)
 template <int NP>
 __host__ __device__ constexpr int vol_lpw() { return 32 % NP == 0 ? 0 : 32 / NP; }
+
 template <int NP>
 __host__ __device__ constexpr int vol_threads() { return VolShape<NP, epb<NP>(), vol_lpw<NP>()>::THREADS; }
 
@@ -284,7 +294,7 @@ __global__ void __launch_bounds__(vol_threads<NP>(), vol_minb<NP>()) volume_kern
   const bool NCGLM = NC != 0 && P.ncGLM != 0;
   constexpr int NP3 = NP * NP * NP, N = NP - 1, NPT = NP * NP, EPB = epb<NP>(), LPW = vol_lpw<NP>();
   constexpr int RS = Rec<VF>::RS, NQ = Rec<VF>::NQ, IB = Rec<VF>::B, IPSI = Rec<VF>::PSI, IV = Rec<VF>::V;
-  constexpr int NS = vol_slots<NP>();
+  constexpr int NS = mpad_slots<NP>();
   extern __shared__ double smem[];
   double* sDvs = smem;        // Dvolsurf(i,l) at [i*NP+l]
   double* sRow = sDvs + NPT;  // sum_l Dvolsurf(i,l)
@@ -308,13 +318,13 @@ __global__ void __launch_bounds__(vol_threads<NP>(), vol_minb<NP>()) volume_kern
 #pragma unroll
     for (int v = 0; v < NV; ++v) u[v] = Ug[v];
     prefetch_l2(P.sJ + (size_t)e * NP3 + t);
-    double* r = rec + vol_slot(t) * RS;
+    double* r = rec + mpad<NP>(t) * RS;
     make_rec<VF>(P, u, r);
     const double* Mg = P.metrics + (size_t)e * 9 * NP3 + t;
 #pragma unroll
     for (int c = 0; c < 9; ++c) r[NQ + c] = Mg[c * NP3];
 #pragma unroll
-    for (int v = 0; v < NACC; ++v) acc[vol_slot(t) * NACC + v] = 0.;
+    for (int v = 0; v < NACC; ++v) acc[mpad<NP>(t) * NACC + v] = 0.;
   }
   __syncthreads();
   {
@@ -342,7 +352,7 @@ __global__ void __launch_bounds__(vol_threads<NP>(), vol_minb<NP>()) volume_kern
     for (int dir = 0; dir < 3; ++dir) {
       const int stride = dir == 0 ? 1 : (dir == 1 ? NP : NPT);
       const int base = dir == 0 ? NP * (la + NP * lb) : (dir == 1 ? la + NPT * lb : la + NP * lb);
-      const int own = base + p * stride, os = vol_slot(own);
+      const int own = base + p * stride, os = mpad<NP>(own);
       double ro[NQ], mo[3], racc[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) racc[v] = 0.;
@@ -362,7 +372,7 @@ __global__ void __launch_bounds__(vol_threads<NP>(), vol_minb<NP>()) volume_kern
         for (int v = 0; v < NV; ++v) F[v] = 0.;
         if (active) {
           // the partner's record is read in place (the log-mean logarithms only when needed)
-          const double* rq = prec + vol_slot(base + q * stride) * RS;
+          const double* rq = prec + mpad<NP>(base + q * stride) * RS;
           pair_flux_mhd<VF>(P, ch, ro, rq, mo, rq + NQ + 3 * dir, F);
         }
         const double dOwn = sDvs[p * NP + q], dPart = sDvs[q * NP + p];
@@ -382,7 +392,7 @@ __global__ void __launch_bounds__(vol_threads<NP>(), vol_minb<NP>()) volume_kern
           double sB0 = 0., sB1 = 0., sB2 = 0., sBh = 0., sPsi = 0.;
 #pragma unroll
           for (int l = 0; l < NP; ++l) {
-            const double* rl = prec + vol_slot(base + l * stride) * RS;
+            const double* rl = prec + mpad<NP>(base + l * stride) * RS;
             const double dl = sDvs[p * NP + l];
             const double b0 = rl[IB], b1 = rl[IB + 1], b2 = rl[IB + 2];
             const double* ml = rl + NQ + 3 * dir;
@@ -409,9 +419,9 @@ __global__ void __launch_bounds__(vol_threads<NP>(), vol_minb<NP>()) volume_kern
   }
   double ut[NV];
 #pragma unroll
-  for (int v = 0; v < NV; ++v) ut[v] = valid ? acc[vol_slot(t) * NACC + v] : 0.;
-  const double ncMHD = valid ? acc[vol_slot(t) * NACC + NV] : 0.;
-  const double ncGLM = valid ? acc[vol_slot(t) * NACC + NV + 1] : 0.;
+  for (int v = 0; v < NV; ++v) ut[v] = valid ? acc[mpad<NP>(t) * NACC + v] : 0.;
+  const double ncMHD = valid ? acc[mpad<NP>(t) * NACC + NV] : 0.;
+  const double ncGLM = valid ? acc[mpad<NP>(t) * NACC + NV + 1] : 0.;
   const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
   if (!valid) return;
   if (NC != 0) {  // Phi(i) * sum of the line terms (Powell / Brackbill / Janhunen)
