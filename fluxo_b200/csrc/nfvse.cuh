@@ -1,5 +1,6 @@
 // NFVSE shock capturing (shockcapturing/nfvse.f90, nfvse_mpi.f90, indicators/indicators.f90) on
-// the sm_100a path, LGL nodes, first-order subcell finite volumes (SubFVMethod = 1):
+// the sm_100a path for the Euler / Navier-Stokes and the MHD systems, LGL nodes, first-order
+// (SubFVMethod = 1) or TVD (SubFVMethod = 2) subcell finite volumes:
 //   alpha_kernel      Persson-Peraire indicator of rho*p (or rho, p, kinetic energy) from its modal
 //                     Legendre coefficients, alpha = 1/(1+exp(-s (eta-T)/T)), clipping;
 //   propagate_kernel  alpha_e = max(alpha_e, SpacePropFactor * max over its sides of the two
