@@ -26,6 +26,18 @@ class FluxoError(RuntimeError):
         self.code = code
 
 
+class FluxoExact(ctypes.Structure):
+    _fields_ = [
+        ("func", ctypes.c_int),
+        ("adv_vel", ctypes.c_double * 3),
+        ("ini_wavenumber", ctypes.c_double * 3),
+        ("ini_amplitude", ctypes.c_double),
+        ("ini_frequency", ctypes.c_double),
+        ("ref_state_prim", ctypes.c_double * 5),
+        ("ini_center", ctypes.c_double * 3),
+    ]
+
+
 class FluxoCfg(ctypes.Structure):
     _fields_ = [
         ("struct_size", ctypes.c_int),
@@ -80,7 +92,7 @@ EXPORTS = [
     "fluxo_gpu_last_error", "fluxo_gpu_set_profiling", "fluxo_gpu_get_profile", "fluxo_gpu_fp64_peak",
     "fluxo_host_box_sizes", "fluxo_host_box_mesh", "fluxo_host_exact_func", "fluxo_gpu_dg_time_derivative_noalloc",
     "fluxo_gpu_set_glm_ch", "fluxo_gpu_get_glm_ch", "fluxo_gpu_get_alpha", "fluxo_gpu_volume_shape",
-    "fluxo_gpu_set_volume_shape",
+    "fluxo_gpu_set_volume_shape", "fluxo_gpu_analyze",
     "fluxo_batch_create", "fluxo_batch_add", "fluxo_batch_run", "fluxo_batch_status", "fluxo_batch_get_state",
     "fluxo_batch_set_state",
     "fluxo_batch_remove", "fluxo_batch_info", "fluxo_batch_stream", "fluxo_batch_instance_bytes",
@@ -129,6 +141,7 @@ def load():
     lib.fluxo_gpu_get_alpha.argtypes = [vp, vp]
     lib.fluxo_gpu_volume_shape.argtypes = [i, i, i, P(i), P(i), P(i), P(i)]
     lib.fluxo_gpu_set_volume_shape.argtypes = [i, i, i, i]
+    lib.fluxo_gpu_analyze.argtypes = [vp, d, P(FluxoExact), vp, vp, vp, vp]
     sz = ctypes.c_size_t
     lib.fluxo_batch_create.argtypes = [i, P(vp)]
     lib.fluxo_batch_add.argtypes = [vp, P(FluxoCfg), i, i] + [vp] * 11 + [d, d, i, P(i)]

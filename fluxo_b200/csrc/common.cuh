@@ -12,6 +12,7 @@
 //   e2s            [elem][6][2]                 ElemToSide, 0-based side ids
 // node = i + (N+1)*(j + (N+1)*k).
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -124,6 +125,22 @@ __device__ __forceinline__ double glm_ch(const KParams& P) { return P.chDev ? *P
 // caller's side: only addresses inside live allocations are passed).
 __device__ __forceinline__ void prefetch_l2(const void* p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// Raises kernel k's dynamic shared-memory limit to `bytes` on the current device.  The attribute
+// belongs to (kernel, device), so `done` keeps one bit per device ordinal < 64 (a launcher passes a
+// function-local static per kernel instantiation); concurrent first calls from several host threads
+// both set the attribute, which is harmless.  Ordinals >= 64 set it on every call.
+template <class K>
+inline cudaError_t smem_attr_once(K* k, size_t bytes, std::atomic<unsigned long long>& done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = (dev >= 0 && dev < 64) ? (1ull << dev) : 0ull;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
+  return e;
 }
 
 }  // namespace fluxo

@@ -98,6 +98,8 @@ struct fluxo_handle {
   TDState* dTD = nullptr;
   unsigned long long* dDtBits = nullptr;
   int* dErrKey = nullptr;
+  // analysis (fluxo_gpu_analyze): per-element partial sums, results, interpolation tables
+  double *dAnaPartial = nullptr, *dAnaRes = nullptr, *dAnaTables = nullptr;
   int nStages = 0;
   double RKA[8]{}, RKb[8]{}, RKc[8]{};
   double CFLScale = 0., DFLScale = 0.;
@@ -495,6 +497,10 @@ int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* S2E, 
                          met, geo, rerr))
     return fail(h, FLUXO_EINVAL_CFG, "set_mesh: " + rerr);
   h->nElems = nElems; h->nSides = nSides;
+  if (h->dAnaPartial) {  // sized by nElems at the next analysis
+    cudaFree(h->dAnaPartial);
+    h->dAnaPartial = nullptr;
+  }
   const int NV = h->nVar;
   const size_t nU = (size_t)NV * NP3 * nElems, nF = (size_t)NV * NPT * nSides;
   const size_t nFlux = (size_t)(h->mhd ? 13 : 5) * NPT * nSides;  // MHD: + non-conservative weights
@@ -686,6 +692,76 @@ int fluxo_gpu_time_disc(fluxo_handle* h, double t, double tEnd, int maxIter, dou
   }
 }
 
+int fluxo_gpu_analyze(fluxo_handle* h, double t, const fluxo_exact* ex, double* L2, double* Linf, double* L2colloc,
+                      double* scalars) {
+  int r = check_ready(h);
+  if (r) return r;
+  const int func = ex ? ex->func : 0;
+  if (func != 0) {
+    if (h->mhd) return fail(h, FLUXO_EINVAL_CFG, "analyze: error norms need an Euler / Navier-Stokes exact function");
+    if (func != 1 && func != 2 && func != 4 && func != 7 && func != 14)
+      return fail(h, FLUXO_EINVAL_CFG, "analyze: exact function must be 1, 2, 4, 7 or 14");
+    if (!h->haveXGP) return fail(h, FLUXO_EINVAL_CFG, "analyze: error norms need Elem_xGP at set_mesh");
+  }
+  // DGTimeDerivative(t) before Analyze (timedisc.f90:387): Ut and the gradients of the current U
+  KParams P = base_params(h);
+  P.stage = 0;
+  P.t = t;
+  P.grad = h->dGrad;
+  if ((r = rhs(h, P))) return r;
+  const int NP = h->NP, NA1 = 2 * NP + 1, NV = h->nVar, K = 3 * NV + 5;
+  if (!h->dAnaTables) {  // LGL weights (NP), interpolation N -> NAnalyze [NA1][NP], NAnalyze weights (NA1)
+    std::vector<double> xa, wa;
+    host::lgl(2 * NP, xa, wa);  // NAnalyze = 2(N+1), InitAnalyzeBasis (analyze.f90)
+    std::vector<double> xg(h->hb.xGP, h->hb.xGP + NP), V = host::interp_matrix(xg, xa);
+    std::vector<double> tab;
+    tab.insert(tab.end(), h->hb.wGP, h->hb.wGP + NP);
+    tab.insert(tab.end(), V.begin(), V.end());
+    tab.insert(tab.end(), wa.begin(), wa.end());
+    if ((r = dalloc(h, &h->dAnaTables, tab.size())) || (r = dalloc(h, &h->dAnaRes, (size_t)K))) return r;
+    FLUXO_CUDA(h, cudaMemcpyAsync(h->dAnaTables, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice, h->stream));
+    FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));  // tab is a host temporary
+  }
+  if (!h->dAnaPartial && (r = dalloc(h, &h->dAnaPartial, (size_t)h->nElems * K))) return r;
+  AnalyzeArgs A{};
+  A.nElems = h->nElems; A.NP = NP; A.NA1 = NA1; A.nVar = NV; A.K = K;
+  A.mhd = h->mhd ? 1 : 0;
+  A.func = func;
+  A.t = t;
+  A.U = h->dU; A.Ut = h->dUt; A.sJ = h->dsJ; A.xGP = h->dXGP;
+  A.grad = (h->visc && !h->mhd) ? h->dGrad : nullptr;
+  A.wGP = h->dAnaTables; A.V = A.wGP + NP; A.wA = A.V + (size_t)NA1 * NP;
+  A.kappa = h->cfg.kappa; A.kappaM1 = h->cfg.kappa - 1.; A.sKappaM1 = 1. / (h->cfg.kappa - 1.);
+  A.s2mu_0 = h->mhd ? 0.5 / h->cfg.mu_0 : 0.;
+  if (ex) {
+    for (int v = 0; v < 5; ++v) A.refPrim[v] = ex->ref_state_prim[v];
+    for (int d = 0; d < 3; ++d) {
+      A.advVel[d] = ex->adv_vel[d]; A.waveNumber[d] = ex->ini_wavenumber[d]; A.center[d] = ex->ini_center[d];
+    }
+    A.amplitude = ex->ini_amplitude; A.frequency = ex->ini_frequency;
+  }
+  A.partial = h->dAnaPartial;
+  FLUXO_CUDA(h, launch_analyze(A, h->dAnaRes, h->stream));
+  h->launches += 2;
+  std::vector<double> res(K);
+  FLUXO_CUDA(h, cudaMemcpyAsync(res.data(), h->dAnaRes, K * 8, cudaMemcpyDeviceToHost, h->stream));
+  FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
+  const double Vol = res[3 * NV + 4];
+  for (int v = 0; v < NV; ++v) {  // analyze.f90:627-629: L2 = sqrt(sum / Vol)
+    if (L2) L2[v] = func ? std::sqrt(res[v] / Vol) : 0.;
+    if (L2colloc) L2colloc[v] = func ? std::sqrt(res[NV + v] / Vol) : 0.;
+    if (Linf) Linf[v] = func ? res[2 * NV + v] : 0.;
+  }
+  if (scalars) {
+    scalars[0] = res[3 * NV] * A.sKappaM1;
+    scalars[1] = res[3 * NV + 1];
+    scalars[2] = res[3 * NV + 2] / Vol;
+    scalars[3] = res[3 * NV + 3] / Vol;
+    scalars[4] = Vol;
+  }
+  return FLUXO_OK;
+}
+
 int fluxo_gpu_set_glm_ch(fluxo_handle* h, double ch) {
   if (!h) return FLUXO_EINVAL_CFG;
   if (!h->mhd) return fail(h, FLUXO_EINVAL_CFG, "GLM_ch exists for MHD only");
@@ -809,7 +885,8 @@ int fluxo_gpu_destroy(fluxo_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   void* ptrs[] = {h->dBasis, h->dU, h->dUt, h->dUtTmp, h->dGrad, h->dUtVisc, h->dMetrics, h->dsJ, h->dFaceGeo, h->dXGP,
                   h->dFlux, h->dLFlux, h->dGTrace, h->dS2E, h->dE2S, h->dTD, h->dDtBits, h->dErrKey,
-                  h->dAlpha, h->dAlphaRaw, h->dAlphaTmp, h->dFV, h->dSVdm, h->dBlendList, h->dBlendCount};
+                  h->dAlpha, h->dAlphaRaw, h->dAlphaTmp, h->dFV, h->dSVdm, h->dBlendList, h->dBlendCount,
+                  h->dAnaPartial, h->dAnaRes, h->dAnaTables};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);

@@ -390,6 +390,16 @@ extern "C" int fluxo_host_exact_func(int func, double t, size_t np, const double
                                            2. * std::cos(2. * X[0]) + std::cos(2 * X[1]) * std::cos(2. * X[2]));
         break;
       }
+      case 14: {  // soft Sedov-Taylor blast around IniCenter = 0 (its default), navierstokes/equation.f90:906-922
+        const double r2 = std::sqrt(X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
+        prim[0] = 1.; prim[1] = prim[2] = prim[3] = 0.; prim[4] = 1.;
+        if (r2 <= 0.5 && r2 != 0.) {
+          prim[0] = 1.3416149068323;
+          for (int d = 0; d < 3; ++d) prim[1 + d] = 0.361538208967199 * X[d] / r2;
+          prim[4] = 1.51333333333333;
+        }
+        break;
+      }
       default:
         return FLUXO_EINVAL_CFG;
     }

@@ -29,7 +29,7 @@ __device__ __forceinline__ int boundary_sides(int i, int j, int k, int N, int* s
 // prolongtoface.f90:43-132, fillflux.f90:41-110, riemann.f90:104-246.
 // ------------------------------------------------------------------------------------------------
 template <int RS, bool VISC>
-__global__ void face_flux_kernel(KParams P, int NP) {
+__device__ __forceinline__ void face_flux_body(const KParams& P, int NP) {
   if (halted(P)) return;
   const int npts = NP * NP;
   const int spb = blockDim.x / npts;
@@ -93,6 +93,13 @@ __global__ void face_flux_kernel(KParams P, int NP) {
   double* out = P.flux + (size_t)side * 5 * npts + pt;
 #pragma unroll
   for (int v = 0; v < 5; ++v) out[v * npts] = F[v] * se;
+}
+
+// One thread per face point, 128 threads per block; MINB resident blocks per SM bound the registers
+// (the memory-bound face pass needs enough warps in flight to cover the DRAM latency).
+template <int RS, bool VISC, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) face_flux_kernel(KParams P, int NP) {
+  face_flux_body<RS, VISC>(P, NP);
 }
 
 // ------------------------------------------------------------------------------------------------

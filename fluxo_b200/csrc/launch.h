@@ -70,6 +70,23 @@ cudaError_t launch_nfvse_alpha(int NP, bool mhd, int nElems, cudaStream_t s, con
 cudaError_t launch_nfvse_fv(int RS, int NP, int nElems, int nSMs, cudaStream_t s, const KParams& P);
 cudaError_t launch_nfvse_fv_ns(int RS, int NP, int nElems, int nSMs, cudaStream_t s, const KParams& P);
 
+// Analysis of a state (analyze.cu): per-element partial sums partial[nElems][K] with
+// K = 3*nVar + 5: L2 error (nVar), collocation L2 error (nVar), L_inf error (nVar), entropy, dS/dU.Ut,
+// kinetic energy, enstrophy, volume (unnormalised); res[K] receives their sums / maxima.
+struct AnalyzeArgs {
+  int nElems, NP, NA1, nVar, K;
+  int mhd;
+  int func;                          // exact function of the error norms (0: none)
+  double t;
+  const double *U, *Ut, *sJ, *xGP, *grad;  // Ut, xGP, grad may be null
+  const double *wGP, *V, *wA;        // LGL weights, N -> NAnalyze interpolation [NA1][NP], NAnalyze weights
+  double kappa, kappaM1, sKappaM1, s2mu_0;
+  double refPrim[5], advVel[3], waveNumber[3], center[3], amplitude, frequency;
+  double* partial;
+};
+size_t analyze_smem_bytes(int NP, int nVar, int threads);
+cudaError_t launch_analyze(const AnalyzeArgs& A, double* res, cudaStream_t s);
+
 // Host helpers of fluxo_gpu.cu for entry points without a handle: the per-N operator tables, and
 // the message that fluxo_gpu_last_error(NULL, ...) returns (returns `code`).
 void basis_tables_for(int N, BasisTables& B);

@@ -9,13 +9,9 @@ template <int NP, int LIFT, int LV>
 static cudaError_t lv_t(int nElems, cudaStream_t s, const KParams& P) {
   constexpr int EPB = lv_epb<NP>();
   constexpr size_t smem = lv_smem_bytes<NP>();
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(lift_visc_kernel<NP, LIFT, LV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  cudaError_t e = smem_attr_once(lift_visc_kernel<NP, LIFT, LV>, smem, attr);
+  if (e != cudaSuccess) return e;
   lift_visc_kernel<NP, LIFT, LV><<<(nElems + EPB - 1) / EPB, EPB * NP * NP * NP, smem, s>>>(P);
   return cudaGetLastError();
 }

@@ -25,7 +25,8 @@ cudaError_t lift_visc_np(int nElems, cudaStream_t s, const KParams& P) {
   constexpr int EPB = mhd::epb<NP>();
   constexpr size_t smem = mhd::lv_smem_bytes<NP>();
   auto k = mhd::lift_visc_kernel<NP, LIFT>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  static std::atomic<unsigned long long> attr{0};
+  cudaError_t e = smem_attr_once(k, smem, attr);
   if (e != cudaSuccess) return e;
   k<<<(nElems + EPB - 1) / EPB, EPB * NP * NP * NP, smem, s>>>(P);
   return cudaGetLastError();

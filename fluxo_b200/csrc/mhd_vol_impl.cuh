@@ -11,7 +11,8 @@ cudaError_t volume_np(int nElems, cudaStream_t s, const KParams& P) {
   constexpr int EPB = mhd::epb<NP>();
   constexpr size_t smem = mhd::vol_smem_bytes<NP, VF>();
   auto k = mhd::volume_kernel<NP, VF>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  static std::atomic<unsigned long long> attr{0};
+  cudaError_t e = smem_attr_once(k, smem, attr);
   if (e != cudaSuccess) return e;
   k<<<(nElems + EPB - 1) / EPB, mhd::vol_threads<NP>(), smem, s>>>(P);
   return cudaGetLastError();

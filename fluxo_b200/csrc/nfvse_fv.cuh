@@ -10,7 +10,8 @@ template <bool MHD, int NP, int RS>
 cudaError_t fv_np(int grid, cudaStream_t s, const KParams& P) {
   constexpr size_t smem = fv_smem_bytes<NP>();
   auto k = fv_kernel<NP, RS, MHD>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  static std::atomic<unsigned long long> attr{0};
+  cudaError_t e = smem_attr_once(k, smem, attr);
   if (e != cudaSuccess) return e;
   k<<<grid, NP * NP * NP, smem, s>>>(P);
   return cudaGetLastError();

@@ -13,8 +13,9 @@
 // face-flux buffer and the operator tables live in g_noalloc_scratch.  Every call on a device
 // shares that array, so calls whose GPU work overlaps (different streams, different host threads)
 // race on it; the call synchronises its stream before it returns, so calls from one host thread
-// never overlap.  No byte of the scratch has to start at zero: each call writes the operator
-// tables and every face flux before any kernel reads them.
+// never overlap.  No byte of the scratch has to start at zero: the operator tables are written by
+// the first call at each N (a call at another N overwrites them) and every call writes every face
+// flux before the volume kernel reads it.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -39,6 +40,7 @@ static_assert(kTablesBytes == 2304, "the scratch size formula in fluxo_gpu.h sta
 
 std::mutex g_mutex;
 void* g_scratch[kMaxDevices];       // device address of g_noalloc_scratch, looked up once per device
+int g_scratch_N[kMaxDevices];       // N whose operator tables the device's scratch holds (0: none yet)
 BasisTables g_tables[8];            // host copies of the operator tables per N (static storage)
 bool g_tables_built[8];
 
@@ -79,6 +81,7 @@ extern "C" int fluxo_gpu_dg_time_derivative_noalloc(const fluxo_cfg* cfg, int nE
   if (cfg->N < 1 || cfg->N > 7) return bad(FLUXO_EINVAL_CFG, "N must be in 1..7");
   if (cfg->eqn != FLUXO_EQN_EULER) return bad(FLUXO_EINVAL_CFG, "only the Euler equations (eqn 0) are supported");
   if (cfg->ini_exact_func == 4) return bad(FLUXO_EINVAL_CFG, "the source term (IniExactFunc 4) is not supported");
+  if (cfg->nfvse != 0) return bad(FLUXO_EINVAL_CFG, "NFVSE shock capturing (nfvse = 1) is not supported");
   if (!riemann_supported(cfg->riemann)) return bad(FLUXO_EINVAL_CFG, "Riemann solver not implemented");
   if (!volume_flux_supported(cfg->volume_flux)) return bad(FLUXO_EINVAL_CFG, "volume flux not implemented");
   if (!(cfg->kappa > 1.)) return bad(FLUXO_EINVAL_CFG, "kappa must be > 1");
@@ -118,14 +121,26 @@ extern "C" int fluxo_gpu_dg_time_derivative_noalloc(const fluxo_cfg* cfg, int nE
       basis_tables_for(cfg->N, g_tables[cfg->N]);
       g_tables_built[cfg->N] = true;
     }
-    tables = &g_tables[cfg->N];
+    // the tables go up only when the device's scratch holds another N's (a copy from pageable host
+    // memory is staged by the runtime, a fixed cost a caller evaluating many right-hand sides on one
+    // mesh would otherwise pay on every call)
+    if (g_scratch_N[cfg->device] != cfg->N) {
+      tables = &g_tables[cfg->N];
+      g_scratch_N[cfg->device] = cfg->N;
+    }
   }
 
   cudaStream_t s = (cudaStream_t)stream;
   BasisTables* dTables = (BasisTables*)scratch;
   double* dFlux = (double*)((unsigned char*)scratch + kTablesBytes);
-  e = cudaMemcpyAsync(dTables, tables, sizeof(BasisTables), cudaMemcpyHostToDevice, s);
-  if (e != cudaSuccess) return bad(FLUXO_ECUDA, std::string("tables copy: ") + cudaGetErrorString(e));
+  if (tables) {
+    e = cudaMemcpyAsync(dTables, tables, sizeof(BasisTables), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+      std::lock_guard<std::mutex> lk(g_mutex);
+      g_scratch_N[cfg->device] = 0;
+      return bad(FLUXO_ECUDA, std::string("tables copy: ") + cudaGetErrorString(e));
+    }
+  }
 
   KParams P{};
   P.nElems = nElems; P.nSides = nSides;

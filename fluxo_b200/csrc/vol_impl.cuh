@@ -15,13 +15,9 @@ static cudaError_t vol_shape_launch(int nElems, cudaStream_t s, const KParams& P
   constexpr VolShapeId sh = kVolShapes[NP][I];
   constexpr int EPB = sh.epb, LPW = sh.lpw, MINB = sh.minb, OWNSM = sh.ownsm;
   constexpr size_t smem = vol_smem_bytes<NP, VF_ID, EPB, LPW>();
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(volume_kernel<NP, VF_ID, VISC, EPB, LPW, MINB, OWNSM>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static std::atomic<unsigned long long> attr{0};
+  cudaError_t e = smem_attr_once(volume_kernel<NP, VF_ID, VISC, EPB, LPW, MINB, OWNSM>, smem, attr);
+  if (e != cudaSuccess) return e;
   const int grid = (nElems + EPB - 1) / EPB;
   volume_kernel<NP, VF_ID, VISC, EPB, LPW, MINB, OWNSM><<<grid, VolShape<NP, EPB, LPW>::THREADS, smem, s>>>(P);
   return cudaGetLastError();

@@ -52,6 +52,7 @@ class ServeStats:
     rebuilds: int = 0
     max_running: int = 0
     max_bytes: int = 0
+    waited_for_memory: set = field(default_factory=set)  # requests that queued because the budget was full
 
     def dof_updates(self):
         """DOFs x RHS evaluations of all finished requests (5 stages per LSERK4-5 step)."""
@@ -63,7 +64,7 @@ class ServeStats:
                 "dof_updates_per_s": self.dof_updates() / self.wall if self.wall > 0 else None,
                 "p50_s": float(np.percentile(tts, 50)), "p99_s": float(np.percentile(tts, 99)),
                 "mean_s": float(tts.mean()), "max_running": self.max_running, "max_device_bytes": self.max_bytes,
-                "failed": sum(1 for r in self.results if r.err)}
+                "failed": sum(1 for r in self.results if r.err), "waited_for_memory": len(self.waited_for_memory)}
 
 
 class Server:
@@ -93,8 +94,9 @@ class Server:
                              (req.rid, req.nbytes, self.budget))
         self.queue.append(req)
 
-    def admit(self, now):
-        """Adds queued requests in arrival order while they fit the budget; returns how many."""
+    def admit(self, now, stats=None):
+        """Adds queued requests in arrival order while they fit the budget; returns how many.  A request
+        left at the head of the queue waits for memory (recorded in stats.waited_for_memory)."""
         n = 0
         while self.queue and self.used + self.queue[0].nbytes <= self.budget:
             req = self.queue.popleft()
@@ -102,6 +104,8 @@ class Server:
             self.running[iid] = (req, now)
             self.used += req.nbytes
             n += 1
+        if self.queue and stats is not None:
+            stats.waited_for_memory.add(self.queue[0].rid)
         return n
 
     def harvest(self, now, stats):
@@ -127,7 +131,7 @@ class Server:
             now = self.clock() - self._t0
             while pending and pending[0].arrival <= now:
                 self.submit(pending.popleft())
-            if self.admit(now):
+            if self.admit(now, stats):
                 stats.rebuilds += 1
             stats.max_running = max(stats.max_running, len(self.running))
             stats.max_bytes = max(stats.max_bytes, self.used)

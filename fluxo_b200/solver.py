@@ -160,6 +160,28 @@ class DGOperator:
     def dg_time_derivative(self, t=0.0):
         self._check(self.lib.fluxo_gpu_dg_time_derivative(self.h, float(t)))
 
+    def analyze(self, t=0.0, exact=None):
+        """Analysis at time t on the device (fluxo_gpu_analyze): a right-hand side at t, then CalcErrorNorms
+        (when ``exact`` names an exact function: dict with func, adv_vel, ini_wavenumber, ini_amplitude,
+        ini_frequency, ref_state_prim, ini_center), CalcEntropy, dS/dU.Ut and the Taylor-Green integrands."""
+        ex = None
+        if exact is not None and exact.get("func", 0):
+            ex = _lib.FluxoExact()
+            ex.func = int(exact["func"])
+            for k, n in (("adv_vel", 3), ("ini_wavenumber", 3), ("ref_state_prim", 5), ("ini_center", 3)):
+                v = exact.get(k, (0.0,) * n)
+                getattr(ex, k)[:] = [float(z) for z in v]
+            ex.ini_amplitude = float(exact.get("ini_amplitude", 0.0))
+            ex.ini_frequency = float(exact.get("ini_frequency", 1.0))
+        nv = self.nVar
+        L2, Li, Lc, sc = np.zeros(nv), np.zeros(nv), np.zeros(nv), np.zeros(5)
+        self._check(self.lib.fluxo_gpu_analyze(self.h, float(t), None if ex is None else ctypes.byref(ex), _ptr(L2),
+                                               _ptr(Li), _ptr(Lc), _ptr(sc)))
+        out = {"entropy": sc[0], "dSdU_Ut": sc[1], "ekin": sc[2], "enstrophy": sc[3], "volume": sc[4]}
+        if ex is not None:
+            out.update(L2=L2, Linf=Li, L2_colloc=Lc)
+        return out
+
     def calc_timestep(self):
         dt, err = ctypes.c_double(), ctypes.c_int()
         r = self.lib.fluxo_gpu_calc_timestep(self.h, ctypes.byref(dt), ctypes.byref(err))

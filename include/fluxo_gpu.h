@@ -2,7 +2,8 @@
  * fluxo_gpu.h — C ABI of the B200 (sm_100a, FP64) DGSEM right-hand side and
  * LSERK time step.  It is the drop-in boundary for the reference's
  * DGTimeDerivative / TimeStep / CALCTIMESTEP path: a Fortran host binds these
- * entry points with ISO_C_BINDING and keeps its own
+ * entry points with ISO_C_BINDING (a TYPE, BIND(C) that mirrors fluxo_cfg field
+ * for field, and one INTERFACE block per entry point) and keeps its own
  * parameter.ini parsing, mesh reading, analysis and output.
  *
  * Conventions
@@ -148,6 +149,38 @@ int fluxo_gpu_get_glm_ch(fluxo_handle* h, double* ch);
  * (src/shockcapturing/nfvse_vars.f90). */
 int fluxo_gpu_get_alpha(fluxo_handle* h, double* alpha);
 
+/* Exact function of the error norms (the reference's AnalyzeExactFunc with the IniExactFunc
+ * parameters, src/equation/navierstokes/equation.f90:575-811): func 0 none, 1 constant reference
+ * state (ref_state_prim: rho, u, v, w, p), 2 density sine wave (adv_vel, ini_wavenumber,
+ * ini_amplitude), 4 manufactured solution (ini_amplitude, ini_frequency), 7 Taylor-Green vortex,
+ * 14 soft Sedov-Taylor blast (ini_center). */
+typedef struct fluxo_exact {
+  int func;
+  double adv_vel[3];
+  double ini_wavenumber[3];
+  double ini_amplitude, ini_frequency;
+  double ref_state_prim[5];
+  double ini_center[3];
+} fluxo_exact;
+
+/* Analysis of the device state at time t, reduced on the device.  Like the reference's TimeDisc at an
+ * analyze point (src/timedisc/timedisc.f90:387-404: DGTimeDerivative(t), then Analyze), it first
+ * evaluates the right-hand side at t (Ut and, for Navier-Stokes, the gradients are then those of the
+ * current U), then reduces:
+ *   L2, Linf, L2colloc (nVar each; ex->func != 0, Euler / Navier-Stokes, needs Elem_xGP at set_mesh):
+ *     CalcErrorNorms (src/analyze/analyze.f90:557-632) on NAnalyze = 2(N+1) LGL points per direction
+ *     and at the collocation points;
+ *   scalars[0] entropy: sum of -rho (log p - kappa log rho)/(kappa-1) * wGPVol/sJ (CalcEntropy,
+ *     navierstokes/analyze_equation.f90:549-599; MHD: mhd/analyze_equation.f90:421-470);
+ *   scalars[1] dS/dU . Ut: the entropy production of the right-hand side, sum of W(U).Ut wGPVol/sJ;
+ *   scalars[2] kinetic energy 1/Vol sum 1/2 rho |v|^2, scalars[3] enstrophy 1/Vol sum 1/2 rho |curl v|^2
+ *     (Navier-Stokes, from the lifted velocity gradients; 0 otherwise): the Taylor-Green integrands of
+ *     src/testcase/taylorgreenvortex/testcase_analyze.f90:127-330;
+ *   scalars[4] the domain volume Vol.
+ * Any output may be NULL.  The reductions run in a fixed order (the result is reproducible). */
+int fluxo_gpu_analyze(fluxo_handle* h, double t, const fluxo_exact* ex, double* L2, double* Linf, double* L2colloc,
+                      double* scalars);
+
 /* Device pointers and stream for zero-copy callers (e.g. torch tensors):
  * U, Ut are device buffers of nVar*(N+1)^3*nElems doubles in the host layout. */
 int fluxo_gpu_device_buffers(fluxo_handle* h, double** dU, double** dUt, void** stream);
@@ -180,18 +213,24 @@ int fluxo_gpu_fp64_peak(int device, double* tflops);
  * allocate while they run (e.g. a host code that reserves one arena of HBM at start-up and
  * evaluates the right-hand side on its own vectors), which therefore cannot create a handle;
  * cudaMalloc would fail once the arena holds the memory, and cudaFree synchronises the device.
- * Same kernels and results as fluxo_gpu_dg_time_derivative for eqn = FLUXO_EQN_EULER (no source
- * term).  Arrays are device memory of cfg->device in the device layouts of fluxo_gpu_set_mesh:
+ * Same kernels and results as fluxo_gpu_dg_time_derivative for eqn = FLUXO_EQN_EULER without a
+ * source term and without NFVSE (ini_exact_func = 4 or nfvse = 1 return FLUXO_EINVAL_CFG).
+ * Arrays are device memory of cfg->device in the device layouts of fluxo_gpu_set_mesh:
  *   dU, dUt  (nVar,0:N,0:N,0:N,nElems) as U;  dsJ (0:N,0:N,0:N,nElems)
  *   dMetrics [elem][9][node]: Metrics_f/g/hTilde (x,y,z) each, node = i+(N+1)(j+(N+1)k) fastest
  *   dFaceGeo [side][10][pt]: NormVec, TangVec1, TangVec2 (x,y,z), SurfElem; pt = p+(N+1)q fastest
  *   dS2E [side][5]: SideToElem with 0-based element ids;  dE2S [elem][6][2]: 0-based side id, flip.
+ * The connectivity is not checked (it is device memory): it must be a mesh that fluxo_gpu_set_mesh
+ * accepts, with element ids in [0,nElems), side ids in [0,nSides), local sides 1..6 and flips 0..4;
+ * other ids make the kernels read and write outside the arrays.
  * The face fluxes and operator tables live in one static device array of
  * FLUXO_NOALLOC_SCRATCH_BYTES shared by all calls on a device: it needs
  * 2304 + nSides*5*(N+1)^2*8 bytes (N=7: about 3270 sides; N=3: about 13100 sides), larger
  * meshes return FLUXO_EINVAL_CFG.  Calls whose GPU work overlaps (other streams or host threads)
  * race on that array; the call runs on `stream` (NULL: the legacy default stream) and
- * synchronises it before returning.  Errors: fluxo_gpu_last_error(NULL, ...). */
+ * synchronises it before returning.  The first call on a device looks up the array's device
+ * address, and the first call at each N copies that N's operator tables into it.
+ * Errors: fluxo_gpu_last_error(NULL, ...). */
 #define FLUXO_NOALLOC_SCRATCH_BYTES (8u * 1024u * 1024u)
 int fluxo_gpu_dg_time_derivative_noalloc(const fluxo_cfg* cfg, int nElems, int nSides, const double* dU,
                                          double* dUt, const double* dMetrics, const double* dsJ,
@@ -252,7 +291,8 @@ int fluxo_host_box_mesh(int N, const int* nElemsXYZ, const double* xmin, const d
                         double* Metrics_gTilde, double* Metrics_hTilde, double* sJ, double* NormVec,
                         double* TangVec1, double* TangVec2, double* SurfElem, double* Elem_xGP);
 /* FillIni(IniExactFunc, U) on the given node coordinates (src/equation/navierstokes/equation.f90:575-950):
- * IniExactFunc 1 (constant refstate, prim given), 2 (density sine wave), 4 (manufactured), 7 (Taylor-Green). */
+ * IniExactFunc 1 (constant refstate, prim given), 2 (density sine wave), 4 (manufactured), 7 (Taylor-Green),
+ * 14 (soft Sedov-Taylor blast around IniCenter = 0). */
 int fluxo_host_exact_func(int func, double t, size_t nPoints, const double* x, double kappa,
                           const double* adv_vel, double ini_amplitude, const double* ini_wavenumber,
                           double ini_frequency, const double* ref_state_prim, double* U);

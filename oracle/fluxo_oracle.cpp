@@ -1288,6 +1288,19 @@ void ExactFunc(const Case& C, int func, double t, const double* x, double* resu)
       PrimToCons(C, prim, resu);
       return;
     }
+    case 14: {  // soft Sedov-Taylor blast, equation.f90:906-922 (dim_ = 3)
+      double nx[3], r2 = 0.;
+      for (int d = 0; d < 3; ++d) { nx[d] = x[d] - P.ini_center[d]; r2 += nx[d] * nx[d]; }
+      r2 = std::sqrt(r2);
+      prim[0] = 1.; prim[1] = prim[2] = prim[3] = 0.; prim[4] = 1.;
+      if (r2 <= 0.5 && r2 != 0.) {
+        prim[0] = 1.3416149068323;
+        for (int d = 0; d < 3; ++d) prim[1 + d] = 0.361538208967199 * nx[d] / r2;
+        prim[4] = 1.51333333333333;
+      }
+      PrimToCons(C, prim, resu);
+      return;
+    }
     default: throw std::runtime_error("ExactFunc not implemented in oracle");
   }
 }

@@ -1,0 +1,115 @@
+"""Parity on the benchmarked configurations at their full sizes, built exactly as bench.py builds them.
+
+The Navier-Stokes Taylor-Green workload (32^3 curved hexahedra, N=7, 16.8 M DOFs, BR1 of the entropy
+variables, EC-KEP volume flux, matrix-dissipation surface flux) and the resistive-MHD Orszag-Tang
+workload (24^3 curved hexahedra, N=4, Derigs EC volume flux, 9-wave entropy-stable surface flux,
+Powell terms, NFVSE from the indicator) are set up through the product's own host setup
+(fluxo_host_box_mesh, FillIni) and compared with the oracle on the same metrics and state: one
+DGTimeDerivative and one device-resident LSERK4-5 step.
+
+Tolerances: relative L2 <= 1e-12 for the Navier-Stokes workload (Ut of a 5 %-perturbed state, the
+energy part of Ut of the workload's own state and the state after one time step; the momentum part of
+that Ut is nearly zero by construction and is held to 1e-9); for the MHD workload 1e-10 on Ut,
+because its 9-wave solver's eigenvectors are ill-conditioned where the averaged B is almost normal
+to a face (in the oracle alone a relative perturbation of U of 1e-16 moves Ut by 4e-11), with the
+blending coefficients alpha to 1e-12.  The MHD state carries 5 % node noise on the density so that the
+shock indicator blends elements (the smooth initial vortex blends none); the test requires blending."""
+import numpy as np
+import pytest
+
+import bench
+import fluxo_b200 as fb
+from oracle.oracle import OracleCase
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    return np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300)
+
+
+def oracle_on(mesh, U, **kw):
+    """An oracle case on the product's mesh arrays: its own periodic-box connectivity (checked equal) and
+    the product's metrics and state."""
+    c = OracleCase(**kw)
+    m = c.mesh()
+    assert np.array_equal(m["SideToElem"], mesh["SideToElem"]) and np.array_equal(m["ElemToSide"], mesh["ElemToSide"])
+    c.set_metrics(mesh)
+    c.set_U(U)
+    return c
+
+
+def test_tgv_workload_full_size(gpu_lib):
+    w = bench.workload()
+    mesh = fb.box_mesh(w["N"], w["elems"], w["xmin"], w["xmax"], NGeo=w["NGeo"], deform_amp=w["deform_amp"])
+    U0 = fb.exact_func(7, 0.0, mesh["Elem_xGP"], kappa=w["kappa"])
+    op = fb.DGOperator(N=w["N"], eqn=1, riemann=w["riemann"], volume_flux=w["volume_flux"], lifting=1, lifting_var=3,
+                       visc=0, mu0=w["mu0"], Pr=w["Pr"], kappa=w["kappa"], cfl_scale=w["cfl_scale"],
+                       dfl_scale=w["dfl_scale"], time_disc=0)
+    op.set_mesh(mesh)
+    op.set_state(U0)
+    c = oracle_on(mesh, U0, N=w["N"], nElems=w["elems"], xmin=w["xmin"], xmax=w["xmax"], NGeo=w["NGeo"],
+                  deform_amp=w["deform_amp"], eqn=1, lifting=1, lifting_var=3, mu0=w["mu0"], Pr=w["Pr"],
+                  kappa=w["kappa"], riemann=w["riemann"], volume_flux=w["volume_flux"], ini_exact_func=7,
+                  cfl_scale=w["cfl_scale"], dfl_scale=w["dfl_scale"])
+    del mesh
+    # the workload's own state: the Taylor-Green pressure balances the advection, so the momentum part
+    # of Ut is ~1e-10 of the flux terms it is summed from; those components agree to the roundoff of
+    # the terms (GPU and oracle sum in different orders), the energy part to 1e-12 of itself
+    ref = c.dg_time_derivative(0.0)
+    op.dg_time_derivative(0.0)
+    ut = op.get_ut()
+    assert rel_l2(ut[..., 4], ref[..., 4]) <= 1e-12
+    assert rel_l2(ut, ref) <= 1e-9
+    # a 5 %-perturbed state on the same mesh: a right-hand side of the size of its terms, 1e-12
+    Up = U0 * (1 + 0.05 * np.random.default_rng(5).standard_normal(U0.shape))
+    c.set_U(Up)
+    op.set_state(Up)
+    ref = c.dg_time_derivative(0.0)
+    op.dg_time_derivative(0.0)
+    assert rel_l2(op.get_ut(), ref) <= 1e-12
+    del ref, ut, Up
+    c.set_U(U0)
+    op.set_state(U0)
+    dt_ref, e_ref = c.calc_timestep()
+    t_ref, n_ref = c.run(0.0, 1e9, max_iter=1)
+    t, n, err = op.time_disc(0.0, 1e9, 1)
+    assert err == e_ref == 0 and n == n_ref == 1 and t == pytest.approx(t_ref, rel=1e-13)
+    assert t == pytest.approx(dt_ref, rel=1e-13)
+    assert rel_l2(op.get_state(), c.get_U()) <= 1e-12
+    op.close()
+
+
+def test_mhd_workload_full_size_blending(gpu_lib):
+    from fluxo_b200.workloads import mhd_orszag_tang_state
+
+    w = bench.mhd_workload()
+    mesh = fb.box_mesh(w["N"], w["elems"], w["xmin"], w["xmax"], NGeo=w["NGeo"], deform_amp=w["deform_amp"])
+    U0 = mhd_orszag_tang_state(mesh["Elem_xGP"], kappa=w["kappa"])
+    U0[..., 0] *= 1.0 + 0.05 * np.random.default_rng(11).standard_normal(U0[..., 0].shape)
+    fields = {k: v for k, v in w.items() if k not in ("elems", "xmin", "xmax", "NGeo", "deform_amp")}
+    op = fb.DGOperator(**fields)
+    op.set_mesh(mesh)
+    op.set_state(U0)
+    okw = dict(N=w["N"], nElems=w["elems"], xmin=w["xmin"], xmax=w["xmax"], NGeo=w["NGeo"], deform_amp=w["deform_amp"],
+               eqn=3, kappa=w["kappa"], eta=w["eta"], mu0=0.0, lifting=1, lifting_var=3, volume_flux=10, riemann=14,
+               noncons=1, nc_glm=0, nfvse=1, compute_alpha=1, alpha_max=w["alpha_max"], alpha_min=w["alpha_min"],
+               space_prop_sweeps=w["space_prop_sweeps"], ini_exact_func=0, glm_scale=0.5, cfl_scale=w["cfl_scale"],
+               dfl_scale=w["dfl_scale"])
+    c = oracle_on(mesh, U0, **okw)
+    del mesh
+    dt_ref, e_ref = c.calc_timestep()
+    dt, e = op.calc_timestep()
+    assert e == e_ref == 0 and dt == pytest.approx(dt_ref, rel=1e-13)
+    c.glm_ch = op.glm_ch
+    ref = c.dg_time_derivative(0.0)
+    op.dg_time_derivative(0.0)
+    a, a_ref = op.alpha(), c.alpha()
+    assert (a_ref > 0).sum() > 0.05 * a.size, "the indicator must blend elements"
+    assert np.abs(a - a_ref).max() <= 1e-12
+    assert rel_l2(op.get_ut(), ref) <= 1e-10
+    t_ref, n_ref = c.run(0.0, 1e9, max_iter=1)
+    t, n, err = op.time_disc(0.0, 1e9, 1)
+    assert err == 0 and n == n_ref == 1 and t == pytest.approx(t_ref, rel=1e-13)
+    assert rel_l2(op.get_state(), c.get_U()) <= 1e-10
+    op.close()

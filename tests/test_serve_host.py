@@ -69,8 +69,8 @@ def make_requests(n, seed=0):
 
 
 class CountingServer(Server):
-    def admit(self, now):
-        n = super().admit(now)
+    def admit(self, now, stats=None):
+        n = super().admit(now, stats)
         assert self.used <= self.budget
         return n
 
@@ -93,6 +93,8 @@ def test_admission_respects_budget_and_order():
         assert r.dofs == req.mesh["ElemToSide"].shape[0] * 64
     s = stats.summary()
     assert s["requests"] == 40 and s["p99_s"] >= s["p50_s"] >= 0 and s["failed"] == 0
+    # the budget holds a few requests at a time: later ones waited for memory, and the count says so
+    assert 0 < s["waited_for_memory"] < 40 and stats.max_running < 40
 
 
 def test_request_larger_than_budget_is_refused():
