@@ -90,7 +90,7 @@ struct Group {
   int N = 0, NP = 0;
   bool visc = false;
   int nStages = 0;
-  double RKA[8]{}, RKb[8]{}, RKc[8]{}, CFLScale = 0., DFLScale = 0.;
+  double RKA[24]{}, RKb[24]{}, RKc[24]{}, CFLScale = 0., DFLScale = 0.;
   int nElems = 0, nSides = 0;
   std::vector<int> members;                   // instance ids in placement order
   int slot0 = 0;                              // members own instance slots slot0 .. slot0+members-1
@@ -441,7 +441,10 @@ int check_cfg(const fluxo_cfg* c, std::string& msg) {
   }
   if (!(c->kappa > 1.)) { msg = "kappa must be > 1"; return FLUXO_EINVAL_CFG; }
   if (c->ini_exact_func == 4) { msg = "source terms are not supported in batches"; return FLUXO_EINVAL_CFG; }
-  if (c->time_disc != 0 && c->time_disc != 1) { msg = "time_disc must be 0 or 1"; return FLUXO_EINVAL_CFG; }
+  if (c->time_disc < 0 || c->time_disc > 5) {  // the fused stage update serves the LSERKW2 schemes 0..5
+    msg = "batched solves take the two-register (LSERKW2) schemes, time_disc 0..5";
+    return FLUXO_EINVAL_CFG;
+  }
   return FLUXO_OK;
 }
 

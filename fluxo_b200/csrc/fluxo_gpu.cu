@@ -17,6 +17,7 @@
 #include "host_basis.h"
 #include "host_setup.h"
 #include "launch.h"
+#include "time_disc.h"
 #include "vol_shapes.h"
 
 using namespace fluxo;
@@ -75,6 +76,77 @@ __global__ void dt_reset_kernel(unsigned long long* bits, int* key) {
   *key = INT_MAX;
 }
 
+// Stage updates of the Runge-Kutta schemes that are not fused into the volume kernel (their registers
+// and combinations differ from LSERKW2's); the right-hand side of the stage was written to Ut.
+//   LSERKK3 (timedisc.f90:489-542): R1 = S2, R2 = Uprev;  SSPRK2 (ssprk4-5, :560-640): R1 = r0, R2 = r1;
+//   SSPRK33 (:647-687): R1 = Ut_temp.  Each line keeps the reference's operations and their order.
+struct RKStageArgs {
+  int type, stage, nStages;
+  size_t n;
+  double* U;
+  const double* Ut;
+  double *R1, *R2;
+  double b, g1, g2, g3, delta, a, d, e;
+  const double* dtDev;  // device time loop: dt in dtDev[0] ...
+  double dt;            // ... or the host value
+  const int* halt;
+};
+
+// before the first stage's right-hand side: LSERKK3 Uprev = S2 = U, SSPRK2 r0 = U
+__global__ void rk_begin_kernel(RKStageArgs A) {
+  if (A.halt && *A.halt) return;
+  for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < A.n; z += (size_t)gridDim.x * blockDim.x) {
+    const double u = A.U[z];
+    A.R1[z] = u;
+    if (A.type == RK_LSERKK3) A.R2[z] = u;
+  }
+}
+
+__global__ void rk_stage_kernel(RKStageArgs A) {
+  if (A.halt && *A.halt) return;
+  const double dt = A.dtDev ? A.dtDev[0] : A.dt;
+  const double bdt = A.b * dt;
+  const int st = A.stage;
+  for (size_t z = (size_t)blockIdx.x * blockDim.x + threadIdx.x; z < A.n; z += (size_t)gridDim.x * blockDim.x) {
+    double u = A.U[z];
+    const double ut = A.Ut[z];
+    if (A.type == RK_LSERKK3) {
+      if (st == 1) {
+        u = u + ut * bdt;
+      } else {
+        const double s2 = A.R1[z] + u * A.delta;  // S2 = S2 + U*RKdelta
+        A.R1[z] = s2;
+        u = u * A.g1 + s2 * A.g2;                 // U = RKg1*U + RKg2*S2
+        u = u + A.R2[z] * A.g3;                   // U = U + RKg3*Uprev
+        u = u + ut * bdt;                         // U = U + Ut*b_dt
+      }
+    } else if (A.type == RK_SSPRK2) {
+      if (st == 1) {
+        u = u + ut * bdt;
+      } else if (st < A.nStages) {
+        u = u * A.d + A.R1[z] * A.a + ut * bdt;
+        if (st == 2) A.R2[z] = u * A.e;
+        else if (st == 3) A.R2[z] = A.R2[z] + u * A.e;
+        else if (st == 4) A.R2[z] = A.R2[z] + dt * ut * A.e;
+      } else {
+        u = u * A.d + A.R1[z] * A.a + ut * bdt + A.R2[z];
+      }
+    } else {  // SSPRK33, cc = (-3/4, 1/4, -1/12, 2/3) times dt
+      if (st == 1) {
+        A.R1[z] = ut;
+        u = u + ut * dt;
+      } else if (st == 2) {
+        const double tmp = A.R1[z];
+        u = u + tmp * (-0.75 * dt) + ut * (0.25 * dt);
+        A.R1[z] = tmp + ut;
+      } else {
+        u = u + A.R1[z] * (-1. / 12. * dt) + ut * (2. / 3. * dt);
+      }
+    }
+    A.U[z] = u;
+  }
+}
+
 }  // namespace
 
 struct fluxo_handle {
@@ -92,6 +164,7 @@ struct fluxo_handle {
   BasisTables hb{};
   BasisTables* dBasis = nullptr;
   double *dU = nullptr, *dUt = nullptr, *dUtTmp = nullptr, *dGrad = nullptr, *dUtVisc = nullptr;
+  double* dUReg2 = nullptr;  // second extra register of LSERKK3 / SSPRK2
   double *dMetrics = nullptr, *dsJ = nullptr, *dFaceGeo = nullptr, *dXGP = nullptr;
   double *dFlux = nullptr, *dLFlux = nullptr, *dGTrace = nullptr;
   int *dS2E = nullptr, *dE2S = nullptr;
@@ -101,7 +174,8 @@ struct fluxo_handle {
   // analysis (fluxo_gpu_analyze): per-element partial sums, results, interpolation tables
   double *dAnaPartial = nullptr, *dAnaRes = nullptr, *dAnaTables = nullptr;
   int nStages = 0;
-  double RKA[8]{}, RKb[8]{}, RKc[8]{};
+  double RKA[24]{}, RKb[24]{}, RKc[24]{};
+  const RKTable* rk = nullptr;  // the scheme's table (type and the other coefficients)
   double CFLScale = 0., DFLScale = 0.;
   uint64_t launches = 0;
   std::string lastError;
@@ -314,6 +388,34 @@ int rk_step(fluxo_handle* h, double t, double dt, const double* dtDev, const int
   KParams P = base_params(h);
   P.dtDev = dtDev; P.haltFlag = halt; P.dt = dt;
   P.chDev = chDev;
+  if (h->rk->type != RK_LSERKW2) {  // right-hand side into Ut, then the scheme's own stage update
+    RKStageArgs A{};
+    A.type = h->rk->type; A.nStages = h->nStages;
+    A.n = (size_t)h->nVar * h->NP * h->NP * h->NP * h->nElems;
+    A.U = h->dU; A.Ut = h->dUt; A.R1 = h->dUtTmp; A.R2 = h->dUReg2;
+    A.dtDev = dtDev; A.dt = dt; A.halt = halt;
+    const int grid = h->nSMs * 8;
+    if (A.type != RK_SSPRK33) {
+      rk_begin_kernel<<<grid, 256, 0, h->stream>>>(A);
+      FLUXO_CUDA(h, cudaGetLastError());
+      h->launches += 1;
+    }
+    for (int st = 1; st <= h->nStages; ++st) {
+      P.stage = 0;
+      P.rkC = h->RKc[st];
+      P.t = t + dt * h->RKc[st];
+      int r = rhs(h, P);
+      if (r) return r;
+      A.stage = st;
+      A.b = h->rk->b[st];
+      A.g1 = h->rk->g1[st]; A.g2 = h->rk->g2[st]; A.g3 = h->rk->g3[st]; A.delta = h->rk->delta[st];
+      A.a = h->rk->A[st]; A.d = h->rk->d[st]; A.e = h->rk->e[st];
+      rk_stage_kernel<<<grid, 256, 0, h->stream>>>(A);
+      FLUXO_CUDA(h, cudaGetLastError());
+      h->launches += 1;
+    }
+    return FLUXO_OK;
+  }
   for (int st = 1; st <= h->nStages; ++st) {
     P.stage = st;
     P.rkA = h->RKA[st]; P.rkB = h->RKb[st]; P.rkC = h->RKc[st];
@@ -352,41 +454,19 @@ void fill_ns_physics(KParams& P, const fluxo_cfg& c) {
   P.KappasPrMax = std::max(4. / 3., P.KappasPr);
 }
 
-// LSERK coefficients (index 1..nStages) and the scaled CFL/DFL numbers of a configuration
-// (timedisc_vars.f90:168-235, FillCFL_DFL timedisc.f90:697-741); false for an unknown time_disc
+// Runge-Kutta coefficients (index 1..nStages: RKA, RKb and RKc of the table) and the scaled CFL/DFL
+// numbers of a configuration (timedisc_vars.f90:94-726, FillCFL_DFL timedisc.f90:697-741); false for an
+// unknown time_disc
 bool time_disc_setup(const fluxo_cfg& c, double* RKA, double* RKb, double* RKc, int* nStages, double* CFLScale,
                      double* DFLScale) {
-  double cflAlpha[15], relDFL;
-  if (c.time_disc == 0) {
-    const double a[15] = {4.7497, 3.4144, 2.8451, 2.4739, 2.2027, 1.9912, 1.8225, 1.6830,
-                          1.5682, 1.4692, 1.3849, 1.3106, 1.2454, 1.1880, 1.1362};
-    std::copy(a, a + 15, cflAlpha);
-    relDFL = 1.853;
-    *nStages = 5;
-    const double A[6] = {0., 0., 567301805773.0 / 1357537059087.0, 2404267990393.0 / 2016746695238.0,
-                         3550918686646.0 / 2091501179385.0, 1275806237668.0 / 842570457699.0};
-    const double B[6] = {0., 1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
-                         1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
-                         2277821191437.0 / 14882151754819.0};
-    const double C[6] = {0., 0., 1432997174477.0 / 9575080441755.0, 2526269341429.0 / 6820363962896.0,
-                         2006345519317.0 / 3224310063776.0, 2802321613138.0 / 2924317926251.0};
-    std::copy(A, A + 6, RKA); std::copy(B, B + 6, RKb); std::copy(C, C + 6, RKc);
-  } else if (c.time_disc == 1) {
-    const double a[15] = {3.1871, 2.2444, 1.7797, 1.5075, 1.3230, 1.1857, 1.0800, 0.9945,
-                          0.9247, 0.8651, 0.8134, 0.7695, 0.7301, 0.6952, 0.6649};
-    std::copy(a, a + 15, cflAlpha);
-    relDFL = 1.;
-    *nStages = 3;
-    const double A[4] = {0., 0., 5. / 9., 153. / 128.}, B[4] = {0., 1. / 3., 15. / 16., 8. / 15.},
-                 C[4] = {0., 0., 1. / 3., 0.75};
-    std::copy(A, A + 4, RKA); std::copy(B, B + 4, RKb); std::copy(C, C + 4, RKc);
-  } else {
-    return false;
-  }
+  if (c.time_disc < 0 || c.time_disc >= kRKTableCount) return false;
+  const RKTable& T = kRKTables[c.time_disc];
+  *nStages = T.nStages;
+  for (int k = 0; k <= T.nStages; ++k) { RKA[k] = T.A[k]; RKb[k] = T.b[k]; RKc[k] = T.c[k]; }
   const int N = c.N;
   const double dflAlpha[10] = {4.50, 1.95, 1.18, 0.79, 0.56, 0.42, 0.32, 0.25, 0.20, 0.17};
-  *CFLScale = c.cfl_scale * cflAlpha[std::min(15, N) - 1] / (2. * N + 1.);
-  *DFLScale = c.dfl_scale * dflAlpha[std::min(10, N) - 1] * relDFL / ((2. * N + 1.) * (2. * N + 1.));
+  *CFLScale = c.cfl_scale * T.cflAlpha[std::min(15, N) - 1] / (2. * N + 1.);
+  *DFLScale = c.dfl_scale * dflAlpha[std::min(10, N) - 1] * T.relativeDFL / ((2. * N + 1.) * (2. * N + 1.));
   return true;
 }
 
@@ -444,8 +524,9 @@ int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {
   h->nVar = mhd ? 9 : 5;
   if (!time_disc_setup(*cfg, h->RKA, h->RKb, h->RKc, &h->nStages, &h->CFLScale, &h->DFLScale)) {
     delete h;
-    return fail(nullptr, FLUXO_EINVAL_CFG, "time_disc must be 0 (carpenterrk4-5) or 1 (standardrk3-3)");
+    return fail(nullptr, FLUXO_EINVAL_CFG, "time_disc must be 0..9 (the TimeDiscMethod list of fluxo_cfg)");
   }
+  h->rk = &kRKTables[cfg->time_disc];
   cudaError_t e = cudaSetDevice(cfg->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
@@ -510,6 +591,7 @@ int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* S2E, 
       (r = dalloc(h, &h->dFaceGeo, geo.size())) || (r = dalloc(h, &h->dFlux, nFlux)) ||
       (r = dalloc(h, &h->dS2E, s2e.size())) || (r = dalloc(h, &h->dE2S, e2s.size())))
     return r;
+  if ((h->rk->type == RK_LSERKK3 || h->rk->type == RK_SSPRK2) && (r = dalloc(h, &h->dUReg2, nU))) return r;
   if (h->visc) {
     if ((r = dalloc(h, &h->dGrad, 3 * nU)) || (r = dalloc(h, &h->dLFlux, nF)) ||
         (r = dalloc(h, &h->dUtVisc, (size_t)(h->mhd ? 7 : 4) * NP3 * nElems)) ||
@@ -886,7 +968,7 @@ int fluxo_gpu_destroy(fluxo_handle* h) {
   void* ptrs[] = {h->dBasis, h->dU, h->dUt, h->dUtTmp, h->dGrad, h->dUtVisc, h->dMetrics, h->dsJ, h->dFaceGeo, h->dXGP,
                   h->dFlux, h->dLFlux, h->dGTrace, h->dS2E, h->dE2S, h->dTD, h->dDtBits, h->dErrKey,
                   h->dAlpha, h->dAlphaRaw, h->dAlphaTmp, h->dFV, h->dSVdm, h->dBlendList, h->dBlendCount,
-                  h->dAnaPartial, h->dAnaRes, h->dAnaTables};
+                  h->dAnaPartial, h->dAnaRes, h->dAnaTables, h->dUReg2};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);

@@ -76,7 +76,10 @@ KEYS = {
     "analyze_dt": ("r", 0.0),
 }
 
-_TIMEDISC = {"carpenterrk4-5": 0, "standardrk3-3": 1}
+# TimeDiscMethod names (timedisc_vars.f90:94-726) -> fluxo_cfg.time_disc, and their stage counts
+_TIMEDISC = {"carpenterrk4-5": 0, "standardrk3-3": 1, "niegemannrk4-14": 2, "toulorgerk4-8c": 3, "toulorgerk3-7c": 4,
+             "toulorgerk4-8f": 5, "ketchesonrk4-20": 6, "ketchesonrk4-18": 7, "ssprk4-5": 8, "ssprk3-3": 9}
+RK_STAGES = {0: 5, 1: 3, 2: 14, 3: 8, 4: 7, 5: 8, 6: 20, 7: 18, 8: 5, 9: 3}
 _INDICATOR = {"density": 1, "pressure": 2, "densitytimespressure": 3, "kinplusmagenergy": 4}
 _LIFTVAR = {"cons_var": 1, "prim_var": 2, "entropy_var": 3}
 _VISC = {"constant": 0, "sutherland": 1, "powerlaw": 2}

@@ -12,7 +12,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from .params import parse_ini, resolve, to_cfg_fields
+from .params import RK_STAGES, parse_ini, resolve, to_cfg_fields
 
 
 def _ptr(a):
@@ -239,7 +239,7 @@ class Fluxo:
         self.op.set_state(self.U0)
         self.t = 0.0
         self.nDOF = self.op.nElems * (o["n"] + 1) ** 3
-        self.nRKStages = 5 if fields["time_disc"] == 0 else 3
+        self.nRKStages = RK_STAGES[fields["time_disc"]]
 
     # reference names -----------------------------------------------------------------------
     def DGTimeDerivative(self, t):

@@ -59,7 +59,10 @@ typedef struct fluxo_cfg {
   int lifting_var;   /* PP_Lifting_Var: 1 cons_var, 2 prim_var, 3 entropy_var */
   int visc;          /* PP_VISC: 0 constant mu0, 1 Sutherland, 2 power law */
   double kappa, R, Pr, mu0, Ts, Tref, ExpoSuth, ExpoPow, etaBR2;
-  int time_disc;     /* TimeDiscMethod: 0 carpenterrk4-5, 1 standardrk3-3 */
+  int time_disc;     /* TimeDiscMethod (timedisc_vars.f90:94-726): 0 carpenterrk4-5, 1 standardrk3-3,
+                        2 niegemannrk4-14, 3 toulorgerk4-8c, 4 toulorgerk3-7c, 5 toulorgerk4-8f (two-register
+                        LSERKW2, fused into the volume kernel), 6 ketchesonrk4-20, 7 ketchesonrk4-18 (LSERKK3),
+                        8 ssprk4-5, 9 ssprk3-3 (batched solves: 0..5) */
   double cfl_scale;  /* CFLScale (unscaled, as read from parameter.ini) */
   double dfl_scale;  /* DFLScale (unscaled) */
   int ini_exact_func;   /* IniExactFunc: only 4 adds a source term (CalcSource) */
@@ -127,8 +130,9 @@ int fluxo_gpu_dg_time_derivative(fluxo_handle* h, double t);
  * Replaces: src/equation/navierstokes/calctimestep.f90:39-170. */
 int fluxo_gpu_calc_timestep(fluxo_handle* h, double* dt, int* errType);
 
-/* One full low-storage RK step from t with step dt (U updated in place).
- * Replaces: src/timedisc/timedisc.f90:424-480 TimeStepByLSERKW2 (TimeStep pointer). */
+/* One full Runge-Kutta step from t with step dt (U updated in place), the scheme of cfg->time_disc.
+ * Replaces the TimeStep pointer: src/timedisc/timedisc.f90:424-480 TimeStepByLSERKW2,
+ * :489-542 TimeStepByLSERKK3, :560-640 TimeStepBySSPRK2, :647-687 TimeStepBySSPRK33. */
 int fluxo_gpu_timestep(fluxo_handle* h, double t, double dt);
 
 /* The TimeDisc loop (src/timedisc/timedisc.f90:274-359) without output: per step

@@ -12,6 +12,7 @@
 // stability, convergence order) rather than on value-level golden arrays,
 // which the reference does not ship.
 #include "fluxo_oracle.h"
+#include "fluxo_oracle_timedisc.h"
 
 #include <algorithm>
 #include <cmath>
@@ -359,6 +360,7 @@ struct Case {
   // time disc
   int nRKStages;
   std::vector<double> RKA, RKb, RKc;  // index 1..nStages (RKA[0], RKc[0] unused)
+  const OrcRKTable* rk = nullptr;     // the TimeDiscMethod's table (type and all its coefficients)
   double CFLScale, DFLScale;
   bool doCalcSource;
 
@@ -1667,31 +1669,14 @@ void InitEquationAndTime(Case& C) {
   // timedisc_vars.f90:94-726
   double cflAlpha[15];
   double relDFL = 1.;
-  if (P.time_disc == 0) {  // carpenterrk4-5 :204-235
-    C.nRKStages = 5;
-    double a[15] = {4.7497, 3.4144, 2.8451, 2.4739, 2.2027, 1.9912, 1.8225, 1.6830,
-                    1.5682, 1.4692, 1.3849, 1.3106, 1.2454, 1.1880, 1.1362};
-    std::copy(a, a + 15, cflAlpha);
-    relDFL = 1.853;
-    C.RKA = {0., 0., 567301805773.0 / 1357537059087.0, 2404267990393.0 / 2016746695238.0,
-             3550918686646.0 / 2091501179385.0, 1275806237668.0 / 842570457699.0};
-    C.RKb = {0., 1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
-             1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
-             2277821191437.0 / 14882151754819.0};
-    C.RKc = {0., 0., 1432997174477.0 / 9575080441755.0, 2526269341429.0 / 6820363962896.0,
-             2006345519317.0 / 3224310063776.0, 2802321613138.0 / 2924317926251.0};
-  } else if (P.time_disc == 1) {  // standardrk3-3 :168-186
-    C.nRKStages = 3;
-    double a[15] = {3.1871, 2.2444, 1.7797, 1.5075, 1.3230, 1.1857, 1.0800, 0.9945,
-                    0.9247, 0.8651, 0.8134, 0.7695, 0.7301, 0.6952, 0.6649};
-    std::copy(a, a + 15, cflAlpha);
-    relDFL = 1.;
-    C.RKA = {0., 0., 5. / 9., 153. / 128.};
-    C.RKb = {0., 1. / 3., 15. / 16., 8. / 15.};
-    C.RKc = {0., 0., 1. / 3., 0.75};
-  } else {
-    throw std::runtime_error("time disc not implemented in oracle");
-  }
+  if (P.time_disc < 0 || P.time_disc > 9) throw std::runtime_error("time disc not implemented in oracle");
+  C.rk = &kOrcRKTables[P.time_disc];  // SetTimeDiscCoefs, timedisc_vars.f90:94-726
+  C.nRKStages = C.rk->nStages;
+  std::copy(C.rk->cflAlpha, C.rk->cflAlpha + 15, cflAlpha);
+  relDFL = C.rk->relativeDFL;
+  C.RKA.assign(C.rk->A, C.rk->A + C.nRKStages + 1);
+  C.RKb.assign(C.rk->b, C.rk->b + C.nRKStages + 1);
+  C.RKc.assign(C.rk->c, C.rk->c + C.nRKStages + 1);
   // FillCFL_DFL, timedisc.f90:697-741
   int N = C.N;
   double alpha = cflAlpha[std::min(15, N) - 1];
@@ -2190,7 +2175,66 @@ double CalcTimeStep(Case& C, int* errType) {
 }
 
 // TimeStepByLSERKW2, timedisc/timedisc.f90:424-480
+// TimeStepByLSERKK3, timedisc.f90:489-542 (S2 and Uprev as extra registers)
+void TimeStepLSERKK3(Case& C, double t, double dt) {
+  const OrcRKTable& T = *C.rk;
+  size_t nt = C.U.size();
+  std::vector<double> b_dt(C.nRKStages + 1);
+  for (int s = 1; s <= C.nRKStages; ++s) b_dt[s] = T.b[s] * dt;
+  std::vector<real> Uprev(C.U.begin(), C.U.end()), S2(C.U.begin(), C.U.end());
+  DGTimeDerivative(C, t);
+  for (size_t z = 0; z < nt; ++z) C.U[z] = C.U[z] + C.Ut[z] * b_dt[1];
+  for (int s = 2; s <= C.nRKStages; ++s) {
+    DGTimeDerivative(C, t + dt * T.c[s]);
+    for (size_t z = 0; z < nt; ++z) S2[z] = S2[z] + C.U[z] * T.delta[s];
+    for (size_t z = 0; z < nt; ++z) C.U[z] = C.U[z] * T.g1[s] + S2[z] * T.g2[s];
+    for (size_t z = 0; z < nt; ++z) C.U[z] = C.U[z] + Uprev[z] * T.g3[s];
+    for (size_t z = 0; z < nt; ++z) C.U[z] = C.U[z] + C.Ut[z] * b_dt[s];
+  }
+}
+
+// TimeStepBySSPRK2 (ssprk4-5), timedisc.f90:560-640
+void TimeStepSSPRK2(Case& C, double t, double dt) {
+  const OrcRKTable& T = *C.rk;
+  const int n = C.nRKStages;
+  size_t nt = C.U.size();
+  std::vector<double> b_dt(n + 1);
+  for (int s = 1; s <= n; ++s) b_dt[s] = T.b[s] * dt;
+  std::vector<real> r0(C.U.begin(), C.U.end()), r1(nt, real(0.));
+  DGTimeDerivative(C, t);
+  for (size_t z = 0; z < nt; ++z) C.U[z] = C.U[z] + C.Ut[z] * b_dt[1];
+  for (int s = 2; s <= n - 1; ++s) {
+    DGTimeDerivative(C, t + dt * T.c[s]);
+    for (size_t z = 0; z < nt; ++z) C.U[z] = C.U[z] * T.d[s] + r0[z] * T.A[s] + C.Ut[z] * b_dt[s];
+    for (size_t z = 0; z < nt; ++z) {
+      if (s == 2) r1[z] = C.U[z] * T.e[s];
+      else if (s == 3) r1[z] = r1[z] + C.U[z] * T.e[s];
+      else if (s == 4) r1[z] = r1[z] + dt * C.Ut[z] * T.e[s];
+    }
+  }
+  DGTimeDerivative(C, t + dt * T.c[n]);
+  for (size_t z = 0; z < nt; ++z) C.U[z] = C.U[z] * T.d[n] + r0[z] * T.A[n] + C.Ut[z] * b_dt[n] + r1[z];
+}
+
+// TimeStepBySSPRK33, timedisc.f90:647-687
+void TimeStepSSPRK33(Case& C, double t, double dt) {
+  size_t nt = C.U.size();
+  const double cc_dt[4] = {-0.75 * dt, 0.25 * dt, -1. / 12. * dt, 2. / 3. * dt};
+  DGTimeDerivative(C, t);
+  std::vector<real> tmp(C.Ut.begin(), C.Ut.end());
+  for (size_t z = 0; z < nt; ++z) C.U[z] = C.U[z] + C.Ut[z] * dt;
+  DGTimeDerivative(C, t + dt);
+  for (size_t z = 0; z < nt; ++z) C.U[z] = C.U[z] + tmp[z] * cc_dt[0] + C.Ut[z] * cc_dt[1];
+  for (size_t z = 0; z < nt; ++z) tmp[z] = tmp[z] + C.Ut[z];
+  DGTimeDerivative(C, t + 0.5 * dt);
+  for (size_t z = 0; z < nt; ++z) C.U[z] = C.U[z] + tmp[z] * cc_dt[2] + C.Ut[z] * cc_dt[3];
+}
+
+// TimeStepByLSERKW2, timedisc.f90:424-480; the other schemes dispatch from here (the TimeStep pointer)
 void TimeStepLSERK(Case& C, double t, double dt) {
+  if (C.rk->type == 1) { TimeStepLSERKK3(C, t, dt); return; }
+  if (C.rk->type == 2) { TimeStepSSPRK2(C, t, dt); return; }
+  if (C.rk->type == 3) { TimeStepSSPRK33(C, t, dt); return; }
   size_t nt = C.U.size();
   std::vector<double> b_dt(C.nRKStages + 1);
   for (int s = 1; s <= C.nRKStages; ++s) b_dt[s] = C.RKb[s] * dt;

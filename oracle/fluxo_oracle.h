@@ -37,7 +37,9 @@ typedef struct orc_params {
   double ini_frequency;   /* IniFrequency */
   double ref_state[5];    /* RefState (primitive) used by IniExactFunc=1 */
   double cfl_scale, dfl_scale;  /* CFLScale, DFLScale (unscaled input values) */
-  int time_disc;          /* 0 carpenterrk4-5, 1 standardrk3-3, 2 niegemannrk4-14 */
+  int time_disc;          /* 0 carpenterrk4-5, 1 standardrk3-3, 2 niegemannrk4-14, 3 toulorgerk4-8c,
+                             4 toulorgerk3-7c, 5 toulorgerk4-8f, 6 ketchesonrk4-20, 7 ketchesonrk4-18,
+                             8 ssprk4-5, 9 ssprk3-3 */
   /* MHD (eqn 2: ideal, eqn 3: with eta / mu, PARABOLIC), equation/mhd/equation.f90:134-285 */
   double mu_0;            /* mu_0 (magnetic permeability) */
   double eta;             /* eta (resistivity); the viscosity mu is mu0 above */

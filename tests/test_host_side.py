@@ -28,7 +28,7 @@ def test_exports_match_header():
 
 def test_invalid_config_fails_loudly():
     lib = fb.load()
-    for bad in (dict(N=0), dict(N=8), dict(riemann=77), dict(volume_flux=11), dict(riemann=25), dict(time_disc=5),
+    for bad in (dict(N=0), dict(N=8), dict(riemann=77), dict(volume_flux=11), dict(riemann=25), dict(time_disc=10), dict(time_disc=-1),
                 dict(eqn=1, lifting=3), dict(kappa=1.0), dict(eqn=2, riemann=5, volume_flux=10, mu_0=2.0),
                 dict(eqn=2, riemann=6, volume_flux=10)):
         cfg = fb.make_cfg(**bad)
