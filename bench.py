@@ -54,11 +54,13 @@ LIFTING_KERNEL_FALG = FALG_PER_DOF["lifting"] + FALG_PER_DOF["volume_viscous"]
 FACE_FLUX_BYTES_PER_POINT = 33 * 8
 LIFT_FLUX_BYTES_PER_POINT = 16 * 8
 
-# ncu figures of the shipped kernels on the 16^3 case of this workload (2.1 M DOFs, one launch each,
-# profiles/*_ns_tgv_N7_16x16x16.md): DRAM bytes (read + write) per DOF of one launch, and the FP64
-# pipe's active fraction (sm__pipe_fp64_cycles_active), which the F_alg fraction sits below where a
-# kernel spends FP64 instructions that F_alg counts as one flop (division, logarithm, sqrt).
-NCU_DRAM_BYTES_PER_DOF = {"volume": 271.4, "gradient": 190.7, "face_flux": 95.3}
+# ncu figures of the shipped kernels.  DRAM bytes (read + write) per DOF of one launch of this
+# workload at its full size (32^3, one-pass capture of one time step's stages >= 2,
+# profiles/launches_dram_ns_tgv_N7_32x32x32.md); the FP64 pipe's active fraction
+# (sm__pipe_fp64_cycles_active, --set full on the 16^3 case, profiles/*_ns_tgv_N7_16x16x16.md), which
+# the F_alg fraction sits below where a kernel spends FP64 instructions that F_alg counts as one flop
+# (division, logarithm) or issues products and sums that a multiply-add would fuse.
+NCU_DRAM_BYTES_PER_DOF = {"volume": 290.2, "gradient": 206.8, "face_flux": 99.5, "lift_flux": 47.7}
 NCU_FP64_PIPE_ACTIVE = {"volume": 0.458, "gradient": 0.288, "face_flux": 0.372}
 VOLUME_KERNEL_DRAM_BYTES_PER_DOF = NCU_DRAM_BYTES_PER_DOF["volume"]
 
@@ -389,7 +391,7 @@ def run_fluxo(args):
     roofline = {"bound": "fp64", "kernel": "mhd::volume_kernel<5,10>" if mhd else "volume_kernel<8,5,true>",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "traffic": None if mhd else VOLUME_KERNEL_DRAM_BYTES_PER_DOF * nd,
-                "traffic_note": None if mhd else "bytes per launch, ncu on 16^3 scaled by DOFs",
+                "traffic_note": None if mhd else "DRAM bytes per launch, one-pass ncu capture of this workload",
                 "flops_per_dof_launch": vol_falg, "launch_ms": vol_avg_ms,
                 "fp64_pipe_active_ncu": None if mhd else NCU_FP64_PIPE_ACTIVE["volume"],
                 "peak_source": "measured in this job: DFMA loop (fluxo_gpu_fp64_peak); MEASURED_PEAKS.json has no FP64"}

@@ -92,6 +92,9 @@ struct KParams {
   int computeAlpha, indicatorQuantity, propSweeps;
   int subFV, reconsBoundaries;       // SubFVMethod (1 first order, 2 TVD), ReconsBoundaries (1..3)
   double threshold, sharpness, alphaMax, alphaMin, propFactor, timeRelFactor, shockBlendCoef;
+  // element kernels: blocks resident at once on the device (0: no prefetch); block b prefetches the
+  // tile of block b + pfTiles into L2
+  int pfTiles;
   // batched solves: the elements of many independent instances in one launch; each instance has
   // its own time step (null for a single solve)
   const int* elemInst;               // [elem] index of the element's instance in the arrays below
@@ -127,6 +130,16 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
+// One bulk prefetch of the 16-byte-aligned interior of [p, p + bytes) into L2 (a TMA-unit request of
+// up to 4 GB; nothing is read into registers).  The element kernels issue it for the element one wave
+// ahead, so that element's prologue reads L2 instead of DRAM.
+__device__ __forceinline__ void prefetch_l2_bulk(const void* p, size_t bytes) {
+  uintptr_t a = (uintptr_t)p, b = a + bytes;
+  a = (a + 15) & ~(uintptr_t)15;
+  b &= ~(uintptr_t)15;
+  if (b > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((unsigned)(b - a)) : "memory");
+}
+
 // Raises kernel k's dynamic shared-memory limit to `bytes` on the current device.  The attribute
 // belongs to (kernel, device), so `done` keeps one bit per device ordinal < 64 (a launcher passes a
 // function-local static per kernel instantiation); concurrent first calls from several host threads
@@ -141,6 +154,28 @@ inline cudaError_t smem_attr_once(K* k, size_t bytes, std::atomic<unsigned long 
   e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e == cudaSuccess && bit) done.fetch_or(bit, std::memory_order_acq_rel);
   return e;
+}
+
+// Blocks of kernel k (threads, dynamic shared memory) resident on the current device at once: the
+// stride of the element kernels' one-wave-ahead prefetch.  Cached per device ordinal < 64 in
+// `cache` (0: not known yet); 0 when the query fails, which turns the prefetch off.
+template <class K>
+inline int resident_blocks(K* k, int threads, size_t smem, std::atomic<int>* cache) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (dev >= 0 && dev < 64) {
+    const int c = cache[dev].load(std::memory_order_relaxed);
+    if (c > 0) return c;
+  }
+  int perSM = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k, threads, smem) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  const int r = perSM * sms;
+  if (dev >= 0 && dev < 64 && r > 0) cache[dev].store(r, std::memory_order_relaxed);
+  return r;
 }
 
 }  // namespace fluxo

@@ -219,6 +219,17 @@ volume_kernel(KParams P) {
     sDhat[z] = P.basis->Dhat[z];
   }
   __shared__ int sE2S[EPB][12];  // the element's ElemToSide (side, flip per local side)
+  if (P.pfTiles > 0 && threadIdx.x == 0) {  // the tile one wave ahead: its inputs into L2
+    const size_t en = ((size_t)blockIdx.x + P.pfTiles) * EPB;
+    if (en < (size_t)P.nElems) {
+      const size_t ne = ((size_t)P.nElems - en < (size_t)EPB ? (size_t)P.nElems - en : (size_t)EPB) * NP3;
+      prefetch_l2_bulk(P.U + 5 * en * NP3, 5 * ne * sizeof(double));
+      prefetch_l2_bulk(P.metrics + 9 * en * NP3, 9 * ne * sizeof(double));
+      prefetch_l2_bulk(P.sJ + en * NP3, ne * sizeof(double));
+      if (VISC) prefetch_l2_bulk(P.utvisc + 4 * en * NP3, 4 * ne * sizeof(double));
+      if (P.stage > 1) prefetch_l2_bulk(P.UtTmp + 5 * en * NP3, 5 * ne * sizeof(double));
+    }
+  }
   double u[5];
   if (valid) {
     for (int z = t; z < 12; z += NP3) sE2S[eb][z] = P.e2s[12 * (size_t)e + z];  // NP3 = 8 for N = 1

@@ -73,6 +73,120 @@ __device__ __forceinline__ void lifting_var_t(const KParams& P, const double* U,
 template <int NP, int LIFT>
 __host__ __device__ constexpr int lv_minb() { return (LIFT == 2 && NP >= 7) ? 1 : 2; }
 
+// Node phase of the lifting kernel: from the derivatives (dx, de, dz along xi, eta, zeta) of the lifting
+// variable at node t of element e to the primitive gradient (metric terms, surface lift, Jacobian,
+// conversion), the face traces n.F_v of the node's sides (gtrace) and the contravariant viscous fluxes
+// of the node, stored as sF[q * fstride + slot], q = 4*dir + v.  e2s is the element's ElemToSide
+// (side, flip per local side) in shared memory.
+template <int NP, int LIFT, int LV>
+__device__ __forceinline__ void lv_node_fluxes(const KParams& P, int e, int t, int i, int j, int k, const double* u,
+                                               const double* dx, const double* de, const double* dz, const int* e2s,
+                                               double* sF, int fstride, int slot) {
+  constexpr int NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1;
+  const double* M = P.metrics + (size_t)e * 9 * NP3 + t;
+  const double sj = P.sJ[(size_t)e * NP3 + t];
+  double g[3][5];
+  {
+    double m[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) m[c] = M[c * NP3];
+#pragma unroll
+    for (int v = 0; v < 5; ++v)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) g[d][v] = m[0 + d] * dx[v] + m[3 + d] * de[v] + m[6 + d] * dz[v];
+  }
+  int sides[3];
+  const int ns = boundary_sides(i, j, k, N, sides);
+  const double lh = P.basis->LhatM0;
+  if constexpr (LIFT == 2) {
+    // g is the volume part of the gradient, the base of every face trace.  First pass: each side's
+    // trace (volume part + etaBR2 * own-side surface part) and its share n.F_v(U, trace) of the
+    // viscous face flux (riemann.f90:155-168); second pass: the plain surface terms into g.  Two
+    // passes (the face data read twice) keep only one gradient copy live beside the trace.
+#pragma unroll
+    for (int v = 0; v < 5; ++v)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) g[d][v] *= sj;
+#pragma unroll 1
+    for (int z = 0; z < ns; ++z) {
+      const int s = sides[z], side = e2s[2 * (s - 1)], flip = e2s[2 * (s - 1) + 1];
+      const int pt = node_side_point(N, s, flip, i, j, k);
+      const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
+      const double* F = P.lflux + (size_t)side * 5 * NPT + pt;
+      const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
+      double tr[3][5];
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const double fl = sj * lh * F[v * NPT];
+        tr[0][v] = g[0][v] + P.etaBR2 * (fl * n0);
+        tr[1][v] = g[1][v] + P.etaBR2 * (fl * n1);
+        tr[2][v] = g[2][v] + P.etaBR2 * (fl * n2);
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) to_grad_prim(P, u, tr[d]);
+      double kf[4], kg[4], kh[4];
+      diff_flux_3d(P, u, tr[0], tr[1], tr[2], kf, kg, kh);
+      double* T = P.gtrace + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 4 * NPT + pt;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) T[(size_t)v * NPT] = n0 * kf[v] + n1 * kg[v] + n2 * kh[v];
+    }
+  }
+  for (int z = 0; z < ns; ++z) {
+    const int s = sides[z], side = e2s[2 * (s - 1)], flip = e2s[2 * (s - 1) + 1];
+    const int pt = node_side_point(N, s, flip, i, j, k);
+    const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
+    const double* F = P.lflux + (size_t)side * 5 * NPT + pt;
+    const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      if constexpr (LIFT == 2) {  // volume gradient gets the plain surface term
+        const double fl = sj * lh * F[v * NPT];
+        g[0][v] += fl * n0; g[1][v] += fl * n1; g[2][v] += fl * n2;
+      } else {
+        const double fl = F[v * NPT] * lh;
+        g[0][v] += fl * n0; g[1][v] += fl * n1; g[2][v] += fl * n2;
+      }
+    }
+  }
+  if constexpr (LIFT == 1) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) g[d][v] *= sj;
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) to_grad_prim(P, u, g[d]);
+  if (P.grad) {  // volume gradients kept for analysis (DGTimeDerivative calls only)
+    double* G = P.grad + 15 * ((size_t)e * NP3 + t);
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int v = 0; v < 5; ++v) G[5 * d + v] = g[d][v];
+  }
+  double f[4], gg[4], h[4];
+  diff_flux_3d(P, u, g[0], g[1], g[2], f, gg, h);
+  if constexpr (LIFT == 1) {
+    // BR1: the face trace of the gradient is the volume gradient at the boundary node, so this
+    // side's share of the viscous face flux is n.F_v of the node (riemann.f90:155-168)
+    for (int z = 0; z < ns; ++z) {
+      const int s = sides[z], side = e2s[2 * (s - 1)], flip = e2s[2 * (s - 1) + 1];
+      const int pt = node_side_point(N, s, flip, i, j, k);
+      const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
+      const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
+      double* T = P.gtrace + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 4 * NPT + pt;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) T[(size_t)v * NPT] = n0 * f[v] + n1 * gg[v] + n2 * h[v];
+    }
+  }
+  // contravariant fluxes (metrics re-read rather than held across the gradient work)
+#pragma unroll
+  for (int dir = 0; dir < 3; ++dir) {
+    const double m0 = M[(3 * dir + 0) * NP3], m1 = M[(3 * dir + 1) * NP3], m2 = M[(3 * dir + 2) * NP3];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) sF[(4 * dir + v) * fstride + slot] = f[v] * m0 + gg[v] * m1 + h[v] * m2;
+  }
+}
+
 template <int NP, int LIFT, int LV>
 __global__ void __launch_bounds__(lv_epb<NP>() * NP * NP * NP, lv_minb<NP, LIFT>()) lift_visc_kernel(KParams P) {
   if (halted(P)) return;
@@ -94,6 +208,15 @@ __global__ void __launch_bounds__(lv_epb<NP>() * NP * NP * NP, lv_minb<NP, LIFT>
   const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
   // first node of the own xi / eta / zeta line; the line's nodes follow at strides 1, NP, NP^2
   const int bx = t - i, be = t - NP * j, bz = t - NPT * k;
+  if (P.pfTiles > 0 && threadIdx.x == 0) {  // the tile one wave ahead: its inputs into L2
+    const size_t en = ((size_t)blockIdx.x + P.pfTiles) * EPB;
+    if (en < (size_t)P.nElems) {
+      const size_t ne = ((size_t)P.nElems - en < (size_t)EPB ? (size_t)P.nElems - en : (size_t)EPB) * NP3;
+      prefetch_l2_bulk(P.U + 5 * en * NP3, 5 * ne * sizeof(double));
+      prefetch_l2_bulk(P.metrics + 9 * en * NP3, 9 * ne * sizeof(double));
+      prefetch_l2_bulk(P.sJ + en * NP3, ne * sizeof(double));
+    }
+  }
   double u[5];
   if (valid) {
     for (int z = t; z < 12; z += NP3) sE2S[eb][z] = P.e2s[12 * (size_t)e + z];  // NP3 = 8 for N = 1
@@ -110,125 +233,24 @@ __global__ void __launch_bounds__(lv_epb<NP>() * NP * NP * NP, lv_minb<NP, LIFT>
   }
   __syncthreads();
   if (valid) {
-    const double* M = P.metrics + (size_t)e * 9 * NP3 + t;
-    const double sj = P.sJ[(size_t)e * NP3 + t];
-    double g[3][5];
-    {
-      // derivatives of the lifting variable along xi, eta, zeta at the own node, l = 0..N
-      double dx[5], de[5], dz[5];
+    // derivatives of the lifting variable along xi, eta, zeta at the own node, l = 0..N
+    double dx[5], de[5], dz[5];
 #pragma unroll
-      for (int v = 0; v < 5; ++v) { dx[v] = 0.; de[v] = 0.; dz[v] = 0.; }
-      const double* Di = sD + i * R;
-      const double* Dj = sD + j * R;
-      const double* Dk = sD + k * R;
+    for (int v = 0; v < 5; ++v) { dx[v] = 0.; de[v] = 0.; dz[v] = 0.; }
+    const double* Di = sD + i * R;
+    const double* Dj = sD + j * R;
+    const double* Dk = sD + k * R;
 #pragma unroll
-      for (int l = 0; l < NP; ++l) {
-        const double a = Di[l], b = Dj[l], c = Dk[l];
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
-          dx[v] += a * sV[v * NP3 + bx + l];
-          de[v] += b * sV[v * NP3 + be + NP * l];
-          dz[v] += c * sV[v * NP3 + bz + NPT * l];
-        }
-      }
-      double m[9];
-#pragma unroll
-      for (int c = 0; c < 9; ++c) m[c] = M[c * NP3];
-#pragma unroll
-      for (int v = 0; v < 5; ++v)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) g[d][v] = m[0 + d] * dx[v] + m[3 + d] * de[v] + m[6 + d] * dz[v];
-    }
-    int sides[3];
-    const int ns = boundary_sides(i, j, k, N, sides);
-    const double lh = P.basis->LhatM0;
-    if constexpr (LIFT == 2) {
-      // g is the volume part of the gradient, the base of every face trace.  First pass: each side's
-      // trace (volume part + etaBR2 * own-side surface part) and its share n.F_v(U, trace) of the
-      // viscous face flux (riemann.f90:155-168); second pass: the plain surface terms into g.  Two
-      // passes (the face data read twice) keep only one gradient copy live beside the trace.
-#pragma unroll
-      for (int v = 0; v < 5; ++v)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) g[d][v] *= sj;
-#pragma unroll 1
-      for (int z = 0; z < ns; ++z) {
-        const int s = sides[z], side = sE2S[eb][2 * (s - 1)], flip = sE2S[eb][2 * (s - 1) + 1];
-        const int pt = node_side_point(N, s, flip, i, j, k);
-        const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
-        const double* F = P.lflux + (size_t)side * 5 * NPT + pt;
-        const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
-        double tr[3][5];
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
-          const double fl = sj * lh * F[v * NPT];
-          tr[0][v] = g[0][v] + P.etaBR2 * (fl * n0);
-          tr[1][v] = g[1][v] + P.etaBR2 * (fl * n1);
-          tr[2][v] = g[2][v] + P.etaBR2 * (fl * n2);
-        }
-#pragma unroll
-        for (int d = 0; d < 3; ++d) to_grad_prim(P, u, tr[d]);
-        double kf[4], kg[4], kh[4];
-        diff_flux_3d(P, u, tr[0], tr[1], tr[2], kf, kg, kh);
-        double* T = P.gtrace + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 4 * NPT + pt;
-#pragma unroll
-        for (int v = 0; v < 4; ++v) T[(size_t)v * NPT] = n0 * kf[v] + n1 * kg[v] + n2 * kh[v];
-      }
-    }
-    for (int z = 0; z < ns; ++z) {
-      const int s = sides[z], side = sE2S[eb][2 * (s - 1)], flip = sE2S[eb][2 * (s - 1) + 1];
-      const int pt = node_side_point(N, s, flip, i, j, k);
-      const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
-      const double* F = P.lflux + (size_t)side * 5 * NPT + pt;
-      const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
+    for (int l = 0; l < NP; ++l) {
+      const double a = Di[l], b = Dj[l], c = Dk[l];
 #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        if constexpr (LIFT == 2) {  // volume gradient gets the plain surface term
-          const double fl = sj * lh * F[v * NPT];
-          g[0][v] += fl * n0; g[1][v] += fl * n1; g[2][v] += fl * n2;
-        } else {
-          const double fl = F[v * NPT] * lh;
-          g[0][v] += fl * n0; g[1][v] += fl * n1; g[2][v] += fl * n2;
-        }
+        dx[v] += a * sV[v * NP3 + bx + l];
+        de[v] += b * sV[v * NP3 + be + NP * l];
+        dz[v] += c * sV[v * NP3 + bz + NPT * l];
       }
     }
-    if constexpr (LIFT == 1) {
-#pragma unroll
-      for (int v = 0; v < 5; ++v)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) g[d][v] *= sj;
-    }
-#pragma unroll
-    for (int d = 0; d < 3; ++d) to_grad_prim(P, u, g[d]);
-    if (P.grad) {  // volume gradients kept for analysis (DGTimeDerivative calls only)
-      double* G = P.grad + 15 * ((size_t)e * NP3 + t);
-#pragma unroll
-      for (int d = 0; d < 3; ++d)
-#pragma unroll
-        for (int v = 0; v < 5; ++v) G[5 * d + v] = g[d][v];
-    }
-    double f[4], gg[4], h[4];
-    diff_flux_3d(P, u, g[0], g[1], g[2], f, gg, h);
-    if constexpr (LIFT == 1) {
-      // BR1: the face trace of the gradient is the volume gradient at the boundary node, so this
-      // side's share of the viscous face flux is n.F_v of the node (riemann.f90:155-168)
-      for (int z = 0; z < ns; ++z) {
-        const int s = sides[z], side = sE2S[eb][2 * (s - 1)], flip = sE2S[eb][2 * (s - 1) + 1];
-        const int pt = node_side_point(N, s, flip, i, j, k);
-        const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
-        const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
-        double* T = P.gtrace + ((size_t)side * 2 + (flip == 0 ? 0 : 1)) * 4 * NPT + pt;
-#pragma unroll
-        for (int v = 0; v < 4; ++v) T[(size_t)v * NPT] = n0 * f[v] + n1 * gg[v] + n2 * h[v];
-      }
-    }
-    // contravariant fluxes (metrics re-read rather than held across the gradient work)
-#pragma unroll
-    for (int dir = 0; dir < 3; ++dir) {
-      const double m0 = M[(3 * dir + 0) * NP3], m1 = M[(3 * dir + 1) * NP3], m2 = M[(3 * dir + 2) * NP3];
-#pragma unroll
-      for (int v = 0; v < 4; ++v) sF[(4 * dir + v) * NP3 + t] = f[v] * m0 + gg[v] * m1 + h[v] * m2;
-    }
+    lv_node_fluxes<NP, LIFT, LV>(P, e, t, i, j, k, u, dx, de, dz, sE2S[eb], sF, NP3, t);
   }
   __syncthreads();
   // viscous volume integral at the own node: sum_l D_hat(i,l) f~(l,j,k) + D_hat(j,l) g~(i,l,k) +

@@ -16,10 +16,14 @@ static cudaError_t vol_shape_launch(int nElems, cudaStream_t s, const KParams& P
   constexpr int EPB = sh.epb, LPW = sh.lpw, MINB = sh.minb, OWNSM = sh.ownsm;
   constexpr size_t smem = vol_smem_bytes<NP, VF_ID, EPB, LPW>();
   static std::atomic<unsigned long long> attr{0};
-  cudaError_t e = smem_attr_once(volume_kernel<NP, VF_ID, VISC, EPB, LPW, MINB, OWNSM>, smem, attr);
+  static std::atomic<int> resident[64];
+  auto k = volume_kernel<NP, VF_ID, VISC, EPB, LPW, MINB, OWNSM>;
+  cudaError_t e = smem_attr_once(k, smem, attr);
   if (e != cudaSuccess) return e;
   const int grid = (nElems + EPB - 1) / EPB;
-  volume_kernel<NP, VF_ID, VISC, EPB, LPW, MINB, OWNSM><<<grid, VolShape<NP, EPB, LPW>::THREADS, smem, s>>>(P);
+  KParams Q = P;
+  Q.pfTiles = resident_blocks(k, VolShape<NP, EPB, LPW>::THREADS, smem, resident);
+  k<<<grid, VolShape<NP, EPB, LPW>::THREADS, smem, s>>>(Q);
   return cudaGetLastError();
 }
 

@@ -10,11 +10,26 @@
 //    (s = a+b, d = b-a; identical to (a+b)*52.5/(105+35u+21u^2+15u^3)), and otherwise uses
 //    (b-a)/(log b - log a) with per-node logarithms;
 //  - every log mean is kept as a (numerator, denominator) pair and all divisions of one pair
-//    flux are merged into a single reciprocal.
+//    flux are merged into a single reciprocal (rcp_nr).
 #pragma once
 #include "common.cuh"
 
 namespace fluxo {
+
+// Reciprocal of x > 0 (normal, not huge) for the pair fluxes: the hardware's approximate reciprocal
+// (PTX rcp.approx.ftz.f64) refined by two Newton-Raphson steps for f(y) = 1/y - x,
+// y <- y + y (1 - x y), each computed with fused multiply-adds.  The approximation's relative error
+// is squared by every step, so two steps reach double precision (within an ulp of the rounded
+// quotient); the denominators here are products of densities, inverse temperatures and their log
+// means, far from zero and from overflow.  It replaces the longer IEEE division sequence (one per pair).
+__device__ __forceinline__ double rcp_nr(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
 
 // log mean of (a, b) as num/den given la = log(a), lb = log(b)
 __device__ __forceinline__ void ln_mean_nd(double a, double b, double la, double lb, double& num, double& den) {
@@ -188,7 +203,7 @@ __device__ __forceinline__ void pair_flux(const KParams& P, const double* L, con
              rq2L * (L[1] * uH + L[2] * vH + L[3] * wH) + rq2R * (R[1] * uH + R[2] * vH + R[3] * wH);
     } else if constexpr (VF == 6) {  // EntropyAndEnergyConservingFluxVec2 :1427-1504 (halves)
       const double rhoM = L[0] + R[0];
-      const double sbM = 2. / (L[4] + R[4]);
+      const double sbM = 2. * rcp_nr(L[4] + R[4]);
       const double uH = L[1] + R[1], vH = L[2] + R[2], wH = L[3] + R[3];
       const double p1 = 0.5 * rhoM * sbM;
       const double q = uH * m1 + vH * m2 + wH * m3;
@@ -208,7 +223,7 @@ __device__ __forceinline__ void pair_flux(const KParams& P, const double* L, con
       F[1] = F[0] * uH + m1 * p1;
       F[2] = F[0] * vH + m2 * p1;
       F[3] = F[0] * wH + m3 * p1;
-      F[4] = F[0] * 0.5 * (P.sKappaM1 * db / nb - (L[6] + R[6])) + uH * F[1] + vH * F[2] + wH * F[3];
+      F[4] = F[0] * 0.5 * (P.sKappaM1 * (db * rcp_nr(nb)) - (L[6] + R[6])) + uH * F[1] + vH * F[2] + wH * F[3];
     } else if constexpr (VF == 8) {  // KennedyAndGruberFluxVec2 :857-929 (halves)
       const double uH = L[1] + R[1], vH = L[2] + R[2], wH = L[3] + R[3];
       const double p1 = L[4] + R[4];
@@ -234,7 +249,7 @@ __device__ __forceinline__ void pair_flux(const KParams& P, const double* L, con
       ln_mean_nd(L, R, 0, 6, nr, dr);
       ln_mean_nd(L, R, 4, 7, nb, db);
       const double sr = L[0] + R[0], sb = L[4] + R[4];
-      const double inv = 1. / (dr * sb * nb);
+      const double inv = rcp_nr(dr * sb * nb);
       const double rhoHat = nr * sb * nb * inv;      // LN(rho)
       const double p1 = 0.5 * sr * dr * nb * inv;    // 0.5*rho_mean/beta_mean
       const double sbHat = db * dr * sb * inv;       // 1/LN(beta)
@@ -250,7 +265,7 @@ __device__ __forceinline__ void pair_flux(const KParams& P, const double* L, con
       ln_mean_nd(L, R, 0, 5, n1, d1);
       ln_mean_nd(L, R, 4, 6, n5, d5);
       const double z1M = 0.5 * (L[0] + R[0]);
-      const double inv = 1. / (d5 * z1M * n1);
+      const double inv = rcp_nr(d5 * z1M * n1);
       const double z5LN = n5 * z1M * n1 * inv;
       const double sz1M = d5 * n1 * inv;
       const double ratio = n5 * d1 * z1M * inv;  // z5LN / z1LN
@@ -269,7 +284,7 @@ __device__ __forceinline__ void pair_flux(const KParams& P, const double* L, con
       double nr, dr, ns, ds;
       ln_mean_nd(L, R, 0, 6, nr, dr);
       ln_mean_nd(L, R, 5, 7, ns, ds);
-      const double inv = 1. / (dr * ns);
+      const double inv = rcp_nr(dr * ns);
       const double rhoLN = nr * ns * inv;
       const double srspM = ds * dr * inv;  // 1/LN(rho/p)
       const double va1 = 0.5 * (L[1] + R[1]), va2 = 0.5 * (L[2] + R[2]), va3 = 0.5 * (L[3] + R[3]);

@@ -2,7 +2,8 @@
 step with the host's dt (fluxo_gpu_timestep) and three steps of the device-resident TimeDisc loop
 (fluxo_gpu_time_disc, dt from CALCTIMESTEP on the device), for the Navier-Stokes right-hand side (BR1
 lifting) and, for the schemes whose stage update is not fused into the volume kernel, for resistive MHD.
-Tolerance: relative L2 <= 1e-12."""
+CFLscale 0.4: Ketcheson RK4-20 takes the CFL scaling of Niegemann RK4-14 in the reference's table and
+is unstable at 0.9 on these cases (the oracle and the GPU both blow up).  Tolerance: relative L2 <= 1e-12."""
 import numpy as np
 import pytest
 
@@ -23,7 +24,7 @@ def rel_l2(a, b):
 def test_navier_stokes_every_scheme(gpu_lib, td):
     c, op = pair(eqn=1, mu0=0.02, ini_exact_func=7, N=3, nElems=(2, 3, 2), NGeo=2, deform_amp=0.05,
                  xmin=(-np.pi,) * 3, xmax=(np.pi,) * 3, lifting=1, lifting_var=3, riemann=44, volume_flux=5,
-                 time_disc=td, perturb=0.02)
+                 time_disc=td, perturb=0.02, cfl_scale=0.4)
     dt_ref, _ = c.calc_timestep()
     dt, err = op.calc_timestep()
     assert err == 0 and dt == pytest.approx(dt_ref, rel=1e-13)
@@ -41,7 +42,7 @@ def test_resistive_mhd_unfused_schemes(gpu_lib, td):
     from test_gpu_mhd import mhd_pair
 
     c, op = mhd_pair(eqn=3, N=3, volume_flux=10, riemann=10, noncons=1, nc_glm=1, eta=0.02, mu0=0.01,
-                     time_disc=td)
+                     time_disc=td, cfl_scale=0.4)
     t_ref, n_ref = c.run(0.0, 10.0, max_iter=2)
     t, n, err = op.time_disc(0.0, 10.0, 2)
     assert err == 0 and n == n_ref == 2 and t == pytest.approx(t_ref, rel=1e-13)
