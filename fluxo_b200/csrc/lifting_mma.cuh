@@ -11,7 +11,7 @@
 // by the shared-memory pipe.  The node phase between the two products (gradient, face traces,
 // fluxes) is lv_node_fluxes, shared with lift_visc_kernel.
 //
-// Shared layout: every per-node array uses slot(i,j,k) = i + 9 j + 68 k (548 slots).  A tile's 8 columns
+// Shared layout: every per-node array uses slot(i,j,k) = i + 9 j + 76 k (603 slots).  A tile's 8 columns
 // are lines of its direction that differ in k (xi: j fixed, eta: i fixed) or in j (zeta: i fixed); with
 // this padding the B loads of all three directions hit distinct banks, and the C stores two-way.
 #pragma once
@@ -19,8 +19,8 @@
 
 namespace fluxo {
 
-__device__ __forceinline__ int lm_slot(int i, int j, int k) { return i + 9 * j + 68 * k; }
-constexpr int kLmStride = 548;  // lm_slot(7, 7, 7) + 1
+__device__ __forceinline__ int lm_slot(int i, int j, int k) { return i + 9 * j + 76 * k; }
+constexpr int kLmStride = 603;  // lm_slot(7, 7, 7) + 1 (slots are distinct: 7 + 9*7 < 76)
 constexpr size_t lm_smem_bytes() { return sizeof(double) * (size_t)20 * kLmStride; }
 
 // d += A(8x4) B(4x8) in FP64: a = A[lane/4][lane%4], b = B[lane%4][lane/4],
