@@ -82,6 +82,9 @@ class FluxoCfg(ctypes.Structure):
         ("indicator_quantity", ctypes.c_int),
         ("sub_fv_method", ctypes.c_int),
         ("recons_boundaries", ctypes.c_int),
+        ("nfvse_corr", ctypes.c_int),
+        ("posit_corr_factor", ctypes.c_double),
+        ("posit_max_iter", ctypes.c_int),
     ]
 
 

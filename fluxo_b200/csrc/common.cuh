@@ -90,8 +90,15 @@ struct KParams {
   double* fv;             // [elem][var][node] alpha * F_FV of the blended elements
   const double* sVdm;     // nodal -> modal Legendre coefficients [m][i]
   int computeAlpha, indicatorQuantity, propSweeps;
-  int subFV, reconsBoundaries;       // SubFVMethod (1 first order, 2 TVD), ReconsBoundaries (1..3)
+  int subFV, reconsBoundaries;       // SubFVMethod (1 first order, 2 TVD, 3 TVD-ES, 4 TVD-Fjordholm),
+                                     // ReconsBoundaries (1..3)
   double threshold, sharpness, alphaMax, alphaMin, propFactor, timeRelFactor, shockBlendCoef;
+  // NFVSE_CORR (Apply_NFVSE_Correction, nfvse.f90:1688-1883): F_FV of every element, and
+  // FFV_m_FDG = (F_FV - Ut_DG) (-sJ) [elem][node][var] written by the volume kernel
+  int nfvseCorr;
+  double* ffvmfdg;
+  double positCorrFactor;
+  int positMaxIter;
   // element kernels: blocks resident at once on the device (0: no prefetch); block b prefetches the
   // tile of block b + pfTiles into L2
   int pfTiles;

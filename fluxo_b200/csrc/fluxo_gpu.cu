@@ -64,6 +64,7 @@ __global__ void td_finalize_kernel(TDState* s) {
 // after the stages: t += dt, iteration count, termination (timedisc.f90:329-359)
 __global__ void td_advance_kernel(TDState* s) {
   if (s->halt) return;
+  if (s->errKey != INT_MAX) { s->err = s->errKey & 7; s->halt = 1; return; }  // NFVSE_CORR during the step
   s->t = s->t + s->dt;
   s->iter += 1;
   if (s->last || (s->maxIter > 0 && s->iter >= s->maxIter)) { s->done = 1; s->halt = 1; }
@@ -90,6 +91,8 @@ struct RKStageArgs {
   const double* dtDev;  // device time loop: dt in dtDev[0] ...
   double dt;            // ... or the host value
   const int* halt;
+  int part;             // SSPRK2 with NFVSE_CORR: 1 the U update only, 2 the r1 update only (after the
+                        // correction of U and Ut); 0 both
 };
 
 // before the first stage's right-hand side: LSERKK3 Uprev = S2 = U, SSPRK2 r0 = U
@@ -121,13 +124,21 @@ __global__ void rk_stage_kernel(RKStageArgs A) {
         u = u + ut * bdt;                         // U = U + Ut*b_dt
       }
     } else if (A.type == RK_SSPRK2) {
+      if (A.part == 2) {  // r1 from the corrected U and Ut (timedisc.f90:600-604)
+        if (st == 2) A.R2[z] = u * A.e;
+        else if (st == 3) A.R2[z] = A.R2[z] + u * A.e;
+        else if (st == 4) A.R2[z] = A.R2[z] + dt * ut * A.e;
+        continue;
+      }
       if (st == 1) {
         u = u + ut * bdt;
       } else if (st < A.nStages) {
         u = u * A.d + A.R1[z] * A.a + ut * bdt;
-        if (st == 2) A.R2[z] = u * A.e;
-        else if (st == 3) A.R2[z] = A.R2[z] + u * A.e;
-        else if (st == 4) A.R2[z] = A.R2[z] + dt * ut * A.e;
+        if (A.part == 0) {
+          if (st == 2) A.R2[z] = u * A.e;
+          else if (st == 3) A.R2[z] = A.R2[z] + u * A.e;
+          else if (st == 4) A.R2[z] = A.R2[z] + dt * ut * A.e;
+        }
       } else {
         u = u * A.d + A.R1[z] * A.a + ut * bdt + A.R2[z];
       }
@@ -157,6 +168,7 @@ struct fluxo_handle {
   double glmCh = 0., glmDtch1 = 0.;  // MHD: GLM_ch, GLM_dtch1 (from the metrics at set_mesh)
   // NFVSE: blending coefficients, list of blended elements, alpha * F_FV, modal transform
   double *dAlpha = nullptr, *dAlphaRaw = nullptr, *dAlphaTmp = nullptr, *dFV = nullptr, *dSVdm = nullptr;
+  double* dFFV = nullptr;  // NFVSE_CORR: FFV_m_FDG [elem][node][var]
   int *dBlendList = nullptr, *dBlendCount = nullptr;
   int nSMs = 148;
   bool visc = false, meshSet = false, stateSet = false, haveXGP = false;
@@ -276,6 +288,8 @@ KParams base_params(fluxo_handle* h) {
     P.sharpness = std::log((1.0 - 1.e-4) / 1.e-4);
     P.alphaMax = c.alpha_max; P.alphaMin = c.alpha_min; P.propFactor = c.space_prop_factor;
     P.timeRelFactor = c.time_rel_factor; P.shockBlendCoef = c.shock_blend_coef;
+    P.nfvseCorr = c.nfvse_corr ? 1 : 0; P.ffvmfdg = h->dFFV;
+    P.positCorrFactor = c.posit_corr_factor; P.positMaxIter = c.posit_max_iter;
   }
   return P;
 }
@@ -384,10 +398,14 @@ __global__ void fp64_fma_kernel(double* out, int iters, double a, double b) {
 
 // One LSERK-2reg step (timedisc.f90:424-480): host dt (dtDev == null) or device dt.
 int rk_step(fluxo_handle* h, double t, double dt, const double* dtDev, const int* halt,
-            const double* chDev = nullptr) {
+            const double* chDev = nullptr, int* errKey = nullptr) {
   KParams P = base_params(h);
   P.dtDev = dtDev; P.haltFlag = halt; P.dt = dt;
   P.chDev = chDev;
+  // NFVSE_CORR: Apply_NFVSE_Correction after each stage update (timedisc.f90:457-473, 583-621); not
+  // for SSPRK33, which the reference steps without it
+  const bool corr = h->cfg.nfvse && h->cfg.nfvse_corr && h->rk->type != RK_SSPRK33;
+  if (!errKey) errKey = h->dErrKey;
   if (h->rk->type != RK_LSERKW2) {  // right-hand side into Ut, then the scheme's own stage update
     RKStageArgs A{};
     A.type = h->rk->type; A.nStages = h->nStages;
@@ -410,9 +428,20 @@ int rk_step(fluxo_handle* h, double t, double dt, const double* dtDev, const int
       A.b = h->rk->b[st];
       A.g1 = h->rk->g1[st]; A.g2 = h->rk->g2[st]; A.g3 = h->rk->g3[st]; A.delta = h->rk->delta[st];
       A.a = h->rk->A[st]; A.d = h->rk->d[st]; A.e = h->rk->e[st];
+      A.part = corr ? 1 : 0;
       rk_stage_kernel<<<grid, 256, 0, h->stream>>>(A);
       FLUXO_CUDA(h, cudaGetLastError());
       h->launches += 1;
+      if (corr) {
+        FLUXO_CUDA(h, launch_nfvse_corr(h->NP, h->mhd, h->nElems, h->stream, P, h->dUt, h->rk->b[st], errKey));
+        h->launches += 1;
+        if (st >= 2 && st <= 4 && st < h->nStages) {
+          A.part = 2;
+          rk_stage_kernel<<<grid, 256, 0, h->stream>>>(A);
+          FLUXO_CUDA(h, cudaGetLastError());
+          h->launches += 1;
+        }
+      }
     }
     return FLUXO_OK;
   }
@@ -422,6 +451,10 @@ int rk_step(fluxo_handle* h, double t, double dt, const double* dtDev, const int
     P.t = t + dt * h->RKc[st];
     int r = rhs(h, P);
     if (r) return r;
+    if (corr) {  // Ut is not kept by the fused stage update (the next stage recomputes it)
+      FLUXO_CUDA(h, launch_nfvse_corr(h->NP, h->mhd, h->nElems, h->stream, P, nullptr, h->RKb[st], errKey));
+      h->launches += 1;
+    }
   }
   return FLUXO_OK;
 }
@@ -505,10 +538,20 @@ int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {
     if (cfg->indicator_quantity < 1 || cfg->indicator_quantity > 4)
       return fail(nullptr, FLUXO_EINVAL_CFG, "ShockIndicatorQuantity must be 1..4");
     if (cfg->space_prop_sweeps < 0) return fail(nullptr, FLUXO_EINVAL_CFG, "SpacePropSweeps must be >= 0");
-    if (cfg->sub_fv_method != 1 && cfg->sub_fv_method != 2)
-      return fail(nullptr, FLUXO_EINVAL_CFG, "SubFVMethod must be 1 (first order) or 2 (TVD)");
-    if (cfg->sub_fv_method == 2 && (cfg->recons_boundaries < 1 || cfg->recons_boundaries > 3))
+    if (cfg->sub_fv_method < 1 || cfg->sub_fv_method > 4) return fail(nullptr, FLUXO_EINVAL_CFG, "SubFVMethod not implemented");
+    if (cfg->sub_fv_method >= 2 && (cfg->recons_boundaries < 1 || cfg->recons_boundaries > 3))
       return fail(nullptr, FLUXO_EINVAL_CFG, "ReconsBoundaries must be 1..3");
+    const int rs = cfg->riemann;
+    const bool matrices = mhd ? (rs == 14 || rs == 15) : (rs == 4 || rs == 44 || rs == 33);
+    if (cfg->sub_fv_method >= 3 && !matrices)  // nfvse.f90:174-187
+      return fail(nullptr, FLUXO_EINVAL_CFG, "SubFVMethod 3/4 need a Riemann solver with RiemannVolFluxAndDissipMatrices");
+    if (cfg->nfvse_corr) {
+      if (cfg->time_disc == 6 || cfg->time_disc == 7)  // timedisc_vars.f90:111-114
+        return fail(nullptr, FLUXO_EINVAL_CFG, "NFVSE correction is only implemented for LSERKW2 methods and ssprk4-5");
+      if (cfg->posit_max_iter < 0) return fail(nullptr, FLUXO_EINVAL_CFG, "PositMaxIter must be >= 0");
+    }
+  } else if (cfg->nfvse_corr) {
+    return fail(nullptr, FLUXO_EINVAL_CFG, "nfvse_corr needs nfvse = 1");
   }
   if (parabolic) {
     if (cfg->lifting != 1 && cfg->lifting != 2) return fail(nullptr, FLUXO_EINVAL_CFG, "lifting must be BR1 or BR2");
@@ -616,9 +659,10 @@ int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* S2E, 
   if (h->cfg.nfvse) {
     if ((r = dalloc(h, &h->dAlpha, (size_t)nElems)) || (r = dalloc(h, &h->dAlphaRaw, (size_t)nElems)) ||
         (r = dalloc(h, &h->dAlphaTmp, (size_t)nElems)) || (r = dalloc(h, &h->dBlendList, (size_t)nElems)) ||
-        (r = dalloc(h, &h->dFV, nU)))
+        (r = dalloc(h, &h->dFV, nU)) || (h->cfg.nfvse_corr && (r = dalloc(h, &h->dFFV, nU))))
       return r;
     FLUXO_CUDA(h, cudaMemsetAsync(h->dAlpha, 0, (size_t)nElems * sizeof(double), h->stream));
+    if (h->cfg.nfvse_corr) FLUXO_CUDA(h, cudaMemsetAsync(h->dFFV, 0, nU * sizeof(double), h->stream));
   }
   cudaStream_t s = h->stream;
   FLUXO_CUDA(h, cudaMemcpyAsync(h->dMetrics, met.data(), met.size() * 8, cudaMemcpyHostToDevice, s));
@@ -725,7 +769,21 @@ int fluxo_gpu_calc_timestep(fluxo_handle* h, double* dt, int* errType) {
 int fluxo_gpu_timestep(fluxo_handle* h, double t, double dt) {
   int r = check_ready(h);
   if (r) return r;
+  const bool corr = h->cfg.nfvse && h->cfg.nfvse_corr;
+  if (corr) {
+    dt_reset_kernel<<<1, 1, 0, h->stream>>>(h->dDtBits, h->dErrKey);
+    FLUXO_CUDA(h, cudaGetLastError());
+  }
   if ((r = rk_step(h, t, dt, nullptr, nullptr))) return r;
+  if (corr) {  // Apply_NFVSE_Correction stops the reference when a safe state is not admissible
+    int key = INT_MAX;
+    FLUXO_CUDA(h, cudaMemcpyAsync(&key, h->dErrKey, 4, cudaMemcpyDeviceToHost, h->stream));
+    FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (key != INT_MAX)
+      return fail(h, FLUXO_ENAN_STATE, "NFVSE correction: safe state not admissible in element " +
+                                           std::to_string(key / 8 + 1));
+    return FLUXO_OK;
+  }
   FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
   return FLUXO_OK;
 }
@@ -755,7 +813,7 @@ int fluxo_gpu_time_disc(fluxo_handle* h, double t, double tEnd, int maxIter, dou
       }
       td_finalize_kernel<<<1, 1, 0, s>>>(td);
       FLUXO_CUDA(h, cudaGetLastError());
-      if ((r = rk_step(h, 0., 0., &td->dt, &td->halt, h->mhd ? &td->ch : nullptr))) return r;
+      if ((r = rk_step(h, 0., 0., &td->dt, &td->halt, h->mhd ? &td->ch : nullptr, &td->errKey))) return r;
       td_advance_kernel<<<1, 1, 0, s>>>(td);
       FLUXO_CUDA(h, cudaGetLastError());
       h->launches += 3;
@@ -967,7 +1025,7 @@ int fluxo_gpu_destroy(fluxo_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   void* ptrs[] = {h->dBasis, h->dU, h->dUt, h->dUtTmp, h->dGrad, h->dUtVisc, h->dMetrics, h->dsJ, h->dFaceGeo, h->dXGP,
                   h->dFlux, h->dLFlux, h->dGTrace, h->dS2E, h->dE2S, h->dTD, h->dDtBits, h->dErrKey,
-                  h->dAlpha, h->dAlphaRaw, h->dAlphaTmp, h->dFV, h->dSVdm, h->dBlendList, h->dBlendCount,
+                  h->dAlpha, h->dAlphaRaw, h->dAlphaTmp, h->dFV, h->dFFV, h->dSVdm, h->dBlendList, h->dBlendCount,
                   h->dAnaPartial, h->dAnaRes, h->dAnaTables, h->dUReg2};
   for (void* p : ptrs)
     if (p) cudaFree(p);

@@ -324,8 +324,17 @@ volume_kernel(KParams P) {
   if (!valid) return;
   if (P.nfvse) {  // VolInt_NFVSE (nfvse.f90:475-565): blend with alpha * F_FV of the subcell FV kernel
     const double a = P.alpha[e];
-    if (a > 4.440892098500626e-16) {
-      const double* FV = P.fv + (size_t)e * 5 * NP3 + t;
+    const double* FV = P.fv + (size_t)e * 5 * NP3 + t;
+    if (P.nfvseCorr) {  // F_FV of every element; FFV_m_FDG = (F_FV - Ut) (-sJ) for the correction
+      const double sjn = P.sJ[(size_t)e * NP3 + t];
+      double* FF = P.ffvmfdg + 5 * ((size_t)e * NP3 + t);
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const double f = FV[v * NP3];
+        FF[v] = (f - ut[v]) * (-sjn);
+        ut[v] = (1. - a) * ut[v] + a * f;
+      }
+    } else if (a > 4.440892098500626e-16) {
 #pragma unroll
       for (int v = 0; v < 5; ++v) ut[v] = (1. - a) * ut[v] + FV[v * NP3];
     }

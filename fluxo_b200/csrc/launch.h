@@ -67,6 +67,10 @@ cudaError_t launch_mhd_timestep(int NP, bool visc, int nElems, cudaStream_t s, c
 // NFVSE shock capturing: blending coefficient (indicator + propagation + list of blended elements;
 // `scratch` holds nElems doubles for sweeps > 1) and the subcell FV volume integral of MHD.
 cudaError_t launch_nfvse_alpha(int NP, bool mhd, int nElems, cudaStream_t s, const KParams& P, double* scratch);
+// NFVSE_CORR: Apply_NFVSE_Correction of every element after a stage update with step b * dt (ut: the
+// stage's Ut to correct as well, or null); errKey records elem*8 + 5 for a safe state that is not admissible
+cudaError_t launch_nfvse_corr(int NP, bool mhd, int nElems, cudaStream_t s, const KParams& P, double* ut, double b,
+                              int* errKey);
 cudaError_t launch_nfvse_fv(int RS, int NP, int nElems, int nSMs, cudaStream_t s, const KParams& P);
 cudaError_t launch_nfvse_fv_ns(int RS, int NP, int nElems, int nSMs, cudaStream_t s, const KParams& P);
 

@@ -433,10 +433,19 @@ __global__ void __launch_bounds__(vol_threads<NP>(), vol_minb<NP>()) volume_kern
     if (NC == 1 || NC == 3) { ut[5] += h * v0; ut[6] += h * v1; ut[7] += h * v2; }
     if (NCGLM) { ut[4] += u[8] * ncGLM; ut[8] += ncGLM; }
   }
-  if (P.nfvse) {  // VolInt_NFVSE (nfvse.f90:475-565): blend with alpha * F_FV of the FV kernel
+  if (P.nfvse) {  // VolInt_NFVSE (nfvse.f90:475-565): blend with alpha * F_FV of the subcell FV kernel
     const double a = P.alpha[e];
-    if (a > 4.440892098500626e-16) {
-      const double* FV = P.fv + (size_t)e * NV * NP3 + t;
+    const double* FV = P.fv + (size_t)e * NV * NP3 + t;
+    if (P.nfvseCorr) {  // F_FV of every element; FFV_m_FDG = (F_FV - Ut) (-sJ) for the correction
+      const double sjn = P.sJ[(size_t)e * NP3 + t];
+      double* FF = P.ffvmfdg + NV * ((size_t)e * NP3 + t);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const double f = FV[v * NP3];
+        FF[v] = (f - ut[v]) * (-sjn);
+        ut[v] = (1. - a) * ut[v] + a * f;
+      }
+    } else if (a > 4.440892098500626e-16) {
 #pragma unroll
       for (int v = 0; v < NV; ++v) ut[v] = (1. - a) * ut[v] + FV[v * NP3];
     }

@@ -46,6 +46,21 @@ cudaError_t launch_nfvse_alpha(int NP, bool mhd, int nElems, cudaStream_t s, con
   return cudaSuccess;
 }
 
+cudaError_t launch_nfvse_corr(int NP, bool mhd, int nElems, cudaStream_t s, const KParams& P, double* ut, double b,
+                              int* errKey) {
+#define FLUXO_NF_C(np)                                                                                        \
+  case np:                                                                                                    \
+    if (mhd) nfvse::corr_kernel<np, 9><<<nElems, np * np * np, 0, s>>>(P, ut, b, errKey);                      \
+    else nfvse::corr_kernel<np, 5><<<nElems, np * np * np, 0, s>>>(P, ut, b, errKey);                          \
+    break;
+  switch (NP) {
+    FLUXO_NF_C(3) FLUXO_NF_C(4) FLUXO_NF_C(5) FLUXO_NF_C(6) FLUXO_NF_C(7) FLUXO_NF_C(8)
+    default: return cudaErrorInvalidValue;
+  }
+#undef FLUXO_NF_C
+  return cudaGetLastError();
+}
+
 cudaError_t launch_nfvse_fv(int RS, int NP, int nElems, int nSMs, cudaStream_t s, const KParams& P) {
   const int grid = std::min(nElems, 8 * nSMs);
   switch (RS) {

@@ -260,10 +260,12 @@ __device__ __forceinline__ void es_llf(const KParams& P, double ch, const double
   F[8] = F[8] - (LM * tau) * (psiA * Vj[4] + Vj[8]);
 }
 
-// EntropyStableDerigsFlux / EntropyStableFloGorFlux (Riemann 14 / 15): EC flux minus
-// 1/2 R |D| T R^T [v] with the 9-wave eigen-decomposition, mhd/riemann.f90:1224-1632, :1633-2042
+// Flux and dissipation matrices of the entropy-stable 9-wave solvers (Riemann 14 Derigs, 15 FloGor):
+// EntropyStableDerigsFlux_VolFluxAndDissipMatrices mhd/riemann.f90:1287-1622 and the FloGor variant
+// :1695-2042: EC flux F, diagonal D (with the entropy scaling T) and right eigenvectors, R[c] = column c
 template <bool FLOGOR>
-__device__ __forceinline__ void es_9wave(const KParams& P, double ch, const double* UL, const double* UR, double* F) {
+__device__ __forceinline__ void es_9wave_matrices(const KParams& P, double ch, const double* UL, const double* UR,
+                                                  double* F, double* Dm, double (*R)[9]) {
   double Vj[9], pL, pR, bL, bR;
   entropy_jump(P, UL, UR, pL, pR, bL, bR, Vj);
   const double sL = 1. / UL[0], sR = 1. / UR[0];
@@ -337,7 +339,7 @@ __device__ __forceinline__ void es_9wave(const KParams& P, double ch, const doub
   const double psiFm = 0.5 * alf * rhoLN * u2A + abeta * als * rhoLN * bperp + alf * rhoLN * aLN * aLN * P.sKappaM1 -
                        alf * cf * rhoLN * uA[0] + als * cs * rhoLN * sg * t23;
   // columns of R (mhd/riemann.f90:1497-1586)
-  const double R[9][9] = {
+  const double Rc[9][9] = {
       {alf * rhoLN, alf * rhoLN * (uA[0] + cf), rhoLN * (alf * uA[1] - als * cs * be2 * sg),
        rhoLN * (alf * uA[2] - als * cs * be3 * sg), psiFp, 0.0, als * abeta * be2 * sqRho, als * abeta * be3 * sqRho, 0.0},
       {0.0, 0.0, rhoLN * sqRhoA * be3, -rhoLN * sqRhoA * be2, -rhoLN * sqRhoA * (be2 * uA[2] - be3 * uA[1]), 0.0,
@@ -363,13 +365,29 @@ __device__ __forceinline__ void es_9wave(const KParams& P, double ch, const doub
   const double T1 = 0.5 / P.kappa / rhoLN, T2 = 0.25 / betaA / rhoLN / rhoLN, T4 = 0.25 / betaA,
                T5 = rhoLN * P.kappaM1 / P.kappa;
   const double Tm[9] = {T1, T2, T1, T4, T5, T4, T1, T2, T1};
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    Dm[c] = ((1. - phi) * fabs(wave[c]) + phi * LM) * Tm[c];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) R[c][r] = Rc[c][r];
+  }
+}
+
+// EntropyStableDerigsFlux / EntropyStableFloGorFlux (mhd/riemann.f90:1224-1283, :1633-1691):
+// F - 1/2 R D R^T [v]
+template <bool FLOGOR>
+__device__ __forceinline__ void es_9wave(const KParams& P, double ch, const double* UL, const double* UR, double* F) {
+  double Vj[9], pL, pR, bL, bR;
+  entropy_jump(P, UL, UR, pL, pR, bL, bR, Vj);
+  double Dm[9], R[9][9];  // R[c] is column c
+  es_9wave_matrices<FLOGOR>(P, ch, UL, UR, F, Dm, R);
   double w[9];
 #pragma unroll
-  for (int c = 0; c < 9; ++c) {  // D * (R^T [v]); R[c] is column c
+  for (int c = 0; c < 9; ++c) {  // D * (R^T [v])
     double s = 0.;
 #pragma unroll
     for (int r = 0; r < 9; ++r) s += R[c][r] * Vj[r];
-    w[c] = ((1. - phi) * fabs(wave[c]) + phi * LM) * Tm[c] * s;
+    w[c] = Dm[c] * s;
   }
 #pragma unroll
   for (int r = 0; r < 9; ++r) {
@@ -379,6 +397,7 @@ __device__ __forceinline__ void es_9wave(const KParams& P, double ch, const doub
     F[r] = F[r] - 0.5 * s;
   }
 }
+
 
 template <int RS>
 __host__ __device__ constexpr bool riemann_supported() {

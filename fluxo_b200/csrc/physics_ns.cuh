@@ -221,6 +221,43 @@ __host__ __device__ constexpr int riemann_llf_point_flux() {
   return RS == 14 ? 2 : RS == 15 ? 3 : RS == 17 ? 7 : RS == 18 ? 8 : RS == 19 ? 4 : RS == 21 ? 9 : 0;
 }
 
+// RiemannSolver_EntropyStable_VolFluxAndDissipMatrices (riemann.f90:936-975): the solver's EC flux
+// (4: Ismail-Roe, 44: EC-KEP, 33: Ranocha; equation.f90:381-404), the diagonal scaling DHat = |Lambda| S
+// and the right eigenvectors Rh[row][col] at the flux's mean state, on rotated states
+template <int RS>
+__device__ __forceinline__ void es_matrices(const KParams& P, const double* L, const double* R, double* Fc,
+                                            double* Dh, double (*Rh)[5]) {
+  constexpr int W = (RS == 4) ? 10 : (RS == 44 ? 5 : 32);
+  Hat h;
+  volume_flux_1d<W>(P, L, R, Fc, h);
+  const double rows[5][5] = {{1., 1., 0., 0., 1.},
+                             {h.u - h.a, h.u, 0., 0., h.u + h.a},
+                             {h.v, h.v, 1., 0., h.v},
+                             {h.w, h.w, 0., 1., h.w},
+                             {h.H - h.u * h.a, 0.5 * (h.u * h.u + h.v * h.v + h.w * h.w), h.v, h.w, h.H + h.u * h.a}};
+#pragma unroll
+  for (int r = 0; r < 5; ++r)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) Rh[r][c] = rows[r][c];
+  Dh[0] = 0.5 * fabs(h.u - h.a) * h.rho / P.kappa;
+  Dh[1] = fabs(h.u) * (P.kappaM1 / P.kappa) * h.rho;
+  Dh[2] = fabs(h.u) * h.p1;
+  Dh[3] = Dh[2];
+  Dh[4] = 0.5 * fabs(h.u + h.a) * h.rho / P.kappa;
+}
+
+// ConsToEntropy (equation_vars.f90:362-391); s = -log(rho_sp * rho^(kappa-1)) as two logarithms
+__device__ __forceinline__ void cons_to_entropy_ns(const KParams& P, const double* U, double* V) {
+  double srho = 1. / U[0];
+  double u = U[1] * srho, v = U[2] * srho, w = U[3] * srho;
+  double v2s2 = 0.5 * (u * u + v * v + w * w);
+  double rho_sp = U[0] / (P.kappaM1 * (U[4] - U[0] * v2s2));
+  double s = -(log(rho_sp) + P.kappaM1 * log(U[0]));
+  V[0] = (P.kappa - s) * P.sKappaM1 - rho_sp * v2s2;
+  V[1] = rho_sp * u; V[2] = rho_sp * v; V[3] = rho_sp * w;
+  V[4] = -rho_sp;
+}
+
 // Riemann solvers on rotated states (navierstokes/riemann.f90).  lmm is the maximum wave speed
 // over the side, used by the LLF-dissipation variants 13-19 and 21.
 template <int RS>
@@ -259,21 +296,8 @@ __device__ __forceinline__ void riemann_rotated(const KParams& P, const double* 
     }
   } else if constexpr (RS == 4 || RS == 44 || RS == 33) {
     // RiemannSolver_EntropyStable :874-931 with the dissipation matrices :936-975
-    constexpr int W = (RS == 4) ? 10 : (RS == 44 ? 5 : 32);
-    double Fc[5];
-    Hat h;
-    volume_flux_1d<W>(P, L, R, Fc, h);
-    const double Rh[5][5] = {{1., 1., 0., 0., 1.},
-                             {h.u - h.a, h.u, 0., 0., h.u + h.a},
-                             {h.v, h.v, 1., 0., h.v},
-                             {h.w, h.w, 0., 1., h.w},
-                             {h.H - h.u * h.a, 0.5 * (h.u * h.u + h.v * h.v + h.w * h.w), h.v, h.w, h.H + h.u * h.a}};
-    double Dh[5];
-    Dh[0] = 0.5 * fabs(h.u - h.a) * h.rho / P.kappa;
-    Dh[1] = fabs(h.u) * (P.kappaM1 / P.kappa) * h.rho;
-    Dh[2] = fabs(h.u) * h.p1;
-    Dh[3] = Dh[2];
-    Dh[4] = 0.5 * fabs(h.u + h.a) * h.rho / P.kappa;
+    double Fc[5], Dh[5], Rh[5][5];
+    es_matrices<RS>(P, L, R, Fc, Dh, Rh);
     double vL[3], vR[3], pL, pR;
     primitive_pv(P, L, vL, pL);
     primitive_pv(P, R, vR, pR);
@@ -522,15 +546,7 @@ __device__ __forceinline__ void lifting_var(const KParams& P, const double* U, d
     V[0] = U[0]; V[1] = U[1] * s; V[2] = U[2] * s; V[3] = U[3] * s;
     V[4] = P.kappaM1 * (U[4] - 0.5 * (U[1] * V[1] + U[2] * V[2] + U[3] * V[3]));
   } else {
-    double srho = 1. / U[0];
-    double u = U[1] * srho, v = U[2] * srho, w = U[3] * srho;
-    double v2s2 = 0.5 * (u * u + v * v + w * w);
-    double rho_sp = U[0] / (P.kappaM1 * (U[4] - U[0] * v2s2));
-    // s = -log(rho_sp * rho^(kappa-1)), written with two logarithms instead of log + pow
-    double s = -(log(rho_sp) + P.kappaM1 * log(U[0]));
-    V[0] = (P.kappa - s) * P.sKappaM1 - rho_sp * v2s2;
-    V[1] = rho_sp * u; V[2] = rho_sp * v; V[3] = rho_sp * w;
-    V[4] = -rho_sp;
+    cons_to_entropy_ns(P, U, V);
   }
 }
 

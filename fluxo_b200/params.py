@@ -67,6 +67,10 @@ KEYS = {
     "shockindicatorquantity": ("s", "DensityTimesPressure"),
     "subfvmethod": ("i", 1),
     "reconsboundaries": ("i", 1),
+    # NFVSE_CORR (nfvse.f90:148-152); "nfvse_corr" stands for the build option FLUXO_SHOCK_NFVSE_CORR
+    "nfvse_corr": ("s", "F"),
+    "positcorrfactor": ("r", 0.1),
+    "positmaxiter": ("i", 10),
     # time discretisation (timedisc.f90:53-70)
     "timediscmethod": ("s", "carpenterrk4-5"),
     "tend": ("r", None),
@@ -169,16 +173,19 @@ def to_cfg_fields(res):
         time_disc=_TIMEDISC[tdm], cfl_scale=res["cflscale"], dfl_scale=res["dflscale"],
         ini_exact_func=res["iniexactfunc"], ini_frequency=res["inifrequency"], ini_amplitude=res["iniamplitude"],
     )
+    ind = str(res["shockindicatorquantity"]).strip().lower()
+    if ind not in _INDICATOR:
+        raise ValueError("ShockIndicatorQuantity %r not implemented" % res["shockindicatorquantity"])
+    f.update(nfvse=1 if _flag(res["nfvse"]) else 0,
+             compute_alpha=res["computealpha"], shock_blend_coef=res["shockblendcoef"],
+             modal_threshold=res["modalthreshold"], alpha_max=res["alpha_max"], alpha_min=res["alpha_min"],
+             space_prop_factor=res["spacepropfactor"], space_prop_sweeps=res["spacepropsweeps"],
+             time_rel_factor=res["timerelfactor"], indicator_quantity=_INDICATOR[ind],
+             sub_fv_method=res["subfvmethod"], recons_boundaries=res["reconsboundaries"],
+             nfvse_corr=1 if _flag(res["nfvse_corr"]) else 0, posit_corr_factor=res["positcorrfactor"],
+             posit_max_iter=res["positmaxiter"])
     if eqsys == "mhd":
-        ind = str(res["shockindicatorquantity"]).strip().lower()
-        if ind not in _INDICATOR:
-            raise ValueError("ShockIndicatorQuantity %r not implemented" % res["shockindicatorquantity"])
         f.update(eqn=3 if parabolic else 2, mu0=res["mu"], mu_0=res["mu_0"], eta=res["eta"],
                  glm_scale=res["glm_scale"], glm_scr=res["glm_scr"], noncons=res["noncons"],
-                 nc_glm=1 if _flag(res["nc_glm"]) else 0, nfvse=1 if _flag(res["nfvse"]) else 0,
-                 compute_alpha=res["computealpha"], shock_blend_coef=res["shockblendcoef"],
-                 modal_threshold=res["modalthreshold"], alpha_max=res["alpha_max"], alpha_min=res["alpha_min"],
-                 space_prop_factor=res["spacepropfactor"], space_prop_sweeps=res["spacepropsweeps"],
-                 time_rel_factor=res["timerelfactor"], indicator_quantity=_INDICATOR[ind],
-                 sub_fv_method=res["subfvmethod"], recons_boundaries=res["reconsboundaries"])
+                 nc_glm=1 if _flag(res["nc_glm"]) else 0)
     return f

@@ -32,7 +32,8 @@ def make_cfg(**fields):
                     mu_0=1.0, eta=0.0, glm_scale=0.5, glm_scr=0.0, noncons=1, nc_glm=0,
                     nfvse=0, compute_alpha=1, shock_blend_coef=0.0, modal_threshold=1, alpha_max=0.5,
                     alpha_min=0.01, space_prop_factor=0.5, space_prop_sweeps=1, time_rel_factor=0.0,
-                    indicator_quantity=3, sub_fv_method=1, recons_boundaries=1)
+                    indicator_quantity=3, sub_fv_method=1, recons_boundaries=1, nfvse_corr=0,
+                    posit_corr_factor=0.1, posit_max_iter=10)
     defaults.update(fields)
     for k, v in defaults.items():
         setattr(cfg, k, v)

@@ -78,7 +78,9 @@ typedef struct fluxo_cfg {
   int noncons;       /* NONCONS: 0 off, 1 Powell, 2 Brackbill, 3 Janhunen (CMake FLUXO_EQN_NONCONS_TYPE) */
   int nc_glm;        /* PP_NC_GLM: non-conservative GLM terms (CMake FLUXO_EQN_NONCONS_GLM) */
   /* NFVSE shock capturing (CMake FLUXO_SHOCKCAP_NFVSE; src/shockcapturing/nfvse.f90:63-260), Euler,
-   * Navier-Stokes and MHD, N >= 2, SubFVMethod = 1 (first-order subcell finite volumes) or 2 (TVD). */
+   * Navier-Stokes and MHD, N >= 2, SubFVMethod = 1 (first-order subcell finite volumes), 2 (TVD),
+   * 3 (TVD-ES) or 4 (TVD-Fjordholm); 3 and 4 need a Riemann solver with dissipation matrices
+   * (Navier-Stokes 4, 44, 33; MHD 14, 15). */
   int nfvse;               /* 0 off, 1 on */
   int compute_alpha;       /* ComputeAlpha: 1 Persson-Peraire indicator, 3 fixed ShockBlendCoef */
   double shock_blend_coef; /* ShockBlendCoef */
@@ -89,8 +91,19 @@ typedef struct fluxo_cfg {
   int indicator_quantity;  /* ShockIndicatorQuantity: 1 Density, 2 Pressure, 3 DensityTimesPressure,
                               4 KinPlusMagEnergy */
   int sub_fv_method;       /* SubFVMethod: 1 first-order subcell FV, 2 TVD (minmod reconstruction of the
-                              primitive variables, nfvse.f90:674-815, 1448-1529) */
-  int recons_boundaries;   /* ReconsBoundaries (SubFVMethod 2): 1 none, 2 central, 3 neighbour element */
+                              primitive variables, nfvse.f90:674-815, 1448-1529), 3 TVD-ES (TVD states with
+                              an entropy-stability switch, :826-1090), 4 TVD-Fjordholm (reconstruction of the
+                              scaled entropy variables, :1101-1386) */
+  int recons_boundaries;   /* ReconsBoundaries (SubFVMethod 2-4): 1 none, 2 central, 3 neighbour element */
+  /* NFVSE_CORR (CMake FLUXO_SHOCK_NFVSE_CORR; Apply_NFVSE_Correction nfvse.f90:1688-1883): after every
+   * stage update the blending coefficient of each element is raised as far as needed to keep density and
+   * pressure at PositCorrFactor of their values under the pure subcell FV update.  Only with the
+   * LSERKW2 schemes (time_disc 0..5) and ssprk4-5 (8); ssprk3-3 (9) runs without the correction as in
+   * the reference.  A safe state with negative density or pressure ends the step with
+   * FLUXO_ENAN_STATE, errType 5 (the reference stops). */
+  int nfvse_corr;          /* 0 off, 1 on (needs nfvse = 1) */
+  double posit_corr_factor; /* PositCorrFactor (reference default 0.1) */
+  int posit_max_iter;      /* PositMaxIter (reference default 10) */
 } fluxo_cfg;
 
 typedef struct fluxo_handle fluxo_handle;
@@ -126,7 +139,8 @@ int fluxo_gpu_get_gradients(fluxo_handle* h, double* gradPx, double* gradPy, dou
 int fluxo_gpu_dg_time_derivative(fluxo_handle* h, double t);
 
 /* CALCTIMESTEP(errType): minimum over elements of the convective (and viscous)
- * time step; errType 1 NaN density, 2 p<=0, 3 NaN dt_conv, 4 NaN dt_visc.
+ * time step; errType 1 NaN density, 2 p<=0, 3 NaN dt_conv, 4 NaN dt_visc (5: NFVSE_CORR safe state
+ * not admissible, from fluxo_gpu_timestep / fluxo_gpu_time_disc).
  * Replaces: src/equation/navierstokes/calctimestep.f90:39-170. */
 int fluxo_gpu_calc_timestep(fluxo_handle* h, double* dt, int* errType);
 

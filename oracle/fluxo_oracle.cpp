@@ -344,6 +344,8 @@ struct Case {
   bool GLM_init = false;
   // NFVSE shock capturing (shockcapturing/nfvse_vars.f90): blending coefficients, sub-cell metrics
   std::vector<double> alpha, alphaMaster, alphaSlave, scNv, scT1, scT2, scNorm;
+  std::vector<real> FFVmFDG;    // NFVSE_CORR: (F_FV - Ut_DG) (-sJ) of the last RHS, nfvse_vars.f90
+  int corrErr = 0;              // element + 1 whose safe state was not admissible (the reference stops)
   // basis (double), dg/dg.f90:181-252
   std::vector<double> xGP, wGP, wBary, D, D_T, Dhat, Dhat_T, Dvolsurf, Dvolsurf_T, Lminus, Lplus;
   double L_HatMinus0, L_HatPlus0;
@@ -797,6 +799,28 @@ inline real lambdaMaxPair(const Case& C, const real* LL, const real* RR) {
 }
 
 // SolveRiemannProblem on one side (all (N+1)^2 points), rotated states.  navierstokes/riemann.f90
+// RiemannSolver_EntropyStable_VolFluxAndDissipMatrices, navierstokes/riemann.f90:936-975: the EC
+// two-point flux of the solver (4: Ismail-Roe, 44: EC-KEP, 33: Ranocha; equation.f90:381-404), the
+// diagonal scaling DHat = |Lambda| S and the right eigenvectors RHat[row][col] at the flux's mean state
+void ES_VolFluxAndDissipMatrices(const Case& C, int rs, const real* L, const real* R, real* Fc, real* Dh,
+                                 real Rh[5][5]) {
+  const int which = (rs == 4) ? 10 : (rs == 44 ? 5 : 32);
+  Hat h;
+  VolumeFluxAverage(C, which, L, R, Fc, h);
+  const real rows[5][5] = {{1., 1., 0., 0., 1.},
+                           {h.u - h.a, h.u, 0., 0., h.u + h.a},
+                           {h.v, h.v, 1., 0., h.v},
+                           {h.w, h.w, 0., 1., h.w},
+                           {h.H - h.u * h.a, 0.5 * (h.u * h.u + h.v * h.v + h.w * h.w), h.v, h.w, h.H + h.u * h.a}};
+  for (int r = 0; r < 5; ++r)
+    for (int c = 0; c < 5; ++c) Rh[r][c] = rows[r][c];
+  Dh[0] = 0.5 * fabs(h.u - h.a) * h.rho / C.kappa;
+  Dh[1] = fabs(h.u) * (C.kappaM1 / C.kappa) * h.rho;
+  Dh[2] = fabs(h.u) * h.p1;
+  Dh[3] = Dh[2];
+  Dh[4] = 0.5 * fabs(h.u + h.a) * h.rho / C.kappa;
+}
+
 void SolveRiemann(const Case& C, int npts, const real* ULL, const real* URR, real* F) {
   const int rs = C.P.riemann;
   const int nv = 5;
@@ -849,24 +873,11 @@ void SolveRiemann(const Case& C, int npts, const real* ULL, const real* URR, rea
       }
       return;
     case 4: case 44: case 33: {  // RiemannSolver_EntropyStable :874-931, matrices :936-975
-      int which = (rs == 4) ? 10 : (rs == 44 ? 5 : 32);
       for (int i = 0; i < npts; ++i) {
         const real* L = ULL + nv * i;
         const real* R = URR + nv * i;
-        real Fc[5];
-        Hat h;
-        VolumeFluxAverage(C, which, L, R, Fc, h);
-        real Rh[5][5] = {{1., 1., 0., 0., 1.},
-                         {h.u - h.a, h.u, 0., 0., h.u + h.a},
-                         {h.v, h.v, 1., 0., h.v},
-                         {h.w, h.w, 0., 1., h.w},
-                         {h.H - h.u * h.a, 0.5 * (h.u * h.u + h.v * h.v + h.w * h.w), h.v, h.w, h.H + h.u * h.a}};
-        real Dh[5];
-        Dh[0] = 0.5 * fabs(h.u - h.a) * h.rho / C.kappa;
-        Dh[1] = fabs(h.u) * (C.kappaM1 / C.kappa) * h.rho;
-        Dh[2] = fabs(h.u) * h.p1;
-        Dh[3] = Dh[2];
-        Dh[4] = 0.5 * fabs(h.u + h.a) * h.rho / C.kappa;
+        real Fc[5], Dh[5], Rh[5][5];
+        ES_VolFluxAndDissipMatrices(C, rs, L, R, Fc, Dh, Rh);
         real sRL = 1. / L[0], sRR = 1. / R[0];
         real vL[3] = {L[1] * sRL, L[2] * sRL, L[3] * sRL};
         real vR[3] = {R[1] * sRR, R[2] * sRR, R[3] * sRR};
@@ -2174,6 +2185,95 @@ double CalcTimeStep(Case& C, int* errType) {
   return std::min(dtConv, dtVisc);
 }
 
+// Get_Pressure / Get_dpdU (navierstokes/equation_vars.f90:752-760, 792-809; mhd/equation_vars.f90:803-812, 844-862)
+inline real CorrPressure(const Case& C, const real* U) {
+  const real m2 = U[1] * U[1] + U[2] * U[2] + U[3] * U[3];
+  if (C.mhd)
+    return C.kappaM1 * (U[4] - 0.5 * (m2 / U[0]) - C.s2mu_0 * (U[5] * U[5] + U[6] * U[6] + U[7] * U[7] + U[8] * U[8]));
+  return C.kappaM1 * (U[4] - 0.5 * (m2 / U[0]));
+}
+inline void CorrDpdU(const Case& C, const real* U, real* d) {
+  const real vel[3] = {U[1] / U[0], U[2] / U[0], U[3] / U[0]};
+  d[0] = 0.5 * (vel[0] * vel[0] + vel[1] * vel[1] + vel[2] * vel[2]);
+  for (int c = 0; c < 3; ++c) d[1 + c] = -vel[c];
+  d[4] = 1.0;
+  if (C.mhd)
+    for (int z = 5; z < 9; ++z) d[z] = -C.smu_0 * U[z];
+  for (int v = 0; v < C.nVar; ++v) d[v] = d[v] * C.kappaM1;
+}
+
+// Apply_NFVSE_Correction (nfvse.f90:1688-1883) after the update of an RK stage with step dt = b_dt(stage):
+// per element the smallest increase of alpha (as a correction of U along FFV_m_FDG) that keeps the density,
+// then the pressure, at PositCorrFactor of the values of the 'safe' state U + dt (1-alpha) FFV_m_FDG
+// (Newton iterations for the pressure); alpha <= 1.  Ut gets the matching change.  A safe state with
+// negative density or pressure sets corrErr (the reference stops the run).
+void ApplyNFVSECorrection(Case& C, double dt) {
+  const double eps = 1.e-14, NEWTON_ABSTOL = 1.e-8, alpha_maxPosit = 1.0;
+  const double sdt = 1. / dt;
+  const int NV = C.nVar, nd = C.nDOFElem;
+  std::vector<real> p_safe(nd);
+  for (int e = 0; e < C.nElems; ++e) {
+    const double alphadiff = C.alpha[e] - alpha_maxPosit;
+    if (std::fabs(alphadiff) < eps) continue;
+    real* U = &C.U[(size_t)NV * nd * e];
+    real* Ut = &C.Ut[(size_t)NV * nd * e];
+    const real* FF = &C.FFVmFDG[(size_t)NV * nd * e];
+    for (int z = 0; z < nd; ++z) {
+      real us[NVMAX];
+      for (int v = 0; v < NV; ++v) us[v] = U[NV * z + v] + dt * FF[NV * z + v] * (1. - C.alpha[e]);
+      p_safe[z] = CorrPressure(C, us);
+      if (p_safe[z] < 0. || us[0] < 0.) { if (!C.corrErr) C.corrErr = e + 1; }
+    }
+    auto correct = [&](double corr) {
+      const double alphacont = C.alpha[e];
+      C.alpha[e] = C.alpha[e] + corr * sdt;
+      if (C.alpha[e] > alpha_maxPosit) {
+        C.alpha[e] = alpha_maxPosit;
+        corr = (alpha_maxPosit - alphacont) * dt;
+      }
+      for (int z = 0; z < NV * nd; ++z) {
+        U[z] = U[z] + corr * FF[z];
+        Ut[z] = Ut[z] + (C.alpha[e] - alphacont) * FF[z];
+      }
+    };
+    // density
+    double corr = -eps;
+    for (int z = 0; z < nd; ++z) {
+      const double us0 = val(U[NV * z]) + dt * val(FF[NV * z]) * (1. - C.alpha[e]);
+      const double a = C.P.posit_corr_factor * us0 - val(U[NV * z]);
+      if (a > 0.) {
+        if (std::fabs(val(FF[NV * z])) < eps) continue;
+        corr = std::max(corr, a / val(FF[NV * z]));
+      }
+    }
+    if (corr > 0.) correct(corr);
+    // pressure
+    corr = -eps;
+    for (int z = 0; z < nd; ++z) {
+      double pres = val(CorrPressure(C, &U[NV * z]));
+      const double p_goal = C.P.posit_corr_factor * val(p_safe[z]);
+      double ap = p_goal - pres;
+      if (ap <= 0.) continue;
+      real Uc[NVMAX], dp[NVMAX];
+      for (int v = 0; v < NV; ++v) Uc[v] = U[NV * z + v];
+      double corr1 = 0.0;
+      for (int it = 1; it <= C.P.posit_max_iter; ++it) {
+        CorrDpdU(C, Uc, dp);
+        real dpa = 0.;
+        for (int v = 0; v < NV; ++v) dpa = dpa + dp[v] * FF[NV * z + v];
+        if (std::fabs(val(dpa)) < eps) break;
+        corr1 = corr1 + ap / val(dpa);
+        for (int v = 0; v < NV; ++v) Uc[v] = U[NV * z + v] + corr1 * FF[NV * z + v];
+        pres = val(CorrPressure(C, Uc));
+        ap = p_goal - pres;
+        if (ap <= 2.220446049250313e-16 && ap > -NEWTON_ABSTOL * p_goal) break;
+      }
+      corr = std::max(corr, corr1);
+    }
+    if (corr > 0.) correct(corr);
+  }
+}
+
 // TimeStepByLSERKW2, timedisc/timedisc.f90:424-480
 // TimeStepByLSERKK3, timedisc.f90:489-542 (S2 and Uprev as extra registers)
 void TimeStepLSERKK3(Case& C, double t, double dt) {
@@ -2201,11 +2301,14 @@ void TimeStepSSPRK2(Case& C, double t, double dt) {
   std::vector<double> b_dt(n + 1);
   for (int s = 1; s <= n; ++s) b_dt[s] = T.b[s] * dt;
   std::vector<real> r0(C.U.begin(), C.U.end()), r1(nt, real(0.));
+  const bool corr = C.P.nfvse && C.P.nfvse_corr;
   DGTimeDerivative(C, t);
   for (size_t z = 0; z < nt; ++z) C.U[z] = C.U[z] + C.Ut[z] * b_dt[1];
+  if (corr) ApplyNFVSECorrection(C, b_dt[1]);
   for (int s = 2; s <= n - 1; ++s) {
     DGTimeDerivative(C, t + dt * T.c[s]);
     for (size_t z = 0; z < nt; ++z) C.U[z] = C.U[z] * T.d[s] + r0[z] * T.A[s] + C.Ut[z] * b_dt[s];
+    if (corr) ApplyNFVSECorrection(C, b_dt[s]);
     for (size_t z = 0; z < nt; ++z) {
       if (s == 2) r1[z] = C.U[z] * T.e[s];
       else if (s == 3) r1[z] = r1[z] + C.U[z] * T.e[s];
@@ -2214,6 +2317,7 @@ void TimeStepSSPRK2(Case& C, double t, double dt) {
   }
   DGTimeDerivative(C, t + dt * T.c[n]);
   for (size_t z = 0; z < nt; ++z) C.U[z] = C.U[z] * T.d[n] + r0[z] * T.A[n] + C.Ut[z] * b_dt[n] + r1[z];
+  if (corr) ApplyNFVSECorrection(C, b_dt[n]);
 }
 
 // TimeStepBySSPRK33, timedisc.f90:647-687
@@ -2241,11 +2345,13 @@ void TimeStepLSERK(Case& C, double t, double dt) {
   DGTimeDerivative(C, t);
   for (size_t z = 0; z < nt; ++z) C.UtTmp[z] = C.Ut[z];
   for (size_t z = 0; z < nt; ++z) C.U[z] = C.U[z] + C.Ut[z] * b_dt[1];
+  if (C.P.nfvse && C.P.nfvse_corr) ApplyNFVSECorrection(C, b_dt[1]);
   for (int s = 2; s <= C.nRKStages; ++s) {
     double ts = t + dt * C.RKc[s];
     DGTimeDerivative(C, ts);
     for (size_t z = 0; z < nt; ++z) C.UtTmp[z] = C.Ut[z] - C.UtTmp[z] * C.RKA[s];  // VAXPBY ConstOut
     for (size_t z = 0; z < nt; ++z) C.U[z] = C.U[z] + C.UtTmp[z] * b_dt[s];
+    if (C.P.nfvse && C.P.nfvse_corr) ApplyNFVSECorrection(C, b_dt[s]);
   }
 }
 
@@ -2277,6 +2383,15 @@ void* orc_create(const orc_params* p) {
       C->alphaMaster.assign(C->nSides, 0.);
       C->alphaSlave.assign(C->nSides, 0.);
       ComputeSubcellMetrics(*C);
+      const int sfm = p->sub_fv_method;
+      if (sfm < 1 || sfm > 4) throw std::runtime_error("SubFVMethod not implemented");
+      if (sfm >= 3 && !HasDissipMatrices(*C))
+        throw std::runtime_error("SubFVMethod 3/4 need a Riemann solver with RiemannVolFluxAndDissipMatrices");
+      if (p->nfvse_corr) {
+        if (C->rk->type == 1)  // timedisc_vars.f90:111-114
+          throw std::runtime_error("NFVSE correction is only implemented for LSERKW2 methods and ssprk4-5");
+        C->FFVmFDG.assign((size_t)C->nVar * C->nDOFElem * C->nElems, 0.);
+      }
     }
     size_t nt = (size_t)C->nVar * C->nDOFElem * C->nElems;
     size_t nf = (size_t)C->nVar * C->np * C->np * C->nSides;
@@ -2561,6 +2676,8 @@ void orc_riemann_point(void* h, const double* UL, const double* UR, const double
     F[b + 2] = val(nv[2] * f2 + t1[2] * f3 + t2[2] * f4);
   }
 }
+
+int orc_corr_error(void* h) { return ((Case*)h)->corrErr; }
 
 void orc_get_alpha(void* h, double* alpha) {
   Case* C = (Case*)h;

@@ -50,7 +50,7 @@ typedef struct orc_params {
   double mhd_ref_state[2][8];  /* RefState 1 and 2 (rho,u,v,w,p,B1,B2,B3) */
   double ini_center[3];   /* IniCenter */
   double ini_halfwidth;   /* IniHalfwidth */
-  /* NFVSE shock capturing (shockcapturing/nfvse.f90:63-260), SubFVMethod = 1, 2 */
+  /* NFVSE shock capturing (shockcapturing/nfvse.f90:63-260), SubFVMethod = 1..4 */
   int nfvse;              /* SHOCK_NFVSE on/off */
   int compute_alpha;      /* ComputeAlpha: 1 Persson-Peraire indicator, 3 fixed ShockBlendCoef */
   double shock_blend_coef;
@@ -59,8 +59,13 @@ typedef struct orc_params {
   int space_prop_sweeps;
   double time_rel_factor;
   int indicator_quantity; /* ShockIndicatorQuantity: 1 Density, 2 Pressure, 3 DensityTimesPressure, 4 KinEnergy */
-  int sub_fv_method;      /* SubFVMethod: 1 first order, 2 TVD (minmod reconstruction of primitive variables) */
-  int recons_boundaries;  /* ReconsBoundaries (SubFVMethod 2): 1 none, 2 central, 3 neighbour element */
+  int sub_fv_method;      /* SubFVMethod: 1 first order, 2 TVD (minmod reconstruction of primitive variables),
+                             3 TVD-ES (TVD states, entropy-stable switch), 4 TVD-Fjordholm (reconstruction of
+                             the scaled entropy variables) */
+  int recons_boundaries;  /* ReconsBoundaries (SubFVMethod 2-4): 1 none, 2 central, 3 neighbour element */
+  int nfvse_corr;         /* NFVSE_CORR (CMake FLUXO_SHOCK_NFVSE_CORR): positivity correction after each stage */
+  double posit_corr_factor;  /* PositCorrFactor */
+  int posit_max_iter;     /* PositMaxIter */
 } orc_params;
 
 void* orc_create(const orc_params* p);
@@ -108,6 +113,8 @@ void orc_riemann_point(void* h, const double* UL, const double* UR, const double
 double orc_ln_mean(double aL, double aR);
 /* NFVSE: blending coefficient alpha(nElems) of the last right-hand side. */
 void orc_get_alpha(void* h, double* alpha);
+/* NFVSE_CORR: element + 1 whose safe state had negative density or pressure (0: none). */
+int orc_corr_error(void* h);
 /* MHD: the GLM cleaning speed GLM_ch (set by CALCTIMESTEP, or explicitly). */
 void orc_set_glm_ch(void* h, double ch);
 double orc_get_glm_ch(void* h);

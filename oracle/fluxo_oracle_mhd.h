@@ -395,11 +395,13 @@ inline void MHD_EntropyStableLLF(const Case& C, const real* UL, const real* UR, 
   F[8] = F[8] - (LM * tau) * (psiA * Vj[4] + Vj[8]);
 }
 
-// EntropyStableDerigsFlux / EntropyStableFloGorFlux (Riemann 14 / 15): EC flux minus
-// 1/2 R |D| T R^T [v], mhd/riemann.f90:1224-1632 and :1633-2042 (same eigen-decomposition).
-inline void MHD_EntropyStable9Wave(const Case& C, const real* UL, const real* UR, bool flogor, real* F) {
-  real Vj[9], pL, pR, bL, bR;
-  MHD_EntropyJump(C, UL, UR, pL, pR, bL, bR, Vj);
+// Flux and dissipation matrices of the entropy-stable 9-wave solvers (Riemann 14 Derigs, 15 FloGor):
+// EntropyStableDerigsFlux_VolFluxAndDissipMatrices mhd/riemann.f90:1287-1622 and
+// EntropyStableFloGorFlux_VolFluxAndDissipMatrices :1695-2042: the EC flux F, the diagonal D and the
+// right eigenvectors R[row][col] (the ES flux is F - 1/2 R D R^T [v]).
+// pL, pR, bL, bR: the pressures and betas of MHD_EntropyJump
+inline void MHD_ES9WaveMatrices(const Case& C, const real* UL, const real* UR, bool flogor, const real& pL,
+                                const real& pR, const real& bL, const real& bR, real* F, real* Dm, real R[9][9]) {
   const double ch = C.GLM_ch;
   real sL = 1. / UL[0], sR = 1. / UR[0];
   real uL[3], uR[3];
@@ -470,7 +472,7 @@ inline void MHD_EntropyStable9Wave(const Case& C, const real* UL, const real* UR
   real psiFm = 0.5 * alf * rhoLN * u2A + abeta * als * rhoLN * bperp + alf * rhoLN * aLN * aLN * C.sKappaM1 -
                alf * cf * rhoLN * uA[0] + als * cs * rhoLN * sg * t23;
   real sqRho = sqrt(rhoLN), sqRhoA = sqrt(rhoA);
-  real R[9][9];  // R[row][col] = Rmatrix(row+1, col+1)
+  // R[row][col] = Rmatrix(row+1, col+1)
   real c1[9] = {alf * rhoLN, alf * rhoLN * (uA[0] + cf), rhoLN * (alf * uA[1] - als * cs * be2 * sg),
                 rhoLN * (alf * uA[2] - als * cs * be3 * sg), psiFp, 0.0, als * abeta * be2 * sqRho,
                 als * abeta * be3 * sqRho, 0.0};
@@ -500,9 +502,16 @@ inline void MHD_EntropyStable9Wave(const Case& C, const real* UL, const real* UR
   real T1 = 0.5 / C.kappa / rhoLN, T2 = 0.25 / betaA / rhoLN / rhoLN, T4 = 0.25 / betaA,
        T5 = rhoLN * C.kappaM1 / C.kappa;
   real Tm[9] = {T1, T2, T1, T4, T5, T4, T1, T2, T1};
-  real Dm[9];
   for (int z = 0; z < 9; ++z) Dm[z] = ((1. - phi) * fabs(wave[z]) + phi * LM) * Tm[z];
-  // Fstar = Fstar - 0.5*MATMUL(R, D*MATMUL(R^T, V_jump))
+}
+
+// EntropyStableDerigsFlux / EntropyStableFloGorFlux (Riemann 14 / 15), mhd/riemann.f90:1224-1283,
+// :1633-1691: Fstar - 0.5*MATMUL(R, D*MATMUL(R^T, V_jump))
+inline void MHD_EntropyStable9Wave(const Case& C, const real* UL, const real* UR, bool flogor, real* F) {
+  real Vj[9], pL, pR, bL, bR;
+  MHD_EntropyJump(C, UL, UR, pL, pR, bL, bR, Vj);
+  real Dm[9], R[9][9];
+  MHD_ES9WaveMatrices(C, UL, UR, flogor, pL, pR, bL, bR, F, Dm, R);
   real w[9];
   for (int c = 0; c < 9; ++c) {
     real s = 0.;
@@ -515,6 +524,7 @@ inline void MHD_EntropyStable9Wave(const Case& C, const real* UL, const real* UR
     F[r] = F[r] - 0.5 * s;
   }
 }
+
 
 // RiemannSolverByHLLC, mhd/riemann.f90:371-501 (with GLM), HLL state EvalHLLState :733-757
 inline void MHD_HLLC(const Case& C, const real* UL, const real* UR, real* F) {

@@ -1,8 +1,9 @@
 // ORACLE — test infrastructure only (part of fluxo_oracle.cpp, included inside its namespace).
 // CPU restatement of the reference's NFVSE shock capturing (shockcapturing/nfvse.f90,
 // nfvse_mpi.f90, indicators/indicators.f90): Persson-Peraire indicator, blending coefficient,
-// its space propagation, the first-order subcell finite-volume volume integral on the LGL
-// subcells (SubFVMethod = 1) and its blending with the split-form volume integral.
+// its space propagation, the subcell finite-volume volume integral on the LGL subcells (SubFVMethod
+// 1 first order, 2 TVD, 3 TVD-ES, 4 TVD-Fjordholm), its blending with the split-form volume integral
+// and the positivity correction of NFVSE_CORR (Apply_NFVSE_Correction).
 
 // Sub-cell metrics, nfvse.f90:261-378: for direction d, subcell face f = -1..N and transverse
 // point (a,b): normal, tangents and the norm of the (unnormalised) face metric
@@ -207,10 +208,103 @@ void ReconstructLine(const Case& C, const real* pr, const real* extL, const real
   }
 }
 
-// External state of ReconsBoundaries 3 (Get_externalU, nfvse.f90:1621-1683): at the boundary node of
-// local side s of element e, the neighbour's face state (U_slave on a master side, U_master on a
-// slave side); returned as primitive variables at [(a + n*b)*NV], (a,b) the tangential node indexes
-void ExternalPrim(const Case& C, int e, int s, std::vector<real>& ext) {
+// RotateState / RotateFluxBack (navierstokes/riemann.f90:218-246, mhd/riemann.f90:185-217): the
+// momentum (and for MHD the magnetic field) into the frame (nv, t1, t2) and back
+inline void FV_Rotate(const Case& C, const real* a, const double* nv, const double* t1, const double* t2, real* o) {
+  for (int v = 0; v < C.nVar; ++v) o[v] = a[v];
+  for (int b = 1; b <= (C.mhd ? 5 : 1); b += 4) {
+    o[b] = a[b] * nv[0] + a[b + 1] * nv[1] + a[b + 2] * nv[2];
+    o[b + 1] = a[b] * t1[0] + a[b + 1] * t1[1] + a[b + 2] * t1[2];
+    o[b + 2] = a[b] * t2[0] + a[b + 1] * t2[1] + a[b + 2] * t2[2];
+  }
+}
+inline void FV_RotateBack(const Case& C, real* F, const double* nv, const double* t1, const double* t2) {
+  for (int b = 1; b <= (C.mhd ? 5 : 1); b += 4) {
+    real f2 = F[b], f3 = F[b + 1], f4 = F[b + 2];
+    for (int c = 0; c < 3; ++c) F[b + c] = nv[c] * f2 + t1[c] * f3 + t2[c] * f4;
+  }
+}
+// ConsToEntropy of the equation system (navierstokes/equation_vars.f90:362-391, mhd/equation_vars.f90:330-361)
+inline void FV_ConsToEntropy(const Case& C, const real* U, real* W) {
+  if (C.mhd) MHD_ConsToEntropy(C, U, W);
+  else ConsToEntropy(C, U, W);
+}
+// Whether the Riemann solver provides RiemannVolFluxAndDissipMatrices (navierstokes/equation.f90:381-404:
+// 4, 44, 33; mhd/equation.f90:367-386: 14, 15), which SubFVMethod 3 and 4 need (nfvse.f90:174-187)
+inline bool HasDissipMatrices(const Case& C) {
+  const int rs = C.P.riemann;
+  return C.mhd ? (rs == 14 || rs == 15) : (rs == 4 || rs == 44 || rs == 33);
+}
+// RiemannVolFluxAndDissipMatrices on rotated states: EC flux F, diagonal D, right eigenvectors R[row][col]
+inline void FV_DissipMatrices(const Case& C, const real* L, const real* R, real* F, real* D, real Rm[NVMAX][NVMAX]) {
+  if (C.mhd) {
+    real R9[9][9], Vj[9], pL, pR, bL, bR;
+    MHD_EntropyJump(C, L, R, pL, pR, bL, bR, Vj);
+    MHD_ES9WaveMatrices(C, L, R, C.P.riemann == 15, pL, pR, bL, bR, F, D, R9);
+    for (int r = 0; r < 9; ++r)
+      for (int c = 0; c < 9; ++c) Rm[r][c] = R9[r][c];
+  } else {
+    real R5[5][5];
+    ES_VolFluxAndDissipMatrices(C, C.P.riemann, L, R, F, D, R5);
+    for (int r = 0; r < 5; ++r)
+      for (int c = 0; c < 5; ++c) Rm[r][c] = R5[r][c];
+  }
+}
+// x = R^T v: x(c) = sum_r R(r,c) v(r) (matmul(RmatT, v))
+inline void FV_RT(int NV, const real Rm[NVMAX][NVMAX], const real* v, real* x) {
+  for (int c = 0; c < NV; ++c) {
+    real s = 0.;
+    for (int r = 0; r < NV; ++r) s = s + Rm[r][c] * v[r];
+    x[c] = s;
+  }
+}
+// F = F - 0.5 R (D x) (matmul(Rmat, Dmat*x))
+inline void FV_Dissipate(int NV, const real Rm[NVMAX][NVMAX], const real* D, const real* x, real* F) {
+  real y[NVMAX];
+  for (int c = 0; c < NV; ++c) y[c] = D[c] * x[c];
+  for (int r = 0; r < NV; ++r) {
+    real s = 0.;
+    for (int c = 0; c < NV; ++c) s = s + Rm[r][c] * y[c];
+    F[r] = F[r] - 0.5 * s;
+  }
+}
+
+// AdvRiemannRecons (nfvse.f90:1036-1090) of one subcell face plane, SubFVMethod 3: the EC flux and the
+// dissipation matrices of the nodal states, and the dissipation of the entropy jump of the reconstructed
+// states (UL_r, UR_r) unless, in some component, it has the opposite sign to the nodal jump (beyond
+// -1e-10), in which case the nodal jump is used.  Output rotated back to the physical frame.
+void SubcellTVD2ES(const Case& C, int npts, const real* UL, const real* UR, const real* ULr, const real* URr,
+                   const double* nv, const double* t1, const double* t2, real* F) {
+  const int NV = C.nVar;
+  for (int z = 0; z < npts; ++z) {
+    const double *n = nv + 3 * z, *a = t1 + 3 * z, *b = t2 + 3 * z;
+    real L[NVMAX], R[NVMAX], Lr[NVMAX], Rr[NVMAX];
+    FV_Rotate(C, UL + NV * z, n, a, b, L);
+    FV_Rotate(C, UR + NV * z, n, a, b, R);
+    FV_Rotate(C, ULr + NV * z, n, a, b, Lr);
+    FV_Rotate(C, URr + NV * z, n, a, b, Rr);
+    real D[NVMAX], Rm[NVMAX][NVMAX];
+    real* Fz = F + NV * z;
+    FV_DissipMatrices(C, L, R, Fz, D, Rm);
+    real vL[NVMAX], vR[NVMAX], vLr[NVMAX], vRr[NVMAX], dv[NVMAX], dvr[NVMAX], x[NVMAX], xr[NVMAX];
+    FV_ConsToEntropy(C, L, vL);
+    FV_ConsToEntropy(C, R, vR);
+    FV_ConsToEntropy(C, Lr, vLr);
+    FV_ConsToEntropy(C, Rr, vRr);
+    for (int v = 0; v < NV; ++v) { dv[v] = vR[v] - vL[v]; dvr[v] = vRr[v] - vLr[v]; }
+    FV_RT(NV, Rm, dv, x);
+    FV_RT(NV, Rm, dvr, xr);
+    bool notES = false;
+    for (int v = 0; v < NV; ++v)
+      if (x[v] * xr[v] < -1.e-10) notES = true;
+    FV_Dissipate(NV, Rm, D, notES ? x : xr, Fz);
+    FV_RotateBack(C, Fz, n, a, b);
+  }
+}
+
+// External states of ReconsBoundaries 3 (Get_externalU, nfvse.f90:1621-1683) as conservative variables
+// at [(a + n*b)*NV] (ExternalPrim below converts them to primitive variables)
+void ExternalCons(const Case& C, int e, int s, std::vector<real>& ext) {
   const int n = C.np, N = C.N, NV = C.nVar;
   ext.assign((size_t)n * n * NV, real(0.));
   const int sideID = C.ElemToSide[2 * (6 * e + (s - 1))] - 1;
@@ -222,16 +316,132 @@ void ExternalPrim(const Case& C, int e, int s, std::vector<real>& ext) {
       int ijk[3];
       SideToVol(N, 0, p, q, master ? 0 : flipE, s, ijk);
       const real* Uf = master ? &C.Uslave[C.fac(0, p, q, sideID)] : &C.Umaster[C.fac(0, p, q, sideID)];
-      real pr[NVMAX];
-      FV_ConsToPrim(C, Uf, pr);
       const int a = ijk[tan1[s - 1]], b = ijk[tan2[s - 1]];
-      for (int v = 0; v < NV; ++v) ext[(a + n * b) * NV + v] = pr[v];
+      for (int v = 0; v < NV; ++v) ext[(a + n * b) * NV + v] = Uf[v];
     }
 }
 
-// VolInt_NFVSE (nfvse.f90:475-565) with Compute_FVFluxes_1st_Order (:566-673) or
-// Compute_FVFluxes_TVD (:674-815) and Compute_FVFluxes_1D (:1389-1447): Ut = (1-alpha) Ut + alpha F_FV
-// on the blended elements
+// External state of ReconsBoundaries 3 (Get_externalU, nfvse.f90:1621-1683): at the boundary node of
+// local side s of element e, the neighbour's face state (U_slave on a master side, U_master on a
+// slave side); returned as primitive variables at [(a + n*b)*NV], (a,b) the tangential node indexes
+void ExternalPrim(const Case& C, int e, int s, std::vector<real>& ext) {
+  const int NV = C.nVar;
+  std::vector<real> cons;
+  ExternalCons(C, e, s, cons);
+  ext.assign(cons.size(), real(0.));
+  for (size_t z = 0; z < cons.size() / NV; ++z) FV_ConsToPrim(C, &cons[z * NV], &ext[z * NV]);
+}
+
+// Compute_FVFluxes_1D_TVD_Fjordholm (nfvse.f90:1187-1386) for one direction of element e: node(x, a, b)
+// gives the volume index of the line position x at the transverse point (a,b); Fout[(x*npt + p)*NV] the
+// rotated-back ES fluxes of the subcell faces x = 0..N-1 (before the non-conservative terms and the norm).
+// The central EC flux uses the nodal states; the dissipation acts on the jump of the minmod-reconstructed
+// scaled entropy variables w = R^T v, each face's w computed with that face's eigenvectors.
+template <class NodeFn>
+void FjordholmDirection(const Case& C, int e, int d, NodeFn node, const std::vector<real>& extL,
+                        const std::vector<real>& extR, std::vector<real>& Fout) {
+  const int n = C.np, N = C.N, NV = C.nVar, npt = n * n;
+  std::vector<double> sdxR(N), sdxL(N), rL(N), rR(N);
+  double sumWm1 = C.wGP[0] - 1.;
+  for (int i = 1; i <= N - 1; ++i) {  // InitNFVSE :218-238
+    sdxR[i] = 1.0 / (C.xGP[i + 1] - C.xGP[i]);
+    sdxL[i] = 1.0 / (C.xGP[i] - C.xGP[i - 1]);
+    rL[i] = sumWm1 - C.xGP[i];
+    sumWm1 = sumWm1 + C.wGP[i];
+    rR[i] = sumWm1 - C.xGP[i];
+  }
+  const int rb = C.P.recons_boundaries;
+  auto metric = [&](int f, int a, int b, double* nvv, double* t1v, double* t2v) {
+    const size_t s = SubcellIdx(C, e, d, f, a, b);
+    for (int c = 0; c < 3; ++c) { nvv[c] = C.scNv[3 * s + c]; t1v[c] = C.scT1[3 * s + c]; t2v[c] = C.scT2[3 * s + c]; }
+  };
+  // per face x and point p: EC flux, D, R and the scaled entropy variables of both nodes
+  std::vector<real> Fc((size_t)N * npt * NV), Dd((size_t)N * npt * NV), Rr((size_t)N * npt * NVMAX * NVMAX),
+      wL((size_t)N * npt * NV), wR((size_t)N * npt * NV);
+  for (int x = 0; x < N; ++x)
+    for (int b = 0; b < n; ++b)
+      for (int a = 0; a < n; ++a) {
+        const int p = a + n * b;
+        const size_t o = ((size_t)x * npt + p) * NV;
+        double nvv[3], t1v[3], t2v[3];
+        metric(x, a, b, nvv, t1v, t2v);
+        real L[NVMAX], R[NVMAX], Rm[NVMAX][NVMAX], vL[NVMAX], vR[NVMAX];
+        FV_Rotate(C, &C.U[NV * node(x, a, b)], nvv, t1v, t2v, L);
+        FV_Rotate(C, &C.U[NV * node(x + 1, a, b)], nvv, t1v, t2v, R);
+        FV_DissipMatrices(C, L, R, &Fc[o], &Dd[o], Rm);
+        for (int r = 0; r < NV; ++r)
+          for (int c = 0; c < NV; ++c) Rr[((size_t)x * npt + p) * NVMAX * NVMAX + r * NVMAX + c] = Rm[r][c];
+        FV_ConsToEntropy(C, L, vL);
+        FV_ConsToEntropy(C, R, vR);
+        FV_RT(NV, Rm, vL, &wL[o]);
+        FV_RT(NV, Rm, vR, &wR[o]);
+      }
+  // scaled entropy variables of the neighbour's boundary state (ReconsBoundaries 3) across the element
+  // face: U_ext and node 1 (left, face -1 metrics), node N-1 and U_ext (right, face N metrics)
+  auto boundaryW = [&](int f, int a, int b, const real* Ua, const real* Ub, real* w0L, real* w0R) {
+    double nvv[3], t1v[3], t2v[3];
+    metric(f, a, b, nvv, t1v, t2v);
+    real L[NVMAX], R[NVMAX], Fd[NVMAX], D0[NVMAX], R0[NVMAX][NVMAX], vL[NVMAX], vR[NVMAX];
+    FV_Rotate(C, Ua, nvv, t1v, t2v, L);
+    FV_Rotate(C, Ub, nvv, t1v, t2v, R);
+    FV_ConsToEntropy(C, L, vL);
+    FV_ConsToEntropy(C, R, vR);
+    FV_DissipMatrices(C, L, R, Fd, D0, R0);
+    FV_RT(NV, R0, vL, w0L);
+    FV_RT(NV, R0, vR, w0R);
+  };
+  std::vector<real> wtR((size_t)n * npt * NV, real(0.)), wtL((size_t)n * npt * NV, real(0.));
+  auto at = [&](int x, int p) { return ((size_t)x * npt + p) * NV; };
+  for (int b = 0; b < n; ++b)
+    for (int a = 0; a < n; ++a) {
+      const int p = a + n * b;
+      real w0L[NVMAX], w0R[NVMAX];
+      // first DOF
+      if (rb == 3) boundaryW(-1, a, b, &extL[(size_t)p * NV], &C.U[NV * node(1, a, b)], w0L, w0R);
+      for (int v = 0; v < NV; ++v) {
+        const real jl = wR[at(0, p) + v] - wL[at(0, p) + v];
+        if (rb == 1) wtR[at(0, p) + v] = wL[at(0, p) + v];
+        else if (rb == 2) wtR[at(0, p) + v] = wL[at(0, p) + v] + jl * sdxL[1] * C.wGP[0];
+        else wtR[at(0, p) + v] = wL[at(0, p) + v] + MinMod(sdxL[1] * jl, sdxL[1] * (w0R[v] - w0L[v])) * C.wGP[0];
+      }
+      // middle DOFs
+      for (int i = 1; i <= N - 1; ++i)
+        for (int v = 0; v < NV; ++v) {
+          const real sg = MinMod(sdxR[i] * (wR[at(i, p) + v] - wL[at(i, p) + v]),
+                                 sdxL[i] * (wR[at(i - 1, p) + v] - wL[at(i - 1, p) + v]));
+          wtR[at(i, p) + v] = wL[at(i, p) + v] + sg * rR[i];
+          wtL[at(i, p) + v] = wR[at(i - 1, p) + v] + sg * rL[i];
+        }
+      // last DOF
+      if (rb == 3) boundaryW(N, a, b, &C.U[NV * node(N - 1, a, b)], &extR[(size_t)p * NV], w0L, w0R);
+      for (int v = 0; v < NV; ++v) {
+        const real jr = wR[at(N - 1, p) + v] - wL[at(N - 1, p) + v];
+        if (rb == 1) wtL[at(N, p) + v] = wR[at(N - 1, p) + v];
+        else if (rb == 2) wtL[at(N, p) + v] = wR[at(N - 1, p) + v] - jr * sdxL[1] * C.wGP[N];
+        else wtL[at(N, p) + v] = wR[at(N - 1, p) + v] - MinMod(sdxL[1] * jr, sdxL[1] * (w0R[v] - w0L[v])) * C.wGP[N];
+      }
+    }
+  Fout.assign((size_t)N * npt * NV, real(0.));
+  for (int x = 0; x < N; ++x)
+    for (int b = 0; b < n; ++b)
+      for (int a = 0; a < n; ++a) {
+        const int p = a + n * b;
+        const size_t o = at(x, p);
+        real Rm[NVMAX][NVMAX], jw[NVMAX];
+        for (int r = 0; r < NV; ++r)
+          for (int c = 0; c < NV; ++c) Rm[r][c] = Rr[((size_t)x * npt + p) * NVMAX * NVMAX + r * NVMAX + c];
+        for (int v = 0; v < NV; ++v) { Fout[o + v] = Fc[o + v]; jw[v] = wtL[at(x + 1, p) + v] - wtR[o + v]; }
+        FV_Dissipate(NV, Rm, &Dd[o], jw, &Fout[o]);
+        double nvv[3], t1v[3], t2v[3];
+        metric(x, a, b, nvv, t1v, t2v);
+        FV_RotateBack(C, &Fout[o], nvv, t1v, t2v);
+      }
+}
+
+// VolInt_NFVSE (nfvse.f90:475-565) with Compute_FVFluxes_1st_Order (:566-673), Compute_FVFluxes_TVD
+// (:674-815), Compute_FVFluxes_TVD2ES (:826-1090) or Compute_FVFluxes_TVD_Fjordholm (:1101-1386) and
+// Compute_FVFluxes_1D (:1389-1447): Ut = (1-alpha) Ut + alpha F_FV on the blended elements; with
+// NFVSE_CORR on every element, keeping FFV_m_FDG = (F_FV - Ut) (-sJ) for Apply_NFVSE_Correction
 void VolIntNFVSE(Case& C) {
   const int n = C.np, N = C.N, NV = C.nVar, npt = n * n;
   if (C.P.space_prop_sweeps > 0) {
@@ -250,7 +460,10 @@ void VolIntNFVSE(Case& C) {
   std::vector<real> FL((size_t)3 * (n + 1) * npt * NV), FR((size_t)3 * (n + 1) * npt * NV);
   std::vector<real> UL((size_t)npt * NV), UR((size_t)npt * NV), F((size_t)npt * NV), G((size_t)npt * NV);
   // TVD: reconstructed face states of the Riemann problems, per direction and line
-  const bool tvd = C.P.sub_fv_method == 2;
+  const int sfm = C.P.sub_fv_method;
+  const bool tvd = sfm == 2 || sfm == 3;  // primitive-variable reconstruction (TVD2ES: for the ES switch)
+  const bool corr = C.P.nfvse_corr != 0;
+  std::vector<real> extCL, extCR, Fj;
   std::vector<real> RL((size_t)npt * NV), RR((size_t)npt * NV), pr((size_t)n * NV), pRl((size_t)n * NV),
       pLl((size_t)n * NV), recR((size_t)3 * n * npt * NV), recL((size_t)3 * n * npt * NV);
   std::vector<real> extL, extR;
@@ -258,7 +471,7 @@ void VolIntNFVSE(Case& C) {
   std::vector<double> nvb(3 * npt), t1b(3 * npt), t2b(3 * npt);
   auto fi = [&](int d, int x, int p) { return ((size_t)(d * (n + 1) + (x + 1)) * npt + p) * NV; };
   for (int e = 0; e < C.nElems; ++e) {
-    if (AlmostEqual(C.alpha[e], 0.0)) continue;
+    if (!corr && AlmostEqual(C.alpha[e], 0.0)) continue;
     std::fill(FL.begin(), FL.end(), real(0.));
     std::fill(FR.begin(), FR.end(), real(0.));
     for (int d = 0; d < 3; ++d) {
@@ -284,6 +497,13 @@ void VolIntNFVSE(Case& C) {
             }
           }
       }
+      if (sfm == 4) {
+        if (C.P.recons_boundaries == 3) {
+          ExternalCons(C, e, sideMinus[d], extCL);
+          ExternalCons(C, e, sidePlus[d], extCR);
+        }
+        FjordholmDirection(C, e, d, node, extCL, extCR, Fj);
+      }
       for (int x = 0; x < N; ++x) {
         for (int b = 0; b < n; ++b)
           for (int a = 0; a < n; ++a) {
@@ -297,12 +517,18 @@ void VolIntNFVSE(Case& C) {
               nvb[3 * p + c] = C.scNv[3 * s + c]; t1b[3 * p + c] = C.scT1[3 * s + c]; t2b[3 * p + c] = C.scT2[3 * s + c];
             }
           }
-        if (tvd) {
+        if (sfm == 4) {
+          for (int z = 0; z < npt * NV; ++z) F[z] = Fj[(size_t)x * npt * NV + z];
+        } else if (tvd) {
           for (int z = 0; z < npt * NV; ++z) {
             RL[z] = recR[(size_t)x * npt * NV + z];
             RR[z] = recL[(size_t)(x + 1) * npt * NV + z];
           }
-          SubcellRiemann(C, npt, RL.data(), RR.data(), nvb.data(), t1b.data(), t2b.data(), F.data());
+          if (sfm == 3)
+            SubcellTVD2ES(C, npt, UL.data(), UR.data(), RL.data(), RR.data(), nvb.data(), t1b.data(), t2b.data(),
+                          F.data());
+          else
+            SubcellRiemann(C, npt, RL.data(), RR.data(), nvb.data(), t1b.data(), t2b.data(), F.data());
         } else {
           SubcellRiemann(C, npt, UL.data(), UR.data(), nvb.data(), t1b.data(), t2b.data(), F.data());
         }
@@ -333,6 +559,7 @@ void VolIntNFVSE(Case& C) {
                        sW[j] * (FR[fi(1, j, i + n * k) + v] - FL[fi(1, j - 1, i + n * k) + v]) +
                        sW[k] * (FR[fi(2, k, i + n * j) + v] - FL[fi(2, k - 1, i + n * j) + v]);
             real& ut = C.Ut[C.vol(v, i, j, k, e)];
+            if (corr) C.FFVmFDG[C.vol(v, i, j, k, e)] = (ffv - ut) * (-C.sJ[C.nod(i, j, k, e)]);
             ut = (1. - al) * ut + al * ffv;
           }
   }

@@ -70,6 +70,9 @@ class OrcParams(ctypes.Structure):
         ("indicator_quantity", ctypes.c_int),
         ("sub_fv_method", ctypes.c_int),
         ("recons_boundaries", ctypes.c_int),
+        ("nfvse_corr", ctypes.c_int),
+        ("posit_corr_factor", ctypes.c_double),
+        ("posit_max_iter", ctypes.c_int),
     ]
 
 
@@ -85,7 +88,7 @@ DEFAULTS = dict(
     ini_center=(0.0, 0.0, 0.0), ini_halfwidth=0.1,
     nfvse=0, compute_alpha=1, shock_blend_coef=0.0, modal_threshold=1, alpha_max=0.5, alpha_min=0.01,
     space_prop_factor=0.5, space_prop_sweeps=1, time_rel_factor=0.0, indicator_quantity=3,
-    sub_fv_method=1, recons_boundaries=1,
+    sub_fv_method=1, recons_boundaries=1, nfvse_corr=0, posit_corr_factor=0.1, posit_max_iter=10,
 )
 
 
@@ -134,6 +137,8 @@ def _lib(counting=False):
     lib.orc_ln_mean.restype = d
     lib.orc_ln_mean.argtypes = [d, d]
     lib.orc_get_alpha.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    lib.orc_corr_error.restype = ctypes.c_int
+    lib.orc_corr_error.argtypes = [ctypes.c_void_p]
     lib.orc_set_glm_ch.argtypes = [ctypes.c_void_p, d]
     lib.orc_get_glm_ch.restype = d
     lib.orc_get_glm_ch.argtypes = [ctypes.c_void_p]
@@ -271,6 +276,11 @@ class OracleCase:
         a = np.zeros(self.nElems)
         self.lib.orc_get_alpha(self.h, _ptr(a))
         return a
+
+    @property
+    def corr_error(self):
+        """NFVSE_CORR: element + 1 whose safe state was not admissible (0: none)."""
+        return self.lib.orc_corr_error(self.h)
 
     @property
     def glm_ch(self):
