@@ -349,6 +349,12 @@ struct Case {
   // basis (double), dg/dg.f90:181-252
   std::vector<double> xGP, wGP, wBary, D, D_T, Dhat, Dhat_T, Dvolsurf, Dvolsurf_T, Lminus, Lplus;
   double L_HatMinus0, L_HatPlus0;
+  // Gauss nodes (PP_NodeType = 1): L_HatMinus(0:N), the surface metrics of every element side
+  // SurfMetrics(3,0:N,0:N,6,nElems) in the master side's point order (mesh_vars.f90:67-70), and the
+  // entropy variables of the entropy-projected ProlongToFace (dg_vars.f90:54-61)
+  bool gauss = false;
+  std::vector<double> LhatMinus, SurfMetrics;
+  std::vector<real> Vent;
   // mesh
   std::vector<int> SideToElem, ElemToSide;   // 1-based ids, reference layout
   std::vector<int> S2V;                      // [((((s-1)*5+f)*np+q)*np+p)*np+l]*3
@@ -1142,6 +1148,20 @@ inline void ConsToEntropy(const Case& C, const real* U, real* W) {
   W[4] = -rho_sp;
 }
 
+// EntropyToCons, navierstokes/equation_vars.f90:434-469
+inline void EntropyToCons(const Case& C, const real* W, real* U) {
+  real rho_sp = -W[4];
+  real p_srho = 1. / rho_sp;
+  real u = W[1] * p_srho, v = W[2] * p_srho, w = W[3] * p_srho;
+  real v2s2 = 0.5 * (u * u + v * v + w * w);
+  real s = C.kappa - ((W[0] + rho_sp * v2s2) * C.kappaM1);
+  U[0] = pow(exp(-s) * p_srho, C.sKappaM1);
+  U[1] = u * U[0];
+  U[2] = v * U[0];
+  U[3] = w * U[0];
+  U[4] = U[0] * (p_srho * C.sKappaM1 + v2s2);
+}
+
 inline void ConsToPrim(const Case& C, const real* U, real* P) {  // equation_vars.f90:243-264
   real sRho = 1. / U[0];
   P[0] = U[0];
@@ -1359,7 +1379,8 @@ void CalcSource(Case& C, double t) {
 void InitBasis(Case& C) {
   int N = C.N, n = C.np;
   C.xGP.resize(n); C.wGP.resize(n); C.wBary.resize(n);
-  LGLNodesWeights(N, C.xGP.data(), C.wGP.data());
+  if (C.gauss) GaussNodesWeights(N, C.xGP.data(), C.wGP.data());  // InitInterpolation, NodeType 'GAUSS'
+  else LGLNodesWeights(N, C.xGP.data(), C.wGP.data());
   BaryWeights(N, C.xGP.data(), C.wBary.data());
   C.D.resize(n * n); C.D_T.resize(n * n); C.Dhat.resize(n * n); C.Dhat_T.resize(n * n);
   C.Dvolsurf.resize(n * n); C.Dvolsurf_T.resize(n * n);
@@ -1376,6 +1397,8 @@ void InitBasis(Case& C) {
   LagrangePolys(-1., N, C.xGP.data(), C.wBary.data(), C.Lminus.data());
   C.L_HatMinus0 = (1. / C.wGP[0]) * C.Lminus[0];
   C.L_HatPlus0 = (1. / C.wGP[N]) * C.Lplus[N];
+  C.LhatMinus.resize(n);  // L_HatMinus = MATMUL(Minv, L_Minus), dg.f90:222-226
+  for (int i = 0; i < n; ++i) C.LhatMinus[i] = (1. / C.wGP[i]) * C.Lminus[i];
   // Dvolsurf = 2*D - Minv*Vf^T*B*Vf, Vf rows (L_Minus, L_Plus), B = diag(-1,1)
   for (int i = 0; i < n; ++i)
     for (int j = 0; j < n; ++j) {
@@ -1508,17 +1531,32 @@ void CalcMetrics(Case& C) {
   std::vector<double> xGLg(ng), DGLg(ng * ng);
   Nodes(NG, NT_GL, xGLg.data());
   DerivMatrix(NG, xGLg.data(), DGLg.data());
-  std::vector<double> V_GLg_Ref = GetVdm(NG, NT_GL, NR, NT_GL, false);
-  std::vector<double> V_Ref_N = GetVdm(NR, NT_GL, N, NT_GL, true);
+  // solution nodes NodeType (metrics.f90:150-160): the Jacobian goes through NgeoRef points of NodeType
+  const NodeType NTS = C.gauss ? NT_GAUSS : NT_GL;
+  std::vector<double> V_GLg_Ref = GetVdm(NG, NT_GL, NR, NTS, false);
+  std::vector<double> V_Ref_N = GetVdm(NR, NTS, N, NTS, true);
   std::vector<double> V_GLg_GLN = GetVdm(NG, NT_GL, N, NT_GL, false);
-  const std::vector<double>& DGLN = C.D;  // GetDerivativeMatrix(PP_N, GL)
+  // GetDerivativeMatrix(PP_N, GL): the solution's D for LGL nodes; Gauss nodes keep the metric terms
+  // on the LGL points of degree N and interpolate them with Vdm_GLN_N (metrics.f90:325-330)
+  std::vector<double> DGLNg, V_GLN_N;
+  if (C.gauss) {
+    std::vector<double> xGLN(n);
+    Nodes(N, NT_GL, xGLN.data());
+    DGLNg.resize(n * n);
+    DerivMatrix(N, xGLN.data(), DGLNg.data());
+    V_GLN_N = GetVdm(N, NT_GL, N, NT_GAUSS, false);
+  }
+  const std::vector<double>& DGLN = C.gauss ? DGLNg : C.D;
+  if (C.gauss) C.SurfMetrics.assign((size_t)3 * n * n * 6 * C.nElems, 0.);
   std::vector<double> XGLg(3 * ng * ng * ng), XGLN(3 * nv), dXg(9 * ng * ng * ng), tmpd(3 * ng * ng * ng),
       tmpo(3 * nr * nr * nr), dXR(9 * nr * nr * nr), detR(nr * nr * nr), detN(nv), dXN(9 * nv), tmpN(3 * nv),
       Rm(9 * nv), Ja(9 * nv);
   for (int e = 0; e < C.nElems; ++e) {
     ChangeBasis3D(3, NG, NG, V_EQ_GL.data(), &C.NodeCoords[3 * (size_t)ng * ng * ng * e], XGLg.data());
     ChangeBasis3D(3, NG, N, V_GLg_GLN.data(), XGLg.data(), XGLN.data());
-    for (size_t z = 0; z < 3 * nv; ++z) C.Elem_xGP[3 * nv * e + z] = XGLN[z];
+    if (C.gauss) ChangeBasis3D(3, N, N, V_GLN_N.data(), XGLN.data(), &C.Elem_xGP[3 * nv * e]);
+    else
+      for (size_t z = 0; z < 3 * nv; ++z) C.Elem_xGP[3 * nv * e + z] = XGLN[z];
     // dXGL_Ngeo(dd,nn,i,j,k): index dd + 3*nn + 9*node
     std::fill(dXg.begin(), dXg.end(), 0.);
     for (int k = 0; k < ng; ++k)
@@ -1602,19 +1640,67 @@ void CalcMetrics(Case& C) {
               J[2 + 3 * nn] = J[2 + 3 * nn] + DGLN[j + n * q] * RR(0, nn, i, q, k);
             }
         }
-    for (size_t z = 0; z < nv; ++z)
-      for (int nn = 0; nn < 3; ++nn) {
-        C.Mf[3 * (nv * e + z) + nn] = Ja[0 + 3 * nn + 9 * z];
-        C.Mg[3 * (nv * e + z) + nn] = Ja[1 + 3 * nn + 9 * z];
-        C.Mh[3 * (nv * e + z) + nn] = Ja[2 + 3 * nn + 9 * z];
+    if (C.gauss) {  // ChangeBasis3D(Vdm_GLN_N) of each metric vector, metrics.f90:325-327
+      std::vector<double> tin(3 * nv), tout(3 * nv);
+      double* M[3] = {&C.Mf[3 * nv * e], &C.Mg[3 * nv * e], &C.Mh[3 * nv * e]};
+      for (int dd = 0; dd < 3; ++dd) {
+        for (size_t z = 0; z < nv; ++z)
+          for (int nn = 0; nn < 3; ++nn) tin[nn + 3 * z] = Ja[dd + 3 * nn + 9 * z];
+        ChangeBasis3D(3, N, N, V_GLN_N.data(), tin.data(), M[dd]);
       }
-    // CalcSurfMetrics: master sides only (LGL)
+    } else {
+      for (size_t z = 0; z < nv; ++z)
+        for (int nn = 0; nn < 3; ++nn) {
+          C.Mf[3 * (nv * e + z) + nn] = Ja[0 + 3 * nn + 9 * z];
+          C.Mg[3 * (nv * e + z) + nn] = Ja[1 + 3 * nn + 9 * z];
+          C.Mh[3 * (nv * e + z) + nn] = Ja[2 + 3 * nn + 9 * z];
+        }
+    }
+    // CalcSurfMetrics (metrics.f90:334-440): Ja of the LGL points on the side, interpolated to the side's
+    // solution points (ChangeBasis2D with Vdm_GLN_N; identity for LGL).  LGL: master sides only; Gauss:
+    // SurfMetrics of every side in the master's point order (FS2M), face vectors of the master sides.
+    std::vector<double> JaF(9 * n * n);  // JaF[dd + 3*nn + 9*(a + n*b)]: face slice in volume index order
     for (int s = 1; s <= 6; ++s) {
       int SideID = C.ElemToSide[0 + 2 * ((s - 1) + 6 * (size_t)e)];
       int flip = C.ElemToSide[1 + 2 * ((s - 1) + 6 * (size_t)e)];
-      if (flip != 0) continue;
+      if (flip != 0 && !C.gauss) continue;
       int nd = NormalDirs[s] - 1, td = TangDirs[s] - 1;
       double sign = NormalSigns[s];
+      if (C.gauss) {
+        std::vector<double> sl(9 * n * n, 0.), b1(9 * n * n, 0.);
+        for (int b = 0; b < n; ++b)
+          for (int a = 0; a < n; ++a) {
+            int i, j, k;
+            switch (s) {
+              case XI_MINUS: i = 0; j = a; k = b; break;
+              case XI_PLUS: i = N; j = a; k = b; break;
+              case ETA_MINUS: i = a; j = 0; k = b; break;
+              case ETA_PLUS: i = a; j = N; k = b; break;
+              case ZETA_MINUS: i = a; j = b; k = 0; break;
+              default: i = a; j = b; k = N; break;
+            }
+            for (int c = 0; c < 9; ++c) sl[c + 9 * (a + n * b)] = Ja[c + 9 * (i + n * (j + n * k))];
+          }
+        for (int b = 0; b < n; ++b)  // ChangeBasis2D: first index, then second
+          for (int ao = 0; ao < n; ++ao)
+            for (int a = 0; a < n; ++a)
+              for (int c = 0; c < 9; ++c) b1[c + 9 * (ao + n * b)] += V_GLN_N[ao + n * a] * sl[c + 9 * (a + n * b)];
+        std::fill(JaF.begin(), JaF.end(), 0.);
+        for (int bo = 0; bo < n; ++bo)
+          for (int b = 0; b < n; ++b)
+            for (int a = 0; a < n; ++a)
+              for (int c = 0; c < 9; ++c) JaF[c + 9 * (a + n * bo)] += V_GLN_N[bo + n * b] * b1[c + 9 * (a + n * b)];
+        for (int q = 0; q < n; ++q)
+          for (int p = 0; p < n; ++p) {
+            int a, b, pm, qm;
+            CGNS_SideToVol2(N, p, q, s, a, b);
+            Flip_S2M(N, p, q, flip, pm, qm);
+            const double* J = &JaF[9 * (a + n * b)];
+            double* SM = &C.SurfMetrics[3 * ((size_t)pm + n * ((size_t)qm + n * ((size_t)(s - 1) + 6 * (size_t)e)))];
+            for (int c = 0; c < 3; ++c) SM[c] = J[nd + 3 * c];
+          }
+        if (flip != 0) continue;
+      }
       for (int q = 0; q < n; ++q)
         for (int p = 0; p < n; ++p) {
           int a, b;
@@ -1628,7 +1714,7 @@ void CalcMetrics(Case& C) {
             case ZETA_MINUS: i = a; j = b; k = 0; break;
             default: i = a; j = b; k = N; break;
           }
-          const double* J = &Ja[9 * (i + n * (j + n * k))];
+          const double* J = C.gauss ? &JaF[9 * (a + n * b)] : &Ja[9 * (i + n * (j + n * k))];
           double jn[3] = {J[nd + 0], J[nd + 3], J[nd + 6]};
           double jt[3] = {J[td + 0], J[td + 3], J[td + 6]};
           size_t fi = (size_t)p + n * ((size_t)q + (size_t)n * (SideID - 1));
@@ -1683,7 +1769,8 @@ void InitEquationAndTime(Case& C) {
   if (P.time_disc < 0 || P.time_disc > 9) throw std::runtime_error("time disc not implemented in oracle");
   C.rk = &kOrcRKTables[P.time_disc];  // SetTimeDiscCoefs, timedisc_vars.f90:94-726
   C.nRKStages = C.rk->nStages;
-  std::copy(C.rk->cflAlpha, C.rk->cflAlpha + 15, cflAlpha);
+  if (C.gauss) std::copy(kOrcGaussCflAlpha[P.time_disc], kOrcGaussCflAlpha[P.time_disc] + 15, cflAlpha);
+  else std::copy(C.rk->cflAlpha, C.rk->cflAlpha + 15, cflAlpha);
   relDFL = C.rk->relativeDFL;
   C.RKA.assign(C.rk->A, C.rk->A + C.nRKStages + 1);
   C.RKb.assign(C.rk->b, C.rk->b + C.nRKStages + 1);
@@ -1693,6 +1780,7 @@ void InitEquationAndTime(Case& C) {
   double alpha = cflAlpha[std::min(15, N) - 1];
   C.CFLScale = P.cfl_scale * alpha / (2. * N + 1.);
   double dflAlpha[10] = {4.50, 1.95, 1.18, 0.79, 0.56, 0.42, 0.32, 0.25, 0.20, 0.17};
+  if (C.gauss) std::copy(kOrcGaussDflAlpha, kOrcGaussDflAlpha + 10, dflAlpha);
   double alphaD = dflAlpha[std::min(10, N) - 1] * relDFL;
   C.DFLScale = P.dfl_scale * alphaD / ((2. * N + 1.) * (2. * N + 1.));
 }
@@ -1700,9 +1788,31 @@ void InitEquationAndTime(Case& C) {
 // ----------------------------------------------------------------------------------------------
 // DG operator, dg/dg.f90:282-452
 // ----------------------------------------------------------------------------------------------
-// ProlongToFace (LGL), interpolation/prolongtoface.f90:43-132
+// ProlongToFace, interpolation/prolongtoface.f90:43-132: LGL copies the side's node, Gauss interpolates
+// along the line with L_Minus (Uface = U(l=0) L_Minus(0) + sum_{l>=1} U(l) L_Minus(l), l counted from the side)
 void ProlongToFace(Case& C, const std::vector<real>& Uvol, std::vector<real>& Um, std::vector<real>& Us) {
   int n = C.np;
+  if (C.gauss) {
+    const int NV = C.nVar;
+    for (int sid = 0; sid < C.nSides; ++sid)
+      for (int side = 0; side < 2; ++side) {
+        const int e = C.SideToElem[side + 5 * sid];
+        if (e == -1) continue;
+        const int ls = C.SideToElem[2 + side + 5 * sid], fl = side ? C.SideToElem[4 + 5 * sid] : 0;
+        std::vector<real>& F = side ? Us : Um;
+        for (int q = 0; q < n; ++q)
+          for (int p = 0; p < n; ++p)
+            for (int v = 0; v < NV; ++v) {
+              auto at = [&](int l) {
+                return Uvol[C.vol(v, C.s2v(l, p, q, fl, ls, 0), C.s2v(l, p, q, fl, ls, 1), C.s2v(l, p, q, fl, ls, 2), e - 1)];
+              };
+              real acc = at(0) * C.Lminus[0];
+              for (int l = 1; l < n; ++l) acc = acc + at(l) * C.Lminus[l];
+              F[C.fac(v, p, q, sid)] = acc;
+            }
+      }
+    return;
+  }
   for (int sid = 0; sid < C.nSides; ++sid) {
     int e = C.SideToElem[0 + 5 * sid];
     if (e != -1) {
@@ -1912,33 +2022,47 @@ void Lifting(Case& C) {
     for (int d = 0; d < 3; ++d) {
       std::vector<real>& g = *G[d];
       std::vector<real>& F = *FF[d];
+      // LGL: the side's node with L_HatMinus0; Gauss: every node of the line with L_HatMinus(l)
+      const int nl = C.gauss ? n : 1;
       for (int sid = 0; sid < C.nSides; ++sid) {
         int e = C.SideToElem[0 + 5 * sid];
         if (e != -1) {
           int ls = C.SideToElem[2 + 5 * sid];
           for (int q = 0; q < n; ++q)
             for (int p = 0; p < n; ++p)
-              for (int v = 0; v < NV; ++v) {
-                size_t idx = C.vol(v, C.s2v(0, p, q, 0, ls, 0), C.s2v(0, p, q, 0, ls, 1), C.s2v(0, p, q, 0, ls, 2), e - 1);
-                g[idx] = g[idx] + F[C.fac(v, p, q, sid)] * C.L_HatMinus0;
-              }
+              for (int l = 0; l < nl; ++l)
+                for (int v = 0; v < NV; ++v) {
+                  size_t idx = C.vol(v, C.s2v(l, p, q, 0, ls, 0), C.s2v(l, p, q, 0, ls, 1), C.s2v(l, p, q, 0, ls, 2), e - 1);
+                  g[idx] = g[idx] + F[C.fac(v, p, q, sid)] * (C.gauss ? C.LhatMinus[l] : C.L_HatMinus0);
+                }
         }
         int nb = C.SideToElem[1 + 5 * sid];
         if (nb != -1) {
           int nls = C.SideToElem[3 + 5 * sid], fl = C.SideToElem[4 + 5 * sid];
           for (int q = 0; q < n; ++q)
             for (int p = 0; p < n; ++p)
-              for (int v = 0; v < NV; ++v) {
-                size_t idx = C.vol(v, C.s2v(0, p, q, fl, nls, 0), C.s2v(0, p, q, fl, nls, 1),
-                                   C.s2v(0, p, q, fl, nls, 2), nb - 1);
-                g[idx] = g[idx] + F[C.fac(v, p, q, sid)] * C.L_HatMinus0;
-              }
+              for (int l = 0; l < nl; ++l)
+                for (int v = 0; v < NV; ++v) {
+                  size_t idx = C.vol(v, C.s2v(l, p, q, fl, nls, 0), C.s2v(l, p, q, fl, nls, 1),
+                                     C.s2v(l, p, q, fl, nls, 2), nb - 1);
+                  g[idx] = g[idx] + F[C.fac(v, p, q, sid)] * (C.gauss ? C.LhatMinus[l] : C.L_HatMinus0);
+                }
         }
       }
       for (size_t z = 0; z < nt / NV; ++z)
         for (int v = 0; v < NV; ++v) g[NV * z + v] = g[NV * z + v] * C.sJ[z];
-      for (size_t z = 0; z < nt / NV; ++z) GradPrim(C, &C.U[NV * z], &g[NV * z]);
-      ProlongToFace(C, g, *GM[d], *GS[d]);
+      if (C.gauss) {  // br1.f90:318-350: prolong the lifting-variable gradient, then convert with U and the face U
+        ProlongToFace(C, g, *GM[d], *GS[d]);
+        for (size_t z = 0; z < nt / NV; ++z) GradPrim(C, &C.U[NV * z], &g[NV * z]);
+        size_t nf = (size_t)n * n * C.nSides;
+        for (size_t z = 0; z < nf; ++z) {
+          GradPrim(C, &C.Umaster[NV * z], &(*GM[d])[NV * z]);
+          GradPrim(C, &C.Uslave[NV * z], &(*GS[d])[NV * z]);
+        }
+      } else {
+        for (size_t z = 0; z < nt / NV; ++z) GradPrim(C, &C.U[NV * z], &g[NV * z]);
+        ProlongToFace(C, g, *GM[d], *GS[d]);
+      }
     }
   } else {
     // BR2: prolong the volume gradient, then BR2_SurfInt (br2_surfint.f90:53-148) adds the
@@ -1953,32 +2077,39 @@ void Lifting(Case& C) {
       std::vector<real>& F = *FF[d];
       std::vector<real>& gm = *GM[d];
       std::vector<real>& gs = *GS[d];
+      // LGL: the side's node; Gauss: every node of the line (br2_surfint.f90:109-115, 131-137), the face
+      // gradient taking etaBR2 L_Minus(l) F_loc
+      const int nl = C.gauss ? n : 1;
       for (int sid = 0; sid < C.nSides; ++sid) {
         int e = C.SideToElem[0 + 5 * sid];
         if (e != -1) {
           int ls = C.SideToElem[2 + 5 * sid];
           for (int q = 0; q < n; ++q)
-            for (int p = 0; p < n; ++p) {
-              size_t o = C.nod(C.s2v(0, p, q, 0, ls, 0), C.s2v(0, p, q, 0, ls, 1), C.s2v(0, p, q, 0, ls, 2), e - 1);
-              for (int v = 0; v < NV; ++v) {
-                real Floc = C.sJ[o] * C.L_HatMinus0 * F[C.fac(v, p, q, sid)];
-                g[NV * o + v] = g[NV * o + v] + Floc;
-                gm[C.fac(v, p, q, sid)] = gm[C.fac(v, p, q, sid)] + C.etaBR2 * Floc;
+            for (int p = 0; p < n; ++p)
+              for (int l = 0; l < nl; ++l) {
+                size_t o = C.nod(C.s2v(l, p, q, 0, ls, 0), C.s2v(l, p, q, 0, ls, 1), C.s2v(l, p, q, 0, ls, 2), e - 1);
+                for (int v = 0; v < NV; ++v) {
+                  real Floc = C.sJ[o] * (C.gauss ? C.LhatMinus[l] : C.L_HatMinus0) * F[C.fac(v, p, q, sid)];
+                  g[NV * o + v] = g[NV * o + v] + Floc;
+                  if (C.gauss) gm[C.fac(v, p, q, sid)] = gm[C.fac(v, p, q, sid)] + C.etaBR2 * C.Lminus[l] * Floc;
+                  else gm[C.fac(v, p, q, sid)] = gm[C.fac(v, p, q, sid)] + C.etaBR2 * Floc;
+                }
               }
-            }
         }
         int nb = C.SideToElem[1 + 5 * sid];
         if (nb != -1) {
           int nls = C.SideToElem[3 + 5 * sid], fl = C.SideToElem[4 + 5 * sid];
           for (int q = 0; q < n; ++q)
-            for (int p = 0; p < n; ++p) {
-              size_t o = C.nod(C.s2v(0, p, q, fl, nls, 0), C.s2v(0, p, q, fl, nls, 1), C.s2v(0, p, q, fl, nls, 2), nb - 1);
-              for (int v = 0; v < NV; ++v) {
-                real Floc = C.sJ[o] * C.L_HatMinus0 * F[C.fac(v, p, q, sid)];
-                g[NV * o + v] = g[NV * o + v] + Floc;
-                gs[C.fac(v, p, q, sid)] = gs[C.fac(v, p, q, sid)] + C.etaBR2 * Floc;
+            for (int p = 0; p < n; ++p)
+              for (int l = 0; l < nl; ++l) {
+                size_t o = C.nod(C.s2v(l, p, q, fl, nls, 0), C.s2v(l, p, q, fl, nls, 1), C.s2v(l, p, q, fl, nls, 2), nb - 1);
+                for (int v = 0; v < NV; ++v) {
+                  real Floc = C.sJ[o] * (C.gauss ? C.LhatMinus[l] : C.L_HatMinus0) * F[C.fac(v, p, q, sid)];
+                  g[NV * o + v] = g[NV * o + v] + Floc;
+                  if (C.gauss) gs[C.fac(v, p, q, sid)] = gs[C.fac(v, p, q, sid)] + C.etaBR2 * C.Lminus[l] * Floc;
+                  else gs[C.fac(v, p, q, sid)] = gs[C.fac(v, p, q, sid)] + C.etaBR2 * Floc;
+                }
               }
-            }
         }
       }
       for (size_t z = 0; z < nt / NV; ++z) GradPrim(C, &C.U[NV * z], &g[NV * z]);
@@ -2075,6 +2206,53 @@ void FillFlux(Case& C) {
 // SurfInt (LGL), dg/surfint.f90:48-264
 void SurfInt(Case& C) {
   int n = C.np;
+  if (C.gauss) {
+    // Gauss nodes (surfint.f90:118-175, 196-253): every node of the line takes the surface flux times
+    // L_HatMinus(l); the split form adds the correction -(FluxB_sum - FluxB(l)) NormalSign with
+    // FluxB(l) = the two-point volume flux between node l and the side's state (metric average of the
+    // node's metric and SurfMetrics) and FluxB_sum = sum_l FluxB(l) L_Minus(l)
+    const int NV = C.nVar;
+    const size_t nv = (size_t)n * n * n;
+    std::vector<real> FB((size_t)NV * n);
+    for (int sid = 0; sid < C.nSides; ++sid)
+      for (int side = 0; side < 2; ++side) {
+        const int e1 = C.SideToElem[side + 5 * sid];
+        if (e1 == -1) continue;
+        const int e = e1 - 1;
+        const int ls = C.SideToElem[2 + side + 5 * sid], fl = side ? C.SideToElem[4 + 5 * sid] : 0;
+        const std::vector<double>& Mx = (ls == 3 || ls == 5) ? C.Mf : ((ls == 2 || ls == 4) ? C.Mg : C.Mh);
+        const std::vector<real>& Uf = side ? C.Uslave : C.Umaster;
+        const std::vector<real>& Ff = side ? C.Fslave : C.Fmaster;
+        const double sg = NormalSigns[ls];
+        for (int q = 0; q < n; ++q)
+          for (int p = 0; p < n; ++p) {
+            const real* UB = &Uf[C.fac(0, p, q, sid)];
+            real aB[NVMAX + 4], aN[NVMAX + 4], sum[NVMAX];
+            Uaux(C, UB, aB);
+            const double* SM = &C.SurfMetrics[3 * ((size_t)p + n * ((size_t)q + n * ((size_t)(ls - 1) + 6 * (size_t)e)))];
+            for (int l = 0; l < n; ++l) {
+              const size_t o = C.nod(C.s2v(l, p, q, fl, ls, 0), C.s2v(l, p, q, fl, ls, 1), C.s2v(l, p, q, fl, ls, 2), e);
+              Uaux(C, &C.U[NV * o], aN);
+              const real mL[3] = {Mx[3 * o], Mx[3 * o + 1], Mx[3 * o + 2]}, mR[3] = {SM[0], SM[1], SM[2]};
+              VolumeFluxVec(C, &C.U[NV * o], UB, aN, aB, mL, mR, &FB[(size_t)NV * l]);
+            }
+            for (int v = 0; v < NV; ++v) sum[v] = 0.;
+            for (int l = 0; l < n; ++l)
+              for (int v = 0; v < NV; ++v) sum[v] = sum[v] + FB[(size_t)NV * l + v] * C.Lminus[l];
+            for (int l = 0; l < n; ++l) {
+              const size_t o = C.nod(C.s2v(l, p, q, fl, ls, 0), C.s2v(l, p, q, fl, ls, 1), C.s2v(l, p, q, fl, ls, 2), e);
+              for (int v = 0; v < NV; ++v) {
+                const real fv = Ff[C.fac(v, p, q, sid)];
+                const real corr = (sum[v] - FB[(size_t)NV * l + v]) * sg;
+                if (side == 0) C.Ut[NV * o + v] = C.Ut[NV * o + v] + (fv - corr) * C.LhatMinus[l];
+                else C.Ut[NV * o + v] = C.Ut[NV * o + v] - (fv + corr) * C.LhatMinus[l];
+              }
+            }
+          }
+      }
+    (void)nv;
+    return;
+  }
   for (int sid = 0; sid < C.nSides; ++sid) {
     int e = C.SideToElem[0 + 5 * sid];
     if (e != -1) {
@@ -2109,11 +2287,35 @@ struct PhaseCount {  // operation count of one phase of the RHS (counting build)
   ~PhaseCount() { g_phase[k] += g_oracle_flops - start; }
 };
 
+// useEntropyProlongToFace (navierstokes/equation.f90:413-455): the EC / EC-KEP volume fluxes
+inline bool UseEntropyProlong(const Case& C) {
+  const int vf = C.P.volume_flux;
+  return !C.mhd && (vf == 5 || vf == 6 || vf == 7 || vf == 10 || vf == 32);
+}
+
+// ProlongToFace_U, dg.f90:458-511: Gauss nodes with an entropy-conservative volume flux prolong the
+// entropy variables V = ConsToEntropyVec(U) (dg.f90:338-340) and convert the face values back
+void ProlongToFaceU(Case& C) {
+  if (!(C.gauss && UseEntropyProlong(C))) {
+    ProlongToFace(C, C.U, C.Umaster, C.Uslave);
+    return;
+  }
+  const int NV = C.nVar;
+  C.Vent.resize(C.U.size());
+  for (size_t z = 0; z < C.U.size() / NV; ++z) ConsToEntropy(C, &C.U[NV * z], &C.Vent[NV * z]);
+  std::vector<real> Vm(C.Umaster.size()), Vs(C.Uslave.size());
+  ProlongToFace(C, C.Vent, Vm, Vs);
+  for (size_t z = 0; z < Vm.size() / NV; ++z) {
+    EntropyToCons(C, &Vm[NV * z], &C.Umaster[NV * z]);
+    EntropyToCons(C, &Vs[NV * z], &C.Uslave[NV * z]);
+  }
+}
+
 // Phases: 0 volume split form, 1 lifting, 2 viscous volume integral, 3 face fluxes,
 //         4 surface integral, 5 Jacobian + source
 void DGTimeDerivative(Case& C, double t) {
   std::fill(C.Ut.begin(), C.Ut.end(), real(0.));  // VNullify
-  ProlongToFace(C, C.U, C.Umaster, C.Uslave);
+  ProlongToFaceU(C);
   if (C.P.nfvse) CalcBlendingCoefficient(C);  // dg.f90:358-361
   { PhaseCount pc(0); VolIntSplitForm(C); }
   if (C.P.nfvse) { PhaseCount pc(6); VolIntNFVSE(C); }  // dg.f90:380-383
@@ -2373,6 +2575,9 @@ void* orc_create(const orc_params* p) {
     C->nAux = C->mhd ? 8 : 6;
     C->nDOFElem = C->np * C->np * C->np;
     C->parabolic = (p->eqn == 1 || p->eqn == 3);
+    C->gauss = (p->node_type == 1);
+    if (C->gauss && C->mhd) throw std::runtime_error("Gauss nodes: only the Euler / Navier-Stokes system");
+    if (C->gauss && p->nfvse) throw std::runtime_error("Gauss nodes: NFVSE needs the LGL subcells");
     InitEquationAndTime(*C);
     InitBasis(*C);
     BuildMesh(*C);
@@ -2678,6 +2883,12 @@ void orc_riemann_point(void* h, const double* UL, const double* UR, const double
 }
 
 int orc_corr_error(void* h) { return ((Case*)h)->corrErr; }
+
+void orc_get_surf_metrics(void* h, double* SM) {
+  Case* C = (Case*)h;
+  const size_t n = (size_t)3 * C->np * C->np * 6 * C->nElems;
+  for (size_t z = 0; z < n; ++z) SM[z] = C->gauss ? C->SurfMetrics[z] : 0.;
+}
 
 void orc_get_alpha(void* h, double* alpha) {
   Case* C = (Case*)h;

@@ -66,6 +66,7 @@ typedef struct orc_params {
   int nfvse_corr;         /* NFVSE_CORR (CMake FLUXO_SHOCK_NFVSE_CORR): positivity correction after each stage */
   double posit_corr_factor;  /* PositCorrFactor */
   int posit_max_iter;     /* PositMaxIter */
+  int node_type;          /* PP_NodeType (CMake FLUXO_DISC_NODETYPE): 1 Gauss, 2 (or 0) Gauss-Lobatto */
 } orc_params;
 
 void* orc_create(const orc_params* p);
@@ -113,6 +114,8 @@ void orc_riemann_point(void* h, const double* UL, const double* UR, const double
 double orc_ln_mean(double aL, double aR);
 /* NFVSE: blending coefficient alpha(nElems) of the last right-hand side. */
 void orc_get_alpha(void* h, double* alpha);
+/* Gauss nodes: SurfMetrics(3,0:N,0:N,6,nElems) of mesh/metrics.f90:420-427 (NULL-safe; LGL: zeros). */
+void orc_get_surf_metrics(void* h, double* SurfMetrics);
 /* NFVSE_CORR: element + 1 whose safe state had negative density or pressure (0: none). */
 int orc_corr_error(void* h);
 /* MHD: the GLM cleaning speed GLM_ch (set by CALCTIMESTEP, or explicitly). */

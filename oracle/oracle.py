@@ -73,6 +73,7 @@ class OrcParams(ctypes.Structure):
         ("nfvse_corr", ctypes.c_int),
         ("posit_corr_factor", ctypes.c_double),
         ("posit_max_iter", ctypes.c_int),
+        ("node_type", ctypes.c_int),
     ]
 
 
@@ -89,6 +90,7 @@ DEFAULTS = dict(
     nfvse=0, compute_alpha=1, shock_blend_coef=0.0, modal_threshold=1, alpha_max=0.5, alpha_min=0.01,
     space_prop_factor=0.5, space_prop_sweeps=1, time_rel_factor=0.0, indicator_quantity=3,
     sub_fv_method=1, recons_boundaries=1, nfvse_corr=0, posit_corr_factor=0.1, posit_max_iter=10,
+    node_type=2,
 )
 
 
@@ -138,6 +140,7 @@ def _lib(counting=False):
     lib.orc_ln_mean.argtypes = [d, d]
     lib.orc_get_alpha.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     lib.orc_corr_error.restype = ctypes.c_int
+    lib.orc_get_surf_metrics.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     lib.orc_corr_error.argtypes = [ctypes.c_void_p]
     lib.orc_set_glm_ch.argtypes = [ctypes.c_void_p, d]
     lib.orc_get_glm_ch.restype = d
@@ -275,6 +278,13 @@ class OracleCase:
         """NFVSE blending coefficient per element after the last right-hand side."""
         a = np.zeros(self.nElems)
         self.lib.orc_get_alpha(self.h, _ptr(a))
+        return a
+
+    def surf_metrics(self):
+        """Gauss nodes: SurfMetrics(3,0:N,0:N,6,nElems) as a C-order array [e, side, q, p, 3]."""
+        n = self.N + 1
+        a = np.zeros((self.nElems, 6, n, n, 3))
+        self.lib.orc_get_surf_metrics(self.h, _ptr(a))
         return a
 
     @property
