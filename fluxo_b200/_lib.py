@@ -85,6 +85,7 @@ class FluxoCfg(ctypes.Structure):
         ("nfvse_corr", ctypes.c_int),
         ("posit_corr_factor", ctypes.c_double),
         ("posit_max_iter", ctypes.c_int),
+        ("node_type", ctypes.c_int),
     ]
 
 
@@ -95,7 +96,7 @@ EXPORTS = [
     "fluxo_gpu_last_error", "fluxo_gpu_set_profiling", "fluxo_gpu_get_profile", "fluxo_gpu_fp64_peak",
     "fluxo_host_box_sizes", "fluxo_host_box_mesh", "fluxo_host_exact_func", "fluxo_gpu_dg_time_derivative_noalloc",
     "fluxo_gpu_set_glm_ch", "fluxo_gpu_get_glm_ch", "fluxo_gpu_get_alpha", "fluxo_gpu_volume_shape",
-    "fluxo_gpu_set_volume_shape", "fluxo_gpu_analyze",
+    "fluxo_gpu_set_volume_shape", "fluxo_gpu_analyze", "fluxo_gpu_set_surf_metrics",
     "fluxo_batch_create", "fluxo_batch_add", "fluxo_batch_run", "fluxo_batch_status", "fluxo_batch_get_state",
     "fluxo_batch_set_state",
     "fluxo_batch_remove", "fluxo_batch_info", "fluxo_batch_stream", "fluxo_batch_instance_bytes",
@@ -120,6 +121,7 @@ def load():
     vp, i, d, P = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.POINTER
     lib.fluxo_gpu_create.argtypes = [P(FluxoCfg), P(vp)]
     lib.fluxo_gpu_set_mesh.argtypes = [vp, i, i] + [vp] * 11
+    lib.fluxo_gpu_set_surf_metrics.argtypes = [vp, vp]
     lib.fluxo_gpu_set_state.argtypes = [vp, vp]
     lib.fluxo_gpu_get_state.argtypes = [vp, vp]
     lib.fluxo_gpu_get_ut.argtypes = [vp, vp]

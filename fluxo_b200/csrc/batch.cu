@@ -434,6 +434,10 @@ int check_cfg(const fluxo_cfg* c, std::string& msg) {
     msg = "batched solves run without shock capturing";
     return FLUXO_EINVAL_CFG;
   }
+  if (c->node_type == 1) {
+    msg = "batched solves run on Gauss-Lobatto nodes";
+    return FLUXO_EINVAL_CFG;
+  }
   if (c->eqn == FLUXO_EQN_NAVIERSTOKES &&
       (c->lifting < 1 || c->lifting > 2 || c->lifting_var < 1 || c->lifting_var > 3 || c->visc < 0 || c->visc > 2)) {
     msg = "lifting / lifting_var / visc out of range";

@@ -32,7 +32,12 @@ struct BasisTables {
   double D[FLUXO_NPMAX * FLUXO_NPMAX];     // D(i,l) at [i*NP+l]
   double LhatM0;                           // L_HatMinus(0)
   double wGP[FLUXO_NPMAX];
-  double xGP[FLUXO_NPMAX];                 // LGL nodes
+  double xGP[FLUXO_NPMAX];                 // LGL (or Gauss) nodes
+  // Gauss nodes (PP_NodeType = 1): the face interpolation L_Minus(l) and L_HatMinus(l) = L_Minus(l)/w(l),
+  // l counted from the side (prolongtoface.f90:103-132, surfint.f90:118-175); zero for LGL
+  double Lminus[FLUXO_NPMAX];
+  double LhatMinus[FLUXO_NPMAX];
+  int gauss;
 };
 
 // Everything a kernel needs, passed by value.
@@ -102,6 +107,12 @@ struct KParams {
   // element kernels: blocks resident at once on the device (0: no prefetch); block b prefetches the
   // tile of block b + pfTiles into L2
   int pfTiles;
+  // Gauss nodes: face states of ProlongToFace_U [side][master|slave][pt][5], the surface integral with
+  // the split-form correction [elem][5][node] (added by the volume kernel instead of the LGL surface
+  // terms), SurfMetrics [elem][6][3][pt] (mesh_vars.f90:67-70); all null for LGL
+  double* uface;
+  double* utsurf;
+  const double* surfMet;
   // batched solves: the elements of many independent instances in one launch; each instance has
   // its own time step (null for a single solve)
   const int* elemInst;               // [elem] index of the element's instance in the arrays below

@@ -169,6 +169,9 @@ struct fluxo_handle {
   // NFVSE: blending coefficients, list of blended elements, alpha * F_FV, modal transform
   double *dAlpha = nullptr, *dAlphaRaw = nullptr, *dAlphaTmp = nullptr, *dFV = nullptr, *dSVdm = nullptr;
   double* dFFV = nullptr;  // NFVSE_CORR: FFV_m_FDG [elem][node][var]
+  // Gauss nodes: face states, surface integral, SurfMetrics (set by fluxo_gpu_set_surf_metrics)
+  bool gauss = false, surfMetSet = false;
+  double *dUface = nullptr, *dUtSurf = nullptr, *dSurfMet = nullptr;
   int *dBlendList = nullptr, *dBlendCount = nullptr;
   int nSMs = 148;
   bool visc = false, meshSet = false, stateSet = false, haveXGP = false;
@@ -232,6 +235,25 @@ int dalloc(fluxo_handle* h, T** p, size_t n) {
   return FLUXO_OK;
 }
 
+// Gauss nodes (InitDGbasis with NodeType 'GAUSS', dg.f90:181-252)
+void build_gauss_basis_tables(int N, BasisTables& B) {
+  host::GaussBasis b(N);
+  const int NP = N + 1;
+  std::memset(&B, 0, sizeof(B));
+  for (int i = 0; i < NP; ++i)
+    for (int l = 0; l < NP; ++l) {
+      B.Dvs[i * NP + l] = (i == l) ? 0. : b.Dvs[(size_t)i * NP + l];  // skew-symmetric: zero diagonal
+      B.Dhat[i * NP + l] = b.Dhat[(size_t)i * NP + l];
+      B.D[i * NP + l] = b.D[(size_t)i * NP + l];
+    }
+  B.LhatM0 = b.LhatMinus[0];
+  for (int i = 0; i < NP; ++i) {
+    B.wGP[i] = b.w[i]; B.xGP[i] = b.x[i];
+    B.Lminus[i] = b.Lminus[i]; B.LhatMinus[i] = b.LhatMinus[i];
+  }
+  B.gauss = 1;
+}
+
 void build_basis_tables(int N, BasisTables& B) {
   host::LGLBasis b(N);
   const int NP = N + 1;
@@ -255,6 +277,7 @@ KParams base_params(fluxo_handle* h) {
   P.s2e = h->dS2E; P.e2s = h->dE2S;
   P.flux = h->dFlux; P.lflux = h->dLFlux; P.gtrace = h->dGTrace;
   P.basis = h->dBasis;
+  if (h->gauss) { P.uface = h->dUface; P.utsurf = h->dUtSurf; P.surfMet = h->dSurfMet; }
   fill_ns_physics(P, c);
   P.source = (c.ini_exact_func == 4 && h->haveXGP) ? 1 : 0;
   if (P.source) {  // CalcSource CASE(4) constants, equation.f90:1000-1012
@@ -354,6 +377,14 @@ int rhs(fluxo_handle* h, KParams P) {
     FLUXO_CUDA(h, launch_nfvse_fv_ns(h->cfg.riemann, h->NP, h->nElems, h->nSMs, s, P));
     h->launches += 3 + (h->cfg.space_prop_sweeps > 1 ? 2 * (h->cfg.space_prop_sweeps - 1) : 0);
   }
+  if (h->gauss) {  // ProlongToFace_U (dg.f90:458-511): interpolated (entropy-projected) face states
+    if (!h->surfMetSet) return fail(h, FLUXO_ENOTREADY, "Gauss nodes: SurfMetrics not set");
+    const int vf = h->cfg.volume_flux;
+    const bool ent = vf == 5 || vf == 6 || vf == 7 || vf == 10 || vf == 32;  // equation.f90:413-455
+    ProfScope ps(h, 2);
+    FLUXO_CUDA(h, launch_gauss_prolong(h->NP, ent, h->nElems, s, P));
+    h->launches += 1;
+  }
   if (h->visc) {
     {
       ProfScope ps(h, 0);
@@ -361,13 +392,19 @@ int rhs(fluxo_handle* h, KParams P) {
     }
     {
       ProfScope ps(h, 1);
-      FLUXO_CUDA(h, launch_gradient(h->NP, h->nElems, s, P));
+      if (h->gauss) FLUXO_CUDA(h, launch_gauss_lift_visc(h->NP, h->cfg.lifting, h->cfg.lifting_var, h->nElems, s, P));
+      else FLUXO_CUDA(h, launch_gradient(h->NP, h->nElems, s, P));
     }
     h->launches += 2;
   }
   {
     ProfScope ps(h, 2);
     FLUXO_CUDA(h, launch_face_flux(h->cfg.riemann, h->visc, h->NP, h->nSides, s, P));
+  }
+  if (h->gauss) {  // SurfInt with the split-form correction (surfint.f90:118-175)
+    ProfScope ps(h, 2);
+    FLUXO_CUDA(h, launch_gauss_surf(h->NP, h->cfg.volume_flux, h->nElems, s, P));
+    h->launches += 1;
   }
   if (volume_shape(h->NP, h->cfg.volume_flux, h->visc) < 0) {  // first RHS of this (N, flux, visc)
     FLUXO_CUDA(h, tune_volume(h->NP, h->cfg.volume_flux, h->visc, h->nElems, s, P));
@@ -497,8 +534,11 @@ bool time_disc_setup(const fluxo_cfg& c, double* RKA, double* RKb, double* RKc, 
   *nStages = T.nStages;
   for (int k = 0; k <= T.nStages; ++k) { RKA[k] = T.A[k]; RKb[k] = T.b[k]; RKc[k] = T.c[k]; }
   const int N = c.N;
-  const double dflAlpha[10] = {4.50, 1.95, 1.18, 0.79, 0.56, 0.42, 0.32, 0.25, 0.20, 0.17};
-  *CFLScale = c.cfl_scale * T.cflAlpha[std::min(15, N) - 1] / (2. * N + 1.);
+  const bool gauss = c.node_type == 1;
+  const double dflLGL[10] = {4.50, 1.95, 1.18, 0.79, 0.56, 0.42, 0.32, 0.25, 0.20, 0.17};
+  const double* dflAlpha = gauss ? kGaussDflAlpha : dflLGL;
+  const double* cflAlpha = gauss ? kGaussCflAlpha[c.time_disc] : T.cflAlpha;
+  *CFLScale = c.cfl_scale * cflAlpha[std::min(15, N) - 1] / (2. * N + 1.);
   *DFLScale = c.dfl_scale * dflAlpha[std::min(10, N) - 1] * T.relativeDFL / ((2. * N + 1.) * (2. * N + 1.));
   return true;
 }
@@ -559,12 +599,19 @@ int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {
     if (cfg->visc < 0 || cfg->visc > 2) return fail(nullptr, FLUXO_EINVAL_CFG, "visc must be 0..2");
   }
   if (!(cfg->kappa > 1.)) return fail(nullptr, FLUXO_EINVAL_CFG, "kappa must be > 1");
+  if (cfg->node_type != 0 && cfg->node_type != 1 && cfg->node_type != 2)
+    return fail(nullptr, FLUXO_EINVAL_CFG, "node_type must be 1 (Gauss) or 2 (Gauss-Lobatto)");
+  if (cfg->node_type == 1) {  // the Gauss path of this library: Euler / Navier-Stokes, no NFVSE subcells
+    if (mhd) return fail(nullptr, FLUXO_EINVAL_CFG, "Gauss nodes: only the Euler / Navier-Stokes system");
+    if (cfg->nfvse) return fail(nullptr, FLUXO_EINVAL_CFG, "Gauss nodes: NFVSE needs the LGL subcells");
+  }
   fluxo_handle* h = new fluxo_handle();
   h->cfg = *cfg;
   h->N = cfg->N; h->NP = cfg->N + 1;
   h->visc = parabolic;
   h->mhd = mhd;
   h->nVar = mhd ? 9 : 5;
+  h->gauss = cfg->node_type == 1;
   if (!time_disc_setup(*cfg, h->RKA, h->RKb, h->RKc, &h->nStages, &h->CFLScale, &h->DFLScale)) {
     delete h;
     return fail(nullptr, FLUXO_EINVAL_CFG, "time_disc must be 0..9 (the TimeDiscMethod list of fluxo_cfg)");
@@ -577,7 +624,8 @@ int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {
     delete h;
     return fail(nullptr, FLUXO_ECUDA, m);
   }
-  build_basis_tables(h->N, h->hb);
+  if (h->gauss) build_gauss_basis_tables(h->N, h->hb);
+  else build_basis_tables(h->N, h->hb);
   cudaDeviceGetAttribute(&h->nSMs, cudaDevAttrMultiProcessorCount, cfg->device);
   if (dalloc(h, &h->dBasis, 1) || dalloc(h, &h->dTD, 1) || dalloc(h, &h->dDtBits, 1) || dalloc(h, &h->dErrKey, 1) ||
       (cfg->nfvse && (dalloc(h, &h->dSVdm, (size_t)h->NP * h->NP) || dalloc(h, &h->dBlendCount, 1)))) {
@@ -642,6 +690,12 @@ int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* S2E, 
         (r = dalloc(h, &h->dGTrace, (size_t)2 * (h->mhd ? 7 : 4) * NPT * nSides)))
       return r;
   }
+  if (h->gauss) {
+    if ((r = dalloc(h, &h->dUface, (size_t)2 * 5 * NPT * nSides)) || (r = dalloc(h, &h->dUtSurf, (size_t)5 * NP3 * nElems)) ||
+        (r = dalloc(h, &h->dSurfMet, (size_t)18 * NPT * nElems)))
+      return r;
+    h->surfMetSet = false;
+  }
   if (h->mhd) {  // InitTimeStep_GLM, mhd/calctimestep.f90:187-223
     double dtch1 = 1.7976931348623157e308;
     for (int e = 0; e < nElems; ++e) {
@@ -680,6 +734,25 @@ int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* S2E, 
   FLUXO_CUDA(h, cudaStreamSynchronize(s));
   h->meshSet = true;
   h->stateSet = false;
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_set_surf_metrics(fluxo_handle* h, const double* SM) {
+  if (!h || !SM) return fail(h, FLUXO_EINVAL_CFG, "set_surf_metrics: null argument");
+  if (!h->gauss) return fail(h, FLUXO_EINVAL_CFG, "set_surf_metrics: only for Gauss nodes (node_type = 1)");
+  if (!h->meshSet) return fail(h, FLUXO_ENOTREADY, "set_surf_metrics: mesh not set");
+  FLUXO_CUDA(h, cudaSetDevice(h->cfg.device));
+  // SurfMetrics(3,0:N,0:N,6,nElems) -> [elem][side][3][pt]
+  const int NP = h->NP, NPT = NP * NP;
+  std::vector<double> d((size_t)18 * NPT * h->nElems);
+  for (int e = 0; e < h->nElems; ++e)
+    for (int s = 0; s < 6; ++s)
+      for (int pt = 0; pt < NPT; ++pt)
+        for (int c = 0; c < 3; ++c)
+          d[(((size_t)e * 6 + s) * 3 + c) * NPT + pt] = SM[c + 3 * (pt + (size_t)NPT * (s + 6 * (size_t)e))];
+  FLUXO_CUDA(h, cudaMemcpyAsync(h->dSurfMet, d.data(), d.size() * 8, cudaMemcpyHostToDevice, h->stream));
+  FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->surfMetSet = true;
   return FLUXO_OK;
 }
 
@@ -1026,7 +1099,7 @@ int fluxo_gpu_destroy(fluxo_handle* h) {
   void* ptrs[] = {h->dBasis, h->dU, h->dUt, h->dUtTmp, h->dGrad, h->dUtVisc, h->dMetrics, h->dsJ, h->dFaceGeo, h->dXGP,
                   h->dFlux, h->dLFlux, h->dGTrace, h->dS2E, h->dE2S, h->dTD, h->dDtBits, h->dErrKey,
                   h->dAlpha, h->dAlphaRaw, h->dAlphaTmp, h->dFV, h->dFFV, h->dSVdm, h->dBlendList, h->dBlendCount,
-                  h->dAnaPartial, h->dAnaRes, h->dAnaTables, h->dUReg2};
+                  h->dAnaPartial, h->dAnaRes, h->dAnaTables, h->dUReg2, h->dUface, h->dUtSurf, h->dSurfMet};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->stream) cudaStreamDestroy(h->stream);

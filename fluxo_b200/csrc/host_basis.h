@@ -187,5 +187,32 @@ struct LGLBasis {
   }
 };
 
+// Gauss-Legendre basis of degree N (InitDGbasis dg.f90:181-252 with NodeType 'GAUSS'): D, D_hat, the
+// interpolation to the element faces L_Minus / L_Plus, L_HatMinus = L_Minus / w and the split-form
+// operator Dvolsurf = 2 D - M^-1 Vf^T B Vf (Vf rows L_Minus, L_Plus; B = diag(-1, 1)), skew-symmetric
+// in the M inner product, so its diagonal is zero.
+struct GaussBasis {
+  int N;
+  std::vector<double> x, w, D, Dhat, Dvs, Lminus, Lplus, LhatMinus;
+  explicit GaussBasis(int N_) : N(N_) {
+    gauss(N, x, w);
+    D = deriv_matrix(x);
+    const int n = N + 1;
+    std::vector<double> wb = bary(x);
+    Lminus.assign(n, 0.); Lplus.assign(n, 0.); LhatMinus.assign(n, 0.);
+    lagrange_at(x, wb, -1., Lminus.data());
+    lagrange_at(x, wb, 1., Lplus.data());
+    for (int i = 0; i < n; ++i) LhatMinus[i] = Lminus[i] / w[i];
+    Dhat.assign((size_t)n * n, 0.);
+    Dvs.assign((size_t)n * n, 0.);
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        Dhat[(size_t)i * n + j] = -D[(size_t)j * n + i] * w[j] / w[i];
+        const double vbv = -Lminus[i] * Lminus[j] + Lplus[i] * Lplus[j];
+        Dvs[(size_t)i * n + j] = 2. * D[(size_t)i * n + j] - vbv / w[i];
+      }
+  }
+};
+
 }  // namespace host
 }  // namespace fluxo

@@ -48,8 +48,11 @@ __device__ __forceinline__ void face_flux_body(const KParams& P, int NP) {
     const int p = pt % NP, q = pt / NP;
     nM = side_node(NP - 1, p, q, 0, lsM);
     nS = side_node(NP - 1, p, q, fl, lsS);
-    const double* UM = P.U + 5 * ((size_t)eM * NP * NP * NP + nM);
-    const double* US = P.U + 5 * ((size_t)eS * NP * NP * NP + nS);
+    // LGL: the side's volume nodes; Gauss: the interpolated face states of both sides
+    const double* UM = P.uface ? P.uface + ((size_t)side * 2 * npts + pt) * 5
+                               : P.U + 5 * ((size_t)eM * NP * NP * NP + nM);
+    const double* US = P.uface ? P.uface + (((size_t)side * 2 + 1) * npts + pt) * 5
+                               : P.U + 5 * ((size_t)eS * NP * NP * NP + nS);
     const double* g = P.facegeo + (size_t)side * 10 * npts + pt;
 #pragma unroll
     for (int d = 0; d < 3; ++d) { nv[d] = g[d * npts]; t1[d] = g[(3 + d) * npts]; t2[d] = g[(6 + d) * npts]; }
@@ -116,8 +119,10 @@ static __global__ void lift_flux_kernel(KParams P, int NP, double* lf) {
   const int p = pt % NP, q = pt / NP;
   const int nM = side_node(NP - 1, p, q, 0, se5[2]);
   const int nS = side_node(NP - 1, p, q, se5[4], se5[3]);
-  const double* UM = P.U + 5 * ((size_t)se5[0] * NP * NP * NP + nM);
-  const double* US = P.U + 5 * ((size_t)se5[1] * NP * NP * NP + nS);
+  const double* UM = P.uface ? P.uface + ((size_t)side * 2 * npts + pt) * 5
+                             : P.U + 5 * ((size_t)se5[0] * NP * NP * NP + nM);
+  const double* US = P.uface ? P.uface + (((size_t)side * 2 + 1) * npts + pt) * 5
+                             : P.U + 5 * ((size_t)se5[1] * NP * NP * NP + nS);
   double uM[5], uS[5], VM[5], VS[5];
   for (int v = 0; v < 5; ++v) { uM[v] = UM[v]; uS[v] = US[v]; }
   lifting_var(P, uM, VM);
@@ -344,18 +349,23 @@ volume_kernel(KParams P) {
 #pragma unroll
     for (int v = 0; v < 4; ++v) ut[1 + v] += V[v * NP3];
   }
-  // surface integral at the boundary nodes (LGL)
-  const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
-  int sides[3];
-  const int ns = boundary_sides(i, j, k, N, sides);
-  const double lh = P.basis->LhatM0;
-  for (int z = 0; z < ns; ++z) {
-    const int s = sides[z], side = sE2S[eb][2 * (s - 1)], flip = sE2S[eb][2 * (s - 1) + 1];
-    const int pt = node_side_point(N, s, flip, i, j, k);
-    const double* F = P.flux + (size_t)side * 5 * NPT + pt;
-    const double sg = (flip == 0) ? lh : -lh;
+  if (P.utsurf) {  // Gauss nodes: the surface integral of every node, formed by the surface kernel
+    const double* S = P.utsurf + (size_t)e * 5 * NP3 + t;
 #pragma unroll
-    for (int v = 0; v < 5; ++v) ut[v] += sg * F[v * NPT];
+    for (int v = 0; v < 5; ++v) ut[v] += S[v * NP3];
+  } else {  // surface integral at the boundary nodes (LGL)
+    const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
+    int sides[3];
+    const int ns = boundary_sides(i, j, k, N, sides);
+    const double lh = P.basis->LhatM0;
+    for (int z = 0; z < ns; ++z) {
+      const int s = sides[z], side = sE2S[eb][2 * (s - 1)], flip = sE2S[eb][2 * (s - 1) + 1];
+      const int pt = node_side_point(N, s, flip, i, j, k);
+      const double* F = P.flux + (size_t)side * 5 * NPT + pt;
+      const double sg = (flip == 0) ? lh : -lh;
+#pragma unroll
+      for (int v = 0; v < 5; ++v) ut[v] += sg * F[v * NPT];
+    }
   }
   // Ut = -Ut*sJ  (+ source)
   const double sj = P.sJ[(size_t)e * NP3 + t];

@@ -82,6 +82,7 @@ extern "C" int fluxo_gpu_dg_time_derivative_noalloc(const fluxo_cfg* cfg, int nE
   if (cfg->eqn != FLUXO_EQN_EULER) return bad(FLUXO_EINVAL_CFG, "only the Euler equations (eqn 0) are supported");
   if (cfg->ini_exact_func == 4) return bad(FLUXO_EINVAL_CFG, "the source term (IniExactFunc 4) is not supported");
   if (cfg->nfvse != 0) return bad(FLUXO_EINVAL_CFG, "NFVSE shock capturing (nfvse = 1) is not supported");
+  if (cfg->node_type == 1) return bad(FLUXO_EINVAL_CFG, "Gauss nodes (node_type = 1) are not supported");
   if (!riemann_supported(cfg->riemann)) return bad(FLUXO_EINVAL_CFG, "Riemann solver not implemented");
   if (!volume_flux_supported(cfg->volume_flux)) return bad(FLUXO_EINVAL_CFG, "volume flux not implemented");
   if (!(cfg->kappa > 1.)) return bad(FLUXO_EINVAL_CFG, "kappa must be > 1");

@@ -33,7 +33,7 @@ def make_cfg(**fields):
                     nfvse=0, compute_alpha=1, shock_blend_coef=0.0, modal_threshold=1, alpha_max=0.5,
                     alpha_min=0.01, space_prop_factor=0.5, space_prop_sweeps=1, time_rel_factor=0.0,
                     indicator_quantity=3, sub_fv_method=1, recons_boundaries=1, nfvse_corr=0,
-                    posit_corr_factor=0.1, posit_max_iter=10)
+                    posit_corr_factor=0.1, posit_max_iter=10, node_type=2)
     defaults.update(fields)
     for k, v in defaults.items():
         setattr(cfg, k, v)
@@ -115,6 +115,8 @@ class DGOperator:
         r = self.lib.fluxo_gpu_set_mesh(self.h, self.nElems, self.nSides, _ptr(self._keep[0]), _ptr(self._keep[1]),
                                         *[_ptr(a) for a in arrs], _ptr(self._keep[3]))
         self._check(r)
+        if m.get("SurfMetrics") is not None:  # Gauss nodes: SurfMetrics(3,0:N,0:N,6,nElems)
+            self._check(self.lib.fluxo_gpu_set_surf_metrics(self.h, _ptr(_c(m["SurfMetrics"]))))
 
     @property
     def shape(self):

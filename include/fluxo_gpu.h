@@ -47,8 +47,8 @@ enum { FLUXO_EQN_EULER = 0, FLUXO_EQN_NAVIERSTOKES = 1, FLUXO_EQN_MHD = 2, FLUXO
 /* Runtime configuration: the parameter.ini keys of the reference's hot path
  * (src/equation/navierstokes/equation.f90:162-470, src/timedisc/timedisc.f90:74-137,
  * src/dg/br2/br2.f90:91-149) plus the compile-time switches the reference fixes
- * with CMake (PARABOLIC, PP_Lifting, PP_Lifting_Var, PP_VISC), which are runtime
- * choices here.  LGL nodes and the split (flux-differencing) form are fixed. */
+ * with CMake (PARABOLIC, PP_Lifting, PP_Lifting_Var, PP_VISC, PP_NodeType), which are runtime
+ * choices here.  The split (flux-differencing) form is fixed. */
 typedef struct fluxo_cfg {
   int struct_size;   /* sizeof(fluxo_cfg) */
   int N;             /* N: polynomial degree, 1..7 (one thread per volume node) */
@@ -104,6 +104,12 @@ typedef struct fluxo_cfg {
   int nfvse_corr;          /* 0 off, 1 on (needs nfvse = 1) */
   double posit_corr_factor; /* PositCorrFactor (reference default 0.1) */
   int posit_max_iter;      /* PositMaxIter (reference default 10) */
+  /* PP_NodeType (CMake FLUXO_DISC_NODETYPE): 2 (or 0) Gauss-Lobatto, 1 Gauss.  Gauss nodes run the
+   * entropy-stable Gauss collocation of the split form (interpolated face states, entropy-projected for
+   * the EC volume fluxes 5, 6, 7, 10, 32; surface correction with SurfMetrics, which the caller supplies
+   * with fluxo_gpu_set_surf_metrics after fluxo_gpu_set_mesh); Euler / Navier-Stokes only, without
+   * NFVSE, batches or the allocation-free entry point. */
+  int node_type;
 } fluxo_cfg;
 
 typedef struct fluxo_handle fluxo_handle;
@@ -123,6 +129,11 @@ int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* SideT
                        const double* Metrics_gTilde, const double* Metrics_hTilde,
                        const double* sJ, const double* NormVec, const double* TangVec1,
                        const double* TangVec2, const double* SurfElem, const double* Elem_xGP);
+
+/* Gauss nodes: SurfMetrics(3,0:N,0:N,6,nElems), the normal metric term of every element side at the
+ * side's points in the master side's point order (src/mesh/metrics.f90:420-427, mesh_vars.f90:67-70).
+ * Required before the first right-hand side of a handle with node_type = 1; FLUXO_EINVAL_CFG for LGL. */
+int fluxo_gpu_set_surf_metrics(fluxo_handle* h, const double* SurfMetrics);
 
 /* MOD_DG_Vars::U host <-> device (src/dg/dg_vars.f90:75).  The device copy is
  * authoritative between set_state and get_state. */

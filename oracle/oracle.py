@@ -219,6 +219,8 @@ class OracleCase:
         self.lib.orc_get_mesh(self.h, *[_ptr(m[k]) for k in (
             "SideToElem", "ElemToSide", "Metrics_fTilde", "Metrics_gTilde", "Metrics_hTilde", "sJ",
             "NormVec", "TangVec1", "TangVec2", "SurfElem", "Elem_xGP")])
+        if self.params.node_type == 1:
+            m["SurfMetrics"] = self.surf_metrics()
         return m
 
     def set_metrics(self, m):
