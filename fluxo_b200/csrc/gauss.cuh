@@ -372,10 +372,12 @@ __global__ void __launch_bounds__(NP * NP * NP) surf_kernel(KParams P) {
       for (int v = 0; v < 5; ++v) us[v] = uf[v];
       make_record<VF>(P, us, rF);
     }
+    // pair_flux takes half metrics for every flux but the standard DG one (the metric average is a sum)
+    constexpr double hm = VF == 0 ? 1.0 : 0.5;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      mN[c] = M[(3 * dir + c) * NP3];
-      mS[c] = P.surfMet[(((size_t)e * 6 + (s - 1)) * 3 + c) * NPT + pt];
+      mN[c] = hm * M[(3 * dir + c) * NP3];
+      mS[c] = hm * P.surfMet[(((size_t)e * 6 + (s - 1)) * 3 + c) * NPT + pt];
     }
     pair_flux<VF>(P, rN, rF, mN, mS, FB);
 #pragma unroll

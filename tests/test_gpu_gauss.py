@@ -28,6 +28,7 @@ def pair(noise=0.03, seed=2, **kw):
     p = c.params
     op = fb.DGOperator(N=p.N, eqn=p.eqn, riemann=p.riemann, volume_flux=p.volume_flux, lifting=p.lifting,
                        lifting_var=p.lifting_var, visc=p.visc, kappa=p.kappa, Pr=p.Pr, mu0=p.mu0, etaBR2=p.etaBR2,
+                       R=p.R, Ts=p.Ts, Tref=p.Tref, ExpoSuth=p.ExpoSuth, ExpoPow=p.ExpoPow,
                        time_disc=p.time_disc, cfl_scale=p.cfl_scale, dfl_scale=p.dfl_scale, ini_exact_func=1,
                        node_type=1)
     op.set_mesh(c.mesh())
