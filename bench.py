@@ -316,10 +316,13 @@ def run_fluxo(args):
         U0 = mhd_orszag_tang_state(mesh["Elem_xGP"], kappa=w["kappa"])
     else:
         w = workload(elems=args.elems or 32, N=args.N or 7)
-        mesh = fb.box_mesh(w["N"], w["elems"], w["xmin"], w["xmax"], NGeo=w["NGeo"], deform_amp=w["deform_amp"])
+        nt = 1 if args.nodes == "gauss" else 2
+        mesh = fb.box_mesh(w["N"], w["elems"], w["xmin"], w["xmax"], NGeo=w["NGeo"], deform_amp=w["deform_amp"],
+                           node_type=nt)
         op = fb.DGOperator(N=w["N"], eqn=1, riemann=w["riemann"], volume_flux=w["volume_flux"], lifting=1,
                            lifting_var=3, visc=0, mu0=w["mu0"], Pr=w["Pr"], kappa=w["kappa"],
-                           cfl_scale=w["cfl_scale"], dfl_scale=w["dfl_scale"], time_disc=0, device=local)
+                           cfl_scale=w["cfl_scale"], dfl_scale=w["dfl_scale"], time_disc=0, device=local,
+                           node_type=nt)
         op.set_mesh(mesh)
         U0 = fb.exact_func(7, 0.0, mesh["Elem_xGP"], kappa=w["kappa"])
     del mesh
@@ -395,7 +398,10 @@ def run_fluxo(args):
                 "flops_per_dof_launch": vol_falg, "launch_ms": vol_avg_ms,
                 "fp64_pipe_active_ncu": None if mhd else NCU_FP64_PIPE_ACTIVE["volume"],
                 "peak_source": "measured in this job: DFMA loop (fluxo_gpu_fp64_peak); MEASURED_PEAKS.json has no FP64"}
-    per_kernel = None if mhd else kernel_rooflines(kinds, w["N"], nd, op.nElems, peak)
+    gauss = args.nodes == "gauss"
+    # Gauss nodes: the face pass also holds the prolongation and the surface kernel, so the per-kernel and
+    # whole-RHS fractions (F_alg of the LGL scheme) do not apply
+    per_kernel = None if (mhd or gauss) else kernel_rooflines(kinds, w["N"], nd, op.nElems, peak)
     falg_rhs = sum((MHD_FALG_PER_DOF if mhd else FALG_PER_DOF).values())
     if mhd:
         alpha = op.alpha()
@@ -408,20 +414,23 @@ def run_fluxo(args):
                   "l2": "inputs larger than L2 (state %d MB)" % (nd * 72 // 10 ** 6), "steps": args.steps}
     else:
         config = config_dict(w, world, args.steps)
+        if gauss:
+            config["workload"] += "_gauss_nodes"
+            config["nodes"] = "Gauss (entropy-projected face states, FluxB surface correction)"
     line = {"metric": MHD_METRIC if mhd else METRIC, "value": value, "unit": "ns/DOF/RHS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config, "roofline": roofline, "roofline_kernels": per_kernel, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clk.summary(),
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kinds.items()},
-            "rhs_roofline_frac": (falg_rhs * nd * rhs / (ms * 1e-3) / 1e12) / peak,
+            "rhs_roofline_frac": None if gauss else (falg_rhs * nd * rhs / (ms * 1e-3) / 1e12) / peak,
             "setup_s": setup_s}
     if not mhd:
         line["volume_shape"] = shape_dict(w["N"], w["volume_flux"], True)
     if world == 1 and not args.no_cpu and not mhd:
         line["cpu_baseline"] = cpu_baseline_subprocess(os.cpu_count() or 1, seconds=args.cpu_seconds)
     op.close()
-    if world == 1 and not mhd and not args.no_mix:
+    if world == 1 and not mhd and not gauss and not args.no_mix:
         # the other half of the headline metric: batched vs plain and served p50/p99, on this GPU
         line["batch"] = measure_batch(args, world, rank, local, steps=args.mix_steps)
         line["serve"] = measure_serve(args, world, rank, local)
@@ -819,6 +828,8 @@ def main():
     ap.add_argument("--poll-steps", type=int, default=2, help="serve: time steps between admission rounds")
     ap.add_argument("--elems", type=int, default=0, help="elements per direction (0: the configuration's)")
     ap.add_argument("--N", type=int, default=0, help="polynomial degree (0: the configuration's)")
+    ap.add_argument("--nodes", default="lgl", choices=("lgl", "gauss"),
+                    help="tgv: Gauss-Lobatto (the headline) or Gauss nodes (PP_NodeType)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)

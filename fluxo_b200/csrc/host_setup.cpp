@@ -276,6 +276,165 @@ void box_geometry(int N, const int* ne, const double* xmin, const double* xmax, 
   }
 }
 
+// Gauss nodes (CalcMetrics / CalcSurfMetrics with NodeType 'GAUSS', metrics.f90:78-440): the coordinates,
+// their derivatives and the curl-form metric terms on the Gauss-Lobatto points of degree N, then
+// interpolated to the Gauss nodes (Vdm_GLN_N); the Jacobian through 3*NGeo Gauss points, projected to N;
+// the side quantities from the Gauss-Lobatto metric terms of the side interpolated to the side's Gauss
+// points, SurfMetrics (the normal metric term) for every side in the master's point order.
+void box_geometry_gauss(int N, const int* ne, const double* xmin, const double* xmax, int NGeo, double amp,
+                        const std::vector<int>& E2S, double* Mf, double* Mg, double* Mh, double* sJ, double* NormVec,
+                        double* TangVec1, double* TangVec2, double* SurfElem, double* Elem_xGP, double* SurfMetrics) {
+  const int nx = ne[0], ny = ne[1], nz = ne[2], nElems = nx * ny * nz;
+  const int n = N + 1, ng = NGeo + 1, NR = 3 * NGeo, nr = NR + 1;
+  const size_t nv = (size_t)n * n * n;
+  GaussBasis bG(N);
+  std::vector<double> xeq(ng), xg, wg, xr, wr, xGL, wGL;
+  for (int i = 0; i < ng; ++i) xeq[i] = NGeo > 0 ? 2. * i / NGeo - 1. : 0.;
+  lgl(NGeo, xg, wg);
+  gauss(NR, xr, wr);
+  lgl(N, xGL, wGL);
+  const std::vector<double> V_eq_g = interp_matrix(xeq, xg);
+  const std::vector<double> V_g_GL = interp_matrix(xg, xGL);
+  const std::vector<double> V_GL_N = interp_matrix(xGL, bG.x);
+  const std::vector<double> V_g_r = interp_matrix(xg, xr);
+  std::vector<double> V_r_N;
+  if (NR > N) V_r_N = modal_projection(xr, bG.x);
+  else if (NR < N) V_r_N = interp_matrix(xr, bG.x);
+  const std::vector<double> Dg = deriv_matrix(xg), DGL = deriv_matrix(xGL);
+  const double L[3] = {xmax[0] - xmin[0], xmax[1] - xmin[1], xmax[2] - xmin[2]};
+  const double c[3] = {0.5 * (xmax[0] + xmin[0]), 0.5 * (xmax[1] + xmin[1]), 0.5 * (xmax[2] + xmin[2])};
+  const double h[3] = {L[0] / nx, L[1] / ny, L[2] / nz};
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int e = 0; e < nElems; ++e) {
+    const int ix = e % nx, iy = (e / nx) % ny, iz = e / (nx * ny);
+    std::vector<double> Xeq(3 * ng * ng * ng), Xg(3 * ng * ng * ng), XGL(3 * nv), dXg(9 * ng * ng * ng),
+        tmp(3 * ng * ng * ng);
+    for (int k = 0; k < ng; ++k)
+      for (int j = 0; j < ng; ++j)
+        for (int i = 0; i < ng; ++i) {
+          const double xs[3] = {xmin[0] + h[0] * (ix + (double)i / NGeo), xmin[1] + h[1] * (iy + (double)j / NGeo),
+                                xmin[2] + h[2] * (iz + (double)k / NGeo)};
+          double f = amp;
+          if (f != 0.)
+            for (int d = 0; d < 3; ++d) f *= std::sin(2. * M_PI * (xs[d] - c[d]) / L[d]);
+          for (int d = 0; d < 3; ++d) Xeq[3 * (i + ng * (j + ng * k)) + d] = xs[d] + f;
+        }
+    tp_interp(3, ng, ng, V_eq_g, Xeq.data(), Xg.data());
+    tp_interp(3, ng, n, V_g_GL, Xg.data(), XGL.data());
+    tp_interp(3, n, n, V_GL_N, XGL.data(), Elem_xGP + 3 * nv * e);
+    for (int dir = 0; dir < 3; ++dir) {
+      tp_deriv(3, ng, Dg, dir, Xg.data(), tmp.data());
+      for (int z = 0; z < ng * ng * ng; ++z)
+        for (int d = 0; d < 3; ++d) dXg[9 * z + 3 * dir + d] = tmp[3 * z + d];
+    }
+    std::vector<double> dXr((size_t)9 * nr * nr * nr), detr((size_t)nr * nr * nr), detN(nv);
+    tp_interp(9, ng, nr, V_g_r, dXg.data(), dXr.data());
+    for (int z = 0; z < nr * nr * nr; ++z) {
+      const double* t = &dXr[9 * z];
+      const double* u = t + 3;
+      const double* w = t + 6;
+      detr[z] = t[0] * (u[1] * w[2] - u[2] * w[1]) - t[1] * (u[0] * w[2] - u[2] * w[0]) + t[2] * (u[0] * w[1] - u[1] * w[0]);
+    }
+    if (NR == N) std::copy(detr.begin(), detr.end(), detN.begin());
+    else tp_interp(1, nr, n, V_r_N, detr.data(), detN.data());
+    for (size_t z = 0; z < nv; ++z) sJ[nv * e + z] = 1. / detN[z];
+    std::vector<double> dXN((size_t)9 * nv), tN(3 * nv);
+    if (N >= NGeo) {
+      tp_interp(9, ng, n, V_g_GL, dXg.data(), dXN.data());
+    } else {
+      for (int dir = 0; dir < 3; ++dir) {
+        tp_deriv(3, n, DGL, dir, XGL.data(), tN.data());
+        for (size_t z = 0; z < nv; ++z)
+          for (int d = 0; d < 3; ++d) dXN[9 * z + 3 * dir + d] = tN[3 * z + d];
+      }
+    }
+    std::vector<double> R((size_t)9 * nv), dR((size_t)9 * nv), Ja((size_t)9 * nv, 0.), JaG((size_t)9 * nv);
+    for (size_t z = 0; z < nv; ++z)
+      for (int dir = 0; dir < 3; ++dir)
+        for (int cc = 0; cc < 3; ++cc) {
+          const int c1 = (cc + 1) % 3, c2 = (cc + 2) % 3;
+          R[9 * z + 3 * dir + cc] = 0.5 * (XGL[3 * z + c2] * dXN[9 * z + 3 * dir + c1] - XGL[3 * z + c1] * dXN[9 * z + 3 * dir + c2]);
+        }
+    for (int dd = 0; dd < 3; ++dd) {
+      tp_deriv(9, n, DGL, dd, R.data(), dR.data());
+      for (size_t z = 0; z < nv; ++z)
+        for (int i = 0; i < 3; ++i)
+          for (int cc = 0; cc < 3; ++cc) {
+            if (dd == (i + 2) % 3) Ja[9 * z + 3 * i + cc] += dR[9 * z + 3 * ((i + 1) % 3) + cc];
+            if (dd == (i + 1) % 3) Ja[9 * z + 3 * i + cc] -= dR[9 * z + 3 * ((i + 2) % 3) + cc];
+          }
+    }
+    tp_interp(9, n, n, V_GL_N, Ja.data(), JaG.data());
+    for (size_t z = 0; z < nv; ++z)
+      for (int cc = 0; cc < 3; ++cc) {
+        Mf[3 * (nv * e + z) + cc] = JaG[9 * z + 0 + cc];
+        Mg[3 * (nv * e + z) + cc] = JaG[9 * z + 3 + cc];
+        Mh[3 * (nv * e + z) + cc] = JaG[9 * z + 6 + cc];
+      }
+    // sides: the Gauss-Lobatto boundary slice of Ja (tangential volume indices in increasing order)
+    // interpolated to the side's Gauss points
+    std::vector<double> sl((size_t)9 * n * n), b1((size_t)9 * n * n), JaF((size_t)9 * n * n);
+    for (int s = 1; s <= 6; ++s) {
+      const int sid = E2S[(size_t)2 * (6 * e + s - 1)], flip = E2S[(size_t)2 * (6 * e + s - 1) + 1];
+      for (int b = 0; b < n; ++b)
+        for (int a = 0; a < n; ++a) {
+          int i, j, k;
+          switch (s) {
+            case 5: i = 0; j = a; k = b; break;
+            case 3: i = N; j = a; k = b; break;
+            case 2: i = a; j = 0; k = b; break;
+            case 4: i = a; j = N; k = b; break;
+            case 1: i = a; j = b; k = 0; break;
+            default: i = a; j = b; k = N; break;
+          }
+          for (int q = 0; q < 9; ++q) sl[q + 9 * (a + n * b)] = Ja[9 * (i + n * (j + (size_t)n * k)) + q];
+        }
+      std::fill(b1.begin(), b1.end(), 0.);
+      std::fill(JaF.begin(), JaF.end(), 0.);
+      for (int b = 0; b < n; ++b)
+        for (int ao = 0; ao < n; ++ao)
+          for (int a = 0; a < n; ++a)
+            for (int q = 0; q < 9; ++q) b1[q + 9 * (ao + n * b)] += V_GL_N[(size_t)ao * n + a] * sl[q + 9 * (a + n * b)];
+      for (int bo = 0; bo < n; ++bo)
+        for (int b = 0; b < n; ++b)
+          for (int a = 0; a < n; ++a)
+            for (int q = 0; q < 9; ++q) JaF[q + 9 * (a + n * bo)] += V_GL_N[(size_t)bo * n + b] * b1[q + 9 * (a + n * b)];
+      const int nd = kNormalDir[s] - 1, td = kTangDir[s] - 1;
+      for (int q = 0; q < n; ++q)
+        for (int p = 0; p < n; ++p) {
+          int ijk[3];
+          side_to_vol(N, 0, p, q, 0, s, ijk);  // the element's own (CGNS) frame of the side
+          const int a = (s == 5 || s == 3) ? ijk[1] : ijk[0];
+          const int b = (s == 1 || s == 6) ? ijk[1] : ijk[2];
+          const double* J = &JaF[9 * (a + n * b)];
+          const double* jn = J + 3 * nd;
+          const double* jt = J + 3 * td;
+          int pm, qm;
+          flip_pq(N, p, q, flip, pm, qm);  // FS2M: the master side's point (the flips are involutions)
+          double* SM = SurfMetrics + 3 * ((size_t)pm + n * ((size_t)qm + n * ((size_t)(s - 1) + 6 * (size_t)e)));
+          for (int d = 0; d < 3; ++d) SM[d] = jn[d];
+          if (flip != 0) continue;
+          const size_t fi = p + n * (q + (size_t)n * (sid - 1));
+          const double se = std::sqrt(jn[0] * jn[0] + jn[1] * jn[1] + jn[2] * jn[2]);
+          double nv3[3], t1[3];
+          for (int d = 0; d < 3; ++d) nv3[d] = kNormalSign[s] * jn[d] / se;
+          const double dot = jt[0] * nv3[0] + jt[1] * nv3[1] + jt[2] * nv3[2];
+          for (int d = 0; d < 3; ++d) t1[d] = jt[d] - dot * nv3[d];
+          const double tn = std::sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+          for (int d = 0; d < 3; ++d) t1[d] /= tn;
+          SurfElem[fi] = se;
+          for (int d = 0; d < 3; ++d) {
+            NormVec[3 * fi + d] = nv3[d];
+            TangVec1[3 * fi + d] = t1[d];
+          }
+          TangVec2[3 * fi + 0] = nv3[1] * t1[2] - nv3[2] * t1[1];
+          TangVec2[3 * fi + 1] = nv3[2] * t1[0] - nv3[0] * t1[2];
+          TangVec2[3 * fi + 2] = nv3[0] * t1[1] - nv3[1] * t1[0];
+        }
+    }
+  }
+}
+
 bool repack_mesh(int N, int nElems, int nSides, const int* S2E, const int* E2S, const double* Mf, const double* Mg,
                  const double* Mh, const double* NormVec, const double* TangVec1, const double* TangVec2,
                  const double* SurfElem, std::vector<int>& s2e, std::vector<int>& e2s, std::vector<double>& met,
@@ -349,6 +508,24 @@ extern "C" int fluxo_host_box_mesh(int N, const int* ne, const double* xmin, con
     std::copy(S2E.begin(), S2E.end(), SideToElem);
     std::copy(E2S.begin(), E2S.end(), ElemToSide);
     box_geometry(N, ne, xmin, xmax, NGeo, amp, E2S, Mf, Mg, Mh, sJ, NormVec, TangVec1, TangVec2, SurfElem, Elem_xGP);
+  } catch (...) {
+    return FLUXO_EINVAL_CFG;
+  }
+  return FLUXO_OK;
+}
+
+extern "C" int fluxo_host_box_mesh_gauss(int N, const int* ne, const double* xmin, const double* xmax, int NGeo,
+                                         double amp, int* SideToElem, int* ElemToSide, double* Mf, double* Mg,
+                                         double* Mh, double* sJ, double* NormVec, double* TangVec1, double* TangVec2,
+                                         double* SurfElem, double* Elem_xGP, double* SurfMetrics) {
+  if (N < 1 || N > 8 || NGeo < 1 || !ne || !SurfMetrics) return FLUXO_EINVAL_CFG;
+  try {
+    std::vector<int> S2E, E2S;
+    box_connectivity(ne, N, S2E, E2S);
+    std::copy(S2E.begin(), S2E.end(), SideToElem);
+    std::copy(E2S.begin(), E2S.end(), ElemToSide);
+    box_geometry_gauss(N, ne, xmin, xmax, NGeo, amp, E2S, Mf, Mg, Mh, sJ, NormVec, TangVec1, TangVec2, SurfElem,
+                       Elem_xGP, SurfMetrics);
   } catch (...) {
     return FLUXO_EINVAL_CFG;
   }

@@ -12,6 +12,8 @@ import re
 KEYS = {
     # interpolation / mesh
     "n": ("i", None),
+    # node set (CMake FLUXO_DISC_NODETYPE, a key here): GAUSS-LOBATTO or GAUSS
+    "nodetype": ("s", "GAUSS-LOBATTO"),
     "boxelems": ("ia", (8, 8, 8)),
     "boxmin": ("ra", (-1.0, -1.0, -1.0)),
     "boxmax": ("ra", (1.0, 1.0, 1.0)),
@@ -173,6 +175,10 @@ def to_cfg_fields(res):
         time_disc=_TIMEDISC[tdm], cfl_scale=res["cflscale"], dfl_scale=res["dflscale"],
         ini_exact_func=res["iniexactfunc"], ini_frequency=res["inifrequency"], ini_amplitude=res["iniamplitude"],
     )
+    nodes = str(res["nodetype"]).strip().upper()
+    if nodes not in ("GAUSS", "GAUSS-LOBATTO"):
+        raise ValueError("NodeType %r not implemented (GAUSS, GAUSS-LOBATTO)" % res["nodetype"])
+    f["node_type"] = 1 if nodes == "GAUSS" else 2
     ind = str(res["shockindicatorquantity"]).strip().lower()
     if ind not in _INDICATOR:
         raise ValueError("ShockIndicatorQuantity %r not implemented" % res["shockindicatorquantity"])

@@ -40,8 +40,9 @@ def make_cfg(**fields):
     return cfg
 
 
-def box_mesh(N, elems, xmin, xmax, NGeo=1, deform_amp=0.0):
-    """Reference-layout mesh arrays of a periodic box (C ABI ``fluxo_host_box_mesh``).
+def box_mesh(N, elems, xmin, xmax, NGeo=1, deform_amp=0.0, node_type=2):
+    """Reference-layout mesh arrays of a periodic box (C ABI ``fluxo_host_box_mesh``; node_type 1: Gauss
+    nodes, ``fluxo_host_box_mesh_gauss``, with ``SurfMetrics[e,side,q,p,:]``).
 
     Numpy shapes are the C-order views of the Fortran arrays, e.g. ``Metrics_fTilde[e,k,j,i,:]``.
     """
@@ -58,8 +59,13 @@ def box_mesh(N, elems, xmin, xmax, NGeo=1, deform_amp=0.0):
         NormVec=np.zeros((nS, n, n, 3)), TangVec1=np.zeros((nS, n, n, 3)), TangVec2=np.zeros((nS, n, n, 3)),
         SurfElem=np.zeros((nS, n, n)), Elem_xGP=np.zeros((nE, n, n, n, 3)),
     )
-    r = lib.fluxo_host_box_mesh(N, _ptr(ne), _ptr(_c(xmin)), _ptr(_c(xmax)), NGeo, float(deform_amp),
-                                *[_ptr(m[k]) for k in MESH_KEYS])
+    if node_type == 1:
+        m["SurfMetrics"] = np.zeros((nE, 6, n, n, 3))
+        r = lib.fluxo_host_box_mesh_gauss(N, _ptr(ne), _ptr(_c(xmin)), _ptr(_c(xmax)), NGeo, float(deform_amp),
+                                          *[_ptr(m[k]) for k in MESH_KEYS], _ptr(m["SurfMetrics"]))
+    else:
+        r = lib.fluxo_host_box_mesh(N, _ptr(ne), _ptr(_c(xmin)), _ptr(_c(xmax)), NGeo, float(deform_amp),
+                                    *[_ptr(m[k]) for k in MESH_KEYS])
     _lib.check(r)
     return m
 
@@ -225,7 +231,8 @@ class Fluxo:
         fields = to_cfg_fields(o)
         fields["device"] = device
         # InitMesh (synthetic periodic box in place of the HOPR file) + CalcMetrics
-        self.mesh = box_mesh(o["n"], o["boxelems"], o["boxmin"], o["boxmax"], o["ngeo"], o["meshdeformamp"])
+        self.mesh = box_mesh(o["n"], o["boxelems"], o["boxmin"], o["boxmax"], o["ngeo"], o["meshdeformamp"],
+                             node_type=fields.get("node_type", 2))
         self.op = DGOperator(**fields)
         self.op.set_mesh(self.mesh)
         # InitDG: FillIni(IniExactFunc, U)

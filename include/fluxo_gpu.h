@@ -319,6 +319,14 @@ int fluxo_host_box_mesh(int N, const int* nElemsXYZ, const double* xmin, const d
                         double deform_amp, int* SideToElem, int* ElemToSide, double* Metrics_fTilde,
                         double* Metrics_gTilde, double* Metrics_hTilde, double* sJ, double* NormVec,
                         double* TangVec1, double* TangVec2, double* SurfElem, double* Elem_xGP);
+/* The same periodic box for Gauss nodes (node_type = 1): metric terms and Jacobian at the Gauss nodes,
+ * side quantities at the sides' Gauss points, and SurfMetrics(3,0:N,0:N,6,nElems) for
+ * fluxo_gpu_set_surf_metrics.  Replaces the NodeType 'GAUSS' branch of src/mesh/metrics.f90:78-440. */
+int fluxo_host_box_mesh_gauss(int N, const int* nElemsXYZ, const double* xmin, const double* xmax, int NGeo,
+                              double deform_amp, int* SideToElem, int* ElemToSide, double* Metrics_fTilde,
+                              double* Metrics_gTilde, double* Metrics_hTilde, double* sJ, double* NormVec,
+                              double* TangVec1, double* TangVec2, double* SurfElem, double* Elem_xGP,
+                              double* SurfMetrics);
 /* FillIni(IniExactFunc, U) on the given node coordinates (src/equation/navierstokes/equation.f90:575-950):
  * IniExactFunc 1 (constant refstate, prim given), 2 (density sine wave), 4 (manufactured), 7 (Taylor-Green),
  * 14 (soft Sedov-Taylor blast around IniCenter = 0). */

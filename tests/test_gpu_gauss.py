@@ -108,3 +108,31 @@ def test_gauss_configuration_checks(gpu_lib):
     op2.set_state(c.get_U())
     with pytest.raises(FluxoError):
         op2.dg_time_derivative(0.0)
+
+
+def test_gauss_product_setup_path(gpu_lib):
+    """Fluxo() from a parameter.ini with NodeType = GAUSS: the product's own Gauss box mesh (metrics at the
+    Gauss nodes, SurfMetrics), initial state and operator, against the oracle."""
+    ini = """
+    N = 4
+    NodeType = GAUSS
+    BoxElems = (/3,2,2/)
+    BoxMin = (/-1.,-1.,-1./)
+    BoxMax = (/1.,1.,1./)
+    NGeo = 2
+    MeshDeformAmp = 0.1
+    IniExactFunc = 2
+    IniAmplitude = 0.3
+    AdvVel = (/0.3,-0.2,0.5/)
+    Riemann = 44
+    VolumeFlux = 5
+    mu0 = 0.01
+    CFLScale = 0.5
+    """
+    f = fb.Fluxo(ini)
+    f.DGTimeDerivative(0.0)
+    c = OracleCase(eqn=1, N=4, nElems=(3, 2, 2), xmin=(-1, -1, -1), xmax=(1, 1, 1), NGeo=2, deform_amp=0.1,
+                   ini_exact_func=2, ini_amplitude=0.3, adv_vel=(0.3, -0.2, 0.5), riemann=44, volume_flux=5,
+                   mu0=0.01, cfl_scale=0.5, node_type=1)
+    ref = c.dg_time_derivative(0.0)
+    assert rel_l2(f.Ut, ref) <= 1e-11

@@ -54,6 +54,22 @@ def test_box_mesh_matches_oracle(N, NGeo, ne, amp):
             assert np.abs(m[k] - ref).max() <= 1e-13 * max(1.0, np.abs(ref).max()), k
 
 
+@pytest.mark.parametrize("N,NGeo,ne,amp", [(3, 2, (3, 3, 3), 0.1), (7, 2, (2, 2, 3), 0.05), (4, 3, (2, 3, 2), 0.05),
+                                           (1, 2, (2, 2, 2), 0.05), (2, 1, (4, 2, 3), 0.0)])
+def test_gauss_box_mesh_matches_oracle(N, NGeo, ne, amp):
+    """Gauss nodes: metric terms, Jacobian and side vectors at the Gauss points, and SurfMetrics, against the
+    oracle's restatement of CalcMetrics / CalcSurfMetrics with NodeType 'GAUSS'."""
+    lo, hi = (-np.pi,) * 3, (np.pi,) * 3
+    m = fb.box_mesh(N, ne, lo, hi, NGeo=NGeo, deform_amp=amp, node_type=1)
+    mo = OracleCase(N=N, nElems=ne, xmin=lo, xmax=hi, NGeo=NGeo, deform_amp=amp, node_type=1).mesh()
+    assert "SurfMetrics" in mo
+    for k, ref in mo.items():
+        if ref.dtype.kind == "i":
+            assert np.array_equal(m[k], ref), k
+        else:
+            assert np.abs(m[k] - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max()), k
+
+
 @pytest.mark.parametrize("func", [1, 2, 4, 7])
 def test_exact_func_matches_oracle(func):
     c = OracleCase(N=2, nElems=(2, 2, 2), xmin=(-1, -1, -1), xmax=(1, 1, 1), ini_exact_func=func,
