@@ -140,9 +140,20 @@ __global__ void __launch_bounds__(NP * NP * NP) prolong_kernel(KParams P) {
   }
 }
 
+// the flux area of the lifting kernel: the 12 contravariant fluxes per node, and before them the 15 staged
+// surface products of each of the 6 (N+1)^2 side points
+template <int NP>
+__host__ __device__ constexpr int lift_farea() {
+  return 12 * NP * NP * NP > 90 * NP * NP ? 12 * NP * NP * NP : 90 * NP * NP;
+}
+// gradient rows of the lifting kernel: node n at slot n + n / NP (row stride NP^3 + NP^2), so that the
+// face-trace sums of the side points of a warp spread over the banks
+template <int NP>
+__host__ __device__ constexpr int lift_gstride() { return NP * NP * NP + NP * NP; }
+__device__ __forceinline__ int lift_gslot(int NP, int n) { return n + n / NP; }
 template <int NP>
 __host__ __device__ constexpr size_t lift_smem_bytes() {
-  return sizeof(double) * (size_t)(2 * NP * NP + 2 * NP + 33 * NP * NP * NP);
+  return sizeof(double) * (size_t)(2 * NP * NP + 2 * NP + 6 * NP * NP * NP + 15 * lift_gstride<NP>() + lift_farea<NP>());
 }
 
 // BR1 / BR2 lifting with Gauss nodes (br1.f90:154-364, br1_surfint.f90:100-128, br2_surfint.f90:109-148),
@@ -158,9 +169,10 @@ __global__ void __launch_bounds__(NP * NP * NP) lift_visc_kernel(KParams P) {
   double* sLm = sDhat + NPT;      // L_Minus(l)
   double* sLh = sLm + NP;         // L_HatMinus(l)
   double* sV = sLh + NP;          // [5][node] lifting variable
-  double* sG = sV + 5 * NP3;      // [15][node] gradient of the lifting variable that is prolonged
-  double* sF = sG + 15 * NP3;     // [12][node] contravariant viscous fluxes
-  double* sSJ = sF + 12 * NP3;    // [node] sJ
+  constexpr int GS = lift_gstride<NP>();
+  double* sG = sV + 5 * NP3;      // [15][slot] gradient of the lifting variable that is prolonged
+  double* sF = sG + 15 * GS;      // [12][node] contravariant viscous fluxes (first: staged side products)
+  double* sSJ = sF + lift_farea<NP>();  // [node] sJ
   __shared__ int sE2S[12];
   const int e = blockIdx.x, t = threadIdx.x;
   const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
@@ -169,6 +181,7 @@ __global__ void __launch_bounds__(NP * NP * NP) lift_visc_kernel(KParams P) {
   for (int z = t; z < 12; z += NP3) sE2S[z] = P.e2s[12 * (size_t)e + z];  // NP3 = 8 for N = 1
   double u[5];
   const double sj = P.sJ[(size_t)e * NP3 + t];
+  const int gs = lift_gslot(NP, t);
   {
     const double* Ug = P.U + 5 * ((size_t)e * NP3 + t);
 #pragma unroll
@@ -211,28 +224,41 @@ __global__ void __launch_bounds__(NP * NP * NP) lift_visc_kernel(KParams P) {
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         g[d][v] *= sj;
-        sG[(5 * d + v) * NP3 + t] = g[d][v];
+        sG[(5 * d + v) * GS + gs] = g[d][v];
       }
   }
-  // surface terms: every node of the line of each side takes the lifting flux times L_HatMinus(l)
-#pragma unroll 1
-  for (int s = 1; s <= 6; ++s) {
-    int l, a, b;
-    line_of_node(N, s, i, j, k, l, a, b);
+  // surface terms: every node of the line of each side takes the lifting flux times L_HatMinus(l).  The
+  // 15 products (flux x normal) of each of the element's 6 (N+1)^2 side points are staged once in the
+  // flux area (free until the volume fluxes), [side point][3 x 5]
+  for (int task = t; task < 6 * NPT; task += NP3) {
+    const int s = task / NPT + 1, ab = task - (s - 1) * NPT, a = ab % NP, b = ab / NP;
     const int side = sE2S[2 * (s - 1)], flip = sE2S[2 * (s - 1) + 1];
     const int pt = face_point_of(NP, s, flip, a, b);
     const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
     const double* F = P.lflux + (size_t)side * 5 * NPT + pt;
     const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
-    const double lh = sLh[l];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
       const double f = F[v * NPT];
+      sF[task * 15 + v] = f * n0;
+      sF[task * 15 + 5 + v] = f * n1;
+      sF[task * 15 + 10 + v] = f * n2;
+    }
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int s = 1; s <= 6; ++s) {
+    int l, a, b;
+    line_of_node(N, s, i, j, k, l, a, b);
+    const double* Fn = sF + ((s - 1) * NPT + a + NP * b) * 15;
+    const double lh = sLh[l];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
       if constexpr (LIFT == 2) {
         const double fl = sj * lh;
-        g[0][v] += fl * (f * n0); g[1][v] += fl * (f * n1); g[2][v] += fl * (f * n2);
+        g[0][v] += fl * Fn[v]; g[1][v] += fl * Fn[5 + v]; g[2][v] += fl * Fn[10 + v];
       } else {
-        g[0][v] += (f * n0) * lh; g[1][v] += (f * n1) * lh; g[2][v] += (f * n2) * lh;
+        g[0][v] += Fn[v] * lh; g[1][v] += Fn[5 + v] * lh; g[2][v] += Fn[10 + v] * lh;
       }
     }
   }
@@ -242,7 +268,7 @@ __global__ void __launch_bounds__(NP * NP * NP) lift_visc_kernel(KParams P) {
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         g[d][v] *= sj;
-        sG[(5 * d + v) * NP3 + t] = g[d][v];
+        sG[(5 * d + v) * GS + gs] = g[d][v];
       }
   }
   __syncthreads();
@@ -256,18 +282,18 @@ __global__ void __launch_bounds__(NP * NP * NP) lift_visc_kernel(KParams P) {
     const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
     double tr[3][5];
     {
-      const int nd = line_node_of(NP, s, a, b, 0);
+      const int nd = lift_gslot(NP, line_node_of(NP, s, a, b, 0));
 #pragma unroll
       for (int d = 0; d < 3; ++d)
 #pragma unroll
-        for (int v = 0; v < 5; ++v) tr[d][v] = sG[(5 * d + v) * NP3 + nd] * sLm[0];
+        for (int v = 0; v < 5; ++v) tr[d][v] = sG[(5 * d + v) * GS + nd] * sLm[0];
     }
     for (int l = 1; l < NP; ++l) {
-      const int nd = line_node_of(NP, s, a, b, l);
+      const int nd = lift_gslot(NP, line_node_of(NP, s, a, b, l));
 #pragma unroll
       for (int d = 0; d < 3; ++d)
 #pragma unroll
-        for (int v = 0; v < 5; ++v) tr[d][v] = tr[d][v] + sG[(5 * d + v) * NP3 + nd] * sLm[l];
+        for (int v = 0; v < 5; ++v) tr[d][v] = tr[d][v] + sG[(5 * d + v) * GS + nd] * sLm[l];
     }
     if constexpr (LIFT == 2) {
       const double* F = P.lflux + (size_t)side * 5 * NPT + pt;
@@ -331,14 +357,30 @@ __global__ void __launch_bounds__(NP * NP * NP) lift_visc_kernel(KParams P) {
   for (int v = 0; v < 4; ++v) O[v * NP3] = r[v];
 }
 
-// SurfInt with Gauss nodes and the split-form correction (surfint.f90:118-175, 196-253).  One element per
-// block, one thread per node; per local side every node forms FluxB(l) with the side's state, the line
-// sum FluxB_sum = sum_l FluxB(l) L_Minus(l) (shared memory, l = 0..N), and its share of the side's terms.
+// shared memory of the surface kernel: per side point of the element the side state's record (NQ), the
+// halved SurfMetrics (3) and the surface flux (5); the line buffer [5][node]
+// stride of a side point's data: record (NQ), metric (3), flux (5), made odd so that the records of
+// consecutive side points fall into different banks
+template <int VF>
+__host__ __device__ constexpr int surf_stride() { return (VolRec<VF>::NQ + 8) | 1; }
 template <int NP, int VF>
-__global__ void __launch_bounds__(NP * NP * NP) surf_kernel(KParams P) {
+__host__ __device__ constexpr size_t surf_smem_bytes() {
+  return sizeof(double) * (size_t)(6 * NP * NP * surf_stride<VF>() + 5 * NP * NP * NP);
+}
+
+// SurfInt with Gauss nodes and the split-form correction (surfint.f90:118-175, 196-253).  One element per
+// block, one thread per node.  The records of the side states (their logarithms included), the surface
+// metrics and the surface fluxes of the element's 6 (N+1)^2 side points are formed once in shared memory;
+// then per local side every node forms FluxB(l) with its line's side state, the line sum
+// FluxB_sum = sum_l FluxB(l) L_Minus(l) (shared memory, l = 0..N), and its share of the side's terms.
+template <int NP, int VF>
+__global__ void __launch_bounds__(NP * NP * NP, NP == 8 ? 2 : 1) surf_kernel(KParams P) {
   if (halted(P)) return;
-  constexpr int NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1, RS = VolRec<VF>::RS;
-  __shared__ double sB[5 * NP3];  // [var][node] FluxB(l) L_Minus(l) of the current side
+  constexpr int NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1, RS = VolRec<VF>::RS, NQ = VolRec<VF>::NQ;
+  constexpr int FS = surf_stride<VF>();  // per side point: record, metric (3), flux (5), padding
+  extern __shared__ double smem[];
+  double* sP = smem;               // [6 * NPT][FS]
+  double* sB = sP + 6 * NPT * FS;  // [var][node] FluxB(l) L_Minus(l) of the current side
   __shared__ double sLm[NP], sLh[NP];
   __shared__ int sE2S[12];
   const int e = blockIdx.x, t = threadIdx.x;
@@ -353,33 +395,49 @@ __global__ void __launch_bounds__(NP * NP * NP) surf_kernel(KParams P) {
     for (int v = 0; v < 5; ++v) u[v] = Ug[v];
     make_record<VF>(P, u, rN);
   }
-  const double* M = P.metrics + (size_t)e * 9 * NP3 + t;
+  // pair_flux takes half metrics for every flux but the standard DG one (the metric average is a sum)
+  constexpr double hm = VF == 0 ? 1.0 : 0.5;
+  double m[9];
+  {
+    const double* M = P.metrics + (size_t)e * 9 * NP3 + t;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) m[c] = hm * M[c * NP3];
+  }
+  __syncthreads();
+  for (int task = t; task < 6 * NPT; task += NP3) {
+    const int s = task / NPT + 1, ab = task - (s - 1) * NPT, a = ab % NP, b = ab / NP;
+    const int side = sE2S[2 * (s - 1)], flip = sE2S[2 * (s - 1) + 1], role = flip == 0 ? 0 : 1;
+    const int pt = face_point_of(NP, s, flip, a, b);
+    double* o = sP + task * FS;
+    {
+      const double* uf = uface_at(P, NPT, side, role, pt);
+      double us[5], r[RS];
+#pragma unroll
+      for (int v = 0; v < 5; ++v) us[v] = uf[v];
+      make_record<VF>(P, us, r);
+#pragma unroll
+      for (int z = 0; z < NQ; ++z) o[z] = r[z];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) o[NQ + c] = hm * P.surfMet[(((size_t)e * 6 + (s - 1)) * 3 + c) * NPT + pt];
+    const double* Fs = P.flux + (size_t)side * 5 * NPT + pt;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) o[NQ + 3 + v] = Fs[v * NPT];
+  }
   double ut[5] = {0., 0., 0., 0., 0.};
   __syncthreads();
 #pragma unroll 1
   for (int s = 1; s <= 6; ++s) {
     int l, a, b;
     line_of_node(N, s, i, j, k, l, a, b);
-    const int side = sE2S[2 * (s - 1)], flip = sE2S[2 * (s - 1) + 1], role = flip == 0 ? 0 : 1;
-    const int pt = face_point_of(NP, s, flip, a, b);
+    const int role = sE2S[2 * (s - 1) + 1] == 0 ? 0 : 1;
     const int dir = (s == XI_MINUS || s == XI_PLUS) ? 0 : ((s == ETA_MINUS || s == ETA_PLUS) ? 1 : 2);
     const double sg = (s == ZETA_MINUS || s == ETA_MINUS || s == XI_MINUS) ? -1. : 1.;  // NormalSigns
-    double rF[RS], mN[3], mS[3], FB[5];
-    {
-      const double* uf = uface_at(P, NPT, side, role, pt);
-      double us[5];
+    const double* o = sP + ((s - 1) * NPT + a + NP * b) * FS;
+    double FB[5], mN[3];
 #pragma unroll
-      for (int v = 0; v < 5; ++v) us[v] = uf[v];
-      make_record<VF>(P, us, rF);
-    }
-    // pair_flux takes half metrics for every flux but the standard DG one (the metric average is a sum)
-    constexpr double hm = VF == 0 ? 1.0 : 0.5;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      mN[c] = hm * M[(3 * dir + c) * NP3];
-      mS[c] = hm * P.surfMet[(((size_t)e * 6 + (s - 1)) * 3 + c) * NPT + pt];
-    }
-    pair_flux<VF>(P, rN, rF, mN, mS, FB);
+    for (int c = 0; c < 3; ++c) mN[c] = dir == 0 ? m[c] : (dir == 1 ? m[3 + c] : m[6 + c]);  // registers
+    pair_flux<VF>(P, rN, o, mN, o + NQ, FB);
 #pragma unroll
     for (int v = 0; v < 5; ++v) sB[v * NP3 + t] = FB[v] * sLm[l];
     __syncthreads();
@@ -389,13 +447,13 @@ __global__ void __launch_bounds__(NP * NP * NP) surf_kernel(KParams P) {
 #pragma unroll
       for (int v = 0; v < 5; ++v) sum[v] = sum[v] + sB[v * NP3 + nd];
     }
-    const double* Fs = P.flux + (size_t)side * 5 * NPT + pt;
     const double lh = sLh[l];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
       const double corr = (sum[v] - FB[v]) * sg;
-      if (role == 0) ut[v] = ut[v] + (Fs[v * NPT] - corr) * lh;
-      else ut[v] = ut[v] - (Fs[v * NPT] + corr) * lh;
+      const double f = o[NQ + 3 + v];
+      if (role == 0) ut[v] = ut[v] + (f - corr) * lh;
+      else ut[v] = ut[v] - (f + corr) * lh;
     }
     __syncthreads();  // sB is rewritten by the next side
   }
