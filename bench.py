@@ -309,6 +309,10 @@ def run_fluxo(args):
         from fluxo_b200.workloads import mhd_orszag_tang_state
 
         w = mhd_workload(elems=args.elems or 24, N=args.N or 4)
+        if args.shock_blend > 0:  # fixed blending (ComputeAlpha 3) so that the subcell kernel does work
+            w.update(compute_alpha=3, shock_blend_coef=args.shock_blend)
+        w.update(sub_fv_method=args.sub_fv, recons_boundaries=3 if args.sub_fv > 1 else 1,
+                 nfvse_corr=1 if args.nfvse_corr else 0)
         mesh = fb.box_mesh(w["N"], w["elems"], w["xmin"], w["xmax"], NGeo=w["NGeo"], deform_amp=w["deform_amp"])
         fields = {k: v for k, v in w.items() if k not in ("elems", "xmin", "xmax", "NGeo", "deform_amp")}
         op = fb.DGOperator(device=local, **fields)
@@ -405,10 +409,14 @@ def run_fluxo(args):
     falg_rhs = sum((MHD_FALG_PER_DOF if mhd else FALG_PER_DOF).values())
     if mhd:
         alpha = op.alpha()
-        config = {"workload": "mhd_glm_resistive_orszag_tang_N%d_%dx%dx%d_curved" % ((w["N"],) + w["elems"]),
+        config = {"workload": "mhd_glm_resistive_orszag_tang_N%d_%dx%dx%d_curved" % ((w["N"],) + w["elems"]) +
+                  ("" if args.shock_blend <= 0 else "_blend%g" % args.shock_blend) +
+                  ("" if args.sub_fv == 1 else "_subfv%d" % args.sub_fv) + ("_corr" if args.nfvse_corr else ""),
                   "N": w["N"], "elements": list(w["elems"]), "dofs_per_gpu": nd, "riemann": 14, "volume_flux": 10,
                   "noncons": "powell", "lifting": "br1_entropy_var", "eta": w["eta"],
-                  "nfvse": "indicator, alpha_max 0.5, alpha_min 0.01, 1 sweep",
+                  "nfvse": ("indicator, alpha_max 0.5, alpha_min 0.01, 1 sweep" if args.shock_blend <= 0 else
+                            "fixed alpha %g (ComputeAlpha 3)" % args.shock_blend) +
+                           ", SubFVMethod %d" % args.sub_fv + (", NFVSE_CORR" if args.nfvse_corr else ""),
                   "blended_elements_last_rhs": int((alpha > 0).sum()), "time_disc": "carpenterrk4-5",
                   "rhs_per_step": 5, "parallelism": "replicas x%d" % world,
                   "l2": "inputs larger than L2 (state %d MB)" % (nd * 72 // 10 ** 6), "steps": args.steps}
@@ -828,6 +836,10 @@ def main():
     ap.add_argument("--poll-steps", type=int, default=2, help="serve: time steps between admission rounds")
     ap.add_argument("--elems", type=int, default=0, help="elements per direction (0: the configuration's)")
     ap.add_argument("--N", type=int, default=0, help="polynomial degree (0: the configuration's)")
+    ap.add_argument("--shock-blend", type=float, default=0.0,
+                    help="mhd: fixed blending coefficient (ComputeAlpha 3) instead of the indicator")
+    ap.add_argument("--sub-fv", type=int, default=1, choices=(1, 2, 3, 4), help="mhd: SubFVMethod")
+    ap.add_argument("--nfvse-corr", action="store_true", help="mhd: NFVSE_CORR positivity correction")
     ap.add_argument("--nodes", default="lgl", choices=("lgl", "gauss"),
                     help="tgv: Gauss-Lobatto (the headline) or Gauss nodes (PP_NodeType)")
     ap.add_argument("--no-e2e", action="store_true")

@@ -383,8 +383,14 @@ __host__ __device__ constexpr size_t fv_smem_bytes() {
 //   TVD-Fjordholm: every face first stores the scaled entropy variables w = R^T v of its two nodes (its
 //   own eigenvectors) in shared memory; after a barrier each face reconstructs w at its two sides with
 //   the minmod slopes of the neighbouring faces and dissipates the jump of the reconstructed values.
+// resident blocks per SM the register allocation must allow: the MHD kernels hold the 9-variable states
+// and the ES solver's mean state; 3 blocks of (N+1)^3 <= 128 threads keep 12 warps per SM at a few
+// spilled doubles instead of 8 warps at 228+ registers
+template <int NP, bool MHD>
+__host__ __device__ constexpr int fv_minb() { return (MHD && NP * NP * NP <= 128) ? 3 : 1; }
+
 template <int NP, int RS, bool MHD, int ES>
-__global__ void __launch_bounds__(NP * NP * NP) fv_kernel(KParams P) {
+__global__ void __launch_bounds__(NP * NP * NP, fv_minb<NP, MHD>()) fv_kernel(KParams P) {
   if (halted(P)) return;
   constexpr int NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1, NV = MHD ? 9 : 5;
   static_assert(ES == 0 || has_dissip_matrices<MHD, RS>(), "SubFVMethod 3/4 need dissipation matrices");

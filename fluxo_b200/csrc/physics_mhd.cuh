@@ -260,13 +260,23 @@ __device__ __forceinline__ void es_llf(const KParams& P, double ch, const double
   F[8] = F[8] - (LM * tau) * (psiA * Vj[4] + Vj[8]);
 }
 
-// Flux and dissipation matrices of the entropy-stable 9-wave solvers (Riemann 14 Derigs, 15 FloGor):
+// The mean state of the entropy-stable 9-wave solvers (Riemann 14 Derigs, 15 FloGor;
 // EntropyStableDerigsFlux_VolFluxAndDissipMatrices mhd/riemann.f90:1287-1622 and the FloGor variant
-// :1695-2042: EC flux F, diagonal D (with the entropy scaling T) and right eigenvectors, R[c] = column c
+// :1695-2042): the scalars of the right eigenvectors and the diagonal D (with the entropy scaling T).
+// The eigenvector matrix is never stored: wave9_column forms column c (mhd/riemann.f90:1497-1586) from
+// these scalars where it is used, which keeps the solver's live registers to a few dozen doubles.
+struct Wave9 {
+  double rhoLN, sqRho, sqRhoA, alf, als, cf, cs, be2, be3, sg, abeta, u2A, psiA, BA0;
+  double uA[3];
+  double psiSp, psiSm, psiFp, psiFm;
+  double D[9];
+};
+
+// central flux F and the mean state W (the jump of the entropy variables in Vj)
 template <bool FLOGOR>
-__device__ __forceinline__ void es_9wave_matrices(const KParams& P, double ch, const double* UL, const double* UR,
-                                                  double* F, double* Dm, double (*R)[9]) {
-  double Vj[9], pL, pR, bL, bR;
+__device__ __forceinline__ void wave9_setup(const KParams& P, double ch, const double* UL, const double* UR,
+                                            double* F, double* Vj, Wave9& W) {
+  double pL, pR, bL, bR;
   entropy_jump(P, UL, UR, pL, pR, bL, bR, Vj);
   const double sL = 1. / UL[0], sR = 1. / UR[0];
   double uL[3], uR[3];
@@ -338,25 +348,11 @@ __device__ __forceinline__ void es_9wave_matrices(const KParams& P, double ch, c
                        alf * cf * rhoLN * uA[0] - als * cs * rhoLN * sg * t23;
   const double psiFm = 0.5 * alf * rhoLN * u2A + abeta * als * rhoLN * bperp + alf * rhoLN * aLN * aLN * P.sKappaM1 -
                        alf * cf * rhoLN * uA[0] + als * cs * rhoLN * sg * t23;
-  // columns of R (mhd/riemann.f90:1497-1586)
-  const double Rc[9][9] = {
-      {alf * rhoLN, alf * rhoLN * (uA[0] + cf), rhoLN * (alf * uA[1] - als * cs * be2 * sg),
-       rhoLN * (alf * uA[2] - als * cs * be3 * sg), psiFp, 0.0, als * abeta * be2 * sqRho, als * abeta * be3 * sqRho, 0.0},
-      {0.0, 0.0, rhoLN * sqRhoA * be3, -rhoLN * sqRhoA * be2, -rhoLN * sqRhoA * (be2 * uA[2] - be3 * uA[1]), 0.0,
-       -rhoLN * be3, rhoLN * be2, 0.0},
-      {als * rhoLN, als * rhoLN * (uA[0] + cs), rhoLN * (als * uA[1] + alf * cf * be2 * sg),
-       rhoLN * (als * uA[2] + alf * cf * be3 * sg), psiSp, 0.0, -alf * abeta * be2 * sqRho, -alf * abeta * be3 * sqRho,
-       0.0},
-      {0.0, 0.0, 0.0, 0.0, BA[0] + psiA, 1.0, 0.0, 0.0, 1.0},
-      {1.0, uA[0], uA[1], uA[2], 0.5 * u2A, 0.0, 0.0, 0.0, 0.0},
-      {0.0, 0.0, 0.0, 0.0, BA[0] - psiA, 1.0, 0.0, 0.0, -1.0},
-      {als * rhoLN, als * rhoLN * (uA[0] - cs), rhoLN * (als * uA[1] - alf * cf * be2 * sg),
-       rhoLN * (als * uA[2] - alf * cf * be3 * sg), psiSm, 0.0, -alf * abeta * be2 * sqRho, -alf * abeta * be3 * sqRho,
-       0.0},
-      {0.0, 0.0, -rhoLN * sqRhoA * be3, rhoLN * sqRhoA * be2, rhoLN * sqRhoA * (be2 * uA[2] - be3 * uA[1]), 0.0,
-       -rhoLN * be3, rhoLN * be2, 0.0},
-      {alf * rhoLN, alf * rhoLN * (uA[0] - cf), rhoLN * (alf * uA[1] + als * cs * be2 * sg),
-       rhoLN * (alf * uA[2] + als * cs * be3 * sg), psiFm, 0.0, als * abeta * be2 * sqRho, als * abeta * be3 * sqRho, 0.0}};
+  W.rhoLN = rhoLN; W.sqRho = sqRho; W.sqRhoA = sqRhoA; W.alf = alf; W.als = als; W.cf = cf; W.cs = cs;
+  W.be2 = be2; W.be3 = be3; W.sg = sg; W.abeta = abeta; W.u2A = u2A; W.psiA = psiA; W.BA0 = BA[0];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) W.uA[d] = uA[d];
+  W.psiSp = psiSp; W.psiSm = psiSm; W.psiFp = psiFp; W.psiFm = psiFm;
   const double ratio = pR * UR[0] / (pL * UL[0]);
   const double phi = sqrt(fabs(1.0 - ratio) / (1.0 + ratio));
   const double LM = fmax(fabs(uA[0] + cf), fabs(uA[0] - cf));
@@ -366,36 +362,115 @@ __device__ __forceinline__ void es_9wave_matrices(const KParams& P, double ch, c
                T5 = rhoLN * P.kappaM1 / P.kappa;
   const double Tm[9] = {T1, T2, T1, T4, T5, T4, T1, T2, T1};
 #pragma unroll
-  for (int c = 0; c < 9; ++c) {
-    Dm[c] = ((1. - phi) * fabs(wave[c]) + phi * LM) * Tm[c];
-#pragma unroll
-    for (int r = 0; r < 9; ++r) R[c][r] = Rc[c][r];
+  for (int c = 0; c < 9; ++c) W.D[c] = ((1. - phi) * fabs(wave[c]) + phi * LM) * Tm[c];
+}
+
+// column c of the right eigenvectors (c = 0..8 resolved at compile time under unrolled loops)
+__device__ __forceinline__ void wave9_column(const Wave9& W, int c, double* col) {
+  const double rhoLN = W.rhoLN, alf = W.alf, als = W.als, cf = W.cf, cs = W.cs, be2 = W.be2, be3 = W.be3,
+               sg = W.sg, abeta = W.abeta, sqRho = W.sqRho, sqRhoA = W.sqRhoA;
+  const double* uA = W.uA;
+  switch (c) {
+    case 0: {
+      const double v[9] = {alf * rhoLN, alf * rhoLN * (uA[0] + cf), rhoLN * (alf * uA[1] - als * cs * be2 * sg),
+                           rhoLN * (alf * uA[2] - als * cs * be3 * sg), W.psiFp, 0.0, als * abeta * be2 * sqRho,
+                           als * abeta * be3 * sqRho, 0.0};
+      for (int r = 0; r < 9; ++r) col[r] = v[r];
+      return;
+    }
+    case 1: {
+      const double v[9] = {0.0, 0.0, rhoLN * sqRhoA * be3, -rhoLN * sqRhoA * be2,
+                           -rhoLN * sqRhoA * (be2 * uA[2] - be3 * uA[1]), 0.0, -rhoLN * be3, rhoLN * be2, 0.0};
+      for (int r = 0; r < 9; ++r) col[r] = v[r];
+      return;
+    }
+    case 2: {
+      const double v[9] = {als * rhoLN, als * rhoLN * (uA[0] + cs), rhoLN * (als * uA[1] + alf * cf * be2 * sg),
+                           rhoLN * (als * uA[2] + alf * cf * be3 * sg), W.psiSp, 0.0, -alf * abeta * be2 * sqRho,
+                           -alf * abeta * be3 * sqRho, 0.0};
+      for (int r = 0; r < 9; ++r) col[r] = v[r];
+      return;
+    }
+    case 3: {
+      const double v[9] = {0.0, 0.0, 0.0, 0.0, W.BA0 + W.psiA, 1.0, 0.0, 0.0, 1.0};
+      for (int r = 0; r < 9; ++r) col[r] = v[r];
+      return;
+    }
+    case 4: {
+      const double v[9] = {1.0, uA[0], uA[1], uA[2], 0.5 * W.u2A, 0.0, 0.0, 0.0, 0.0};
+      for (int r = 0; r < 9; ++r) col[r] = v[r];
+      return;
+    }
+    case 5: {
+      const double v[9] = {0.0, 0.0, 0.0, 0.0, W.BA0 - W.psiA, 1.0, 0.0, 0.0, -1.0};
+      for (int r = 0; r < 9; ++r) col[r] = v[r];
+      return;
+    }
+    case 6: {
+      const double v[9] = {als * rhoLN, als * rhoLN * (uA[0] - cs), rhoLN * (als * uA[1] - alf * cf * be2 * sg),
+                           rhoLN * (als * uA[2] - alf * cf * be3 * sg), W.psiSm, 0.0, -alf * abeta * be2 * sqRho,
+                           -alf * abeta * be3 * sqRho, 0.0};
+      for (int r = 0; r < 9; ++r) col[r] = v[r];
+      return;
+    }
+    case 7: {
+      const double v[9] = {0.0, 0.0, -rhoLN * sqRhoA * be3, rhoLN * sqRhoA * be2,
+                           rhoLN * sqRhoA * (be2 * uA[2] - be3 * uA[1]), 0.0, -rhoLN * be3, rhoLN * be2, 0.0};
+      for (int r = 0; r < 9; ++r) col[r] = v[r];
+      return;
+    }
+    default: {
+      const double v[9] = {alf * rhoLN, alf * rhoLN * (uA[0] - cf), rhoLN * (alf * uA[1] + als * cs * be2 * sg),
+                           rhoLN * (alf * uA[2] + als * cs * be3 * sg), W.psiFm, 0.0, als * abeta * be2 * sqRho,
+                           als * abeta * be3 * sqRho, 0.0};
+      for (int r = 0; r < 9; ++r) col[r] = v[r];
+      return;
+    }
   }
 }
+
+// Flux and dissipation matrices (R[c] = column c) for the subcell schemes that need them explicitly
+template <bool FLOGOR>
+__device__ __forceinline__ void es_9wave_matrices(const KParams& P, double ch, const double* UL, const double* UR,
+                                                  double* F, double* Dm, double (*R)[9]) {
+  double Vj[9];
+  Wave9 W;
+  wave9_setup<FLOGOR>(P, ch, UL, UR, F, Vj, W);
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    Dm[c] = W.D[c];
+    wave9_column(W, c, R[c]);
+  }
+}
+
 
 // EntropyStableDerigsFlux / EntropyStableFloGorFlux (mhd/riemann.f90:1224-1283, :1633-1691):
 // F - 1/2 R D R^T [v]
 template <bool FLOGOR>
 __device__ __forceinline__ void es_9wave(const KParams& P, double ch, const double* UL, const double* UR, double* F) {
-  double Vj[9], pL, pR, bL, bR;
-  entropy_jump(P, UL, UR, pL, pR, bL, bR, Vj);
-  double Dm[9], R[9][9];  // R[c] is column c
-  es_9wave_matrices<FLOGOR>(P, ch, UL, UR, F, Dm, R);
+  double Vj[9];
+  Wave9 W;
+  wave9_setup<FLOGOR>(P, ch, UL, UR, F, Vj, W);
   double w[9];
 #pragma unroll
-  for (int c = 0; c < 9; ++c) {  // D * (R^T [v])
+  for (int c = 0; c < 9; ++c) {  // D * (R^T [v]), column by column
+    double col[9];
+    wave9_column(W, c, col);
     double s = 0.;
 #pragma unroll
-    for (int r = 0; r < 9; ++r) s += R[c][r] * Vj[r];
-    w[c] = Dm[c] * s;
+    for (int r = 0; r < 9; ++r) s += col[r] * Vj[r];
+    w[c] = W.D[c] * s;
+  }
+  double acc[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};  // R (D R^T [v]): row sums in column order
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    double col[9];
+    wave9_column(W, c, col);
+#pragma unroll
+    for (int r = 0; r < 9; ++r) acc[r] += col[r] * w[c];
   }
 #pragma unroll
-  for (int r = 0; r < 9; ++r) {
-    double s = 0.;
-#pragma unroll
-    for (int c = 0; c < 9; ++c) s += R[c][r] * w[c];
-    F[r] = F[r] - 0.5 * s;
-  }
+  for (int r = 0; r < 9; ++r) F[r] = F[r] - 0.5 * acc[r];
 }
 
 
