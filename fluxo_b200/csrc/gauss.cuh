@@ -90,8 +90,9 @@ __device__ __forceinline__ double* uface_at(const KParams& P, int NPT, int side,
 template <int NP, bool ENT>
 __global__ void __launch_bounds__(NP * NP * NP) prolong_kernel(KParams P) {
   if (halted(P)) return;
-  constexpr int NP3 = NP * NP * NP, NPT = NP * NP;
-  __shared__ double sX[5 * NP3];  // [var][node]
+  constexpr int NP3 = NP * NP * NP, NPT = NP * NP, XS = NP3 + NPT;
+  __shared__ double sX[5 * XS];  // [var][slot], node n at slot n + n / NP (the lines of a warp's side
+                                 // points spread over the banks)
   __shared__ double sL[NP];
   __shared__ int sE2S[12];
   const int e = blockIdx.x, t = threadIdx.x;
@@ -109,7 +110,7 @@ __global__ void __launch_bounds__(NP * NP * NP) prolong_kernel(KParams P) {
       for (int v = 0; v < 5; ++v) x[v] = u[v];
     }
 #pragma unroll
-    for (int v = 0; v < 5; ++v) sX[v * NP3 + t] = x[v];
+    for (int v = 0; v < 5; ++v) sX[v * XS + t + t / NP] = x[v];
   }
   __syncthreads();
   for (int task = t; task < 6 * NPT; task += NP3) {
@@ -119,13 +120,13 @@ __global__ void __launch_bounds__(NP * NP * NP) prolong_kernel(KParams P) {
     {
       const int n0 = line_node_of(NP, s, a, b, 0);
 #pragma unroll
-      for (int v = 0; v < 5; ++v) acc[v] = sX[v * NP3 + n0] * sL[0];
+      for (int v = 0; v < 5; ++v) acc[v] = sX[v * XS + n0 + n0 / NP] * sL[0];
     }
 #pragma unroll
     for (int l = 1; l < NP; ++l) {
       const int n = line_node_of(NP, s, a, b, l);
 #pragma unroll
-      for (int v = 0; v < 5; ++v) acc[v] = acc[v] + sX[v * NP3 + n] * sL[l];
+      for (int v = 0; v < 5; ++v) acc[v] = acc[v] + sX[v * XS + n + n / NP] * sL[l];
     }
     double c[5];
     if constexpr (ENT) {
