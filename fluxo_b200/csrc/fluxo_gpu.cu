@@ -200,6 +200,15 @@ struct fluxo_handle {
 
 namespace {
 
+// SplitMix64 (Steele, Lea, Flood 2014): the next uniform double in [0,1) of the stream `state`
+double splitmix64_unit(uint64_t& state) {
+  uint64_t z = (state += 0x9e3779b97f4a7c15ULL);
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  z ^= z >> 31;
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
 std::mutex g_err_mutex;
 std::string g_create_error;
 
@@ -573,8 +582,8 @@ int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {
   }
   if (cfg->nfvse) {  // InitShockCapturing / InitNFVSE checks (shockcapturing.f90:82-112, nfvse.f90:120-170)
     if (cfg->N < 2) return fail(nullptr, FLUXO_EINVAL_CFG, "NFVSE needs N >= 2");
-    if (cfg->compute_alpha != 1 && cfg->compute_alpha != 3)
-      return fail(nullptr, FLUXO_EINVAL_CFG, "ComputeAlpha must be 1 (indicator) or 3 (fixed)");
+    if (cfg->compute_alpha != 1 && cfg->compute_alpha != 3 && cfg->compute_alpha != 20)
+      return fail(nullptr, FLUXO_EINVAL_CFG, "ComputeAlpha must be 1 (indicator), 3 (fixed) or 20 (random, kept)");
     if (cfg->indicator_quantity < 1 || cfg->indicator_quantity > 4)
       return fail(nullptr, FLUXO_EINVAL_CFG, "ShockIndicatorQuantity must be 1..4");
     if (cfg->space_prop_sweeps < 0) return fail(nullptr, FLUXO_EINVAL_CFG, "SpacePropSweeps must be >= 0");
@@ -715,7 +724,17 @@ int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* S2E, 
         (r = dalloc(h, &h->dAlphaTmp, (size_t)nElems)) || (r = dalloc(h, &h->dBlendList, (size_t)nElems)) ||
         (r = dalloc(h, &h->dFV, nU)) || (h->cfg.nfvse_corr && (r = dalloc(h, &h->dFFV, nU))))
       return r;
-    FLUXO_CUDA(h, cudaMemsetAsync(h->dAlpha, 0, (size_t)nElems * sizeof(double), h->stream));
+    if (h->cfg.compute_alpha == 20) {
+      // ComputeAlpha 20 (nfvse.f90:1591-1596): alpha = RANDOM_NUMBER * alpha_max once, then kept.  The
+      // reference's stream is compiler-specific; this one is SplitMix64 from state 0, one draw per
+      // element in element order (fluxo_gpu_set_alpha replaces it).
+      std::vector<double> a((size_t)nElems);
+      uint64_t state = 0;
+      for (int e = 0; e < nElems; ++e) a[e] = splitmix64_unit(state) * h->cfg.alpha_max;
+      FLUXO_CUDA(h, cudaMemcpy(h->dAlpha, a.data(), a.size() * sizeof(double), cudaMemcpyHostToDevice));
+    } else {
+      FLUXO_CUDA(h, cudaMemsetAsync(h->dAlpha, 0, (size_t)nElems * sizeof(double), h->stream));
+    }
     if (h->cfg.nfvse_corr) FLUXO_CUDA(h, cudaMemsetAsync(h->dFFV, 0, nU * sizeof(double), h->stream));
   }
   cudaStream_t s = h->stream;
@@ -986,6 +1005,16 @@ int fluxo_gpu_get_glm_ch(fluxo_handle* h, double* ch) {
   if (!h || !ch) return FLUXO_EINVAL_CFG;
   if (!h->mhd) return fail(h, FLUXO_EINVAL_CFG, "GLM_ch exists for MHD only");
   *ch = h->glmCh;
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_set_alpha(fluxo_handle* h, const double* alpha) {
+  int r = check_ready(h);
+  if (r) return r;
+  if (!alpha) return FLUXO_EINVAL_CFG;
+  if (!h->cfg.nfvse) return fail(h, FLUXO_EINVAL_CFG, "NFVSE is off");
+  FLUXO_CUDA(h, cudaMemcpyAsync(h->dAlpha, alpha, (size_t)h->nElems * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
   return FLUXO_OK;
 }
 

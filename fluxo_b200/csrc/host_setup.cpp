@@ -14,6 +14,9 @@
 #include "host_setup.h"
 
 namespace fluxo {
+// fluxo_gpu.cu: the message that fluxo_gpu_last_error(NULL, ...) returns (returns `code`)
+int record_unbound_error(int code, const std::string& msg);
+
 namespace host {
 
 // Side <-> volume index maps with the reference's conventions (src/mesh/mappings.f90:262-464):
@@ -151,31 +154,17 @@ void box_connectivity(const int* ne, int N, std::vector<int>& S2E, std::vector<i
   if (next != nSides) throw std::runtime_error("box_connectivity: side count");
 }
 
-void box_geometry(int N, const int* ne, const double* xmin, const double* xmax, int NGeo, double amp,
-                  const std::vector<int>& E2S, double* Mf, double* Mg, double* Mh, double* sJ, double* NormVec,
-                  double* TangVec1, double* TangVec2, double* SurfElem, double* Elem_xGP) {
-  const int nx = ne[0], ny = ne[1], nz = ne[2], nElems = nx * ny * nz;
-  const int n = N + 1, ng = NGeo + 1, NR = 3 * NGeo, nr = NR + 1;
-  const size_t nv = (size_t)n * n * n;
-  LGLBasis bN(N);
-  std::vector<double> xeq(ng), xg, wg, xr, wr;
-  for (int i = 0; i < ng; ++i) xeq[i] = NGeo > 0 ? 2. * i / NGeo - 1. : 0.;
-  lgl(NGeo, xg, wg);
-  lgl(NR, xr, wr);
-  const std::vector<double> V_eq_g = interp_matrix(xeq, xg);
-  const std::vector<double> V_g_N = interp_matrix(xg, bN.x);
-  const std::vector<double> V_g_r = interp_matrix(xg, xr);
-  std::vector<double> V_r_N;
-  if (NR > N) V_r_N = modal_projection(xr, bN.x);
-  else V_r_N = interp_matrix(xr, bN.x);
-  const std::vector<double> Dg = deriv_matrix(xg);
+// Node coordinates NodeCoords(3,0:NGeo,0:NGeo,0:NGeo,nElems) of the periodic box on equidistant points,
+// deformed by X_d += amp * prod_e sin(2 pi (x_e - c_e) / L_e) (which keeps the box periodic).
+std::vector<double> box_nodes(const int* ne, const double* xmin, const double* xmax, int NGeo, double amp) {
+  const int nx = ne[0], ny = ne[1], nz = ne[2], nElems = nx * ny * nz, ng = NGeo + 1;
   const double L[3] = {xmax[0] - xmin[0], xmax[1] - xmin[1], xmax[2] - xmin[2]};
   const double c[3] = {0.5 * (xmax[0] + xmin[0]), 0.5 * (xmax[1] + xmin[1]), 0.5 * (xmax[2] + xmin[2])};
   const double h[3] = {L[0] / nx, L[1] / ny, L[2] / nz};
-#pragma omp parallel for schedule(dynamic, 16)
+  std::vector<double> X((size_t)3 * ng * ng * ng * nElems);
   for (int e = 0; e < nElems; ++e) {
     const int ix = e % nx, iy = (e / nx) % ny, iz = e / (nx * ny);
-    std::vector<double> Xeq(3 * ng * ng * ng), Xg(3 * ng * ng * ng), XN(3 * nv), dXg(9 * ng * ng * ng), tmp(3 * ng * ng * ng);
+    double* Xe = &X[(size_t)3 * ng * ng * ng * e];
     for (int k = 0; k < ng; ++k)
       for (int j = 0; j < ng; ++j)
         for (int i = 0; i < ng; ++i) {
@@ -184,9 +173,35 @@ void box_geometry(int N, const int* ne, const double* xmin, const double* xmax, 
           double f = amp;
           if (f != 0.)
             for (int d = 0; d < 3; ++d) f *= std::sin(2. * M_PI * (xs[d] - c[d]) / L[d]);
-          for (int d = 0; d < 3; ++d) Xeq[3 * (i + ng * (j + ng * k)) + d] = xs[d] + f;
+          for (int d = 0; d < 3; ++d) Xe[3 * (i + ng * (j + ng * k)) + d] = xs[d] + f;
         }
-    tp_interp(3, ng, ng, V_eq_g, Xeq.data(), Xg.data());
+  }
+  return X;
+}
+
+// LGL nodes (CalcMetrics / CalcSurfMetrics, metrics.f90:78-440) from node coordinates of degree NGeo on
+// equidistant (nodesGL false) or Gauss-Lobatto points.
+void nodes_geometry(int N, int nElems, int NGeo, bool nodesGL, const double* NodeCoords, const std::vector<int>& E2S,
+                    double* Mf, double* Mg, double* Mh, double* sJ, double* NormVec, double* TangVec1,
+                    double* TangVec2, double* SurfElem, double* Elem_xGP) {
+  const int n = N + 1, ng = NGeo + 1, NR = 3 * NGeo, nr = NR + 1;
+  const size_t nv = (size_t)n * n * n;
+  LGLBasis bN(N);
+  std::vector<double> xeq(ng), xg, wg, xr, wr;
+  lgl(NGeo, xg, wg);
+  for (int i = 0; i < ng; ++i) xeq[i] = nodesGL ? xg[i] : 2. * i / NGeo - 1.;
+  lgl(NR, xr, wr);
+  const std::vector<double> V_eq_g = interp_matrix(xeq, xg);
+  const std::vector<double> V_g_N = interp_matrix(xg, bN.x);
+  const std::vector<double> V_g_r = interp_matrix(xg, xr);
+  std::vector<double> V_r_N;
+  if (NR > N) V_r_N = modal_projection(xr, bN.x);
+  else V_r_N = interp_matrix(xr, bN.x);
+  const std::vector<double> Dg = deriv_matrix(xg);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int e = 0; e < nElems; ++e) {
+    std::vector<double> Xg(3 * ng * ng * ng), XN(3 * nv), dXg(9 * ng * ng * ng), tmp(3 * ng * ng * ng);
+    tp_interp(3, ng, ng, V_eq_g, NodeCoords + (size_t)3 * ng * ng * ng * e, Xg.data());
     tp_interp(3, ng, n, V_g_N, Xg.data(), XN.data());
     std::copy(XN.begin(), XN.end(), Elem_xGP + 3 * nv * e);
     // dXg[dir][node][coord]: derivative of the coordinates along reference direction dir (NGeo nodes)
@@ -281,16 +296,16 @@ void box_geometry(int N, const int* ne, const double* xmin, const double* xmax, 
 // interpolated to the Gauss nodes (Vdm_GLN_N); the Jacobian through 3*NGeo Gauss points, projected to N;
 // the side quantities from the Gauss-Lobatto metric terms of the side interpolated to the side's Gauss
 // points, SurfMetrics (the normal metric term) for every side in the master's point order.
-void box_geometry_gauss(int N, const int* ne, const double* xmin, const double* xmax, int NGeo, double amp,
-                        const std::vector<int>& E2S, double* Mf, double* Mg, double* Mh, double* sJ, double* NormVec,
-                        double* TangVec1, double* TangVec2, double* SurfElem, double* Elem_xGP, double* SurfMetrics) {
-  const int nx = ne[0], ny = ne[1], nz = ne[2], nElems = nx * ny * nz;
+void nodes_geometry_gauss(int N, int nElems, int NGeo, bool nodesGL, const double* NodeCoords,
+                          const std::vector<int>& E2S, double* Mf, double* Mg, double* Mh, double* sJ,
+                          double* NormVec, double* TangVec1, double* TangVec2, double* SurfElem, double* Elem_xGP,
+                          double* SurfMetrics) {
   const int n = N + 1, ng = NGeo + 1, NR = 3 * NGeo, nr = NR + 1;
   const size_t nv = (size_t)n * n * n;
   GaussBasis bG(N);
   std::vector<double> xeq(ng), xg, wg, xr, wr, xGL, wGL;
-  for (int i = 0; i < ng; ++i) xeq[i] = NGeo > 0 ? 2. * i / NGeo - 1. : 0.;
   lgl(NGeo, xg, wg);
+  for (int i = 0; i < ng; ++i) xeq[i] = nodesGL ? xg[i] : 2. * i / NGeo - 1.;
   gauss(NR, xr, wr);
   lgl(N, xGL, wGL);
   const std::vector<double> V_eq_g = interp_matrix(xeq, xg);
@@ -301,25 +316,10 @@ void box_geometry_gauss(int N, const int* ne, const double* xmin, const double* 
   if (NR > N) V_r_N = modal_projection(xr, bG.x);
   else if (NR < N) V_r_N = interp_matrix(xr, bG.x);
   const std::vector<double> Dg = deriv_matrix(xg), DGL = deriv_matrix(xGL);
-  const double L[3] = {xmax[0] - xmin[0], xmax[1] - xmin[1], xmax[2] - xmin[2]};
-  const double c[3] = {0.5 * (xmax[0] + xmin[0]), 0.5 * (xmax[1] + xmin[1]), 0.5 * (xmax[2] + xmin[2])};
-  const double h[3] = {L[0] / nx, L[1] / ny, L[2] / nz};
 #pragma omp parallel for schedule(dynamic, 16)
   for (int e = 0; e < nElems; ++e) {
-    const int ix = e % nx, iy = (e / nx) % ny, iz = e / (nx * ny);
-    std::vector<double> Xeq(3 * ng * ng * ng), Xg(3 * ng * ng * ng), XGL(3 * nv), dXg(9 * ng * ng * ng),
-        tmp(3 * ng * ng * ng);
-    for (int k = 0; k < ng; ++k)
-      for (int j = 0; j < ng; ++j)
-        for (int i = 0; i < ng; ++i) {
-          const double xs[3] = {xmin[0] + h[0] * (ix + (double)i / NGeo), xmin[1] + h[1] * (iy + (double)j / NGeo),
-                                xmin[2] + h[2] * (iz + (double)k / NGeo)};
-          double f = amp;
-          if (f != 0.)
-            for (int d = 0; d < 3; ++d) f *= std::sin(2. * M_PI * (xs[d] - c[d]) / L[d]);
-          for (int d = 0; d < 3; ++d) Xeq[3 * (i + ng * (j + ng * k)) + d] = xs[d] + f;
-        }
-    tp_interp(3, ng, ng, V_eq_g, Xeq.data(), Xg.data());
+    std::vector<double> Xg(3 * ng * ng * ng), XGL(3 * nv), dXg(9 * ng * ng * ng), tmp(3 * ng * ng * ng);
+    tp_interp(3, ng, ng, V_eq_g, NodeCoords + (size_t)3 * ng * ng * ng * e, Xg.data());
     tp_interp(3, ng, n, V_g_GL, Xg.data(), XGL.data());
     tp_interp(3, n, n, V_GL_N, XGL.data(), Elem_xGP + 3 * nv * e);
     for (int dir = 0; dir < 3; ++dir) {
@@ -435,6 +435,73 @@ void box_geometry_gauss(int N, const int* ne, const double* xmin, const double* 
   }
 }
 
+// Connectivity of a HOPR mesh from the arrays of its file (ReadMesh, mesh_readin.f90:295-445;
+// setLocalSideIDs, prepare_mesh.f90:59-215; fillMeshInfo, prepare_mesh.f90:662-710), for one process.
+// ElemInfo(6,nElems): ELEM_FirstSideInd (row 3) is the 0-based offset of the element's six SideInfo
+// records.  SideInfo(5,nSideInfo): SIDE_Type, SIDE_ID (> 0: the oriented side, flip 0; < 0: flip
+// MOD(SIDE_Flip,10)), SIDE_nbElemID, SIDE_Flip, SIDE_BCID.  BCType(4,nBCs): BC_TYPE 1 (periodic) and
+// 100 keep their connection.  Both records of a unique side are paired through |SIDE_ID|; side ids
+// are handed out in element / local-side order as the reference does when every side is an inner
+// side.  Mortar sides and sides of non-periodic boundaries are refused (the product's face kernels
+// hold inner sides only).
+bool hopr_connectivity(int nElems, const int* ElemInfo, int nSideInfo, const int* SideInfo, int nBCs,
+                       const int* BCType, std::vector<int>& S2E, std::vector<int>& E2S, std::string& err) {
+  const size_t nRec = 6 * (size_t)nElems;
+  std::vector<int> uid(nRec), flip(nRec), nb(nRec);
+  int maxUid = 0;
+  for (int e = 0; e < nElems; ++e) {
+    const int first = ElemInfo[6 * (size_t)e + 2];
+    for (int ls = 0; ls < 6; ++ls) {
+      const long row = (long)first + ls;
+      if (row < 0 || row >= nSideInfo) { err = "ElemInfo: side offset out of range"; return false; }
+      const int* r = SideInfo + 5 * row;
+      if (r[0] < 0 || r[2] < 0) { err = "mortar sides are not supported"; return false; }
+      if (r[4] != 0) {
+        if (r[4] < 1 || r[4] > nBCs) { err = "SideInfo: BC index out of range"; return false; }
+        const int type = BCType[4 * (size_t)(r[4] - 1)];
+        if (type != 1 && type != 100) { err = "non-periodic boundary sides are not supported"; return false; }
+      }
+      if (r[2] == 0) { err = "boundary sides are not supported"; return false; }
+      if (r[2] > nElems) { err = "SideInfo: neighbour element out of range"; return false; }
+      const size_t a = 6 * (size_t)e + ls;
+      uid[a] = r[1] > 0 ? r[1] : -r[1];
+      flip[a] = r[1] > 0 ? 0 : r[3] % 10;
+      if (uid[a] == 0 || flip[a] < 0 || flip[a] > 4) { err = "SideInfo: invalid side id or flip"; return false; }
+      nb[a] = r[2] - 1;
+      maxUid = std::max(maxUid, uid[a]);
+    }
+  }
+  // pair the two records of every unique side
+  std::vector<long> firstRec((size_t)maxUid + 1, -1), partner(nRec, -1);
+  for (size_t a = 0; a < nRec; ++a) {
+    long& f = firstRec[uid[a]];
+    if (f < 0) { f = (long)a; continue; }
+    if (f == -2 || partner[f] >= 0) { err = "a unique side with more than two element sides"; return false; }
+    partner[f] = (long)a;
+    partner[a] = f;
+  }
+  for (size_t a = 0; a < nRec; ++a) {
+    if (partner[a] < 0) { err = "a side without a neighbour"; return false; }
+    if (nb[a] != (int)(partner[a] / 6)) { err = "SideInfo: neighbour element does not hold the side"; return false; }
+    if ((flip[a] == 0) == (flip[partner[a]] == 0)) { err = "a side needs one oriented (flip 0) element side"; return false; }
+  }
+  const int nSides = (int)(nRec / 2);
+  S2E.assign((size_t)5 * nSides, -1);
+  E2S.assign((size_t)2 * nRec, 0);
+  std::vector<int> sid(nRec, 0);
+  int next = 0;
+  for (size_t a = 0; a < nRec; ++a) {
+    if (!sid[a]) sid[a] = sid[partner[a]] = ++next;
+    const int e = (int)(a / 6), ls = (int)(a % 6) + 1;
+    E2S[2 * a] = sid[a];
+    E2S[2 * a + 1] = flip[a];
+    int* se = &S2E[(size_t)5 * (sid[a] - 1)];
+    if (flip[a] == 0) { se[0] = e + 1; se[2] = ls; }
+    else { se[1] = e + 1; se[3] = ls; se[4] = flip[a]; }
+  }
+  return true;
+}
+
 bool repack_mesh(int N, int nElems, int nSides, const int* S2E, const int* E2S, const double* Mf, const double* Mg,
                  const double* Mh, const double* NormVec, const double* TangVec1, const double* TangVec2,
                  const double* SurfElem, std::vector<int>& s2e, std::vector<int>& e2s, std::vector<double>& met,
@@ -507,7 +574,9 @@ extern "C" int fluxo_host_box_mesh(int N, const int* ne, const double* xmin, con
     box_connectivity(ne, N, S2E, E2S);
     std::copy(S2E.begin(), S2E.end(), SideToElem);
     std::copy(E2S.begin(), E2S.end(), ElemToSide);
-    box_geometry(N, ne, xmin, xmax, NGeo, amp, E2S, Mf, Mg, Mh, sJ, NormVec, TangVec1, TangVec2, SurfElem, Elem_xGP);
+    const std::vector<double> X = box_nodes(ne, xmin, xmax, NGeo, amp);
+    nodes_geometry(N, ne[0] * ne[1] * ne[2], NGeo, false, X.data(), E2S, Mf, Mg, Mh, sJ, NormVec, TangVec1, TangVec2,
+                   SurfElem, Elem_xGP);
   } catch (...) {
     return FLUXO_EINVAL_CFG;
   }
@@ -524,8 +593,57 @@ extern "C" int fluxo_host_box_mesh_gauss(int N, const int* ne, const double* xmi
     box_connectivity(ne, N, S2E, E2S);
     std::copy(S2E.begin(), S2E.end(), SideToElem);
     std::copy(E2S.begin(), E2S.end(), ElemToSide);
-    box_geometry_gauss(N, ne, xmin, xmax, NGeo, amp, E2S, Mf, Mg, Mh, sJ, NormVec, TangVec1, TangVec2, SurfElem,
-                       Elem_xGP, SurfMetrics);
+    const std::vector<double> X = box_nodes(ne, xmin, xmax, NGeo, amp);
+    nodes_geometry_gauss(N, ne[0] * ne[1] * ne[2], NGeo, false, X.data(), E2S, Mf, Mg, Mh, sJ, NormVec, TangVec1,
+                         TangVec2, SurfElem, Elem_xGP, SurfMetrics);
+  } catch (...) {
+    return FLUXO_EINVAL_CFG;
+  }
+  return FLUXO_OK;
+}
+
+extern "C" int fluxo_host_hopr_mesh(int N, int node_type, int nElems, const int* ElemInfo, int nSideInfo,
+                                    const int* SideInfo, int nBCs, const int* BCType, int NGeo, int mesh_nodes_gl,
+                                    const double* NodeCoords, double mesh_scale, int use_curveds, int* SideToElem,
+                                    int* ElemToSide, double* Mf, double* Mg, double* Mh, double* sJ, double* NormVec,
+                                    double* TangVec1, double* TangVec2, double* SurfElem, double* Elem_xGP,
+                                    double* SurfMetrics) {
+  if (N < 1 || N > 8 || NGeo < 1 || nElems < 1 || !ElemInfo || !SideInfo || !NodeCoords || (nBCs > 0 && !BCType) ||
+      (node_type != 1 && node_type != 2) || (node_type == 1 && !SurfMetrics))
+    return FLUXO_EINVAL_CFG;
+  try {
+    std::vector<int> S2E, E2S;
+    std::string err;
+    if (!hopr_connectivity(nElems, ElemInfo, nSideInfo, SideInfo, nBCs, BCType, S2E, E2S, err))
+      return fluxo::record_unbound_error(FLUXO_EINVAL_CFG, "fluxo_host_hopr_mesh: " + err);
+    std::copy(S2E.begin(), S2E.end(), SideToElem);
+    std::copy(E2S.begin(), E2S.end(), ElemToSide);
+    // useCurveds = F keeps the eight corners (NGeo = 1); meshScale multiplies (mesh_readin.f90:466-481,
+    // mesh.f90:233-236)
+    const int ng = NGeo + 1;
+    std::vector<double> X;
+    int NG = NGeo;
+    if (use_curveds) {
+      X.assign(NodeCoords, NodeCoords + (size_t)3 * ng * ng * ng * nElems);
+    } else {
+      NG = 1;
+      X.resize((size_t)24 * nElems);
+      for (int e = 0; e < nElems; ++e)
+        for (int c = 0; c < 8; ++c) {
+          const int i = (c & 1) * NGeo, j = ((c >> 1) & 1) * NGeo, k = (c >> 2) * NGeo;
+          for (int d = 0; d < 3; ++d)
+            X[(size_t)24 * e + 3 * c + d] = NodeCoords[3 * (i + ng * (j + ng * (k + (size_t)ng * e))) + d];
+        }
+    }
+    if (std::fabs(mesh_scale - 1.) > 1e-14)
+      for (double& x : X) x *= mesh_scale;
+    const bool gl = mesh_nodes_gl && use_curveds;
+    if (node_type == 1)
+      nodes_geometry_gauss(N, nElems, NG, gl, X.data(), E2S, Mf, Mg, Mh, sJ, NormVec, TangVec1, TangVec2, SurfElem,
+                           Elem_xGP, SurfMetrics);
+    else
+      nodes_geometry(N, nElems, NG, gl, X.data(), E2S, Mf, Mg, Mh, sJ, NormVec, TangVec1, TangVec2, SurfElem,
+                     Elem_xGP);
   } catch (...) {
     return FLUXO_EINVAL_CFG;
   }

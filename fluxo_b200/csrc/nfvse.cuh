@@ -98,6 +98,8 @@ __global__ void __launch_bounds__(512) alpha_kernel(KParams P) {
     double eta = fmax((LU - LUM1) / LU, (LUM1 - LUM2) / LUM1);
     if (eta < 2.220446049250313e-16) eta = 2.220446049250313e-16;
     a = fmax(P.timeRelFactor * P.alpha[e], 1.0 / (1.0 + exp(-P.sharpness * (eta - P.threshold) / P.threshold)));
+  } else if (P.computeAlpha == 20) {  // random values drawn once, kept over time (nfvse.f90:1591-1596)
+    a = P.alpha[e];
   } else {
     a = P.shockBlendCoef;
   }

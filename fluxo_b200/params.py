@@ -2,9 +2,10 @@
 case-insensitive ``key = value`` lines, ``!`` and ``#`` comments, Fortran array literals
 ``(/ a, b, c /)``, logicals ``T/F/.true./.false.``.
 
-Only the keys of the accelerated path are interpreted (see ``KEYS``); the mesh of the
-reference (``MeshFile``, a HOPR HDF5 file) is replaced by a periodic box described by
-the ``Box*`` keys.
+Only the keys of the accelerated path are interpreted (see ``KEYS``).  The mesh is the
+reference's ``MeshFile`` (a HOPR HDF5 file, read by ``hopr``; ``useCurveds``, ``meshScale`` and
+``BoundaryName`` / ``BoundaryType`` pairs apply as in src/mesh/mesh.f90 and mesh_readin.f90), or,
+without it, a periodic box described by the ``Box*`` keys.
 """
 import re
 
@@ -19,6 +20,13 @@ KEYS = {
     "boxmax": ("ra", (1.0, 1.0, 1.0)),
     "ngeo": ("i", 1),
     "meshdeformamp": ("r", 0.0),
+    "meshfile": ("s", None),
+    "usecurveds": ("s", "T"),
+    "meshscale": ("r", 1.0),
+    "boundaryname": ("s", None),
+    "boundarytype": ("ia", None),
+    "projectname": ("s", "FLUXO"),
+    "resettime": ("s", "F"),
     # equation (navierstokes/equation.f90:65-155)
     "equation": ("s", "navierstokes"),
     "parabolic": ("s", "T"),
@@ -128,6 +136,10 @@ def parse_ini(text):
             out[k] = v.strip()
         if k == "refstate":  # a repeated option: IniRefState selects one (equation.f90 RefStatePrim)
             out.setdefault("refstates", []).append(out[k])
+        if k == "boundaryname":  # repeated pairs BoundaryName / BoundaryType (mesh_readin.f90:80-90)
+            out.setdefault("boundarynames", []).append(out[k])
+        if k == "boundarytype":
+            out.setdefault("boundarytypes", []).append(out[k])
     return out
 
 
@@ -148,6 +160,10 @@ def resolve(opts):
     if res["kappa"] is None:
         res["kappa"] = 5.0 / 3.0 if mhd else 1.4
     res["refstates"] = opts.get("refstates", [res["refstate"]])
+    names, types = opts.get("boundarynames", []), opts.get("boundarytypes", [])
+    if len(names) != len(types):
+        raise ValueError("parameter.ini: every BoundaryName needs a BoundaryType")
+    res["boundarytypes"] = dict(zip(names, types))
     return res
 
 

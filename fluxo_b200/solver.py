@@ -8,11 +8,12 @@ reference's initialisation order (InitInterpolation -> InitMesh -> InitEquation 
 All compute runs on the GPU through ``libfluxo_gpu.so``; there is no CPU fallback.
 """
 import ctypes
+import os
 
 import numpy as np
 
 from . import _lib
-from .params import RK_STAGES, parse_ini, resolve, to_cfg_fields
+from .params import RK_STAGES, _flag, parse_ini, resolve, to_cfg_fields
 
 
 def _ptr(a):
@@ -146,6 +147,13 @@ class DGOperator:
         self._check(self.lib.fluxo_gpu_get_alpha(self.h, _ptr(a)))
         return a
 
+    def set_alpha(self, alpha):
+        """Sets the NFVSE blending coefficients that the next right-hand side starts from
+        (ComputeAlpha 20 keeps them)."""
+        a = _c(alpha)
+        assert a.size == self.nElems, "alpha needs one value per element"
+        self._check(self.lib.fluxo_gpu_set_alpha(self.h, _ptr(a)))
+
     def set_state(self, U):
         U = _c(U)
         assert U.size == int(np.prod(self.shape)), "U has the wrong size"
@@ -223,16 +231,30 @@ class DGOperator:
 class Fluxo:
     """The reference's program flow for one ``parameter.ini`` on one GPU."""
 
-    def __init__(self, ini=None, device=0, **overrides):
+    def __init__(self, ini=None, device=0, restart_file=None, base_dir=None, **overrides):
+        """``ini``: parameter.ini text or a dict of options; ``restart_file``: a State file to start
+        from (the reference's second command-line argument); ``base_dir``: the directory that a
+        relative ``MeshFile`` is taken from (the reference's working directory; default: cwd)."""
         opts = parse_ini(ini) if isinstance(ini, str) else dict(ini or {})
         opts.update({k.lower(): v for k, v in overrides.items()})
         self.opts = resolve(opts)
         o = self.opts
         fields = to_cfg_fields(o)
         fields["device"] = device
-        # InitMesh (synthetic periodic box in place of the HOPR file) + CalcMetrics
-        self.mesh = box_mesh(o["n"], o["boxelems"], o["boxmin"], o["boxmax"], o["ngeo"], o["meshdeformamp"],
-                             node_type=fields.get("node_type", 2))
+        node_type = fields.get("node_type", 2)
+        # InitMesh + CalcMetrics: the HOPR file of MeshFile, else the periodic box of the Box* keys
+        if o["meshfile"]:
+            from . import hopr
+            path = o["meshfile"]
+            if not os.path.isabs(path):
+                path = os.path.join(base_dir or os.getcwd(), path)
+            self.mesh_file = o["meshfile"]
+            self.mesh = hopr.load_mesh(path, o["n"], node_type=node_type, mesh_scale=o["meshscale"],
+                                       use_curveds=_flag(o["usecurveds"]), boundary_types=o["boundarytypes"])
+        else:
+            self.mesh_file = ""
+            self.mesh = box_mesh(o["n"], o["boxelems"], o["boxmin"], o["boxmax"], o["ngeo"], o["meshdeformamp"],
+                                 node_type=node_type)
         self.op = DGOperator(**fields)
         self.op.set_mesh(self.mesh)
         # InitDG: FillIni(IniExactFunc, U)
@@ -246,8 +268,20 @@ class Fluxo:
             self.U0 = exact_func(o["iniexactfunc"], 0.0, self.mesh["Elem_xGP"], kappa=o["kappa"],
                                  adv_vel=o["advvel"], amplitude=o["iniamplitude"], wavenumber=o["iniwavenumber"],
                                  frequency=o["inifrequency"], ref_state=o["refstate"])
-        self.op.set_state(self.U0)
         self.t = 0.0
+        if restart_file:  # InitRestart / Restart (restart.f90:60-200), same N and node set only
+            from . import hopr
+            st = hopr.read_state(restart_file)
+            want = "GAUSS" if node_type == 1 else "GAUSS-LOBATTO"
+            if st["N"] != o["n"] or st["NodeType"].strip().upper() != want:
+                raise ValueError("restart from N=%d %s onto N=%d %s (interpolation) is not implemented"
+                                 % (st["N"], st["NodeType"], o["n"], want))
+            if st["U"].shape != self.U0.shape:
+                raise ValueError("restart file %s: DG_Solution shape %s does not match %s"
+                                 % (restart_file, st["U"].shape, self.U0.shape))
+            self.U0 = st["U"]
+            self.t = 0.0 if _flag(o["resettime"]) else st["Time"]
+        self.op.set_state(self.U0)
         self.nDOF = self.op.nElems * (o["n"] + 1) ** 3
         self.nRKStages = RK_STAGES[fields["time_disc"]]
 
@@ -270,6 +304,17 @@ class Fluxo:
         if err:
             raise _lib.FluxoError(-4, "CALCTIMESTEP errType=%d at t=%g" % (err, self.t))
         return n
+
+    def WriteState(self, path=None, next_time=None):
+        """WriteState (src/io_hdf5/hdf5_output.f90:74-160): the current U and t to a State file
+        (default name ProjectName_State_<time>.h5 in the working directory); returns the path."""
+        from . import hopr
+        o = self.opts
+        path = path or hopr.state_file_name(o["projectname"], self.t)
+        hopr.write_state(path, self.U, self.t, self.mesh_file, o["projectname"],
+                         node_type="GAUSS" if self.op.cfg.node_type == 1 else "GAUSS-LOBATTO",
+                         next_time=next_time)
+        return path
 
     @property
     def U(self):

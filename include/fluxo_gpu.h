@@ -82,7 +82,8 @@ typedef struct fluxo_cfg {
    * 3 (TVD-ES) or 4 (TVD-Fjordholm); 3 and 4 need a Riemann solver with dissipation matrices
    * (Navier-Stokes 4, 44, 33; MHD 14, 15). */
   int nfvse;               /* 0 off, 1 on */
-  int compute_alpha;       /* ComputeAlpha: 1 Persson-Peraire indicator, 3 fixed ShockBlendCoef */
+  int compute_alpha;       /* ComputeAlpha: 1 Persson-Peraire indicator, 3 fixed ShockBlendCoef,
+                              20 random values drawn once and kept (see fluxo_gpu_set_alpha) */
   double shock_blend_coef; /* ShockBlendCoef */
   int modal_threshold;     /* ModalThreshold: 1 T = 0.5*10^(-1.8 (N+1)^0.25), 2 T = 0.5*10^(-1.8 N^0.25) */
   double alpha_max, alpha_min, space_prop_factor; /* alpha_max, alpha_min, SpacePropFactor */
@@ -177,6 +178,11 @@ int fluxo_gpu_get_glm_ch(fluxo_handle* h, double* ch);
 /* NFVSE: MOD_NFVSE_Vars::alpha(nElems), the blending coefficients of the last right-hand side
  * (src/shockcapturing/nfvse_vars.f90). */
 int fluxo_gpu_get_alpha(fluxo_handle* h, double* alpha);
+/* Sets alpha(nElems) before the next right-hand side: the values that ComputeAlpha 20 keeps (the
+ * reference draws them once with RANDOM_NUMBER * alpha_max, src/shockcapturing/nfvse.f90:1591-1596;
+ * fluxo_gpu_set_mesh draws them from a SplitMix64 stream), or the previous alpha that TimeRelFactor
+ * weighs for ComputeAlpha 1.  No counterpart call in the reference (there alpha is module data). */
+int fluxo_gpu_set_alpha(fluxo_handle* h, const double* alpha);
 
 /* Exact function of the error norms (the reference's AnalyzeExactFunc with the IniExactFunc
  * parameters, src/equation/navierstokes/equation.f90:575-811): func 0 none, 1 constant reference
@@ -327,6 +333,25 @@ int fluxo_host_box_mesh_gauss(int N, const int* nElemsXYZ, const double* xmin, c
                               double* Metrics_gTilde, double* Metrics_hTilde, double* sJ, double* NormVec,
                               double* TangVec1, double* TangVec2, double* SurfElem, double* Elem_xGP,
                               double* SurfMetrics);
+/* A HOPR mesh from the arrays of its HDF5 file: ElemInfo(6,nElems), SideInfo(5,nSideInfo),
+ * BCType(4,nBCs) and NodeCoords(3,(NGeo+1)^3*nElems) as the file stores them (first index fastest),
+ * the node coordinates on equidistant (mesh_nodes_gl = 0, OutputNodeType 'EQUIDISTANT') or
+ * Gauss-Lobatto points (1); use_curveds = 0 keeps the element corners (NGeo = 1); mesh_scale
+ * multiplies the coordinates (parameter.ini: useCurveds, meshScale).  Conforming meshes whose
+ * boundaries are all periodic (BCType 1): every side is an inner side, nSides = 3*nElems, and
+ * mortar or other boundary sides return FLUXO_EINVAL_CFG with the reason in
+ * fluxo_gpu_last_error(NULL, ...).  node_type 2 (LGL) fills the outputs of fluxo_host_box_mesh,
+ * node_type 1 (Gauss) also SurfMetrics.  Side ids, flips and SideToElem follow the reference for
+ * a single process.
+ * Replaces: src/mesh/mesh_readin.f90:168-511 ReadMesh (connectivity and node coordinates),
+ *           src/mesh/prepare_mesh.f90:59-215 setLocalSideIDs, :662-710 fillMeshInfo,
+ *           src/mesh/mesh.f90:141-245 (useCurveds, meshScale), src/mesh/metrics.f90:78-484. */
+int fluxo_host_hopr_mesh(int N, int node_type, int nElems, const int* ElemInfo, int nSideInfo,
+                         const int* SideInfo, int nBCs, const int* BCType, int NGeo, int mesh_nodes_gl,
+                         const double* NodeCoords, double mesh_scale, int use_curveds, int* SideToElem,
+                         int* ElemToSide, double* Metrics_fTilde, double* Metrics_gTilde, double* Metrics_hTilde,
+                         double* sJ, double* NormVec, double* TangVec1, double* TangVec2, double* SurfElem,
+                         double* Elem_xGP, double* SurfMetrics);
 /* FillIni(IniExactFunc, U) on the given node coordinates (src/equation/navierstokes/equation.f90:575-950):
  * IniExactFunc 1 (constant refstate, prim given), 2 (density sine wave), 4 (manufactured), 7 (Taylor-Green),
  * 14 (soft Sedov-Taylor blast around IniCenter = 0). */

@@ -359,6 +359,7 @@ struct Case {
   std::vector<int> SideToElem, ElemToSide;   // 1-based ids, reference layout
   std::vector<int> S2V;                      // [((((s-1)*5+f)*np+q)*np+p)*np+l]*3
   std::vector<double> NodeCoords, Elem_xGP, Mf, Mg, Mh, sJ, NormVec, TangVec1, TangVec2, SurfElem;
+  bool meshNodesGL = false;                  // NodeCoords on Gauss-Lobatto (else equidistant) points
   // state
   std::vector<real> U, Ut, Umaster, Uslave, Fmaster, Fslave, UtTmp;
   std::vector<real> gx, gy, gz, gxm, gym, gzm, gxs, gys, gzs, FX, FY, FZ;
@@ -1412,11 +1413,8 @@ void InitBasis(Case& C) {
 // Periodic box connectivity with the reference's side numbering rule (mesh/prepare_mesh.f90:59-260,
 // :662-715): side ids are assigned in element / local-side order, the first element that meets a
 // side owns it as master (flip 0) and the slave's flip is found from the node lattice.
-void BuildMesh(Case& C) {
-  const orc_params& P = C.P;
-  int nx = P.nElems[0], ny = P.nElems[1], nz = P.nElems[2], N = C.N, n = C.np;
-  C.nElems = nx * ny * nz;
-  C.nSides = 3 * C.nElems;
+void BuildS2V(Case& C) {
+  const int N = C.N, n = C.np;
   // S2V, mappings.f90:93-255
   C.S2V.assign((size_t)6 * 5 * n * n * n * 3, 0);
   for (int s = 1; s <= 6; ++s)
@@ -1428,6 +1426,14 @@ void BuildMesh(Case& C) {
             SideToVol(N, l, p, q, f, s, ijk);
             for (int c = 0; c < 3; ++c) C.S2V[((((((s - 1) * 5 + f) * n + q) * n + p) * n + l) * 3) + c] = ijk[c];
           }
+}
+
+void BuildMesh(Case& C) {
+  const orc_params& P = C.P;
+  int nx = P.nElems[0], ny = P.nElems[1], nz = P.nElems[2], N = C.N, n = C.np;
+  C.nElems = nx * ny * nz;
+  C.nSides = 3 * C.nElems;
+  BuildS2V(C);
   auto eid = [&](int ix, int iy, int iz) { return ((iz + nz) % nz) * nx * ny + ((iy + ny) % ny) * nx + ((ix + nx) % nx); };
   auto neighbor = [&](int e, int s, int& nbE, int& nbS) {
     int ix = e % nx, iy = (e / nx) % ny, iz = e / (nx * ny);
@@ -1516,6 +1522,107 @@ void BuildMesh(Case& C) {
   }
 }
 
+// A HOPR mesh given by the arrays of its file (ElemInfo, SideInfo, BCType, NodeCoords), restating
+// ReadMesh (mesh/mesh_readin.f90:295-511), setLocalSideIDs (mesh/prepare_mesh.f90:59-215) and
+// fillMeshInfo (mesh/prepare_mesh.f90:662-710) for a single process.  Sides are records
+// (element, local side) indexed 6*e + (locSide-1); mortar sides and sides of non-periodic
+// boundaries have no counterpart in the product and are refused.
+struct HoprMesh {
+  int nElems, nSideInfo, nBCs, NGeo, nodesGL, useCurveds;
+  const int *ElemInfo, *SideInfo, *BCType;
+  const double* NodeCoords;
+  double meshScale;
+};
+
+void BuildMeshHOPR(Case& C, const HoprMesh& M) {
+  const int nE = M.nElems;
+  C.nElems = nE;
+  BuildS2V(C);
+  std::vector<int> ind(6 * (size_t)nE), flip(6 * (size_t)nE), conn(6 * (size_t)nE, -1), sideID(6 * (size_t)nE, -1);
+  auto SI = [&](int row, int f) { return M.SideInfo[5 * (size_t)row + (f - 1)]; };  // SideInfo(f, row+1)
+  for (int e = 0; e < nE; ++e) {
+    const int first = M.ElemInfo[6 * (size_t)e + 2];  // ELEM_FirstSideInd (0-based offset)
+    for (int ls = 1; ls <= 6; ++ls) {
+      const int row = first + ls - 1;
+      if (row < 0 || row >= M.nSideInfo) throw std::runtime_error("HOPR mesh: SideInfo index out of range");
+      if (SI(row, 3) < 0 || SI(row, 1) < 0) throw std::runtime_error("HOPR mesh: mortar sides are not supported");
+      const size_t a = 6 * (size_t)e + ls - 1;
+      ind[a] = std::abs(SI(row, 2));
+      if (SI(row, 2) > 0) flip[a] = 0;
+      else {
+        flip[a] = SI(row, 4) % 10;
+        if (flip[a] < 0 || flip[a] > 4) throw std::runtime_error("HOPR mesh: NodeID doesnt belong to side");
+      }
+    }
+  }
+  for (int e = 0; e < nE; ++e) {
+    const int first = M.ElemInfo[6 * (size_t)e + 2];
+    for (int ls = 1; ls <= 6; ++ls) {
+      const int row = first + ls - 1;
+      const size_t a = 6 * (size_t)e + ls - 1;
+      const int elemID = SI(row, 3), bc = SI(row, 5);
+      if (bc != 0) {
+        if (bc < 1 || bc > M.nBCs) throw std::runtime_error("HOPR mesh: BC index out of range");
+        const int type = M.BCType[4 * (size_t)(bc - 1)];
+        if (type != 1 && type != 100) throw std::runtime_error("HOPR mesh: non-periodic boundary sides are not supported");
+      }
+      if (conn[a] >= 0) continue;
+      if (elemID == 0) throw std::runtime_error("HOPR mesh: boundary sides are not supported");
+      if (elemID < 1 || elemID > nE) throw std::runtime_error("HOPR mesh: neighbour element out of range");
+      for (int nls = 1; nls <= 6; ++nls) {
+        const size_t b = 6 * (size_t)(elemID - 1) + nls - 1;
+        if (ind[b] == ind[a]) {
+          conn[a] = (int)b;
+          conn[b] = (int)a;
+          break;
+        }
+      }
+      if (conn[a] < 0) throw std::runtime_error("HOPR mesh: side connection not found");
+    }
+  }
+  int iInner = 0;
+  for (size_t a = 0; a < 6 * (size_t)nE; ++a)
+    if (sideID[a] == -1) {
+      sideID[a] = ++iInner;
+      sideID[conn[a]] = iInner;
+    }
+  C.nSides = iInner;
+  C.ElemToSide.assign((size_t)2 * 6 * nE, 0);
+  C.SideToElem.assign((size_t)5 * C.nSides, -1);
+  for (int e = 0; e < nE; ++e)
+    for (int ls = 1; ls <= 6; ++ls) {
+      const size_t a = 6 * (size_t)e + ls - 1;
+      const int sid = sideID[a];
+      C.ElemToSide[0 + 2 * a] = sid;
+      C.ElemToSide[1 + 2 * a] = flip[a];
+      int* se = &C.SideToElem[5 * (size_t)(sid - 1)];
+      if (flip[a] == 0) { se[0] = e + 1; se[2] = ls; }
+      else { se[1] = e + 1; se[3] = ls; se[4] = flip[a]; }
+    }
+  for (int s = 0; s < C.nSides; ++s)
+    for (int f = 0; f < 5; ++f)
+      if (C.SideToElem[5 * (size_t)s + f] < 0) throw std::runtime_error("HOPR mesh: a side without master or slave");
+  // NodeCoords(3,0:NGeo,0:NGeo,0:NGeo,nElems); useCurveds=F keeps the corners (NGeo=1), mesh.f90:233-236 scales
+  const int NG = M.NGeo, ng = NG + 1;
+  if (M.useCurveds) {
+    C.NodeCoords.assign(M.NodeCoords, M.NodeCoords + (size_t)3 * ng * ng * ng * nE);
+    C.P.NGeo = NG;
+  } else {
+    C.NodeCoords.assign((size_t)24 * nE, 0.);
+    for (int e = 0; e < nE; ++e)
+      for (int k = 0; k < 2; ++k)
+        for (int j = 0; j < 2; ++j)
+          for (int i = 0; i < 2; ++i)
+            for (int d = 0; d < 3; ++d)
+              C.NodeCoords[3 * (i + 2 * (j + 2 * (k + 2 * (size_t)e))) + d] =
+                  M.NodeCoords[3 * (i * NG + ng * (j * NG + ng * (k * NG + (size_t)ng * e))) + d];
+    C.P.NGeo = 1;
+  }
+  if (std::fabs(M.meshScale - 1.) > 1e-14)
+    for (double& x : C.NodeCoords) x *= M.meshScale;
+  C.meshNodesGL = M.nodesGL && M.useCurveds;
+}
+
 // CalcMetrics (curl form), mesh/metrics.f90:78-333, and CalcSurfMetrics :334-484 (LGL nodes)
 void CalcMetrics(Case& C) {
   int N = C.N, n = C.np, NG = C.P.NGeo, ng = NG + 1, NR = 3 * NG, nr = NR + 1;
@@ -1527,7 +1634,8 @@ void CalcMetrics(Case& C) {
   C.TangVec1.assign((size_t)3 * n * n * C.nSides, 0.);
   C.TangVec2.assign((size_t)3 * n * n * C.nSides, 0.);
   C.SurfElem.assign((size_t)n * n * C.nSides, 0.);
-  std::vector<double> V_EQ_GL = GetVdm(NG, NT_EQUI, NG, NT_GL, false);
+  // Vdm_EQNgeo_GLNgeo from the mesh file's OutputNodeType (metrics.f90:147)
+  std::vector<double> V_EQ_GL = GetVdm(NG, C.meshNodesGL ? NT_GL : NT_EQUI, NG, NT_GL, false);
   std::vector<double> xGLg(ng), DGLg(ng * ng);
   Nodes(NG, NT_GL, xGLg.data());
   DerivMatrix(NG, xGLg.data(), DGLg.data());
@@ -2562,9 +2670,7 @@ void TimeStepLSERK(Case& C, double t, double dt) {
 // ----------------------------------------------------------------------------------------------
 // C interface
 // ----------------------------------------------------------------------------------------------
-extern "C" {
-
-void* orc_create(const orc_params* p) {
+static void* orc_create_impl(const orc_params* p, const HoprMesh* M) {
   try {
     Case* C = new Case();
     C->P = *p;
@@ -2580,11 +2686,24 @@ void* orc_create(const orc_params* p) {
     if (C->gauss && p->nfvse) throw std::runtime_error("Gauss nodes: NFVSE needs the LGL subcells");
     InitEquationAndTime(*C);
     InitBasis(*C);
-    BuildMesh(*C);
+    if (M) BuildMeshHOPR(*C, *M);
+    else BuildMesh(*C);
     CalcMetrics(*C);
     if (p->nfvse) {  // InitNFVSE, nfvse.f90:106-260
       if (p->N < 2) throw std::runtime_error("NFVSE needs N >= 2 (shockcapturing.f90)");
       C->alpha.assign(C->nElems, 0.);
+      if (p->compute_alpha == 20) {
+        // RANDOM_NUMBER * alpha_max (nfvse.f90:1591-1596); the reference's stream is compiler-specific,
+        // this one is SplitMix64 (Steele, Lea, Flood 2014) from state 0, one draw per element
+        uint64_t st = 0;
+        for (int e = 0; e < C->nElems; ++e) {
+          uint64_t z = (st += 0x9e3779b97f4a7c15ULL);
+          z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+          z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+          z ^= z >> 31;
+          C->alpha[e] = (double)(z >> 11) / 9007199254740992.0 * p->alpha_max;
+        }
+      }
       C->alphaMaster.assign(C->nSides, 0.);
       C->alphaSlave.assign(C->nSides, 0.);
       ComputeSubcellMetrics(*C);
@@ -2623,7 +2742,24 @@ void* orc_create(const orc_params* p) {
   }
 }
 
+extern "C" {
+
+void* orc_create(const orc_params* p) { return orc_create_impl(p, nullptr); }
+
+void* orc_create_hopr(const orc_params* p, int nElems, const int* ElemInfo, int nSideInfo, const int* SideInfo,
+                      int nBCs, const int* BCType, int NGeo, int nodesGL, const double* NodeCoords, double meshScale,
+                      int useCurveds) {
+  if (!ElemInfo || !SideInfo || !BCType || !NodeCoords || nElems < 1 || NGeo < 1) return nullptr;
+  HoprMesh M{nElems, nSideInfo, nBCs, NGeo, nodesGL, useCurveds, ElemInfo, SideInfo, BCType, NodeCoords, meshScale};
+  return orc_create_impl(p, &M);
+}
+
 void orc_destroy(void* h) { delete (Case*)h; }
+
+void orc_set_alpha(void* h, const double* alpha) {
+  Case* C = (Case*)h;
+  if (!C->alpha.empty()) std::copy(alpha, alpha + C->nElems, C->alpha.begin());
+}
 
 void orc_sizes(void* h, int* nElems, int* nSides, int* nVar, int* N) {
   Case* C = (Case*)h;

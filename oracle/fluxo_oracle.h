@@ -52,7 +52,8 @@ typedef struct orc_params {
   double ini_halfwidth;   /* IniHalfwidth */
   /* NFVSE shock capturing (shockcapturing/nfvse.f90:63-260), SubFVMethod = 1..4 */
   int nfvse;              /* SHOCK_NFVSE on/off */
-  int compute_alpha;      /* ComputeAlpha: 1 Persson-Peraire indicator, 3 fixed ShockBlendCoef */
+  int compute_alpha;      /* ComputeAlpha: 1 Persson-Peraire indicator, 3 fixed ShockBlendCoef,
+                             20 random values drawn once and kept */
   double shock_blend_coef;
   int modal_threshold;    /* ModalThreshold 1 or 2 */
   double alpha_max, alpha_min, space_prop_factor;
@@ -70,6 +71,13 @@ typedef struct orc_params {
 } orc_params;
 
 void* orc_create(const orc_params* p);
+/* The same case on a HOPR mesh given by the arrays of its file (mesh/mesh_readin.f90:168-716):
+   ElemInfo(6,nElems), SideInfo(5,nSideInfo), BCType(4,nBCs), NodeCoords(3,(NGeo+1)^3*nElems) on
+   equidistant (nodesGL=0) or Gauss-Lobatto (nodesGL=1) points; p->nElems, xmin, xmax, NGeo and
+   deform_amp are ignored.  Conforming meshes whose boundaries are all periodic. */
+void* orc_create_hopr(const orc_params* p, int nElems, const int* ElemInfo, int nSideInfo, const int* SideInfo,
+                      int nBCs, const int* BCType, int NGeo, int nodesGL, const double* NodeCoords,
+                      double meshScale, int useCurveds);
 void orc_destroy(void* h);
 void orc_sizes(void* h, int* nElems, int* nSides, int* nVar, int* N);
 /* Mesh arrays in the reference layout (any pointer may be NULL). */
@@ -114,6 +122,8 @@ void orc_riemann_point(void* h, const double* UL, const double* UR, const double
 double orc_ln_mean(double aL, double aR);
 /* NFVSE: blending coefficient alpha(nElems) of the last right-hand side. */
 void orc_get_alpha(void* h, double* alpha);
+/* NFVSE: alpha(nElems) that the next right-hand side starts from (ComputeAlpha 20 keeps it). */
+void orc_set_alpha(void* h, const double* alpha);
 /* Gauss nodes: SurfMetrics(3,0:N,0:N,6,nElems) of mesh/metrics.f90:420-427 (NULL-safe; LGL: zeros). */
 void orc_get_surf_metrics(void* h, double* SurfMetrics);
 /* NFVSE_CORR: element + 1 whose safe state had negative density or pressure (0: none). */

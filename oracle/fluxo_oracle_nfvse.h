@@ -101,6 +101,8 @@ void CalcBlendingCoefficient(Case& C) {
     }
   } else if (P.compute_alpha == 3) {
     for (int e = 0; e < C.nElems; ++e) C.alpha[e] = P.shock_blend_coef;
+  } else if (P.compute_alpha == 20) {
+    // random values drawn once (at creation or by orc_set_alpha) and kept, nfvse.f90:1591-1596
   } else {
     throw std::runtime_error("ComputeAlpha not implemented in oracle");
   }

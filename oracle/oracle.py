@@ -115,6 +115,9 @@ def _lib(counting=False):
     d, i = ctypes.c_double, ctypes.c_int
     lib.orc_create.restype = ctypes.c_void_p
     lib.orc_create.argtypes = [P(OrcParams)]
+    lib.orc_create_hopr.restype = ctypes.c_void_p
+    lib.orc_create_hopr.argtypes = [P(OrcParams), i, ctypes.c_void_p, i, ctypes.c_void_p, i, ctypes.c_void_p, i, i,
+                                    ctypes.c_void_p, d, i]
     lib.orc_destroy.argtypes = [ctypes.c_void_p]
     lib.orc_sizes.argtypes = [ctypes.c_void_p, P(i), P(i), P(i), P(i)]
     lib.orc_get_mesh.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 11
@@ -139,6 +142,7 @@ def _lib(counting=False):
     lib.orc_ln_mean.restype = d
     lib.orc_ln_mean.argtypes = [d, d]
     lib.orc_get_alpha.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    lib.orc_set_alpha.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     lib.orc_corr_error.restype = ctypes.c_int
     lib.orc_get_surf_metrics.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     lib.orc_corr_error.argtypes = [ctypes.c_void_p]
@@ -177,10 +181,21 @@ def make_params(**kw):
 class OracleCase:
     """One discretised case (mesh + state) in the CPU oracle."""
 
-    def __init__(self, counting=False, **kw):
+    def __init__(self, counting=False, hopr=None, **kw):
+        """``hopr``: the arrays of a HOPR mesh file (keys ElemInfo, SideInfo, BCType, NodeCoords,
+        NGeo, optional nodes_gl, mesh_scale, use_curveds) instead of the periodic box."""
         self.lib = _lib(counting)
         self.params = make_params(**kw)
-        self.h = self.lib.orc_create(ctypes.byref(self.params))
+        if hopr is None:
+            self.h = self.lib.orc_create(ctypes.byref(self.params))
+        else:
+            self._hopr = {k: np.ascontiguousarray(hopr[k], dtype=np.int32) for k in ("ElemInfo", "SideInfo", "BCType")}
+            self._hopr["NodeCoords"] = np.ascontiguousarray(hopr["NodeCoords"], dtype=np.float64)
+            self.h = self.lib.orc_create_hopr(
+                ctypes.byref(self.params), self._hopr["ElemInfo"].shape[0], _ptr(self._hopr["ElemInfo"]),
+                self._hopr["SideInfo"].shape[0], _ptr(self._hopr["SideInfo"]), self._hopr["BCType"].shape[0],
+                _ptr(self._hopr["BCType"]), int(hopr["NGeo"]), int(hopr.get("nodes_gl", 0)),
+                _ptr(self._hopr["NodeCoords"]), float(hopr.get("mesh_scale", 1.0)), int(hopr.get("use_curveds", 1)))
         if not self.h:
             raise RuntimeError("oracle: case creation failed")
         ne, ns, nv, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
@@ -281,6 +296,12 @@ class OracleCase:
         a = np.zeros(self.nElems)
         self.lib.orc_get_alpha(self.h, _ptr(a))
         return a
+
+    def set_alpha(self, alpha):
+        """NFVSE blending coefficients that the next right-hand side starts from."""
+        a = np.ascontiguousarray(alpha, dtype=np.float64)
+        assert a.size == self.nElems
+        self.lib.orc_set_alpha(self.h, _ptr(a))
 
     def surf_metrics(self):
         """Gauss nodes: SurfMetrics(3,0:N,0:N,6,nElems) as a C-order array [e, side, q, p, 3]."""

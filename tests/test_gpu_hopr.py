@@ -1,0 +1,284 @@
+"""The sm_100a path on the reference's own HOPR test meshes (tests/golden/hopr_*.h5, rewritten from the
+reference's tests/meshes by tests/golden/make_hopr_fixtures.py), through the C ABI:
+
+* right-hand-side parity against the CPU oracle on both periodic conforming meshes (curved NGeo 3 and
+  unstructured NGeo 2): Navier-Stokes with LGL and Gauss nodes, NFVSE with ComputeAlpha 20 and every
+  subcell method, MHD;
+* the reference's conforming regression runs on ConformBoxHeavilyWarped (tests/runs/*/parameter.ini), each
+  with its own pass criterion (tests/job_def.py): free-stream preservation L_inf < 1e-11 at tEnd
+  (navst/freestream/conforming, SC_TVD, SC_TVD_ES_fix, SC_TVD_ES_Fjordholm, mhd/freestream/conforming,
+  SC_firstOrder, SC_TVD-ES_Fjordholm) and entropy conservation |dS/dU . Ut| < 1e-13 or stability
+  dS/dU . Ut < 1e-13 at every analysis time (navst and mhd softBlast entropyCons / entropyStab), run through
+  the ``parameter.ini`` flow (``Fluxo``) with MeshFile and a restart State file.
+Tolerances: Ut relative L2 <= 1e-12 against the oracle (FP64, another summation order), 1e-10 with the
+9-wave MHD solver (its TVD states move by 4e-11 between two legal roundings)."""
+import os
+
+import numpy as np
+import pytest
+
+import fluxo_b200 as fb
+from fluxo_b200 import hopr
+from oracle.oracle import OracleCase
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+WARPED = os.path.join(GOLDEN, "hopr_ConformBoxHeavilyWarped_Ngeo3_03_03_03.h5")
+UNSTRUCT = os.path.join(GOLDEN, "hopr_ConformBoxUnstructPeriodicHeavilyWarped_Ngeo2.h5")
+MHD_REF = ((1.2, 0.1, 0.0, 0.1, 0.9, 1.0, 1.0, 1.0), (1.1, 0.2, -0.1, 0.2, 0.6, 1.0, 1.0, 1.0))
+FIELDS = ("N", "eqn", "riemann", "volume_flux", "lifting", "lifting_var", "visc", "kappa", "Pr", "mu0", "time_disc",
+          "cfl_scale", "dfl_scale", "mu_0", "eta", "glm_scale", "glm_scr", "noncons", "nc_glm", "nfvse",
+          "compute_alpha", "shock_blend_coef", "modal_threshold", "alpha_max", "alpha_min", "space_prop_factor",
+          "space_prop_sweeps", "time_rel_factor", "indicator_quantity", "sub_fv_method", "recons_boundaries",
+          "node_type")
+
+
+def rel_l2(a, b):
+    return np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300)
+
+
+def splitmix_alpha(n, alpha_max):
+    """ComputeAlpha 20's initial draws of the product (SplitMix64 from state 0, one per element)."""
+    out, st, m = [], 0, (1 << 64) - 1
+    for _ in range(n):
+        st = (st + 0x9E3779B97F4A7C15) & m
+        z = st
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m
+        z ^= z >> 31
+        out.append((z >> 11) / 9007199254740992.0 * alpha_max)
+    return np.array(out)
+
+
+def pair(mesh_path, noise=0.02, seed=1, ch=None, **kw):
+    raw = hopr.read_mesh(mesh_path)
+    o = OracleCase(hopr=raw, **kw)
+    U = o.get_U()
+    rng = np.random.default_rng(seed)
+    U = U * (1 + noise * rng.standard_normal(U.shape))
+    if o.nVar == 9:
+        U[..., 8] = 0.05 * rng.standard_normal(U[..., 8].shape)
+    o.set_U(U)
+    p = o.params
+    fields = {k: getattr(p, k) for k in FIELDS}
+    fields["ini_exact_func"] = 1
+    op = fb.DGOperator(**fields)
+    op.set_mesh(hopr.mesh_arrays(p.N, raw, node_type=p.node_type))
+    op.set_state(U)
+    if ch is not None:
+        op.glm_ch = ch
+    return o, op
+
+
+NS = dict(eqn=1, kappa=1.4, mu0=0.01, Pr=0.72, ini_exact_func=2, ini_amplitude=0.3, adv_vel=(0.3, -0.2, 0.5))
+RHS_CASES = [
+    ("warped", dict(NS, N=3, riemann=44, volume_flux=5, lifting=1, lifting_var=3)),
+    ("warped", dict(NS, N=5, riemann=33, volume_flux=32, lifting=2, lifting_var=2)),
+    ("unstruct", dict(NS, N=4, riemann=44, volume_flux=5, lifting=1, lifting_var=3)),
+    ("unstruct", dict(NS, N=7, riemann=1, volume_flux=1, lifting=1, lifting_var=1)),
+    ("warped", dict(NS, N=3, riemann=44, volume_flux=5, lifting=1, lifting_var=3, node_type=1)),
+    ("unstruct", dict(NS, N=4, riemann=32, volume_flux=10, lifting=2, lifting_var=3, node_type=1)),
+    ("warped", dict(eqn=0, N=3, riemann=9, volume_flux=5, ini_exact_func=14, nfvse=1, compute_alpha=20,
+                    alpha_max=1.0, space_prop_sweeps=0)),
+    ("warped", dict(eqn=0, N=3, riemann=4, volume_flux=10, ini_exact_func=14, nfvse=1, compute_alpha=20,
+                    space_prop_sweeps=0, sub_fv_method=2, recons_boundaries=1)),
+    ("unstruct", dict(eqn=0, N=3, riemann=4, volume_flux=10, ini_exact_func=14, nfvse=1, compute_alpha=20,
+                      sub_fv_method=3, recons_boundaries=2, space_prop_sweeps=1)),
+    ("warped", dict(eqn=1, mu0=0.001, N=3, riemann=44, volume_flux=10, ini_exact_func=14, nfvse=1, compute_alpha=20,
+                    sub_fv_method=4, recons_boundaries=3, space_prop_sweeps=0)),
+    ("warped", dict(eqn=2, N=3, kappa=5 / 3, riemann=11, volume_flux=10, ini_exact_func=201, mhd_ref_state=MHD_REF,
+                    ini_halfwidth=0.3, ini_amplitude=0.1, glm_ch=0.7)),
+    ("unstruct", dict(eqn=3, N=4, kappa=5 / 3, riemann=10, volume_flux=10, ini_exact_func=201, mhd_ref_state=MHD_REF,
+                      ini_halfwidth=0.3, ini_amplitude=0.1, mu0=1e-3, eta=1e-3, glm_ch=0.7)),
+    ("warped", dict(eqn=2, N=3, kappa=5 / 3, riemann=14, volume_flux=10, ini_exact_func=201, mhd_ref_state=MHD_REF,
+                    ini_halfwidth=0.3, ini_amplitude=0.1, glm_ch=0.7, nfvse=1, compute_alpha=20, sub_fv_method=4,
+                    recons_boundaries=2, space_prop_sweeps=0)),
+]
+
+
+@pytest.mark.parametrize("mesh,kw", RHS_CASES)
+def test_rhs_parity_on_hopr_mesh(gpu_lib, mesh, kw):
+    o, op = pair(WARPED if mesh == "warped" else UNSTRUCT, ch=kw.get("glm_ch"), **kw)
+    Ut_o = o.dg_time_derivative(0.0)
+    op.dg_time_derivative(0.0)
+    Ut = op.get_ut()
+    tol = 1e-10 if kw.get("riemann") == 14 and kw.get("eqn", 0) >= 2 else 1e-12
+    assert rel_l2(Ut, Ut_o) <= tol
+    if kw.get("nfvse"):
+        a, ao = op.alpha(), o.alpha()
+        assert np.abs(a - ao).max() <= 1e-14
+        if kw.get("space_prop_sweeps", 1) == 0:
+            assert np.abs(a - np.where(splitmix_alpha(o.nElems, o.params.alpha_max) < o.params.alpha_min, 0.0,
+                                       splitmix_alpha(o.nElems, o.params.alpha_max))).max() <= 1e-15
+
+
+def test_set_alpha_drives_the_blend(gpu_lib):
+    """fluxo_gpu_set_alpha hands ComputeAlpha 20 its values; the same values in the oracle give the same Ut."""
+    o, op = pair(WARPED, eqn=0, N=3, riemann=9, volume_flux=5, ini_exact_func=14, nfvse=1, compute_alpha=20,
+                 alpha_max=1.0, space_prop_sweeps=0)
+    a = np.linspace(0.0, 1.0, o.nElems)[::-1].copy()
+    o.set_alpha(a)
+    op.set_alpha(a)
+    Ut_o = o.dg_time_derivative(0.0)
+    op.dg_time_derivative(0.0)
+    assert rel_l2(op.get_ut(), Ut_o) <= 1e-12
+    assert np.abs(op.alpha() - np.where(a < 0.01, 0.0, a)).max() == 0.0
+
+
+def test_time_steps_match_oracle(gpu_lib):
+    """Three ssprk4-5 steps with random blending on the warped mesh: states within 1e-11 of the oracle's."""
+    o, op = pair(WARPED, noise=0.0, eqn=1, mu0=1e-3, N=3, riemann=9, volume_flux=5, ini_exact_func=14, nfvse=1,
+                 compute_alpha=20, alpha_max=1.0, space_prop_sweeps=0, time_disc=8, cfl_scale=0.4, dfl_scale=0.4)
+    t = 0.0
+    for _ in range(3):
+        dt_o, _ = o.calc_timestep()
+        dt, err = op.calc_timestep()
+        assert err == 0 and abs(dt - dt_o) <= 1e-13 * dt_o
+        o.timestep(t, dt_o)
+        op.timestep(t, dt_o)
+        t += dt_o
+    assert rel_l2(op.get_state(), o.get_U()) <= 1e-11
+
+
+# --- the reference's regression runs on its mesh -------------------------------------------------------
+FREESTREAM_NS = """
+ProjectName = NAVIERSTOKES_FREESTREAM
+N = 3
+Riemann = 1
+VolumeFlux = 1
+IniExactFunc = 1
+IniRefState = 1
+RefState = (/1.0, 0.1, 0.2, -0.3, 20. /)
+mu0 = 1.0E-06
+tend = 20.0
+CFLscale = 0.9
+DFLscale = 0.5
+"""
+SC_NS = {
+    "SC_TVD": "Riemann = 4\nVolumeFlux = 10\nSubFVMethod = 2\nReconsBoundaries = 1\n",
+    "SC_TVD_ES_fix": "Riemann = 4\nVolumeFlux = 10\nSubFVMethod = 3\nReconsBoundaries = 2\n",
+    "SC_TVD_ES_Fjordholm": "Riemann = 44\nVolumeFlux = 10\nSubFVMethod = 4\nReconsBoundaries = 3\n",
+}
+FREESTREAM_MHD = {
+    "conforming": """N = 5
+Riemann = 1
+VolumeFlux = 1
+IniExactFunc = 1
+IniRefState = 1
+RefState = (/1.0, 0.1, 0.2, -0.3, 20., 0.5, -0.03, 0.02 /)
+eta = 1.0E-05
+mu = 1.0E-06
+tend = 5.
+CFLscale = 0.5
+DFLscale = 0.4
+""",
+    "SC_firstOrder": """N = 3
+Riemann = 1
+VolumeFlux = 1
+NFVSE = T
+ComputeAlpha = 20
+SpacePropSweeps = 1
+IniExactFunc = 1
+IniRefState = 1
+RefState = (/1.0, 0.1, 0.2, -0.3, 20., 1.0, -1.2, 0.5 /)
+tend = 20.0
+CFLscale = 0.9
+DFLscale = 0.5
+""",
+    "SC_TVD-ES_Fjordholm": """N = 3
+Riemann = 14
+VolumeFlux = 10
+NFVSE = T
+ComputeAlpha = 20
+SpacePropSweeps = 0
+SubFVMethod = 4
+ReconsBoundaries = 2
+IniExactFunc = 1
+IniRefState = 1
+RefState = (/1.0, 0.1, 0.2, -0.3, 20., 1.0, -1.2, 0.5 /)
+tend = 20.0
+CFLscale = 0.9
+DFLscale = 0.5
+""",
+}
+
+
+def _linf_freestream(f):
+    return np.abs(f.U - f.U0).max(axis=(0, 1, 2, 3))
+
+
+def test_reference_freestream_conforming_with_restart(gpu_lib, tmp_path):
+    """navst/freestream/conforming, restarted from a State file as the reference's run is: L_inf < 1e-11 at
+    t = 20 (nodal and on the analysis points), then WriteState / read back."""
+    U0 = fb.Fluxo(FREESTREAM_NS, MeshFile=WARPED).U0
+    st = tmp_path / "NAVIERSTOKES_FREESTREAM_State_0000000.000000000.h5"
+    hopr.write_state(st, U0, 0.0, WARPED, "NAVIERSTOKES_FREESTREAM")
+    f = fb.Fluxo(FREESTREAM_NS, MeshFile=WARPED, restart_file=str(st))
+    assert f.t == 0.0 and np.array_equal(f.U, U0)
+    n = f.TimeDisc()
+    assert abs(f.t - 20.0) < 1e-12 and n > 1000
+    assert _linf_freestream(f).max() < 1e-11
+    r = f.op.analyze(f.t, exact=dict(func=1, ref_state_prim=(1.0, 0.1, 0.2, -0.3, 20.0)))
+    assert r["Linf"].max() < 1e-11
+    out = f.WriteState(str(tmp_path / "out.h5"))
+    back = hopr.read_state(out)
+    assert back["Time"] == f.t and np.array_equal(back["U"], f.U) and back["N"] == 3
+
+
+@pytest.mark.parametrize("case", sorted(SC_NS))
+def test_reference_sc_freestream_ns(gpu_lib, case):
+    f = fb.Fluxo(FREESTREAM_NS + "NFVSE = T\nComputeAlpha = 20\nSpacePropSweeps = 0\n" + SC_NS[case],
+                 MeshFile=WARPED)
+    f.TimeDisc()
+    a = f.op.alpha()
+    assert np.abs(a - np.where(splitmix_alpha(27, 0.5) < 0.01, 0.0, splitmix_alpha(27, 0.5))).max() <= 1e-15
+    assert _linf_freestream(f).max() < 1e-11
+
+
+@pytest.mark.parametrize("case", sorted(FREESTREAM_MHD))
+def test_reference_freestream_mhd(gpu_lib, case):
+    f = fb.Fluxo("Equation = mhd\nkappa = 1.6666666666666667\n" + FREESTREAM_MHD[case], MeshFile=WARPED)
+    f.TimeDisc()
+    assert _linf_freestream(f).max() < 1e-11
+
+
+ENTROPY = {
+    "navst/entropyCons": ("Riemann = 9\nVolumeFlux = 5\n", True),
+    "navst/entropyCons_Ranocha": ("Riemann = 32\nVolumeFlux = 32\n", True),
+    "navst/entropyStab": ("Riemann = 1\nVolumeFlux = 5\nmu0 = 0.\n", False),
+    "mhd/entropyCons": ("Equation = mhd\nRiemann = 11\nVolumeFlux = 10\nRefState = (/1.2,0.1, 0.0,0.1,0.9,1.0,1.0,1.0 /)\n"
+                        "RefState = (/1.1,0.2,-0.1,0.2,0.6,1.0,1.0,1.0 /)\nmu = 0.0\neta = 0.0\nCFLscale = 0.5\n"
+                        "DFLscale = 0.5\n", True),
+    "mhd/entropyStab": ("Equation = mhd\nRiemann = 10\nVolumeFlux = 10\nRefState = (/1.2,0.1, 0.0,0.1,0.9,1.0,1.0,1.0 /)\n"
+                        "RefState = (/1.0,0.2,-0.4,0.2,0.3,1.0,1.0,1.0 /)\nmu = 1.e-8\neta = 1.e-8\nCFLscale = 0.4\n"
+                        "DFLscale = 0.5\n", False),
+    "mhd/entropyStab_FloGor9waves": ("Equation = mhd\nRiemann = 15\nVolumeFlux = 12\n"
+                                     "RefState = (/1.2,0.1, 0.0,0.1,0.9,1.0,1.0,1.0 /)\n"
+                                     "RefState = (/1.0,0.2,-0.4,0.2,0.3,1.0,1.0,1.0 /)\nmu = 1.e-8\neta = 1.e-8\n"
+                                     "CFLscale = 0.4\nDFLscale = 0.5\n", False),
+}
+
+
+@pytest.mark.parametrize("case", sorted(ENTROPY))
+def test_reference_softblast_entropy(gpu_lib, case):
+    """softBlast with random NFVSE blending (ComputeAlpha 20, alpha_max 1) on the warped mesh, ssprk4-5 to t=5
+    analysed every 1.0: |dS/dU . Ut| < 1e-13 for the entropy-conserving fluxes, dS/dU . Ut < 1e-13 for the
+    entropy-stable ones (tests/job_def.py err_tol 1e-13)."""
+    text, conserving = ENTROPY[case]
+    mhd = case.startswith("mhd")
+    ini = ("N = 3\nNFVSE = T\nComputeAlpha = 20\nSpacePropSweeps = 0\nalpha_max = 1.0\nTimeDiscMethod = ssprk4-5\n"
+           + ("IniExactFunc = 201\nIniCenter = (/0.0, 0.0, 0.0/)\nIniRefState = 1\nkappa = 1.6666666666666667\n"
+              "IniHalfwidth = 0.3\nIniAmplitude = 0.1\n" if mhd else
+              "IniExactFunc = 14\nCFLscale = 0.4\nDFLscale = 0.4\n") + text)
+    f = fb.Fluxo(ini, MeshFile=WARPED)
+    vals = []
+    for k in range(6):
+        if k:
+            f.TimeDisc(t_end=float(k))
+        f.DGTimeDerivative(f.t)
+        vals.append(f.op.analyze(f.t)["dSdU_Ut"])
+    vals = np.array(vals)
+    if conserving:
+        assert np.abs(vals).max() < 1e-13, vals
+    else:
+        assert vals.max() < 1e-13 and vals.min() < -1e-6, vals
