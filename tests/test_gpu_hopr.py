@@ -259,12 +259,19 @@ ENTROPY = {
 }
 
 
+# With this package's ComputeAlpha 20 draw (the reference's RANDOM_NUMBER stream is compiler-specific) the
+# purely entropy-conserving Ranocha scheme loses positivity at t = 4.6951 (the oracle does the same at the
+# same time): that case is analysed to t = 4, and its break is checked against the oracle's.
+BREAKS = {"navst/entropyCons_Ranocha": 4}
+
+
 @pytest.mark.parametrize("case", sorted(ENTROPY))
 def test_reference_softblast_entropy(gpu_lib, case):
     """softBlast with random NFVSE blending (ComputeAlpha 20, alpha_max 1) on the warped mesh, ssprk4-5 to t=5
     analysed every 1.0: |dS/dU . Ut| < 1e-13 for the entropy-conserving fluxes, dS/dU . Ut < 1e-13 for the
     entropy-stable ones (tests/job_def.py err_tol 1e-13)."""
     text, conserving = ENTROPY[case]
+    last = BREAKS.get(case, 5)
     mhd = case.startswith("mhd")
     ini = ("N = 3\nNFVSE = T\nComputeAlpha = 20\nSpacePropSweeps = 0\nalpha_max = 1.0\nTimeDiscMethod = ssprk4-5\n"
            + ("IniExactFunc = 201\nIniCenter = (/0.0, 0.0, 0.0/)\nIniRefState = 1\nkappa = 1.6666666666666667\n"
@@ -272,7 +279,7 @@ def test_reference_softblast_entropy(gpu_lib, case):
               "IniExactFunc = 14\nCFLscale = 0.4\nDFLscale = 0.4\n") + text)
     f = fb.Fluxo(ini, MeshFile=WARPED)
     vals = []
-    for k in range(6):
+    for k in range(last + 1):
         if k:
             f.TimeDisc(t_end=float(k))
         f.DGTimeDerivative(f.t)
@@ -282,3 +289,15 @@ def test_reference_softblast_entropy(gpu_lib, case):
         assert np.abs(vals).max() < 1e-13, vals
     else:
         assert vals.max() < 1e-13 and vals.min() < -1e-6, vals
+    if case in BREAKS:
+        o = OracleCase(hopr=hopr.read_mesh(WARPED), N=3, eqn=1, mu0=0.0, riemann=32, volume_flux=32,
+                       ini_exact_func=14, nfvse=1, compute_alpha=20, space_prop_sweeps=0, alpha_max=1.0, time_disc=8,
+                       cfl_scale=0.4, dfl_scale=0.4)
+        t_o = 0.0
+        for k in range(1, 6):  # the same analysis times clip the same steps
+            t_o, _ = o.run(t_o, float(k))
+            if t_o < k:
+                break
+        with pytest.raises(fb.FluxoError, match="errType=4"):
+            f.TimeDisc(t_end=5.0)
+        assert t_o < 5.0 and abs(f.t - t_o) < 1e-9 * t_o
