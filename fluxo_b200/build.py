@@ -20,7 +20,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-
 CU_SOURCES = (["fluxo_gpu.cu", "launch_misc.cu", "lift_impl.cu", "noalloc.cu", "analyze.cu"] +
               ["vol_vf%d.cu" % v for v in (0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 32)] +
               ["mhd_launch.cu", "mhd_vol_ec.cu", "mhd_vol_std.cu", "nfvse_launch.cu", "nfvse_ns.cu", "batch.cu",
-               "gauss_launch.cu", "gauss_surf.cu"])
+               "gauss_launch.cu", "gauss_surf.cu", "gauss_mhd.cu"])
 CPP_SOURCES = ["host_setup.cpp"]
 
 

@@ -356,6 +356,13 @@ int rhs(fluxo_handle* h, KParams P) {
       FLUXO_CUDA(h, launch_nfvse_fv(h->cfg.riemann, h->NP, h->nElems, h->nSMs, s, P));
       h->launches += 3 + (h->cfg.space_prop_sweeps > 1 ? 2 * (h->cfg.space_prop_sweeps - 1) : 0);
     }
+    if (h->gauss) {  // ProlongToFace_U (dg.f90:458-511), entropy-projected for Derigs / FloGor (10, 12)
+      if (!h->surfMetSet) return fail(h, FLUXO_ENOTREADY, "Gauss nodes: SurfMetrics not set");
+      const int vf = h->cfg.volume_flux;
+      ProfScope ps(h, 2);
+      FLUXO_CUDA(h, launch_gauss_prolong(h->NP, vf == 10 || vf == 12, true, h->nElems, s, P));
+      h->launches += 1;
+    }
     if (h->visc) {
       {
         ProfScope ps(h, 0);
@@ -370,6 +377,11 @@ int rhs(fluxo_handle* h, KParams P) {
     {
       ProfScope ps(h, 2);
       FLUXO_CUDA(h, launch_mhd_face(h->cfg.riemann, h->visc, h->NP, h->nSides, s, P));
+    }
+    if (h->gauss) {  // SurfInt with the split-form correction and the non-conservative terms
+      ProfScope ps(h, 2);
+      FLUXO_CUDA(h, launch_gauss_surf_mhd(h->NP, h->cfg.volume_flux, h->nElems, s, P));
+      h->launches += 1;
     }
     {
       ProfScope ps(h, 3);
@@ -391,7 +403,7 @@ int rhs(fluxo_handle* h, KParams P) {
     const int vf = h->cfg.volume_flux;
     const bool ent = vf == 5 || vf == 6 || vf == 7 || vf == 10 || vf == 32;  // equation.f90:413-455
     ProfScope ps(h, 2);
-    FLUXO_CUDA(h, launch_gauss_prolong(h->NP, ent, h->nElems, s, P));
+    FLUXO_CUDA(h, launch_gauss_prolong(h->NP, ent, false, h->nElems, s, P));
     h->launches += 1;
   }
   if (h->visc) {
@@ -610,8 +622,9 @@ int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {
   if (!(cfg->kappa > 1.)) return fail(nullptr, FLUXO_EINVAL_CFG, "kappa must be > 1");
   if (cfg->node_type != 0 && cfg->node_type != 1 && cfg->node_type != 2)
     return fail(nullptr, FLUXO_EINVAL_CFG, "node_type must be 1 (Gauss) or 2 (Gauss-Lobatto)");
-  if (cfg->node_type == 1) {  // the Gauss path of this library: Euler / Navier-Stokes, no NFVSE subcells
-    if (mhd) return fail(nullptr, FLUXO_EINVAL_CFG, "Gauss nodes: only the Euler / Navier-Stokes system");
+  if (cfg->node_type == 1) {  // the Gauss path of this library: Euler / Navier-Stokes / ideal MHD, no NFVSE
+    if (cfg->eqn == FLUXO_EQN_MHD_PARABOLIC)
+      return fail(nullptr, FLUXO_EINVAL_CFG, "Gauss nodes: MHD without the parabolic terms only");
     if (cfg->nfvse) return fail(nullptr, FLUXO_EINVAL_CFG, "Gauss nodes: NFVSE needs the LGL subcells");
   }
   fluxo_handle* h = new fluxo_handle();
@@ -700,7 +713,8 @@ int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* S2E, 
       return r;
   }
   if (h->gauss) {
-    if ((r = dalloc(h, &h->dUface, (size_t)2 * 5 * NPT * nSides)) || (r = dalloc(h, &h->dUtSurf, (size_t)5 * NP3 * nElems)) ||
+    const size_t nv = (size_t)h->nVar;
+    if ((r = dalloc(h, &h->dUface, 2 * nv * NPT * nSides)) || (r = dalloc(h, &h->dUtSurf, nv * NP3 * nElems)) ||
         (r = dalloc(h, &h->dSurfMet, (size_t)18 * NPT * nElems)))
       return r;
     h->surfMetSet = false;

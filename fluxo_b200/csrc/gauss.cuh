@@ -24,6 +24,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "lifting.cuh"
+#include "physics_mhd.cuh"
 #include "physics_ns.cuh"
 #include "volume_pairs.cuh"
 
@@ -80,64 +81,69 @@ __device__ __forceinline__ void entropy_to_cons(const KParams& P, const double* 
   U[4] = U[0] * (p_srho * P.sKappaM1 + v2s2);
 }
 
-// face-state slot of (side, role, point)
-__device__ __forceinline__ double* uface_at(const KParams& P, int NPT, int side, int role, int pt) {
-  return P.uface + (((size_t)side * 2 + role) * NPT + pt) * 5;
+// face-state slot of (side, role, point), nv variables per point
+__device__ __forceinline__ double* uface_at(const KParams& P, int NPT, int side, int role, int pt, int nv = 5) {
+  return P.uface + (((size_t)side * 2 + role) * NPT + pt) * nv;
 }
 
 // ProlongToFace_U (dg.f90:458-511) with the Gauss interpolation of prolongtoface.f90:103-132; ENT: the
-// entropy variables are interpolated and the face values converted back (useEntropyProlongToFace).
-template <int NP, bool ENT>
+// entropy variables are interpolated and the face values converted back (useEntropyProlongToFace);
+// NVT = 5 (Euler / Navier-Stokes) or 9 (MHD + GLM, mhd/equation_vars.f90:330-401).
+template <int NP, bool ENT, int NVT>
 __global__ void __launch_bounds__(NP * NP * NP) prolong_kernel(KParams P) {
   if (halted(P)) return;
   constexpr int NP3 = NP * NP * NP, NPT = NP * NP, XS = NP3 + NPT;
-  __shared__ double sX[5 * XS];  // [var][slot], node n at slot n + n / NP (the lines of a warp's side
-                                 // points spread over the banks)
+  __shared__ double sX[NVT * XS];  // [var][slot], node n at slot n + n / NP (the lines of a warp's side
+                                   // points spread over the banks)
   __shared__ double sL[NP];
   __shared__ int sE2S[12];
   const int e = blockIdx.x, t = threadIdx.x;
   for (int z = t; z < 12; z += NP3) sE2S[z] = P.e2s[12 * (size_t)e + z];  // NP3 = 8 for N = 1
   if (t < NP) sL[t] = P.basis->Lminus[t];
   {
-    const double* Ug = P.U + 5 * ((size_t)e * NP3 + t);
-    double u[5], x[5];
+    const double* Ug = P.U + NVT * ((size_t)e * NP3 + t);
+    double u[NVT], x[NVT];
 #pragma unroll
-    for (int v = 0; v < 5; ++v) u[v] = Ug[v];
-    if constexpr (ENT) {
+    for (int v = 0; v < NVT; ++v) u[v] = Ug[v];
+    if constexpr (ENT && NVT == 9) {
+      mhd::cons_to_entropy(P, u, x);
+    } else if constexpr (ENT) {
       cons_to_entropy_ns(P, u, x);
     } else {
 #pragma unroll
-      for (int v = 0; v < 5; ++v) x[v] = u[v];
+      for (int v = 0; v < NVT; ++v) x[v] = u[v];
     }
 #pragma unroll
-    for (int v = 0; v < 5; ++v) sX[v * XS + t + t / NP] = x[v];
+    for (int v = 0; v < NVT; ++v) sX[v * XS + t + t / NP] = x[v];
   }
   __syncthreads();
   for (int task = t; task < 6 * NPT; task += NP3) {
     const int s = task / NPT + 1, ab = task - (s - 1) * NPT, a = ab % NP, b = ab / NP;
     const int side = sE2S[2 * (s - 1)], flip = sE2S[2 * (s - 1) + 1];
-    double acc[5];
+    double acc[NVT];
     {
       const int n0 = line_node_of(NP, s, a, b, 0);
 #pragma unroll
-      for (int v = 0; v < 5; ++v) acc[v] = sX[v * XS + n0 + n0 / NP] * sL[0];
+      for (int v = 0; v < NVT; ++v) acc[v] = sX[v * XS + n0 + n0 / NP] * sL[0];
     }
 #pragma unroll
     for (int l = 1; l < NP; ++l) {
       const int n = line_node_of(NP, s, a, b, l);
 #pragma unroll
-      for (int v = 0; v < 5; ++v) acc[v] = acc[v] + sX[v * XS + n + n / NP] * sL[l];
+      for (int v = 0; v < NVT; ++v) acc[v] = acc[v] + sX[v * XS + n + n / NP] * sL[l];
     }
-    double c[5];
-    if constexpr (ENT) {
+    double c[NVT];
+    if constexpr (ENT && NVT == 9) {
+      mhd::entropy_to_cons(P, acc, c);
+    } else if constexpr (ENT) {
       entropy_to_cons(P, acc, c);
     } else {
 #pragma unroll
-      for (int v = 0; v < 5; ++v) c[v] = acc[v];
+      for (int v = 0; v < NVT; ++v) c[v] = acc[v];
     }
-    double* o = uface_at(P, NPT, side, flip == 0 ? 0 : 1, face_point_of(NP, s, flip, a, b));
+    double* o = uface_at(P, NPT, side, flip == 0 ? 0 : 1, face_point_of(NP, s, flip, a, b), NVT);
 #pragma unroll
-    for (int v = 0; v < 5; ++v) o[v] = c[v];
+    for (int v = 0; v < NVT; ++v) o[v] = c[v];
   }
 }
 

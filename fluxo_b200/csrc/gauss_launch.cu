@@ -6,9 +6,14 @@ namespace fluxo {
 
 namespace {
 template <int NP>
-cudaError_t prolong_np(bool ent, int nElems, cudaStream_t s, const KParams& P) {
-  if (ent) gauss::prolong_kernel<NP, true><<<nElems, NP * NP * NP, 0, s>>>(P);
-  else gauss::prolong_kernel<NP, false><<<nElems, NP * NP * NP, 0, s>>>(P);
+cudaError_t prolong_np(bool ent, bool mhd, int nElems, cudaStream_t s, const KParams& P) {
+  if (mhd) {
+    if (ent) gauss::prolong_kernel<NP, true, 9><<<nElems, NP * NP * NP, 0, s>>>(P);
+    else gauss::prolong_kernel<NP, false, 9><<<nElems, NP * NP * NP, 0, s>>>(P);
+  } else {
+    if (ent) gauss::prolong_kernel<NP, true, 5><<<nElems, NP * NP * NP, 0, s>>>(P);
+    else gauss::prolong_kernel<NP, false, 5><<<nElems, NP * NP * NP, 0, s>>>(P);
+  }
   return cudaGetLastError();
 }
 
@@ -38,15 +43,15 @@ cudaError_t lift_np(int lift, int lv, int nElems, cudaStream_t s, const KParams&
 }
 }  // namespace
 
-cudaError_t launch_gauss_prolong(int NP, bool ent, int nElems, cudaStream_t s, const KParams& P) {
+cudaError_t launch_gauss_prolong(int NP, bool ent, bool mhd, int nElems, cudaStream_t s, const KParams& P) {
   switch (NP) {
-    case 2: return prolong_np<2>(ent, nElems, s, P);
-    case 3: return prolong_np<3>(ent, nElems, s, P);
-    case 4: return prolong_np<4>(ent, nElems, s, P);
-    case 5: return prolong_np<5>(ent, nElems, s, P);
-    case 6: return prolong_np<6>(ent, nElems, s, P);
-    case 7: return prolong_np<7>(ent, nElems, s, P);
-    case 8: return prolong_np<8>(ent, nElems, s, P);
+    case 2: return prolong_np<2>(ent, mhd, nElems, s, P);
+    case 3: return prolong_np<3>(ent, mhd, nElems, s, P);
+    case 4: return prolong_np<4>(ent, mhd, nElems, s, P);
+    case 5: return prolong_np<5>(ent, mhd, nElems, s, P);
+    case 6: return prolong_np<6>(ent, mhd, nElems, s, P);
+    case 7: return prolong_np<7>(ent, mhd, nElems, s, P);
+    case 8: return prolong_np<8>(ent, mhd, nElems, s, P);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -68,9 +68,10 @@ cudaError_t launch_mhd_timestep(int NP, bool visc, int nElems, cudaStream_t s, c
 // `scratch` holds nElems doubles for sweeps > 1) and the subcell FV volume integral of MHD.
 // Gauss nodes (gauss.cuh): face states (ent: entropy-projected), lifting + viscous volume integral, and
 // the surface integral with the split-form correction
-cudaError_t launch_gauss_prolong(int NP, bool ent, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_gauss_prolong(int NP, bool ent, bool mhd, int nElems, cudaStream_t s, const KParams& P);
 cudaError_t launch_gauss_lift_visc(int NP, int lift, int lv, int nElems, cudaStream_t s, const KParams& P);
 cudaError_t launch_gauss_surf(int NP, int vf, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_gauss_surf_mhd(int NP, int vf, int nElems, cudaStream_t s, const KParams& P);
 cudaError_t launch_nfvse_alpha(int NP, bool mhd, int nElems, cudaStream_t s, const KParams& P, double* scratch);
 // NFVSE_CORR: Apply_NFVSE_Correction of every element after a stage update with step b * dt (ut: the
 // stage's Ut to correct as well, or null); errKey records elem*8 + 5 for a safe state that is not admissible

@@ -34,8 +34,9 @@ __global__ void face_kernel(KParams P, int NP) {
   const int nM = side_node(NP - 1, pt % NP, pt / NP, 0, se5[2]);
   const int nS = side_node(NP - 1, pt % NP, pt / NP, se5[4], se5[3]);
   const size_t NP3 = (size_t)NP * NP * NP;
-  const double* UM = P.U + NV * ((size_t)eM * NP3 + nM);
-  const double* US = P.U + NV * ((size_t)eS * NP3 + nS);
+  // LGL: the sides' boundary nodes; Gauss nodes: the interpolated face states [side][master|slave][pt][9]
+  const double* UM = P.uface ? P.uface + ((size_t)side * 2 * npts + pt) * NV : P.U + NV * ((size_t)eM * NP3 + nM);
+  const double* US = P.uface ? P.uface + (((size_t)side * 2 + 1) * npts + pt) * NV : P.U + NV * ((size_t)eS * NP3 + nS);
   const double* g = P.facegeo + (size_t)side * 10 * npts + pt;
   double nv[3], t1[3], t2[3];
 #pragma unroll
@@ -455,9 +456,14 @@ __global__ void __launch_bounds__(vol_threads<NP>(), vol_minb<NP>()) volume_kern
 #pragma unroll
     for (int v = 0; v < 7; ++v) ut[1 + v] += V[v * NP3];
   }
+  if (P.utsurf) {  // Gauss nodes: the surface integral of every node, formed by gauss::surf_mhd_kernel
+    const double* S = P.utsurf + (size_t)e * NV * NP3 + t;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) ut[v] += S[v * NP3];
+  }
   // surface integral at the boundary nodes (LGL), with the own side's non-conservative part
   int sides[3];
-  const int ns = boundary_sides(i, j, k, N, sides);
+  const int ns = P.utsurf ? 0 : boundary_sides(i, j, k, N, sides);
   const double lh = P.basis->LhatM0;
   for (int z = 0; z < ns; ++z) {
     const int s = sides[z];

@@ -56,6 +56,22 @@ __device__ __forceinline__ void cons_to_entropy(const KParams& P, const double* 
   for (int z = 5; z < 9; ++z) W[z] = rho_sp * U[z];
 }
 
+// EntropyToCons, mhd/equation_vars.f90:366-401
+__device__ __forceinline__ void entropy_to_cons(const KParams& P, const double* W, double* U) {
+  const double rho_sp = -W[4];
+  const double p_srho = 1. / rho_sp;
+  const double u = W[1] * p_srho, v = W[2] * p_srho, w = W[3] * p_srho;
+  const double v2s2 = 0.5 * (u * u + v * v + w * w);
+  const double s = P.kappa - ((W[0] + rho_sp * v2s2) * P.kappaM1);
+  U[0] = pow(exp(-s) * p_srho, P.sKappaM1);
+  U[1] = u * U[0];
+  U[2] = v * U[0];
+  U[3] = w * U[0];
+#pragma unroll
+  for (int z = 5; z < 9; ++z) U[z] = W[z] * p_srho;
+  U[4] = U[0] * (P.sKappaM1 * p_srho + v2s2) + P.s2mu_0 * (U[5] * U[5] + U[6] * U[6] + U[7] * U[7] + U[8] * U[8]);
+}
+
 // FastestWave1D, mhd/equation_vars.f90:663-684 (primitive input)
 __device__ __forceinline__ double fastest_wave_1d(const KParams& P, const double* Q) {
   const double sRho = 1. / Q[0];

@@ -2318,7 +2318,9 @@ void SurfInt(Case& C) {
     // Gauss nodes (surfint.f90:118-175, 196-253): every node of the line takes the surface flux times
     // L_HatMinus(l); the split form adds the correction -(FluxB_sum - FluxB(l)) NormalSign with
     // FluxB(l) = the two-point volume flux between node l and the side's state (metric average of the
-    // node's metric and SurfMetrics) and FluxB_sum = sum_l FluxB(l) L_Minus(l)
+    // node's metric and SurfMetrics) and FluxB_sum = sum_l FluxB(l) L_Minus(l).  MHD with NONCONS: the
+    // sum takes FluxB(l) plus the non-conservative flux from the side state to node l, and FluxB(l)
+    // itself gains the one from node l to the side state (AddNonConsFluxVec, mhd/flux_average.f90:378-418)
     const int NV = C.nVar;
     const size_t nv = (size_t)n * n * n;
     std::vector<real> FB((size_t)NV * n);
@@ -2338,15 +2340,24 @@ void SurfInt(Case& C) {
             real aB[NVMAX + 4], aN[NVMAX + 4], sum[NVMAX];
             Uaux(C, UB, aB);
             const double* SM = &C.SurfMetrics[3 * ((size_t)p + n * ((size_t)q + n * ((size_t)(ls - 1) + 6 * (size_t)e)))];
+            for (int v = 0; v < NV; ++v) sum[v] = 0.;
             for (int l = 0; l < n; ++l) {
               const size_t o = C.nod(C.s2v(l, p, q, fl, ls, 0), C.s2v(l, p, q, fl, ls, 1), C.s2v(l, p, q, fl, ls, 2), e);
               Uaux(C, &C.U[NV * o], aN);
               const real mL[3] = {Mx[3 * o], Mx[3 * o + 1], Mx[3 * o + 2]}, mR[3] = {SM[0], SM[1], SM[2]};
-              VolumeFluxVec(C, &C.U[NV * o], UB, aN, aB, mL, mR, &FB[(size_t)NV * l]);
+              real* F = &FB[(size_t)NV * l];
+              if (C.mhd) MHD_VolumeFluxVec(C, C.P.volume_flux, &C.U[NV * o], UB, aN, aB, mL, mR, F);
+              else VolumeFluxVec(C, &C.U[NV * o], UB, aN, aB, mL, mR, F);
+              if (C.mhd && C.noncons) {
+                real Fc[NVMAX];
+                for (int v = 0; v < NV; ++v) Fc[v] = F[v];
+                MHD_NonConsPair(C, UB, aB, &C.U[NV * o], mR, mL, Fc);  // side state -> node l
+                for (int v = 0; v < NV; ++v) sum[v] = sum[v] + Fc[v] * C.Lminus[l];
+                MHD_NonConsPair(C, &C.U[NV * o], aN, UB, mL, mR, F);   // node l -> side state
+              } else {
+                for (int v = 0; v < NV; ++v) sum[v] = sum[v] + F[v] * C.Lminus[l];
+              }
             }
-            for (int v = 0; v < NV; ++v) sum[v] = 0.;
-            for (int l = 0; l < n; ++l)
-              for (int v = 0; v < NV; ++v) sum[v] = sum[v] + FB[(size_t)NV * l + v] * C.Lminus[l];
             for (int l = 0; l < n; ++l) {
               const size_t o = C.nod(C.s2v(l, p, q, fl, ls, 0), C.s2v(l, p, q, fl, ls, 1), C.s2v(l, p, q, fl, ls, 2), e);
               for (int v = 0; v < NV; ++v) {
@@ -2395,10 +2406,12 @@ struct PhaseCount {  // operation count of one phase of the RHS (counting build)
   ~PhaseCount() { g_phase[k] += g_oracle_flops - start; }
 };
 
-// useEntropyProlongToFace (navierstokes/equation.f90:413-455): the EC / EC-KEP volume fluxes
+// useEntropyProlongToFace: the EC / EC-KEP volume fluxes (navierstokes/equation.f90:413-455; MHD:
+// Derigs 10 and FloGor 12, mhd/equation.f90:411-427)
 inline bool UseEntropyProlong(const Case& C) {
   const int vf = C.P.volume_flux;
-  return !C.mhd && (vf == 5 || vf == 6 || vf == 7 || vf == 10 || vf == 32);
+  if (C.mhd) return vf == 10 || vf == 12;
+  return vf == 5 || vf == 6 || vf == 7 || vf == 10 || vf == 32;
 }
 
 // ProlongToFace_U, dg.f90:458-511: Gauss nodes with an entropy-conservative volume flux prolong the
@@ -2410,12 +2423,20 @@ void ProlongToFaceU(Case& C) {
   }
   const int NV = C.nVar;
   C.Vent.resize(C.U.size());
-  for (size_t z = 0; z < C.U.size() / NV; ++z) ConsToEntropy(C, &C.U[NV * z], &C.Vent[NV * z]);
+  for (size_t z = 0; z < C.U.size() / NV; ++z) {
+    if (C.mhd) MHD_ConsToEntropy(C, &C.U[NV * z], &C.Vent[NV * z]);
+    else ConsToEntropy(C, &C.U[NV * z], &C.Vent[NV * z]);
+  }
   std::vector<real> Vm(C.Umaster.size()), Vs(C.Uslave.size());
   ProlongToFace(C, C.Vent, Vm, Vs);
   for (size_t z = 0; z < Vm.size() / NV; ++z) {
-    EntropyToCons(C, &Vm[NV * z], &C.Umaster[NV * z]);
-    EntropyToCons(C, &Vs[NV * z], &C.Uslave[NV * z]);
+    if (C.mhd) {
+      MHD_EntropyToCons(C, &Vm[NV * z], &C.Umaster[NV * z]);
+      MHD_EntropyToCons(C, &Vs[NV * z], &C.Uslave[NV * z]);
+    } else {
+      EntropyToCons(C, &Vm[NV * z], &C.Umaster[NV * z]);
+      EntropyToCons(C, &Vs[NV * z], &C.Uslave[NV * z]);
+    }
   }
 }
 
@@ -2682,7 +2703,6 @@ static void* orc_create_impl(const orc_params* p, const HoprMesh* M) {
     C->nDOFElem = C->np * C->np * C->np;
     C->parabolic = (p->eqn == 1 || p->eqn == 3);
     C->gauss = (p->node_type == 1);
-    if (C->gauss && C->mhd) throw std::runtime_error("Gauss nodes: only the Euler / Navier-Stokes system");
     if (C->gauss && p->nfvse) throw std::runtime_error("Gauss nodes: NFVSE needs the LGL subcells");
     InitEquationAndTime(*C);
     InitBasis(*C);

@@ -202,6 +202,22 @@ inline void MHD_ConsToEntropy(const Case& C, const real* U, real* W) {
   for (int z = 5; z < 9; ++z) W[z] = rho_sp * U[z];
 }
 
+// EntropyToCons, mhd/equation_vars.f90:366-401
+inline void MHD_EntropyToCons(const Case& C, const real* W, real* U) {
+  real rho_sp = -W[4];
+  real p_srho = 1. / rho_sp;
+  real u = W[1] * p_srho, v = W[2] * p_srho, w = W[3] * p_srho;
+  real v2s2 = 0.5 * (u * u + v * v + w * w);
+  real s = C.kappa - ((W[0] + rho_sp * v2s2) * C.kappaM1);
+  U[0] = pow(exp(-s) * p_srho, C.sKappaM1);
+  U[1] = u * U[0];
+  U[2] = v * U[0];
+  U[3] = w * U[0];
+  for (int z = 5; z < 9; ++z) U[z] = W[z] * p_srho;
+  U[4] = U[0] * (C.sKappaM1 * p_srho + v2s2) +
+         C.s2mu_0 * (U[5] * U[5] + U[6] * U[6] + U[7] * U[7] + U[8] * U[8]);
+}
+
 // FastestWave1D, mhd/equation_vars.f90:663-684 (primitive input, normal direction 1)
 inline real MHD_FastestWave1D(const Case& C, const real* P) {
   real sRho = 1. / P[0];

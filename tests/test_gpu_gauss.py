@@ -97,7 +97,7 @@ def test_gauss_time_disc_parity(gpu_lib, time_disc, eqn):
 
 def test_gauss_configuration_checks(gpu_lib):
     with pytest.raises(FluxoError):
-        fb.DGOperator(N=3, eqn=2, riemann=14, volume_flux=10, kappa=5 / 3, node_type=1)
+        fb.DGOperator(N=3, eqn=3, riemann=14, volume_flux=10, kappa=5 / 3, mu0=0.01, eta=0.01, node_type=1)
     with pytest.raises(FluxoError):
         fb.DGOperator(N=3, eqn=0, riemann=44, volume_flux=5, nfvse=1, node_type=1)
     c, op = pair()
@@ -136,3 +136,80 @@ def test_gauss_product_setup_path(gpu_lib):
                    mu0=0.01, cfl_scale=0.5, node_type=1)
     ref = c.dg_time_derivative(0.0)
     assert rel_l2(f.Ut, ref) <= 1e-11
+
+
+# --- ideal MHD + GLM with Gauss nodes ---------------------------------------------------------------------------
+MHD_REF = ((1.2, 0.1, 0.0, 0.1, 0.9, 1.0, 1.0, 1.0), (1.1, 0.2, -0.1, 0.2, 0.6, 1.0, 1.0, 1.0))
+
+
+def mhd_pair(noise=0.01, seed=0, ch=0.7, **kw):
+    base = dict(eqn=2, N=3, nElems=(3, 2, 2), xmin=(-1, -1, -1), xmax=(1, 1, 1), NGeo=2, deform_amp=0.1,
+                kappa=5 / 3, mhd_ref_state=MHD_REF, ini_exact_func=201, ini_center=(0.1, 0.05, 0.0),
+                ini_halfwidth=0.4, ini_amplitude=0.02, glm_ch=ch, node_type=1, volume_flux=10, riemann=11)
+    base.update(kw)
+    c = OracleCase(**base)
+    U = c.get_U()
+    if noise:
+        rng = np.random.default_rng(seed)
+        U = U * (1 + noise * rng.standard_normal(U.shape))
+        U[..., 8] = 0.05 * rng.standard_normal(U[..., 8].shape)
+        c.set_U(U)
+    p = c.params
+    op = fb.DGOperator(N=p.N, eqn=p.eqn, riemann=p.riemann, volume_flux=p.volume_flux, kappa=p.kappa, mu_0=p.mu_0,
+                       glm_scale=p.glm_scale, glm_scr=p.glm_scr, noncons=p.noncons, nc_glm=p.nc_glm,
+                       time_disc=p.time_disc, cfl_scale=p.cfl_scale, dfl_scale=p.dfl_scale, ini_exact_func=1,
+                       node_type=1)
+    op.set_mesh(c.mesh())
+    op.set_state(U)
+    op.glm_ch = ch
+    return c, op
+
+
+MHD_CASES = [
+    dict(N=1, volume_flux=10, riemann=11), dict(N=2, volume_flux=12, riemann=12), dict(N=3, volume_flux=10, riemann=11),
+    dict(N=3, volume_flux=10, riemann=10, nc_glm=1), dict(N=3, volume_flux=1, riemann=1), dict(N=3, volume_flux=0, riemann=4),
+    dict(N=3, volume_flux=12, riemann=15, noncons=2), dict(N=4, volume_flux=10, riemann=14, noncons=3),
+    dict(N=4, volume_flux=10, riemann=5), dict(N=5, volume_flux=12, riemann=13), dict(N=6, volume_flux=10, riemann=2),
+    dict(N=7, volume_flux=10, riemann=10, nElems=(2, 1, 1)), dict(N=7, volume_flux=1, riemann=3, nElems=(2, 1, 1)),
+    dict(N=3, volume_flux=10, riemann=11, noncons=0),
+]
+
+
+@pytest.mark.parametrize("case", MHD_CASES, ids=lambda c: "N%d_vf%d_rs%d_nc%d%s" % (
+    c["N"], c["volume_flux"], c["riemann"], c.get("noncons", 1), "_ncglm" if c.get("nc_glm") else ""))
+def test_gauss_mhd_parity(gpu_lib, case):
+    """Ideal MHD + GLM with Gauss nodes: entropy-projected face states (Derigs, FloGor), the MHD FluxB surface
+    correction with the non-conservative fluxes of both directions, the sides' own non-conservative surface
+    terms from the face states; Ut against the oracle (1e-10 with the 9-wave solver 14, else 1e-12)."""
+    c, op = mhd_pair(**case)
+    ref = c.dg_time_derivative(0.0)
+    op.dg_time_derivative(0.0)
+    assert rel_l2(op.get_ut(), ref) <= (1e-10 if case["riemann"] == 14 else 1e-12)
+
+
+def test_gauss_mhd_entropy_and_freestream_on_gpu(gpu_lib):
+    c, op = mhd_pair(volume_flux=10, riemann=11, nElems=(3, 3, 2))
+    op.dg_time_derivative(0.0)
+    assert abs(op.analyze(0.0)["dSdU_Ut"]) < 1e-13
+    c, op = mhd_pair(volume_flux=10, riemann=14, nElems=(3, 3, 2))
+    op.dg_time_derivative(0.0)
+    assert op.analyze(0.0)["dSdU_Ut"] < -1e-6
+    c, op = mhd_pair(noise=0.0, ini_exact_func=1, volume_flux=12, riemann=15)
+    op.dg_time_derivative(0.0)
+    assert np.abs(op.get_ut()).max() < 1e-11
+
+
+@pytest.mark.parametrize("time_disc", [0, 8])
+def test_gauss_mhd_time_steps(gpu_lib, time_disc):
+    """CALCTIMESTEP with the Gauss CFL table and GLM_ch, and three steps: states within 1e-11 of the oracle's."""
+    c, op = mhd_pair(time_disc=time_disc, cfl_scale=0.5)
+    t = 0.0
+    for _ in range(3):
+        dt_o, err_o = c.calc_timestep()
+        dt, err = op.calc_timestep()
+        assert err == err_o == 0 and abs(dt - dt_o) <= 1e-12 * dt_o
+        assert abs(op.glm_ch - c.glm_ch) <= 1e-12 * c.glm_ch
+        c.timestep(t, dt_o)
+        op.timestep(t, dt_o)
+        t += dt_o
+    assert rel_l2(op.get_state(), c.get_U()) <= 1e-11

@@ -67,8 +67,65 @@ def test_gauss_converges_at_order_n_plus_1_and_beats_lgl():
 
 
 def test_gauss_restrictions():
-    """Gauss nodes here: Euler / Navier-Stokes without the NFVSE subcells (which need LGL nodes)."""
-    with pytest.raises(Exception):
-        OracleCase(eqn=2, ini_exact_func=1, volume_flux=10, riemann=14, kappa=5 / 3, **WARPED)
+    """Gauss nodes here run without the NFVSE subcells (which need LGL nodes)."""
     with pytest.raises(Exception):
         OracleCase(eqn=0, ini_exact_func=1, volume_flux=5, riemann=44, nfvse=1, **WARPED)
+
+
+MHD_REF = ((1.2, 0.1, 0.0, 0.1, 0.9, 1.0, 1.0, 1.0), (1.1, 0.2, -0.1, 0.2, 0.6, 1.0, 1.0, 1.0))
+MHD = dict(eqn=2, N=3, nElems=(3, 3, 2), xmin=(-1, -1, -1), xmax=(1, 1, 1), NGeo=2, deform_amp=0.1, kappa=5 / 3,
+           mhd_ref_state=MHD_REF, ini_exact_func=201, ini_center=(0.1, 0.05, 0.0), ini_halfwidth=0.4,
+           ini_amplitude=0.02, glm_ch=0.7, node_type=1)
+
+
+def noisy_mhd(seed=0, **kw):
+    c = OracleCase(**dict(MHD, **kw))
+    U = c.get_U()
+    rng = np.random.default_rng(seed)
+    U = U * (1 + 0.01 * rng.standard_normal(U.shape))
+    U[..., 8] = 0.05 * rng.standard_normal(U[..., 8].shape)
+    c.set_U(U)
+    return c
+
+
+@pytest.mark.parametrize("vf,rs,nc", [(1, 1, 1), (10, 11, 1), (12, 12, 2), (10, 14, 3), (0, 4, 1)])
+def test_gauss_mhd_freestream(vf, rs, nc):
+    """MHD + GLM with Gauss nodes on a curved box: a constant state stays constant (|Ut| < 1e-11), with the
+    non-conservative terms in the volume, on the faces and in the split-form surface correction."""
+    c = OracleCase(**dict(MHD, ini_exact_func=1, volume_flux=vf, riemann=rs, noncons=nc))
+    assert np.abs(c.dg_time_derivative()).max() < 1e-11
+
+
+@pytest.mark.parametrize("vf,rs,ncg", [(10, 11, 0), (10, 11, 1), (12, 12, 0)])
+def test_gauss_mhd_entropy_conservation(vf, rs, ncg):
+    """Derigs (10) / FloGor (12) volume and surface fluxes with Powell terms, Gauss nodes with the entropy-projected
+    face states and the FluxB correction with the non-conservative fluxes (surfint.f90:118-175): dS/dU . Ut
+    vanishes to round-off (the criterion of the reference's mhd softBlast/entropyCons runs, 1e-13)."""
+    c = noisy_mhd(volume_flux=vf, riemann=rs, noncons=1, nc_glm=ncg)
+    c.dg_time_derivative()
+    assert abs(c.analyze(0.0)["dSdU_Ut"]) < 1e-13
+
+
+@pytest.mark.parametrize("vf,rs", [(10, 10), (12, 15), (10, 14)])
+def test_gauss_mhd_entropy_stability(vf, rs):
+    c = noisy_mhd(volume_flux=vf, riemann=rs, noncons=1)
+    c.dg_time_derivative()
+    assert c.analyze(0.0)["dSdU_Ut"] < -1e-6
+
+
+def test_gauss_mhd_needs_the_powell_terms_for_entropy_conservation():
+    c = noisy_mhd(volume_flux=10, riemann=11, noncons=0)
+    c.dg_time_derivative()
+    assert abs(c.analyze(0.0)["dSdU_Ut"]) > 1e-6
+
+
+@pytest.mark.parametrize("lifting,lv", [(1, 3), (2, 2)])
+def test_gauss_resistive_mhd(lifting, lv):
+    """Resistive / viscous MHD with Gauss nodes (the lifting's Gauss branches): free-stream preserving and
+    dissipative with the entropy-conserving inviscid fluxes."""
+    kw = dict(eqn=3, mu0=0.01, eta=0.01, lifting=lifting, lifting_var=lv, volume_flux=10, riemann=11)
+    f = OracleCase(**dict(MHD, ini_exact_func=1, **kw))
+    assert np.abs(f.dg_time_derivative()).max() < 1e-11
+    c = noisy_mhd(**kw)
+    c.dg_time_derivative()
+    assert c.analyze(0.0)["dSdU_Ut"] < -1e-6
