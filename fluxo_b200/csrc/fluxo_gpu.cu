@@ -370,7 +370,8 @@ int rhs(fluxo_handle* h, KParams P) {
       }
       {
         ProfScope ps(h, 1);
-        FLUXO_CUDA(h, launch_mhd_lift_visc(h->NP, h->cfg.lifting, h->nElems, s, P));
+        if (h->gauss) FLUXO_CUDA(h, launch_gauss_mhd_lift_visc(h->NP, h->cfg.lifting, h->nElems, s, P));
+        else FLUXO_CUDA(h, launch_mhd_lift_visc(h->NP, h->cfg.lifting, h->nElems, s, P));
       }
       h->launches += 2;
     }
@@ -622,9 +623,7 @@ int fluxo_gpu_create(const fluxo_cfg* cfg, fluxo_handle** out) {
   if (!(cfg->kappa > 1.)) return fail(nullptr, FLUXO_EINVAL_CFG, "kappa must be > 1");
   if (cfg->node_type != 0 && cfg->node_type != 1 && cfg->node_type != 2)
     return fail(nullptr, FLUXO_EINVAL_CFG, "node_type must be 1 (Gauss) or 2 (Gauss-Lobatto)");
-  if (cfg->node_type == 1) {  // the Gauss path of this library: Euler / Navier-Stokes / ideal MHD, no NFVSE
-    if (cfg->eqn == FLUXO_EQN_MHD_PARABOLIC)
-      return fail(nullptr, FLUXO_EINVAL_CFG, "Gauss nodes: MHD without the parabolic terms only");
+  if (cfg->node_type == 1) {  // the Gauss path of this library: every equation system, no NFVSE
     if (cfg->nfvse) return fail(nullptr, FLUXO_EINVAL_CFG, "Gauss nodes: NFVSE needs the LGL subcells");
   }
   fluxo_handle* h = new fluxo_handle();

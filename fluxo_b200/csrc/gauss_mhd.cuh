@@ -10,9 +10,17 @@
 // state (AddNonConsFlux, mhd/riemann.f90:230-267, fillflux.f90:87-99).  The face states U_master /
 // U_slave come from gauss::prolong_kernel (9 variables per point).  Output: [elem][9][node] for the MHD
 // volume kernel, which adds it in place of its LGL surface terms.
+//
+// The resistive / viscous terms with Gauss nodes (mhd_lift_visc_kernel): BR1 / BR2 gradients of the
+// lifting variable with the surface terms at every node of each line (L_HatMinus(l)), the face traces of
+// the gradient interpolated to the 6 sides and converted with the face states into each side's share
+// n.F_v of the face flux (7 components, br1.f90:318-350, br2_surfint.f90:109-148), and the viscous /
+// resistive volume integral of variables 2..8 (volint.f90:228-271), as gauss::lift_visc_kernel does for
+// the Navier-Stokes equations.
 #pragma once
 #include "gauss.cuh"
 #include "mhd_kernels.cuh"
+#include "mhd_lifting.cuh"
 
 namespace fluxo {
 namespace gauss {
@@ -153,6 +161,215 @@ __global__ void __launch_bounds__(NP * NP * NP, 1) surf_mhd_kernel(KParams P) {
   double* O = P.utsurf + (size_t)e * NV9 * NP3 + t;
 #pragma unroll
   for (int v = 0; v < NV9; ++v) O[v * NP3] = ut[v];
+}
+
+// shared memory of the MHD lifting kernel: operators, sJ, the 27 gradient rows (slot n + n / NP), and one
+// area used in turn for the lifting variable [9][node], the staged side products [side point][27] and
+// the contravariant fluxes [21][node]
+template <int NP>
+__host__ __device__ constexpr int mlift_area() {
+  constexpr int a = 9 * NP * NP * NP, b = 27 * 6 * NP * NP, c = 21 * NP * NP * NP;
+  return a > b ? (a > c ? a : c) : (b > c ? b : c);
+}
+template <int NP>
+__host__ __device__ constexpr size_t mlift_smem_bytes() {
+  return sizeof(double) * (size_t)(2 * NP * NP + 2 * NP + NP * NP * NP + 27 * lift_gstride<NP>() + mlift_area<NP>());
+}
+
+template <int NP, int LIFT>
+__global__ void __launch_bounds__(NP * NP * NP) mhd_lift_visc_kernel(KParams P) {
+  if (halted(P)) return;
+  constexpr int NV9 = 9, NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1, GS = lift_gstride<NP>();
+  extern __shared__ double smem[];
+  double* sD = smem;              // D(i,l) at [i*NP+l]
+  double* sDhat = sD + NPT;       // D_hat(i,l)
+  double* sLm = sDhat + NPT;      // L_Minus(l)
+  double* sLh = sLm + NP;         // L_HatMinus(l)
+  double* sSJ = sLh + NP;         // [node] sJ
+  double* sG = sSJ + NP3;         // [27][slot] gradient of the lifting variable that is prolonged
+  double* sA = sG + 27 * GS;      // lifting variable, then staged side products, then contravariant fluxes
+  __shared__ int sE2S[12];
+  const int e = blockIdx.x, t = threadIdx.x;
+  const int i = t % NP, j = (t / NP) % NP, k = t / NPT;
+  for (int z = t; z < NPT; z += NP3) { sD[z] = P.basis->D[z]; sDhat[z] = P.basis->Dhat[z]; }
+  if (t < NP) { sLm[t] = P.basis->Lminus[t]; sLh[t] = P.basis->LhatMinus[t]; }
+  for (int z = t; z < 12; z += NP3) sE2S[z] = P.e2s[12 * (size_t)e + z];  // NP3 = 8 for N = 1
+  double u[NV9];
+  const double sj = P.sJ[(size_t)e * NP3 + t];
+  const int gs = lift_gslot(NP, t);
+  {
+    const double* Ug = P.U + NV9 * ((size_t)e * NP3 + t);
+#pragma unroll
+    for (int v = 0; v < NV9; ++v) u[v] = Ug[v];
+    double V[NV9];
+    mhd::lifting_var_rt(P, u, V);
+#pragma unroll
+    for (int v = 0; v < NV9; ++v) sA[v * NP3 + t] = V[v];
+    sSJ[t] = sj;
+  }
+  __syncthreads();
+  const double* M = P.metrics + (size_t)e * 9 * NP3 + t;
+  double g[3][NV9];
+  {
+    // Lifting_VolInt (br1_volint.f90:45-98): the derivatives along the lines, metric terms
+    double dx[NV9], de[NV9], dz[NV9];
+#pragma unroll
+    for (int v = 0; v < NV9; ++v) { dx[v] = 0.; de[v] = 0.; dz[v] = 0.; }
+#pragma unroll
+    for (int l = 0; l < NP; ++l) {
+      const double a = sD[i * NP + l], b = sD[j * NP + l], c = sD[k * NP + l];
+#pragma unroll
+      for (int v = 0; v < NV9; ++v) {
+        dx[v] += a * sA[v * NP3 + l + NP * (j + NP * k)];
+        de[v] += b * sA[v * NP3 + i + NP * (l + NP * k)];
+        dz[v] += c * sA[v * NP3 + i + NP * (j + NP * l)];
+      }
+    }
+    double m[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) m[c] = M[c * NP3];
+#pragma unroll
+    for (int v = 0; v < NV9; ++v)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) g[d][v] = m[0 + d] * dx[v] + m[3 + d] * de[v] + m[6 + d] * dz[v];
+  }
+  if constexpr (LIFT == 2) {  // br2_volint.f90: the volume part carries sJ; it is what is prolonged
+#pragma unroll
+    for (int v = 0; v < NV9; ++v)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        g[d][v] *= sj;
+        sG[(NV9 * d + v) * GS + gs] = g[d][v];
+      }
+  }
+  __syncthreads();  // the lifting variable is read; the area takes the staged side products
+  // surface terms: every node of the line of each side takes the lifting flux times L_HatMinus(l); the 27
+  // products (flux x normal) of each side point are staged once, [side point][3 x 9]
+  for (int task = t; task < 6 * NPT; task += NP3) {
+    const int s = task / NPT + 1, ab = task - (s - 1) * NPT, a = ab % NP, b = ab / NP;
+    const int side = sE2S[2 * (s - 1)], flip = sE2S[2 * (s - 1) + 1];
+    const int pt = face_point_of(NP, s, flip, a, b);
+    const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
+    const double* F = P.lflux + (size_t)side * NV9 * NPT + pt;
+    const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
+#pragma unroll
+    for (int v = 0; v < NV9; ++v) {
+      const double f = F[v * NPT];
+      sA[task * 27 + v] = f * n0;
+      sA[task * 27 + 9 + v] = f * n1;
+      sA[task * 27 + 18 + v] = f * n2;
+    }
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int s = 1; s <= 6; ++s) {
+    int l, a, b;
+    line_of_node(N, s, i, j, k, l, a, b);
+    const double* Fn = sA + ((s - 1) * NPT + a + NP * b) * 27;
+    const double lh = sLh[l];
+#pragma unroll
+    for (int v = 0; v < NV9; ++v) {
+      if constexpr (LIFT == 2) {
+        const double fl = sj * lh;
+        g[0][v] += fl * Fn[v]; g[1][v] += fl * Fn[9 + v]; g[2][v] += fl * Fn[18 + v];
+      } else {
+        g[0][v] += Fn[v] * lh; g[1][v] += Fn[9 + v] * lh; g[2][v] += Fn[18 + v] * lh;
+      }
+    }
+  }
+  if constexpr (LIFT == 1) {
+#pragma unroll
+    for (int v = 0; v < NV9; ++v)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        g[d][v] *= sj;
+        sG[(NV9 * d + v) * GS + gs] = g[d][v];
+      }
+  }
+  __syncthreads();  // the staged products are read; the gradient rows are complete
+  // face traces: the gradient interpolated to each side's points (BR2: plus etaBR2 L_Minus(l) times the
+  // own side's surface terms), converted with the side's state, n.F_v for the face kernel
+  for (int task = t; task < 6 * NPT; task += NP3) {
+    const int s = task / NPT + 1, ab = task - (s - 1) * NPT, a = ab % NP, b = ab / NP;
+    const int side = sE2S[2 * (s - 1)], flip = sE2S[2 * (s - 1) + 1], role = flip == 0 ? 0 : 1;
+    const int pt = face_point_of(NP, s, flip, a, b);
+    const double* nvec = P.facegeo + (size_t)side * 10 * NPT + pt;
+    const double n0 = nvec[0], n1 = nvec[NPT], n2 = nvec[2 * NPT];
+    double tr[3][NV9];
+    {
+      const int nd = lift_gslot(NP, line_node_of(NP, s, a, b, 0));
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int v = 0; v < NV9; ++v) tr[d][v] = sG[(NV9 * d + v) * GS + nd] * sLm[0];
+    }
+    for (int l = 1; l < NP; ++l) {
+      const int nd = lift_gslot(NP, line_node_of(NP, s, a, b, l));
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int v = 0; v < NV9; ++v) tr[d][v] = tr[d][v] + sG[(NV9 * d + v) * GS + nd] * sLm[l];
+    }
+    if constexpr (LIFT == 2) {
+      const double* F = P.lflux + (size_t)side * NV9 * NPT + pt;
+      double f[NV9];
+#pragma unroll
+      for (int v = 0; v < NV9; ++v) f[v] = F[v * NPT];
+      for (int l = 0; l < NP; ++l) {
+        const double w = P.etaBR2 * sLm[l], fl = sSJ[line_node_of(NP, s, a, b, l)] * sLh[l];
+#pragma unroll
+        for (int v = 0; v < NV9; ++v) {
+          tr[0][v] = tr[0][v] + w * (fl * (f[v] * n0));
+          tr[1][v] = tr[1][v] + w * (fl * (f[v] * n1));
+          tr[2][v] = tr[2][v] + w * (fl * (f[v] * n2));
+        }
+      }
+    }
+    const double* uf = uface_at(P, NPT, side, role, pt, NV9);
+    double us[NV9];
+#pragma unroll
+    for (int v = 0; v < NV9; ++v) us[v] = uf[v];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) mhd::to_grad_prim_rt(P, us, tr[d]);
+    double kf[7], kg[7], kh[7];
+    mhd::visc_flux_3d(P, us, tr[0], tr[1], tr[2], kf, kg, kh);
+    double* T = P.gtrace + ((size_t)side * 2 + role) * 7 * NPT + pt;
+#pragma unroll
+    for (int v = 0; v < 7; ++v) T[(size_t)v * NPT] = n0 * kf[v] + n1 * kg[v] + n2 * kh[v];
+  }
+  // volume: primitive gradients of the node, contravariant viscous / resistive fluxes
+#pragma unroll
+  for (int d = 0; d < 3; ++d) mhd::to_grad_prim_rt(P, u, g[d]);
+  if (P.grad) {
+    double* G = P.grad + 27 * ((size_t)e * NP3 + t);
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int v = 0; v < NV9; ++v) G[9 * d + v] = g[d][v];
+  }
+  {
+    double f[7], gg[7], h[7];
+    mhd::visc_flux_3d(P, u, g[0], g[1], g[2], f, gg, h);
+#pragma unroll
+    for (int dir = 0; dir < 3; ++dir) {
+      const double m0 = M[(3 * dir + 0) * NP3], m1 = M[(3 * dir + 1) * NP3], m2 = M[(3 * dir + 2) * NP3];
+#pragma unroll
+      for (int v = 0; v < 7; ++v) sA[(7 * dir + v) * NP3 + t] = f[v] * m0 + gg[v] * m1 + h[v] * m2;
+    }
+  }
+  __syncthreads();
+  double r[7] = {0., 0., 0., 0., 0., 0., 0.};
+#pragma unroll
+  for (int l = 0; l < NP; ++l) {
+    const double a = sDhat[i * NP + l], b = sDhat[j * NP + l], c = sDhat[k * NP + l];
+#pragma unroll
+    for (int v = 0; v < 7; ++v)
+      r[v] += a * sA[v * NP3 + l + NP * (j + NP * k)] + b * sA[(7 + v) * NP3 + i + NP * (l + NP * k)] +
+              c * sA[(14 + v) * NP3 + i + NP * (j + NP * l)];
+  }
+  double* O = P.utvisc + (size_t)e * 7 * NP3 + t;
+#pragma unroll
+  for (int v = 0; v < 7; ++v) O[v * NP3] = r[v];
 }
 
 }  // namespace gauss

@@ -72,6 +72,7 @@ cudaError_t launch_gauss_prolong(int NP, bool ent, bool mhd, int nElems, cudaStr
 cudaError_t launch_gauss_lift_visc(int NP, int lift, int lv, int nElems, cudaStream_t s, const KParams& P);
 cudaError_t launch_gauss_surf(int NP, int vf, int nElems, cudaStream_t s, const KParams& P);
 cudaError_t launch_gauss_surf_mhd(int NP, int vf, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_gauss_mhd_lift_visc(int NP, int lift, int nElems, cudaStream_t s, const KParams& P);
 cudaError_t launch_nfvse_alpha(int NP, bool mhd, int nElems, cudaStream_t s, const KParams& P, double* scratch);
 // NFVSE_CORR: Apply_NFVSE_Correction of every element after a stage update with step b * dt (ut: the
 // stage's Ut to correct as well, or null); errKey records elem*8 + 5 for a safe state that is not admissible

@@ -94,8 +94,8 @@ __global__ void lift_flux_kernel(KParams P, int NP) {
   const int nM = side_node(NP - 1, pt % NP, pt / NP, 0, se5[2]);
   const int nS = side_node(NP - 1, pt % NP, pt / NP, se5[4], se5[3]);
   const size_t NP3 = (size_t)NP * NP * NP;
-  const double* UM = P.U + NV * ((size_t)se5[0] * NP3 + nM);
-  const double* US = P.U + NV * ((size_t)se5[1] * NP3 + nS);
+  const double* UM = P.uface ? P.uface + ((size_t)side * 2 * npts + pt) * NV : P.U + NV * ((size_t)se5[0] * NP3 + nM);
+  const double* US = P.uface ? P.uface + (((size_t)side * 2 + 1) * npts + pt) * NV : P.U + NV * ((size_t)se5[1] * NP3 + nS);
   double uM[NV], uS[NV], VM[NV], VS[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) { uM[v] = UM[v]; uS[v] = US[v]; }
