@@ -313,7 +313,11 @@ def run_fluxo(args):
             w.update(compute_alpha=3, shock_blend_coef=args.shock_blend)
         w.update(sub_fv_method=args.sub_fv, recons_boundaries=3 if args.sub_fv > 1 else 1,
                  nfvse_corr=1 if args.nfvse_corr else 0)
-        mesh = fb.box_mesh(w["N"], w["elems"], w["xmin"], w["xmax"], NGeo=w["NGeo"], deform_amp=w["deform_amp"])
+        nt = 1 if args.nodes == "gauss" else 2
+        if nt == 1:  # the NFVSE subcells need LGL nodes: the Gauss variant runs the pure DG scheme
+            w.update(nfvse=0, nfvse_corr=0, node_type=1)
+        mesh = fb.box_mesh(w["N"], w["elems"], w["xmin"], w["xmax"], NGeo=w["NGeo"], deform_amp=w["deform_amp"],
+                           node_type=nt)
         fields = {k: v for k, v in w.items() if k not in ("elems", "xmin", "xmax", "NGeo", "deform_amp")}
         op = fb.DGOperator(device=local, **fields)
         op.set_mesh(mesh)
@@ -408,15 +412,17 @@ def run_fluxo(args):
     per_kernel = None if (mhd or gauss) else kernel_rooflines(kinds, w["N"], nd, op.nElems, peak)
     falg_rhs = sum((MHD_FALG_PER_DOF if mhd else FALG_PER_DOF).values())
     if mhd:
-        alpha = op.alpha()
+        alpha = op.alpha() if w["nfvse"] else np.zeros(op.nElems)
         config = {"workload": "mhd_glm_resistive_orszag_tang_N%d_%dx%dx%d_curved" % ((w["N"],) + w["elems"]) +
+                  ("_gauss_nodes_no_nfvse" if gauss else "") +
                   ("" if args.shock_blend <= 0 else "_blend%g" % args.shock_blend) +
                   ("" if args.sub_fv == 1 else "_subfv%d" % args.sub_fv) + ("_corr" if args.nfvse_corr else ""),
                   "N": w["N"], "elements": list(w["elems"]), "dofs_per_gpu": nd, "riemann": 14, "volume_flux": 10,
                   "noncons": "powell", "lifting": "br1_entropy_var", "eta": w["eta"],
-                  "nfvse": ("indicator, alpha_max 0.5, alpha_min 0.01, 1 sweep" if args.shock_blend <= 0 else
-                            "fixed alpha %g (ComputeAlpha 3)" % args.shock_blend) +
-                           ", SubFVMethod %d" % args.sub_fv + (", NFVSE_CORR" if args.nfvse_corr else ""),
+                  "nfvse": "off (Gauss nodes)" if gauss else (
+                      ("indicator, alpha_max 0.5, alpha_min 0.01, 1 sweep" if args.shock_blend <= 0 else
+                       "fixed alpha %g (ComputeAlpha 3)" % args.shock_blend) +
+                      ", SubFVMethod %d" % args.sub_fv + (", NFVSE_CORR" if args.nfvse_corr else "")),
                   "blended_elements_last_rhs": int((alpha > 0).sum()), "time_disc": "carpenterrk4-5",
                   "rhs_per_step": 5, "parallelism": "replicas x%d" % world,
                   "l2": "inputs larger than L2 (state %d MB)" % (nd * 72 // 10 ** 6), "steps": args.steps}
@@ -841,7 +847,7 @@ def main():
     ap.add_argument("--sub-fv", type=int, default=1, choices=(1, 2, 3, 4), help="mhd: SubFVMethod")
     ap.add_argument("--nfvse-corr", action="store_true", help="mhd: NFVSE_CORR positivity correction")
     ap.add_argument("--nodes", default="lgl", choices=("lgl", "gauss"),
-                    help="tgv: Gauss-Lobatto (the headline) or Gauss nodes (PP_NodeType)")
+                    help="Gauss-Lobatto (the headline) or Gauss nodes (PP_NodeType; mhd: without NFVSE)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
