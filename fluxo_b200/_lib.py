@@ -17,7 +17,12 @@ ERRORS = {
     -4: "FLUXO_ENAN_STATE",
     -5: "FLUXO_ETIMEOUT",
     -6: "FLUXO_ENOTREADY",
+    -7: "FLUXO_EXCHANGE",
 }
+FLUXO_XCHG_STATE, FLUXO_XCHG_GTRACE, FLUXO_XCHG_DT = 1, 2, 3
+# fluxo_exchange_fn of include/fluxo_gpu.h: (ctx, what, stream, a, b) -> 0 or a failure
+EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                               ctypes.c_void_p)
 
 
 class FluxoError(RuntimeError):
@@ -96,7 +101,8 @@ EXPORTS = [
     "fluxo_gpu_last_error", "fluxo_gpu_set_profiling", "fluxo_gpu_get_profile", "fluxo_gpu_fp64_peak",
     "fluxo_host_box_sizes", "fluxo_host_box_mesh", "fluxo_host_box_mesh_gauss", "fluxo_host_hopr_mesh",
     "fluxo_host_exact_func", "fluxo_gpu_dg_time_derivative_noalloc",
-    "fluxo_gpu_set_glm_ch", "fluxo_gpu_get_glm_ch", "fluxo_gpu_get_alpha", "fluxo_gpu_set_alpha", "fluxo_gpu_volume_shape",
+    "fluxo_gpu_set_glm_ch", "fluxo_gpu_get_glm_ch", "fluxo_gpu_get_alpha", "fluxo_gpu_set_alpha",
+    "fluxo_gpu_set_partition", "fluxo_gpu_exchange_buffers", "fluxo_gpu_volume_shape",
     "fluxo_gpu_set_volume_shape", "fluxo_gpu_analyze", "fluxo_gpu_set_surf_metrics",
     "fluxo_batch_create", "fluxo_batch_add", "fluxo_batch_run", "fluxo_batch_status", "fluxo_batch_get_state",
     "fluxo_batch_set_state",
@@ -148,6 +154,8 @@ def load():
     lib.fluxo_gpu_get_glm_ch.argtypes = [vp, P(d)]
     lib.fluxo_gpu_get_alpha.argtypes = [vp, vp]
     lib.fluxo_gpu_set_alpha.argtypes = [vp, vp]
+    lib.fluxo_gpu_set_partition.argtypes = [vp, i, EXCHANGE_FN, vp]
+    lib.fluxo_gpu_exchange_buffers.argtypes = [vp, P(vp)]
     lib.fluxo_gpu_volume_shape.argtypes = [i, i, i, P(i), P(i), P(i), P(i)]
     lib.fluxo_gpu_set_volume_shape.argtypes = [i, i, i, i]
     lib.fluxo_gpu_analyze.argtypes = [vp, d, P(FluxoExact), vp, vp, vp, vp]

@@ -163,6 +163,11 @@ __global__ void rk_stage_kernel(RKStageArgs A) {
 struct fluxo_handle {
   fluxo_cfg cfg{};
   int N = 0, NP = 0, nElems = 0, nSides = 0;
+  // a partition of one solve over several handles: the first nOwn elements are this handle's, the
+  // others ghost copies of the neighbours that the exchange callback refreshes
+  int nOwn = 0;
+  fluxo_exchange_fn xfn = nullptr;
+  void* xctx = nullptr;
   int nVar = 5;                     // 5 (Euler / Navier-Stokes), 9 (MHD + GLM)
   bool mhd = false;
   double glmCh = 0., glmDtch1 = 0.;  // MHD: GLM_ch, GLM_dtch1 (from the metrics at set_mesh)
@@ -280,7 +285,7 @@ void build_basis_tables(int N, BasisTables& B) {
 KParams base_params(fluxo_handle* h) {
   KParams P{};
   const fluxo_cfg& c = h->cfg;
-  P.nElems = h->nElems; P.nSides = h->nSides;
+  P.nElems = h->nOwn; P.nSides = h->nSides;
   P.U = h->dU; P.Ut = h->dUt; P.UtTmp = h->dUtTmp; P.grad = nullptr; P.utvisc = h->dUtVisc;
   P.metrics = h->dMetrics; P.sJ = h->dsJ; P.facegeo = h->dFaceGeo; P.xGP = h->dXGP;
   P.s2e = h->dS2E; P.e2s = h->dE2S;
@@ -346,21 +351,32 @@ struct ProfScope {
   }
 };
 
+// The exchange callback of a partitioned solve (a no-op without one); a failure ends the call.
+int exchange(fluxo_handle* h, int what, void* a, void* b) {
+  if (!h->xfn) return FLUXO_OK;
+  const int r = h->xfn(h->xctx, what, (void*)h->stream, a, b);
+  if (r != 0) return fail(h, FLUXO_EXCHANGE, "exchange callback failed (what = " + std::to_string(what) + ")");
+  return FLUXO_OK;
+}
+
 // One DGTimeDerivative; stage 0 writes Ut, stage >= 1 applies the fused LSERK stage update.
 int rhs(fluxo_handle* h, KParams P) {
   cudaStream_t s = h->stream;
+  // a partitioned solve: the ghost elements' state from their owners (StartReceiveMPIData /
+  // StartSendMPIData of U_slave, dg.f90:342-356, here whole ghost elements)
+  if (int r = exchange(h, FLUXO_XCHG_STATE, h->dU, nullptr)) return r;
   if (h->mhd) {
     if (h->cfg.nfvse) {  // CalcBlendingCoefficient (dg.f90:358-361) and VolInt_NFVSE's FV part (:380-383)
       ProfScope ps(h, 5);
-      FLUXO_CUDA(h, launch_nfvse_alpha(h->NP, true, h->nElems, s, P, h->dAlphaTmp));
-      FLUXO_CUDA(h, launch_nfvse_fv(h->cfg.riemann, h->NP, h->nElems, h->nSMs, s, P));
+      FLUXO_CUDA(h, launch_nfvse_alpha(h->NP, true, h->nOwn, s, P, h->dAlphaTmp));
+      FLUXO_CUDA(h, launch_nfvse_fv(h->cfg.riemann, h->NP, h->nOwn, h->nSMs, s, P));
       h->launches += 3 + (h->cfg.space_prop_sweeps > 1 ? 2 * (h->cfg.space_prop_sweeps - 1) : 0);
     }
     if (h->gauss) {  // ProlongToFace_U (dg.f90:458-511), entropy-projected for Derigs / FloGor (10, 12)
       if (!h->surfMetSet) return fail(h, FLUXO_ENOTREADY, "Gauss nodes: SurfMetrics not set");
       const int vf = h->cfg.volume_flux;
       ProfScope ps(h, 2);
-      FLUXO_CUDA(h, launch_gauss_prolong(h->NP, vf == 10 || vf == 12, true, h->nElems, s, P));
+      FLUXO_CUDA(h, launch_gauss_prolong(h->NP, vf == 10 || vf == 12, true, h->nOwn, s, P));
       h->launches += 1;
     }
     if (h->visc) {
@@ -370,8 +386,8 @@ int rhs(fluxo_handle* h, KParams P) {
       }
       {
         ProfScope ps(h, 1);
-        if (h->gauss) FLUXO_CUDA(h, launch_gauss_mhd_lift_visc(h->NP, h->cfg.lifting, h->nElems, s, P));
-        else FLUXO_CUDA(h, launch_mhd_lift_visc(h->NP, h->cfg.lifting, h->nElems, s, P));
+        if (h->gauss) FLUXO_CUDA(h, launch_gauss_mhd_lift_visc(h->NP, h->cfg.lifting, h->nOwn, s, P));
+        else FLUXO_CUDA(h, launch_mhd_lift_visc(h->NP, h->cfg.lifting, h->nOwn, s, P));
       }
       h->launches += 2;
     }
@@ -381,22 +397,22 @@ int rhs(fluxo_handle* h, KParams P) {
     }
     if (h->gauss) {  // SurfInt with the split-form correction and the non-conservative terms
       ProfScope ps(h, 2);
-      FLUXO_CUDA(h, launch_gauss_surf_mhd(h->NP, h->cfg.volume_flux, h->nElems, s, P));
+      FLUXO_CUDA(h, launch_gauss_surf_mhd(h->NP, h->cfg.volume_flux, h->nOwn, s, P));
       h->launches += 1;
     }
     {
       ProfScope ps(h, 3);
       const int vf = h->cfg.volume_flux;
-      FLUXO_CUDA(h, (vf == 10 || vf == 12) ? launch_mhd_volume_ec(h->NP, vf, h->nElems, s, P)
-                                           : launch_mhd_volume_std(h->NP, vf, h->nElems, s, P));
+      FLUXO_CUDA(h, (vf == 10 || vf == 12) ? launch_mhd_volume_ec(h->NP, vf, h->nOwn, s, P)
+                                           : launch_mhd_volume_std(h->NP, vf, h->nOwn, s, P));
     }
     h->launches += 2;
     return FLUXO_OK;
   }
   if (h->cfg.nfvse) {  // CalcBlendingCoefficient (dg.f90:358-361) and VolInt_NFVSE's FV part (:380-383)
     ProfScope ps(h, 5);
-    FLUXO_CUDA(h, launch_nfvse_alpha(h->NP, false, h->nElems, s, P, h->dAlphaTmp));
-    FLUXO_CUDA(h, launch_nfvse_fv_ns(h->cfg.riemann, h->NP, h->nElems, h->nSMs, s, P));
+    FLUXO_CUDA(h, launch_nfvse_alpha(h->NP, false, h->nOwn, s, P, h->dAlphaTmp));
+    FLUXO_CUDA(h, launch_nfvse_fv_ns(h->cfg.riemann, h->NP, h->nOwn, h->nSMs, s, P));
     h->launches += 3 + (h->cfg.space_prop_sweeps > 1 ? 2 * (h->cfg.space_prop_sweeps - 1) : 0);
   }
   if (h->gauss) {  // ProlongToFace_U (dg.f90:458-511): interpolated (entropy-projected) face states
@@ -404,7 +420,7 @@ int rhs(fluxo_handle* h, KParams P) {
     const int vf = h->cfg.volume_flux;
     const bool ent = vf == 5 || vf == 6 || vf == 7 || vf == 10 || vf == 32;  // equation.f90:413-455
     ProfScope ps(h, 2);
-    FLUXO_CUDA(h, launch_gauss_prolong(h->NP, ent, false, h->nElems, s, P));
+    FLUXO_CUDA(h, launch_gauss_prolong(h->NP, ent, false, h->nOwn, s, P));
     h->launches += 1;
   }
   if (h->visc) {
@@ -414,10 +430,12 @@ int rhs(fluxo_handle* h, KParams P) {
     }
     {
       ProfScope ps(h, 1);
-      if (h->gauss) FLUXO_CUDA(h, launch_gauss_lift_visc(h->NP, h->cfg.lifting, h->cfg.lifting_var, h->nElems, s, P));
-      else FLUXO_CUDA(h, launch_gradient(h->NP, h->nElems, s, P));
+      if (h->gauss) FLUXO_CUDA(h, launch_gauss_lift_visc(h->NP, h->cfg.lifting, h->cfg.lifting_var, h->nOwn, s, P));
+      else FLUXO_CUDA(h, launch_gradient(h->NP, h->nOwn, s, P));
     }
     h->launches += 2;
+    // the ghost sides' shares n.F_v of the viscous face flux (the gradient traces of br1.f90:154-364)
+    if (int r = exchange(h, FLUXO_XCHG_GTRACE, h->dGTrace, nullptr)) return r;
   }
   {
     ProfScope ps(h, 2);
@@ -425,16 +443,16 @@ int rhs(fluxo_handle* h, KParams P) {
   }
   if (h->gauss) {  // SurfInt with the split-form correction (surfint.f90:118-175)
     ProfScope ps(h, 2);
-    FLUXO_CUDA(h, launch_gauss_surf(h->NP, h->cfg.volume_flux, h->nElems, s, P));
+    FLUXO_CUDA(h, launch_gauss_surf(h->NP, h->cfg.volume_flux, h->nOwn, s, P));
     h->launches += 1;
   }
   if (volume_shape(h->NP, h->cfg.volume_flux, h->visc) < 0) {  // first RHS of this (N, flux, visc)
-    FLUXO_CUDA(h, tune_volume(h->NP, h->cfg.volume_flux, h->visc, h->nElems, s, P));
+    FLUXO_CUDA(h, tune_volume(h->NP, h->cfg.volume_flux, h->visc, h->nOwn, s, P));
     if (volume_shape_count(h->NP) > 1) h->launches += 4 * volume_shape_count(h->NP);
   }
   {
     ProfScope ps(h, 3);
-    FLUXO_CUDA(h, launch_volume(h->NP, h->cfg.volume_flux, h->visc, h->nElems, s, P));
+    FLUXO_CUDA(h, launch_volume(h->NP, h->cfg.volume_flux, h->visc, h->nOwn, s, P));
   }
   h->launches += 2;
   return FLUXO_OK;
@@ -468,7 +486,7 @@ int rk_step(fluxo_handle* h, double t, double dt, const double* dtDev, const int
   if (h->rk->type != RK_LSERKW2) {  // right-hand side into Ut, then the scheme's own stage update
     RKStageArgs A{};
     A.type = h->rk->type; A.nStages = h->nStages;
-    A.n = (size_t)h->nVar * h->NP * h->NP * h->NP * h->nElems;
+    A.n = (size_t)h->nVar * h->NP * h->NP * h->NP * h->nOwn;
     A.U = h->dU; A.Ut = h->dUt; A.R1 = h->dUtTmp; A.R2 = h->dUReg2;
     A.dtDev = dtDev; A.dt = dt; A.halt = halt;
     const int grid = h->nSMs * 8;
@@ -492,7 +510,7 @@ int rk_step(fluxo_handle* h, double t, double dt, const double* dtDev, const int
       FLUXO_CUDA(h, cudaGetLastError());
       h->launches += 1;
       if (corr) {
-        FLUXO_CUDA(h, launch_nfvse_corr(h->NP, h->mhd, h->nElems, h->stream, P, h->dUt, h->rk->b[st], errKey));
+        FLUXO_CUDA(h, launch_nfvse_corr(h->NP, h->mhd, h->nOwn, h->stream, P, h->dUt, h->rk->b[st], errKey));
         h->launches += 1;
         if (st >= 2 && st <= 4 && st < h->nStages) {
           A.part = 2;
@@ -511,7 +529,7 @@ int rk_step(fluxo_handle* h, double t, double dt, const double* dtDev, const int
     int r = rhs(h, P);
     if (r) return r;
     if (corr) {  // Ut is not kept by the fused stage update (the next stage recomputes it)
-      FLUXO_CUDA(h, launch_nfvse_corr(h->NP, h->mhd, h->nElems, h->stream, P, nullptr, h->RKb[st], errKey));
+      FLUXO_CUDA(h, launch_nfvse_corr(h->NP, h->mhd, h->nOwn, h->stream, P, nullptr, h->RKb[st], errKey));
       h->launches += 1;
     }
   }
@@ -690,6 +708,9 @@ int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* S2E, 
                          met, geo, rerr))
     return fail(h, FLUXO_EINVAL_CFG, "set_mesh: " + rerr);
   h->nElems = nElems; h->nSides = nSides;
+  h->nOwn = nElems;
+  h->xfn = nullptr;
+  h->xctx = nullptr;
   if (h->dAnaPartial) {  // sized by nElems at the next analysis
     cudaFree(h->dAnaPartial);
     h->dAnaPartial = nullptr;
@@ -854,9 +875,10 @@ int fluxo_gpu_calc_timestep(fluxo_handle* h, double* dt, int* errType) {
   KParams P = base_params(h);
   dt_reset_kernel<<<1, 1, 0, h->stream>>>(h->dDtBits, h->dErrKey);
   FLUXO_CUDA(h, cudaGetLastError());
-  if (h->mhd) FLUXO_CUDA(h, launch_mhd_timestep(h->NP, h->visc, h->nElems, h->stream, P, h->dDtBits, h->dErrKey));
-  else FLUXO_CUDA(h, launch_timestep(h->NP, h->visc, h->nElems, h->stream, P, h->dDtBits, h->dErrKey));
+  if (h->mhd) FLUXO_CUDA(h, launch_mhd_timestep(h->NP, h->visc, h->nOwn, h->stream, P, h->dDtBits, h->dErrKey));
+  else FLUXO_CUDA(h, launch_timestep(h->NP, h->visc, h->nOwn, h->stream, P, h->dDtBits, h->dErrKey));
   h->launches += 2;
+  if ((r = exchange(h, FLUXO_XCHG_DT, h->dDtBits, h->dErrKey))) return r;  // MPI_ALLREDUCE(MIN), calctimestep.f90:159-167
   unsigned long long bits = 0;
   int key = 0;
   FLUXO_CUDA(h, cudaMemcpyAsync(&bits, h->dDtBits, 8, cudaMemcpyDeviceToHost, h->stream));
@@ -913,9 +935,10 @@ int fluxo_gpu_time_disc(fluxo_handle* h, double t, double tEnd, int maxIter, dou
       P.haltFlag = &td->halt;
       {
         ProfScope ps(h, 4);
-        if (h->mhd) FLUXO_CUDA(h, launch_mhd_timestep(h->NP, h->visc, h->nElems, s, P, &td->dtBits, &td->errKey));
-        else FLUXO_CUDA(h, launch_timestep(h->NP, h->visc, h->nElems, s, P, &td->dtBits, &td->errKey));
+        if (h->mhd) FLUXO_CUDA(h, launch_mhd_timestep(h->NP, h->visc, h->nOwn, s, P, &td->dtBits, &td->errKey));
+        else FLUXO_CUDA(h, launch_timestep(h->NP, h->visc, h->nOwn, s, P, &td->dtBits, &td->errKey));
       }
+      if ((r = exchange(h, FLUXO_XCHG_DT, &td->dtBits, &td->errKey))) return r;
       td_finalize_kernel<<<1, 1, 0, s>>>(td);
       FLUXO_CUDA(h, cudaGetLastError());
       if ((r = rk_step(h, 0., 0., &td->dt, &td->halt, h->mhd ? &td->ch : nullptr, &td->errKey))) return r;
@@ -941,6 +964,7 @@ int fluxo_gpu_analyze(fluxo_handle* h, double t, const fluxo_exact* ex, double* 
                       double* scalars) {
   int r = check_ready(h);
   if (r) return r;
+  if (h->nOwn != h->nElems) return fail(h, FLUXO_EINVAL_CFG, "analyze: not on a partitioned handle");
   const int func = ex ? ex->func : 0;
   if (func != 0) {
     if (h->mhd) return fail(h, FLUXO_EINVAL_CFG, "analyze: error norms need an Euler / Navier-Stokes exact function");
@@ -1018,6 +1042,25 @@ int fluxo_gpu_get_glm_ch(fluxo_handle* h, double* ch) {
   if (!h || !ch) return FLUXO_EINVAL_CFG;
   if (!h->mhd) return fail(h, FLUXO_EINVAL_CFG, "GLM_ch exists for MHD only");
   *ch = h->glmCh;
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_set_partition(fluxo_handle* h, int nOwned, fluxo_exchange_fn fn, void* ctx) {
+  if (!h) return FLUXO_EINVAL_CFG;
+  if (!h->meshSet) return fail(h, FLUXO_ENOTREADY, "set_partition: mesh not set");
+  if (nOwned < 1 || nOwned > h->nElems) return fail(h, FLUXO_EINVAL_CFG, "set_partition: nOwned out of range");
+  if (h->mhd || h->gauss || h->cfg.nfvse)
+    return fail(h, FLUXO_EINVAL_CFG, "set_partition: Euler / Navier-Stokes on LGL nodes without NFVSE only");
+  h->nOwn = nOwned;
+  h->xfn = fn;
+  h->xctx = ctx;
+  return FLUXO_OK;
+}
+
+int fluxo_gpu_exchange_buffers(fluxo_handle* h, double** gtrace) {
+  if (!h || !gtrace) return FLUXO_EINVAL_CFG;
+  if (!h->meshSet) return fail(h, FLUXO_ENOTREADY, "exchange_buffers: mesh not set");
+  *gtrace = h->dGTrace;
   return FLUXO_OK;
 }
 

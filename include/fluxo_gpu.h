@@ -39,7 +39,8 @@ enum {
   FLUXO_ECUDA = -3,       /* CUDA runtime error (message in last_error) */
   FLUXO_ENAN_STATE = -4,  /* CALCTIMESTEP found an invalid state, see errType */
   FLUXO_ETIMEOUT = -5,    /* a bounded device wait expired */
-  FLUXO_ENOTREADY = -6    /* mesh or state not set */
+  FLUXO_ENOTREADY = -6,   /* mesh or state not set */
+  FLUXO_EXCHANGE = -7     /* the exchange callback of a partitioned solve reported a failure */
 };
 
 enum { FLUXO_EQN_EULER = 0, FLUXO_EQN_NAVIERSTOKES = 1, FLUXO_EQN_MHD = 2, FLUXO_EQN_MHD_PARABOLIC = 3 };
@@ -115,6 +116,22 @@ typedef struct fluxo_cfg {
 
 typedef struct fluxo_handle fluxo_handle;
 
+/* Exchange points of a partitioned solve (fluxo_gpu_set_partition).  The callback runs on the calling
+ * host thread and enqueues its work on `stream` (the handle's CUDA stream), in stream order with the
+ * handle's kernels; it returns 0, or nonzero to make the call fail with FLUXO_EXCHANGE.  Every handle of
+ * the solve reaches the same exchange points in the same order.
+ *   FLUXO_XCHG_STATE   a = U (device, [elem][node][var]): before each right-hand side, the ghost
+ *                      elements' U from their owners (dg.f90:342-356 exchanges U_slave of MPI sides;
+ *                      here whole ghost elements);
+ *   FLUXO_XCHG_GTRACE  a = the viscous face shares [side][master|slave][4][pt] (Navier-Stokes): after
+ *                      the lifting kernel, the ghost side's share of every partition side (the gradient
+ *                      traces of br1.f90:154-364);
+ *   FLUXO_XCHG_DT      a = dt bits (uint64, the IEEE bits of a non-negative double), b = error key
+ *                      (int32, INT_MAX = none): after CALCTIMESTEP, both reduced with MIN over the
+ *                      handles (MPI_ALLREDUCE, calctimestep.f90:159-167). */
+enum { FLUXO_XCHG_STATE = 1, FLUXO_XCHG_GTRACE = 2, FLUXO_XCHG_DT = 3 };
+typedef int (*fluxo_exchange_fn)(void* ctx, int what, void* stream, void* a, void* b);
+
 /* InitEquation + InitDGbasis + InitTimeDisc equivalent.
  * Replaces: src/equation/navierstokes/equation.f90:162 InitEquation,
  *           src/dg/dg.f90:61 InitDG / :181 InitDGbasis,
@@ -174,6 +191,20 @@ int fluxo_gpu_time_disc(fluxo_handle* h, double t, double tEnd, int maxIter, dou
  * GLM_scale*GLM_dtch1/dt (src/equation/mhd/calctimestep.f90:175-177, InitTimeStep_GLM :187-223). */
 int fluxo_gpu_set_glm_ch(fluxo_handle* h, double ch);
 int fluxo_gpu_get_glm_ch(fluxo_handle* h, double* ch);
+
+/* One solve over several handles (one per GPU, or several on one GPU): this handle's mesh holds its
+ * nOwned elements first and then ghost copies of the neighbouring elements of other handles, its sides
+ * are every side of an owned element (both elements of each present), and the element kernels,
+ * CALCTIMESTEP and the stage updates run over the owned elements only.  Both handles of a partition
+ * side compute its flux from the same two states, so fluxes need no exchange.  `fn(ctx, ...)` is called
+ * at the exchange points above; the caller moves the data (NCCL, peer copies).  Euler / Navier-Stokes on
+ * LGL nodes without NFVSE; fluxo_gpu_analyze and the batch entry points are not available on a
+ * partitioned handle.  A later fluxo_gpu_set_mesh removes the partition.
+ * Replaces the single-process part of the reference's MPI decomposition (mesh_readin.f90:246-292
+ * offsetElemMPI, prepare_mesh.f90 MPI sides, dg.f90:342-442 the exchanges). */
+int fluxo_gpu_set_partition(fluxo_handle* h, int nOwned, fluxo_exchange_fn fn, void* ctx);
+/* Device buffer of the FLUXO_XCHG_GTRACE exchange (NULL without parabolic terms). */
+int fluxo_gpu_exchange_buffers(fluxo_handle* h, double** gtrace);
 
 /* NFVSE: MOD_NFVSE_Vars::alpha(nElems), the blending coefficients of the last right-hand side
  * (src/shockcapturing/nfvse_vars.f90). */

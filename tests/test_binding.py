@@ -143,6 +143,8 @@ def test_structs_match(name, ctype):
 def compatible(ctype, kind, value):
     if ctype in ("int", "double", "size_t"):
         return value and kind == C_SCALAR[ctype][0]
+    if ctype == "fluxo_exchange_fn":  # a C function pointer passed by value
+        return value and kind == "C_FUNPTR"
     if ctype.endswith("**"):
         return kind == "C_PTR" and not value
     base = ctype[:-1]

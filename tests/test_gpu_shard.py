@@ -1,0 +1,96 @@
+"""One solve partitioned over several handles, run on one GPU: each handle owns a contiguous element range
+(the reference's offsetElemMPI) plus ghost copies of its neighbours, and the library calls the exchange
+callback for the ghost states, the viscous face shares of the partition sides and the global dt.  Here
+the handles share one GPU and exchange through host threads (ThreadExchange: each handle's thread waits
+for its own stream and meets the others at a barrier; no kernel waits for another handle).  The owned
+rows of Ut and of the states after device-resident time steps equal those of one handle on the whole
+mesh (same arithmetic on the same data: to 1e-15)."""
+import threading
+
+import numpy as np
+import pytest
+
+import fluxo_b200 as fb
+from fluxo_b200 import _lib
+from fluxo_b200.shard import ShardedOperator, ThreadExchange
+
+pytestmark = pytest.mark.gpu
+
+
+def run_threads(n, fn, timeout=600):
+    errs = [None] * n
+
+    def work(i):
+        try:
+            fn(i)
+        except Exception as ex:  # re-raised in the test thread
+            errs[i] = ex
+
+    th = [threading.Thread(target=work, args=(i,)) for i in range(n)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout)
+    assert not any(t.is_alive() for t in th), "a rank did not finish"
+    for e in errs:
+        if e is not None:
+            raise e
+
+
+def setup(n_ranks, ne=(4, 3, 3), N=3, **kw):
+    fields = dict(N=N, eqn=1, riemann=44, volume_flux=5, lifting=1, lifting_var=3, mu0=0.01, kappa=1.4,
+                  cfl_scale=0.6, dfl_scale=0.5, time_disc=0, ini_exact_func=1)
+    fields.update(kw)
+    mesh = fb.box_mesh(N, ne, (-1, -1, -1), (1, 1, 1), NGeo=2, deform_amp=0.1)
+    U0 = fb.exact_func(2, 0.0, mesh["Elem_xGP"], adv_vel=(0.3, -0.2, 0.5), amplitude=0.3)
+    U0 = U0 * (1 + 0.02 * np.random.default_rng(3).standard_normal(U0.shape))
+    ref = fb.DGOperator(**fields)
+    ref.set_mesh(mesh)
+    ref.set_state(U0)
+    hub = ThreadExchange(n_ranks)
+    shards = [ShardedOperator(mesh, n_ranks, r, hub.rank, **fields) for r in range(n_ranks)]
+    for s in shards:
+        s.set_state(U0)
+    return ref, shards, U0
+
+
+def gather(shards, what):
+    return np.concatenate([getattr(s, what)() for s in shards])
+
+
+CASES = [dict(n=2), dict(n=3), dict(n=2, eqn=0), dict(n=4, lifting=2, lifting_var=2), dict(n=3, riemann=1, volume_flux=10),
+         dict(n=2, N=7, ne=(3, 2, 2)), dict(n=5, N=2, ne=(5, 2, 2), time_disc=8)]
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "_".join("%s%s" % kv for kv in c.items()))
+def test_partitioned_rhs_and_steps_match_one_handle(gpu_lib, case):
+    case = dict(case)
+    n = case.pop("n")
+    ref, shards, U0 = setup(n, **case)
+    ref.dg_time_derivative(0.0)
+    Ut = ref.get_ut()
+    run_threads(n, lambda i: shards[i].op.dg_time_derivative(0.0))
+    Uts = gather(shards, "get_ut")
+    assert np.abs(Uts - Ut).max() <= 1e-15 * np.abs(Ut).max()
+    # CALCTIMESTEP with the dt reduction, then device-resident steps of the TimeDisc loop
+    dt_ref, _ = ref.calc_timestep()
+    dts = [None] * n
+    run_threads(n, lambda i: dts.__setitem__(i, shards[i].op.calc_timestep()))
+    assert all(d[0] == dt_ref and d[1] == 0 for d in dts)
+    t_ref, n_ref, _ = ref.time_disc(0.0, 1e30, 12)
+    res = [None] * n
+    run_threads(n, lambda i: res.__setitem__(i, shards[i].op.time_disc(0.0, 1e30, 12)))
+    assert all(r[0] == t_ref and r[1] == n_ref and r[2] == 0 for r in res)
+    U = ref.get_state()
+    Us = gather(shards, "get_state")
+    assert np.abs(Us - U).max() <= 1e-14 * np.abs(U).max()
+    for s in shards:
+        s.close()
+
+
+def test_partition_restrictions(gpu_lib):
+    mesh = fb.box_mesh(3, (2, 2, 2), (-1, -1, -1), (1, 1, 1))
+    op = fb.DGOperator(N=3, eqn=2, riemann=11, volume_flux=10, kappa=5 / 3)
+    op.set_mesh(mesh)
+    with pytest.raises(fb.FluxoError):
+        _lib.check(op.lib.fluxo_gpu_set_partition(op.h, 4, _lib.EXCHANGE_FN(lambda *a: 0), None), op.h)
