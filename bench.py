@@ -327,17 +327,28 @@ def run_fluxo(args):
         nt = 1 if args.nodes == "gauss" else 2
         mesh = fb.box_mesh(w["N"], w["elems"], w["xmin"], w["xmax"], NGeo=w["NGeo"], deform_amp=w["deform_amp"],
                            node_type=nt)
-        op = fb.DGOperator(N=w["N"], eqn=1, riemann=w["riemann"], volume_flux=w["volume_flux"], lifting=1,
-                           lifting_var=3, visc=0, mu0=w["mu0"], Pr=w["Pr"], kappa=w["kappa"],
-                           cfl_scale=w["cfl_scale"], dfl_scale=w["dfl_scale"], time_disc=0, device=local,
-                           node_type=nt)
-        op.set_mesh(mesh)
+        tgv_fields = dict(N=w["N"], eqn=1, riemann=w["riemann"], volume_flux=w["volume_flux"], lifting=1,
+                          lifting_var=3, visc=0, mu0=w["mu0"], Pr=w["Pr"], kappa=w["kappa"],
+                          cfl_scale=w["cfl_scale"], dfl_scale=w["dfl_scale"], time_disc=0, node_type=nt)
         U0 = fb.exact_func(7, 0.0, mesh["Elem_xGP"], kappa=w["kappa"])
+        if args.shard and world > 1:  # one solve over the ranks: owned elements + ghosts, NCCL exchanges
+            from fluxo_b200.shard import DistExchange, ShardedOperator
+
+            shard = ShardedOperator(mesh, world, rank, DistExchange, device=local, **tgv_fields)
+            op = shard.op
+            U0 = shard.part.local_state(U0)
+            nd_total = int(np.prod(w["elems"])) * (w["N"] + 1) ** 3
+        else:
+            op = fb.DGOperator(device=local, **tgv_fields)
+            op.set_mesh(mesh)
     del mesh
     op.set_state(U0)
     setup_s = time.time() - t0
     nvar = 9 if mhd else 5
-    nd = op.nElems * (w["N"] + 1) ** 3
+    sharded = args.shard and world > 1 and not mhd
+    nd = (shard.part.n_owned if sharded else op.nElems) * (w["N"] + 1) ** 3
+    if sharded:
+        args.no_e2e, args.no_mix, args.no_cpu = True, True, True
     _, _, stream_ptr = op.device_buffers()
     stream = torch.cuda.ExternalStream(stream_ptr, device=dev)
     peak = fp64_peak(local)
@@ -369,7 +380,7 @@ def run_fluxo(args):
     set_profiling(op, False)
     ms_max = max_over_ranks(ms, world, dev)
     rhs = 5 * args.steps
-    value = ms_max * 1e6 / (world * nd * rhs)
+    value = ms_max * 1e6 / ((nd_total if sharded else world * nd) * rhs)
 
     # ---- end-to-end through the public API with pinned host buffers ----
     e2e = None
@@ -409,7 +420,7 @@ def run_fluxo(args):
     gauss = args.nodes == "gauss"
     # Gauss nodes: the face pass also holds the prolongation and the surface kernel, so the per-kernel and
     # whole-RHS fractions (F_alg of the LGL scheme) do not apply
-    per_kernel = None if (mhd or gauss) else kernel_rooflines(kinds, w["N"], nd, op.nElems, peak)
+    per_kernel = None if (mhd or gauss or sharded) else kernel_rooflines(kinds, w["N"], nd, op.nElems, peak)
     falg_rhs = sum((MHD_FALG_PER_DOF if mhd else FALG_PER_DOF).values())
     if mhd:
         alpha = op.alpha() if w["nfvse"] else np.zeros(op.nElems)
@@ -428,12 +439,16 @@ def run_fluxo(args):
                   "l2": "inputs larger than L2 (state %d MB)" % (nd * 72 // 10 ** 6), "steps": args.steps}
     else:
         config = config_dict(w, world, args.steps)
+        if sharded:
+            config["parallelism"] = "one solve over %d GPUs (contiguous element ranges + ghost elements, NCCL)" % world
+            config["dofs_per_gpu"] = nd
         if gauss:
             config["workload"] += "_gauss_nodes"
             config["nodes"] = "Gauss (entropy-projected face states, FluxB surface correction)"
     line = {"metric": MHD_METRIC if mhd else METRIC, "value": value, "unit": "ns/DOF/RHS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
-            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "higher_is_better": False, "scaling": "strong" if sharded else "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
             "config": config, "roofline": roofline, "roofline_kernels": per_kernel, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clk.summary(),
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kinds.items()},
@@ -846,6 +861,8 @@ def main():
                     help="mhd: fixed blending coefficient (ComputeAlpha 3) instead of the indicator")
     ap.add_argument("--sub-fv", type=int, default=1, choices=(1, 2, 3, 4), help="mhd: SubFVMethod")
     ap.add_argument("--nfvse-corr", action="store_true", help="mhd: NFVSE_CORR positivity correction")
+    ap.add_argument("--shard", action="store_true",
+                    help="tgv with --gpus > 1: one solve over the GPUs (strong scaling) instead of replicas")
     ap.add_argument("--nodes", default="lgl", choices=("lgl", "gauss"),
                     help="Gauss-Lobatto (the headline) or Gauss nodes (PP_NodeType; mhd: without NFVSE)")
     ap.add_argument("--no-e2e", action="store_true")

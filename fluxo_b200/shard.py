@@ -20,14 +20,13 @@ between the handles' kernels).
 
 from __future__ import annotations
 
-import ctypes
 import threading
 import traceback
 
 import numpy as np
 
 from . import _lib
-from .solver import MESH_KEYS, DGOperator
+from .solver import DGOperator
 
 VOLUME_KEYS = ("Metrics_fTilde", "Metrics_gTilde", "Metrics_hTilde", "sJ", "Elem_xGP")
 FACE_KEYS = ("NormVec", "TangVec1", "TangVec2", "SurfElem")
@@ -185,16 +184,19 @@ class DistExchange(_Exchange):
         import torch
         import torch.distributed as dist
 
-        reqs, recvs = [], []
+        # one group of all sends and receives (ncclGroupStart/End under NCCL: separate point-to-point calls
+        # between two ranks that both send first would wait on each other)
+        ops, recvs = [], []
         for q, ix in self.idx.items():
             if ix[send_key].numel():
-                reqs.append(dist.isend(X.index_select(0, ix[send_key]).contiguous(), q))
+                ops.append(dist.P2POp(dist.isend, X.index_select(0, ix[send_key]).contiguous(), q))
             if ix[recv_key].numel():
                 buf = torch.empty((ix[recv_key].numel(), X.shape[1]), dtype=X.dtype, device=X.device)
-                reqs.append(dist.irecv(buf, q))
+                ops.append(dist.P2POp(dist.irecv, buf, q))
                 recvs.append((ix[recv_key], buf))
-        for r in reqs:
-            r.wait()
+        if ops:
+            for r in dist.batch_isend_irecv(ops):
+                r.wait()
         for rows, buf in recvs:
             X.index_copy_(0, rows, buf)
 

@@ -5,6 +5,8 @@ the handles share one GPU and exchange through host threads (ThreadExchange: eac
 for its own stream and meets the others at a barrier; no kernel waits for another handle).  The owned
 rows of Ut and of the states after device-resident time steps equal those of one handle on the whole
 mesh (same arithmetic on the same data: to 1e-15)."""
+import os
+import socket
 import threading
 
 import numpy as np
@@ -94,3 +96,45 @@ def test_partition_restrictions(gpu_lib):
     op.set_mesh(mesh)
     with pytest.raises(fb.FluxoError):
         _lib.check(op.lib.fluxo_gpu_set_partition(op.h, 4, _lib.EXCHANGE_FN(lambda *a: 0), None), op.h)
+
+
+def _nccl_rank(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+
+    from fluxo_b200.shard import DistExchange
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.cuda.set_device(0)
+    import datetime
+
+    dist.init_process_group("nccl", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        ref, _, U0 = setup(1, ne=(3, 2, 2))
+        mesh = fb.box_mesh(3, (3, 2, 2), (-1, -1, -1), (1, 1, 1), NGeo=2, deform_amp=0.1)
+        sh = ShardedOperator(mesh, world, rank, DistExchange, N=3, eqn=1, riemann=44, volume_flux=5, lifting=1,
+                             lifting_var=3, mu0=0.01, kappa=1.4, cfl_scale=0.6, dfl_scale=0.5, time_disc=0,
+                             ini_exact_func=1)
+        sh.set_state(U0)
+        t1, n1, e1 = sh.op.time_disc(0.0, 1e30, 5)
+        t0, n0, e0 = ref.time_disc(0.0, 1e30, 5)
+        out[rank] = (t1 == t0 and n1 == n0 and e1 == e0 == 0, float(np.abs(sh.get_state() - ref.get_state()).max()))
+        sh.close()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+def test_nccl_exchange_path_one_rank(gpu_lib):
+    """The torch.distributed transport under NCCL through the library's callback (one rank on one GPU: the
+    dt all-reduce and an empty halo); several GPUs are not available to these tests."""
+    import torch.multiprocessing as mp
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    with mp.get_context("spawn").Manager() as m:
+        out = m.dict()
+        mp.spawn(_nccl_rank, args=(1, port, out), nprocs=1, join=True)
+        ok, diff = out[0]
+    assert ok and diff == 0.0

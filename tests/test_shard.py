@@ -124,7 +124,7 @@ def _rank(rank, world, port, out):
 @pytest.mark.timeout(180)
 @pytest.mark.parametrize("world", [2, 3])
 def test_gloo_exchange(world):
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_rank, args=(world, _free_port(), out), nprocs=world, join=True)
         res = dict(out)
