@@ -390,6 +390,7 @@ int rhs(fluxo_handle* h, KParams P) {
         else FLUXO_CUDA(h, launch_mhd_lift_visc(h->NP, h->cfg.lifting, h->nOwn, s, P));
       }
       h->launches += 2;
+      if (int r = exchange(h, FLUXO_XCHG_GTRACE, h->dGTrace, nullptr)) return r;  // the ghost sides' shares
     }
     {
       ProfScope ps(h, 2);
@@ -1049,11 +1050,22 @@ int fluxo_gpu_set_partition(fluxo_handle* h, int nOwned, fluxo_exchange_fn fn, v
   if (!h) return FLUXO_EINVAL_CFG;
   if (!h->meshSet) return fail(h, FLUXO_ENOTREADY, "set_partition: mesh not set");
   if (nOwned < 1 || nOwned > h->nElems) return fail(h, FLUXO_EINVAL_CFG, "set_partition: nOwned out of range");
-  if (h->mhd || h->gauss || h->cfg.nfvse)
-    return fail(h, FLUXO_EINVAL_CFG, "set_partition: Euler / Navier-Stokes on LGL nodes without NFVSE only");
+  if (h->gauss || h->cfg.nfvse)
+    return fail(h, FLUXO_EINVAL_CFG, "set_partition: LGL nodes without NFVSE only");
   h->nOwn = nOwned;
   h->xfn = fn;
   h->xctx = ctx;
+  if (h->mhd) {  // GLM_dtch1 of the whole mesh: MIN over the handles (InitTimeStep_GLM's MPI_ALLREDUCE)
+    unsigned long long bits;
+    const int none = INT_MAX;
+    std::memcpy(&bits, &h->glmDtch1, 8);
+    FLUXO_CUDA(h, cudaMemcpyAsync(h->dDtBits, &bits, 8, cudaMemcpyHostToDevice, h->stream));
+    FLUXO_CUDA(h, cudaMemcpyAsync(h->dErrKey, &none, 4, cudaMemcpyHostToDevice, h->stream));
+    if (int r = exchange(h, FLUXO_XCHG_DT, h->dDtBits, h->dErrKey)) return r;
+    FLUXO_CUDA(h, cudaMemcpyAsync(&bits, h->dDtBits, 8, cudaMemcpyDeviceToHost, h->stream));
+    FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
+    std::memcpy(&h->glmDtch1, &bits, 8);
+  }
   return FLUXO_OK;
 }
 

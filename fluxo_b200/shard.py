@@ -153,7 +153,8 @@ class _Exchange:
         import torch
 
         np3 = self.npts ** 3
-        nst, ngt = self.n_local * self.nvar * np3, 2 * self.n_sides * 4 * self.npts ** 2
+        nvisc = 7 if self.nvar == 9 else 4  # n.F_v components per face point (MHD: variables 2..8)
+        nst, ngt = self.n_local * self.nvar * np3, 2 * self.n_sides * nvisc * self.npts ** 2
 
         def cb(ctx, what, stream, a, b):
             try:

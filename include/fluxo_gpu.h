@@ -123,12 +123,13 @@ typedef struct fluxo_handle fluxo_handle;
  *   FLUXO_XCHG_STATE   a = U (device, [elem][node][var]): before each right-hand side, the ghost
  *                      elements' U from their owners (dg.f90:342-356 exchanges U_slave of MPI sides;
  *                      here whole ghost elements);
- *   FLUXO_XCHG_GTRACE  a = the viscous face shares [side][master|slave][4][pt] (Navier-Stokes): after
- *                      the lifting kernel, the ghost side's share of every partition side (the gradient
- *                      traces of br1.f90:154-364);
+ *   FLUXO_XCHG_GTRACE  a = the viscous face shares [side][master|slave][nv][pt] (nv = 4 Navier-Stokes,
+ *                      7 MHD): after the lifting kernel, the ghost side's share of every partition side
+ *                      (the gradient traces of br1.f90:154-364);
  *   FLUXO_XCHG_DT      a = dt bits (uint64, the IEEE bits of a non-negative double), b = error key
  *                      (int32, INT_MAX = none): after CALCTIMESTEP, both reduced with MIN over the
- *                      handles (MPI_ALLREDUCE, calctimestep.f90:159-167). */
+ *                      handles (MPI_ALLREDUCE, calctimestep.f90:159-167); for MHD also once inside
+ *                      fluxo_gpu_set_partition, with a = the bits of GLM_dtch1. */
 enum { FLUXO_XCHG_STATE = 1, FLUXO_XCHG_GTRACE = 2, FLUXO_XCHG_DT = 3 };
 typedef int (*fluxo_exchange_fn)(void* ctx, int what, void* stream, void* a, void* b);
 
@@ -197,9 +198,10 @@ int fluxo_gpu_get_glm_ch(fluxo_handle* h, double* ch);
  * are every side of an owned element (both elements of each present), and the element kernels,
  * CALCTIMESTEP and the stage updates run over the owned elements only.  Both handles of a partition
  * side compute its flux from the same two states, so fluxes need no exchange.  `fn(ctx, ...)` is called
- * at the exchange points above; the caller moves the data (NCCL, peer copies).  Euler / Navier-Stokes on
- * LGL nodes without NFVSE; fluxo_gpu_analyze and the batch entry points are not available on a
- * partitioned handle.  A later fluxo_gpu_set_mesh removes the partition.
+ * at the exchange points above; the caller moves the data (NCCL, peer copies).  LGL nodes without NFVSE
+ * (Euler, Navier-Stokes, MHD; for MHD this call is itself collective: it reduces GLM_dtch1);
+ * fluxo_gpu_analyze and the batch entry points are not available on a partitioned handle.  A later
+ * fluxo_gpu_set_mesh removes the partition.
  * Replaces the single-process part of the reference's MPI decomposition (mesh_readin.f90:246-292
  * offsetElemMPI, prepare_mesh.f90 MPI sides, dg.f90:342-442 the exchanges). */
 int fluxo_gpu_set_partition(fluxo_handle* h, int nOwned, fluxo_exchange_fn fn, void* ctx);

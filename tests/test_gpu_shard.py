@@ -39,20 +39,35 @@ def run_threads(n, fn, timeout=600):
             raise e
 
 
-def setup(n_ranks, ne=(4, 3, 3), N=3, **kw):
+MHD_FIELDS = dict(eqn=3, riemann=14, volume_flux=10, kappa=5 / 3, mu0=0.005, eta=0.01, lifting=1, lifting_var=3,
+                  noncons=1, glm_scale=0.5)
+
+
+def setup(n_ranks, ne=(4, 3, 3), N=3, mhd=False, **kw):
     fields = dict(N=N, eqn=1, riemann=44, volume_flux=5, lifting=1, lifting_var=3, mu0=0.01, kappa=1.4,
                   cfl_scale=0.6, dfl_scale=0.5, time_disc=0, ini_exact_func=1)
+    if mhd:
+        fields.update(MHD_FIELDS)
     fields.update(kw)
     mesh = fb.box_mesh(N, ne, (-1, -1, -1), (1, 1, 1), NGeo=2, deform_amp=0.1)
-    U0 = fb.exact_func(2, 0.0, mesh["Elem_xGP"], adv_vel=(0.3, -0.2, 0.5), amplitude=0.3)
+    if mhd:
+        from fluxo_b200.workloads import mhd_orszag_tang_state
+
+        U0 = mhd_orszag_tang_state(mesh["Elem_xGP"], kappa=5 / 3)
+    else:
+        U0 = fb.exact_func(2, 0.0, mesh["Elem_xGP"], adv_vel=(0.3, -0.2, 0.5), amplitude=0.3)
     U0 = U0 * (1 + 0.02 * np.random.default_rng(3).standard_normal(U0.shape))
     ref = fb.DGOperator(**fields)
     ref.set_mesh(mesh)
     ref.set_state(U0)
     hub = ThreadExchange(n_ranks)
-    shards = [ShardedOperator(mesh, n_ranks, r, hub.rank, **fields) for r in range(n_ranks)]
-    for s in shards:
-        s.set_state(U0)
+    shards = [None] * n_ranks
+
+    def make(r):  # MHD: set_partition reduces GLM_dtch1 over the ranks, so the ranks build together
+        shards[r] = ShardedOperator(mesh, n_ranks, r, hub.rank, **fields)
+        shards[r].set_state(U0)
+
+    run_threads(n_ranks, make)
     return ref, shards, U0
 
 
@@ -61,7 +76,8 @@ def gather(shards, what):
 
 
 CASES = [dict(n=2), dict(n=3), dict(n=2, eqn=0), dict(n=4, lifting=2, lifting_var=2), dict(n=3, riemann=1, volume_flux=10),
-         dict(n=2, N=7, ne=(3, 2, 2)), dict(n=5, N=2, ne=(5, 2, 2), time_disc=8)]
+         dict(n=2, N=7, ne=(3, 2, 2)), dict(n=5, N=2, ne=(5, 2, 2), time_disc=8),
+         dict(n=2, mhd=True), dict(n=3, mhd=True, N=4, lifting=2), dict(n=2, mhd=True, eqn=2, riemann=10)]
 
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: "_".join("%s%s" % kv for kv in c.items()))
@@ -73,16 +89,19 @@ def test_partitioned_rhs_and_steps_match_one_handle(gpu_lib, case):
     Ut = ref.get_ut()
     run_threads(n, lambda i: shards[i].op.dg_time_derivative(0.0))
     Uts = gather(shards, "get_ut")
-    assert np.abs(Uts - Ut).max() <= 1e-15 * np.abs(Ut).max()
+    assert np.abs(Uts - Ut).max() <= 1e-15 * np.abs(Ut).max(), np.abs(Uts - Ut).max()
     # CALCTIMESTEP with the dt reduction, then device-resident steps of the TimeDisc loop
     dt_ref, _ = ref.calc_timestep()
     dts = [None] * n
     run_threads(n, lambda i: dts.__setitem__(i, shards[i].op.calc_timestep()))
     assert all(d[0] == dt_ref and d[1] == 0 for d in dts)
-    t_ref, n_ref, _ = ref.time_disc(0.0, 1e30, 12)
+    if case.get("mhd"):
+        assert all(s.op.glm_ch == ref.glm_ch for s in shards)
+    t_ref, n_ref, e_ref = ref.time_disc(0.0, 1e30, 12)
     res = [None] * n
     run_threads(n, lambda i: res.__setitem__(i, shards[i].op.time_disc(0.0, 1e30, 12)))
-    assert all(r[0] == t_ref and r[1] == n_ref and r[2] == 0 for r in res)
+    assert e_ref == 0 and n_ref == 12
+    assert all(r == (t_ref, n_ref, e_ref) for r in res), (t_ref, n_ref, res)
     U = ref.get_state()
     Us = gather(shards, "get_state")
     assert np.abs(Us - U).max() <= 1e-14 * np.abs(U).max()
@@ -92,7 +111,7 @@ def test_partitioned_rhs_and_steps_match_one_handle(gpu_lib, case):
 
 def test_partition_restrictions(gpu_lib):
     mesh = fb.box_mesh(3, (2, 2, 2), (-1, -1, -1), (1, 1, 1))
-    op = fb.DGOperator(N=3, eqn=2, riemann=11, volume_flux=10, kappa=5 / 3)
+    op = fb.DGOperator(N=3, eqn=0, riemann=44, volume_flux=5, nfvse=1)
     op.set_mesh(mesh)
     with pytest.raises(fb.FluxoError):
         _lib.check(op.lib.fluxo_gpu_set_partition(op.h, 4, _lib.EXCHANGE_FN(lambda *a: 0), None), op.h)
