@@ -19,7 +19,7 @@ ERRORS = {
     -6: "FLUXO_ENOTREADY",
     -7: "FLUXO_EXCHANGE",
 }
-FLUXO_XCHG_STATE, FLUXO_XCHG_GTRACE, FLUXO_XCHG_DT = 1, 2, 3
+FLUXO_XCHG_STATE, FLUXO_XCHG_GTRACE, FLUXO_XCHG_DT, FLUXO_XCHG_ALPHA = 1, 2, 3, 4
 # fluxo_exchange_fn of include/fluxo_gpu.h: (ctx, what, stream, a, b) -> 0 or a failure
 EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                ctypes.c_void_p)

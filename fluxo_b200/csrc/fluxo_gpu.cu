@@ -359,6 +359,31 @@ int exchange(fluxo_handle* h, int what, void* a, void* b) {
   return FLUXO_OK;
 }
 
+// CalcBlendingCoefficient with PropagateBlendingCoeff (nfvse.f90:1537-1620, nfvse_mpi.f90:62-131); a
+// partitioned solve exchanges the ghost elements' coefficients before every propagation sweep
+int nfvse_alpha(fluxo_handle* h, const KParams& P, cudaStream_t s) {
+  if (!h->xfn) {
+    FLUXO_CUDA(h, launch_nfvse_alpha(h->NP, h->mhd, h->nOwn, s, P, h->dAlphaTmp));
+    return FLUXO_OK;
+  }
+  FLUXO_CUDA(h, launch_nfvse_indicator(h->NP, h->mhd, h->nOwn, s, P));
+  if (P.propSweeps <= 0) {
+    FLUXO_CUDA(h, launch_nfvse_list(h->nOwn, s, P));
+    return FLUXO_OK;
+  }
+  if (int r = exchange(h, FLUXO_XCHG_ALPHA, h->dAlphaRaw, nullptr)) return r;
+  for (int sw = 1; sw <= P.propSweeps; ++sw) {
+    const double* src = P.alphaRaw;
+    if (sw > 1) {
+      if (int r = exchange(h, FLUXO_XCHG_ALPHA, h->dAlpha, nullptr)) return r;
+      FLUXO_CUDA(h, cudaMemcpyAsync(h->dAlphaTmp, h->dAlpha, sizeof(double) * h->nElems, cudaMemcpyDeviceToDevice, s));
+      src = h->dAlphaTmp;
+    }
+    FLUXO_CUDA(h, launch_nfvse_sweep(h->nOwn, s, P, src, sw == P.propSweeps));
+  }
+  return FLUXO_OK;
+}
+
 // One DGTimeDerivative; stage 0 writes Ut, stage >= 1 applies the fused LSERK stage update.
 int rhs(fluxo_handle* h, KParams P) {
   cudaStream_t s = h->stream;
@@ -368,7 +393,7 @@ int rhs(fluxo_handle* h, KParams P) {
   if (h->mhd) {
     if (h->cfg.nfvse) {  // CalcBlendingCoefficient (dg.f90:358-361) and VolInt_NFVSE's FV part (:380-383)
       ProfScope ps(h, 5);
-      FLUXO_CUDA(h, launch_nfvse_alpha(h->NP, true, h->nOwn, s, P, h->dAlphaTmp));
+      if (int r = nfvse_alpha(h, P, s)) return r;
       FLUXO_CUDA(h, launch_nfvse_fv(h->cfg.riemann, h->NP, h->nOwn, h->nSMs, s, P));
       h->launches += 3 + (h->cfg.space_prop_sweeps > 1 ? 2 * (h->cfg.space_prop_sweeps - 1) : 0);
     }
@@ -412,7 +437,7 @@ int rhs(fluxo_handle* h, KParams P) {
   }
   if (h->cfg.nfvse) {  // CalcBlendingCoefficient (dg.f90:358-361) and VolInt_NFVSE's FV part (:380-383)
     ProfScope ps(h, 5);
-    FLUXO_CUDA(h, launch_nfvse_alpha(h->NP, false, h->nOwn, s, P, h->dAlphaTmp));
+    if (int r = nfvse_alpha(h, P, s)) return r;
     FLUXO_CUDA(h, launch_nfvse_fv_ns(h->cfg.riemann, h->NP, h->nOwn, h->nSMs, s, P));
     h->launches += 3 + (h->cfg.space_prop_sweeps > 1 ? 2 * (h->cfg.space_prop_sweeps - 1) : 0);
   }
@@ -1050,8 +1075,7 @@ int fluxo_gpu_set_partition(fluxo_handle* h, int nOwned, fluxo_exchange_fn fn, v
   if (!h) return FLUXO_EINVAL_CFG;
   if (!h->meshSet) return fail(h, FLUXO_ENOTREADY, "set_partition: mesh not set");
   if (nOwned < 1 || nOwned > h->nElems) return fail(h, FLUXO_EINVAL_CFG, "set_partition: nOwned out of range");
-  if (h->gauss || h->cfg.nfvse)
-    return fail(h, FLUXO_EINVAL_CFG, "set_partition: LGL nodes without NFVSE only");
+  if (h->gauss) return fail(h, FLUXO_EINVAL_CFG, "set_partition: LGL nodes only");
   h->nOwn = nOwned;
   h->xfn = fn;
   h->xctx = ctx;

@@ -74,6 +74,9 @@ cudaError_t launch_gauss_surf(int NP, int vf, int nElems, cudaStream_t s, const 
 cudaError_t launch_gauss_surf_mhd(int NP, int vf, int nElems, cudaStream_t s, const KParams& P);
 cudaError_t launch_gauss_mhd_lift_visc(int NP, int lift, int nElems, cudaStream_t s, const KParams& P);
 cudaError_t launch_nfvse_alpha(int NP, bool mhd, int nElems, cudaStream_t s, const KParams& P, double* scratch);
+cudaError_t launch_nfvse_indicator(int NP, bool mhd, int nElems, cudaStream_t s, const KParams& P);
+cudaError_t launch_nfvse_sweep(int nElems, cudaStream_t s, const KParams& P, const double* src, bool last);
+cudaError_t launch_nfvse_list(int nElems, cudaStream_t s, const KParams& P);
 // NFVSE_CORR: Apply_NFVSE_Correction of every element after a stage update with step b * dt (ut: the
 // stage's Ut to correct as well, or null); errKey records elem*8 + 5 for a safe state that is not admissible
 cudaError_t launch_nfvse_corr(int NP, bool mhd, int nElems, cudaStream_t s, const KParams& P, double* ut, double b,

@@ -46,6 +46,31 @@ cudaError_t launch_nfvse_alpha(int NP, bool mhd, int nElems, cudaStream_t s, con
   return cudaSuccess;
 }
 
+// The steps of launch_nfvse_alpha one by one, for a partitioned solve that exchanges the ghost elements'
+// coefficients between them: the indicator (alphaRaw), one propagation sweep from src (the last one
+// also lists the blended elements), or the list without propagation.
+cudaError_t launch_nfvse_indicator(int NP, bool mhd, int nElems, cudaStream_t s, const KParams& P) {
+#define FLUXO_NF_I(np) \
+  case np: return mhd ? alpha_np<np, 9>(nElems, s, P) : alpha_np<np, 5>(nElems, s, P);
+  switch (NP) {
+    FLUXO_NF_I(3) FLUXO_NF_I(4) FLUXO_NF_I(5) FLUXO_NF_I(6) FLUXO_NF_I(7) FLUXO_NF_I(8)
+    default: return cudaErrorInvalidValue;
+  }
+#undef FLUXO_NF_I
+}
+
+cudaError_t launch_nfvse_sweep(int nElems, cudaStream_t s, const KParams& P, const double* src, bool last) {
+  const int bs = 256, grid = (nElems + bs - 1) / bs;
+  nfvse::propagate_kernel<<<grid, bs, 0, s>>>(P, src, last);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_nfvse_list(int nElems, cudaStream_t s, const KParams& P) {
+  const int bs = 256, grid = (nElems + bs - 1) / bs;
+  nfvse::list_kernel<<<grid, bs, 0, s>>>(P);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_nfvse_corr(int NP, bool mhd, int nElems, cudaStream_t s, const KParams& P, double* ut, double b,
                               int* errKey) {
 #define FLUXO_NF_C(np)                                                                                        \

@@ -10,6 +10,7 @@ its flux from the same two states, so the exchanges are
 * FLUXO_XCHG_STATE  - the ghost elements' U (before each right-hand side),
 * FLUXO_XCHG_GTRACE - the ghost side's viscous face share of each partition side (after the lifting),
 * FLUXO_XCHG_DT     - MIN over the ranks of the dt bits and the error key (after CALCTIMESTEP),
+* FLUXO_XCHG_ALPHA  - the ghost elements' NFVSE blending coefficients (before each propagation sweep),
 
 driven by the library through the callback of ``fluxo_gpu_set_partition``.  ``Partition`` builds a
 rank's local mesh and its exchange lists (host logic only); ``DistExchange`` moves the data with
@@ -145,6 +146,8 @@ class _Exchange:
                 self._swap(a.view(2 * self.n_sides, -1), "gt_send", "gt_recv")
         elif what == _lib.FLUXO_XCHG_DT:
             self._min(a, b)
+        elif what == _lib.FLUXO_XCHG_ALPHA:
+            self._swap(a.view(self.n_local, 1), "state_send", "state_recv")
         else:
             raise ValueError("unknown exchange %d" % what)
 
@@ -165,6 +168,9 @@ class _Exchange:
                         self.apply(what, A, None)
                     elif what == _lib.FLUXO_XCHG_GTRACE:
                         A = torch.as_tensor(_DeviceArray(a, ngt, "<f8"), device=dev) if a else None
+                        self.apply(what, A, None)
+                    elif what == _lib.FLUXO_XCHG_ALPHA:
+                        A = torch.as_tensor(_DeviceArray(a, self.n_local, "<f8"), device=dev)
                         self.apply(what, A, None)
                     else:
                         A = torch.as_tensor(_DeviceArray(a, 1, "<i8"), device=dev)

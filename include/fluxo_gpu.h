@@ -129,8 +129,10 @@ typedef struct fluxo_handle fluxo_handle;
  *   FLUXO_XCHG_DT      a = dt bits (uint64, the IEEE bits of a non-negative double), b = error key
  *                      (int32, INT_MAX = none): after CALCTIMESTEP, both reduced with MIN over the
  *                      handles (MPI_ALLREDUCE, calctimestep.f90:159-167); for MHD also once inside
- *                      fluxo_gpu_set_partition, with a = the bits of GLM_dtch1. */
-enum { FLUXO_XCHG_STATE = 1, FLUXO_XCHG_GTRACE = 2, FLUXO_XCHG_DT = 3 };
+ *                      fluxo_gpu_set_partition, with a = the bits of GLM_dtch1;
+ *   FLUXO_XCHG_ALPHA   a = NFVSE blending coefficients (double per element): the ghost elements' values
+ *                      before every propagation sweep (ProlongBlendingCoeffToFaces, nfvse_mpi.f90:31-58). */
+enum { FLUXO_XCHG_STATE = 1, FLUXO_XCHG_GTRACE = 2, FLUXO_XCHG_DT = 3, FLUXO_XCHG_ALPHA = 4 };
 typedef int (*fluxo_exchange_fn)(void* ctx, int what, void* stream, void* a, void* b);
 
 /* InitEquation + InitDGbasis + InitTimeDisc equivalent.
@@ -198,8 +200,9 @@ int fluxo_gpu_get_glm_ch(fluxo_handle* h, double* ch);
  * are every side of an owned element (both elements of each present), and the element kernels,
  * CALCTIMESTEP and the stage updates run over the owned elements only.  Both handles of a partition
  * side compute its flux from the same two states, so fluxes need no exchange.  `fn(ctx, ...)` is called
- * at the exchange points above; the caller moves the data (NCCL, peer copies).  LGL nodes without NFVSE
- * (Euler, Navier-Stokes, MHD; for MHD this call is itself collective: it reduces GLM_dtch1);
+ * at the exchange points above; the caller moves the data (NCCL, peer copies).  LGL nodes (Euler,
+ * Navier-Stokes, MHD, NFVSE; for MHD this call is itself collective: it reduces GLM_dtch1; ComputeAlpha
+ * 20 draws per handle);
  * fluxo_gpu_analyze and the batch entry points are not available on a partitioned handle.  A later
  * fluxo_gpu_set_mesh removes the partition.
  * Replaces the single-process part of the reference's MPI decomposition (mesh_readin.f90:246-292

@@ -77,7 +77,12 @@ def gather(shards, what):
 
 CASES = [dict(n=2), dict(n=3), dict(n=2, eqn=0), dict(n=4, lifting=2, lifting_var=2), dict(n=3, riemann=1, volume_flux=10),
          dict(n=2, N=7, ne=(3, 2, 2)), dict(n=5, N=2, ne=(5, 2, 2), time_disc=8),
-         dict(n=2, mhd=True), dict(n=3, mhd=True, N=4, lifting=2), dict(n=2, mhd=True, eqn=2, riemann=10)]
+         dict(n=2, mhd=True), dict(n=3, mhd=True, N=4, lifting=2), dict(n=2, mhd=True, eqn=2, riemann=10),
+         dict(n=3, nfvse=1, compute_alpha=1, space_prop_sweeps=2, alpha_min=1e-4, riemann=44, sub_fv_method=2,
+              recons_boundaries=3),
+         dict(n=2, nfvse=1, compute_alpha=3, shock_blend_coef=0.4, sub_fv_method=4, recons_boundaries=3, eqn=0),
+         dict(n=2, mhd=True, N=4, nfvse=1, compute_alpha=1, space_prop_sweeps=1, alpha_min=1e-4),
+         dict(n=3, nfvse=1, compute_alpha=3, shock_blend_coef=0.3, nfvse_corr=1, time_disc=8, eqn=0)]
 
 
 @pytest.mark.parametrize("case", CASES, ids=lambda c: "_".join("%s%s" % kv for kv in c.items()))
@@ -90,6 +95,10 @@ def test_partitioned_rhs_and_steps_match_one_handle(gpu_lib, case):
     run_threads(n, lambda i: shards[i].op.dg_time_derivative(0.0))
     Uts = gather(shards, "get_ut")
     assert np.abs(Uts - Ut).max() <= 1e-15 * np.abs(Ut).max(), np.abs(Uts - Ut).max()
+    if case.get("nfvse"):  # the blending coefficients after the propagation sweeps over the partition sides
+        a_ref = ref.alpha()
+        a_sh = np.concatenate([s.op.alpha()[: s.part.n_owned] for s in shards])
+        assert (a_ref > 0).any() and np.array_equal(a_sh, a_ref)
     # CALCTIMESTEP with the dt reduction, then device-resident steps of the TimeDisc loop
     dt_ref, _ = ref.calc_timestep()
     dts = [None] * n
@@ -110,8 +119,8 @@ def test_partitioned_rhs_and_steps_match_one_handle(gpu_lib, case):
 
 
 def test_partition_restrictions(gpu_lib):
-    mesh = fb.box_mesh(3, (2, 2, 2), (-1, -1, -1), (1, 1, 1))
-    op = fb.DGOperator(N=3, eqn=0, riemann=44, volume_flux=5, nfvse=1)
+    mesh = fb.box_mesh(3, (2, 2, 2), (-1, -1, -1), (1, 1, 1), node_type=1)
+    op = fb.DGOperator(N=3, eqn=0, riemann=44, volume_flux=5, node_type=1)
     op.set_mesh(mesh)
     with pytest.raises(fb.FluxoError):
         _lib.check(op.lib.fluxo_gpu_set_partition(op.h, 4, _lib.EXCHANGE_FN(lambda *a: 0), None), op.h)
