@@ -319,9 +319,17 @@ def run_fluxo(args):
         mesh = fb.box_mesh(w["N"], w["elems"], w["xmin"], w["xmax"], NGeo=w["NGeo"], deform_amp=w["deform_amp"],
                            node_type=nt)
         fields = {k: v for k, v in w.items() if k not in ("elems", "xmin", "xmax", "NGeo", "deform_amp")}
-        op = fb.DGOperator(device=local, **fields)
-        op.set_mesh(mesh)
         U0 = mhd_orszag_tang_state(mesh["Elem_xGP"], kappa=w["kappa"])
+        if args.shard and world > 1 and nt == 2:  # one solve over the ranks (set_partition is collective)
+            from fluxo_b200.shard import DistExchange, ShardedOperator
+
+            shard = ShardedOperator(mesh, world, rank, DistExchange, device=local, **fields)
+            op = shard.op
+            U0 = shard.part.local_state(U0)
+            nd_total = int(np.prod(w["elems"])) * (w["N"] + 1) ** 3
+        else:
+            op = fb.DGOperator(device=local, **fields)
+            op.set_mesh(mesh)
     else:
         w = workload(elems=args.elems or 32, N=args.N or 7)
         nt = 1 if args.nodes == "gauss" else 2
@@ -345,7 +353,7 @@ def run_fluxo(args):
     op.set_state(U0)
     setup_s = time.time() - t0
     nvar = 9 if mhd else 5
-    sharded = args.shard and world > 1 and not mhd
+    sharded = args.shard and world > 1 and args.nodes == "lgl"
     nd = (shard.part.n_owned if sharded else op.nElems) * (w["N"] + 1) ** 3
     if sharded:
         args.no_e2e, args.no_mix, args.no_cpu = True, True, True
@@ -423,7 +431,7 @@ def run_fluxo(args):
     per_kernel = None if (mhd or gauss or sharded) else kernel_rooflines(kinds, w["N"], nd, op.nElems, peak)
     falg_rhs = sum((MHD_FALG_PER_DOF if mhd else FALG_PER_DOF).values())
     if mhd:
-        alpha = op.alpha() if w["nfvse"] else np.zeros(op.nElems)
+        alpha = op.alpha()[: nd // (w["N"] + 1) ** 3] if w["nfvse"] else np.zeros(op.nElems)
         config = {"workload": "mhd_glm_resistive_orszag_tang_N%d_%dx%dx%d_curved" % ((w["N"],) + w["elems"]) +
                   ("_gauss_nodes_no_nfvse" if gauss else "") +
                   ("" if args.shock_blend <= 0 else "_blend%g" % args.shock_blend) +
@@ -435,7 +443,9 @@ def run_fluxo(args):
                        "fixed alpha %g (ComputeAlpha 3)" % args.shock_blend) +
                       ", SubFVMethod %d" % args.sub_fv + (", NFVSE_CORR" if args.nfvse_corr else "")),
                   "blended_elements_last_rhs": int((alpha > 0).sum()), "time_disc": "carpenterrk4-5",
-                  "rhs_per_step": 5, "parallelism": "replicas x%d" % world,
+                  "rhs_per_step": 5,
+                  "parallelism": ("one solve over %d GPUs (contiguous element ranges + ghost elements, NCCL)" % world
+                                  if sharded else "replicas x%d" % world),
                   "l2": "inputs larger than L2 (state %d MB)" % (nd * 72 // 10 ** 6), "steps": args.steps}
     else:
         config = config_dict(w, world, args.steps)
@@ -862,7 +872,7 @@ def main():
     ap.add_argument("--sub-fv", type=int, default=1, choices=(1, 2, 3, 4), help="mhd: SubFVMethod")
     ap.add_argument("--nfvse-corr", action="store_true", help="mhd: NFVSE_CORR positivity correction")
     ap.add_argument("--shard", action="store_true",
-                    help="tgv with --gpus > 1: one solve over the GPUs (strong scaling) instead of replicas")
+                    help="tgv / mhd with --gpus > 1: one solve over the GPUs (strong scaling) instead of replicas")
     ap.add_argument("--nodes", default="lgl", choices=("lgl", "gauss"),
                     help="Gauss-Lobatto (the headline) or Gauss nodes (PP_NodeType; mhd: without NFVSE)")
     ap.add_argument("--no-e2e", action="store_true")
