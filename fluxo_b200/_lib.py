@@ -100,6 +100,7 @@ EXPORTS = [
     "fluxo_gpu_time_disc", "fluxo_gpu_device_buffers", "fluxo_gpu_launch_count", "fluxo_gpu_destroy",
     "fluxo_gpu_last_error", "fluxo_gpu_set_profiling", "fluxo_gpu_get_profile", "fluxo_gpu_fp64_peak",
     "fluxo_host_box_sizes", "fluxo_host_box_mesh", "fluxo_host_box_mesh_gauss", "fluxo_host_hopr_mesh",
+    "fluxo_host_nodes",
     "fluxo_host_exact_func", "fluxo_gpu_dg_time_derivative_noalloc",
     "fluxo_gpu_set_glm_ch", "fluxo_gpu_get_glm_ch", "fluxo_gpu_get_alpha", "fluxo_gpu_set_alpha",
     "fluxo_gpu_set_partition", "fluxo_gpu_exchange_buffers", "fluxo_gpu_volume_shape",
@@ -148,6 +149,7 @@ def load():
     lib.fluxo_host_box_mesh.argtypes = [i, vp, vp, vp, i, d] + [vp] * 11
     lib.fluxo_host_box_mesh_gauss.argtypes = [i, vp, vp, vp, i, d] + [vp] * 12
     lib.fluxo_host_hopr_mesh.argtypes = [i, i, i, vp, i, vp, i, vp, i, i, vp, d, i] + [vp] * 12
+    lib.fluxo_host_nodes.argtypes = [i, i, vp, vp]
     lib.fluxo_host_exact_func.argtypes = [i, d, ctypes.c_size_t, vp, d, vp, d, vp, d, vp, vp]
     lib.fluxo_gpu_dg_time_derivative_noalloc.argtypes = [P(FluxoCfg), i, i] + [vp] * 8
     lib.fluxo_gpu_set_glm_ch.argtypes = [vp, d]

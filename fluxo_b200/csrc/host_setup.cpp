@@ -650,6 +650,16 @@ extern "C" int fluxo_host_hopr_mesh(int N, int node_type, int nElems, const int*
   return FLUXO_OK;
 }
 
+extern "C" int fluxo_host_nodes(int N, int node_type, double* x, double* w) {
+  if (N < 0 || N > 32 || !x || (node_type != 1 && node_type != 2)) return FLUXO_EINVAL_CFG;
+  std::vector<double> xs, ws;
+  if (node_type == 1) gauss(N, xs, ws);
+  else lgl(N, xs, ws);
+  std::copy(xs.begin(), xs.end(), x);
+  if (w) std::copy(ws.begin(), ws.end(), w);
+  return FLUXO_OK;
+}
+
 extern "C" int fluxo_host_exact_func(int func, double t, size_t np, const double* x, double kappa,
                                      const double* adv, double amp, const double* wave, double freq,
                                      const double* ref, double* U) {

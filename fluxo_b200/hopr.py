@@ -7,7 +7,8 @@
   metrics, face geometry) through the C ABI ``fluxo_host_hopr_mesh``;
 * ``read_state`` / ``write_state`` read and write State files with the attributes and the
   ``DG_Solution`` dataset of WriteState / GenerateFileSkeleton (src/io_hdf5/hdf5_output.f90:74-160)
-  for restarts (src/restart/restart.f90:60-200).
+  for restarts (src/restart/restart.f90:60-200); ``restart_state`` interpolates a state of lower
+  degree or of the other node set onto the run's nodes.
 
 HDF5 access goes through ``h5lite`` (the format subset these files use).
 """
@@ -22,7 +23,8 @@ import numpy as np
 from . import _lib
 from .h5lite import H5File, write_h5
 
-__all__ = ["read_mesh", "mesh_arrays", "load_mesh", "read_state", "write_state", "state_file_name"]
+__all__ = ["read_mesh", "mesh_arrays", "load_mesh", "read_state", "write_state", "state_file_name", "nodes",
+           "restart_state"]
 
 def _i32(a):
     return np.ascontiguousarray(a, dtype=np.int32)
@@ -135,6 +137,47 @@ def read_state(path):
                 NodeType=str(f.attr("NodeType", "GAUSS-LOBATTO")), MeshFile=f.attr("MeshFile", ""),
                 Project_Name=f.attr("Project_Name", ""), VarNames=f.attr("VarNames", []),
                 File_Type=f.attr("File_Type", ""))
+
+
+def nodes(N, node_type):
+    """1D nodes of degree N: node_type 1 Gauss, 2 Gauss-Lobatto (C ABI ``fluxo_host_nodes``)."""
+    x = np.zeros(N + 1)
+    _lib.check(_lib.load().fluxo_host_nodes(int(N), int(node_type), x.ctypes.data_as(ctypes.c_void_p), None))
+    return x
+
+
+def _interp_matrix(x_in, x_out):
+    """Lagrange interpolation from x_in to x_out (InitializeVandermonde with barycentric weights,
+    interpolation/basis.f90); a point on a node takes that node's value."""
+    w = np.array([1.0 / np.prod([xi - xj for j, xj in enumerate(x_in) if j != i]) for i, xi in enumerate(x_in)])
+    V = np.zeros((len(x_out), len(x_in)))
+    for o, y in enumerate(x_out):
+        hit = np.nonzero(np.abs(y - x_in) <= 2.220446049250313e-16 * np.maximum(np.abs(y), np.abs(x_in)))[0]
+        if hit.size:
+            V[o, hit[0]] = 1.0
+            continue
+        t = w / (y - x_in)
+        V[o] = t / t.sum()
+    return V
+
+
+def restart_state(st, N, node_type):
+    """The restart state on (N, node_type) from a State file's (read_state) solution: unchanged when N and
+    the node set match, else interpolated with the Lagrange Vandermonde (Restart, restart.f90:150-217, the
+    case N_Restart <= N).  N_Restart > N projects J*U modally with the Jacobian at 3*NGeo points, which
+    this host setup does not keep: refused."""
+    U = np.asarray(st["U"])
+    n_in = int(st["N"])
+    t_in = 1 if str(st.get("NodeType", "GAUSS-LOBATTO")).strip().upper() == "GAUSS" else 2
+    if n_in == N and t_in == node_type:
+        return U
+    if n_in > N:
+        raise ValueError("restart from N=%d onto N=%d (projection with the Jacobian) is not implemented" % (n_in, N))
+    V = _interp_matrix(nodes(n_in, t_in), nodes(N, node_type))
+    # ChangeBasis3D on the C view [elem][k][j][i][var]: i, then j, then k
+    out = np.einsum("ai,ekjiv->ekjav", V, U)
+    out = np.einsum("bj,ekjav->ekbav", V, out)
+    return np.ascontiguousarray(np.einsum("ck,ekbav->ecbav", V, out))
 
 
 _VARNAMES = {5: ["Density", "MomentumX", "MomentumY", "MomentumZ", "EnergyStagnationDensity"],

@@ -269,17 +269,14 @@ class Fluxo:
                                  adv_vel=o["advvel"], amplitude=o["iniamplitude"], wavenumber=o["iniwavenumber"],
                                  frequency=o["inifrequency"], ref_state=o["refstate"])
         self.t = 0.0
-        if restart_file:  # InitRestart / Restart (restart.f90:60-200), same N and node set only
+        if restart_file:  # InitRestart / Restart (restart.f90:60-217), interpolated when N or the nodes differ
             from . import hopr
             st = hopr.read_state(restart_file)
-            want = "GAUSS" if node_type == 1 else "GAUSS-LOBATTO"
-            if st["N"] != o["n"] or st["NodeType"].strip().upper() != want:
-                raise ValueError("restart from N=%d %s onto N=%d %s (interpolation) is not implemented"
-                                 % (st["N"], st["NodeType"], o["n"], want))
-            if st["U"].shape != self.U0.shape:
+            U = hopr.restart_state(st, o["n"], node_type)
+            if U.shape != self.U0.shape:
                 raise ValueError("restart file %s: DG_Solution shape %s does not match %s"
-                                 % (restart_file, st["U"].shape, self.U0.shape))
-            self.U0 = st["U"]
+                                 % (restart_file, U.shape, self.U0.shape))
+            self.U0 = U
             self.t = 0.0 if _flag(o["resettime"]) else st["Time"]
         self.op.set_state(self.U0)
         self.nDOF = self.op.nElems * (o["n"] + 1) ** 3

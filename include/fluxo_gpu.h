@@ -388,6 +388,9 @@ int fluxo_host_hopr_mesh(int N, int node_type, int nElems, const int* ElemInfo, 
                          int* ElemToSide, double* Metrics_fTilde, double* Metrics_gTilde, double* Metrics_hTilde,
                          double* sJ, double* NormVec, double* TangVec1, double* TangVec2, double* SurfElem,
                          double* Elem_xGP, double* SurfMetrics);
+/* The 1D nodes and weights of degree N: node_type 1 Gauss (LegendreGaussNodesAndWeights), 2 Gauss-Lobatto
+ * (LegGaussLobNodesAndWeights), src/interpolation/basis.f90:430-608; w may be NULL. */
+int fluxo_host_nodes(int N, int node_type, double* x, double* w);
 /* FillIni(IniExactFunc, U) on the given node coordinates (src/equation/navierstokes/equation.f90:575-950):
  * IniExactFunc 1 (constant refstate, prim given), 2 (density sine wave), 4 (manufactured), 7 (Taylor-Green),
  * 14 (soft Sedov-Taylor blast around IniCenter = 0). */

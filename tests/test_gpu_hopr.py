@@ -301,3 +301,17 @@ def test_reference_softblast_entropy(gpu_lib, case):
         with pytest.raises(fb.FluxoError, match="errType=4"):
             f.TimeDisc(t_end=5.0)
         assert t_o < 5.0 and abs(f.t - t_o) < 1e-9 * t_o
+
+
+def test_restart_onto_a_higher_degree(gpu_lib, tmp_path):
+    """A State file of N=3 restarts a run of N=5 (InterpolateSolution, restart.f90:150-217): the constant
+    free stream stays exact and the time of the file is kept."""
+    f3 = fb.Fluxo(FREESTREAM_NS, MeshFile=WARPED)
+    st = tmp_path / "NAVIERSTOKES_FREESTREAM_State_0000001.500000000.h5"
+    hopr.write_state(st, f3.U0, 1.5, WARPED, "NAVIERSTOKES_FREESTREAM")
+    f5 = fb.Fluxo(FREESTREAM_NS.replace("N = 3", "N = 5"), MeshFile=WARPED, restart_file=str(st))
+    assert f5.t == 1.5 and f5.U.shape[1] == 6
+    ref = fb.Fluxo(FREESTREAM_NS.replace("N = 3", "N = 5"), MeshFile=WARPED).U0
+    assert np.abs(f5.U - ref).max() < 1e-12
+    f5.TimeDisc(t_end=2.0)
+    assert _linf_freestream(f5).max() < 1e-11

@@ -265,3 +265,41 @@ def test_parameter_ini_mesh_keys():
     assert r["meshfile"].endswith("03_03_03_mesh.h5") and r["usecurveds"] == "F" and r["meshscale"] == 0.5
     assert r["boundarytypes"] == {"BC_zminus": (1, 0), "BC_zplus": (1, 0)}
     assert r["projectname"] == "NAVIERSTOKES_FREESTREAM"
+
+
+def test_nodes_match_the_golden_lgl_and_gauss():
+    import json
+
+    kat = json.load(open(os.path.join(GOLDEN, "lgl_kat.json")))
+    for N in range(1, 9):
+        assert np.allclose(hopr.nodes(N, 2), kat[str(N)]["x"], rtol=0, atol=1e-15)
+        xg, _ = np.polynomial.legendre.leggauss(N + 1)
+        assert np.allclose(hopr.nodes(N, 1), xg, rtol=0, atol=1e-15)
+
+
+@pytest.mark.parametrize("n_in,t_in,n_out,t_out", [(3, 2, 3, 2), (3, 2, 5, 2), (2, 2, 4, 1), (4, 1, 4, 2), (3, 1, 6, 1)])
+def test_restart_interpolation_is_exact_for_polynomials(n_in, t_in, n_out, t_out):
+    """Restart with N_Restart <= N or the other node set (restart.f90:150-217): the Lagrange Vandermonde
+    reproduces a polynomial of degree N_Restart at the new nodes."""
+    f = lambda x, y, z: 1.0 + x ** n_in - 2.0 * y * z ** (n_in - 1) + 0.5 * x * y * z  # noqa: E731
+    xi = hopr.nodes(n_in, t_in)
+    U = np.zeros((3, n_in + 1, n_in + 1, n_in + 1, 5))
+    for k in range(n_in + 1):
+        for j in range(n_in + 1):
+            for i in range(n_in + 1):
+                U[:, k, j, i, :] = f(xi[i], xi[j], xi[k]) * np.arange(1, 6)
+    st = dict(U=U, N=n_in, NodeType="GAUSS" if t_in == 1 else "GAUSS-LOBATTO")
+    out = hopr.restart_state(st, n_out, t_out)
+    xo = hopr.nodes(n_out, t_out)
+    ref = np.array([[[f(xo[i], xo[j], xo[k]) for i in range(n_out + 1)] for j in range(n_out + 1)]
+                    for k in range(n_out + 1)])
+    assert out.shape == (3, n_out + 1, n_out + 1, n_out + 1, 5)
+    assert np.abs(out[..., 2] - 3 * ref).max() < 1e-13
+    if (n_in, t_in) == (n_out, t_out):
+        assert out is st["U"] or np.array_equal(out, U)
+
+
+def test_restart_from_higher_degree_is_refused():
+    st = dict(U=np.zeros((1, 5, 5, 5, 5)), N=4, NodeType="GAUSS-LOBATTO")
+    with pytest.raises(ValueError, match="not implemented"):
+        hopr.restart_state(st, 3, 2)
