@@ -54,8 +54,13 @@ __host__ __device__ constexpr size_t surf_mhd_smem_bytes() {
 }
 
 // One element per block, one thread per node (as gauss::surf_kernel).
+// resident blocks per SM the register allocation must allow: one element per block leaves small-N blocks
+// of (N+1)^3 threads, so for N <= 4 four of them (a register cap of 128), else one
+template <int NP>
+__host__ __device__ constexpr int surf_mhd_minb() { return NP * NP * NP <= 125 ? 4 : 1; }
+
 template <int NP, int VF>
-__global__ void __launch_bounds__(NP * NP * NP, 1) surf_mhd_kernel(KParams P) {
+__global__ void __launch_bounds__(NP * NP * NP, surf_mhd_minb<NP>()) surf_mhd_kernel(KParams P) {
   if (halted(P)) return;
   constexpr int NV9 = 9, NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1, NQ = mhd::Rec<VF>::NQ;
   constexpr int FS = surf_mhd_stride<VF>();
@@ -176,8 +181,13 @@ __host__ __device__ constexpr size_t mlift_smem_bytes() {
   return sizeof(double) * (size_t)(2 * NP * NP + 2 * NP + NP * NP * NP + 27 * lift_gstride<NP>() + mlift_area<NP>());
 }
 
+// resident blocks per SM for the lifting kernel: for N <= 4 three (as many as its shared memory allows at
+// N = 4, a register cap of 170), else one
+template <int NP>
+__host__ __device__ constexpr int mlift_minb() { return NP * NP * NP <= 125 ? 3 : 1; }
+
 template <int NP, int LIFT>
-__global__ void __launch_bounds__(NP * NP * NP) mhd_lift_visc_kernel(KParams P) {
+__global__ void __launch_bounds__(NP * NP * NP, mlift_minb<NP>()) mhd_lift_visc_kernel(KParams P) {
   if (halted(P)) return;
   constexpr int NV9 = 9, NP3 = NP * NP * NP, NPT = NP * NP, N = NP - 1, GS = lift_gstride<NP>();
   extern __shared__ double smem[];
