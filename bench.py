@@ -732,7 +732,7 @@ def measure_serve(args, world, rank, local):
     barrier(world)
     torch.cuda.synchronize(dev)
     b = Batch(device=local)
-    srv = Server(b, budget, instance_bytes, steps_per_poll=args.poll_steps)
+    srv = Server(b, budget, instance_bytes, steps_per_poll=args.poll_steps, device_loop=not args.host_poll)
     with ClockSampler(local) as clk:
         served = srv.serve(reqs)
         torch.cuda.synchronize(dev)
@@ -767,7 +767,10 @@ def measure_serve(args, world, rank, local):
                                                                        s_sum["max_running"] < len(reqs)),
               "requests_waiting_for_memory": s_sum["waited_for_memory"],
               "max_running": s_sum["max_running"], "max_device_bytes": s_sum["max_device_bytes"],
-              "graph_rebuilds": served.rebuilds, "steps_per_poll": args.poll_steps,
+              "graph_rebuilds": served.rebuilds,
+              "loop": ("host-polled, %d steps per poll" % args.poll_steps) if args.host_poll
+              else "device-resident (CUDA graph while-node)",
+              "device_loops": served.loops, "loop_wakes": served.wakes,
               "stopped_by_calctimestep": len(failed),
               "parallelism": "replicas x%d (own stream per rank)" % world}
     line = {"metric": SERVE_METRIC, "value": value, "unit": "DOF-updates/s", "n_gpus": world, "steps": len(reqs),
@@ -864,7 +867,10 @@ def main():
     ap.add_argument("--no-mix", action="store_true",
                     help="tgv: skip the batched and served measurements that the default line carries")
     ap.add_argument("--mix-steps", type=int, default=10, help="tgv: timed steps of the embedded batched measurement")
-    ap.add_argument("--poll-steps", type=int, default=2, help="serve: time steps between admission rounds")
+    ap.add_argument("--poll-steps", type=int, default=2,
+                    help="serve with --host-poll: time steps between admission rounds")
+    ap.add_argument("--host-poll", action="store_true",
+                    help="serve: the host-polled loop (fluxo_batch_run) instead of the device-resident loop")
     ap.add_argument("--elems", type=int, default=0, help="elements per direction (0: the configuration's)")
     ap.add_argument("--N", type=int, default=0, help="polynomial degree (0: the configuration's)")
     ap.add_argument("--shock-blend", type=float, default=0.0,

@@ -109,8 +109,12 @@ EXPORTS = [
     "fluxo_batch_set_state",
     "fluxo_batch_remove", "fluxo_batch_info", "fluxo_batch_stream", "fluxo_batch_instance_bytes",
     "fluxo_batch_last_error",
-    "fluxo_batch_destroy",
+    "fluxo_batch_destroy", "fluxo_batch_loop_start", "fluxo_batch_loop_wake", "fluxo_batch_loop_poll",
+    "fluxo_batch_loop_wait",
 ]
+
+# fluxo_batch_loop_* end reasons (FLUXO_LOOP_* of fluxo_gpu.h)
+LOOP_IDLE, LOOP_FINISHED, LOOP_WOKEN, LOOP_STEP_LIMIT = 0, 1, 2, 3
 
 # FLUXO_NOALLOC_SCRATCH_BYTES of fluxo_gpu.h: the static scratch of fluxo_gpu_dg_time_derivative_noalloc
 NOALLOC_SCRATCH_BYTES = 8 * 1024 * 1024
@@ -174,6 +178,10 @@ def load():
     lib.fluxo_batch_instance_bytes.argtypes = [P(FluxoCfg), i, i, P(sz)]
     lib.fluxo_batch_last_error.argtypes = [vp, ctypes.c_char_p, sz]
     lib.fluxo_batch_destroy.argtypes = [vp]
+    lib.fluxo_batch_loop_start.argtypes = [vp, i]
+    lib.fluxo_batch_loop_wake.argtypes = [vp]
+    lib.fluxo_batch_loop_poll.argtypes = [vp, P(i), P(i), P(i), P(i)]
+    lib.fluxo_batch_loop_wait.argtypes = [vp, P(i), P(i), P(i)]
     for name in EXPORTS:
         getattr(lib, name).restype = ctypes.c_int
     _lib = lib

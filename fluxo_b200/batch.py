@@ -77,6 +77,29 @@ class Batch:
                 return
             max_steps -= k
 
+    def loop_start(self, max_steps):
+        """Starts the device-resident loop (``fluxo_batch_loop_start``) and returns at once: the GPU
+        repeats the time step of all instances until one finishes, ``loop_wake`` is called, or
+        ``max_steps`` steps ran."""
+        self._check(self.lib.fluxo_batch_loop_start(self.b, int(max_steps)))
+
+    def loop_wake(self):
+        """Asks the running loop to return after its current step."""
+        self._check(self.lib.fluxo_batch_loop_wake(self.b))
+
+    def loop_poll(self):
+        """None while the loop runs; else (steps run, end reason, instances still running)."""
+        fin, n, why, run = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.fluxo_batch_loop_poll(self.b, ctypes.byref(fin), ctypes.byref(n), ctypes.byref(why),
+                                                   ctypes.byref(run)))
+        return (n.value, why.value, run.value) if fin.value else None
+
+    def loop_wait(self):
+        """Waits for the loop's end; returns (steps run, end reason, instances still running)."""
+        n, why, run = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.fluxo_batch_loop_wait(self.b, ctypes.byref(n), ctypes.byref(why), ctypes.byref(run)))
+        return n.value, why.value, run.value
+
     def status(self, iid):
         """(t, steps taken, finished, errType) of an instance."""
         t, n, done, err = ctypes.c_double(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()

@@ -8,10 +8,14 @@
 //     per-instance minimum, the LSERK update reads the element's instance dt, and a finished
 //     instance gets dt = 0 until it is removed;
 //   * one time step of all groups (CALCTIMESTEP, the stages, the per-instance bookkeeping) is
-//     captured once as a CUDA graph and replayed; the graph is rebuilt when instances join or leave.
+//     captured once as a CUDA graph and replayed; the graph is rebuilt when instances join or leave;
+//   * the request loop of a server runs on the device: a second graph repeats that step inside a
+//     conditional while-node until an instance finishes, the host raises a wake word in mapped pinned
+//     memory (a request can be admitted), or a step limit is reached (fluxo_batch_loop_start).
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -74,6 +78,31 @@ __global__ void batch_advance_kernel(int first, int n, InstState* s) {
   if (S.last || (S.maxIter > 0 && S.iter >= S.maxIter)) S.done = 1;
 }
 
+// Last node of the device-resident loop's body (one per time step): counts the unfinished instances
+// and ends the while-loop (condition 0) when fewer are running than at the loop's start, when the
+// host raised the wake word, or after loop[1] steps.  loop = {steps done, step limit, running at the
+// start, end reason, running now}.  The step limit bounds every loop, whatever the host does.
+__global__ void batch_loop_cond_kernel(cudaGraphConditionalHandle h, const InstState* s, int nInst, int* loop,
+                                       const volatile int* wake) {
+  __shared__ int running;
+  if (threadIdx.x == 0) running = 0;
+  __syncthreads();
+  int r = 0;
+  for (int i = threadIdx.x; i < nInst; i += blockDim.x) r += s[i].done ? 0 : 1;
+  if (r) atomicAdd(&running, r);
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const int steps = loop[0] + 1;
+  loop[0] = steps;
+  int why = 0;
+  if (running < loop[2]) why = FLUXO_LOOP_FINISHED;
+  else if (*wake != 0) why = FLUXO_LOOP_WOKEN;
+  else if (steps >= loop[1]) why = FLUXO_LOOP_STEP_LIMIT;
+  loop[3] = why;
+  loop[4] = running;
+  cudaGraphSetConditional(h, why == 0 ? 1u : 0u);
+}
+
 struct Instance {
   int id = 0;
   fluxo_cfg cfg{};
@@ -132,6 +161,18 @@ struct fluxo_batch {
   cudaGraphExec_t exec = nullptr;
   std::vector<cudaStream_t> branch;            // one capture stream per group
   std::vector<cudaEvent_t> joins;              // fork / join points of the capture
+  // device-resident loop: the while-graph (captured at the first loop_start after a commit), the
+  // mapped pinned words (wake word [0], loop words [8..12] copied in and out), the loop's end event
+  cudaGraph_t loopGraph = nullptr;
+  cudaGraphExec_t loopExec = nullptr;
+  bool loopStale = true;
+  int* hWords = nullptr;
+  int* dWake = nullptr;
+  int* dLoop = nullptr;
+  InstState* hStates = nullptr;                // pinned copy of the states at the loop's end
+  int hStatesCap = 0;
+  cudaEvent_t loopEnd = nullptr;
+  bool loopActive = false;
   std::string lastError;
 };
 
@@ -389,6 +430,9 @@ int commit(fluxo_batch* b) {
   // the step graph
   if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
   if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+  if (b->loopExec) { cudaGraphExecDestroy(b->loopExec); b->loopExec = nullptr; }
+  if (b->loopGraph) { cudaGraphDestroy(b->loopGraph); b->loopGraph = nullptr; }
+  b->loopStale = true;
   while (b->branch.size() < b->groups.size()) {
     cudaStream_t st;
     BATCH_CUDA(b, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -418,6 +462,77 @@ int commit(fluxo_batch* b) {
   b->dirty = false;
   return FLUXO_OK;
 }
+
+// The device-resident loop graph: one conditional while-node whose body is the captured time step
+// of all groups followed by batch_loop_cond_kernel.  Built after a commit, at the first loop_start.
+int build_loop_graph(fluxo_batch* b) {
+  if (!b->loopStale && b->loopExec) return FLUXO_OK;
+  if (b->loopExec) { cudaGraphExecDestroy(b->loopExec); b->loopExec = nullptr; }
+  if (b->loopGraph) { cudaGraphDestroy(b->loopGraph); b->loopGraph = nullptr; }
+  cudaStream_t s = b->stream;
+  cudaGraph_t lg = nullptr;
+  BATCH_CUDA(b, cudaGraphCreate(&lg, 0));
+  b->loopGraph = lg;
+  cudaGraphConditionalHandle h;
+  BATCH_CUDA(b, cudaGraphConditionalHandleCreate(&h, lg, 1u, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  BATCH_CUDA(b, cudaGraphAddNode(&node, lg, nullptr, 0, &np));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  BATCH_CUDA(b, cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = enqueue_step(b);
+  if (e == cudaSuccess) {
+    batch_loop_cond_kernel<<<1, 256, 0, s>>>(h, b->dState, b->nInst, b->dLoop, b->dWake);
+    e = cudaGetLastError();
+  }
+  cudaGraph_t out = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(s, &out);
+  if (e != cudaSuccess || e2 != cudaSuccess)
+    return bfail(b, FLUXO_ECUDA, std::string("loop capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+  BATCH_CUDA(b, cudaGraphInstantiate(&b->loopExec, lg, 0));
+  b->loopStale = false;
+  return FLUXO_OK;
+}
+
+// pinned words, pinned state copy and the end event of the device-resident loop (first use)
+int loop_resources(fluxo_batch* b) {
+  if (!b->hWords) {
+    BATCH_CUDA(b, cudaHostAlloc((void**)&b->hWords, 64 * sizeof(int), cudaHostAllocMapped));
+    std::memset(b->hWords, 0, 64 * sizeof(int));
+    BATCH_CUDA(b, cudaHostGetDevicePointer((void**)&b->dWake, b->hWords, 0));
+    BATCH_CUDA(b, cudaMalloc((void**)&b->dLoop, 8 * sizeof(int)));
+    BATCH_CUDA(b, cudaEventCreateWithFlags(&b->loopEnd, cudaEventDisableTiming));
+  }
+  if (b->hStatesCap < b->nInst) {
+    if (b->hStates) cudaFreeHost(b->hStates);
+    b->hStates = nullptr;
+    b->hStatesCap = 0;
+    BATCH_CUDA(b, cudaHostAlloc((void**)&b->hStates, sizeof(InstState) * (size_t)b->nInst, cudaHostAllocDefault));
+    b->hStatesCap = b->nInst;
+  }
+  return FLUXO_OK;
+}
+
+// after the loop's end event: the instances' host states and the loop words
+void loop_collect(fluxo_batch* b, int* steps, int* reason, int* nRunning) {
+  const int* w = b->hWords + 8;
+  for (auto& kv : b->inst)
+    if (kv.second.placed && kv.second.slot >= 0 && kv.second.slot < b->nInst) kv.second.st = b->hStates[kv.second.slot];
+  if (steps) *steps = w[0];
+  if (reason) *reason = w[3];
+  if (nRunning) *nRunning = w[4];
+  b->loopActive = false;
+}
+
+#define BATCH_IDLE(b)                                                                              \
+  do {                                                                                             \
+    if ((b)->loopActive)                                                                           \
+      return bfail((b), FLUXO_ENOTREADY, "a device-resident loop is running (loop_poll / loop_wait first)"); \
+  } while (0)
 
 int check_cfg(const fluxo_cfg* c, std::string& msg) {
   if (!c || c->struct_size != (int)sizeof(fluxo_cfg)) { msg = "fluxo_cfg size mismatch"; return FLUXO_EINVAL_CFG; }
@@ -509,6 +624,7 @@ int fluxo_batch_add(fluxo_batch* b, const fluxo_cfg* cfg, int nElems, int nSides
 
 int fluxo_batch_run(fluxo_batch* b, int nSteps, int* nRunning) {
   if (!b) return FLUXO_EINVAL_CFG;
+  BATCH_IDLE(b);
   BATCH_CUDA(b, cudaSetDevice(b->device));
   int r = commit(b);
   if (r) return r;
@@ -548,6 +664,7 @@ int fluxo_batch_status(fluxo_batch* b, int id, double* t, int* nIter, int* done,
 
 int fluxo_batch_get_state(fluxo_batch* b, int id, double* U) {
   if (!b || !U) return FLUXO_EINVAL_CFG;
+  BATCH_IDLE(b);
   auto it = b->inst.find(id);
   if (it == b->inst.end() || it->second.removed) return bfail(b, FLUXO_EINVAL_CFG, "unknown instance id");
   const Instance& I = it->second;
@@ -566,6 +683,7 @@ int fluxo_batch_get_state(fluxo_batch* b, int id, double* U) {
 
 int fluxo_batch_set_state(fluxo_batch* b, int id, const double* U) {
   if (!b || !U) return FLUXO_EINVAL_CFG;
+  BATCH_IDLE(b);
   auto it = b->inst.find(id);
   if (it == b->inst.end() || it->second.removed) return bfail(b, FLUXO_EINVAL_CFG, "unknown instance id");
   Instance& I = it->second;
@@ -579,6 +697,75 @@ int fluxo_batch_set_state(fluxo_batch* b, int id, const double* U) {
   const size_t eU = (size_t)5 * g.NP * g.NP * g.NP;
   BATCH_CUDA(b, cudaMemcpyAsync(g.U + eU * I.elemOff, U, n * 8, cudaMemcpyHostToDevice, b->stream));
   BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
+  return FLUXO_OK;
+}
+
+int fluxo_batch_loop_start(fluxo_batch* b, int maxSteps) {
+  if (!b || maxSteps < 1) return bfail(b, FLUXO_EINVAL_CFG, "loop_start: maxSteps must be >= 1");
+  BATCH_IDLE(b);
+  BATCH_CUDA(b, cudaSetDevice(b->device));
+  int r = commit(b);
+  if (r) return r;
+  if ((r = loop_resources(b))) return r;
+  int running = 0;
+  for (const auto& kv : b->inst)
+    if (kv.second.placed && !kv.second.removed && kv.second.slot >= 0 && !kv.second.st.done) ++running;
+  int* w = b->hWords + 8;
+  w[0] = 0; w[1] = maxSteps; w[2] = running; w[3] = FLUXO_LOOP_IDLE; w[4] = running;
+  *(volatile int*)b->hWords = 0;  // wake word, lowered before the loop starts
+  std::atomic_thread_fence(std::memory_order_seq_cst);
+  if (running == 0 || b->nInst == 0) {  // nothing to advance: an empty loop that ends at once
+    BATCH_CUDA(b, cudaEventRecord(b->loopEnd, b->stream));
+    b->loopActive = true;
+    for (int i = 0; i < b->nInst; ++i) b->hStates[i] = InstState{};
+    for (const auto& kv : b->inst)
+      if (kv.second.slot >= 0 && kv.second.slot < b->nInst) b->hStates[kv.second.slot] = kv.second.st;
+    return FLUXO_OK;
+  }
+  if ((r = build_loop_graph(b))) return r;
+  BATCH_CUDA(b, cudaMemcpyAsync(b->dLoop, w, 5 * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  BATCH_CUDA(b, cudaGraphLaunch(b->loopExec, b->stream));
+  BATCH_CUDA(b, cudaMemcpyAsync(w, b->dLoop, 5 * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  BATCH_CUDA(b, cudaMemcpyAsync(b->hStates, b->dState, sizeof(InstState) * b->nInst, cudaMemcpyDeviceToHost,
+                                b->stream));
+  BATCH_CUDA(b, cudaEventRecord(b->loopEnd, b->stream));
+  b->loopActive = true;
+  return FLUXO_OK;
+}
+
+int fluxo_batch_loop_wake(fluxo_batch* b) {
+  if (!b) return FLUXO_EINVAL_CFG;
+  if (b->hWords) {
+    *(volatile int*)b->hWords = 1;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+  }
+  return FLUXO_OK;
+}
+
+int fluxo_batch_loop_poll(fluxo_batch* b, int* finished, int* steps, int* reason, int* nRunning) {
+  if (!b || !finished) return FLUXO_EINVAL_CFG;
+  *finished = 0;
+  if (!b->loopActive) return bfail(b, FLUXO_ENOTREADY, "loop_poll: no loop was started");
+  cudaError_t e = cudaEventQuery(b->loopEnd);
+  if (e == cudaErrorNotReady) return FLUXO_OK;
+  if (e != cudaSuccess) {
+    b->loopActive = false;
+    return bfail(b, FLUXO_ECUDA, std::string("loop_poll: ") + cudaGetErrorString(e));
+  }
+  loop_collect(b, steps, reason, nRunning);
+  *finished = 1;
+  return FLUXO_OK;
+}
+
+int fluxo_batch_loop_wait(fluxo_batch* b, int* steps, int* reason, int* nRunning) {
+  if (!b) return FLUXO_EINVAL_CFG;
+  if (!b->loopActive) return bfail(b, FLUXO_ENOTREADY, "loop_wait: no loop was started");
+  cudaError_t e = cudaEventSynchronize(b->loopEnd);
+  if (e != cudaSuccess) {
+    b->loopActive = false;
+    return bfail(b, FLUXO_ECUDA, std::string("loop_wait: ") + cudaGetErrorString(e));
+  }
+  loop_collect(b, steps, reason, nRunning);
   return FLUXO_OK;
 }
 
@@ -631,6 +818,12 @@ int fluxo_batch_destroy(fluxo_batch* b) {
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->loopExec) cudaGraphExecDestroy(b->loopExec);
+  if (b->loopGraph) cudaGraphDestroy(b->loopGraph);
+  if (b->hWords) cudaFreeHost(b->hWords);
+  if (b->hStates) cudaFreeHost(b->hStates);
+  if (b->dLoop) cudaFree(b->dLoop);
+  if (b->loopEnd) cudaEventDestroy(b->loopEnd);
   for (Group& g : b->groups) {
     free_group_arrays(b, g);
     if (g.dBasis) cudaFreeAsync(g.dBasis, b->stream);

@@ -7,6 +7,13 @@ graph replay per time step.  A request is admitted when its device bytes fit the
 the requests already running (first come, first served: a request that does not fit holds the ones
 behind it), and leaves the batch as soon as it reaches its end time, which frees its bytes for
 the next ones.  Each result is what the same solve gives alone (``DGOperator.time_disc``).
+
+The step loop itself runs on the device (``Batch.loop_start``, a conditional while-node of a CUDA
+graph): the GPU repeats the time step of all admitted requests and returns to the host only when a
+request finishes, when the host wakes it because a newly arrived request fits the budget, or at a
+step limit.  While it runs, the host takes in arrivals and prepares the admitted ones (``Batch.add``
+is host-only), so that preparation overlaps the GPU's steps.  ``device_loop=False`` keeps the older
+host-polled form (``steps_per_poll`` steps per ``Batch.run`` call).
 """
 import time
 from collections import deque
@@ -50,6 +57,8 @@ class ServeStats:
     results: list = field(default_factory=list)
     wall: float = 0.0
     rebuilds: int = 0
+    loops: int = 0                  # device-resident loops started
+    wakes: int = 0                  # loops the host woke for an admission
     max_running: int = 0
     max_bytes: int = 0
     waited_for_memory: set = field(default_factory=set)  # requests that queued because the budget was full
@@ -74,12 +83,17 @@ class Server:
     gives a request's device bytes; ``steps_per_poll`` time steps run between two admission rounds.
     """
 
-    def __init__(self, batch, hbm_budget, instance_bytes, steps_per_poll=2, clock=time.perf_counter):
+    def __init__(self, batch, hbm_budget, instance_bytes, steps_per_poll=2, clock=time.perf_counter,
+                 device_loop=True, max_loop_steps=1 << 20, poll_interval=2e-4, sleep=time.sleep):
         self.batch = batch
         self.budget = int(hbm_budget)
         self.instance_bytes = instance_bytes
         self.steps_per_poll = int(steps_per_poll)
         self.clock = clock
+        self.device_loop = bool(device_loop)
+        self.max_loop_steps = int(max_loop_steps)
+        self.poll_interval = float(poll_interval)
+        self.sleep = sleep
         self.queue = deque()
         self.running = {}           # batch id -> (request, admitted time)
         self.used = 0
@@ -133,15 +147,44 @@ class Server:
                 self.submit(pending.popleft())
             if self.admit(now, stats):
                 stats.rebuilds += 1
-            stats.max_running = max(stats.max_running, len(self.running))
-            stats.max_bytes = max(stats.max_bytes, self.used)
+            self._track(stats)
             if self.running:
-                self.batch.run(self.steps_per_poll)
+                if self.device_loop:
+                    self._device_loop(pending, stats)
+                else:
+                    self.batch.run(self.steps_per_poll)
                 self.harvest(self.clock() - self._t0, stats)
             elif pending:
-                time.sleep(max(0.0, pending[0].arrival - (self.clock() - self._t0)))
+                self.sleep(max(0.0, pending[0].arrival - (self.clock() - self._t0)))
         stats.wall = self.clock() - self._t0
         return stats
+
+    def _track(self, stats):
+        stats.max_running = max(stats.max_running, len(self.running))
+        stats.max_bytes = max(stats.max_bytes, self.used)
+
+    def _device_loop(self, pending, stats):
+        """One device-resident loop: the GPU steps all admitted requests until one finishes.  Meanwhile
+        arrivals are queued and admitted while they fit the budget (their host-side preparation runs
+        during the GPU's steps); the first admission wakes the loop so that they join at the next start."""
+        self.batch.loop_start(self.max_loop_steps)
+        stats.loops += 1
+        woken = False
+        while True:
+            r = self.batch.loop_poll()
+            if r is not None:
+                return r
+            now = self.clock() - self._t0
+            while pending and pending[0].arrival <= now:
+                self.submit(pending.popleft())
+            if self.queue and self.admit(now, stats):
+                stats.rebuilds += 1
+                self._track(stats)
+                if not woken:
+                    self.batch.loop_wake()
+                    stats.wakes += 1
+                    woken = True
+            self.sleep(self.poll_interval)
 
 
 def serve_one_at_a_time(requests, make_operator, clock=time.perf_counter):

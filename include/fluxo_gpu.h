@@ -348,6 +348,27 @@ int fluxo_batch_instance_bytes(const fluxo_cfg* cfg, int nElems, int nSides, siz
 int fluxo_batch_last_error(fluxo_batch* b, char* buf, size_t len);
 int fluxo_batch_destroy(fluxo_batch* b);
 
+/* Device-resident request loop (no counterpart in the reference).  A server calls loop_start and goes
+ * on with host work (admitting, preparing and reading back requests); the GPU repeats the time step of
+ * all instances, one conditional while-node of a CUDA graph, without returning to the host until
+ *   FLUXO_LOOP_FINISHED    an instance finished (reached its end time or maxIter, or CALCTIMESTEP
+ *                          stopped it),
+ *   FLUXO_LOOP_WOKEN       the host called fluxo_batch_loop_wake (e.g. a request can be admitted:
+ *                          fluxo_batch_add is host-only and may be called while the loop runs; the
+ *                          instance joins at the next loop_start or run),
+ *   FLUXO_LOOP_STEP_LIMIT  maxSteps steps ran (every loop ends),
+ *   FLUXO_LOOP_IDLE        nothing was running (no step ran).
+ * The wake word is a store into mapped pinned host memory that the loop reads once per step.
+ * loop_poll returns at once (*finished 0 while the loop runs); loop_wait waits for the end; both
+ * then update every instance's status and give the steps run, the reason and the instances still
+ * running.  Each instance advances exactly as under fluxo_batch_run (the same step graph).  While a
+ * loop runs, run, get_state, set_state and loop_start return FLUXO_ENOTREADY. */
+enum { FLUXO_LOOP_IDLE = 0, FLUXO_LOOP_FINISHED = 1, FLUXO_LOOP_WOKEN = 2, FLUXO_LOOP_STEP_LIMIT = 3 };
+int fluxo_batch_loop_start(fluxo_batch* b, int maxSteps);
+int fluxo_batch_loop_wake(fluxo_batch* b);
+int fluxo_batch_loop_poll(fluxo_batch* b, int* finished, int* steps, int* reason, int* nRunning);
+int fluxo_batch_loop_wait(fluxo_batch* b, int* steps, int* reason, int* nRunning);
+
 /* ------------------------------------------------------------------------------------------
  * Host-side setup (no GPU needed).  The reference builds these arrays in InitMesh /
  * CalcMetrics from an HDF5 (HOPR) mesh; here they are generated for a periodic box

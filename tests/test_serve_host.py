@@ -22,6 +22,7 @@ class FakeBatch:
         self.live_bytes = []
 
     def add(self, mesh, U, t, t_end, cfg=None):
+        self.added_during_loop = getattr(self, "added_during_loop", 0) + (getattr(self, "loop", None) is not None)
         iid = self.next
         self.next += 1
         self.inst[iid] = dict(U=U.copy(), t=t, t_end=t_end, steps=0, done=False)
@@ -38,6 +39,26 @@ class FakeBatch:
                 s["U"] += 1.0
                 s["done"] = s["t"] >= s["t_end"]
         return sum(not s["done"] for s in self.inst.values())
+
+    # device-resident loop: one poll advances one step (a stand-in for the GPU's progress between polls)
+    def loop_start(self, max_steps):
+        assert getattr(self, "loop", None) is None, "loop_start while a loop runs"
+        self.loop = dict(max=max_steps, steps=0, woken=False,
+                         running0=sum(not s["done"] for s in self.inst.values()))
+        self.loops = getattr(self, "loops", 0) + 1
+
+    def loop_wake(self):
+        self.loop["woken"] = True
+
+    def loop_poll(self):
+        lp = self.loop
+        running = self.run(1)
+        lp["steps"] += 1
+        why = 1 if running < lp["running0"] else 2 if lp["woken"] else 3 if lp["steps"] >= lp["max"] else 0
+        if why == 0:
+            return None
+        self.loop = None
+        return lp["steps"], why, running
 
     def status(self, iid):
         s = self.inst[iid]
@@ -75,9 +96,11 @@ class CountingServer(Server):
         return n
 
 
-def test_admission_respects_budget_and_order():
+@pytest.mark.parametrize("device_loop", [True, False])
+def test_admission_respects_budget_and_order(device_loop):
     fb = FakeBatch()
-    srv = CountingServer(fb, hbm_budget=12000, instance_bytes=fake_bytes, steps_per_poll=1)
+    srv = CountingServer(fb, hbm_budget=12000, instance_bytes=fake_bytes, steps_per_poll=1,
+                         device_loop=device_loop, sleep=lambda s: None)
     reqs = make_requests(40)
     stats = srv.serve(reqs)
     assert len(stats.results) == 40
@@ -108,3 +131,38 @@ def test_stats_throughput_counts_rhs_evaluations():
     srv = Server(FakeBatch(dt=0.25), hbm_budget=10 ** 9, instance_bytes=fake_bytes)
     stats = srv.serve([Request(rid=0, cfg=FakeCfg(3), mesh=mesh(2), U=np.zeros(4), t_end=1.0)], st)
     assert stats.dof_updates() == 2 * 64 * 4 * 5
+
+
+class StepClock:
+    """A clock that advances by a fixed amount per reading (the stream's arrivals then fall inside
+    device loops, as they do on the GPU)."""
+
+    def __init__(self, dt):
+        self.t, self.dt = 0.0, dt
+
+    def __call__(self):
+        self.t += self.dt
+        return self.t
+
+
+def test_device_loop_wakes_for_arrivals_that_fit():
+    """Requests arriving while a loop runs are admitted during the loop (prepared on the host while
+    the device steps) and wake it; a loop ends otherwise only when a request finishes."""
+    fb = FakeBatch(dt=0.05)
+    rng = np.random.default_rng(3)
+    reqs = [Request(rid=i, cfg=FakeCfg(3), mesh=mesh(int(rng.integers(1, 4))), U=np.full(4, float(i)),
+                    t_end=float(rng.uniform(0.5, 1.5)), arrival=0.01 * i) for i in range(30)]
+    srv = Server(fb, hbm_budget=10 ** 9, instance_bytes=fake_bytes, clock=StepClock(1e-3), sleep=lambda s: None)
+    stats = srv.serve(reqs)
+    assert len(stats.results) == 30 and not fb.inst
+    assert stats.loops >= 2 and stats.wakes >= 1
+    assert fb.added_during_loop >= 1                   # admitted while the device stepped
+    for r in stats.results:
+        steps = int(np.ceil(reqs[r.rid].t_end / 0.05 - 1e-12))
+        assert r.steps == steps and np.array_equal(r.U, reqs[r.rid].U + steps)
+    # with a budget that holds one request, arrivals never wake the loop: they wait for memory
+    fb = FakeBatch(dt=0.05)
+    one = [Request(rid=r.rid, cfg=r.cfg, mesh=mesh(3), U=r.U, t_end=r.t_end, arrival=r.arrival) for r in reqs[:10]]
+    srv = Server(fb, hbm_budget=3000, instance_bytes=fake_bytes, clock=StepClock(1e-3), sleep=lambda s: None)
+    stats = srv.serve(one)
+    assert len(stats.results) == 10 and stats.wakes == 0 and stats.max_running == 1
