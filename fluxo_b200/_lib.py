@@ -110,7 +110,7 @@ EXPORTS = [
     "fluxo_batch_remove", "fluxo_batch_info", "fluxo_batch_stream", "fluxo_batch_instance_bytes",
     "fluxo_batch_last_error",
     "fluxo_batch_destroy", "fluxo_batch_loop_start", "fluxo_batch_loop_wake", "fluxo_batch_loop_poll",
-    "fluxo_batch_loop_wait",
+    "fluxo_batch_loop_wait", "fluxo_batch_prepare", "fluxo_batch_add_prepared", "fluxo_batch_prepared_free",
 ]
 
 # fluxo_batch_loop_* end reasons (FLUXO_LOOP_* of fluxo_gpu.h)
@@ -178,6 +178,9 @@ def load():
     lib.fluxo_batch_instance_bytes.argtypes = [P(FluxoCfg), i, i, P(sz)]
     lib.fluxo_batch_last_error.argtypes = [vp, ctypes.c_char_p, sz]
     lib.fluxo_batch_destroy.argtypes = [vp]
+    lib.fluxo_batch_prepare.argtypes = [P(FluxoCfg), i, i] + [vp] * 11 + [d, d, i, P(vp)]
+    lib.fluxo_batch_add_prepared.argtypes = [vp, vp, P(i)]
+    lib.fluxo_batch_prepared_free.argtypes = [vp]
     lib.fluxo_batch_loop_start.argtypes = [vp, i]
     lib.fluxo_batch_loop_wake.argtypes = [vp]
     lib.fluxo_batch_loop_poll.argtypes = [vp, P(i), P(i), P(i), P(i)]

@@ -22,6 +22,18 @@ def instance_bytes(cfg, n_elems, n_sides):
     return b.value
 
 
+class Prepared:
+    """A request repacked on the host (``fluxo_batch_prepare``), waiting for ``Batch.add_prepared``."""
+
+    def __init__(self, lib, p, shape):
+        self.lib, self.p, self.shape = lib, p, shape
+
+    def __del__(self):
+        if getattr(self, "p", None) is not None:
+            self.lib.fluxo_batch_prepared_free(self.p)
+            self.p = None
+
+
 class Batch:
     """A set of independent solves on one device (``fluxo_batch_*``)."""
 
@@ -62,6 +74,34 @@ class Batch:
                                      _ptr(U), float(t), float(t_end), int(max_iter), ctypes.byref(iid))
         self._check(r)
         self._shapes[iid.value] = (nE, n, n, n, 5)
+        return iid.value
+
+    def prepare(self, mesh, U, t, t_end, cfg=None, max_iter=-1, **fields):
+        """The host work of ``add`` (checks, mesh repack) without touching the batch: returns a
+        ``Prepared`` for ``add_prepared``.  Safe to call from another thread while the batch runs."""
+        cfg = cfg if cfg is not None else make_cfg(**fields)
+        S2E = _c(mesh["SideToElem"], np.int32)
+        E2S = _c(mesh["ElemToSide"], np.int32)
+        arrs = [_c(mesh[k]) for k in MESH_KEYS[2:10]]
+        U = _c(U)
+        nE, nS = E2S.shape[0], S2E.shape[0]
+        n = cfg.N + 1
+        if U.size != nE * n ** 3 * 5:
+            raise ValueError("U has the wrong size")
+        p = ctypes.c_void_p()
+        _lib.check(self.lib.fluxo_batch_prepare(ctypes.byref(cfg), nE, nS, _ptr(S2E), _ptr(E2S),
+                                                *[_ptr(a) for a in arrs], _ptr(U), float(t), float(t_end),
+                                                int(max_iter), ctypes.byref(p)), None)
+        return Prepared(self.lib, p, (nE, n, n, n, 5))
+
+    def add_prepared(self, prep):
+        """Adds a prepared instance (ownership passes to the batch); returns its id."""
+        if prep.p is None:
+            raise ValueError("prepared instance already added")
+        iid = ctypes.c_int()
+        self._check(self.lib.fluxo_batch_add_prepared(self.b, prep.p, ctypes.byref(iid)))
+        prep.p = None
+        self._shapes[iid.value] = prep.shape
         return iid.value
 
     def run(self, n_steps):

@@ -103,6 +103,12 @@ __global__ void batch_loop_cond_kernel(cudaGraphConditionalHandle h, const InstS
   cudaGraphSetConditional(h, why == 0 ? 1u : 0u);
 }
 
+// host copies of a placed instance, freed after the GPU work that follows the placement is enqueued
+// (returning a large request's 1 GB to the system takes time the GPU need not wait for)
+struct Retired {
+  std::vector<double> met, sJ, geo, U;
+};
+
 struct Instance {
   int id = 0;
   fluxo_cfg cfg{};
@@ -173,7 +179,13 @@ struct fluxo_batch {
   int hStatesCap = 0;
   cudaEvent_t loopEnd = nullptr;
   bool loopActive = false;
+  std::vector<Retired> retired;                // host copies of newly placed instances (freed after launch)
   std::string lastError;
+};
+
+// an instance repacked on the host, not yet in a batch (fluxo_batch_prepare)
+struct fluxo_batch_prepared {
+  Instance inst;
 };
 
 namespace {
@@ -420,8 +432,9 @@ int commit(fluxo_batch* b) {
     Instance& I = it->second;
     if (!I.placed) {
       I.placed = true;
-      std::vector<double>().swap(I.met); std::vector<double>().swap(I.sJ);
-      std::vector<double>().swap(I.geo); std::vector<double>().swap(I.U);
+      Retired r;
+      r.met.swap(I.met); r.sJ.swap(I.sJ); r.geo.swap(I.geo); r.U.swap(I.U);
+      b->retired.push_back(std::move(r));
     }
     ++it;
   }
@@ -567,6 +580,40 @@ int check_cfg(const fluxo_cfg* c, std::string& msg) {
   return FLUXO_OK;
 }
 
+// Host-only part of an admission: configuration checks, the mesh repacked into the device layout,
+// the initial state and time-loop state (no batch state is touched, so any host thread may run it).
+int prepare_instance(const fluxo_cfg* cfg, int nElems, int nSides, const int* SideToElem, const int* ElemToSide,
+                     const double* Mf, const double* Mg, const double* Mh, const double* sJ, const double* NormVec,
+                     const double* TangVec1, const double* TangVec2, const double* SurfElem, const double* U,
+                     double t, double tEnd, int maxIter, Instance& I, std::string& msg) {
+  int r = check_cfg(cfg, msg);
+  if (r) return r;
+  if (nElems < 1 || nSides < 1 || !SideToElem || !ElemToSide || !Mf || !Mg || !Mh || !sJ || !NormVec || !TangVec1 ||
+      !TangVec2 || !SurfElem || !U) {
+    msg = "missing array";
+    return FLUXO_EINVAL_CFG;
+  }
+  I.cfg = *cfg;
+  I.nElems = nElems; I.nSides = nSides;
+  if (!host::repack_mesh(cfg->N, nElems, nSides, SideToElem, ElemToSide, Mf, Mg, Mh, NormVec, TangVec1, TangVec2,
+                         SurfElem, I.s2e, I.e2s, I.met, I.geo, msg))
+    return FLUXO_EINVAL_CFG;
+  const size_t NP3 = (size_t)(cfg->N + 1) * (cfg->N + 1) * (cfg->N + 1);
+  I.sJ.assign(sJ, sJ + NP3 * nElems);
+  I.U.assign(U, U + 5 * NP3 * nElems);
+  I.st.t = t; I.st.tEnd = tEnd; I.st.dt = 0.; I.st.iter = 0; I.st.maxIter = maxIter; I.st.last = 0;
+  I.st.done = (t >= tEnd || maxIter == 0) ? 1 : 0;
+  I.st.err = 0;
+  return FLUXO_OK;
+}
+
+void add_instance(fluxo_batch* b, Instance&& I, int* id) {
+  I.id = b->nextId++;
+  *id = I.id;
+  b->inst[I.id] = std::move(I);
+  b->dirty = true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -592,33 +639,47 @@ int fluxo_batch_create(int device, fluxo_batch** out) {
   return FLUXO_OK;
 }
 
+int fluxo_batch_prepare(const fluxo_cfg* cfg, int nElems, int nSides, const int* SideToElem, const int* ElemToSide,
+                        const double* Mf, const double* Mg, const double* Mh, const double* sJ, const double* NormVec,
+                        const double* TangVec1, const double* TangVec2, const double* SurfElem, const double* U,
+                        double t, double tEnd, int maxIter, fluxo_batch_prepared** out) {
+  if (!out) return bfail(nullptr, FLUXO_EINVAL_CFG, "batch_prepare: null argument");
+  *out = nullptr;
+  fluxo_batch_prepared* p = new fluxo_batch_prepared();
+  std::string msg;
+  const int r = prepare_instance(cfg, nElems, nSides, SideToElem, ElemToSide, Mf, Mg, Mh, sJ, NormVec, TangVec1,
+                                 TangVec2, SurfElem, U, t, tEnd, maxIter, p->inst, msg);
+  if (r) {
+    delete p;
+    return bfail(nullptr, r, "batch_prepare: " + msg);
+  }
+  *out = p;
+  return FLUXO_OK;
+}
+
+int fluxo_batch_add_prepared(fluxo_batch* b, fluxo_batch_prepared* p, int* id) {
+  if (!b || !p || !id) return bfail(b, FLUXO_EINVAL_CFG, "batch_add_prepared: null argument");
+  add_instance(b, std::move(p->inst), id);
+  delete p;
+  return FLUXO_OK;
+}
+
+int fluxo_batch_prepared_free(fluxo_batch_prepared* p) {
+  delete p;
+  return FLUXO_OK;
+}
+
 int fluxo_batch_add(fluxo_batch* b, const fluxo_cfg* cfg, int nElems, int nSides, const int* SideToElem,
                     const int* ElemToSide, const double* Mf, const double* Mg, const double* Mh, const double* sJ,
                     const double* NormVec, const double* TangVec1, const double* TangVec2, const double* SurfElem,
                     const double* U, double t, double tEnd, int maxIter, int* id) {
   if (!b || !id) return bfail(b, FLUXO_EINVAL_CFG, "null argument");
-  std::string msg;
-  int r = check_cfg(cfg, msg);
-  if (r) return bfail(b, r, "batch_add: " + msg);
-  if (nElems < 1 || nSides < 1 || !SideToElem || !ElemToSide || !Mf || !Mg || !Mh || !sJ || !NormVec || !TangVec1 ||
-      !TangVec2 || !SurfElem || !U)
-    return bfail(b, FLUXO_EINVAL_CFG, "batch_add: missing array");
   Instance I;
-  I.id = b->nextId++;
-  I.cfg = *cfg;
-  I.nElems = nElems; I.nSides = nSides;
-  if (!host::repack_mesh(cfg->N, nElems, nSides, SideToElem, ElemToSide, Mf, Mg, Mh, NormVec, TangVec1, TangVec2,
-                         SurfElem, I.s2e, I.e2s, I.met, I.geo, msg))
-    return bfail(b, FLUXO_EINVAL_CFG, "batch_add: " + msg);
-  const size_t NP3 = (size_t)(cfg->N + 1) * (cfg->N + 1) * (cfg->N + 1);
-  I.sJ.assign(sJ, sJ + NP3 * nElems);
-  I.U.assign(U, U + 5 * NP3 * nElems);
-  I.st.t = t; I.st.tEnd = tEnd; I.st.dt = 0.; I.st.iter = 0; I.st.maxIter = maxIter; I.st.last = 0;
-  I.st.done = (t >= tEnd || maxIter == 0) ? 1 : 0;
-  I.st.err = 0;
-  *id = I.id;
-  b->inst[I.id] = std::move(I);
-  b->dirty = true;
+  std::string msg;
+  const int r = prepare_instance(cfg, nElems, nSides, SideToElem, ElemToSide, Mf, Mg, Mh, sJ, NormVec, TangVec1,
+                                 TangVec2, SurfElem, U, t, tEnd, maxIter, I, msg);
+  if (r) return bfail(b, r, "batch_add: " + msg);
+  add_instance(b, std::move(I), id);
   return FLUXO_OK;
 }
 
@@ -646,6 +707,7 @@ int fluxo_batch_run(fluxo_batch* b, int nSteps, int* nRunning) {
     for (auto& kv : b->inst)
       if (kv.second.slot >= 0 && kv.second.slot < b->nInst) kv.second.st = hs[kv.second.slot];
   }
+  b->retired.clear();
   if (nRunning) *nRunning = running;
   return FLUXO_OK;
 }
@@ -730,6 +792,7 @@ int fluxo_batch_loop_start(fluxo_batch* b, int maxSteps) {
                                 b->stream));
   BATCH_CUDA(b, cudaEventRecord(b->loopEnd, b->stream));
   b->loopActive = true;
+  b->retired.clear();  // the uploads completed inside commit; freeing overlaps the loop
   return FLUXO_OK;
 }
 

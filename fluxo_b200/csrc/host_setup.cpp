@@ -529,16 +529,20 @@ bool repack_mesh(int N, int nElems, int nSides, const int* S2E, const int* E2S, 
       e2s[2 * (6 * (size_t)e + ls)] = sid - 1;
       e2s[2 * (6 * (size_t)e + ls) + 1] = fl;
     }
-  met.assign((size_t)9 * NP3 * nElems, 0.);
-  geo.assign((size_t)10 * NPT * nSides, 0.);
+  met.resize((size_t)9 * NP3 * nElems);
+  geo.resize((size_t)10 * NPT * nSides);
+  // element- and side-parallel: a large request (24^3 elements at N=7, 0.7 GB) is repacked while a
+  // served batch keeps the GPU busy, and before the first step of a single solve
+#pragma omp parallel for schedule(static)
   for (int e = 0; e < nElems; ++e)
-    for (int n = 0; n < NP3; ++n)
-      for (int d = 0; d < 3; ++d) {
+    for (int d = 0; d < 3; ++d)
+      for (int n = 0; n < NP3; ++n) {
         const size_t src = 3 * ((size_t)e * NP3 + n) + d;
         met[((size_t)e * 9 + d) * NP3 + n] = Mf[src];
         met[((size_t)e * 9 + 3 + d) * NP3 + n] = Mg[src];
         met[((size_t)e * 9 + 6 + d) * NP3 + n] = Mh[src];
       }
+#pragma omp parallel for schedule(static)
   for (int s = 0; s < nSides; ++s)
     for (int p = 0; p < NPT; ++p) {
       const size_t src = (size_t)s * NPT + p;

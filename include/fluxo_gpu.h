@@ -333,6 +333,20 @@ int fluxo_batch_add(fluxo_batch* b, const fluxo_cfg* cfg, int nElems, int nSides
                     const double* Metrics_hTilde, const double* sJ, const double* NormVec,
                     const double* TangVec1, const double* TangVec2, const double* SurfElem, const double* U,
                     double t, double tEnd, int maxIter, int* id);
+/* The same admission in two parts, so that its host work can run ahead of it: fluxo_batch_prepare
+ * checks the configuration and repacks the mesh arrays and U on the host into an opaque object (it
+ * touches no batch and no GPU, and any host thread may call it while a batch runs);
+ * fluxo_batch_add_prepared hands that object to a batch (it takes ownership; nothing is copied) and
+ * returns the instance id; fluxo_batch_prepared_free drops one that is not added.  Errors of prepare:
+ * fluxo_gpu_last_error(NULL, ...). */
+typedef struct fluxo_batch_prepared fluxo_batch_prepared;
+int fluxo_batch_prepare(const fluxo_cfg* cfg, int nElems, int nSides, const int* SideToElem, const int* ElemToSide,
+                        const double* Metrics_fTilde, const double* Metrics_gTilde, const double* Metrics_hTilde,
+                        const double* sJ, const double* NormVec, const double* TangVec1, const double* TangVec2,
+                        const double* SurfElem, const double* U, double t, double tEnd, int maxIter,
+                        fluxo_batch_prepared** out);
+int fluxo_batch_add_prepared(fluxo_batch* b, fluxo_batch_prepared* p, int* id);
+int fluxo_batch_prepared_free(fluxo_batch_prepared* p);
 int fluxo_batch_run(fluxo_batch* b, int nSteps, int* nRunning);
 int fluxo_batch_status(fluxo_batch* b, int id, double* t, int* nIter, int* done, int* errType);
 int fluxo_batch_get_state(fluxo_batch* b, int id, double* U);

@@ -149,7 +149,7 @@ def compatible(ctype, kind, value):
         return kind == "C_PTR" and not value
     base = ctype[:-1]
     if value:  # a pointer passed as an address
-        return kind == "C_PTR" and base in ("void", "fluxo_handle", "fluxo_batch", "double", "int")
+        return kind == "C_PTR" and base in ("void", "fluxo_handle", "fluxo_batch", "fluxo_batch_prepared", "double", "int")
     return {"int": "C_INT", "double": "C_DOUBLE", "size_t": "C_SIZE_T", "uint64_t": "C_INT64_T", "char": "C_CHAR",
             "fluxo_cfg": "fluxo_cfg", "fluxo_exact": "fluxo_exact"}.get(base) == kind
 

@@ -90,3 +90,23 @@ def test_device_loop_ends_and_matches_run(gpu_lib):
     assert b1.loop_wait() == (0, _lib.LOOP_IDLE, 0)
     b1.close()
     b2.close()
+
+
+def test_prepared_admission_equals_add(gpu_lib):
+    """fluxo_batch_prepare (run on another thread) + fluxo_batch_add_prepared gives the same instance as
+    fluxo_batch_add: same steps and identical states."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    reqs = requests(3)
+    b1, b2 = Batch(), Batch()
+    with ThreadPoolExecutor(1) as ex:
+        preps = [ex.submit(b1.prepare, r.mesh, r.U, 0.0, r.t_end, cfg=r.cfg) for r in reqs]
+        ids1 = [b1.add_prepared(f.result()) for f in preps]
+    ids2 = [b2.add(r.mesh, r.U, 0.0, r.t_end, cfg=r.cfg) for r in reqs]
+    b1.run_to_end()
+    b2.run_to_end()
+    for i1, i2 in zip(ids1, ids2):
+        assert b1.status(i1) == b2.status(i2) and b1.status(i1)[2]
+        assert np.array_equal(b1.get_state(i1), b2.get_state(i2))
+    b1.close()
+    b2.close()

@@ -90,8 +90,8 @@ def make_requests(n, seed=0):
 
 
 class CountingServer(Server):
-    def admit(self, now, stats=None):
-        n = super().admit(now, stats)
+    def admit(self, now, stats=None, ready_only=False):
+        n = super().admit(now, stats, ready_only)
         assert self.used <= self.budget
         return n
 
@@ -166,3 +166,36 @@ def test_device_loop_wakes_for_arrivals_that_fit():
     srv = Server(fb, hbm_budget=3000, instance_bytes=fake_bytes, clock=StepClock(1e-3), sleep=lambda s: None)
     stats = srv.serve(one)
     assert len(stats.results) == 10 and stats.wakes == 0 and stats.max_running == 1
+
+
+class PreparingBatch(FakeBatch):
+    """A fake batch with the two-part admission: prepare (host work, any thread) and add_prepared."""
+
+    def prepare(self, mesh, U, t, t_end, cfg=None):
+        self.prepared = getattr(self, "prepared", 0) + 1
+        return ("prepared", mesh, U.copy(), t, t_end, cfg)
+
+    def add_prepared(self, p):
+        assert p[0] == "prepared"
+        return self.add(p[1], p[2], p[3], p[4], cfg=p[5])
+
+
+def test_requests_are_prepared_ahead_of_admission():
+    """Requests queued behind others are prepared on the worker thread before their admission, and
+    the results are those of plain admissions."""
+    fb = PreparingBatch(dt=0.05)
+    reqs = make_requests(25, seed=5)
+    srv = Server(fb, hbm_budget=12000, instance_bytes=fake_bytes, clock=StepClock(1e-3), sleep=lambda s: None)
+    stats = srv.serve(reqs)
+    assert len(stats.results) == 25 and fb.prepared >= 20 and fb.order == list(range(25))
+    for r in stats.results:
+        steps = int(np.ceil(reqs[r.rid].t_end / 0.05 - 1e-12))
+        assert r.steps == steps and np.array_equal(r.U, reqs[r.rid].U + steps)
+    # the preparation holds at most prepare_budget bytes beyond the admitted requests (the first one
+    # always starts)
+    srv = Server(PreparingBatch(), hbm_budget=12000, instance_bytes=fake_bytes, prepare_budget=3000)
+    for r in make_requests(10, seed=6):
+        srv.submit(r)
+    srv.prepare()
+    started = [r for r in srv.queue if r.prepared is not None]
+    assert len(started) >= 1 and (len(started) == 1 or sum(r.nbytes for r in started) <= 3000)
