@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(512) timestep_kernel(KParams P, unsigned long 
   constexpr int NP3 = NP * NP * NP;
   constexpr int EPB = (256 / NP3) > 0 ? (256 / NP3) : 1;
   constexpr int RSTART = (NP3 > 256) ? 256 : (NP3 > 128) ? 128 : (NP3 > 64) ? 64 : (NP3 > 32) ? 32 : (NP3 > 16) ? 16 : (NP3 > 8) ? 8 : 4;
-  __shared__ double s_l[EPB][6][NP3];
+  __shared__ double s_l[EPB][6][NP3 % 32 == 0 ? 1 : NP3];
   __shared__ int s_err[EPB];
   const int eb = threadIdx.x / NP3, n = threadIdx.x - eb * NP3;
   const int e = blockIdx.x * EPB + eb;
@@ -441,16 +441,33 @@ __global__ void __launch_bounds__(512) timestep_kernel(KParams P, unsigned long 
       }
     }
   }
-  // per-element max: tree reduction in shared memory
+  // per-element max (fmax is exact, so the order of the reduction does not change the result)
   if (code != 0) atomicMax(&s_err[eb], n * 8 + code);
-  for (int d = 0; d < 6; ++d) s_l[eb][d][n] = lam[d];
-  __syncthreads();
-  for (int stride = RSTART; stride > 0; stride >>= 1) {
-    if (n < stride && n + stride < NP3)
-      for (int d = 0; d < 6; ++d) s_l[eb][d][n] = fmax(s_l[eb][d][n], s_l[eb][d][n + stride]);
+  if constexpr (NP3 % 32 == 0) {  // whole warps per element: shuffles, then one value per warp
+    constexpr int WPE = NP3 / 32;
+    __shared__ double s_w[EPB * WPE][6];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int d = 0; d < 6; ++d) lam[d] = fmax(lam[d], __shfl_xor_sync(0xffffffffu, lam[d], o));
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+      for (int d = 0; d < 6; ++d) s_w[threadIdx.x >> 5][d] = lam[d];
     __syncthreads();
+    if (n == 0)
+      for (int w = 1; w < WPE; ++w)
+#pragma unroll
+        for (int d = 0; d < 6; ++d) lam[d] = fmax(lam[d], s_w[eb * WPE + w][d]);
+  } else {  // tree reduction in shared memory
+    for (int d = 0; d < 6; ++d) s_l[eb][d][n] = lam[d];
+    __syncthreads();
+    for (int stride = RSTART; stride > 0; stride >>= 1) {
+      if (n < stride && n + stride < NP3)
+        for (int d = 0; d < 6; ++d) s_l[eb][d][n] = fmax(s_l[eb][d][n], s_l[eb][d][n + stride]);
+      __syncthreads();
+    }
+    for (int d = 0; d < 6; ++d) lam[d] = s_l[eb][d][0];
   }
-  for (int d = 0; d < 6; ++d) lam[d] = s_l[eb][d][0];
   if (n != 0 || !valid) return;
   int err = (s_err[eb] >= 0) ? (s_err[eb] & 7) : 0;
   double dtE = P.CFLScale * 2. / (lam[0] + lam[1] + lam[2]);
