@@ -878,6 +878,7 @@ int fluxo_batch_last_error(fluxo_batch* b, char* buf, size_t len) {
 int fluxo_batch_destroy(fluxo_batch* b) {
   if (!b) return FLUXO_OK;
   cudaSetDevice(b->device);
+  if (b->loopActive) fluxo_batch_loop_wake(b);  // a running loop ends after its current step
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
