@@ -61,7 +61,7 @@ LIFT_FLUX_BYTES_PER_POINT = 16 * 8
 # the F_alg fraction sits below where a kernel spends FP64 instructions that F_alg counts as one flop
 # (division, logarithm) or issues products and sums that a multiply-add would fuse.
 NCU_DRAM_BYTES_PER_DOF = {"volume": 290.2, "gradient": 206.8, "face_flux": 99.5, "lift_flux": 47.7}
-NCU_FP64_PIPE_ACTIVE = {"volume": 0.458, "gradient": 0.288, "face_flux": 0.372}
+NCU_FP64_PIPE_ACTIVE = {"volume": 0.458, "gradient": 0.204, "face_flux": 0.372}  # gradient: DMMA tiles 0.119 more
 VOLUME_KERNEL_DRAM_BYTES_PER_DOF = NCU_DRAM_BYTES_PER_DOF["volume"]
 
 METRIC = "PID ns/DOF/RHS, NS Taylor-Green N=7 32^3 curved, BR1 + EC-KEP + ES (Riemann 44), LSERK4-5"
@@ -493,7 +493,8 @@ def kernel_rooflines(kinds, N, nd, nElems, fp64_peak):
     npts = 3 * nElems * (N + 1) ** 2
     out = {}
     for k, name, falg in (("volume", "volume_kernel<%d,5,true>" % (N + 1), VOLUME_KERNEL_FALG),
-                          ("gradient", "lift_visc_kernel<%d,1,3>" % (N + 1), LIFTING_KERNEL_FALG)):
+                          ("gradient", "lift_visc_mma_kernel<1,3>" if N == 7 else "lift_visc_kernel<%d,1,3>" % (N + 1),
+                           LIFTING_KERNEL_FALG)):
         ms, n = kinds.get(k, (0.0, 0))
         if n:
             a = falg * nd / (ms / n * 1e-3) / 1e12
