@@ -772,6 +772,7 @@ def measure_serve(args, world, rank, local):
               "loop": ("host-polled, %d steps per poll" % args.poll_steps) if args.host_poll
               else "device-resident (CUDA graph while-node)",
               "device_loops": served.loops, "loop_wakes": served.wakes,
+              "host_loop_start_s": served.start_s, "host_harvest_s": served.harvest_s,
               "stopped_by_calctimestep": len(failed),
               "parallelism": "replicas x%d (own stream per rank)" % world}
     line = {"metric": SERVE_METRIC, "value": value, "unit": "DOF-updates/s", "n_gpus": world, "steps": len(reqs),

@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "libfluxo_gpu.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fopenmp",
                      "--expt-relaxed-constexpr", "-I" + CSRC]
-CU_SOURCES = (["fluxo_gpu.cu", "launch_misc.cu", "lift_impl.cu", "noalloc.cu", "analyze.cu"] +
+CU_SOURCES = (["fluxo_gpu.cu", "launch_misc.cu", "lift_impl.cu", "noalloc.cu", "analyze.cu", "host_copy.cu"] +
               ["vol_vf%d.cu" % v for v in (0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 32)] +
               ["mhd_launch.cu", "mhd_vol_ec.cu", "mhd_vol_std.cu", "nfvse_launch.cu", "nfvse_ns.cu", "batch.cu",
                "gauss_launch.cu", "gauss_surf.cu", "gauss_mhd.cu"])

@@ -27,6 +27,7 @@
 #include "../../include/fluxo_gpu.h"
 #include "common.cuh"
 #include "host_setup.h"
+#include "host_copy.h"
 #include "launch.h"
 
 using namespace fluxo;
@@ -399,10 +400,10 @@ int commit(fluxo_batch* b) {
           BATCH_CUDA(b, cudaMemcpyAsync(g.facegeo + sG * so, old.facegeo + sG * I.sideOff, sG * I.nSides * 8,
                                         cudaMemcpyDeviceToDevice, s));
         } else {
-          BATCH_CUDA(b, cudaMemcpyAsync(g.U + eU * eo, I.U.data(), eU * I.nElems * 8, cudaMemcpyHostToDevice, s));
-          BATCH_CUDA(b, cudaMemcpyAsync(g.metrics + eM * eo, I.met.data(), eM * I.nElems * 8, cudaMemcpyHostToDevice, s));
-          BATCH_CUDA(b, cudaMemcpyAsync(g.sJ + eJ * eo, I.sJ.data(), eJ * I.nElems * 8, cudaMemcpyHostToDevice, s));
-          BATCH_CUDA(b, cudaMemcpyAsync(g.facegeo + sG * so, I.geo.data(), sG * I.nSides * 8, cudaMemcpyHostToDevice, s));
+          BATCH_CUDA(b, copy_h2d(g.U + eU * eo, I.U.data(), eU * I.nElems * 8, s));
+          BATCH_CUDA(b, copy_h2d(g.metrics + eM * eo, I.met.data(), eM * I.nElems * 8, s));
+          BATCH_CUDA(b, copy_h2d(g.sJ + eJ * eo, I.sJ.data(), eJ * I.nElems * 8, s));
+          BATCH_CUDA(b, copy_h2d(g.facegeo + sG * so, I.geo.data(), sG * I.nSides * 8, s));
         }
         I.elemOff = eo; I.sideOff = so; I.group = (int)gi;
         eo += I.nElems; so += I.nSides;
@@ -738,8 +739,7 @@ int fluxo_batch_get_state(fluxo_batch* b, int id, double* U) {
   BATCH_CUDA(b, cudaSetDevice(b->device));
   const Group& g = b->groups[I.group];
   const size_t eU = (size_t)5 * g.NP * g.NP * g.NP;
-  BATCH_CUDA(b, cudaMemcpyAsync(U, g.U + eU * I.elemOff, n * 8, cudaMemcpyDeviceToHost, b->stream));
-  BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
+  BATCH_CUDA(b, copy_d2h(U, g.U + eU * I.elemOff, n * 8, b->stream));
   return FLUXO_OK;
 }
 

@@ -16,6 +16,7 @@
 #include "common.cuh"
 #include "host_basis.h"
 #include "host_setup.h"
+#include "host_copy.h"
 #include "launch.h"
 #include "time_disc.h"
 #include "vol_shapes.h"
@@ -798,9 +799,9 @@ int fluxo_gpu_set_mesh(fluxo_handle* h, int nElems, int nSides, const int* S2E, 
     if (h->cfg.nfvse_corr) FLUXO_CUDA(h, cudaMemsetAsync(h->dFFV, 0, nU * sizeof(double), h->stream));
   }
   cudaStream_t s = h->stream;
-  FLUXO_CUDA(h, cudaMemcpyAsync(h->dMetrics, met.data(), met.size() * 8, cudaMemcpyHostToDevice, s));
-  FLUXO_CUDA(h, cudaMemcpyAsync(h->dsJ, sJ, (size_t)NP3 * nElems * 8, cudaMemcpyHostToDevice, s));
-  FLUXO_CUDA(h, cudaMemcpyAsync(h->dFaceGeo, geo.data(), geo.size() * 8, cudaMemcpyHostToDevice, s));
+  FLUXO_CUDA(h, copy_h2d(h->dMetrics, met.data(), met.size() * 8, s));
+  FLUXO_CUDA(h, copy_h2d(h->dsJ, sJ, (size_t)NP3 * nElems * 8, s));
+  FLUXO_CUDA(h, copy_h2d(h->dFaceGeo, geo.data(), geo.size() * 8, s));
   FLUXO_CUDA(h, cudaMemcpyAsync(h->dS2E, s2e.data(), s2e.size() * 4, cudaMemcpyHostToDevice, s));
   FLUXO_CUDA(h, cudaMemcpyAsync(h->dE2S, e2s.data(), e2s.size() * 4, cudaMemcpyHostToDevice, s));
   FLUXO_CUDA(h, cudaMemsetAsync(h->dUtTmp, 0, nU * 8, s));
@@ -840,7 +841,7 @@ int fluxo_gpu_set_state(fluxo_handle* h, const double* U) {
   if (!h->meshSet) return fail(h, FLUXO_ENOTREADY, "mesh not set");
   FLUXO_CUDA(h, cudaSetDevice(h->cfg.device));
   const size_t nU = (size_t)h->nVar * h->NP * h->NP * h->NP * h->nElems;
-  FLUXO_CUDA(h, cudaMemcpyAsync(h->dU, U, nU * 8, cudaMemcpyHostToDevice, h->stream));
+  FLUXO_CUDA(h, copy_h2d(h->dU, U, nU * 8, h->stream));
   FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
   h->stateSet = true;
   return FLUXO_OK;
@@ -850,7 +851,7 @@ int fluxo_gpu_get_state(fluxo_handle* h, double* U) {
   int r = check_ready(h);
   if (r) return r;
   const size_t nU = (size_t)h->nVar * h->NP * h->NP * h->NP * h->nElems;
-  FLUXO_CUDA(h, cudaMemcpyAsync(U, h->dU, nU * 8, cudaMemcpyDeviceToHost, h->stream));
+  FLUXO_CUDA(h, copy_d2h(U, h->dU, nU * 8, h->stream));
   FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
   return FLUXO_OK;
 }
@@ -859,7 +860,7 @@ int fluxo_gpu_get_ut(fluxo_handle* h, double* Ut) {
   int r = check_ready(h);
   if (r) return r;
   const size_t nU = (size_t)h->nVar * h->NP * h->NP * h->NP * h->nElems;
-  FLUXO_CUDA(h, cudaMemcpyAsync(Ut, h->dUt, nU * 8, cudaMemcpyDeviceToHost, h->stream));
+  FLUXO_CUDA(h, copy_d2h(Ut, h->dUt, nU * 8, h->stream));
   FLUXO_CUDA(h, cudaStreamSynchronize(h->stream));
   return FLUXO_OK;
 }

@@ -66,6 +66,8 @@ class ServeStats:
     rebuilds: int = 0
     loops: int = 0                  # device-resident loops started
     wakes: int = 0                  # loops the host woke for an admission
+    start_s: float = 0.0            # host time in loop starts (placing admitted requests, graph launch)
+    harvest_s: float = 0.0          # host time reading back and removing finished requests
     max_running: int = 0
     max_bytes: int = 0
     waited_for_memory: set = field(default_factory=set)  # requests that queued because the budget was full
@@ -185,7 +187,9 @@ class Server:
                     self._device_loop(pending, stats)
                 else:
                     self.batch.run(self.steps_per_poll)
-                self.harvest(self.clock() - self._t0, stats)
+                h0 = self.clock()
+                self.harvest(h0 - self._t0, stats)
+                stats.harvest_s += self.clock() - h0
             elif pending:
                 self.sleep(max(0.0, pending[0].arrival - (self.clock() - self._t0)))
         stats.wall = self.clock() - self._t0
@@ -199,7 +203,9 @@ class Server:
         """One device-resident loop: the GPU steps all admitted requests until one finishes.  Meanwhile
         arrivals are queued and admitted while they fit the budget (their host-side preparation runs
         during the GPU's steps); the first admission wakes the loop so that they join at the next start."""
+        s0 = self.clock()
         self.batch.loop_start(self.max_loop_steps)
+        stats.start_s += self.clock() - s0
         stats.loops += 1
         woken = False
         while True:
