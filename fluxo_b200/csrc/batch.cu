@@ -8,7 +8,8 @@
 //     per-instance minimum, the LSERK update reads the element's instance dt, and a finished
 //     instance gets dt = 0 until it is removed;
 //   * one time step of all groups (CALCTIMESTEP, the stages, the per-instance bookkeeping) is
-//     captured once as a CUDA graph and replayed; the graph is rebuilt when instances join or leave;
+//     captured once as a CUDA graph and replayed; the graph is captured again after instances join or
+//     leave, when a run needs it;
 //   * the request loop of a server runs on the device: a second graph repeats that step inside a
 //     conditional while-node until an instance finishes, the host raises a wake word in mapped pinned
 //     memory (a request can be admitted), or a step limit is reached (fluxo_batch_loop_start).
@@ -461,19 +462,26 @@ int commit(fluxo_batch* b) {
   for (const Group& g : b->groups)
     if (g.nElems > 0 && volume_shape(g.NP, g.key.volume_flux, g.visc) < 0)
       BATCH_CUDA(b, tune_volume(g.NP, g.key.volume_flux, g.visc, g.nElems, s, group_params(b, g)));
-  if (nInst > 0) {
-    BATCH_CUDA(b, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = enqueue_step(b);
-    cudaGraph_t gr = nullptr;
-    cudaError_t e2 = cudaStreamEndCapture(s, &gr);
-    if (e != cudaSuccess || e2 != cudaSuccess) {
-      if (gr) cudaGraphDestroy(gr);
-      return bfail(b, FLUXO_ECUDA, std::string("step capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
-    }
-    b->graph = gr;
-    BATCH_CUDA(b, cudaGraphInstantiate(&b->exec, b->graph, 0));
-  }
+  // the step graph itself is captured by the first fluxo_batch_run after this (a server that only
+  // runs device-resident loops captures the loop graph alone)
   b->dirty = false;
+  return FLUXO_OK;
+}
+
+// The step graph (one time step of all groups), captured when a run needs it.
+int build_step_graph(fluxo_batch* b) {
+  if (b->exec || b->nInst == 0) return FLUXO_OK;
+  cudaStream_t s = b->stream;
+  BATCH_CUDA(b, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = enqueue_step(b);
+  cudaGraph_t gr = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(s, &gr);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (gr) cudaGraphDestroy(gr);
+    return bfail(b, FLUXO_ECUDA, std::string("step capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  b->graph = gr;
+  BATCH_CUDA(b, cudaGraphInstantiate(&b->exec, b->graph, 0));
   return FLUXO_OK;
 }
 
@@ -690,6 +698,7 @@ int fluxo_batch_run(fluxo_batch* b, int nSteps, int* nRunning) {
   BATCH_CUDA(b, cudaSetDevice(b->device));
   int r = commit(b);
   if (r) return r;
+  if ((r = build_step_graph(b))) return r;
   int running = 0;
   if (b->nInst > 0) {
     const int chunk = 8;
