@@ -726,7 +726,8 @@ def measure_serve(args, world, rank, local):
     # warm-up: a short stream of the first requests (library, context and graph paths), untimed
     warm = [Request(rid=r.rid, cfg=r.cfg, mesh=r.mesh, U=r.U, t_end=r.t_end * 0.05, arrival=0.0) for r in reqs[:3]]
     b = Batch(device=local)
-    Server(b, budget, instance_bytes).serve(warm)
+    with Server(b, budget, instance_bytes) as warm_srv:
+        warm_srv.serve(warm)
     b.close()
     serve_one_at_a_time(warm[:1], lambda cfg: fb.DGOperator(cfg=cfg))
 
@@ -737,6 +738,7 @@ def measure_serve(args, world, rank, local):
     with ClockSampler(local) as clk:
         served = srv.serve(reqs)
         torch.cuda.synchronize(dev)
+    srv.close()
     b.close()
     barrier(world)
     plain = None

@@ -111,6 +111,19 @@ class Server:
         self.running = {}           # batch id -> (request, admitted time)
         self.used = 0
 
+    def close(self):
+        """Stops the preparation worker (requests still queued keep their preparations)."""
+        if self._pool is not None:
+            self._pool.shutdown(wait=True)
+            self._pool = None
+            self.prepare_ahead = False
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
     def submit(self, req):
         if not req.nbytes:
             nE = req.mesh["ElemToSide"].shape[0]

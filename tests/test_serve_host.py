@@ -199,3 +199,10 @@ def test_requests_are_prepared_ahead_of_admission():
     srv.prepare()
     started = [r for r in srv.queue if r.prepared is not None]
     assert len(started) >= 1 and (len(started) == 1 or sum(r.nbytes for r in started) <= 3000)
+
+
+def test_close_stops_the_preparation_worker():
+    srv = Server(PreparingBatch(), hbm_budget=12000, instance_bytes=fake_bytes)
+    with srv:
+        stats = srv.serve(make_requests(5, seed=9))
+    assert len(stats.results) == 5 and srv._pool is None and not srv.prepare_ahead
