@@ -376,7 +376,8 @@ int fluxo_batch_destroy(fluxo_batch* b);
  * loop_poll returns at once (*finished 0 while the loop runs); loop_wait waits for the end; both
  * then update every instance's status and give the steps run, the reason and the instances still
  * running.  Each instance advances exactly as under fluxo_batch_run (the same step graph).  While a
- * loop runs, run, get_state, set_state and loop_start return FLUXO_ENOTREADY. */
+ * loop runs, run, get_state, set_state and loop_start return FLUXO_ENOTREADY; fluxo_batch_destroy wakes
+ * a running loop and waits for its end. */
 enum { FLUXO_LOOP_IDLE = 0, FLUXO_LOOP_FINISHED = 1, FLUXO_LOOP_WOKEN = 2, FLUXO_LOOP_STEP_LIMIT = 3 };
 int fluxo_batch_loop_start(fluxo_batch* b, int maxSteps);
 int fluxo_batch_loop_wake(fluxo_batch* b);
