@@ -60,7 +60,7 @@ LIFT_FLUX_BYTES_PER_POINT = 16 * 8
 # (sm__pipe_fp64_cycles_active, --set full on the 16^3 case, profiles/*_ns_tgv_N7_16x16x16.md), which
 # the F_alg fraction sits below where a kernel spends FP64 instructions that F_alg counts as one flop
 # (division, logarithm) or issues products and sums that a multiply-add would fuse.
-NCU_DRAM_BYTES_PER_DOF = {"volume": 290.2, "gradient": 206.8, "face_flux": 99.5, "lift_flux": 47.7}
+NCU_DRAM_BYTES_PER_DOF = {"volume": 321.0, "gradient": 209.1, "face_flux": 107.9, "lift_flux": 47.8}
 NCU_FP64_PIPE_ACTIVE = {"volume": 0.458, "gradient": 0.204, "face_flux": 0.372}  # gradient: DMMA tiles 0.119 more
 VOLUME_KERNEL_DRAM_BYTES_PER_DOF = NCU_DRAM_BYTES_PER_DOF["volume"]
 
