@@ -152,6 +152,13 @@ class Batch:
         self._check(self.lib.fluxo_batch_get_state(self.b, int(iid), _ptr(U)))
         return U
 
+    def set_state(self, iid, U):
+        """Overwrites the instance's U (``fluxo_batch_set_state``; its time and step count stay)."""
+        U = _c(U)
+        if U.size != int(np.prod(self._shapes[iid])):
+            raise ValueError("U has the wrong size")
+        self._check(self.lib.fluxo_batch_set_state(self.b, int(iid), _ptr(U)))
+
     def remove(self, iid):
         self._check(self.lib.fluxo_batch_remove(self.b, int(iid)))
         self._shapes.pop(iid, None)

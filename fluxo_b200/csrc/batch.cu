@@ -766,8 +766,7 @@ int fluxo_batch_set_state(fluxo_batch* b, int id, const double* U) {
   BATCH_CUDA(b, cudaSetDevice(b->device));
   const Group& g = b->groups[I.group];
   const size_t eU = (size_t)5 * g.NP * g.NP * g.NP;
-  BATCH_CUDA(b, cudaMemcpyAsync(g.U + eU * I.elemOff, U, n * 8, cudaMemcpyHostToDevice, b->stream));
-  BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
+  BATCH_CUDA(b, copy_h2d(g.U + eU * I.elemOff, U, n * 8, b->stream));
   return FLUXO_OK;
 }
 

@@ -60,5 +60,8 @@ def test_batch_placement_and_readback(gpu_lib, big):
     t, n, err = op.time_disc(0.0, 1.0, 1)
     assert err == 0 and n == 1 and b.status(iid)[1] == 1
     assert np.array_equal(b.get_state(iid), op.get_state())
+    W = U[:, ::-1].copy()
+    b.set_state(iid, W)  # staged upload into the placed instance
+    assert np.array_equal(b.get_state(iid), W)
     op.close()
     b.close()
